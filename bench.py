@@ -1,0 +1,404 @@
+"""Benchmark: particle-steps/s of the stepping path on B200.
+
+Default workload (grid_bp_256): fixed-step PropagationBP (1 kpc, 5000 steps)
+of 10^6 protons (log-uniform 1-100 EeV, isotropic, from the origin) through a
+256^3 Kolmogorov Grid3f (201 MB float32, 5 kpc spacing, periodic, Brms 10 nG,
+lMin 10 kpc, lMax 500 kpc, seed 42).  One bench step = one full pass of that
+batch (every candidate to MaximumTrajectoryLength).
+
+Headline `value`: the mixed-precision form, state resident in HBM.  The same
+line carries the FP64 form's rate, the mixed form's per-candidate error
+against the FP64 form (which is bit-identical to the reference, see
+tests/test_gpu_parity.py), the end-to-end rate through crp_run() with host
+buffers, the roofline of the stepping kernel and the reference's own CPU
+ModuleList::run on this host's cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s, 1 B200: mixed-prec vs FP64 at stated error; adjoint cost/fwd"
+UNIT = "particle-steps/s"
+ALGO_BYTES_PER_STEP = 96  # 8 corners x 12 B Grid3f payload per field evaluation
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_dist(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ CPU legs
+def reference_cpu_rate(spec_fp64, cands, n_sample, threads):
+    """The reference's ModuleList::run (timing build) on n_sample candidates."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference, reference_available
+    if not reference_available(fast=True):
+        return None
+    ref = Reference(fast=True)
+    sub = cands.copy()
+    for name in sub.MEMBERS:
+        a = getattr(sub, name)
+        if a is not None:
+            setattr(sub, name, np.ascontiguousarray(a[:n_sample]))
+    sub.n = n_sample
+    steps, secs = ref.run(spec_fp64, sub, threads=threads)
+    return {"value": steps / secs, "steps": steps, "seconds": secs}
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's own CPU path, bounded samples."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference, reference_available
+    if not reference_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libcrp_ref_fast.so not built (needs the reference sources at build time)"}))
+        return 0
+    from crpropa3_b200 import _abi, plan as P, units as U
+    from crpropa3_b200.state import CandidateArrays
+    from crpropa3_b200 import turbulence
+    ref = Reference(fast=True)
+    threads = cpu_threads()
+    n = args.n or 1_000_000
+    n_sample = min(n, max(1000, 1500 * threads))
+    # grid: the reference's own MT19937 draws (ref_random), host FFT
+    grid = turbulence.grid_turbulence_with_draws(
+        args.grid_n, 5 * U.kpc, 10 * U.nG, 10 * U.kpc, 500 * U.kpc, 42,
+        lambda seed, count: ref.random(seed, 0, count))
+    spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (5 * U.kpc,) * 3)],
+                       [P.Propagation(_abi.PROP_BP, 0.42, 1 * U.kpc, 1 * U.kpc),
+                        P.MaxTrajectoryLength(args.track * U.kpc)])
+    ids, e, d = ref.sample_source(1, n_sample, (0, 0, 0), [1000010010], None, 1 * U.EeV,
+                                  100 * U.EeV, -1.0)
+    base = CandidateArrays(n_sample)
+    base.id[:] = ids
+    base.energy[:] = e
+    base.charge[:] = ref.charge(1000010010)
+    base.set_direction(d)
+    base.set_position(np.zeros((n_sample, 3)))
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        c = base.copy()
+        c.active[:] = 1
+        sub = c
+        sub_n = max(100, n_sample // 10)
+        for name in sub.MEMBERS:
+            a = getattr(sub, name)
+            if a is not None:
+                setattr(sub, name, np.ascontiguousarray(a[:sub_n]))
+        sub.n = sub_n
+        ref.run(spec, sub, threads=threads)
+    tot_steps, tot_secs = 0, 0.0
+    for _ in range(args.steps):
+        c = base.copy()
+        steps, secs = ref.run(spec, c, threads=threads)
+        tot_steps += steps
+        tot_secs += secs
+    value = tot_steps / tot_secs
+    sample = (f"{n_sample} of the {n} protons per step, full {args.track}-step trajectories, "
+              f"libcrp_ref_fast.so (-O3 -mavx2 -mfma), OpenMP schedule(static,100)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * tot_secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "candidates": n, "grid": f"{args.grid_n}^3",
+                       "steps_per_candidate": args.track},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="grid_bp_256")
+    ap.add_argument("--n", type=int, default=0)
+    ap.add_argument("--grid-n", type=int, default=256)
+    ap.add_argument("--track", type=int, default=5000, help="steps per candidate (1 kpc each)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    world, rank, local = setup_dist(args)
+    torch.cuda.set_device(local)
+    from crpropa3_b200 import _abi, engine, units as U, workloads as W
+    from crpropa3_b200.state import CandidateArrays
+
+    n = args.n or 1_000_000
+    dev = f"cuda:{local}"
+    t0 = time.time()
+    spec_mx, cands, grid = W.grid_bp_256(n=n, grid_n=args.grid_n, steps=args.track,
+                                         precision=_abi.PRECISION_MIXED, device=dev, seed=1 + rank)
+    spec_64, _, _ = W.grid_bp_256(n=1, grid_n=args.grid_n, steps=args.track,
+                                  precision=_abi.PRECISION_FP64, grid=grid)
+    plan_mx = engine.Plan(spec_mx)
+    plan_64 = engine.Plan(spec_64)
+    log(f"[bench] setup {time.time() - t0:.1f}s (grid {args.grid_n}^3, {n} candidates)")
+
+    d_init = cands.to_device(dev)
+    d_work = cands.to_device(dev)
+
+    def reset():
+        for name in d_work.MEMBERS:
+            a = getattr(d_work, name)
+            if a is not None:
+                a.copy_(getattr(d_init, name))
+
+    def one_step(plan):
+        reset()
+        return plan.run(d_work)
+
+    # warm-up (both forms)
+    for _ in range(args.warmup):
+        one_step(plan_mx)
+    for _ in range(min(args.warmup, 3)):
+        one_step(plan_64)
+    torch.cuda.synchronize()
+
+    # ---- timed: mixed form, device-resident
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    kernel_ms, steps_mx, launches = 0.0, 0, 0
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            st = one_step(plan_mx)
+            kernel_ms += st.device_ms
+            steps_mx += st.particle_steps
+            launches += st.launches
+        ev1.record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    total_steps = steps_mx * world  # weak scaling: each rank its own batch
+    value = total_steps / (ms_max / 1e3)
+    final_mx = d_work.to_host()
+
+    # ---- FP64 form
+    k64 = args.fp64_steps or max(1, min(args.steps, 3))
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0.record()
+    steps_64 = 0
+    kernel64_ms = 0.0
+    for _ in range(k64):
+        st = one_step(plan_64)
+        steps_64 += st.particle_steps
+        kernel64_ms += st.device_ms
+    ev1.record()
+    torch.cuda.synchronize()
+    ms64 = max_over_ranks(ev0.elapsed_time(ev1), world)
+    value_64 = steps_64 * world / (ms64 / 1e3)
+    final_64 = d_work.to_host()
+
+    # per-candidate error of the mixed form against the FP64 form
+    p_mx, p_64 = final_mx.position(), final_64.position()
+    err = np.linalg.norm(p_mx - p_64, axis=1) / np.linalg.norm(p_64, axis=1)
+
+    # ---- end to end through crp_run with pinned host buffers
+    host = cands.copy()
+    pinned = {}
+    for name in host.MEMBERS:
+        a = getattr(host, name)
+        if a is None:
+            continue
+        t = torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else
+                             a.view(np.int64) if a.dtype == np.uint64 else a).pin_memory()
+        pinned[name] = t
+    h_work = CandidateArrays.__new__(CandidateArrays)
+    h_work.n, h_work.device = n, None
+    for name in host.MEMBERS:
+        a = getattr(host, name)
+        setattr(h_work, name, None if a is None else pinned[name].numpy().view(a.dtype))
+    bytes_state = h_work.nbytes()
+    e2e_steps, e2e_s = 0, 0.0
+    k_e2e = max(1, min(args.steps, 3))
+    barrier(world)
+    for _ in range(k_e2e):
+        for name, t in pinned.items():  # fresh inputs each step
+            t.numpy()[...] = (getattr(host, name).view(t.numpy().dtype))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        st = plan_mx.run(h_work)
+        t2 = time.perf_counter()
+        e2e_steps += st.particle_steps
+        e2e_s += t2 - t1
+    e2e_s = max_over_ranks(e2e_s, world)
+    e2e_value = e2e_steps * world / e2e_s
+    # inputs: every member; outputs: the members crp_run copies back
+    out_members = ["x", "y", "z", "dx", "dy", "dz", "px", "py", "pz", "trajectory_length", "time",
+                   "current_step", "next_step", "flags", "active"]
+    d2h = sum(getattr(h_work, m).nbytes for m in out_members)
+
+    # ---- roofline of the stepping kernel (device_ms = CUDA events around its launches)
+    peak, peak_kind = measured_peaks()
+    achieved = ALGO_BYTES_PER_STEP * steps_mx / (kernel_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "basis": "96 B (8 corners x 12 B) per particle-step over the stepping kernel time"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = cpu_threads()
+        n_cpu = min(n, 1500 * threads)
+        r = reference_cpu_rate(spec_64, cands, n_cpu, threads)
+        if r is not None:
+            cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{n_cpu} of the {n} protons, full {args.track}-step trajectories, "
+                             f"{r['seconds']:.1f} s, libcrp_ref_fast.so (-O3 -mavx2 -mfma) with "
+                             f"OpenMP schedule(static,100)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "candidates": n, "grid": f"{args.grid_n}^3 float32 "
+                       "Kolmogorov, 5 kpc, periodic, Brms 10 nG", "propagation": "PropagationBP fixed 1 kpc",
+                       "steps_per_candidate": args.track, "precision": "mixed (FP32 field/rotation, FP64 accumulation)",
+                       "l2": "grid 201 MB > 126 MB L2 (inputs larger than L2)", "parallelism": f"replicas x{world}"},
+            "fp64": {"value": value_64, "unit": UNIT, "ms_per_step": ms64 / k64,
+                     "mixed_over_fp64": value / value_64},
+            "mixed_error_vs_fp64": {"max": float(err.max()), "median": float(np.median(err)),
+                                    "p99": float(np.quantile(err, 0.99)),
+                                    "measure": "|x_mixed - x_fp64| / |x_fp64| per candidate"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
+                    "d2h_bytes_per_step": d2h, "api": "crp_run (host arrays, pinned)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,179 @@
+"""ctypes mirror of include/crp_gpu.h and the loader of the engine library.
+
+The engine is the shared library ``crpropa3_b200/lib/libcrp_b200.so`` built by
+``__graft_entry__.build()`` (nvcc, sm_100a).  Loading fails loudly when the
+library is missing: there is no CPU fallback for the stepping path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
+
+ABI_VERSION = 1
+
+# crp_status
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_OUT_OF_MEMORY = 4
+ERR_TIMEOUT = 5
+ERR_CANCELLED = 6
+ERR_CAPACITY = 7
+ERR_NO_DEVICE = 8
+
+STATUS_NAMES = {
+    OK: "CRP_OK", ERR_INVALID_ARGUMENT: "CRP_ERR_INVALID_ARGUMENT",
+    ERR_UNSUPPORTED: "CRP_ERR_UNSUPPORTED", ERR_CUDA: "CRP_ERR_CUDA",
+    ERR_OUT_OF_MEMORY: "CRP_ERR_OUT_OF_MEMORY", ERR_TIMEOUT: "CRP_ERR_TIMEOUT",
+    ERR_CANCELLED: "CRP_ERR_CANCELLED", ERR_CAPACITY: "CRP_ERR_CAPACITY",
+    ERR_NO_DEVICE: "CRP_ERR_NO_DEVICE",
+}
+
+FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL = 1, 2, 3, 4
+MODULE_PROPAGATION, MODULE_MAX_TRAJECTORY_LENGTH, MODULE_OBSERVER = 1, 2, 3
+PROP_CK, PROP_BP, PROP_SDE = 1, 2, 3
+OBSERVER_SURFACE_SPHERE, OBSERVER_DETECT_ALL = 1, 2
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+FLAG_REJECTED, FLAG_DETECTED, FLAG_NAN = 1, 2, 4
+MODE_AUTO, MODE_CHUNKED, MODE_PERSISTENT = 0, 1, 2
+
+_d = C.c_double
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("values", _fp), ("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64),
+                ("origin", _d * 3), ("spacing", _d * 3), ("reflective", C.c_int32),
+                ("clip_volume", C.c_int32)]
+
+
+class PlaneWaveDesc(C.Structure):
+    _fields_ = [("n_modes", C.c_int32), ("seed", C.c_int32), ("xi", _dp), ("kappa", _dp),
+                ("k", _dp), ("beta", _dp), ("ak", _dp), ("brms", _d), ("lmin", _d),
+                ("lmax", _d), ("lbendover", _d), ("sindex", _d), ("qindex", _d)]
+
+
+class FieldComponent(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
+                ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
+                ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
+                ("toroidal_b0", _d)]
+
+
+class ModuleDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("propagator", C.c_int32), ("tolerance", _d),
+                ("min_step", _d), ("max_step", _d), ("sde_epsilon", _d), ("sde_alpha", _d),
+                ("sde_scale", _d), ("max_length", _d), ("per_candidate_length", C.c_int32),
+                ("observer_feature", C.c_int32), ("sphere_center", _d * 3),
+                ("sphere_radius", _d), ("deactivate_on_detection", C.c_int32),
+                ("record", C.c_int32)]
+
+
+class PlanDesc(C.Structure):
+    _fields_ = [("abi_version", C.c_uint32), ("precision", C.c_int32),
+                ("fields", C.POINTER(FieldComponent)), ("n_fields", C.c_int32),
+                ("n_modules", C.c_int32), ("modules", C.POINTER(ModuleDesc)),
+                ("seed", C.c_uint64)]
+
+
+CANDIDATE_FIELDS = [
+    ("id", C.c_int32), ("charge", _d), ("energy", _d), ("x", _d), ("y", _d), ("z", _d),
+    ("dx", _d), ("dy", _d), ("dz", _d), ("px", _d), ("py", _d), ("pz", _d),
+    ("trajectory_length", _d), ("time", _d), ("current_step", _d), ("next_step", _d),
+    ("active", C.c_uint8), ("flags", C.c_uint32), ("max_length", _d),
+    ("step_count", C.c_uint64),
+]
+
+
+class SourceDesc(C.Structure):
+    _fields_ = [("n_types", C.c_int32), ("spectrum", C.c_int32), ("ids", C.POINTER(C.c_int32)),
+                ("abundances", _dp), ("emin", _d), ("emax", _d), ("index", _d), ("energy", _d),
+                ("isotropic", C.c_int32), ("_pad0", C.c_int32), ("direction", _d * 3)]
+
+
+class OutputDesc(C.Structure):
+    _fields_ = [("columns", C.c_uint32), ("one_dimensional", C.c_int32), ("length_scale", _d),
+                ("time_scale", _d), ("energy_scale", _d), ("version", C.c_char_p)]
+
+
+class OutputRows(C.Structure):
+    _fields_ = [("serial", C.POINTER(C.c_uint64)), ("trajectory_length", _dp), ("time", _dp),
+                ("id", C.POINTER(C.c_int32)), ("energy", _dp), ("position", _dp),
+                ("direction", _dp), ("source_id", C.POINTER(C.c_int32)), ("source_energy", _dp),
+                ("source_position", _dp), ("source_direction", _dp), ("weight", _dp)]
+
+
+class Candidates(C.Structure):
+    _fields_ = [(name, C.POINTER(t)) for name, t in CANDIDATE_FIELDS]
+
+
+RECORD_FIELDS = [
+    ("index", C.c_uint64), ("module", C.c_int32), ("trajectory_length", _d), ("time", _d),
+    ("x", _d), ("y", _d), ("z", _d), ("dx", _d), ("dy", _d), ("dz", _d), ("energy", _d),
+    ("id", C.c_int32),
+]
+
+
+class Records(C.Structure):
+    _fields_ = [("capacity", C.c_uint64), ("count", C.POINTER(C.c_uint64))] + \
+               [(name, C.POINTER(t)) for name, t in RECORD_FIELDS]
+
+
+class RunOpts(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("block_size", C.c_int32), ("ctas_per_sm", C.c_int32),
+                ("steps_per_launch", C.c_int32), ("refill_threshold", C.c_int32),
+                ("_pad0", C.c_int32), ("max_steps", C.c_uint64),
+                ("cancel", C.POINTER(C.c_int32)), ("stream", C.c_void_p),
+                ("records", C.POINTER(Records))]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("particle_steps", C.c_uint64), ("tries", C.c_uint64),
+                ("field_evaluations", C.c_uint64), ("launches", C.c_uint64),
+                ("active_left", C.c_uint64), ("device_ms", _d)]
+
+
+_lib = None
+
+
+class CrpError(RuntimeError):
+    """A non-zero crp_status, carrying the status code and the library message."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load():
+    """Load libcrp_b200.so; raises if it is absent (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"crpropa3_b200: engine library {LIB_PATH} is missing; run "
+            "__graft_entry__.build() (nvcc, sm_100a) first")
+    lib = C.CDLL(LIB_PATH)
+    from . import _signatures
+    _signatures.declare(lib)
+    if lib.crp_abi_version() != ABI_VERSION:
+        raise RuntimeError("crpropa3_b200: ABI version mismatch between Python and the library")
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    lib = load()
+    buf = C.create_string_buffer(4096)
+    lib.crp_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+def check(status):
+    if status != OK:
+        raise CrpError(status, last_error())

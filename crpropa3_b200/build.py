@@ -1,0 +1,84 @@
+"""Build the engine library crpropa3_b200/lib/libcrp_b200.so for sm_100a.
+
+nvcc cross-compiles without a GPU.  The FP64 stepping translation unit is
+compiled with -fmad=false so that no multiply-add is contracted (bit parity
+with the reference built without FMA); the other units use the default
+contraction.  Objects go to _build/ at the repository root.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+OBJ = os.path.join(ROOT, "_build")
+LIB = os.path.join(PKG, "lib", "libcrp_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
+
+# source -> extra flags
+SOURCES = {
+    "step_fp64.cu": ["-fmad=false"],
+    "step_mixed.cu": [],
+    "adjoint.cu": ["-fmad=false"],
+    "persistent.cu": [],
+    "turbulence.cu": [],
+    "crp_engine.cu": [],
+    "host_tools.cpp": ["-Xcompiler", "-ffp-contract=off"],
+}
+LINK_LIBS = ["-lcufft"]
+
+
+def _nvcc():
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _compile(nvcc, src, flags, verbose):
+    out = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+    path = os.path.join(CSRC, src)
+    deps = [path] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(INCLUDE, "crp_gpu.h"))
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
+        return out
+    cmd = [nvcc] + ARCH + COMMON + flags
+    if src.endswith(".cu"):
+        cmd += ["-Xptxas", "-v"]
+    cmd += ["-c", path, "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr[-6000:]}")
+    with open(out + ".log", "w") as f:
+        f.write(r.stderr)
+    if verbose:
+        print(f"[build] {src}", file=sys.stderr)
+    return out
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    nvcc = _nvcc()
+    present = {s: f for s, f in SOURCES.items() if os.path.exists(os.path.join(CSRC, s))}
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(lambda kv: _compile(nvcc, kv[0], kv[1], verbose), present.items()))
+    if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
+        return LIB
+    cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-L/usr/local/cuda/lib64"] + LINK_LIBS
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stderr[-6000:]}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True))

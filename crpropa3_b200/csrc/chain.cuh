@@ -1,0 +1,211 @@
+// chain.cuh -- per-candidate register state, the counter-based random
+// stream, the break condition and observer modules, output records, and the
+// ModuleList loop.  Shared by the FP64 and the mixed-precision translation
+// units; the propagation modules come in through the Prop template argument.
+#pragma once
+
+#include "device_plan.cuh"
+#include "crp_gpu.h"
+
+namespace crp {
+
+// include/crpropa/Units.h:55, :114-115
+constexpr double kCLight = 2.99792458e8;
+constexpr double kPi = 3.14159265358979323846;
+#define CRP_KPC (1e3 * (648000 / 3.14159265358979323846 * 149597870700.0))
+
+// Candidate state while it is being stepped (Candidate.h:27).
+struct Cand {
+    double x, y, z;     // current position
+    double dx, dy, dz;  // current direction
+    double px, py, pz;  // previous position
+    double E, q;
+    double len, time, cur, next, maxlen;
+    uint64_t index, steps;
+    uint32_t flags;
+    int32_t id;
+    bool active;
+};
+
+__device__ __forceinline__ void load_cand(const DevState &s, uint64_t i, Cand &c) {
+    c.x = s.x[i]; c.y = s.y[i]; c.z = s.z[i];
+    c.dx = s.dx[i]; c.dy = s.dy[i]; c.dz = s.dz[i];
+    c.px = s.px[i]; c.py = s.py[i]; c.pz = s.pz[i];
+    c.E = s.energy[i]; c.q = s.charge[i];
+    c.len = s.len[i]; c.time = s.time[i]; c.cur = s.cur[i]; c.next = s.next[i];
+    c.maxlen = s.max_length ? s.max_length[i] : 0.0;
+    c.index = i;
+    c.steps = s.steps ? s.steps[i] : 0;
+    c.flags = s.flags[i];
+    c.id = s.id[i];
+    c.active = s.active[i] != 0;
+}
+
+__device__ __forceinline__ void store_cand(const DevState &s, const Cand &c) {
+    uint64_t i = c.index;
+    s.x[i] = c.x; s.y[i] = c.y; s.z[i] = c.z;
+    s.dx[i] = c.dx; s.dy[i] = c.dy; s.dz[i] = c.dz;
+    s.px[i] = c.px; s.py[i] = c.py; s.pz[i] = c.pz;
+    s.len[i] = c.len; s.time[i] = c.time; s.cur[i] = c.cur; s.next[i] = c.next;
+    if (s.steps) s.steps[i] = c.steps;
+    s.flags[i] = c.flags;
+    s.active[i] = c.active ? 1 : 0;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        uint32_t lo0 = 0xD2511F53u * ctr.x, hi0 = __umulhi(0xD2511F53u, ctr.x);
+        uint32_t lo1 = 0xCD9E8D57u * ctr.z, hi1 = __umulhi(0xCD9E8D57u, ctr.z);
+        ctr = make_uint4(hi1 ^ ctr.y ^ k0, lo1, hi0 ^ ctr.w ^ k1, lo0);
+    }
+    return ctr;
+}
+
+// The per-step stream of one candidate: word w of step s of candidate i is
+// word w%4 of Philox(ctr = {lo(4s+w/4), hi(4s+w/4), lo(i), hi(i)}, key = seed).
+struct Stream {
+    uint64_t seed, cand, step;
+    uint4 block;
+    int cursor;
+    __device__ uint32_t next_u32() {
+        int w = cursor++;
+        if ((w & 3) == 0) {
+            uint64_t c = step * 4 + (uint64_t)(w >> 2);
+            block = philox4x32_10(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)cand,
+                                             (uint32_t)(cand >> 32)),
+                                  (uint32_t)seed, (uint32_t)(seed >> 32));
+        }
+        switch (w & 3) {
+        case 0: return block.x;
+        case 1: return block.y;
+        case 2: return block.z;
+        default: return block.w;
+        }
+    }
+};
+
+__device__ __forceinline__ void write_record(const DevRecords &rec, const Cand &c, int module) {
+    if (!rec.count) return;
+    unsigned long long slot = atomicAdd(rec.count, 1ull);
+    if (slot >= rec.capacity) return;
+    rec.index[slot] = c.index;
+    rec.module[slot] = module;
+    rec.len[slot] = c.len;
+    rec.time[slot] = c.time;
+    rec.x[slot] = c.x; rec.y[slot] = c.y; rec.z[slot] = c.z;
+    rec.dx[slot] = c.dx; rec.dy[slot] = c.dy; rec.dz[slot] = c.dz;
+    rec.energy[slot] = c.E;
+    rec.id[slot] = c.id;
+}
+
+struct StepCount {
+    unsigned long long tries = 0;
+    unsigned long long evals = 0;
+};
+
+// MaximumTrajectoryLength::process (BreakCondition.cpp:42) and
+// AbstractCondition::reject (Module.cpp:25).
+__device__ __forceinline__ void max_trajectory_length(const DevModule &m, Cand &c,
+                                                      const DevRecords &rec, int mi) {
+    double maxLength = m.per_candidate ? c.maxlen : m.max_length;
+    if (c.len >= maxLength) {
+        if (m.record) write_record(rec, c, mi);
+        c.flags |= CRP_FLAG_REJECTED;
+        c.active = false;
+    } else {
+        double lim = maxLength - c.len;
+        c.next = (lim < c.next) ? lim : c.next;  // Candidate::limitNextStep (Candidate.cpp:102)
+    }
+}
+
+// Observer::process (Observer.cpp:27) with ObserverSurface(Sphere)
+// (Observer.cpp:394, Geometry.cpp:41) or ObserverDetectAll (Observer.cpp:93).
+__device__ __forceinline__ void observer(const DevModule &m, Cand &c, const DevRecords &rec,
+                                         int mi) {
+    bool detected;
+    if (m.observer == CRP_OBSERVER_SURFACE_SPHERE) {
+        double ax = c.x - m.cx, ay = c.y - m.cy, az = c.z - m.cz;
+        double bx = c.px - m.cx, by = c.py - m.cy, bz = c.pz - m.cz;
+        double cd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)), __dmul_rn(az, az))) - m.radius;
+        double pd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz))) - m.radius;
+        double lim = fabs(cd);
+        c.next = (lim < c.next) ? lim : c.next;
+        if (cd * pd > 0) detected = false;
+        else if (pd == 0) detected = false;
+        else detected = true;
+    } else {
+        detected = true;
+    }
+    if (detected) {
+        if (m.record) write_record(rec, c, mi);
+        c.flags |= CRP_FLAG_DETECTED;
+        if (m.deactivate) c.active = false;
+    }
+}
+
+// ModuleList::process (ModuleList.cpp.in:54): every module of the chain, in
+// order, whether or not an earlier module deactivated the candidate.
+template <class Prop>
+__device__ __forceinline__ void chain_process(const DevPlan &P, Cand &c, const DevRecords &rec,
+                                              StepCount &sc) {
+#pragma unroll 1
+    for (int mi = 0; mi < P.n_modules; mi++) {
+        const DevModule &m = P.modules[mi];
+        if (m.kind == CRP_MODULE_PROPAGATION) Prop::process(P, m, c, sc);
+        else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) max_trajectory_length(m, c, rec, mi);
+        else observer(m, c, rec, mi);
+    }
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Add this thread's counts to the run counters, one atomic per warp.
+__device__ __forceinline__ void flush_counters(DevCounters *cnt, unsigned long long steps,
+                                               const StepCount &sc, unsigned long long active) {
+    unsigned long long s = warp_sum(steps), t = warp_sum(sc.tries), e = warp_sum(sc.evals),
+                       a = warp_sum(active);
+    if ((threadIdx.x & 31) == 0) {
+        if (s) atomicAdd(&cnt->steps, s);
+        if (t) atomicAdd(&cnt->tries, t);
+        if (e) atomicAdd(&cnt->field_evals, e);
+        if (a) atomicAdd(&cnt->active_left, a);
+    }
+}
+
+// One thread per candidate, at most max_steps chain iterations per launch.
+// perm (optional) maps thread -> candidate index.
+template <class Prop>
+__device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, uint64_t n,
+                                           int max_steps, uint64_t step_cap,
+                                           DevCounters *cnt, const DevRecords &rec,
+                                           const uint32_t *perm) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    StepCount sc;
+    unsigned long long steps = 0, left = 0;
+    if (t < n) {
+        uint64_t i = perm ? perm[t] : t;
+        if (s.active[i]) {
+            Cand c;
+            load_cand(s, i, c);
+            int k = 0;
+            while (c.active && k < max_steps && (step_cap == 0 || c.steps < step_cap)) {
+                chain_process<Prop>(P, c, rec, sc);
+                c.steps++;
+                k++;
+            }
+            steps = (unsigned long long)k;
+            left = (c.active && (step_cap == 0 || c.steps < step_cap)) ? 1 : 0;
+            store_cand(s, c);
+        }
+    }
+    flush_counters(cnt, steps, sc, left);
+}
+
+}  // namespace crp

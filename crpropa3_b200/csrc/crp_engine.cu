@@ -1,0 +1,499 @@
+// crp_engine.cu -- host side of the C-ABI in include/crp_gpu.h: plan
+// validation and upload, the run loop over the stepping kernels, the
+// host-array path, field evaluation.
+//
+// The run loop replaces ModuleList::run(candidate_vector)
+// (src/ModuleList.cpp.in:97): instead of an OpenMP loop over heap
+// candidates, the structure-of-arrays state stays resident on the device and
+// the kernels advance every active candidate, one thread per candidate,
+// until it is inactive.  Cancellation (the reference's SIGINT flag,
+// ModuleList.cpp.in:110) is a host flag polled between launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "crp_gpu.h"
+#include "engine_internal.h"
+
+using namespace crp;
+
+namespace {
+
+thread_local std::string g_error;
+
+crp_status fail(crp_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return st;
+}
+
+crp_status cuda_fail(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(CRP_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    return fail(CRP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(call)                                        \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+    } while (0)
+
+bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
+
+}  // namespace
+
+namespace crp {
+void set_last_error(const char *msg) { g_error = msg; }
+}  // namespace crp
+
+struct crp_plan {
+    int device = 0;
+    int precision = CRP_PRECISION_FP64;
+    int fs = FS_GENERIC;
+    DevPlan dev{};
+    std::vector<void *> owned;  // device allocations of grids and tables
+    DevCounters *d_cnt = nullptr;
+    DevCounters *h_cnt = nullptr;  // pinned
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // device copies for crp_run() on host arrays
+    uint64_t scratch_n = 0;
+    void *scratch = nullptr;
+    uint64_t rec_cap = 0;
+    void *rec_scratch = nullptr;
+    int tuned_block = 0;
+
+    ~crp_plan() {
+        for (void *p : owned) cudaFree(p);
+        if (d_cnt) cudaFree(d_cnt);
+        if (h_cnt) cudaFreeHost(h_cnt);
+        if (scratch) cudaFree(scratch);
+        if (rec_scratch) cudaFree(rec_scratch);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+template <class T>
+crp_status upload(crp_plan *p, const T *host, size_t count, const T **out) {
+    void *d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(T) * count));
+    p->owned.push_back(d);
+    CUDA_TRY(cudaMemcpy(d, host, sizeof(T) * count, cudaMemcpyHostToDevice));
+    *out = static_cast<const T *>(d);
+    return CRP_OK;
+}
+
+crp_status validate_module(const crp_module_desc &m) {
+    if (m.kind == CRP_MODULE_PROPAGATION) {
+        const char *name = m.propagator == CRP_PROP_CK ? "PropagationCK"
+                         : m.propagator == CRP_PROP_BP ? "PropagationBP"
+                         : m.propagator == CRP_PROP_SDE ? "DiffusionSDE" : nullptr;
+        if (!name) return fail(CRP_ERR_UNSUPPORTED, "unknown propagator %d", m.propagator);
+        // setTolerance / setMinimumStep / setMaximumStep
+        // (PropagationCK.cpp:160-179, PropagationBP.cpp, DiffusionSDE.cpp)
+        if (m.tolerance > 1 || m.tolerance < 0)
+            return fail(CRP_ERR_INVALID_ARGUMENT, m.propagator == CRP_PROP_SDE
+                        ? "%s: tolerance error not in range 0-1" : "%s: target error not in range 0-1", name);
+        if (m.min_step < 0) return fail(CRP_ERR_INVALID_ARGUMENT, "%s: minStep < 0 ", name);
+        if (m.min_step > m.max_step) return fail(CRP_ERR_INVALID_ARGUMENT, "%s: minStep > maxStep", name);
+        if (!(m.max_step > 0)) return fail(CRP_ERR_INVALID_ARGUMENT, "%s: maxStep must be > 0", name);
+        if (m.propagator == CRP_PROP_SDE) {
+            if (m.sde_epsilon > 1 || m.sde_epsilon < 0)
+                return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: epsilon not in range 0-1");
+            if (m.sde_alpha > 2. || m.sde_alpha < 0)
+                return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: alpha not in range 0-2");
+            if (m.sde_scale < 0)
+                return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: Scale error: Scale < 0");
+        }
+    } else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
+    } else if (m.kind == CRP_MODULE_OBSERVER) {
+        if (m.observer_feature != CRP_OBSERVER_SURFACE_SPHERE && m.observer_feature != CRP_OBSERVER_DETECT_ALL)
+            return fail(CRP_ERR_UNSUPPORTED, "unsupported observer feature %d", m.observer_feature);
+    } else {
+        return fail(CRP_ERR_UNSUPPORTED, "unsupported module kind %d", m.kind);
+    }
+    return CRP_OK;
+}
+
+crp_status build_component(crp_plan *p, const crp_field_component &f, DevComponent &d) {
+    d.kind = f.kind;
+    d.periodic = f.periodic;
+    d.periodic_reflective = f.periodic_reflective;
+    for (int a = 0; a < 3; a++) {
+        d.po[a] = f.periodic_origin[a];
+        d.pe[a] = f.periodic_extends[a];
+        d.uniform[a] = f.uniform[a];
+    }
+    d.b0 = f.toroidal_b0;
+    if (f.periodic && !(f.periodic_extends[0] > 0 && f.periodic_extends[1] > 0 && f.periodic_extends[2] > 0))
+        return fail(CRP_ERR_INVALID_ARGUMENT, "PeriodicMagneticField: extends must be > 0");
+    if (f.kind == CRP_FIELD_GRID) {
+        const crp_grid3f_desc &g = f.grid;
+        if (!g.values || g.nx == 0 || g.ny == 0 || g.nz == 0)
+            return fail(CRP_ERR_INVALID_ARGUMENT, "Grid3f: empty grid");
+        if (g.nx > (1u << 20) || g.ny > (1u << 20) || g.nz > (1u << 20))
+            return fail(CRP_ERR_CAPACITY, "Grid3f: a dimension beyond 2^20 cells");
+        size_t cells = (size_t)g.nx * g.ny * g.nz;
+        DevGrid &dg = d.grid;
+        crp_status st = upload(p, g.values, cells * 3, &dg.values);
+        if (st) return st;
+        dg.values4 = nullptr;
+        if (p->precision == CRP_PRECISION_MIXED) {
+            // 16-byte cells: one aligned 128-bit load per corner
+            std::vector<float4> pad(cells);
+            for (size_t i = 0; i < cells; i++)
+                pad[i] = make_float4(g.values[3 * i], g.values[3 * i + 1], g.values[3 * i + 2], 0.f);
+            st = upload(p, pad.data(), cells, &dg.values4);
+            if (st) return st;
+        }
+        dg.nx = (int)g.nx; dg.ny = (int)g.ny; dg.nz = (int)g.nz;
+        dg.reflective = g.reflective;
+        dg.clip_volume = g.clip_volume;
+        dg.pow2 = is_pow2(g.nx) && is_pow2(g.ny) && is_pow2(g.nz);
+        // Grid::setOrigin (Grid.h:225): gridOrigin = origin + spacing/2
+        dg.gox = g.origin[0] + g.spacing[0] / 2;
+        dg.goy = g.origin[1] + g.spacing[1] / 2;
+        dg.goz = g.origin[2] + g.spacing[2] / 2;
+        dg.sx = g.spacing[0]; dg.sy = g.spacing[1]; dg.sz = g.spacing[2];
+        dg.inv_sx = 1.0 / g.spacing[0]; dg.inv_sy = 1.0 / g.spacing[1]; dg.inv_sz = 1.0 / g.spacing[2];
+        dg.ox = g.origin[0]; dg.oy = g.origin[1]; dg.oz = g.origin[2];
+        // edge = origin + Vector3d(Nx, Ny, Nz) * spacing (Grid.h:322)
+        dg.ex = g.origin[0] + (double)g.nx * g.spacing[0];
+        dg.ey = g.origin[1] + (double)g.ny * g.spacing[1];
+        dg.ez = g.origin[2] + (double)g.nz * g.spacing[2];
+    } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
+        const crp_plane_wave_desc &w = f.plane_wave;
+        if (w.n_modes <= 1)
+            return fail(CRP_ERR_INVALID_ARGUMENT,
+                        "PlaneWaveTurbulence: Nm <= 1. Specify at least two wavemodes in order to generate the k distribution properly.");
+        if (!w.xi || !w.kappa || !w.k || !w.beta || !w.ak)
+            return fail(CRP_ERR_INVALID_ARGUMENT, "PlaneWaveTurbulence: mode arrays missing");
+        int n = w.n_modes;
+        std::vector<double> m9((size_t)n * 9), kk((size_t)n * 4);
+        std::vector<float4> a32((size_t)n);
+        for (int i = 0; i < n; i++) {
+            for (int a = 0; a < 3; a++) {
+                m9[9 * i + a] = w.xi[3 * i + a];
+                m9[9 * i + 3 + a] = w.kappa[3 * i + a];
+                kk[4 * i + a] = w.k[i] * w.kappa[3 * i + a];
+            }
+            m9[9 * i + 6] = w.k[i];
+            m9[9 * i + 7] = w.beta[i];
+            m9[9 * i + 8] = w.ak[i];
+            kk[4 * i + 3] = w.beta[i];
+            a32[i] = make_float4((float)(w.ak[i] * w.xi[3 * i]), (float)(w.ak[i] * w.xi[3 * i + 1]),
+                                 (float)(w.ak[i] * w.xi[3 * i + 2]), 0.f);
+        }
+        crp_status st = upload(p, m9.data(), m9.size(), &d.pw.modes);
+        if (st) return st;
+        st = upload(p, kk.data(), kk.size(), &d.pw.kk);
+        if (st) return st;
+        st = upload(p, a32.data(), a32.size(), &d.pw.modes32);
+        if (st) return st;
+        d.pw.n = n;
+    } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {
+    } else {
+        return fail(CRP_ERR_UNSUPPORTED, "unsupported field kind %d", f.kind);
+    }
+    return CRP_OK;
+}
+
+crp_status ensure_counters(crp_plan *p) {
+    if (!p->d_cnt) CUDA_TRY(cudaMalloc(&p->d_cnt, sizeof(DevCounters)));
+    if (!p->h_cnt) CUDA_TRY(cudaMallocHost(&p->h_cnt, sizeof(DevCounters)));
+    if (!p->ev0) CUDA_TRY(cudaEventCreate(&p->ev0));
+    if (!p->ev1) CUDA_TRY(cudaEventCreate(&p->ev1));
+    return CRP_OK;
+}
+
+DevState to_dev_state(const crp_candidates &c) {
+    DevState s;
+    s.id = c.id; s.charge = c.charge; s.energy = c.energy;
+    s.x = c.x; s.y = c.y; s.z = c.z;
+    s.dx = c.dx; s.dy = c.dy; s.dz = c.dz;
+    s.px = c.px; s.py = c.py; s.pz = c.pz;
+    s.len = c.trajectory_length; s.time = c.time; s.cur = c.current_step; s.next = c.next_step;
+    s.active = c.active; s.flags = c.flags; s.max_length = c.max_length; s.steps = c.step_count;
+    return s;
+}
+
+DevRecords to_dev_records(const crp_records *r) {
+    DevRecords d{};
+    if (!r) return d;
+    d.capacity = r->capacity;
+    d.count = reinterpret_cast<unsigned long long *>(r->count);
+    d.index = r->index; d.module = r->module;
+    d.len = r->trajectory_length; d.time = r->time;
+    d.x = r->x; d.y = r->y; d.z = r->z;
+    d.dx = r->dx; d.dy = r->dy; d.dz = r->dz;
+    d.energy = r->energy; d.id = r->id;
+    return d;
+}
+
+bool needs_per_candidate(const crp_plan *p) {
+    for (int i = 0; i < p->dev.n_modules; i++)
+        if (p->dev.modules[i].kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH && p->dev.modules[i].per_candidate)
+            return true;
+    return false;
+}
+
+bool needs_step_count(const crp_plan *p) {
+    return p->dev.modules[p->dev.prop_index].propagator == CRP_PROP_SDE;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t crp_abi_version(void) { return CRP_ABI_VERSION; }
+
+crp_status crp_last_error(char *buffer, size_t size) {
+    if (!buffer || size == 0) return CRP_ERR_INVALID_ARGUMENT;
+    snprintf(buffer, size, "%s", g_error.c_str());
+    return CRP_OK;
+}
+
+crp_status crp_device_count(int32_t *count) {
+    if (!count) return fail(CRP_ERR_INVALID_ARGUMENT, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(CRP_ERR_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    *count = n;
+    return CRP_OK;
+}
+
+crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
+    if (!desc || !out) return fail(CRP_ERR_INVALID_ARGUMENT, "desc or plan pointer is NULL");
+    *out = nullptr;
+    if (desc->abi_version != CRP_ABI_VERSION)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "ABI version %u, library has %u", desc->abi_version, CRP_ABI_VERSION);
+    if (desc->precision != CRP_PRECISION_FP64 && desc->precision != CRP_PRECISION_MIXED)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "unknown precision %d", desc->precision);
+    if (desc->n_fields < 0 || desc->n_fields > kMaxFields)
+        return fail(CRP_ERR_UNSUPPORTED, "at most %d field components (got %d)", kMaxFields, desc->n_fields);
+    if (desc->n_modules < 1 || desc->n_modules > kMaxModules)
+        return fail(CRP_ERR_UNSUPPORTED, "1 to %d modules (got %d)", kMaxModules, desc->n_modules);
+    int nprop = 0, prop_index = -1;
+    for (int i = 0; i < desc->n_modules; i++) {
+        crp_status st = validate_module(desc->modules[i]);
+        if (st) return st;
+        if (desc->modules[i].kind == CRP_MODULE_PROPAGATION) { nprop++; prop_index = i; }
+    }
+    if (nprop != 1) return fail(CRP_ERR_UNSUPPORTED, "the device path needs exactly one propagation module (got %d)", nprop);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(CRP_ERR_NO_DEVICE, "no CUDA device visible");
+
+    crp_plan *p = new crp_plan();
+    cudaGetDevice(&p->device);
+    p->precision = desc->precision;
+    DevPlan &d = p->dev;
+    d.n_fields = desc->n_fields;
+    d.n_modules = desc->n_modules;
+    d.prop_index = prop_index;
+    d.seed = desc->seed;
+    for (int i = 0; i < desc->n_fields; i++) {
+        crp_status st = build_component(p, desc->fields[i], d.fields[i]);
+        if (st) { delete p; return st; }
+    }
+    for (int i = 0; i < desc->n_modules; i++) {
+        const crp_module_desc &m = desc->modules[i];
+        DevModule &dm = d.modules[i];
+        dm.kind = m.kind; dm.propagator = m.propagator;
+        dm.tolerance = m.tolerance; dm.min_step = m.min_step; dm.max_step = m.max_step;
+        dm.eps = m.sde_epsilon; dm.alpha = m.sde_alpha; dm.scale = m.sde_scale;
+        dm.max_length = m.max_length; dm.per_candidate = m.per_candidate_length;
+        dm.observer = m.observer_feature;
+        dm.cx = m.sphere_center[0]; dm.cy = m.sphere_center[1]; dm.cz = m.sphere_center[2];
+        dm.radius = m.sphere_radius;
+        dm.deactivate = m.deactivate_on_detection; dm.record = m.record;
+    }
+    if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_GRID)
+        p->fs = FS_GRID;
+    else if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_PLANE_WAVE)
+        p->fs = FS_PLANE_WAVE;
+    else
+        p->fs = FS_GENERIC;
+    crp_status st = ensure_counters(p);
+    if (st) { delete p; return st; }
+    *out = p;
+    return CRP_OK;
+}
+
+crp_status crp_plan_destroy(crp_plan *plan) {
+    delete plan;
+    return CRP_OK;
+}
+
+crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
+                          const crp_run_opts *opts, crp_run_stats *stats) {
+    if (!p || !c) return fail(CRP_ERR_INVALID_ARGUMENT, "plan or candidates is NULL");
+    crp_run_opts o{};
+    if (opts) o = *opts;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return CRP_OK;
+    if (!c->id || !c->charge || !c->energy || !c->x || !c->y || !c->z || !c->dx || !c->dy ||
+        !c->dz || !c->px || !c->py || !c->pz || !c->trajectory_length || !c->time ||
+        !c->current_step || !c->next_step || !c->active || !c->flags)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "a candidate array is NULL");
+    if (needs_per_candidate(p) && !c->max_length)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "per-candidate MaximumTrajectoryLength needs max_length");
+    if (needs_step_count(p) && !c->step_count)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE needs step_count (random stream counter)");
+    if (o.mode == CRP_MODE_PERSISTENT)
+        return fail(CRP_ERR_UNSUPPORTED, "persistent mode is not available in this build");
+    cudaStream_t st = (cudaStream_t)o.stream;
+    DevState s = to_dev_state(*c);
+    DevRecords rec = to_dev_records(o.records);
+    int block = o.block_size > 0 ? o.block_size : (p->tuned_block > 0 ? p->tuned_block : 128);
+    if (block % 32 || block > 1024) return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d", block);
+    int spl = o.steps_per_launch > 0 ? o.steps_per_launch : 4096;
+    double ms_total = 0;
+    uint64_t launches = 0;
+    for (;;) {
+        CUDA_TRY(cudaMemsetAsync(p->d_cnt, 0, sizeof(DevCounters), st));
+        CUDA_TRY(cudaEventRecord(p->ev0, st));
+        cudaError_t e = (p->precision == CRP_PRECISION_FP64)
+            ? launch_fp64_chunk(p->dev, s, n, spl, o.max_steps, p->d_cnt, rec, nullptr, p->fs, block, st)
+            : launch_mixed_chunk(p->dev, s, n, spl, o.max_steps, p->d_cnt, rec, nullptr, p->fs, block, st);
+        if (e != cudaSuccess) return cuda_fail(e, "stepping kernel launch");
+        CUDA_TRY(cudaEventRecord(p->ev1, st));
+        CUDA_TRY(cudaMemcpyAsync(p->h_cnt, p->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
+        ms_total += ms;
+        launches++;
+        if (stats) {
+            stats->particle_steps += p->h_cnt->steps;
+            stats->tries += p->h_cnt->tries;
+            stats->field_evaluations += p->h_cnt->field_evals;
+            stats->active_left = p->h_cnt->active_left;
+        }
+        if (p->h_cnt->active_left == 0) break;
+        if (o.cancel && *o.cancel) {
+            if (stats) { stats->launches = launches; stats->device_ms = ms_total; }
+            return fail(CRP_ERR_CANCELLED, "run cancelled by the host flag");
+        }
+    }
+    if (stats) { stats->launches = launches; stats->device_ms = ms_total; }
+    return CRP_OK;
+}
+
+crp_status crp_run(crp_plan *p, const crp_candidates *h, uint64_t n, const crp_run_opts *opts,
+                   crp_run_stats *stats) {
+    if (!p || !h) return fail(CRP_ERR_INVALID_ARGUMENT, "plan or candidates is NULL");
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return CRP_OK;
+    crp_run_opts o{};
+    if (opts) o = *opts;
+    cudaStream_t st = (cudaStream_t)o.stream;
+    const bool per = h->max_length != nullptr, steps = h->step_count != nullptr;
+    // 17 doubles (with max_length and step_count) + id + flags + active per candidate
+    const size_t per_cand = 17 * 8 + 4 + 4 + 1;
+    const size_t slack = 32 * 256;
+    if (p->scratch_n < n) {
+        if (p->scratch) { cudaFree(p->scratch); p->scratch = nullptr; p->scratch_n = 0; }
+        CUDA_TRY(cudaMalloc(&p->scratch, per_cand * n + slack));
+        p->scratch_n = n;
+    }
+    char *base = static_cast<char *>(p->scratch);
+    crp_candidates d{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) { void *r = base + off; off += (bytes + 255) / 256 * 256; return r; };
+    // layout: doubles first (aligned), then 4-byte and 1-byte members
+    d.charge = (double *)take(8 * n); d.energy = (double *)take(8 * n);
+    d.x = (double *)take(8 * n); d.y = (double *)take(8 * n); d.z = (double *)take(8 * n);
+    d.dx = (double *)take(8 * n); d.dy = (double *)take(8 * n); d.dz = (double *)take(8 * n);
+    d.px = (double *)take(8 * n); d.py = (double *)take(8 * n); d.pz = (double *)take(8 * n);
+    d.trajectory_length = (double *)take(8 * n); d.time = (double *)take(8 * n);
+    d.current_step = (double *)take(8 * n); d.next_step = (double *)take(8 * n);
+    d.max_length = per ? (double *)take(8 * n) : nullptr;
+    d.step_count = steps ? (uint64_t *)take(8 * n) : nullptr;
+    d.id = (int32_t *)take(4 * n); d.flags = (uint32_t *)take(4 * n);
+    d.active = (uint8_t *)take(n);
+    if (off > per_cand * n + slack) return fail(CRP_ERR_CUDA, "scratch layout overflow");
+#define H2D(m, bytes) CUDA_TRY(cudaMemcpyAsync(d.m, h->m, (bytes), cudaMemcpyHostToDevice, st))
+#define D2H(m, bytes) CUDA_TRY(cudaMemcpyAsync(h->m, d.m, (bytes), cudaMemcpyDeviceToHost, st))
+    H2D(charge, 8 * n); H2D(energy, 8 * n); H2D(x, 8 * n); H2D(y, 8 * n); H2D(z, 8 * n);
+    H2D(dx, 8 * n); H2D(dy, 8 * n); H2D(dz, 8 * n); H2D(px, 8 * n); H2D(py, 8 * n); H2D(pz, 8 * n);
+    H2D(trajectory_length, 8 * n); H2D(time, 8 * n); H2D(current_step, 8 * n); H2D(next_step, 8 * n);
+    if (per) H2D(max_length, 8 * n);
+    if (steps) H2D(step_count, 8 * n);
+    H2D(id, 4 * n); H2D(flags, 4 * n); H2D(active, n);
+    // records: device buffer of the same capacity, copied back afterwards
+    crp_records drec{};
+    crp_records *hrec = o.records;
+    if (hrec) {
+        uint64_t cap = hrec->capacity;
+        size_t rbytes = 8 + cap * (8 + 4 + 10 * 8 + 4) + 16 * 256;
+        if (p->rec_cap < cap || !p->rec_scratch) {
+            if (p->rec_scratch) cudaFree(p->rec_scratch);
+            p->rec_scratch = nullptr;
+            CUDA_TRY(cudaMalloc(&p->rec_scratch, rbytes));
+            p->rec_cap = cap;
+        }
+        char *rb = static_cast<char *>(p->rec_scratch);
+        size_t ro = 0;
+        auto rtake = [&](size_t bytes) { void *r = rb + ro; ro += (bytes + 255) / 256 * 256; return r; };
+        drec.capacity = cap;
+        drec.count = (uint64_t *)rtake(8);
+        drec.index = (uint64_t *)rtake(8 * cap); drec.module = (int32_t *)rtake(4 * cap);
+        drec.trajectory_length = (double *)rtake(8 * cap); drec.time = (double *)rtake(8 * cap);
+        drec.x = (double *)rtake(8 * cap); drec.y = (double *)rtake(8 * cap); drec.z = (double *)rtake(8 * cap);
+        drec.dx = (double *)rtake(8 * cap); drec.dy = (double *)rtake(8 * cap); drec.dz = (double *)rtake(8 * cap);
+        drec.energy = (double *)rtake(8 * cap); drec.id = (int32_t *)rtake(4 * cap);
+        CUDA_TRY(cudaMemcpyAsync(drec.count, hrec->count, 8, cudaMemcpyHostToDevice, st));
+        o.records = &drec;
+    }
+    crp_status rs = crp_run_device(p, &d, n, &o, stats);
+    if (rs != CRP_OK && rs != CRP_ERR_CANCELLED) return rs;
+    D2H(x, 8 * n); D2H(y, 8 * n); D2H(z, 8 * n); D2H(dx, 8 * n); D2H(dy, 8 * n); D2H(dz, 8 * n);
+    D2H(px, 8 * n); D2H(py, 8 * n); D2H(pz, 8 * n);
+    D2H(trajectory_length, 8 * n); D2H(time, 8 * n); D2H(current_step, 8 * n); D2H(next_step, 8 * n);
+    if (steps) D2H(step_count, 8 * n);
+    D2H(flags, 4 * n); D2H(active, n);
+    if (hrec) {
+        CUDA_TRY(cudaMemcpyAsync(hrec->count, drec.count, 8, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        uint64_t k = std::min<uint64_t>(*hrec->count, hrec->capacity);
+        if (k) {
+#define RD2H(m, sz) CUDA_TRY(cudaMemcpyAsync(hrec->m, drec.m, (sz) * k, cudaMemcpyDeviceToHost, st))
+            RD2H(index, 8); RD2H(module, 4); RD2H(trajectory_length, 8); RD2H(time, 8);
+            RD2H(x, 8); RD2H(y, 8); RD2H(z, 8); RD2H(dx, 8); RD2H(dy, 8); RD2H(dz, 8);
+            RD2H(energy, 8); RD2H(id, 4);
+#undef RD2H
+        }
+    }
+#undef H2D
+#undef D2H
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return rs;
+}
+
+crp_status crp_field_eval(crp_plan *p, uint64_t n, const double *pos, double *out, void *stream) {
+    if (!p || (n && (!pos || !out))) return fail(CRP_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaError_t e = (p->precision == CRP_PRECISION_FP64)
+        ? launch_fp64_field(p->dev, n, pos, out, (cudaStream_t)stream)
+        : launch_mixed_field(p->dev, n, pos, out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "field kernel launch");
+    return CRP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// device_plan.cuh -- device-side description of a stepping plan and the
+// candidate state layout.  Plain structs passed by value as kernel
+// parameters (they live in the constant bank, so every lane reads them as a
+// uniform broadcast).
+#pragma once
+
+#include <cstdint>
+
+namespace crp {
+
+constexpr int kMaxFields = 4;
+constexpr int kMaxModules = 8;
+
+struct DevGrid {
+    const float *values;   // packed Vector3f cells, 12 B each (Grid.h:338 order)
+    const float4 *values4; // the same cells padded to 16 B (mixed form), or null
+    int nx, ny, nz;
+    int reflective;
+    int clip_volume;
+    int pow2;              // nx, ny, nz all powers of two (periodic wrap by mask)
+    double gox, goy, goz;  // gridOrigin = origin + spacing/2 (Grid.h:227)
+    double sx, sy, sz;     // spacing
+    double inv_sx, inv_sy, inv_sz;  // 1/spacing (mixed form only)
+    double ox, oy, oz;     // origin (clipVolume test)
+    double ex, ey, ez;     // origin + N*spacing (clipVolume test, Grid.h:322)
+};
+
+struct DevPlaneWave {
+    const double *modes;   // FP64 form: per mode {xi x y z, kappa x y z, k, beta, Ak} (9 doubles)
+    const float4 *modes32; // mixed form: per mode {k*kappa (FP64 split), Ak*xi} (see step_mixed.cu)
+    const double *kk;      // mixed form: per mode k*kappa as 3 doubles + beta (4 doubles)
+    int n;
+};
+
+struct DevComponent {
+    int kind;       // crp_field_kind
+    int periodic;
+    int periodic_reflective;
+    int pad;
+    double po[3], pe[3];
+    DevGrid grid;
+    DevPlaneWave pw;
+    double uniform[3];
+    double b0;
+};
+
+struct DevModule {
+    int kind;        // crp_module_kind
+    int propagator;  // crp_propagator
+    double tolerance, min_step, max_step;
+    double eps, alpha, scale;
+    double max_length;
+    int per_candidate;
+    int observer;    // crp_observer_feature
+    double cx, cy, cz, radius;
+    int deactivate;
+    int record;
+};
+
+struct DevPlan {
+    int n_fields;
+    int n_modules;
+    int prop_index;  // position of the propagation module in the chain
+    int pad;
+    uint64_t seed;
+    DevComponent fields[kMaxFields];
+    DevModule modules[kMaxModules];
+};
+
+// Candidate arrays (include/crp_gpu.h crp_candidates), device pointers.
+struct DevState {
+    int32_t *id;
+    double *charge, *energy;
+    double *x, *y, *z;
+    double *dx, *dy, *dz;
+    double *px, *py, *pz;
+    double *len, *time, *cur, *next;
+    uint8_t *active;
+    uint32_t *flags;
+    double *max_length;
+    uint64_t *steps;
+};
+
+struct DevRecords {
+    uint64_t capacity;
+    unsigned long long *count;
+    uint64_t *index;
+    int32_t *module;
+    double *len, *time, *x, *y, *z, *dx, *dy, *dz, *energy;
+    int32_t *id;
+};
+
+// Run counters, accumulated with one atomic per warp.
+struct DevCounters {
+    unsigned long long steps;
+    unsigned long long tries;
+    unsigned long long field_evals;
+    unsigned long long active_left;
+    unsigned long long queue_head;   // persistent mode: next candidate to take
+    unsigned long long pending_count;
+    unsigned long long status;       // non-zero: a bounded wait ran out / bad state
+    unsigned long long pad;
+};
+
+}  // namespace crp

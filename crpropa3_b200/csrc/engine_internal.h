@@ -1,0 +1,40 @@
+// engine_internal.h -- declarations shared between the host engine
+// (crp_engine.cu) and the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_plan.cuh"
+
+namespace crp {
+
+// Field signature the stepping kernels are specialised for.
+enum FieldSig {
+    FS_GENERIC = 0,    // any sum of (possibly periodic) components
+    FS_GRID = 1,       // one MagneticFieldGrid, not wrapped
+    FS_PLANE_WAVE = 2  // one PlaneWaveTurbulence, not wrapped
+};
+
+// step_fp64.cu
+cudaError_t launch_fp64_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
+                              uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
+                              const uint32_t *perm, int fs, int block, cudaStream_t st);
+cudaError_t launch_fp64_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
+                              cudaStream_t st);
+
+// step_mixed.cu
+cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
+                               uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
+                               const uint32_t *perm, int fs, int block, cudaStream_t st);
+cudaError_t launch_mixed_persistent(const DevPlan &P, const DevState &s, uint64_t n,
+                                    uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
+                                    int fs, int block, int grid, int refill,
+                                    unsigned long long deadline_ns, uint32_t *pending_in,
+                                    uint64_t n_pending_in, uint32_t *pending_out,
+                                    cudaStream_t st);
+cudaError_t launch_mixed_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
+                               cudaStream_t st);
+
+}  // namespace crp

@@ -1,0 +1,345 @@
+// host_tools.cpp -- host-side set-up and output of the stepping engine:
+//   * crpropa::Random (MT19937, src/Random.cpp) for the draws the reference
+//     makes on the host: PlaneWaveTurbulence modes, Source features;
+//   * PlaneWaveTurbulence mode set-up (PlaneWaveTurbulence.cpp:79-229);
+//   * Source sampling for the stepping workloads (Source.cpp);
+//   * particle charge (ParticleState::setId, ParticleState.cpp:50);
+//   * the TextOutput line formatter (TextOutput.cpp:55, :166).
+// No device is needed for any of these.
+#include <cinttypes>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "crp_gpu.h"
+
+namespace crp {
+void set_last_error(const char *msg);  // crp_engine.cu
+}
+
+namespace {
+
+crp_status host_fail(crp_status st, const char *msg) {
+    crp::set_last_error(msg);
+    return st;
+}
+
+// MT19937 with the seeding, tempering and real conversions of crpropa::Random.
+class Mt {
+    uint32_t s_[624];
+    int left_ = 0, next_ = 0;
+    static uint32_t twist(uint32_t m, uint32_t a, uint32_t b) {
+        uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
+        return m ^ (y >> 1) ^ ((0u - (b & 1u)) & 0x9908b0dfu);
+    }
+    void reload() {
+        int i = 0;
+        for (; i < 624 - 397; i++) s_[i] = twist(s_[i + 397], s_[i], s_[i + 1]);
+        for (; i < 623; i++) s_[i] = twist(s_[i - (624 - 397)], s_[i], s_[i + 1]);
+        s_[623] = twist(s_[396], s_[623], s_[0]);
+        left_ = 624;
+        next_ = 0;
+    }
+
+public:
+    explicit Mt(uint32_t seed) {
+        s_[0] = seed;
+        for (int i = 1; i < 624; i++) s_[i] = 1812433253u * (s_[i - 1] ^ (s_[i - 1] >> 30)) + (uint32_t)i;
+        reload();
+    }
+    uint32_t u32() {
+        if (left_ == 0) reload();
+        --left_;
+        uint32_t y = s_[next_++];
+        y ^= y >> 11;
+        y ^= (y << 7) & 0x9d2c5680u;
+        y ^= (y << 15) & 0xefc60000u;
+        return y ^ (y >> 18);
+    }
+    double rand() { return double(u32()) * (1.0 / 4294967295.0); }
+    double uniform(double a, double b) { return a + (b - a) * rand(); }
+    void vector(double &x, double &y, double &z) {
+        double zz = uniform(-1.0, 1.0);
+        double t = uniform(-1.0 * M_PI, M_PI);
+        double r = std::sqrt(1 - zz * zz);
+        x = r * std::cos(t); y = r * std::sin(t); z = zz;
+    }
+    double power_law(double index, double mn, double mx) {
+        if (std::fabs(index + 1.0) < 2.220446049250313e-16) {
+            double p1 = std::log(mx), p2 = std::log(mn);
+            return std::exp((p1 - p2) * rand() + p2);
+        }
+        double p1 = std::pow(mx, index + 1), p2 = std::pow(mn, index + 1);
+        double ex = 1 / (index + 1);
+        return std::pow((p1 - p2) * rand() + p2, ex);
+    }
+};
+
+// HepPID nucleus test for +/-10LZZZAAAI ids (L = 0, A >= Z), 2212 and 2112.
+bool nucleus(int32_t id, int &Z) {
+    int64_t a = id < 0 ? -(int64_t)id : id;
+    if (a == 2212) { Z = 1; return true; }
+    if (a == 2112) { Z = 0; return true; }
+    if (a >= 1000000000LL && a < 2000000000LL && (a / 100000000) % 10 == 0) {
+        int z = (int)((a / 10000) % 1000), A = (int)((a / 10) % 1000);
+        if (A >= z) { Z = z; return true; }
+    }
+    return false;
+}
+
+const double kEplus = 1.602176487e-19;  // Units.h:54
+
+}  // namespace
+
+extern "C" {
+
+crp_status crp_particle_charge(int32_t id, double *charge) {
+    if (!charge) return host_fail(CRP_ERR_INVALID_ARGUMENT, "charge is NULL");
+    int Z;
+    if (nucleus(id, Z)) {
+        // ParticleState::setId: chargeNumber(id) * eplus, negated for anti-nuclei
+        double q = Z * kEplus;
+        if (id < 0) q *= -1;
+        *charge = q;
+        return CRP_OK;
+    }
+    switch (id) {
+    case 11: case 13: case 15: *charge = -1 * kEplus; return CRP_OK;
+    case -11: case -13: case -15: *charge = 1 * kEplus; return CRP_OK;
+    case 22: case 12: case -12: case 14: case -14: case 16: case -16: *charge = 0; return CRP_OK;
+    default: break;
+    }
+    return host_fail(CRP_ERR_UNSUPPORTED, "particle id outside the charge table of the device path");
+}
+
+crp_status crp_random_draws(uint32_t seed, int32_t kind, uint64_t n, double a, double b, double c,
+                            double *out) {
+    if (!out && n) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    Mt r(seed);
+    for (uint64_t i = 0; i < n; i++) {
+        switch (kind) {
+        case 0: out[i] = r.rand(); break;
+        case 1: out[i] = r.uniform(a, b); break;
+        case 2: r.vector(out[3 * i], out[3 * i + 1], out[3 * i + 2]); break;
+        case 3: out[i] = r.power_law(a, b, c); break;
+        case 6: out[i] = (double)r.u32(); break;
+        default: return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown draw kind");
+        }
+    }
+    return CRP_OK;
+}
+
+crp_status crp_plane_wave_modes(double brms, double lmin, double lmax, double lbendover,
+                                double sindex, double qindex, int32_t nm, int32_t seed,
+                                double *xi, double *kappa, double *k, double *beta, double *ak) {
+    if (nm <= 1)
+        return host_fail(CRP_ERR_INVALID_ARGUMENT,
+                         "PlaneWaveTurbulence: Nm <= 1. Specify at least two wavemodes in order to generate the k distribution properly.");
+    if (lmin > lmax) return host_fail(CRP_ERR_INVALID_ARGUMENT, "TurbulenceSpectrum: lMin > lMax");
+    if (lmin <= 0) return host_fail(CRP_ERR_INVALID_ARGUMENT, "TurbulenceSpectrum: lMin <= 0");
+    if (!xi || !kappa || !k || !beta || !ak) return host_fail(CRP_ERR_INVALID_ARGUMENT, "NULL mode array");
+    if (seed == 0)
+        return host_fail(CRP_ERR_INVALID_ARGUMENT,
+                         "PlaneWaveTurbulence: seed 0 draws from /dev/urandom; give a non-zero seed");
+    Mt r((uint32_t)seed);
+    const double kmax = 2 * M_PI / lmin, kmin = 2 * M_PI / lmax;
+    const double delta = std::log10(kmax / kmin);
+    for (int i = 0; i < nm; i++)
+        k[i] = std::pow(10, std::log10(kmin) + ((double)i) / ((double)(nm - 1)) * delta);
+    const double delta_k0 = (k[1] - k[0]) / k[1];
+    double sum = 0;
+    for (int i = 0; i < nm; i++) {
+        double kk = k[i];
+        double kHat = kk * lbendover;
+        // TurbulenceSpectrum::energySpectrum (TurbulentField.h:75)
+        double es = std::pow(kHat, qindex) / std::pow(1.0 + kHat * kHat, (sindex + qindex) / 2.0 + 1.0);
+        double Gk = es * (1 + kHat * kHat);
+        ak[i] = Gk * delta_k0 * kk;
+        sum += ak[i];
+        double phi = r.uniform(-M_PI, M_PI);
+        double costheta = r.uniform(-1., 1.);
+        double sintheta = std::sqrt(1 - costheta * costheta);
+        double alpha = r.uniform(0, 2 * M_PI);
+        double b = r.uniform(0, 2 * M_PI);
+        kappa[3 * i] = sintheta * std::cos(phi);
+        kappa[3 * i + 1] = sintheta * std::sin(phi);
+        kappa[3 * i + 2] = costheta;
+        xi[3 * i] = costheta * std::cos(phi) * std::cos(alpha) + std::sin(phi) * std::sin(alpha);
+        xi[3 * i + 1] = costheta * std::sin(phi) * std::cos(alpha) - std::cos(phi) * std::sin(alpha);
+        xi[3 * i + 2] = -sintheta * std::cos(alpha);
+        beta[i] = b;
+    }
+    for (int i = 0; i < nm; i++) ak[i] = std::sqrt(2 * ak[i] / sum) * brms;
+    return CRP_OK;
+}
+
+crp_status crp_source_sample(const crp_source_desc *src, uint32_t seed, uint64_t n, int32_t *id,
+                             double *energy, double *dir_xyz) {
+    if (!src || (n && (!id || !energy || !dir_xyz)))
+        return host_fail(CRP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (src->n_types < 1 || src->n_types > 256 || !src->ids)
+        return host_fail(CRP_ERR_INVALID_ARGUMENT, "SourceMultipleParticleTypes: no nuclei set");
+    if (src->spectrum && ((src->emin < 0) || (src->emax < src->emin)))
+        return host_fail(CRP_ERR_INVALID_ARGUMENT, "Power law distribution only possible for 0 <= min <= max");
+    std::vector<double> cdf((size_t)src->n_types);
+    double acc = 0;
+    for (int i = 0; i < src->n_types; i++) {
+        acc = (i ? cdf[i - 1] : 0) + (src->abundances ? src->abundances[i] : 1.0);
+        cdf[i] = acc;
+    }
+    Mt r(seed);
+    for (uint64_t i = 0; i < n; i++) {
+        int32_t pid = src->ids[0];
+        if (src->n_types > 1) {  // Random::randBin: lower_bound over the CDF
+            double u = r.rand() * cdf.back();
+            int k = 0;
+            while (k < src->n_types && cdf[k] < u) k++;
+            pid = src->ids[k];
+        }
+        id[i] = pid;
+        energy[i] = src->spectrum ? r.power_law(src->index, src->emin, src->emax) : src->energy;
+        double x, y, z;
+        if (src->isotropic) r.vector(x, y, z);
+        else { x = src->direction[0]; y = src->direction[1]; z = src->direction[2]; }
+        double nrm = std::sqrt(x * x + y * y + z * z);  // ParticleState::setDirection
+        dir_xyz[i] = x / nrm; dir_xyz[n + i] = y / nrm; dir_xyz[2 * n + i] = z / nrm;
+    }
+    return CRP_OK;
+}
+
+// TextOutput line (TextOutput.cpp:166-292): the enabled columns of the
+// Output column bitset in the reference's order and printf formats.
+static void format_row(const crp_output_desc *d, const crp_output_rows *r, uint64_t i,
+                       std::string &out) {
+    char buf[2048];
+    size_t p = 0;
+    const uint32_t f = d->columns;
+    auto on = [&](int c) { return (f >> c) & 1u; };
+    auto put = [&](const char *fmt, double v) { p += snprintf(buf + p, sizeof(buf) - p, fmt, v); };
+    auto put3 = [&](const double *v, double s) {
+        p += snprintf(buf + p, sizeof(buf) - p, "%8.5E\t%8.5E\t%8.5E\t", v[3 * i] / s, v[3 * i + 1] / s, v[3 * i + 2] / s);
+    };
+    auto putu = [&](uint64_t v) { p += snprintf(buf + p, sizeof(buf) - p, "%10" PRIu64 "\t", v); };
+    auto puti = [&](int v) { p += snprintf(buf + p, sizeof(buf) - p, "%10i\t", v); };
+    const bool d1 = d->one_dimensional != 0;
+    if (on(CRP_COL_TRAJECTORY_LENGTH)) put("%8.5E\t", r->trajectory_length[i] / d->length_scale);
+    if (on(CRP_COL_TIME)) put("%8.5E\t", r->time[i] / d->time_scale);
+    if (on(CRP_COL_REDSHIFT)) put("%1.5E\t", 0.0);
+    if (on(CRP_COL_SERIAL_NUMBER)) putu(r->serial ? r->serial[i] : 0);
+    if (on(CRP_COL_CURRENT_ID)) puti(r->id[i]);
+    if (on(CRP_COL_CURRENT_ENERGY)) put("%8.5E\t", r->energy[i] / d->energy_scale);
+    if (on(CRP_COL_CURRENT_POSITION)) {
+        if (d1) put("%8.5E\t", r->position[3 * i] / d->length_scale);
+        else put3(r->position, d->length_scale);
+    }
+    if (on(CRP_COL_CURRENT_DIRECTION) && !d1) put3(r->direction, 1.0);
+    // primaries: source and created serial numbers are the candidate's own (Candidate.cpp:240-252)
+    if (on(CRP_COL_SERIAL_NUMBER)) putu(r->serial ? r->serial[i] : 0);
+    if (on(CRP_COL_SOURCE_ID)) puti(r->source_id[i]);
+    if (on(CRP_COL_SOURCE_ENERGY)) put("%8.5E\t", r->source_energy[i] / d->energy_scale);
+    if (on(CRP_COL_SOURCE_POSITION)) {
+        if (d1) put("%8.5E\t", r->source_position[3 * i] / d->length_scale);
+        else put3(r->source_position, d->length_scale);
+    }
+    if (on(CRP_COL_SOURCE_DIRECTION) && !d1) put3(r->source_direction, 1.0);
+    if (on(CRP_COL_SERIAL_NUMBER)) putu(r->serial ? r->serial[i] : 0);
+    if (on(CRP_COL_CREATED_ID)) puti(r->source_id[i]);
+    if (on(CRP_COL_CREATED_ENERGY)) put("%8.5E\t", r->source_energy[i] / d->energy_scale);
+    if (on(CRP_COL_CREATED_POSITION)) {
+        if (d1) put("%8.5E\t", r->source_position[3 * i] / d->length_scale);
+        else put3(r->source_position, d->length_scale);
+    }
+    if (on(CRP_COL_CREATED_DIRECTION) && !d1) put3(r->source_direction, 1.0);
+    if (on(CRP_COL_WEIGHT)) put("%8.5E\t", r->weight ? r->weight[i] : 1.0);
+    if (on(CRP_COL_CANDIDATE_TAG)) p += snprintf(buf + p, sizeof(buf) - p, "%s\t", "PRIM");
+    if (p == 0) return;
+    buf[p - 1] = '\n';
+    out.append(buf, p);
+}
+
+// TextOutput::printHeader (TextOutput.cpp:55)
+static void format_header(const crp_output_desc *d, std::string &o) {
+    const uint32_t f = d->columns;
+    auto on = [&](int c) { return (f >> c) & 1u; };
+    const bool d1 = d->one_dimensional != 0;
+    char buf[256];
+    o += "#";
+    if (on(CRP_COL_TRAJECTORY_LENGTH)) o += "\tD";
+    if (on(CRP_COL_TIME)) o += "\ttime";
+    if (on(CRP_COL_REDSHIFT)) o += "\tz";
+    if (on(CRP_COL_SERIAL_NUMBER)) o += "\tSN";
+    if (on(CRP_COL_CURRENT_ID)) o += "\tID";
+    if (on(CRP_COL_CURRENT_ENERGY)) o += "\tE";
+    if (on(CRP_COL_CURRENT_POSITION) && d1) o += "\tX";
+    if (on(CRP_COL_CURRENT_POSITION) && !d1) o += "\tX\tY\tZ";
+    if (on(CRP_COL_CURRENT_DIRECTION) && !d1) o += "\tPx\tPy\tPz";
+    if (on(CRP_COL_SERIAL_NUMBER)) o += "\tSN0";
+    if (on(CRP_COL_SOURCE_ID)) o += "\tID0";
+    if (on(CRP_COL_SOURCE_ENERGY)) o += "\tE0";
+    if (on(CRP_COL_SOURCE_POSITION) && d1) o += "\tX0";
+    if (on(CRP_COL_SOURCE_POSITION) && !d1) o += "\tX0\tY0\tZ0";
+    if (on(CRP_COL_SOURCE_DIRECTION) && !d1) o += "\tP0x\tP0y\tP0z";
+    if (on(CRP_COL_SERIAL_NUMBER)) o += "\tSN1";
+    if (on(CRP_COL_CREATED_ID)) o += "\tID1";
+    if (on(CRP_COL_CREATED_ENERGY)) o += "\tE1";
+    if (on(CRP_COL_CREATED_POSITION) && d1) o += "\tX1";
+    if (on(CRP_COL_CREATED_POSITION) && !d1) o += "\tX1\tY1\tZ1";
+    if (on(CRP_COL_CREATED_DIRECTION) && !d1) o += "\tP1x\tP1y\tP1z";
+    if (on(CRP_COL_WEIGHT)) o += "\tW";
+    if (on(CRP_COL_CANDIDATE_TAG)) o += "\ttag";
+    o += "\n#\n";
+    // the stream prints the scale ratios with the default ostream precision (6 significant digits)
+    if (on(CRP_COL_TRAJECTORY_LENGTH)) {
+        snprintf(buf, sizeof(buf), "# D             Trajectory length [%g Mpc]\n", d->length_scale / 3.0856775814913673e22);
+        o += buf;
+    }
+    if (on(CRP_COL_TIME)) {
+        snprintf(buf, sizeof(buf), "# time          Time [%g Myr]\n", d->time_scale / (1e6 * 365.25 * 24 * 3600));
+        o += buf;
+    }
+    if (on(CRP_COL_REDSHIFT)) o += "# z             Redshift\n";
+    if (on(CRP_COL_SERIAL_NUMBER)) o += "# SN/SN0/SN1    Serial number. Unique (within this run) id of the particle.\n";
+    if (on(CRP_COL_CURRENT_ID) || on(CRP_COL_CREATED_ID) || on(CRP_COL_SOURCE_ID))
+        o += "# ID/ID0/ID1    Particle type (PDG MC numbering scheme)\n";
+    if (on(CRP_COL_CURRENT_ENERGY) || on(CRP_COL_CREATED_ENERGY) || on(CRP_COL_SOURCE_ENERGY)) {
+        snprintf(buf, sizeof(buf), "# E/E0/E1       Energy [%g EeV]\n", d->energy_scale / (1e18 * 1.602176487e-19));
+        o += buf;
+    }
+    if (on(CRP_COL_CURRENT_POSITION) || on(CRP_COL_CREATED_POSITION) || on(CRP_COL_SOURCE_POSITION)) {
+        snprintf(buf, sizeof(buf), "# X/X0/X1...    Position [%g Mpc]\n", d->length_scale / 3.0856775814913673e22);
+        o += buf;
+    }
+    if (on(CRP_COL_CURRENT_DIRECTION) || on(CRP_COL_CREATED_DIRECTION) || on(CRP_COL_SOURCE_DIRECTION))
+        o += "# Px/P0x/P1x... Heading (unit vector of momentum)\n";
+    if (on(CRP_COL_WEIGHT)) o += "# W             Weights \n";
+    o += "# no index = current, 0 = at source, 1 = at point of creation\n#\n";
+    o += "# CRPropa version: ";
+    o += d->version ? d->version : "";
+    o += "\n#\n";
+}
+
+crp_status crp_text_output_write(const char *path, int32_t append, int32_t header,
+                                 const crp_output_desc *desc, uint64_t n,
+                                 const crp_output_rows *rows) {
+    if (!path || !desc || (n && !rows)) return host_fail(CRP_ERR_INVALID_ARGUMENT, "NULL argument");
+    FILE *f = fopen(path, append ? "ab" : "wb");
+    if (!f) return host_fail(CRP_ERR_INVALID_ARGUMENT, "Cannot create file");
+    std::string out;
+    out.reserve(256 * (size_t)(n < 4096 ? n + 1 : 4096));
+    if (header) format_header(desc, out);
+    for (uint64_t i = 0; i < n; i++) {
+        format_row(desc, rows, i, out);
+        if (out.size() > (1u << 22)) {
+            fwrite(out.data(), 1, out.size(), f);
+            out.clear();
+        }
+    }
+    fwrite(out.data(), 1, out.size(), f);
+    fclose(f);
+    return CRP_OK;
+}
+
+}  // extern "C"

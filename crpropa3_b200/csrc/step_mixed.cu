@@ -1,0 +1,546 @@
+// step_mixed.cu -- the mixed-precision form of the stepping path.
+//
+// Same modules and module order as the FP64 form (step_fp64.cu), with the
+// arithmetic split by what each quantity needs:
+//   * FP64: position, trajectory length, time, the step controller's error
+//     sum and its pow(), grid coordinates before the cell split, wave phases
+//     before range reduction, and the direction vector (accumulated as
+//     u <- u + du with du formed in FP32);
+//   * FP32: field interpolation and wave sums, the Boris rotation, the
+//     Cash-Karp and DiffusionSDE stage derivatives and their weighted sums.
+// Rounding errors of FP32 then enter only through increments that are small
+// against the FP64 quantities they are added to, which keeps the
+// accumulated error of 10^3-10^6 steps at the FP64 level of the increments'
+// relative error times their size.
+#include "chain.cuh"
+#include "engine_internal.h"
+
+namespace crp {
+namespace {
+
+struct f3 { float x, y, z; };
+__device__ __forceinline__ f3 f3mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 cross(f3 a, f3 v) {
+    return {a.y * v.z - v.y * a.z, a.z * v.x - v.z * a.x, a.x * v.y - v.x * a.y};
+}
+__device__ __forceinline__ float dot(f3 a, f3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double clipd(double x, double lo, double hi) { return dmax(lo, dmin(x, hi)); }
+
+__device__ __forceinline__ int wrap(int i, int n, bool pow2) {
+    return pow2 ? (i & (n - 1)) : (((i % n) + n) % n);
+}
+
+// Trilinear Grid3f interpolation: FP64 cell coordinates, FP32 weights and
+// values (the reference's own interpolation arithmetic is FP32, Grid.h:571).
+__device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
+    if (g.clip_volume) {
+        bool in = (x >= g.ox) && (x <= g.ex) && (y >= g.oy) && (y <= g.ey) && (z >= g.oz) && (z <= g.ez);
+        if (!in) return f3mk(0.f, 0.f, 0.f);
+    }
+    double rx = (x - g.gox) * g.inv_sx, ry = (y - g.goy) * g.inv_sy, rz = (z - g.goz) * g.inv_sz;
+    double flx = floor(rx), fly = floor(ry), flz = floor(rz);
+    float fx0 = (float)(rx - flx), fy0 = (float)(ry - fly), fz0 = (float)(rz - flz);
+    int ix0, ix1, iy0, iy1, iz0, iz1;
+    if (g.reflective) {
+        double r[3] = {rx, ry, rz};
+        int n[3] = {g.nx, g.ny, g.nz}, lo[3], hi[3];
+        float f[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            double v = r[a];
+            int guard = 0;
+            while (((v < -0.5) || (v > (n[a] - 0.5))) && guard < 64) {
+                v = 2 * n[a] * (v > (n[a] - 0.5)) - v - 1;
+                guard++;
+            }
+            lo[a] = (int)floor(v);
+            hi[a] = lo[a] + (lo[a] < n[a] - 1);
+            if (v < 0) { lo[a] = 0; hi[a] = 0; }
+            if (lo[a] < 0 || lo[a] >= n[a]) { lo[a] = 0; hi[a] = 0; }
+            f[a] = (float)(v - floor(v));
+        }
+        ix0 = lo[0]; ix1 = hi[0]; iy0 = lo[1]; iy1 = hi[1]; iz0 = lo[2]; iz1 = hi[2];
+        fx0 = f[0]; fy0 = f[1]; fz0 = f[2];
+    } else {
+        bool p2 = g.pow2 != 0;
+        ix0 = wrap((int)flx, g.nx, p2); ix1 = (ix0 + 1 == g.nx) ? 0 : ix0 + 1;
+        iy0 = wrap((int)fly, g.ny, p2); iy1 = (iy0 + 1 == g.ny) ? 0 : iy0 + 1;
+        iz0 = wrap((int)flz, g.nz, p2); iz1 = (iz0 + 1 == g.nz) ? 0 : iz0 + 1;
+    }
+    const float fx1 = 1.f - fx0, fy1 = 1.f - fy0, fz1 = 1.f - fz0;
+    const size_t sy = (size_t)g.nz, sx = (size_t)g.ny * (size_t)g.nz;
+    const size_t b00 = (size_t)ix0 * sx + (size_t)iy0 * sy, b10 = (size_t)ix1 * sx + (size_t)iy0 * sy;
+    const size_t b01 = (size_t)ix0 * sx + (size_t)iy1 * sy, b11 = (size_t)ix1 * sx + (size_t)iy1 * sy;
+    const size_t idx[8] = {b00 + iz0, b10 + iz0, b01 + iz0, b00 + iz1, b10 + iz1, b01 + iz1, b11 + iz0, b11 + iz1};
+    const float w[8] = {fx1 * fy1 * fz1, fx0 * fy1 * fz1, fx1 * fy0 * fz1, fx1 * fy1 * fz0,
+                        fx0 * fy1 * fz0, fx1 * fy0 * fz0, fx0 * fy0 * fz1, fx0 * fy0 * fz0};
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    if (g.values4) {
+        float4 c[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) c[k] = __ldg(g.values4 + idx[k]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            bx = fmaf(c[k].x, w[k], bx);
+            by = fmaf(c[k].y, w[k], by);
+            bz = fmaf(c[k].z, w[k], bz);
+        }
+    } else {
+        float c[8][3];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const float *p = g.values + 3 * idx[k];
+            c[k][0] = __ldg(p); c[k][1] = __ldg(p + 1); c[k][2] = __ldg(p + 2);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            bx = fmaf(c[k][0], w[k], bx);
+            by = fmaf(c[k][1], w[k], by);
+            bz = fmaf(c[k][2], w[k], bz);
+        }
+    }
+    return f3mk(bx, by, bz);
+}
+
+// PlaneWaveTurbulence sum: FP64 phase k*kappa.x + beta, reduced to
+// [-pi, pi] in FP64 (two-constant Cody-Waite), then FP32 hardware cosine
+// and FP32 accumulation.  Table per mode: kk = {k kappa_x, k kappa_y,
+// k kappa_z, beta} (FP64), modes32 = {Ak xi_x, Ak xi_y, Ak xi_z, 0} (FP32).
+__device__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double z) {
+    const double inv2pi = 0.15915494309189533577;
+    const double twopi_hi = 6.28318530717958623200, twopi_lo = 2.44929359829470635445e-16;
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    const double2 *kk = reinterpret_cast<const double2 *>(w.kk);
+#pragma unroll 4
+    for (int i = 0; i < w.n; i++) {
+        double2 m0 = __ldg(kk + 2 * i), m1 = __ldg(kk + 2 * i + 1);
+        float4 a = __ldg(w.modes32 + i);
+        double ph = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
+        double nr = rint(ph * inv2pi);
+        double red = fma(-nr, twopi_lo, fma(-nr, twopi_hi, ph));
+        float c = __cosf((float)red);
+        bx = fmaf(a.x, c, bx);
+        by = fmaf(a.y, c, by);
+        bz = fmaf(a.z, c, bz);
+    }
+    return f3mk(bx, by, bz);
+}
+
+__device__ f3 component_field(const DevComponent &f, double x, double y, double z) {
+    if (f.periodic) {
+        double qx = x - f.po[0], qy = y - f.po[1], qz = z - f.po[2];
+        double nx = floor(qx / f.pe[0]), ny = floor(qy / f.pe[1]), nz = floor(qz / f.pe[2]);
+        x = qx - nx * f.pe[0]; y = qy - ny * f.pe[1]; z = qz - nz * f.pe[2];
+        if (f.periodic_reflective) {
+            if ((long long)fabs(nx) % 2 == 1) x = f.pe[0] - x;
+            if ((long long)fabs(ny) % 2 == 1) y = f.pe[1] - y;
+            if ((long long)fabs(nz) % 2 == 1) z = f.pe[2] - z;
+        }
+    }
+    switch (f.kind) {
+    case CRP_FIELD_GRID: return grid_field(f.grid, x, y, z);
+    case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z);
+    case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
+    default: {
+        double r = sqrt(x * x + y * y);
+        double s = f.b0 / r;
+        return f3mk((float)(-y * s), (float)(x * s), 0.f);
+    }
+    }
+}
+
+template <int FS>
+__device__ __forceinline__ f3 field_at(const DevPlan &P, double x, double y, double z) {
+    if (FS == FS_GRID) return grid_field(P.fields[0].grid, x, y, z);
+    if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, x, y, z);
+    if (P.n_fields == 1) return component_field(P.fields[0], x, y, z);
+    f3 b = f3mk(0.f, 0.f, 0.f);
+#pragma unroll 1
+    for (int i = 0; i < P.n_fields; i++) {
+        f3 c = component_field(P.fields[i], x, y, z);
+        b.x += c.x; b.y += c.y; b.z += c.z;
+    }
+    return b;
+}
+
+__device__ __forceinline__ void set_current_step(Cand &c, double s) {
+    c.cur = s;
+    c.len += s;
+    c.time += s / kCLight;
+}
+
+// Renormalise an FP64 direction that is within rounding of unit length:
+// one Newton step of 1/sqrt(n2) from 1.
+__device__ __forceinline__ void renorm(double &x, double &y, double &z) {
+    double n2 = fma(x, x, fma(y, y, z * z));
+    double f = fma(-0.5, n2, 1.5);
+    if (fabs(n2 - 1.0) > 1e-6) f = rsqrt(n2);  // far from unit length: plain rescale
+    x *= f; y *= f; z *= f;
+}
+
+// ---------------------------------------------------------------- Boris push
+// One PropagationBP::dY (PropagationBP.cpp:19) with FP32 rotation increment.
+template <int FS>
+__device__ __forceinline__ void bp_dy(const DevPlan &P, double &x, double &y, double &z, double &ux,
+                                      double &uy, double &uz, double step, float kt) {
+    double hh = 0.5 * step;
+    x = fma(ux, hh, x); y = fma(uy, hh, y); z = fma(uz, hh, z);
+    f3 B = field_at<FS>(P, x, y, z);
+    f3 t = f3mk(B.x * kt, B.y * kt, B.z * kt);   // t = B q step / (2 m c)
+    float sf = __fdividef(2.f, 1.f + dot(t, t));
+    f3 s = f3mk(t.x * sf, t.y * sf, t.z * sf);
+    f3 u = f3mk((float)ux, (float)uy, (float)uz);
+    f3 ut = cross(u, t);
+    f3 v = f3mk(u.x + ut.x, u.y + ut.y, u.z + ut.z);
+    f3 du = cross(v, s);
+    ux += (double)du.x; uy += (double)du.y; uz += (double)du.z;
+    x = fma(ux, hh, x); y = fma(uy, hh, y); z = fma(uz, hh, z);
+}
+
+template <int FS>
+struct BP {
+    __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
+        c.px = c.x; c.py = c.y; c.pz = c.z;
+        double q = c.q, step = m.max_step;
+        if (q == 0) {
+            step = clipd(c.next, m.min_step, m.max_step);
+            c.x = fma(c.dx, step, c.x); c.y = fma(c.dy, step, c.y); c.z = fma(c.dz, step, c.z);
+            set_current_step(c, step);
+            c.next = m.max_step;
+            return;
+        }
+        double newStep = step;
+        // t = B * q / 2 / m * step / c with m = E/c^2  ->  B * (q c step / (2 E))
+        const double kq = q * kCLight / (2.0 * c.E);
+        double xo = c.x, yo = c.y, zo = c.z, uxo = c.dx, uyo = c.dy, uzo = c.dz;
+        if (m.min_step == m.max_step) {
+            bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, (float)(kq * step));
+            sc.tries++; sc.evals++;
+        } else {
+            step = clipd(c.next, m.min_step, m.max_step);
+            newStep = step;
+            for (int guard = 0; guard < 4096; guard++) {
+                double x1 = c.x, y1 = c.y, z1 = c.z, u1x = c.dx, u1y = c.dy, u1z = c.dz;
+                double x2 = c.x, y2 = c.y, z2 = c.z, u2x = c.dx, u2y = c.dy, u2z = c.dz;
+                bp_dy<FS>(P, x1, y1, z1, u1x, u1y, u1z, step, (float)(kq * step));
+                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2));
+                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2));
+                sc.tries++; sc.evals += 3;
+                double ex = x1 - x2, ey = y1 - y2, ez = z1 - z2;
+                double S = sqrt(ex * ex + ey * ey + ez * ez) / (step * 0.75);
+                xo = x1; yo = y1; zo = z1; uxo = u1x; uyo = u1y; uzo = u1z;
+                double r = sqrt(3.0 * S * S) / m.tolerance;
+                if (r > 1) {
+                    if (step == m.min_step) break;
+                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = dmax(newStep, 0.1 * step);
+                    newStep = dmax(newStep, m.min_step);
+                    step = newStep;
+                } else {
+                    if (step != m.max_step) {
+                        newStep = step * 0.95 * pow(r, -0.2);
+                        newStep = dmin(newStep, 5 * step);
+                        newStep = dmin(newStep, m.max_step);
+                    }
+                    break;
+                }
+            }
+        }
+        renorm(uxo, uyo, uzo);
+        c.x = xo; c.y = yo; c.z = zo;
+        c.dx = uxo; c.dy = uyo; c.dz = uzo;
+        set_current_step(c, step);
+        c.next = newStep;
+    }
+};
+
+// --------------------------------------------------------------- Cash-Karp
+__constant__ float ck_af[36] = {
+    0.f, 0.f, 0.f, 0.f, 0.f, 0.f,
+    1.f / 5.f, 0.f, 0.f, 0.f, 0.f, 0.f,
+    3.f / 40.f, 9.f / 40.f, 0.f, 0.f, 0.f, 0.f,
+    3.f / 10.f, -9.f / 10.f, 6.f / 5.f, 0.f, 0.f, 0.f,
+    -11.f / 54.f, 5.f / 2.f, -70.f / 27.f, 35.f / 27.f, 0.f, 0.f,
+    1631.f / 55296.f, 175.f / 512.f, 575.f / 13824.f, 44275.f / 110592.f, 253.f / 4096.f, 0.f};
+__constant__ float ck_bf[6] = {37.f / 378.f, 0.f, 250.f / 621.f, 125.f / 594.f, 0.f, 512.f / 1771.f};
+__constant__ double ck_eb[6] = {37. / 378. - 2825. / 27648., 0. - 0., 250. / 621. - 18575. / 48384.,
+                                125. / 594. - 13525. / 55296., 0. - 277. / 14336., 512. / 1771. - 1. / 4.};
+
+// One Cash-Karp try in time h (PropagationCK::tryStep): stage derivatives in
+// FP32, stage positions as FP64 base + FP32 offset, error sum in FP64.
+// Returns the position / direction increments and the direction error norm.
+template <int FS>
+__device__ __forceinline__ double ck_try(const DevPlan &P, const Cand &c, double h, float qc2E,
+                                         double &ddx, double &ddy, double &ddz, double &dux,
+                                         double &duy, double &duz) {
+    // stage derivative kx_i = c * unit(u_i) (as a unit vector, the factor c
+    // is applied to the sums), ku_i = (q c / E) (v_i x B_i)
+    f3 kx[6], ku[6];
+    const float hf = (float)h;
+    const float hc = (float)(h * kCLight);  // h * c, metres per unit velocity
+    const f3 u0 = f3mk((float)c.dx, (float)c.dy, (float)c.dz);
+    double eux = 0, euy = 0, euz = 0;
+    float sxx = 0.f, sxy = 0.f, sxz = 0.f, sux = 0.f, suy = 0.f, suz = 0.f;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        float ox = 0.f, oy = 0.f, oz = 0.f, vx = u0.x, vy = u0.y, vz = u0.z;
+#pragma unroll
+        for (int j = 0; j < i; j++) {
+            float a = ck_af[i * 6 + j];
+            ox = fmaf(kx[j].x, a, ox); oy = fmaf(kx[j].y, a, oy); oz = fmaf(kx[j].z, a, oz);
+            vx = fmaf(ku[j].x, a * hf, vx); vy = fmaf(ku[j].y, a * hf, vy); vz = fmaf(ku[j].z, a * hf, vz);
+        }
+        float inv = rsqrtf(vx * vx + vy * vy + vz * vz);
+        f3 vel = f3mk(vx * inv, vy * inv, vz * inv);  // unit velocity
+        f3 B = field_at<FS>(P, c.x + (double)(ox * hc), c.y + (double)(oy * hc), c.z + (double)(oz * hc));
+        f3 d = cross(vel, B);
+        kx[i] = vel;
+        ku[i] = f3mk(d.x * qc2E, d.y * qc2E, d.z * qc2E);  // (q c / E) (c vel x B)
+        float b = ck_bf[i];
+        sxx = fmaf(kx[i].x, b, sxx); sxy = fmaf(kx[i].y, b, sxy); sxz = fmaf(kx[i].z, b, sxz);
+        sux = fmaf(ku[i].x, b, sux); suy = fmaf(ku[i].y, b, suy); suz = fmaf(ku[i].z, b, suz);
+        double e = ck_eb[i] * h;
+        eux = fma((double)ku[i].x, e, eux); euy = fma((double)ku[i].y, e, euy); euz = fma((double)ku[i].z, e, euz);
+    }
+    ddx = (double)sxx * (h * kCLight); ddy = (double)sxy * (h * kCLight); ddz = (double)sxz * (h * kCLight);
+    dux = (double)(sux * hf); duy = (double)(suy * hf); duz = (double)(suz * hf);
+    return sqrt(eux * eux + euy * euy + euz * euz);
+}
+
+template <int FS>
+struct CK {
+    __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
+        c.px = c.x; c.py = c.y; c.pz = c.z;
+        double step = m.max_step;
+        if (c.q == 0) {
+            step = clipd(c.next, m.min_step, m.max_step);
+            c.x = fma(c.dx, step, c.x); c.y = fma(c.dy, step, c.y); c.z = fma(c.dz, step, c.z);
+            set_current_step(c, step);
+            c.next = m.max_step;
+            return;
+        }
+        const float qc2E = (float)(c.q * kCLight * kCLight / c.E);
+        double ddx, ddy, ddz, dux, duy, duz;
+        double newStep = step;
+        if (m.min_step == m.max_step) {
+            ck_try<FS>(P, c, step / kCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
+            sc.tries++; sc.evals += 6;
+        } else {
+            step = clipd(c.next, m.min_step, m.max_step);
+            newStep = step;
+            for (int guard = 0; guard < 4096; guard++) {
+                double err = ck_try<FS>(P, c, step / kCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
+                sc.tries++; sc.evals += 6;
+                double r = err / m.tolerance;
+                if (r > 1) {
+                    if (step == m.min_step) break;
+                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = dmax(newStep, 0.1 * step);
+                    newStep = dmax(newStep, m.min_step);
+                    step = newStep;
+                } else {
+                    if (step != m.max_step) {
+                        newStep = step * 0.95 * pow(r, -0.2);
+                        newStep = dmin(newStep, 5 * step);
+                        newStep = dmin(newStep, m.max_step);
+                    }
+                    break;
+                }
+            }
+        }
+        c.x += ddx; c.y += ddy; c.z += ddz;
+        double ux = c.dx + dux, uy = c.dy + duy, uz = c.dz + duz;
+        double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
+        c.dx = ux * inv; c.dy = uy * inv; c.dz = uz * inv;
+        set_current_step(c, step);
+        c.next = newStep;
+    }
+};
+
+// ------------------------------------------------------------ DiffusionSDE
+__device__ __forceinline__ double s_rand(Stream &s) { return (double)s.next_u32() * (1.0 / 4294967295.0); }
+__device__ __forceinline__ double s_uniform(Stream &s, double a, double b) { return a + (b - a) * s_rand(s); }
+__device__ __forceinline__ double s_norm(Stream &s) {
+    double dblexc = ((double)s.next_u32() + 0.5) * (1.0 / 4294967296.0);
+    double r = sqrt(-2.0 * log(1.0 - dblexc));
+    double phi = 2.0 * kPi * ((double)s.next_u32() * (1.0 / 4294967296.0));
+    return r * cos(phi);
+}
+
+// Field-line trace of DiffusionSDE::tryStep (DiffusionSDE.cpp:233): unit B
+// stage directions in FP32, FP64 base position + FP32 offsets, FP64 error.
+template <int FS>
+__device__ __forceinline__ void sde_try(const DevPlan &P, double x, double y, double z, double t,
+                                        double &ox, double &oy, double &oz, double &err) {
+    f3 k[6];
+    const float tc = (float)(t * kCLight);
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    double ex = 0, ey = 0, ez = 0;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+        for (int j = 0; j < i; j++) {
+            float a = ck_af[i * 6 + j];
+            ax = fmaf(k[j].x, a, ax); ay = fmaf(k[j].y, a, ay); az = fmaf(k[j].z, a, az);
+        }
+        f3 B = field_at<FS>(P, x + (double)(ax * tc), y + (double)(ay * tc), z + (double)(az * tc));
+        float inv = rsqrtf(B.x * B.x + B.y * B.y + B.z * B.z);
+        k[i] = f3mk(B.x * inv, B.y * inv, B.z * inv);
+        float b = ck_bf[i];
+        sx = fmaf(k[i].x, b, sx); sy = fmaf(k[i].y, b, sy); sz = fmaf(k[i].z, b, sz);
+        double e = ck_eb[i];
+        ex = fma((double)k[i].x, e, ex); ey = fma((double)k[i].y, e, ey); ez = fma((double)k[i].z, e, ez);
+    }
+    const double tcd = t * kCLight;
+    ox = x + (double)sx * tcd; oy = y + (double)sy * tcd; oz = z + (double)sz * tcd;
+    err = sqrt(ex * ex + ey * ey + ez * ez) * fabs(tcd) / CRP_KPC;
+}
+
+template <int FS>
+struct SDE {
+    __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
+        c.px = c.x; c.py = c.y; c.pz = c.z;
+        double h = clipd(c.next, m.min_step, m.max_step) / kCLight;
+        if (c.q == 0) {
+            c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+            set_current_step(c, h * kCLight);
+            c.next = m.max_step;
+            return;
+        }
+        double rig = c.E / c.q;
+        double D = m.scale * 6.1e24 * pow(fabs(rig) / 4.0e9, m.alpha);
+        double BT0 = sqrt(2 * D), BT4 = sqrt(2 * m.eps * D);
+        Stream s{P.seed, c.index, c.steps, make_uint4(0, 0, 0, 0), 0};
+        double eta0 = s_norm(s), eta1 = s_norm(s), eta2 = s_norm(s);
+        double TStep = BT0 * eta0, NStep = BT4 * eta1, BStep = BT4 * eta2;
+        double sh = sqrt(h);
+        double propTime = TStep * sh / kCLight;
+        unsigned counter = 0;
+        double r, ox, oy, oz, err;
+        do {
+            sde_try<FS>(P, c.x, c.y, c.z, propTime, ox, oy, oz, err);
+            sc.tries++; sc.evals += 6;
+            r = err / m.tolerance;
+            propTime *= 0.5;
+            counter += 1;
+        } while (r > 1 && fabs(propTime) >= m.min_step / kCLight && counter < 60);
+        unsigned long long stepNumber = 1ull << (counter - 1);
+        double allowedTime = TStep * sh / kCLight / (double)stepNumber;
+        double sx = c.x, sy = c.y, sz = c.z;
+        for (unsigned long long j = 0; j < stepNumber; j++) {
+            sde_try<FS>(P, sx, sy, sz, allowedTime, ox, oy, oz, err);
+            sc.tries++; sc.evals += 6;
+            sx = ox; sy = oy; sz = oz;
+        }
+        double tx = ox - c.x, ty = oy - c.y, tz = oz - c.z;
+        double tn = sqrt(tx * tx + ty * ty + tz * tz);
+        tx /= tn; ty /= tn; tz /= tn;
+        if (!(tn == tn) || tn == 0.0) {
+            c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+            set_current_step(c, h * kCLight);
+            c.next = clipd(5 * h * kCLight, m.min_step, m.max_step);
+            return;
+        }
+        double nx = 0, ny = 0, nz = 0;
+        for (int guard = 0; nx == 0 && ny == 0 && nz == 0 && guard < 3; guard++) {
+            double zr = s_uniform(s, -1.0, 1.0), tr = s_uniform(s, -kPi, kPi);
+            double rr = sqrt(1 - zr * zr), sn, cs;
+            sincos(tr, &sn, &cs);
+            double rx = rr * cs, ry = rr * sn, rz = zr;
+            nx = ty * rz - ry * tz; ny = tz * rx - rz * tx; nz = tx * ry - rx * ty;
+        }
+        double nn = sqrt(nx * nx + ny * ny + nz * nz);
+        if (nn == 0.0) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
+        nx /= nn; ny /= nn; nz /= nn;
+        double bx = ty * nz - ny * tz, by = tz * nx - nz * tx, bz = tx * ny - nx * ty;
+        double bn = sqrt(bx * bx + by * by + bz * bz);
+        bx /= bn; by /= bn; bz /= bn;
+        double POx = ox + (nx * NStep + bx * BStep) * sh;
+        double POy = oy + (ny * NStep + by * BStep) * sh;
+        double POz = oz + (nz * NStep + bz * BStep) * sh;
+        if (isnan(POx + POy + POz)) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
+        // randConeVector(T, pi/2) (Random.cpp:159): rotate T by theta about T x randVector
+        s.cursor = 12;
+        double theta = acos(s_uniform(s, 1, cos(kPi / 2.)));
+        double zr = s_uniform(s, -1.0, 1.0), tr = s_uniform(s, -kPi, kPi);
+        double rr = sqrt(1 - zr * zr), sn, cs;
+        sincos(tr, &sn, &cs);
+        double rx = rr * cs, ry = rr * sn, rz = zr;
+        double ax = ty * rz - ry * tz, ay = tz * rx - rz * tx, az = tx * ry - rx * ty;
+        double an = sqrt(ax * ax + ay * ay + az * az);
+        if (an != 0.) { ax /= an; ay /= an; az /= an; }
+        double st, ct;
+        sincos(theta, &st, &ct);
+        // Rodrigues rotation of T about the unit axis a
+        double adt = ax * tx + ay * ty + az * tz;
+        double cx_ = ay * tz - az * ty, cy_ = az * tx - ax * tz, cz_ = ax * ty - ay * tx;
+        double dx = tx * ct + cx_ * st + ax * adt * (1 - ct);
+        double dy = ty * ct + cy_ * st + ay * adt * (1 - ct);
+        double dz = tz * ct + cz_ * st + az * adt * (1 - ct);
+        double dn = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+        c.x = POx; c.y = POy; c.z = POz;
+        c.dx = dx * dn; c.dy = dy * dn; c.dz = dz * dn;
+        set_current_step(c, h * kCLight);
+        c.next = (stepNumber > 1) ? h / ((double)stepNumber * (double)stepNumber) * kCLight : 4 * h * kCLight;
+    }
+};
+
+template <template <int> class Prop, int FS>
+__global__ void __launch_bounds__(128) mixed_chunk_kernel(DevPlan P, DevState s, uint64_t n,
+                                                          int max_steps, uint64_t step_cap,
+                                                          DevCounters *cnt, DevRecords rec,
+                                                          const uint32_t *perm) {
+    chunk_body<Prop<FS>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+}
+
+__global__ void mixed_field_kernel(DevPlan P, uint64_t n, const double *pos, double *out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 b = field_at<FS_GENERIC>(P, pos[i], pos[n + i], pos[2 * n + i]);
+    out[i] = b.x; out[n + i] = b.y; out[2 * n + i] = b.z;
+}
+
+template <template <int> class Prop>
+cudaError_t launch_prop(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
+                        uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
+                        const uint32_t *perm, int fs, int block, cudaStream_t st) {
+    unsigned grid = (unsigned)((n + block - 1) / block);
+    if (fs == FS_GRID)
+        mixed_chunk_kernel<Prop, FS_GRID><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+    else if (fs == FS_PLANE_WAVE)
+        mixed_chunk_kernel<Prop, FS_PLANE_WAVE><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+    else
+        mixed_chunk_kernel<Prop, FS_GENERIC><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
+                               uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
+                               const uint32_t *perm, int fs, int block, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    int prop = P.modules[P.prop_index].propagator;
+    if (prop == CRP_PROP_BP) return launch_prop<BP>(P, s, n, max_steps, step_cap, cnt, rec, perm, fs, block, st);
+    if (prop == CRP_PROP_CK) return launch_prop<CK>(P, s, n, max_steps, step_cap, cnt, rec, perm, fs, block, st);
+    return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, fs, block, st);
+}
+
+cudaError_t launch_mixed_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
+                               cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    mixed_field_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(P, n, pos, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_persistent(const DevPlan &, const DevState &, uint64_t, uint64_t,
+                                    DevCounters *, const DevRecords &, int, int, int, int,
+                                    unsigned long long, uint32_t *, uint64_t, uint32_t *,
+                                    cudaStream_t) {
+    return cudaErrorNotSupported;
+}
+
+}  // namespace crp

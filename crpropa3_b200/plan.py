@@ -1,0 +1,181 @@
+"""Building crp_plan_desc structures (include/crp_gpu.h) from Python values.
+
+A `ChainSpec` holds the field components and the module chain in ModuleList
+order; `desc()` returns the ctypes PlanDesc view and keeps every array it
+points into alive for as long as the spec lives.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+
+
+def _v3(v) -> tuple:
+    v = tuple(float(x) for x in (v if hasattr(v, "__len__") else (v, v, v)))
+    if len(v) != 3:
+        raise ValueError("expected a 3-vector")
+    return v
+
+
+@dataclass
+class GridField:
+    """MagneticFieldGrid over a Grid3f (MagneticFieldGrid.cpp:17)."""
+    values: np.ndarray            # (nx, ny, nz, 3) float32, z fastest (Grid.h:338)
+    origin: Sequence[float] = (0.0, 0.0, 0.0)
+    spacing: Sequence[float] = (1.0, 1.0, 1.0)
+    reflective: bool = False
+    clip_volume: bool = False
+    periodic: Optional[tuple] = None  # (origin, extends, reflective) PeriodicMagneticField
+
+
+@dataclass
+class PlaneWaveField:
+    """PlaneWaveTurbulence modes (PlaneWaveTurbulence.cpp:79)."""
+    xi: np.ndarray
+    kappa: np.ndarray
+    k: np.ndarray
+    beta: np.ndarray
+    ak: np.ndarray
+    spectrum: tuple = (0.0, 1.0, 1.0, 1.0, 5.0 / 3.0, 4.0)  # brms lmin lmax lbendover s q
+    seed: int = 0
+    periodic: Optional[tuple] = None
+
+
+@dataclass
+class UniformField:
+    value: Sequence[float]
+    periodic: Optional[tuple] = None
+
+
+@dataclass
+class ToroidalField:
+    """B = b0 (-y, x, 0) / sqrt(x^2 + y^2)."""
+    b0: float
+    periodic: Optional[tuple] = None
+
+
+@dataclass
+class Propagation:
+    propagator: int               # _abi.PROP_CK / PROP_BP / PROP_SDE
+    tolerance: float
+    min_step: float
+    max_step: float
+    epsilon: float = 0.1
+    alpha: float = 1.0 / 3.0
+    scale: float = 1.0
+
+
+@dataclass
+class MaxTrajectoryLength:
+    max_length: float = 0.0
+    per_candidate: bool = False
+    record: bool = False
+
+
+@dataclass
+class ObserverSpec:
+    feature: int = _abi.OBSERVER_SURFACE_SPHERE
+    center: Sequence[float] = (0.0, 0.0, 0.0)
+    radius: float = 0.0
+    deactivate: bool = True
+    record: bool = False
+
+
+@dataclass
+class ChainSpec:
+    fields: List[object]
+    modules: List[object]
+    precision: int = _abi.PRECISION_FP64
+    seed: int = 0
+    _keep: list = field(default_factory=list, repr=False)
+
+    def desc(self) -> _abi.PlanDesc:
+        self._keep = []
+        comps = (_abi.FieldComponent * max(1, len(self.fields)))()
+        for i, f in enumerate(self.fields):
+            self._fill_component(comps[i], f)
+        mods = (_abi.ModuleDesc * len(self.modules))()
+        for i, m in enumerate(self.modules):
+            self._fill_module(mods[i], m)
+        self._keep += [comps, mods]
+        d = _abi.PlanDesc()
+        d.abi_version = _abi.ABI_VERSION
+        d.precision = int(self.precision)
+        d.fields = C.cast(comps, C.POINTER(_abi.FieldComponent))
+        d.n_fields = len(self.fields)
+        d.n_modules = len(self.modules)
+        d.modules = C.cast(mods, C.POINTER(_abi.ModuleDesc))
+        d.seed = int(self.seed)
+        self._keep.append(d)
+        return d
+
+    def _arr(self, a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        self._keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_float if dtype == np.float32 else C.c_double))
+
+    def _fill_component(self, c, f):
+        per = getattr(f, "periodic", None)
+        if per is not None:
+            o, e, refl = per
+            c.periodic = 1
+            c.periodic_origin[:] = _v3(o)
+            c.periodic_extends[:] = _v3(e)
+            c.periodic_reflective = int(bool(refl))
+        if isinstance(f, GridField):
+            v = np.ascontiguousarray(f.values, dtype=np.float32)
+            if v.ndim != 4 or v.shape[3] != 3:
+                raise ValueError("grid values must have shape (nx, ny, nz, 3)")
+            c.kind = _abi.FIELD_GRID
+            c.grid.values = self._arr(v, np.float32)
+            c.grid.nx, c.grid.ny, c.grid.nz = v.shape[:3]
+            c.grid.origin[:] = _v3(f.origin)
+            c.grid.spacing[:] = _v3(f.spacing)
+            c.grid.reflective = int(bool(f.reflective))
+            c.grid.clip_volume = int(bool(f.clip_volume))
+        elif isinstance(f, PlaneWaveField):
+            c.kind = _abi.FIELD_PLANE_WAVE
+            w = c.plane_wave
+            w.n_modes = len(f.k)
+            w.seed = int(f.seed)
+            w.xi = self._arr(f.xi, np.float64)
+            w.kappa = self._arr(f.kappa, np.float64)
+            w.k = self._arr(f.k, np.float64)
+            w.beta = self._arr(f.beta, np.float64)
+            w.ak = self._arr(f.ak, np.float64)
+            w.brms, w.lmin, w.lmax, w.lbendover, w.sindex, w.qindex = f.spectrum
+        elif isinstance(f, UniformField):
+            c.kind = _abi.FIELD_UNIFORM
+            c.uniform[:] = _v3(f.value)
+        elif isinstance(f, ToroidalField):
+            c.kind = _abi.FIELD_TOROIDAL
+            c.toroidal_b0 = float(f.b0)
+        else:
+            raise TypeError(f"unsupported field component {type(f).__name__}")
+
+    @staticmethod
+    def _fill_module(d, m):
+        if isinstance(m, Propagation):
+            d.kind = _abi.MODULE_PROPAGATION
+            d.propagator = int(m.propagator)
+            d.tolerance, d.min_step, d.max_step = float(m.tolerance), float(m.min_step), float(m.max_step)
+            d.sde_epsilon, d.sde_alpha, d.sde_scale = float(m.epsilon), float(m.alpha), float(m.scale)
+        elif isinstance(m, MaxTrajectoryLength):
+            d.kind = _abi.MODULE_MAX_TRAJECTORY_LENGTH
+            d.max_length = float(m.max_length)
+            d.per_candidate_length = int(bool(m.per_candidate))
+            d.record = int(bool(m.record))
+        elif isinstance(m, ObserverSpec):
+            d.kind = _abi.MODULE_OBSERVER
+            d.observer_feature = int(m.feature)
+            d.sphere_center[:] = _v3(m.center)
+            d.sphere_radius = float(m.radius)
+            d.deactivate_on_detection = int(bool(m.deactivate))
+            d.record = int(bool(m.record))
+        else:
+            raise TypeError(f"unsupported module {type(m).__name__}")

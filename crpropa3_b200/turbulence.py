@@ -1,0 +1,124 @@
+"""Turbulent Grid3f set-up: GridTurbulence (GridTurbulence.cpp:29-123).
+
+The k-space field is drawn exactly as GridTurbulence::initTurbulence does:
+loop over ix, iy, iz (iz over n/2+1 values) with the discrete wave numbers
+K[i] = i/n - i/(n/2) in float, keep modes with kMin <= |k| <= kMax, and for
+each kept mode draw theta then phase from one crpropa::Random(seed) stream
+(the engine's MT19937, crp_random_draws); the amplitude is
+sqrt(energySpectrum(|k| 2 pi / spacing)) along e1 cos(theta) + e2 sin(theta)
+with the (1,1,1) construction of the orthogonal base.  The inverse real FFT
+then runs on the device (torch.fft / cuFFT) when one is present, else on the
+host, and the grid is rescaled to Brms (scaleGrid / rmsFieldStrength,
+GridTools.cpp:16, :59).  FFTW is not part of this image, so the FFT is not
+the reference's: grid values are equal to the reference's only in
+distribution (zero mean, rms = Brms, the spectrum), not bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi
+
+
+def energy_spectrum(k, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0):
+    """TurbulenceSpectrum::energySpectrum (TurbulentField.h:75), not normalised."""
+    kh = k * lbendover
+    return kh ** qindex / (1.0 + kh * kh) ** ((sindex + qindex) / 2.0 + 1.0)
+
+
+def check_grid_requirements(n, spacing, lmin, lmax):
+    """GridTurbulence::checkGridRequirements (GridTurbulence.cpp:126)."""
+    if lmin < 2 * spacing:
+        raise RuntimeError("turbulentField: lMin < 2 * spacing")
+    if lmax > n * spacing:
+        raise RuntimeError("turbulentField: lMax > size")
+    if lmax < lmin:
+        raise RuntimeError("lMax < lMin")
+
+
+def _mt_rand(seed: int, count: int) -> np.ndarray:
+    lib = _abi.load()
+    out = np.zeros(count)
+    _abi.check(lib.crp_random_draws(seed, 0, count, 0.0, 0.0, 0.0,
+                                    out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out
+
+
+def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0, seed=42,
+           draws=None):
+    """The three complex (n, n, n/2+1) arrays B(k) of initTurbulence.
+    `draws(seed, count)` returns count Random::rand() values (default: the
+    engine's MT19937)."""
+    if seed == 0:
+        raise ValueError("seed 0 means a random seed in the reference; give a non-zero seed")
+    check_grid_requirements(n, spacing, lmin, lmax)
+    n2 = n // 2 + 1
+    i = np.arange(n)
+    K = (i / n - (i // (n // 2))).astype(np.float32)
+    ex, ey, ez = np.meshgrid(K, K, K[:n2], indexing="ij")
+    k = np.sqrt(ex * ex + ey * ey + ez * ez).astype(np.float32)
+    kmin, kmax = spacing / lmax, spacing / lmin
+    keep = ~((k.astype(np.float64) < kmin) | (k.astype(np.float64) > kmax))
+    m = int(keep.sum())
+    u = (draws or _mt_rand)(seed, 2 * m)
+    theta = 2 * math.pi * u[0::2]
+    phase = 2 * math.pi * u[1::2]
+    kx, ky, kz, kk = ex[keep], ey[keep], ez[keep], k[keep]
+    one = np.float32(1.0)
+    # e1 = n0 x ek, e2 = ek x e1 with n0 = (1, 1, 1), in float (Vector3f)
+    e1 = np.stack([one * kz - ky * one, one * kx - kz * one, one * ky - kx * one], 1).astype(np.float32)
+    e2 = np.stack([ky * e1[:, 2] - e1[:, 1] * kz, kz * e1[:, 0] - e1[:, 2] * kx,
+                   kx * e1[:, 1] - e1[:, 0] * ky], 1).astype(np.float32)
+    # ek parallel to (1,1,1) within 1e-3 rad: fixed base (GridTurbulence.cpp:79)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        cosd = ((kx + ky + kz) / np.sqrt(np.float32(3)) / kk).astype(np.float32)
+        ang = np.where(cosd >= 1, 0, np.arccos(np.clip(cosd, -1, 1)))
+    par = ang < 1e-3
+    e1[par] = np.array([-1, 1, 0], np.float32)
+    e2[par] = np.array([1, 1, -2], np.float32)
+    e1 /= np.sqrt((e1 * e1).sum(1))[:, None].astype(np.float32)
+    e2 /= np.sqrt((e2 * e2).sum(1))[:, None].astype(np.float32)
+    b = (e1 * np.cos(theta).astype(np.float32)[:, None] +
+         e2 * np.sin(theta).astype(np.float32)[:, None]).astype(np.float32)
+    lam = 1 / spacing * 2 * math.pi
+    amp = np.sqrt(energy_spectrum(kk.astype(np.float64) * lam, brms, lmin, lmax, lbendover, sindex,
+                                  qindex)).astype(np.float32)
+    b *= amp[:, None]
+    cph, sph = np.cos(phase), np.sin(phase)
+    out = []
+    for a in range(3):
+        arr = np.zeros((n, n, n2), dtype=np.complex64)
+        arr[keep] = (b[:, a] * cph).astype(np.float32) + 1j * (b[:, a] * sph).astype(np.float32)
+        out.append(arr)
+    return out
+
+
+def grid_turbulence(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0,
+                    seed=42, device=None, draws=None) -> np.ndarray:
+    """(n, n, n, 3) float32 Grid3f values of GridTurbulence(spectrum, grid, seed)."""
+    bk = kspace(n, spacing, brms, lmin, lmax, lbendover, sindex, qindex, seed, draws)
+    comps = []
+    use_torch = False
+    if device is not None:
+        import torch
+        use_torch = torch.cuda.is_available()
+    for arr in bk:
+        if use_torch:
+            import torch
+            t = torch.from_numpy(arr).to(device)
+            comps.append(torch.fft.irfftn(t, s=(n, n, n)).cpu().numpy().astype(np.float32))
+        else:
+            comps.append(np.fft.irfftn(arr, s=(n, n, n)).astype(np.float32))
+    g = np.stack(comps, axis=-1).astype(np.float32)
+    g64 = g.astype(np.float64)
+    rms = math.sqrt(float((g64 * g64).sum()) / (n * n * n))
+    g *= np.float32(brms / rms)
+    return g
+
+
+def grid_turbulence_with_draws(n, spacing, brms, lmin, lmax, seed, draws):
+    """grid_turbulence with the MT19937 draws supplied by the caller (host FFT)."""
+    return grid_turbulence(n, spacing, brms, lmin, lmax, seed=seed, draws=draws)

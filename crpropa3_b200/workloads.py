@@ -1,0 +1,102 @@
+"""The stepping workloads the engine is measured on, with their sizes.
+
+grid_bp_256:  fixed-step PropagationBP (1 kpc) over a Kolmogorov Grid3f of
+              256^3 float32 cells (201 MB) at 5 kpc spacing, periodic,
+              Brms 10 nG, lMin 10 kpc, lMax 500 kpc, grid seed 42; 10^6
+              protons from the origin, isotropic, energies log-uniform
+              1-100 EeV; MaximumTrajectoryLength 5 Mpc (5000 steps).
+grid_ck_64:   PropagationCK (tolerance 1e-4, 0.1-10 kpc) over a 64^3
+              Kolmogorov grid at 10 kpc (Brms 1 nG, lMin 20 kpc, lMax
+              200 kpc, seed 42); 10^4 protons; MaximumTrajectoryLength 10 Mpc.
+grid_ck_nuclei: PropagationCK (1e-4, 0.1-100 kpc) over the 256^3 grid with
+              H, He-4, N-14, Fe-56 in equal parts, E^-2 over 0.1-100 EeV and a
+              per-candidate maximum length uniform in 1-50 Mpc.
+Inputs are synthetic and seeded; sizes are scaled down through `n`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, plan as P, units as U
+from .state import CandidateArrays
+from .turbulence import grid_turbulence
+
+IDS = {"H": 1000010010, "He": 1000020040, "N": 1000070140, "Fe": 1000260560}
+
+
+def charge_of(pid: int) -> float:
+    lib = _abi.load()
+    q = C.c_double()
+    _abi.check(lib.crp_particle_charge(int(pid), C.byref(q)))
+    return q.value
+
+
+def source_candidates(n, ids, emin, emax, index, seed, position=(0.0, 0.0, 0.0),
+                      abundances=None, per_candidate_length=False) -> CandidateArrays:
+    """Candidates from a Source(SourcePosition, particle type(s),
+    SourcePowerLawSpectrum, SourceIsotropicEmission) via crp_source_sample."""
+    lib = _abi.load()
+    ids = np.asarray(ids, dtype=np.int32)
+    ab = np.ones(len(ids)) if abundances is None else np.asarray(abundances, dtype=np.float64)
+    d = _abi.SourceDesc()
+    d.n_types = len(ids)
+    d.spectrum = 1
+    d.ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
+    d.abundances = ab.ctypes.data_as(C.POINTER(C.c_double))
+    d.emin, d.emax, d.index = emin, emax, index
+    d.isotropic = 1
+    c = CandidateArrays(n, per_candidate_length=per_candidate_length)
+    dirs = np.zeros(3 * n)
+    _abi.check(lib.crp_source_sample(C.byref(d), seed, n,
+                                     c.id.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     c.energy.ctypes.data_as(C.POINTER(C.c_double)),
+                                     dirs.ctypes.data_as(C.POINTER(C.c_double))))
+    c.set_direction(dirs.reshape(3, n).T)
+    c.set_position(np.tile(np.asarray(position, dtype=np.float64), (n, 1)))
+    qs = {int(p): charge_of(int(p)) for p in np.unique(c.id)}
+    c.charge[:] = np.vectorize(lambda p: qs[int(p)])(c.id) if n else 0
+    return c
+
+
+def kolmogorov_grid(n, spacing, brms, lmin, lmax, seed=42, device=None):
+    return grid_turbulence(n, spacing, brms, lmin, lmax, seed=seed, device=device)
+
+
+def grid_bp_256(n=1_000_000, grid_n=256, steps=5000, precision=_abi.PRECISION_MIXED, grid=None,
+                device=None, seed=1):
+    spacing = 5 * U.kpc
+    if grid is None:
+        grid = kolmogorov_grid(grid_n, spacing, 10 * U.nG, 10 * U.kpc, 500 * U.kpc, 42, device)
+    spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (spacing,) * 3)],
+                       [P.Propagation(_abi.PROP_BP, 0.42, 1 * U.kpc, 1 * U.kpc),
+                        P.MaxTrajectoryLength(steps * U.kpc)], precision=precision)
+    cands = source_candidates(n, [IDS["H"]], 1 * U.EeV, 100 * U.EeV, -1.0, seed)
+    return spec, cands, grid
+
+
+def grid_ck_64(n=10_000, precision=_abi.PRECISION_FP64, grid=None, device=None, seed=1):
+    spacing = 10 * U.kpc
+    if grid is None:
+        grid = kolmogorov_grid(64, spacing, 1 * U.nG, 20 * U.kpc, 200 * U.kpc, 42, device)
+    spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (spacing,) * 3)],
+                       [P.Propagation(_abi.PROP_CK, 1e-4, 0.1 * U.kpc, 10 * U.kpc),
+                        P.MaxTrajectoryLength(10 * U.Mpc)], precision=precision)
+    cands = source_candidates(n, [IDS["H"]], 1 * U.EeV, 100 * U.EeV, -1.0, seed)
+    return spec, cands, grid
+
+
+def grid_ck_nuclei(n=10_000_000, grid=None, precision=_abi.PRECISION_MIXED, device=None, seed=3,
+                   grid_n=256):
+    spacing = 5 * U.kpc
+    if grid is None:
+        grid = kolmogorov_grid(grid_n, spacing, 10 * U.nG, 10 * U.kpc, 500 * U.kpc, 42, device)
+    spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (spacing,) * 3)],
+                       [P.Propagation(_abi.PROP_CK, 1e-4, 0.1 * U.kpc, 100 * U.kpc),
+                        P.MaxTrajectoryLength(per_candidate=True)], precision=precision)
+    cands = source_candidates(n, [IDS[k] for k in ("H", "He", "N", "Fe")], 0.1 * U.EeV,
+                              100 * U.EeV, -2.0, seed, per_candidate_length=True)
+    rng = np.random.default_rng(seed)
+    cands.max_length[:] = rng.uniform(1, 50, n) * U.Mpc
+    return spec, cands, grid

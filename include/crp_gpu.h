@@ -1,0 +1,343 @@
+/*
+ * crp_gpu.h -- C-ABI of the B200 charged-particle stepping engine.
+ *
+ * This is the drop-in boundary for CRPropa's charged-particle stepping path:
+ * a chain of one propagation module (PropagationCK, PropagationBP or
+ * DiffusionSDE) over a magnetic field (MagneticFieldGrid over a Grid3f,
+ * PeriodicMagneticField, PlaneWaveTurbulence, UniformMagneticField, a
+ * MagneticFieldList of those, or a toroidal field), followed by
+ * MaximumTrajectoryLength and Observer modules, run to completion over a set
+ * of candidates.  It replaces, for such chains,
+ *
+ *   ModuleList::run(const candidate_vector_t*, bool, bool)
+ *       include/crpropa/ModuleList.h:43, src/ModuleList.cpp.in:97
+ *   ModuleList::run(SourceInterface*, size_t, bool, bool)
+ *       include/crpropa/ModuleList.h:44, src/ModuleList.cpp.in:153
+ *
+ * Only plain C types cross this boundary: pointers, sizes and POD structs.
+ * No call throws; every entry point returns a crp_status and leaves a
+ * message retrievable with crp_last_error().  A C++ wrapper maps a non-zero
+ * status to std::runtime_error, which SWIG maps to a Python RuntimeError
+ * (python/1_swig.i:53-63 of the reference).
+ *
+ * Units are SI throughout, as in include/crpropa/Units.h: metres, seconds,
+ * joules, coulombs, tesla.
+ */
+#ifndef CRP_GPU_H
+#define CRP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRP_ABI_VERSION 1u
+
+typedef enum crp_status {
+    CRP_OK = 0,
+    CRP_ERR_INVALID_ARGUMENT = 1, /* a parameter the reference setters would reject */
+    CRP_ERR_UNSUPPORTED = 2,      /* chain or field outside the device path: run the CPU ModuleList */
+    CRP_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    CRP_ERR_OUT_OF_MEMORY = 4,
+    CRP_ERR_TIMEOUT = 5,          /* a bounded device-side wait ran out */
+    CRP_ERR_CANCELLED = 6,        /* the host cancel flag was raised */
+    CRP_ERR_CAPACITY = 7,         /* a size beyond a documented limit */
+    CRP_ERR_NO_DEVICE = 8         /* no CUDA device is visible */
+} crp_status;
+
+/* ------------------------------------------------------------------------
+ * Magnetic field description
+ * ---------------------------------------------------------------------- */
+
+enum crp_field_kind {
+    CRP_FIELD_GRID = 1,       /* MagneticFieldGrid over Grid3f (MagneticFieldGrid.cpp:17) */
+    CRP_FIELD_PLANE_WAVE = 2, /* PlaneWaveTurbulence (PlaneWaveTurbulence.cpp:231) */
+    CRP_FIELD_UNIFORM = 3,    /* UniformMagneticField (MagneticField.h:109) */
+    CRP_FIELD_TOROIDAL = 4    /* B = b0 * (-y, x, 0) / r, r = sqrt(x^2 + y^2) */
+};
+
+/* Grid3f payload and GridProperties (Grid.h:75).  values holds Nx*Ny*Nz
+ * Vector3f cells (12 bytes each, x y z floats), cell (ix,iy,iz) at
+ * ix*Ny*Nz + iy*Nz + iz (Grid.h:338).  Host memory. */
+typedef struct crp_grid3f_desc {
+    const float *values;
+    uint64_t nx, ny, nz;
+    double origin[3];  /* lower-left-front corner of the volume */
+    double spacing[3];
+    int32_t reflective;  /* Grid::setReflective */
+    int32_t clip_volume; /* Grid::setClipVolume */
+} crp_grid3f_desc;
+
+/* Wave modes of a PlaneWaveTurbulence (PlaneWaveTurbulence.cpp:79-229),
+ * as produced by crp_plane_wave_modes().  Host memory. */
+typedef struct crp_plane_wave_desc {
+    int32_t n_modes;
+    int32_t seed;        /* constructor seed the modes were drawn with */
+    const double *xi;    /* 3*n_modes, polarisation unit vectors, mode-major */
+    const double *kappa; /* 3*n_modes, propagation unit vectors, mode-major */
+    const double *k;     /* n_modes, wave numbers [1/m] */
+    const double *beta;  /* n_modes, phases */
+    const double *ak;    /* n_modes, amplitudes [T] */
+    /* TurbulenceSpectrum the modes came from (TurbulentField.h:17): the
+     * device reads only the mode arrays above. */
+    double brms, lmin, lmax, lbendover, sindex, qindex;
+} crp_plane_wave_desc;
+
+/* One summand of the field (a MagneticFieldList of these is their sum,
+ * MagneticField.cpp:64).  A component may be wrapped in a
+ * PeriodicMagneticField (MagneticField.cpp:41). */
+typedef struct crp_field_component {
+    int32_t kind;
+    int32_t periodic;            /* wrap in PeriodicMagneticField */
+    int32_t periodic_reflective; /* PeriodicMagneticField reflective flag */
+    int32_t _pad0;
+    double periodic_origin[3];
+    double periodic_extends[3];
+    crp_grid3f_desc grid;
+    crp_plane_wave_desc plane_wave;
+    double uniform[3];
+    double toroidal_b0;
+} crp_field_component;
+
+/* ------------------------------------------------------------------------
+ * Module chain description (ModuleList order)
+ * ---------------------------------------------------------------------- */
+
+enum crp_module_kind {
+    CRP_MODULE_PROPAGATION = 1,
+    CRP_MODULE_MAX_TRAJECTORY_LENGTH = 2, /* MaximumTrajectoryLength (BreakCondition.cpp:42) */
+    CRP_MODULE_OBSERVER = 3               /* Observer (Observer.cpp:27) */
+};
+
+enum crp_propagator {
+    CRP_PROP_CK = 1,  /* PropagationCK (PropagationCK.cpp:77) */
+    CRP_PROP_BP = 2,  /* PropagationBP (PropagationBP.cpp:62) */
+    CRP_PROP_SDE = 3  /* DiffusionSDE  (DiffusionSDE.cpp:47) */
+};
+
+enum crp_observer_feature {
+    CRP_OBSERVER_SURFACE_SPHERE = 1, /* ObserverSurface(Sphere) (Observer.cpp:394, Geometry.cpp:41) */
+    CRP_OBSERVER_DETECT_ALL = 2      /* ObserverDetectAll (Observer.cpp:93) */
+};
+
+typedef struct crp_module_desc {
+    int32_t kind;
+    /* CRP_MODULE_PROPAGATION */
+    int32_t propagator;
+    double tolerance;
+    double min_step; /* [m] */
+    double max_step; /* [m]; min_step == max_step selects the fixed-step branch */
+    double sde_epsilon; /* DiffusionSDE::setEpsilon */
+    double sde_alpha;   /* DiffusionSDE::setAlpha */
+    double sde_scale;   /* DiffusionSDE::setScale */
+    /* CRP_MODULE_MAX_TRAJECTORY_LENGTH */
+    double max_length;            /* [m] */
+    int32_t per_candidate_length; /* use crp_candidates.max_length[i] instead */
+    /* CRP_MODULE_OBSERVER */
+    int32_t observer_feature;
+    double sphere_center[3];
+    double sphere_radius;
+    int32_t deactivate_on_detection; /* Observer::setDeactivateOnDetection, default 1 */
+    int32_t record;                  /* the detection (or rejection) action writes a record */
+} crp_module_desc;
+
+enum crp_precision {
+    CRP_PRECISION_FP64 = 0,  /* the reference's arithmetic, operation for operation */
+    CRP_PRECISION_MIXED = 1  /* FP32 field and stage arithmetic, FP64 accumulation */
+};
+
+typedef struct crp_plan_desc {
+    uint32_t abi_version; /* CRP_ABI_VERSION */
+    int32_t precision;
+    const crp_field_component *fields;
+    int32_t n_fields;
+    int32_t n_modules;
+    const crp_module_desc *modules;
+    uint64_t seed; /* key of the counter-based random stream (DiffusionSDE) */
+} crp_plan_desc;
+
+/* ------------------------------------------------------------------------
+ * Candidate state, structure of arrays (Candidate.h:27, ParticleState.h:22)
+ * ---------------------------------------------------------------------- */
+
+enum crp_candidate_flags {
+    CRP_FLAG_REJECTED = 1u, /* property "Rejected" set by MaximumTrajectoryLength */
+    CRP_FLAG_DETECTED = 2u, /* Observer detection */
+    CRP_FLAG_NAN = 4u       /* DiffusionSDE deactivated a NaN position (DiffusionSDE.cpp:177) */
+};
+
+/* Every array has n entries.  All pointers are host pointers for crp_run()
+ * and device pointers for crp_run_device().  max_length may be NULL unless a
+ * module sets per_candidate_length. */
+typedef struct crp_candidates {
+    int32_t *id;        /* PDG id (ParticleState::setId) */
+    double *charge;     /* [C] */
+    double *energy;     /* [J] */
+    double *x, *y, *z;  /* current position [m] */
+    double *dx, *dy, *dz; /* current direction (unit vector) */
+    double *px, *py, *pz; /* previous position (Candidate::previous) */
+    double *trajectory_length; /* [m] */
+    double *time;              /* [s] */
+    double *current_step;      /* [m] */
+    double *next_step;         /* [m] */
+    uint8_t *active;
+    uint32_t *flags;     /* crp_candidate_flags */
+    double *max_length;  /* per-candidate MaximumTrajectoryLength [m], optional */
+    uint64_t *step_count; /* accepted steps taken so far, optional */
+} crp_candidates;
+
+/* Output records written by an Observer or MaximumTrajectoryLength module
+ * with record != 0 (the detection / reject action, e.g. TextOutput).  Device
+ * memory for crp_run_device(), host memory for crp_run().  One record holds
+ * the candidate index and its state at the moment of the action. */
+typedef struct crp_records {
+    uint64_t capacity;
+    uint64_t *count;      /* records written (may exceed capacity: the rest were dropped) */
+    uint64_t *index;      /* candidate index */
+    int32_t *module;      /* module position in the chain */
+    double *trajectory_length, *time;
+    double *x, *y, *z;
+    double *dx, *dy, *dz;
+    double *energy;
+    int32_t *id;
+} crp_records;
+
+enum crp_run_mode {
+    CRP_MODE_AUTO = 0,
+    CRP_MODE_CHUNKED = 1,   /* one thread per candidate, fixed steps per launch */
+    CRP_MODE_PERSISTENT = 2 /* persistent CTAs refill lanes from a device queue */
+};
+
+typedef struct crp_run_opts {
+    int32_t mode;
+    int32_t block_size;        /* 0: autotuned */
+    int32_t ctas_per_sm;       /* 0: autotuned (persistent mode) */
+    int32_t steps_per_launch;  /* 0: default (chunked mode) */
+    int32_t refill_threshold;  /* persistent: lanes idle before a warp refills, 0: autotuned */
+    int32_t _pad0;
+    uint64_t max_steps;        /* per-candidate cap on accepted steps, 0: none */
+    volatile int32_t *cancel;  /* host flag polled between launches, may be NULL */
+    void *stream;              /* cudaStream_t, NULL: the legacy default stream */
+    crp_records *records;      /* may be NULL */
+} crp_run_opts;
+
+typedef struct crp_run_stats {
+    uint64_t particle_steps;    /* accepted propagation steps */
+    uint64_t tries;             /* propagation tries including rejected ones */
+    uint64_t field_evaluations; /* getField calls */
+    uint64_t launches;          /* kernel launches of the stepping path */
+    uint64_t active_left;       /* candidates still active on return */
+    double device_ms;           /* device time of the stepping kernels */
+} crp_run_stats;
+
+typedef struct crp_plan crp_plan;
+
+/* Library and device */
+uint32_t crp_abi_version(void);
+crp_status crp_last_error(char *buffer, size_t size);
+crp_status crp_device_count(int32_t *count);
+
+/* Plan: validates the chain the way the reference constructors and setters
+ * do (PropagationCK.cpp:163-190, PropagationBP.cpp:148-178,
+ * DiffusionSDE.cpp:280-320), uploads grids and wave-mode tables to the
+ * current device. */
+crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **plan);
+crp_status crp_plan_destroy(crp_plan *plan);
+
+/* Run every active candidate until it is inactive (or max_steps).  Host
+ * arrays: copied to the device and back inside the call. */
+crp_status crp_run(crp_plan *plan, const crp_candidates *host, uint64_t n,
+                   const crp_run_opts *opts, crp_run_stats *stats);
+/* Same, on device-resident arrays, asynchronous with respect to the host
+ * only where stats is NULL and no cancel flag is given. */
+crp_status crp_run_device(crp_plan *plan, const crp_candidates *device, uint64_t n,
+                          const crp_run_opts *opts, crp_run_stats *stats);
+
+/* Field of the plan (sum of its components) at n positions (device arrays,
+ * planar x[n] y[n] z[n] in and out).  MagneticField::getField. */
+crp_status crp_field_eval(crp_plan *plan, uint64_t n, const double *pos_xyz,
+                          double *b_xyz, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Host-side set-up and output (no device needed)
+ * ---------------------------------------------------------------------- */
+
+/* Charge of a particle id as ParticleState::setId assigns it
+ * (ParticleState.cpp:50): Z*eplus for nuclei (negative for anti-nuclei),
+ * HepPID charge for leptons, photons and neutrinos. */
+crp_status crp_particle_charge(int32_t id, double *charge);
+
+/* n draws of crpropa::Random seeded with seed (Random.cpp): kind 0 rand(),
+ * 1 randUniform(a, b), 2 randVector() (3 values per draw), 3
+ * randPowerLaw(a, b, c), 6 randInt(). */
+crp_status crp_random_draws(uint32_t seed, int32_t kind, uint64_t n, double a, double b,
+                            double c, double *out);
+
+/* Wave modes of PlaneWaveTurbulence(TurbulenceSpectrum(brms, lmin, lmax,
+ * lbendover, sindex, qindex), nm, seed) (PlaneWaveTurbulence.cpp:79-229),
+ * drawn with the reference's MT19937 sequence.  seed must be non-zero. */
+crp_status crp_plane_wave_modes(double brms, double lmin, double lmax, double lbendover,
+                                double sindex, double qindex, int32_t nm, int32_t seed,
+                                double *xi, double *kappa, double *k, double *beta, double *ak);
+
+/* A Source with SourceParticleType / SourceMultipleParticleTypes,
+ * SourceEnergy or SourcePowerLawSpectrum, and SourceIsotropicEmission or
+ * SourceDirection (Source.cpp:74-150, :742, :808), sampled in that feature
+ * order from one crpropa::Random stream (Random::seedThreads(seed), one
+ * thread). */
+typedef struct crp_source_desc {
+    int32_t n_types;
+    int32_t spectrum;   /* 1: power law emin..emax with index; 0: fixed energy */
+    const int32_t *ids;
+    const double *abundances; /* NULL: equal */
+    double emin, emax, index;
+    double energy;
+    int32_t isotropic;  /* 1: SourceIsotropicEmission; 0: direction[] */
+    int32_t _pad0;
+    double direction[3];
+} crp_source_desc;
+
+crp_status crp_source_sample(const crp_source_desc *src, uint32_t seed, uint64_t n, int32_t *id,
+                             double *energy, double *dir_xyz /* planar x[n] y[n] z[n] */);
+
+/* Output columns (Output.h:76 OutputColumn, bit = enum value). */
+enum crp_output_column {
+    CRP_COL_TRAJECTORY_LENGTH = 0, CRP_COL_COLUMN_DENSITY = 1, CRP_COL_REDSHIFT = 2,
+    CRP_COL_CURRENT_ID = 3, CRP_COL_CURRENT_ENERGY = 4, CRP_COL_CURRENT_POSITION = 5,
+    CRP_COL_CURRENT_DIRECTION = 6, CRP_COL_SOURCE_ID = 7, CRP_COL_SOURCE_ENERGY = 8,
+    CRP_COL_SOURCE_POSITION = 9, CRP_COL_SOURCE_DIRECTION = 10, CRP_COL_CREATED_ID = 11,
+    CRP_COL_CREATED_ENERGY = 12, CRP_COL_CREATED_POSITION = 13, CRP_COL_CREATED_DIRECTION = 14,
+    CRP_COL_CANDIDATE_TAG = 15, CRP_COL_SERIAL_NUMBER = 16, CRP_COL_WEIGHT = 17, CRP_COL_TIME = 18
+};
+
+typedef struct crp_output_desc {
+    uint32_t columns;        /* bitset of crp_output_column */
+    int32_t one_dimensional; /* Output::set1D */
+    double length_scale, time_scale, energy_scale;
+    const char *version;     /* "CRPropa version" header line */
+} crp_output_desc;
+
+/* Rows to print: one per detected candidate, vectors interleaved xyz. */
+typedef struct crp_output_rows {
+    const uint64_t *serial;
+    const double *trajectory_length, *time;
+    const int32_t *id;
+    const double *energy, *position, *direction;
+    const int32_t *source_id;
+    const double *source_energy, *source_position, *source_direction;
+    const double *weight; /* NULL: 1 */
+} crp_output_rows;
+
+/* TextOutput (TextOutput.cpp:55 printHeader, :166 process): write (or
+ * append) n lines, optionally preceded by the header. */
+crp_status crp_text_output_write(const char *path, int32_t append, int32_t header,
+                                 const crp_output_desc *desc, uint64_t n,
+                                 const crp_output_rows *rows);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRP_GPU_H */

@@ -1,0 +1,759 @@
+/*
+ * crp_oracle.c -- TEST INFRASTRUCTURE: the oracle.
+ *
+ * A plain-C restatement of CRPropa3's charged-particle stepping path, used
+ * only as the checker of the CUDA path (by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg).  The product
+ * never links, loads or calls it.
+ *
+ * Every function follows the reference operation for operation, so that the
+ * FP64 device path can be compared bit for bit where the reference uses only
+ * + - * / sqrt floor (Boris push over a Grid3f).  Build without FMA
+ * contraction (-ffp-contract=off) and without -ffast-math.  Citations are to
+ * files of the reference project (CRPropa3).
+ *
+ * Pinned against the reference itself: tests/test_oracle_vs_reference.py
+ * runs this oracle and the reference compiled from its sources
+ * (oracle/Makefile) on the same inputs, and tests/golden/ holds vectors
+ * generated from the reference by tests/golden/make_golden.py.
+ *
+ * Randomness: crpropa::Random (MT19937, src/Random.cpp) is restated for the
+ * host-side draws (source sampling, PlaneWaveTurbulence and GridTurbulence
+ * set-up).  DiffusionSDE here draws from Philox4x32-10 (Salmon et al.,
+ * "Parallel random numbers: as easy as 1, 2, 3", SC'11) keyed by the run seed
+ * with counter (step, candidate), exactly as the device does, and transforms
+ * the 32-bit words the way Random::randNorm / randUniform / randVector /
+ * randConeVector do (src/Random.cpp:104-166); the reference's own MT stream
+ * is compared with it only in distribution.
+ */
+#include "crp_gpu.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* include/crpropa/Units.h:54-55, :114-115 */
+static const double c_light = 2.99792458e8;
+static const double kpc_unit = 1e3 * (648000 / M_PI * 149597870700.0);
+
+/* ------------------------------------------------------------------------
+ * Vector3d (include/crpropa/Vector3.h)
+ * ---------------------------------------------------------------------- */
+typedef struct { double x, y, z; } v3;
+
+static inline v3 mk(double x, double y, double z) { v3 r = {x, y, z}; return r; }
+static inline v3 add(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 muls(v3 a, double f) { return mk(a.x * f, a.y * f, a.z * f); }  /* :305 */
+static inline v3 divs(v3 a, double f) { return mk(a.x / f, a.y / f, a.z / f); }  /* :317 */
+static inline v3 mulv(v3 a, v3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline v3 divv(v3 a, v3 b) { return mk(a.x / b.x, a.y / b.y, a.z / b.z); }
+static inline double dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; } /* :259 */
+static inline v3 cross(v3 a, v3 v) {  /* :264 */
+    return mk(a.y * v.z - v.y * a.z, a.z * v.x - v.z * a.x, a.x * v.y - v.x * a.y);
+}
+static inline double norm(v3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); } /* :127 */
+static inline v3 unit(v3 a) { return divs(a, norm(a)); }                           /* :157 */
+static inline v3 vfloor(v3 a) { return mk(floor(a.x), floor(a.y), floor(a.z)); }
+static inline double dmin(double a, double b) { return (b < a) ? b : a; } /* std::min */
+static inline double dmax(double a, double b) { return (a < b) ? b : a; } /* std::max */
+static inline double clipd(double x, double lo, double hi) { return dmax(lo, dmin(x, hi)); } /* Common.h:30 */
+
+/* ------------------------------------------------------------------------
+ * MT19937 as crpropa::Random (src/Random.cpp)
+ * ---------------------------------------------------------------------- */
+typedef struct { uint32_t state[624]; int left; int next; } mt_t;
+
+static uint32_t mt_twist(uint32_t m, uint32_t s0, uint32_t s1) {
+    uint32_t y = (s0 & 0x80000000u) | (s1 & 0x7fffffffu);
+    return m ^ (y >> 1) ^ ((uint32_t)(-(int32_t)(s1 & 1u)) & 0x9908b0dfu);
+}
+
+static void mt_reload(mt_t *r) { /* Random.cpp:379 */
+    uint32_t *s = r->state;
+    int i;
+    for (i = 0; i < 624 - 397; i++) s[i] = mt_twist(s[i + 397], s[i], s[i + 1]);
+    for (; i < 623; i++) s[i] = mt_twist(s[i + 397 - 624], s[i], s[i + 1]);
+    s[623] = mt_twist(s[396], s[623], s[0]);
+    r->left = 624;
+    r->next = 0;
+}
+
+void oracle_mt_seed(mt_t *r, uint32_t seed) { /* Random.cpp:306, :367 */
+    r->state[0] = seed;
+    for (int i = 1; i < 624; i++)
+        r->state[i] = 1812433253u * (r->state[i - 1] ^ (r->state[i - 1] >> 30)) + (uint32_t)i;
+    mt_reload(r);
+}
+
+static uint32_t mt_int(mt_t *r) { /* Random.cpp:248 */
+    if (r->left == 0) mt_reload(r);
+    --r->left;
+    uint32_t s1 = r->state[r->next++];
+    s1 ^= (s1 >> 11);
+    s1 ^= (s1 << 7) & 0x9d2c5680u;
+    s1 ^= (s1 << 15) & 0xefc60000u;
+    return s1 ^ (s1 >> 18);
+}
+
+static double mt_rand(mt_t *r) { return (double)mt_int(r) * (1.0 / 4294967295.0); } /* :75 */
+static double mt_uniform(mt_t *r, double a, double b) { return a + (b - a) * mt_rand(r); } /* :117 */
+
+static v3 mt_vector(mt_t *r) { /* Random.cpp:141 */
+    double z = mt_uniform(r, -1.0, 1.0);
+    double t = mt_uniform(r, -1.0 * M_PI, M_PI);
+    double rr = sqrt(1 - z * z);
+    return mk(rr * cos(t), rr * sin(t), z);
+}
+
+static double mt_power_law(mt_t *r, double index, double mn, double mx) { /* :189 */
+    if (fabs(index + 1.0) < 2.220446049250313e-16) {
+        double p1 = log(mx), p2 = log(mn);
+        return exp((p1 - p2) * mt_rand(r) + p2);
+    }
+    double p1 = pow(mx, index + 1), p2 = pow(mn, index + 1);
+    double ex = 1 / (index + 1);
+    return pow((p1 - p2) * mt_rand(r) + p2, ex);
+}
+
+size_t oracle_mt_size(void) { return sizeof(mt_t); }
+
+/* Draw n values the way ref_shim's ref_random() does (same kinds). */
+int oracle_random(uint32_t seed, int kind, uint64_t n, double a, double b, double c, double *out) {
+    mt_t r;
+    oracle_mt_seed(&r, seed);
+    for (uint64_t i = 0; i < n; i++) {
+        if (kind == 0) out[i] = mt_rand(&r);
+        else if (kind == 1) out[i] = mt_uniform(&r, a, b);
+        else if (kind == 2) { v3 v = mt_vector(&r); out[3*i] = v.x; out[3*i+1] = v.y; out[3*i+2] = v.z; }
+        else if (kind == 3) out[i] = mt_power_law(&r, a, b, c);
+        else if (kind == 6) out[i] = (double)mt_int(&r);
+        else return 1;
+    }
+    return 0;
+}
+
+/* Source of the stepping workloads (Source.cpp:22): SourcePosition,
+ * SourceParticleType / SourceMultipleParticleTypes (randBin over the
+ * abundance CDF, Random.cpp:128), SourcePowerLawSpectrum, SourceIsotropicEmission,
+ * drawn in that order from one MT19937 stream. */
+int oracle_sample_source(uint32_t seed, uint64_t n, int ntypes, const int32_t *ids,
+                         const double *abundances, double emin, double emax, double index,
+                         int32_t *id_out, double *e_out, double *dir_out) {
+    mt_t r;
+    oracle_mt_seed(&r, seed);
+    double cdf[64];
+    if (ntypes < 1 || ntypes > 64) return 1;
+    double acc = 0;
+    for (int i = 0; i < ntypes; i++) { acc = (i ? cdf[i - 1] : 0) + abundances[i]; cdf[i] = acc; }
+    for (uint64_t i = 0; i < n; i++) {
+        int32_t id = ids[0];
+        if (ntypes > 1) {
+            double u = mt_rand(&r) * cdf[ntypes - 1];
+            int k = 0;
+            while (k < ntypes && cdf[k] < u) k++;  /* std::lower_bound */
+            id = ids[k];
+        }
+        id_out[i] = id;
+        e_out[i] = mt_power_law(&r, index, emin, emax);
+        v3 d = mt_vector(&r);
+        d = divs(d, norm(d)); /* ParticleState::setDirection */
+        dir_out[3*i] = d.x; dir_out[3*i+1] = d.y; dir_out[3*i+2] = d.z;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Philox4x32-10 (published algorithm) and the reference's transforms
+ * ---------------------------------------------------------------------- */
+typedef struct { uint32_t v[4]; } u32x4;
+
+u32x4 oracle_philox(u32x4 ctr, uint32_t k0, uint32_t k1) {
+    for (int round = 0; round < 10; round++) {
+        if (round) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        uint64_t p0 = (uint64_t)0xD2511F53u * ctr.v[0];
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * ctr.v[2];
+        u32x4 o;
+        o.v[0] = (uint32_t)(p1 >> 32) ^ ctr.v[1] ^ k0;
+        o.v[1] = (uint32_t)p1;
+        o.v[2] = (uint32_t)(p0 >> 32) ^ ctr.v[3] ^ k1;
+        o.v[3] = (uint32_t)p0;
+        ctr = o;
+    }
+    return ctr;
+}
+
+void oracle_philox_block(const uint32_t *ctr, const uint32_t *key, uint32_t *out) {
+    u32x4 c = {{ctr[0], ctr[1], ctr[2], ctr[3]}};
+    u32x4 o = oracle_philox(c, key[0], key[1]);
+    memcpy(out, o.v, sizeof(o.v));
+}
+
+/* Per-step stream of a candidate: word w of step s of candidate i is word
+ * (w % 4) of Philox(ctr = {lo(4s + w/4), hi(4s + w/4), lo(i), hi(i)},
+ * key = {lo(seed), hi(seed)}). */
+typedef struct {
+    uint64_t seed, cand, step;
+    u32x4 block;
+    int cursor;
+} stream_t;
+
+static uint32_t stream_int(stream_t *s) {
+    int w = s->cursor++;
+    if ((w & 3) == 0) {
+        uint64_t c = s->step * 4 + (uint64_t)(w >> 2);
+        u32x4 ctr = {{(uint32_t)c, (uint32_t)(c >> 32), (uint32_t)s->cand, (uint32_t)(s->cand >> 32)}};
+        s->block = oracle_philox(ctr, (uint32_t)s->seed, (uint32_t)(s->seed >> 32));
+    }
+    return s->block.v[w & 3];
+}
+static double stream_rand(stream_t *s) { return (double)stream_int(s) * (1.0 / 4294967295.0); }
+static double stream_uniform(stream_t *s, double a, double b) { return a + (b - a) * stream_rand(s); }
+static double stream_norm(stream_t *s) { /* Random.cpp:104 randNorm(0, 1) */
+    double dblexc = ((double)stream_int(s) + 0.5) * (1.0 / 4294967296.0);
+    double r = sqrt(-2.0 * log(1.0 - dblexc)) * 1.0;
+    double phi = 2.0 * 3.14159265358979323846264338328 * ((double)stream_int(s) * (1.0 / 4294967296.0));
+    return 0.0 + r * cos(phi);
+}
+static v3 stream_vector(stream_t *s) { /* Random.cpp:141 */
+    double z = stream_uniform(s, -1.0, 1.0);
+    double t = stream_uniform(s, -1.0 * M_PI, M_PI);
+    double r = sqrt(1 - z * z);
+    return mk(r * cos(t), r * sin(t), z);
+}
+static v3 rotated(v3 v, v3 axis, double angle) { /* Vector3.h:206 getRotated */
+    v3 u = axis;
+    if (norm(u) != 0.) u = divs(u, norm(u));
+    double c = cos(angle), s = sin(angle);
+    v3 Rx = mk(c + u.x * u.x * (1 - c), u.x * u.y * (1 - c) - u.z * s, u.x * u.z * (1 - c) + u.y * s);
+    v3 Ry = mk(u.y * u.x * (1 - c) + u.z * s, c + u.y * u.y * (1 - c), u.y * u.z * (1 - c) - u.x * s);
+    v3 Rz = mk(u.z * u.x * (1 - c) - u.y * s, u.z * u.y * (1 - c) + u.x * s, c + u.z * u.z * (1 - c));
+    return mk(dot(v, Rx), dot(v, Ry), dot(v, Rz));
+}
+static v3 stream_cone(stream_t *s, v3 mean, double radius) { /* Random.cpp:159, :147 */
+    double theta = acos(stream_uniform(s, 1, cos(radius)));
+    v3 axis = cross(mean, stream_vector(s));
+    return rotated(mean, axis, theta);
+}
+
+/* ------------------------------------------------------------------------
+ * Fields
+ * ---------------------------------------------------------------------- */
+
+/* Grid<Vector3f>::interpolate / trilinearInterpolate (Grid.h:318, :540),
+ * values and weights in float as Vector3f * double converts the weight to
+ * float (Vector3.h:305). */
+static v3 grid_field(const crp_grid3f_desc *g, v3 pos) {
+    v3 origin = mk(g->origin[0], g->origin[1], g->origin[2]);
+    v3 spacing = mk(g->spacing[0], g->spacing[1], g->spacing[2]);
+    int Nx = (int)g->nx, Ny = (int)g->ny, Nz = (int)g->nz;
+    if (g->clip_volume) { /* Grid.h:320 */
+        v3 edge = add(origin, mulv(mk((double)g->nx, (double)g->ny, (double)g->nz), spacing));
+        int in = (pos.x >= origin.x) && (pos.x <= edge.x);
+        in &= (pos.y >= origin.y) && (pos.y <= edge.y);
+        in &= (pos.z >= origin.z) && (pos.z <= edge.z);
+        if (!in) return mk(0, 0, 0);
+    }
+    v3 gridOrigin = add(origin, divs(spacing, 2)); /* Grid.h:227 */
+    v3 r = divv(sub(pos, gridOrigin), spacing);
+    int ix0, ix1, iy0, iy1, iz0, iz1;
+    double fX0, fY0, fZ0;
+    if (g->reflective) { /* Grid.h:49 reflectiveClamp */
+        double rr[3] = {r.x, r.y, r.z};
+        int n[3] = {Nx, Ny, Nz}, lo[3], hi[3];
+        double res[3];
+        for (int a = 0; a < 3; a++) {
+            double x = rr[a];
+            while ((x < -0.5) || (x > (n[a] - 0.5)))
+                x = 2 * n[a] * (x > (n[a] - 0.5)) - x - 1;
+            res[a] = x;
+            lo[a] = (int)floor(x);
+            hi[a] = lo[a] + (lo[a] < n[a] - 1);
+            if (x < 0) { lo[a] = 0; hi[a] = 0; }
+        }
+        ix0 = lo[0]; ix1 = hi[0]; iy0 = lo[1]; iy1 = hi[1]; iz0 = lo[2]; iz1 = hi[2];
+        fX0 = res[0] - floor(res[0]);
+        fY0 = res[1] - floor(res[1]);
+        fZ0 = res[2] - floor(res[2]);
+    } else { /* Grid.h:31 periodicClamp */
+        ix0 = (((int)floor(r.x) % Nx) + Nx) % Nx; ix1 = (ix0 + 1) % Nx;
+        iy0 = (((int)floor(r.y) % Ny) + Ny) % Ny; iy1 = (iy0 + 1) % Ny;
+        iz0 = (((int)floor(r.z) % Nz) + Nz) % Nz; iz1 = (iz0 + 1) % Nz;
+        fX0 = r.x - floor(r.x);
+        fY0 = r.y - floor(r.y);
+        fZ0 = r.z - floor(r.z);
+    }
+    float fx1 = (float)(1 - fX0), fy1 = (float)(1 - fY0), fz1 = (float)(1 - fZ0);
+    float fx0 = (float)fX0, fy0 = (float)fY0, fz0 = (float)fZ0;
+    const float *v = g->values;
+    size_t sy = (size_t)Nz, sx = (size_t)Ny * (size_t)Nz;
+#define CELL(i, j, k) (v + 3 * ((size_t)(i) * sx + (size_t)(j) * sy + (size_t)(k)))
+    const int cx[8] = {ix0, ix1, ix0, ix0, ix1, ix0, ix1, ix1};
+    const int cy[8] = {iy0, iy0, iy1, iy0, iy0, iy1, iy1, iy1};
+    const int cz[8] = {iz0, iz0, iz0, iz1, iz1, iz1, iz0, iz1};
+    const float wx[8] = {fx1, fx0, fx1, fx1, fx0, fx1, fx0, fx0};
+    const float wy[8] = {fy1, fy1, fy0, fy1, fy1, fy0, fy0, fy0};
+    const float wz[8] = {fz1, fz1, fz1, fz0, fz0, fz0, fz1, fz0};
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    for (int c = 0; c < 8; c++) {
+        const float *p = CELL(cx[c], cy[c], cz[c]);
+        bx += p[0] * wx[c] * wy[c] * wz[c];
+        by += p[1] * wx[c] * wy[c] * wz[c];
+        bz += p[2] * wx[c] * wy[c] * wz[c];
+    }
+#undef CELL
+    return mk(bx, by, bz);
+}
+
+/* PlaneWaveTurbulence::getField, scalar branch (PlaneWaveTurbulence.cpp:233-239). */
+static v3 plane_wave_field(const crp_plane_wave_desc *p, v3 pos) {
+    v3 B = mk(0, 0, 0);
+    for (int i = 0; i < p->n_modes; i++) {
+        v3 kap = mk(p->kappa[3*i], p->kappa[3*i+1], p->kappa[3*i+2]);
+        v3 xi = mk(p->xi[3*i], p->xi[3*i+1], p->xi[3*i+2]);
+        double z_ = dot(pos, kap);
+        B = add(B, muls(muls(xi, p->ak[i]), cos(p->k[i] * z_ + p->beta[i])));
+    }
+    return B;
+}
+
+static v3 component_field(const crp_field_component *f, v3 position) {
+    v3 pos = position;
+    if (f->periodic) { /* MagneticField.cpp:41 */
+        v3 o = mk(f->periodic_origin[0], f->periodic_origin[1], f->periodic_origin[2]);
+        v3 e = mk(f->periodic_extends[0], f->periodic_extends[1], f->periodic_extends[2]);
+        v3 n = vfloor(divv(sub(position, o), e));
+        v3 p = sub(sub(position, o), mulv(n, e));
+        if (f->periodic_reflective) {
+            if ((long)fabs(n.x) % 2 == 1) p.x = e.x - p.x;
+            if ((long)fabs(n.y) % 2 == 1) p.y = e.y - p.y;
+            if ((long)fabs(n.z) % 2 == 1) p.z = e.z - p.z;
+        }
+        pos = p;
+    }
+    switch (f->kind) {
+    case CRP_FIELD_GRID: return grid_field(&f->grid, pos);
+    case CRP_FIELD_PLANE_WAVE: return plane_wave_field(&f->plane_wave, pos);
+    case CRP_FIELD_UNIFORM: return mk(f->uniform[0], f->uniform[1], f->uniform[2]);
+    case CRP_FIELD_TOROIDAL: {
+        double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+        return muls(mk(-pos.y, pos.x, 0.), f->toroidal_b0 / r);
+    }
+    }
+    return mk(0, 0, 0);
+}
+
+/* MagneticFieldList::getField (MagneticField.cpp:64) or the single field. */
+static v3 field_at(const crp_plan_desc *d, v3 pos) {
+    if (d->n_fields == 1) return component_field(&d->fields[0], pos);
+    v3 b = mk(0, 0, 0);
+    for (int i = 0; i < d->n_fields; i++) b = add(b, component_field(&d->fields[i], pos));
+    return b;
+}
+
+int oracle_field_eval(const crp_plan_desc *d, uint64_t n, const double *pos, double *out) {
+    for (uint64_t i = 0; i < n; i++) {
+        v3 b = field_at(d, mk(pos[i], pos[n + i], pos[2 * n + i]));
+        out[i] = b.x; out[n + i] = b.y; out[2 * n + i] = b.z;
+    }
+    return 0;
+}
+
+/* PlaneWaveTurbulence constructor (PlaneWaveTurbulence.cpp:79-229) with
+ * TurbulenceSpectrum::energySpectrum (TurbulentField.h:75). */
+int oracle_plane_wave_modes(double brms, double lmin, double lmax, double lbendover,
+                            double sindex, double qindex, int nm, uint32_t seed, double *xi,
+                            double *kappa, double *k, double *beta, double *ak) {
+    if (nm <= 1) return 1;
+    mt_t r;
+    oracle_mt_seed(&r, seed);
+    double kmax = 2 * M_PI / lmin, kmin = 2 * M_PI / lmax;
+    double delta = log10(kmax / kmin);
+    for (int i = 0; i < nm; i++)
+        k[i] = pow(10, log10(kmin) + ((double)i) / ((double)(nm - 1)) * delta);
+    double delta_k0 = (k[1] - k[0]) / k[1];
+    double sum = 0;
+    for (int i = 0; i < nm; i++) {
+        double kk = k[i];
+        double kHat = kk * lbendover;
+        double kh = kk * lbendover;
+        double es = pow(kh, qindex) / pow(1.0 + kh * kh, (sindex + qindex) / 2.0 + 1.0);
+        double Gk = es * (1 + kHat * kHat);
+        ak[i] = Gk * delta_k0 * kk;
+        sum += ak[i];
+        double phi = mt_uniform(&r, -M_PI, M_PI);
+        double costheta = mt_uniform(&r, -1., 1.);
+        double sintheta = sqrt(1 - costheta * costheta);
+        double alpha = mt_uniform(&r, 0, 2 * M_PI);
+        double b = mt_uniform(&r, 0, 2 * M_PI);
+        kappa[3*i] = sintheta * cos(phi);
+        kappa[3*i+1] = sintheta * sin(phi);
+        kappa[3*i+2] = costheta;
+        xi[3*i] = costheta * cos(phi) * cos(alpha) + sin(phi) * sin(alpha);
+        xi[3*i+1] = costheta * sin(phi) * cos(alpha) - cos(phi) * sin(alpha);
+        xi[3*i+2] = -sintheta * cos(alpha);
+        beta[i] = b;
+    }
+    for (int i = 0; i < nm; i++) ak[i] = sqrt(2 * ak[i] / sum) * brms;
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Candidate (Candidate.cpp) and the modules
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    v3 pos, dir, prev;
+    double E, q, len, time, cur, next, maxlen;
+    int32_t id;
+    int active;
+    uint32_t flags;
+    uint64_t index, steps;
+} cand_t;
+
+static void set_current_step(cand_t *c, double s) { /* Candidate.cpp:92 */
+    c->cur = s;
+    c->len += s;
+    c->time += s / c_light;
+}
+static void limit_next_step(cand_t *c, double s) { c->next = dmin(c->next, s); } /* :102 */
+
+/* PropagationBP::dY (PropagationBP.cpp:19) */
+static void bp_dy(const crp_plan_desc *d, v3 *pos, v3 *dir, double step, double q, double m) {
+    v3 x = *pos, u = *dir;
+    x = add(x, divs(muls(u, step), 2.));
+    v3 B = field_at(d, x);
+    v3 t = divs(muls(divs(divs(muls(B, q), 2), m), step), c_light);
+    v3 s = divs(muls(t, 2), (1 + dot(t, t)));
+    v3 vh = add(u, cross(u, t));
+    u = add(u, cross(vh, s));
+    x = add(x, divs(muls(u, step), 2.));
+    *pos = x; *dir = u;
+}
+
+/* PropagationBP::process (PropagationBP.cpp:62) */
+static void bp_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t *c, uint64_t *tries) {
+    c->prev = c->pos;
+    double q = c->q, step = m->max_step;
+    if (q == 0) {
+        step = clipd(c->next, m->min_step, m->max_step);
+        c->pos = add(c->pos, muls(c->dir, step));
+        set_current_step(c, step);
+        c->next = m->max_step;
+        return;
+    }
+    double newStep = step;
+    double mass = c->E / (c_light * c_light);
+    v3 xo = c->pos, uo = c->dir;
+    if (m->min_step == m->max_step) {
+        bp_dy(d, &xo, &uo, step, q, mass);
+        (*tries)++;
+    } else {
+        step = clipd(c->next, m->min_step, m->max_step);
+        newStep = step;
+        while (1) {
+            v3 x1 = c->pos, u1 = c->dir, xh = c->pos, uh = c->dir;
+            bp_dy(d, &x1, &u1, step, q, mass);           /* tryStep :8 */
+            bp_dy(d, &xh, &uh, step / 2, q, mass);
+            bp_dy(d, &xh, &uh, step / 2, q, mass);
+            (*tries)++;
+            double S = norm(sub(x1, xh)) / (step * (1 - 1 / 4.)); /* :152 */
+            xo = x1; uo = u1;
+            double r = norm(mk(S, S, S)) / m->tolerance;
+            if (r > 1) {
+                if (step == m->min_step) break;
+                newStep = step * 0.95 * pow(r, -0.2);
+                newStep = dmax(newStep, 0.1 * step);
+                newStep = dmax(newStep, m->min_step);
+                step = newStep;
+            } else {
+                if (step != m->max_step) {
+                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = dmin(newStep, 5 * step);
+                    newStep = dmin(newStep, m->max_step);
+                }
+                break;
+            }
+        }
+    }
+    c->pos = xo;
+    v3 u = unit(uo);
+    c->dir = divs(u, norm(u)); /* ParticleState::setDirection */
+    set_current_step(c, step);
+    c->next = newStep;
+}
+
+/* Cash-Karp tableau (PropagationCK.cpp:11-26) */
+static const double ck_a[36] = {
+    0., 0., 0., 0., 0., 0.,
+    1. / 5., 0., 0., 0., 0., 0.,
+    3. / 40., 9. / 40., 0., 0., 0., 0.,
+    3. / 10., -9. / 10., 6. / 5., 0., 0., 0.,
+    -11. / 54., 5. / 2., -70. / 27., 35. / 27., 0., 0.,
+    1631. / 55296., 175. / 512., 575. / 13824., 44275. / 110592., 253. / 4096., 0.};
+static const double ck_b[6] = {37. / 378., 0, 250. / 621., 125. / 594., 0., 512. / 1771.};
+static const double ck_bs[6] = {2825. / 27648., 0., 18575. / 48384., 13525. / 55296.,
+                                277. / 14336., 1. / 4.};
+
+/* PropagationCK::tryStep / dYdt (PropagationCK.cpp:28, :51) */
+static void ck_try(const crp_plan_desc *d, v3 x, v3 u, double h, double q, double E,
+                   v3 *xo, v3 *uo, v3 *ex, v3 *eu) {
+    v3 kx[6], ku[6];
+    *xo = x; *uo = u;
+    *ex = mk(0, 0, 0); *eu = mk(0, 0, 0);
+    for (int i = 0; i < 6; i++) {
+        v3 yx = x, yu = u;
+        for (int j = 0; j < i; j++) {
+            yx = add(yx, muls(muls(kx[j], ck_a[i * 6 + j]), h));
+            yu = add(yu, muls(muls(ku[j], ck_a[i * 6 + j]), h));
+        }
+        v3 vel = muls(unit(yu), c_light);
+        v3 B = field_at(d, yx);
+        v3 dudt = muls(cross(vel, B), q * c_light / E);
+        kx[i] = vel; ku[i] = dudt;
+        *xo = add(*xo, muls(muls(kx[i], ck_b[i]), h));
+        *uo = add(*uo, muls(muls(ku[i], ck_b[i]), h));
+        *ex = add(*ex, muls(muls(kx[i], ck_b[i] - ck_bs[i]), h));
+        *eu = add(*eu, muls(muls(ku[i], ck_b[i] - ck_bs[i]), h));
+    }
+}
+
+/* PropagationCK::process (PropagationCK.cpp:77) */
+static void ck_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t *c, uint64_t *tries) {
+    c->prev = c->pos;
+    double step = m->max_step;
+    if (c->q == 0) {
+        step = clipd(c->next, m->min_step, m->max_step);
+        c->pos = add(c->pos, muls(c->dir, step));
+        set_current_step(c, step);
+        c->next = m->max_step;
+        return;
+    }
+    v3 xo, uo, ex, eu;
+    double newStep = step;
+    if (m->min_step == m->max_step) {
+        ck_try(d, c->pos, c->dir, step / c_light, c->q, c->E, &xo, &uo, &ex, &eu);
+        (*tries)++;
+    } else {
+        step = clipd(c->next, m->min_step, m->max_step);
+        newStep = step;
+        while (1) {
+            ck_try(d, c->pos, c->dir, step / c_light, c->q, c->E, &xo, &uo, &ex, &eu);
+            (*tries)++;
+            double r = norm(eu) / m->tolerance;
+            if (r > 1) {
+                if (step == m->min_step) break;
+                newStep = step * 0.95 * pow(r, -0.2);
+                newStep = dmax(newStep, 0.1 * step);
+                newStep = dmax(newStep, m->min_step);
+                step = newStep;
+            } else {
+                if (step != m->max_step) {
+                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = dmin(newStep, 5 * step);
+                    newStep = dmin(newStep, m->max_step);
+                }
+                break;
+            }
+        }
+    }
+    c->pos = xo;
+    v3 u = unit(uo);
+    c->dir = divs(u, norm(u));
+    set_current_step(c, step);
+    c->next = newStep;
+}
+
+/* DiffusionSDE::tryStep (DiffusionSDE.cpp:233) */
+static void sde_try(const crp_plan_desc *d, v3 PosIn, v3 *POut, v3 *PosErr, double propStep) {
+    v3 k[6];
+    *POut = PosIn;
+    for (int i = 0; i < 6; i++) {
+        v3 y_n = PosIn;
+        for (int j = 0; j < i; j++) y_n = add(y_n, muls(muls(k[j], ck_a[i * 6 + j]), propStep));
+        v3 B = field_at(d, y_n);
+        k[i] = muls(unit(B), c_light);
+        *POut = add(*POut, muls(muls(k[i], ck_b[i]), propStep));
+        *PosErr = add(*PosErr, divs(muls(muls(k[i], ck_b[i] - ck_bs[i]), propStep), kpc_unit));
+    }
+}
+
+/* DiffusionSDE::process (DiffusionSDE.cpp:47), without an advection field. */
+static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t *c, uint64_t *tries) {
+    c->prev = c->pos;
+    double h = clipd(c->next, m->min_step, m->max_step) / c_light;
+    v3 PosIn = c->pos, DirIn = c->dir;
+    (void)DirIn;
+    if (c->q == 0) {
+        c->pos = add(add(c->pos, mk(0, 0, 0)), muls(muls(c->dir, h), c_light));
+        set_current_step(c, h * c_light);
+        c->next = m->max_step;
+        return;
+    }
+    double rig = c->E / c->q;
+    double DifCoeff = m->sde_scale * 6.1e24 * pow((fabs(rig) / 4.0e9), m->sde_alpha);
+    double BT0 = pow(2 * DifCoeff, 0.5);
+    double BT4 = pow(2 * m->sde_epsilon * DifCoeff, 0.5);
+    double BT8 = BT4;
+    stream_t s = {d->seed, c->index, c->steps, {{0, 0, 0, 0}}, 0};
+    double eta0 = stream_norm(&s), eta1 = stream_norm(&s), eta2 = stream_norm(&s);
+    double TStep = BT0 * eta0, NStep = BT4 * eta1, BStep = BT8 * eta2;
+    double propTime = TStep * sqrt(h) / c_light;
+    size_t counter = 0;
+    double r = 42.;
+    do {
+        v3 PosOut = mk(0, 0, 0), PosErr = mk(0, 0, 0);
+        sde_try(d, PosIn, &PosOut, &PosErr, propTime);
+        (*tries)++;
+        r = norm(PosErr) / m->tolerance;
+        propTime *= 0.5;
+        counter += 1;
+    } while (r > 1 && fabs(propTime) >= m->min_step / c_light);
+    size_t stepNumber = (size_t)pow(2, (double)(counter - 1));
+    double allowedTime = TStep * sqrt(h) / c_light / (double)stepNumber;
+    v3 Start = PosIn, PosOut = mk(0, 0, 0), PosErr = mk(0, 0, 0);
+    for (size_t j = 0; j < stepNumber; j++) {
+        sde_try(d, Start, &PosOut, &PosErr, allowedTime);
+        (*tries)++;
+        Start = PosOut;
+    }
+    v3 TVec = unit(sub(PosOut, PosIn));
+    double tTest = norm(TVec);
+    if (tTest != tTest) {
+        c->pos = add(c->pos, muls(muls(c->dir, h), c_light));
+        set_current_step(c, h * c_light);
+        double newStep = 5 * h * c_light;
+        c->next = clipd(newStep, m->min_step, m->max_step);
+        return;
+    }
+    v3 NVec = mk(0, 0, 0);
+    int guard = 0;
+    while (norm(NVec) == 0. && guard < 3) { NVec = cross(TVec, stream_vector(&s)); guard++; }
+    if (norm(NVec) == 0.) { c->active = 0; c->flags |= CRP_FLAG_NAN; return; }
+    NVec = unit(NVec);
+    v3 BVec = unit(cross(TVec, NVec));
+    v3 PO = add(add(PosOut, mk(0, 0, 0)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
+    if (isnan(norm(PO))) { c->active = 0; c->flags |= CRP_FLAG_NAN; return; }
+    s.cursor = 12; /* the cone draw uses the fourth block of the step */
+    v3 DirOut = stream_cone(&s, TVec, M_PI / 2.);
+    c->pos = PO;
+    c->dir = divs(DirOut, norm(DirOut));
+    set_current_step(c, h * c_light);
+    double nextStep;
+    if (stepNumber > 1) nextStep = h * pow((double)stepNumber, -2.) * c_light;
+    else nextStep = 4 * h * c_light;
+    c->next = nextStep;
+}
+
+typedef struct {
+    crp_records *rec;
+} rec_ctx;
+
+static void write_record(crp_records *rec, const cand_t *c, int module) {
+    if (!rec) return;
+    uint64_t slot;
+#ifdef _OPENMP
+#pragma omp atomic capture
+#endif
+    slot = (*rec->count)++;
+    if (slot >= rec->capacity) return;
+    rec->index[slot] = c->index;
+    rec->module[slot] = module;
+    rec->trajectory_length[slot] = c->len;
+    rec->time[slot] = c->time;
+    rec->x[slot] = c->pos.x; rec->y[slot] = c->pos.y; rec->z[slot] = c->pos.z;
+    rec->dx[slot] = c->dir.x; rec->dy[slot] = c->dir.y; rec->dz[slot] = c->dir.z;
+    rec->energy[slot] = c->E;
+    rec->id[slot] = c->id;
+}
+
+/* One ModuleList::process (ModuleList.cpp.in:54): every module in order. */
+static void chain_process(const crp_plan_desc *d, cand_t *c, crp_records *rec, uint64_t *tries) {
+    for (int i = 0; i < d->n_modules; i++) {
+        const crp_module_desc *m = &d->modules[i];
+        if (m->kind == CRP_MODULE_PROPAGATION) {
+            if (m->propagator == CRP_PROP_BP) bp_process(d, m, c, tries);
+            else if (m->propagator == CRP_PROP_CK) ck_process(d, m, c, tries);
+            else sde_process(d, m, c, tries);
+        } else if (m->kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) { /* BreakCondition.cpp:42 */
+            double maxLength = m->per_candidate_length ? c->maxlen : m->max_length;
+            if (c->len >= maxLength) {
+                if (m->record) write_record(rec, c, i);
+                c->flags |= CRP_FLAG_REJECTED;  /* AbstractCondition::reject, Module.cpp:25 */
+                c->active = 0;
+            } else {
+                limit_next_step(c, maxLength - c->len);
+            }
+        } else if (m->kind == CRP_MODULE_OBSERVER) { /* Observer.cpp:27 */
+            int detected;
+            if (m->observer_feature == CRP_OBSERVER_SURFACE_SPHERE) { /* Observer.cpp:394 */
+                v3 ctr = mk(m->sphere_center[0], m->sphere_center[1], m->sphere_center[2]);
+                double cd = norm(sub(c->pos, ctr)) - m->sphere_radius;
+                double pd = norm(sub(c->prev, ctr)) - m->sphere_radius;
+                limit_next_step(c, fabs(cd));
+                if (cd * pd > 0) detected = 0;
+                else if (pd == 0) detected = 0;
+                else detected = 1;
+            } else {
+                detected = 1;
+            }
+            if (detected) {
+                if (m->record) write_record(rec, c, i);
+                c->flags |= CRP_FLAG_DETECTED;
+                if (m->deactivate_on_detection) c->active = 0;
+            }
+        }
+    }
+}
+
+/* ModuleList::run(candidate_vector) (ModuleList.cpp.in:97) over the arrays:
+ * each active candidate is processed until inactive, or until it has taken
+ * max_steps steps in this call (0: no cap). */
+int oracle_run(const crp_plan_desc *d, const crp_candidates *a, uint64_t n, crp_records *rec,
+               int nthreads, uint64_t max_steps, uint64_t *steps_out, uint64_t *tries_out) {
+    uint64_t steps = 0, tries = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : steps, tries)
+#endif
+    for (int64_t ii = 0; ii < (int64_t)n; ii++) {
+        uint64_t i = (uint64_t)ii;
+        cand_t c;
+        c.pos = mk(a->x[i], a->y[i], a->z[i]);
+        c.dir = mk(a->dx[i], a->dy[i], a->dz[i]);
+        c.prev = mk(a->px[i], a->py[i], a->pz[i]);
+        c.E = a->energy[i]; c.q = a->charge[i]; c.id = a->id[i];
+        c.len = a->trajectory_length[i]; c.time = a->time[i];
+        c.cur = a->current_step[i]; c.next = a->next_step[i];
+        c.maxlen = a->max_length ? a->max_length[i] : 0;
+        c.active = a->active[i] != 0; c.flags = a->flags[i];
+        c.index = i;
+        c.steps = a->step_count ? a->step_count[i] : 0;
+        uint64_t taken = 0, t = 0;
+        while (c.active && (max_steps == 0 || taken < max_steps)) {
+            chain_process(d, &c, rec, &t);
+            c.steps++;
+            taken++;
+        }
+        steps += taken;
+        tries += t;
+        a->x[i] = c.pos.x; a->y[i] = c.pos.y; a->z[i] = c.pos.z;
+        a->dx[i] = c.dir.x; a->dy[i] = c.dir.y; a->dz[i] = c.dir.z;
+        a->px[i] = c.prev.x; a->py[i] = c.prev.y; a->pz[i] = c.prev.z;
+        a->trajectory_length[i] = c.len; a->time[i] = c.time;
+        a->current_step[i] = c.cur; a->next_step[i] = c.next;
+        a->active[i] = (uint8_t)c.active; a->flags[i] = c.flags;
+        if (a->step_count) a->step_count[i] = c.steps;
+    }
+    if (steps_out) *steps_out = steps;
+    if (tries_out) *tries_out = tries;
+    return 0;
+}

@@ -1,0 +1,194 @@
+"""TEST INFRASTRUCTURE: Python access to the oracle and to the reference.
+
+* `Oracle` wraps oracle/_build/libcrp_oracle.so, the plain-C restatement of
+  the stepping path (crp_oracle.c).
+* `Reference` wraps oracle/_ref/libcrp_ref.so, the reference itself compiled
+  from its sources with the shim ref_shim.cpp (oracle/Makefile), when it has
+  been built (it needs the reference checkout at build time only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs use this module;
+the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from crpropa3_b200 import _abi
+from crpropa3_b200.state import CandidateArrays, RecordArrays
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "_build", "libcrp_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libcrp_ref.so")
+REF_FAST_LIB = os.path.join(HERE, "_ref", "libcrp_ref_fast.so")
+
+_dp = C.POINTER(C.c_double)
+
+
+def build_oracle():
+    """Compile the oracle (gcc) if its library is missing or stale."""
+    src = os.path.join(HERE, "crp_oracle.c")
+    if os.path.exists(ORACLE_LIB) and os.path.getmtime(ORACLE_LIB) >= os.path.getmtime(src):
+        return ORACLE_LIB
+    subprocess.run(["make", "-C", HERE, "oracle"], check=True, capture_output=True)
+    return ORACLE_LIB
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+class Oracle:
+    def __init__(self):
+        build_oracle()
+        lib = C.CDLL(ORACLE_LIB)
+        lib.oracle_run.restype = C.c_int
+        lib.oracle_run.argtypes = [C.POINTER(_abi.PlanDesc), C.POINTER(_abi.Candidates), C.c_uint64,
+                                   C.POINTER(_abi.Records), C.c_int, C.c_uint64,
+                                   C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        lib.oracle_field_eval.argtypes = [C.POINTER(_abi.PlanDesc), C.c_uint64, _dp, _dp]
+        lib.oracle_random.argtypes = [C.c_uint32, C.c_int, C.c_uint64, C.c_double, C.c_double,
+                                      C.c_double, _dp]
+        lib.oracle_plane_wave_modes.argtypes = [C.c_double] * 6 + [C.c_int, C.c_uint32] + [_dp] * 5
+        lib.oracle_sample_source.argtypes = [C.c_uint32, C.c_uint64, C.c_int,
+                                             C.POINTER(C.c_int32), _dp, C.c_double, C.c_double,
+                                             C.c_double, C.POINTER(C.c_int32), _dp, _dp]
+        lib.oracle_philox_block.argtypes = [C.POINTER(C.c_uint32)] * 3
+        self.lib = lib
+
+    def run(self, spec, cands: CandidateArrays, records: RecordArrays = None, threads=0,
+            max_steps=0):
+        desc = spec.desc()
+        s = cands.struct()
+        rs = records.struct() if records is not None else None
+        steps, tries = C.c_uint64(), C.c_uint64()
+        r = self.lib.oracle_run(C.byref(desc), C.byref(s), cands.n,
+                                C.byref(rs) if rs is not None else None, threads, max_steps,
+                                C.byref(steps), C.byref(tries))
+        assert r == 0
+        return steps.value, tries.value
+
+    def field(self, spec, pos):
+        pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).T)
+        n = pos.shape[1]
+        out = np.zeros((3, n))
+        self.lib.oracle_field_eval(C.byref(spec.desc()), n, _dptr(pos), _dptr(out))
+        return out.T
+
+    def random(self, seed, kind, n, a=0.0, b=0.0, c=0.0):
+        out = np.zeros(n * (3 if kind == 2 else 1))
+        assert self.lib.oracle_random(seed, kind, n, a, b, c, _dptr(out)) == 0
+        return out
+
+    def plane_wave_modes(self, brms, lmin, lmax, lbendover, s, q, nm, seed):
+        xi, kappa = np.zeros(3 * nm), np.zeros(3 * nm)
+        k, beta, ak = np.zeros(nm), np.zeros(nm), np.zeros(nm)
+        assert self.lib.oracle_plane_wave_modes(brms, lmin, lmax, lbendover, s, q, nm, seed,
+                                                _dptr(xi), _dptr(kappa), _dptr(k), _dptr(beta),
+                                                _dptr(ak)) == 0
+        return xi, kappa, k, beta, ak
+
+    def sample_source(self, seed, n, ids, abundances, emin, emax, index):
+        ids = np.asarray(ids, dtype=np.int32)
+        ab = np.asarray(abundances if abundances is not None else np.ones(len(ids)), dtype=np.float64)
+        out_id, e, d = np.zeros(n, np.int32), np.zeros(n), np.zeros(3 * n)
+        assert self.lib.oracle_sample_source(seed, n, len(ids), ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                             _dptr(ab), emin, emax, index,
+                                             out_id.ctypes.data_as(C.POINTER(C.c_int32)),
+                                             _dptr(e), _dptr(d)) == 0
+        return out_id, e, d.reshape(n, 3)
+
+    def philox(self, ctr, key):
+        c = (C.c_uint32 * 4)(*ctr)
+        k = (C.c_uint32 * 2)(*key)
+        o = (C.c_uint32 * 4)()
+        self.lib.oracle_philox_block(c, k, o)
+        return list(o)
+
+
+def reference_available(fast=False) -> bool:
+    return os.path.exists(REF_FAST_LIB if fast else REF_LIB)
+
+
+class Reference:
+    """The reference's own modules, driven through ref_shim.cpp."""
+
+    def __init__(self, fast=False):
+        path = REF_FAST_LIB if fast else REF_LIB
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference library {path} is not built (make -C oracle ref)")
+        lib = C.CDLL(path)
+        lib.ref_run.restype = C.c_int
+        lib.ref_run.argtypes = [C.POINTER(_abi.PlanDesc), C.POINTER(_abi.Candidates), C.c_uint64,
+                                C.POINTER(_abi.Records), C.c_int, C.c_uint32,
+                                C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+        lib.ref_field_eval.argtypes = [C.POINTER(_abi.PlanDesc), C.c_uint64, _dp, _dp]
+        lib.ref_random.argtypes = [C.c_uint32, C.c_int, C.c_uint64, C.c_double, C.c_double,
+                                   C.c_double, _dp]
+        lib.ref_sample_source.argtypes = [C.c_uint32, C.c_uint64, _dp, C.c_int,
+                                          C.POINTER(C.c_int32), _dp, C.c_double, C.c_double,
+                                          C.c_double, C.POINTER(C.c_int32), _dp, _dp]
+        lib.ref_charge.restype = C.c_double
+        lib.ref_charge.argtypes = [C.c_int32]
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_text_output.argtypes = [C.c_char_p, C.c_int, C.c_uint64, C.POINTER(C.c_uint64),
+                                        C.POINTER(C.c_int32), _dp, _dp, _dp, _dp,
+                                        C.POINTER(C.c_int32), _dp, _dp, _dp]
+        self.lib = lib
+
+    def _check(self, r):
+        if r != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def run(self, spec, cands: CandidateArrays, records: RecordArrays = None, threads=0, seed=0):
+        desc = spec.desc()
+        s = cands.struct()
+        rs = records.struct() if records is not None else None
+        steps, secs = C.c_uint64(), C.c_double()
+        self._check(self.lib.ref_run(C.byref(desc), C.byref(s), cands.n,
+                                     C.byref(rs) if rs is not None else None, threads, seed,
+                                     C.byref(steps), C.byref(secs)))
+        return steps.value, secs.value
+
+    def field(self, spec, pos):
+        pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).T)
+        n = pos.shape[1]
+        out = np.zeros((3, n))
+        self._check(self.lib.ref_field_eval(C.byref(spec.desc()), n, _dptr(pos), _dptr(out)))
+        return out.T
+
+    def random(self, seed, kind, n, a=0.0, b=0.0, c=0.0):
+        out = np.zeros(n * (3 if kind in (2, 5) else 1))
+        self._check(self.lib.ref_random(seed, kind, n, a, b, c, _dptr(out)))
+        return out
+
+    def sample_source(self, seed, n, position, ids, abundances, emin, emax, index):
+        ids = np.asarray(ids, dtype=np.int32)
+        ab = np.asarray(abundances if abundances is not None else np.ones(len(ids)), dtype=np.float64)
+        pos = np.asarray(position, dtype=np.float64)
+        out_id, e, d = np.zeros(n, np.int32), np.zeros(n), np.zeros(3 * n)
+        self._check(self.lib.ref_sample_source(seed, n, _dptr(pos), len(ids),
+                                               ids.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(ab),
+                                               emin, emax, index,
+                                               out_id.ctypes.data_as(C.POINTER(C.c_int32)),
+                                               _dptr(e), _dptr(d)))
+        return out_id, e, d.reshape(n, 3)
+
+    def charge(self, pid):
+        return self.lib.ref_charge(pid)
+
+    def text_output(self, path, output_type, serial, ids, energy, pos, dirs, length, src_id,
+                    src_e, src_pos, src_dir):
+        n = len(serial)
+        a = lambda x, t=np.float64: np.ascontiguousarray(x, dtype=t)
+        serial, ids, src_id = a(serial, np.uint64), a(ids, np.int32), a(src_id, np.int32)
+        energy, pos, dirs, length = a(energy), a(pos), a(dirs), a(length)
+        src_e, src_pos, src_dir = a(src_e), a(src_pos), a(src_dir)
+        self._check(self.lib.ref_text_output(
+            path.encode(), output_type, n, serial.ctypes.data_as(C.POINTER(C.c_uint64)),
+            ids.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(energy), _dptr(pos), _dptr(dirs),
+            _dptr(length), src_id.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(src_e),
+            _dptr(src_pos), _dptr(src_dir)))

@@ -1,0 +1,428 @@
+/*
+ * ref_shim.cpp -- TEST INFRASTRUCTURE, not product code.
+ *
+ * Drives the reference's own CPU modules (CRPropa3, compiled from its
+ * sources by oracle/Makefile into oracle/_ref/) from the plain arrays of
+ * include/crp_gpu.h, so that the tests, the golden-fixture generator and
+ * bench.py's CPU baseline can run the unmodified reference path on exactly
+ * the inputs the device path gets.  Only tests/, bench.py's reference arm and
+ * __graft_entry__.smoke() load this library.
+ *
+ * What comes from the reference (unchanged, linked): Candidate, ModuleList
+ * (src/ModuleList.cpp.in:97 run(candidate_vector) with OpenMP
+ * schedule(static,100)), PropagationCK, PropagationBP, DiffusionSDE,
+ * MagneticFieldGrid, PeriodicMagneticField, MagneticFieldList,
+ * UniformMagneticField, PlaneWaveTurbulence, MaximumTrajectoryLength,
+ * Observer, ObserverSurface(Sphere), ObserverDetectAll, TextOutput, Source
+ * features and Random.
+ *
+ * Helpers written here (no reference counterpart):
+ *   ToroidalField         B = b0 (-y, x, 0)/r  (analytic field of the
+ *                         diffusion workload; ToroidalHaloField has another
+ *                         form)
+ *   PerCandidateLength    MaximumTrajectoryLength with the limit read from a
+ *                         candidate property (one limit per candidate)
+ *   RecordAction          detection / reject action that stores a record
+ *   StepCounter           counts process() calls of the chain = steps
+ */
+#include "crp_gpu.h"
+
+#include "crpropa/Candidate.h"
+#include "crpropa/Grid.h"
+#include "crpropa/ModuleList.h"
+#include "crpropa/Random.h"
+#include "crpropa/Source.h"
+#include "crpropa/Units.h"
+#include "crpropa/magneticField/MagneticField.h"
+#include "crpropa/magneticField/MagneticFieldGrid.h"
+#include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
+#include "crpropa/magneticField/turbulentField/TurbulentField.h"
+#include "crpropa/module/BreakCondition.h"
+#include "crpropa/module/DiffusionSDE.h"
+#include "crpropa/module/Observer.h"
+#include "crpropa/module/PropagationBP.h"
+#include "crpropa/module/PropagationCK.h"
+#include "crpropa/module/TextOutput.h"
+#include "crpropa/Geometry.h"
+
+#include <dlfcn.h>
+#include <omp.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+using namespace crpropa;
+
+namespace {
+
+std::string g_error;
+
+/* The mass table is read on the first ParticleState::setId of a nucleus
+ * (ParticleMass.cpp:24); the stepping path never uses the mass.  Point
+ * CRPROPA_DATA_PATH at the stub table the Makefile writes beside this
+ * library. */
+void ensure_data_path() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    Dl_info info;
+    if (dladdr((void *)&ensure_data_path, &info) && info.dli_fname) {
+        std::string p(info.dli_fname);
+        size_t s = p.rfind('/');
+        std::string dir = (s == std::string::npos) ? std::string(".") : p.substr(0, s);
+        setenv("CRPROPA_DATA_PATH", (dir + "/data").c_str(), 1);
+    }
+}
+
+class ToroidalField : public MagneticField {
+    double b0;
+public:
+    explicit ToroidalField(double b0) : b0(b0) {}
+    Vector3d getField(const Vector3d &p) const {
+        double r = std::sqrt(p.x * p.x + p.y * p.y);
+        return Vector3d(-p.y, p.x, 0.) * (b0 / r);
+    }
+};
+
+class PerCandidateLength : public AbstractCondition {
+public:
+    void process(Candidate *c) const {
+        double maxLength = c->getProperty("CrpMaxLength").asDouble();
+        double length = c->getTrajectoryLength();
+        if (length >= maxLength)
+            reject(c);
+        else
+            c->limitNextStep(maxLength - length);
+    }
+};
+
+class RecordAction : public Module {
+    crp_records *rec;
+    int module;
+public:
+    RecordAction(crp_records *rec, int module) : rec(rec), module(module) {}
+    void process(Candidate *c) const {
+        if (!rec) return;
+        uint64_t slot;
+#pragma omp critical(crp_record)
+        { slot = (*rec->count)++; }
+        if (slot >= rec->capacity) return;
+        rec->index[slot] = (uint64_t)c->getProperty("CrpIndex").asUInt64();
+        rec->module[slot] = module;
+        rec->trajectory_length[slot] = c->getTrajectoryLength();
+        rec->time[slot] = c->getTime();
+        const Vector3d &p = c->current.getPosition();
+        const Vector3d &d = c->current.getDirection();
+        rec->x[slot] = p.x; rec->y[slot] = p.y; rec->z[slot] = p.z;
+        rec->dx[slot] = d.x; rec->dy[slot] = d.y; rec->dz[slot] = d.z;
+        rec->energy[slot] = c->current.getEnergy();
+        rec->id[slot] = c->current.getId();
+    }
+};
+
+class StepCounter : public Module {
+public:
+    mutable std::vector<uint64_t> perThread;
+    StepCounter() : perThread(256 * 8, 0) {}
+    void process(Candidate *c) const { perThread[omp_get_thread_num() * 8]++; }
+    uint64_t total() const {
+        uint64_t s = 0;
+        for (size_t i = 0; i < perThread.size(); i += 8) s += perThread[i];
+        return s;
+    }
+};
+
+struct Built {
+    ref_ptr<ModuleList> sim;
+    ref_ptr<MagneticField> field;
+    std::vector<ref_ptr<Referenced> > keep;  // spectra, grids
+    ref_ptr<StepCounter> counter;
+};
+
+ref_ptr<MagneticField> build_component(const crp_field_component &f, Built &b) {
+    ref_ptr<MagneticField> m;
+    if (f.kind == CRP_FIELD_GRID) {
+        const crp_grid3f_desc &g = f.grid;
+        ref_ptr<Grid3f> grid = new Grid3f(Vector3d(g.origin[0], g.origin[1], g.origin[2]),
+                                          g.nx, g.ny, g.nz,
+                                          Vector3d(g.spacing[0], g.spacing[1], g.spacing[2]));
+        grid->setReflective(g.reflective != 0);
+        grid->setClipVolume(g.clip_volume != 0);
+        std::vector<Vector3f> &v = grid->getGrid();
+        std::memcpy(&v[0], g.values, sizeof(float) * 3 * g.nx * g.ny * g.nz);
+        b.keep.push_back(grid.get());
+        m = new MagneticFieldGrid(grid);
+    } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
+        const crp_plane_wave_desc &p = f.plane_wave;
+        TurbulenceSpectrum *spec = new TurbulenceSpectrum(p.brms, p.lmin, p.lmax, p.lbendover,
+                                                          p.sindex, p.qindex);
+        b.keep.push_back(spec);
+        m = new PlaneWaveTurbulence(*spec, p.n_modes, p.seed);
+    } else if (f.kind == CRP_FIELD_UNIFORM) {
+        m = new UniformMagneticField(Vector3d(f.uniform[0], f.uniform[1], f.uniform[2]));
+    } else if (f.kind == CRP_FIELD_TOROIDAL) {
+        m = new ToroidalField(f.toroidal_b0);
+    } else {
+        throw std::runtime_error("ref_shim: unknown field kind");
+    }
+    if (f.periodic) {
+        m = new PeriodicMagneticField(
+            m, Vector3d(f.periodic_extends[0], f.periodic_extends[1], f.periodic_extends[2]),
+            Vector3d(f.periodic_origin[0], f.periodic_origin[1], f.periodic_origin[2]),
+            f.periodic_reflective != 0);
+    }
+    return m;
+}
+
+ref_ptr<MagneticField> build_field(const crp_plan_desc *d, Built &b) {
+    if (d->n_fields == 1)
+        return build_component(d->fields[0], b);
+    ref_ptr<MagneticFieldList> list = new MagneticFieldList();
+    for (int i = 0; i < d->n_fields; i++)
+        list->addField(build_component(d->fields[i], b));
+    return list;
+}
+
+void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b) {
+    b.field = build_field(d, b);
+    b.sim = new ModuleList();
+    for (int i = 0; i < d->n_modules; i++) {
+        const crp_module_desc &m = d->modules[i];
+        if (m.kind == CRP_MODULE_PROPAGATION) {
+            if (m.propagator == CRP_PROP_CK) {
+                b.sim->add(new PropagationCK(b.field, m.tolerance, m.min_step, m.max_step));
+            } else if (m.propagator == CRP_PROP_BP) {
+                if (m.min_step == m.max_step)
+                    b.sim->add(new PropagationBP(b.field, m.max_step));
+                else
+                    b.sim->add(new PropagationBP(b.field, m.tolerance, m.min_step, m.max_step));
+            } else if (m.propagator == CRP_PROP_SDE) {
+                DiffusionSDE *sde = new DiffusionSDE(b.field, m.tolerance, m.min_step, m.max_step,
+                                                     m.sde_epsilon);
+                sde->setAlpha(m.sde_alpha);
+                sde->setScale(m.sde_scale);
+                b.sim->add(sde);
+            } else {
+                throw std::runtime_error("ref_shim: unknown propagator");
+            }
+        } else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
+            AbstractCondition *c;
+            if (m.per_candidate_length)
+                c = new PerCandidateLength();
+            else
+                c = new MaximumTrajectoryLength(m.max_length);
+            if (m.record) c->onReject(new RecordAction(rec, i));
+            b.sim->add(c);
+        } else if (m.kind == CRP_MODULE_OBSERVER) {
+            Observer *o = new Observer();
+            if (m.observer_feature == CRP_OBSERVER_SURFACE_SPHERE)
+                o->add(new ObserverSurface(new Sphere(
+                    Vector3d(m.sphere_center[0], m.sphere_center[1], m.sphere_center[2]),
+                    m.sphere_radius)));
+            else
+                o->add(new ObserverDetectAll());
+            o->setDeactivateOnDetection(m.deactivate_on_detection != 0);
+            o->setFlag("Detected", "Detected");
+            if (m.record) o->onDetection(new RecordAction(rec, i));
+            b.sim->add(o);
+        } else {
+            throw std::runtime_error("ref_shim: unknown module kind");
+        }
+    }
+    b.counter = new StepCounter();
+    b.sim->add(b.counter.get());
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ref_last_error() { return g_error.c_str(); }
+
+/* Run the reference ModuleList over n candidates given as arrays (in/out).
+ * nthreads OpenMP threads; Random::seedThreads(seed) before the run.
+ * Returns 0 on success, and the number of chain process() calls (= steps
+ * taken, one per candidate per loop iteration) in *steps. */
+int ref_run(const crp_plan_desc *desc, const crp_candidates *c, uint64_t n,
+            crp_records *rec, int nthreads, uint32_t seed, uint64_t *steps,
+            double *seconds) {
+    try {
+        ensure_data_path();
+        Built b;
+        build_chain(desc, rec, b);
+        ModuleList::candidate_vector_t cands;
+        cands.reserve(n);
+        for (uint64_t i = 0; i < n; i++) {
+            ref_ptr<Candidate> cand = new Candidate(
+                c->id[i], c->energy[i], Vector3d(c->x[i], c->y[i], c->z[i]),
+                Vector3d(c->dx[i], c->dy[i], c->dz[i]));
+            cand->previous.setPosition(Vector3d(c->px[i], c->py[i], c->pz[i]));
+            cand->setTrajectoryLength(c->trajectory_length[i]);
+            cand->setTime(c->time[i]);
+            cand->setNextStep(c->next_step[i]);
+            cand->setActive(c->active[i] != 0);
+            cand->setProperty("CrpIndex", Variant((uint64_t)i));
+            if (c->max_length)
+                cand->setProperty("CrpMaxLength", Variant(c->max_length[i]));
+            cands.push_back(cand);
+        }
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+        Random::seedThreads(seed);
+        // ModuleList::run prints a thread-count banner on stdout; keep
+        // stdout clean for the caller.
+        std::streambuf *old = std::cout.rdbuf();
+        std::ostringstream sink;
+        std::cout.rdbuf(sink.rdbuf());
+        double t0 = omp_get_wtime();
+        b.sim->run(&cands, true, false);
+        double t1 = omp_get_wtime();
+        std::cout.rdbuf(old);
+        if (seconds) *seconds = t1 - t0;
+        if (steps) *steps = b.counter->total();
+        for (uint64_t i = 0; i < n; i++) {
+            Candidate *cand = cands[i];
+            const Vector3d &p = cand->current.getPosition();
+            const Vector3d &d = cand->current.getDirection();
+            const Vector3d &q = cand->previous.getPosition();
+            c->x[i] = p.x; c->y[i] = p.y; c->z[i] = p.z;
+            c->dx[i] = d.x; c->dy[i] = d.y; c->dz[i] = d.z;
+            c->px[i] = q.x; c->py[i] = q.y; c->pz[i] = q.z;
+            c->trajectory_length[i] = cand->getTrajectoryLength();
+            c->time[i] = cand->getTime();
+            c->current_step[i] = cand->getCurrentStep();
+            c->next_step[i] = cand->getNextStep();
+            c->active[i] = cand->isActive() ? 1 : 0;
+            uint32_t fl = 0;
+            if (cand->hasProperty("Rejected")) fl |= CRP_FLAG_REJECTED;
+            if (cand->hasProperty("Detected")) fl |= CRP_FLAG_DETECTED;
+            c->flags[i] = fl;
+        }
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/* Field of the chain description at n positions (planar xyz in/out). */
+int ref_field_eval(const crp_plan_desc *desc, uint64_t n, const double *pos, double *out) {
+    try {
+        ensure_data_path();
+        Built b;
+        ref_ptr<MagneticField> f = build_field(desc, b);
+        for (uint64_t i = 0; i < n; i++) {
+            Vector3d B = f->getField(Vector3d(pos[i], pos[n + i], pos[2 * n + i]));
+            out[i] = B.x; out[n + i] = B.y; out[2 * n + i] = B.z;
+        }
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/* Draw `n` values from crpropa::Random seeded with `seed`:
+ * kind 0 rand(), 1 randUniform(a,b), 2 randVector() (3 per draw),
+ * 3 randPowerLaw(a, b, c) with index a, 4 randNorm(), 5 randConeVector around
+ * (0,0,1) with angle a (3 per draw), 6 randInt() */
+int ref_random(uint32_t seed, int kind, uint64_t n, double a, double b, double c, double *out) {
+    Random r(seed);
+    for (uint64_t i = 0; i < n; i++) {
+        switch (kind) {
+        case 0: out[i] = r.rand(); break;
+        case 1: out[i] = r.randUniform(a, b); break;
+        case 2: { Vector3d v = r.randVector(); out[3*i] = v.x; out[3*i+1] = v.y; out[3*i+2] = v.z; } break;
+        case 3: out[i] = r.randPowerLaw(a, b, c); break;
+        case 4: out[i] = r.randNorm(); break;
+        case 5: { Vector3d v = r.randConeVector(Vector3d(0, 0, 1), a); out[3*i] = v.x; out[3*i+1] = v.y; out[3*i+2] = v.z; } break;
+        case 6: out[i] = (double)r.randInt(); break;
+        default: g_error = "ref_random: unknown kind"; return 1;
+        }
+    }
+    return 0;
+}
+
+/* Candidates from the reference Source with the features of the stepping
+ * workloads: SourcePosition(pos), one or several particle types,
+ * SourcePowerLawSpectrum(emin, emax, index), SourceIsotropicEmission, drawn
+ * by one thread from Random::seedThreads(seed).  Feature order as added
+ * here: position, type(s), spectrum, direction. */
+int ref_sample_source(uint32_t seed, uint64_t n, const double *pos, int ntypes,
+                      const int32_t *ids, const double *abundances, double emin,
+                      double emax, double index, int32_t *id_out, double *e_out,
+                      double *dir_out) {
+    try {
+        ensure_data_path();
+        Source src;
+        src.add(new SourcePosition(Vector3d(pos[0], pos[1], pos[2])));
+        if (ntypes == 1) {
+            src.add(new SourceParticleType(ids[0]));
+        } else {
+            SourceMultipleParticleTypes *m = new SourceMultipleParticleTypes();
+            for (int i = 0; i < ntypes; i++) m->add(ids[i], abundances[i]);
+            src.add(m);
+        }
+        src.add(new SourcePowerLawSpectrum(emin, emax, index));
+        src.add(new SourceIsotropicEmission());
+        omp_set_num_threads(1);
+        Random::seedThreads(seed);
+        for (uint64_t i = 0; i < n; i++) {
+            ref_ptr<Candidate> c = src.getCandidate();
+            id_out[i] = c->current.getId();
+            e_out[i] = c->current.getEnergy();
+            const Vector3d &d = c->current.getDirection();
+            dir_out[3*i] = d.x; dir_out[3*i+1] = d.y; dir_out[3*i+2] = d.z;
+        }
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/* Charge the reference assigns to a particle id (ParticleState::setId). */
+double ref_charge(int32_t id) {
+    ensure_data_path();
+    ParticleState s;
+    s.setId(id);
+    return s.getCharge();
+}
+
+/* Write TextOutput(Event3D or Trajectory3D) lines for n candidate states
+ * with the reference's own TextOutput into `path` (header included).
+ * Source state columns use the src_* arrays. */
+int ref_text_output(const char *path, int output_type, uint64_t n, const uint64_t *serial,
+                    const int32_t *id, const double *energy, const double *xyz,
+                    const double *dir, const double *trajectory_length,
+                    const int32_t *src_id, const double *src_energy, const double *src_xyz,
+                    const double *src_dir) {
+    try {
+        ensure_data_path();
+        ref_ptr<TextOutput> out = new TextOutput(std::string(path),
+                                                 (Output::OutputType)output_type);
+        for (uint64_t i = 0; i < n; i++) {
+            ref_ptr<Candidate> c = new Candidate(src_id[i], src_energy[i],
+                Vector3d(src_xyz[3*i], src_xyz[3*i+1], src_xyz[3*i+2]),
+                Vector3d(src_dir[3*i], src_dir[3*i+1], src_dir[3*i+2]));
+            c->current.setId(id[i]);
+            c->current.setEnergy(energy[i]);
+            c->current.setPosition(Vector3d(xyz[3*i], xyz[3*i+1], xyz[3*i+2]));
+            c->current.setDirection(Vector3d(dir[3*i], dir[3*i+1], dir[3*i+2]));
+            c->setTrajectoryLength(trajectory_length[i]);
+            c->setSerialNumber(serial[i]);
+            out->process(c);
+        }
+        out->close();
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+}  // extern "C"
