@@ -235,6 +235,8 @@ def main():
     ap.add_argument("--track", type=int, default=5000, help="steps per candidate (1 kpc each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=0)
+    ap.add_argument("--uniform-start", action="store_true",
+                    help="start candidates uniformly over the grid volume (profiling case)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -252,6 +254,9 @@ def main():
                                          precision=_abi.PRECISION_MIXED, device=dev, seed=1 + rank)
     spec_64, _, _ = W.grid_bp_256(n=1, grid_n=args.grid_n, steps=args.track,
                                   precision=_abi.PRECISION_FP64, grid=grid)
+    if args.uniform_start:
+        box = args.grid_n * 5 * U.kpc
+        cands.set_position(np.random.default_rng(7).uniform(0, box, (n, 3)))
     plan_mx = engine.Plan(spec_mx)
     plan_64 = engine.Plan(spec_64)
     log(f"[bench] setup {time.time() - t0:.1f}s (grid {args.grid_n}^3, {n} candidates)")
@@ -314,9 +319,22 @@ def main():
     value_64 = steps_64 * world / (ms64 / 1e3)
     final_64 = d_work.to_host()
 
-    # per-candidate error of the mixed form against the FP64 form
+    # per-candidate error of the mixed form against the FP64 form, beside the
+    # FP64 form's own sensitivity: the same FP64 run started with the x
+    # direction component one ulp larger
     p_mx, p_64 = final_mx.position(), final_64.position()
     err = np.linalg.norm(p_mx - p_64, axis=1) / np.linalg.norm(p_64, axis=1)
+    d_init.dx.copy_(torch.nextafter(d_init.dx, torch.full_like(d_init.dx, float("inf"))))
+    one_step(plan_64)
+    torch.cuda.synchronize()
+    p_ulp = d_work.to_host().position()
+    floor = np.linalg.norm(p_ulp - p_64, axis=1) / np.linalg.norm(p_64, axis=1)
+    stable = floor <= 1e-12
+
+    def stats(e):
+        return {"median": float(np.median(e)), "p90": float(np.quantile(e, 0.9)),
+                "p99": float(np.quantile(e, 0.99)), "max": float(e.max()),
+                "frac_le_1e-6": float(np.mean(e <= 1e-6))}
 
     # ---- end to end through crp_run with pinned host buffers
     host = cands.copy()
@@ -383,9 +401,12 @@ def main():
                        "l2": "grid 201 MB > 126 MB L2 (inputs larger than L2)", "parallelism": f"replicas x{world}"},
             "fp64": {"value": value_64, "unit": UNIT, "ms_per_step": ms64 / k64,
                      "mixed_over_fp64": value / value_64},
-            "mixed_error_vs_fp64": {"max": float(err.max()), "median": float(np.median(err)),
-                                    "p99": float(np.quantile(err, 0.99)),
-                                    "measure": "|x_mixed - x_fp64| / |x_fp64| per candidate"},
+            "mixed_error_vs_fp64": dict(stats(err), measure="|x_mixed - x_fp64| / |x_fp64| per candidate",
+                                        well_conditioned={
+                                            "definition": "candidates whose FP64 run with a 1-ulp direction change stays within 1e-12",
+                                            "fraction": float(stable.mean()),
+                                            "max_error": float(err[stable].max()) if stable.any() else None}),
+            "fp64_one_ulp_divergence": dict(stats(floor), measure="|x_fp64(dx0 + 1 ulp) - x_fp64(dx0)| / |x_fp64|"),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": d2h, "api": "crp_run (host arrays, pinned)"},
             "roofline": roofline,

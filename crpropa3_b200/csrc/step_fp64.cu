@@ -9,9 +9,12 @@
 // unit is compiled with -fmad=false so that no multiply-add is contracted:
 // where the reference uses only + - * / sqrt floor (the Boris push over a
 // Grid3f) the device result is bit-identical to the reference built without
-// FMA.  Transcendentals (pow in the CK step controller, cos in the wave sum,
-// log/cos in the normal draws) are CUDA's, within a few ulp of glibc's.
+// FMA.  pow in the step controllers and DiffusionSDE is cr_pow (crmath.cuh),
+// correctly rounded, which agrees with glibc's pow except where glibc itself
+// misrounds (about 1e-3 of inputs); cos in the wave sum and log/cos in the
+// normal draws are CUDA's, within a few ulp of glibc's.
 #include "chain.cuh"
+#include "crmath.cuh"
 #include "engine_internal.h"
 
 namespace crp {
@@ -207,13 +210,13 @@ struct BP {
                 double r = norm(mk(S, S, S)) / m.tolerance;
                 if (r > 1) {
                     if (step == m.min_step) break;
-                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = step * 0.95 * cr_pow(r, -0.2);
                     newStep = dmax(newStep, 0.1 * step);
                     newStep = dmax(newStep, m.min_step);
                     step = newStep;
                 } else {
                     if (step != m.max_step) {
-                        newStep = step * 0.95 * pow(r, -0.2);
+                        newStep = step * 0.95 * cr_pow(r, -0.2);
                         newStep = dmin(newStep, 5 * step);
                         newStep = dmin(newStep, m.max_step);
                     }
@@ -294,13 +297,13 @@ struct CK {
                 double r = norm(eu) / m.tolerance;
                 if (r > 1) {
                     if (step == m.min_step) break;
-                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = step * 0.95 * cr_pow(r, -0.2);
                     newStep = dmax(newStep, 0.1 * step);
                     newStep = dmax(newStep, m.min_step);
                     step = newStep;
                 } else {
                     if (step != m.max_step) {
-                        newStep = step * 0.95 * pow(r, -0.2);
+                        newStep = step * 0.95 * cr_pow(r, -0.2);
                         newStep = dmin(newStep, 5 * step);
                         newStep = dmin(newStep, m.max_step);
                     }
@@ -374,9 +377,9 @@ struct SDE {
             return;
         }
         double rig = c.E / c.q;
-        double DifCoeff = m.scale * 6.1e24 * pow((fabs(rig) / 4.0e9), m.alpha);
-        double BT0 = pow(2 * DifCoeff, 0.5);
-        double BT4 = pow(2 * m.eps * DifCoeff, 0.5);
+        double DifCoeff = m.scale * 6.1e24 * cr_pow((fabs(rig) / 4.0e9), m.alpha);
+        double BT0 = cr_pow(2 * DifCoeff, 0.5);
+        double BT4 = cr_pow(2 * m.eps * DifCoeff, 0.5);
         Stream s{P.seed, c.index, c.steps, make_uint4(0, 0, 0, 0), 0};
         double eta0 = s_norm(s), eta1 = s_norm(s), eta2 = s_norm(s);
         double TStep = BT0 * eta0, NStep = BT4 * eta1, BStep = BT4 * eta2;

@@ -41,6 +41,18 @@
 #define M_PI 3.14159265358979323846
 #endif
 
+/* The step controllers' and DiffusionSDE's pow (PropagationCK.cpp:116,
+ * PropagationBP.cpp:104, DiffusionSDE.cpp:263).  The default build calls
+ * glibc's pow, as the reference does.  The build with
+ * -DORACLE_POW=oracle_cr_pow calls a correctly rounded pow instead (crpow.cpp),
+ * to separate last-place differences of pow implementations from every other
+ * operation when the device's FP64 form is compared with this oracle. */
+#ifndef ORACLE_POW
+#define ORACLE_POW pow
+#else
+double ORACLE_POW(double, double);
+#endif
+
 /* include/crpropa/Units.h:54-55, :114-115 */
 static const double c_light = 2.99792458e8;
 static const double kpc_unit = 1e3 * (648000 / M_PI * 149597870700.0);
@@ -470,13 +482,13 @@ static void bp_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t 
             double r = norm(mk(S, S, S)) / m->tolerance;
             if (r > 1) {
                 if (step == m->min_step) break;
-                newStep = step * 0.95 * pow(r, -0.2);
+                newStep = step * 0.95 * ORACLE_POW(r, -0.2);
                 newStep = dmax(newStep, 0.1 * step);
                 newStep = dmax(newStep, m->min_step);
                 step = newStep;
             } else {
                 if (step != m->max_step) {
-                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = step * 0.95 * ORACLE_POW(r, -0.2);
                     newStep = dmin(newStep, 5 * step);
                     newStep = dmin(newStep, m->max_step);
                 }
@@ -551,13 +563,13 @@ static void ck_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t 
             double r = norm(eu) / m->tolerance;
             if (r > 1) {
                 if (step == m->min_step) break;
-                newStep = step * 0.95 * pow(r, -0.2);
+                newStep = step * 0.95 * ORACLE_POW(r, -0.2);
                 newStep = dmax(newStep, 0.1 * step);
                 newStep = dmax(newStep, m->min_step);
                 step = newStep;
             } else {
                 if (step != m->max_step) {
-                    newStep = step * 0.95 * pow(r, -0.2);
+                    newStep = step * 0.95 * ORACLE_POW(r, -0.2);
                     newStep = dmin(newStep, 5 * step);
                     newStep = dmin(newStep, m->max_step);
                 }
@@ -599,9 +611,9 @@ static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t
         return;
     }
     double rig = c->E / c->q;
-    double DifCoeff = m->sde_scale * 6.1e24 * pow((fabs(rig) / 4.0e9), m->sde_alpha);
-    double BT0 = pow(2 * DifCoeff, 0.5);
-    double BT4 = pow(2 * m->sde_epsilon * DifCoeff, 0.5);
+    double DifCoeff = m->sde_scale * 6.1e24 * ORACLE_POW((fabs(rig) / 4.0e9), m->sde_alpha);
+    double BT0 = ORACLE_POW(2 * DifCoeff, 0.5);
+    double BT4 = ORACLE_POW(2 * m->sde_epsilon * DifCoeff, 0.5);
     double BT8 = BT4;
     stream_t s = {d->seed, c->index, c->steps, {{0, 0, 0, 0}}, 0};
     double eta0 = stream_norm(&s), eta1 = stream_norm(&s), eta2 = stream_norm(&s);

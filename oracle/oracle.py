@@ -22,6 +22,7 @@ from crpropa3_b200.state import CandidateArrays, RecordArrays
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libcrp_oracle.so")
+ORACLE_CRPOW_LIB = os.path.join(HERE, "_build", "libcrp_oracle_crpow.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcrp_ref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libcrp_ref_fast.so")
 
@@ -31,7 +32,8 @@ _dp = C.POINTER(C.c_double)
 def build_oracle():
     """Compile the oracle (gcc) if its library is missing or stale."""
     src = os.path.join(HERE, "crp_oracle.c")
-    if os.path.exists(ORACLE_LIB) and os.path.getmtime(ORACLE_LIB) >= os.path.getmtime(src):
+    if all(os.path.exists(p) and os.path.getmtime(p) >= os.path.getmtime(src)
+           for p in (ORACLE_LIB, ORACLE_CRPOW_LIB)):
         return ORACLE_LIB
     subprocess.run(["make", "-C", HERE, "oracle"], check=True, capture_output=True)
     return ORACLE_LIB
@@ -42,9 +44,12 @@ def _dptr(a):
 
 
 class Oracle:
-    def __init__(self):
+    """The oracle.  cr_pow=True loads the build whose step controllers use the
+    correctly rounded pow of the device's FP64 form instead of glibc's."""
+
+    def __init__(self, cr_pow=False):
         build_oracle()
-        lib = C.CDLL(ORACLE_LIB)
+        lib = C.CDLL(ORACLE_CRPOW_LIB if cr_pow else ORACLE_LIB)
         lib.oracle_run.restype = C.c_int
         lib.oracle_run.argtypes = [C.POINTER(_abi.PlanDesc), C.POINTER(_abi.Candidates), C.c_uint64,
                                    C.POINTER(_abi.Records), C.c_int, C.c_uint64,

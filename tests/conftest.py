@@ -21,6 +21,12 @@ def oracle():
 
 
 @pytest.fixture(scope="session")
+def oracle_crpow():
+    from oracle import Oracle
+    return Oracle(cr_pow=True)
+
+
+@pytest.fixture(scope="session")
 def reference():
     from oracle import Reference, reference_available
     if not reference_available():

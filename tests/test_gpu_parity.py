@@ -5,11 +5,13 @@ Tolerances:
     + - * / sqrt floor only, compiled without contraction on both sides).
   * FP64 form, fixed-step Cash-Karp: bit-identical.
   * FP64 form, adaptive Cash-Karp / Boris: the step controller calls
-    pow(r, -0.2), which CUDA and glibc round differently in the last place on
-    a small fraction of inputs; a different last bit of a step size can flip a
-    later accept/reject decision, after which that trajectory differs at the
-    level of the integration tolerance.  Bar: >= 90 % of candidates
-    bit-identical, every candidate within 1e-2 relative position.
+    pow(r, -0.2).  The device uses a correctly rounded pow; glibc's pow
+    misrounds about 1e-3 of inputs, and one different last bit of a step size
+    changes the rest of that trajectory (chaotically, in a turbulent field).
+    Bar: bit-identical to the oracle built with the same correctly rounded pow
+    (every other operation is then the reference's), and >= 80 % of
+    candidates bit-identical to the glibc-pow oracle.
+  * mixed form: see test_mixed_precision.py.
   * mixed form: relative final-position error <= 1e-6 against the FP64
     oracle (the stated bound of the mixed-precision form).
 """
@@ -74,30 +76,32 @@ def test_bp_fixed_fp64_bitwise_non_pow2_grid_and_offset_origin(oracle):
     _assert_same_state(a, b)
 
 
-def test_bp_adaptive_fp64(oracle):
+def test_bp_adaptive_fp64(oracle, oracle_crpow):
     rng = np.random.default_rng(13)
     grid = random_grid(rng, 16)
     spec = grid_chain(grid, 10 * U.kpc, P.Propagation(_abi.PROP_BP, 1e-3, 0.1 * U.kpc, 10 * U.kpc),
-                      2 * U.Mpc)
+                      2 * U.Mpc, observer_radius=0.7 * U.Mpc)
     c = protons(rng, 300)
-    a, b, *_ = _run_both(oracle, spec, c)
-    err = rel_pos_err(b, a)
-    assert np.mean(err == 0) >= 0.9, np.mean(err == 0)
-    assert err.max() <= 1e-2, err.max()
-    np.testing.assert_array_equal(a.active, b.active)
+    a, b, ra, rb, _ = _run_both(oracle_crpow, spec, c)
+    _assert_same_state(a, b)
+    _assert_same_records(ra, rb)
+    g = c.copy()
+    oracle.run(spec, g)
+    assert np.mean(rel_pos_err(b, g) == 0) >= 0.8
 
 
-def test_ck_adaptive_fp64(oracle):
+def test_ck_adaptive_fp64(oracle, oracle_crpow):
     rng = np.random.default_rng(14)
     grid = random_grid(rng, 16)
     spec = grid_chain(grid, 10 * U.kpc, ck(1e-4, 0.1 * U.kpc, 10 * U.kpc), 2 * U.Mpc,
                       observer_radius=0.7 * U.Mpc)
     c = protons(rng, 300)
-    a, b, ra, rb, _ = _run_both(oracle, spec, c)
-    err = rel_pos_err(b, a)
-    assert np.mean(err == 0) >= 0.9, np.mean(err == 0)
-    assert err.max() <= 1e-2, err.max()
-    assert np.mean(a.flags == b.flags) >= 0.95
+    a, b, ra, rb, _ = _run_both(oracle_crpow, spec, c)
+    _assert_same_state(a, b)
+    _assert_same_records(ra, rb)
+    g = c.copy()
+    oracle.run(spec, g)
+    assert np.mean(rel_pos_err(b, g) == 0) >= 0.8
 
 
 def test_ck_fixed_fp64_bitwise(oracle):
@@ -107,41 +111,6 @@ def test_ck_fixed_fp64_bitwise(oracle):
     c = protons(rng, 200)
     a, b, *_ = _run_both(oracle, spec, c)
     _assert_same_state(a, b)
-
-
-def test_bp_fixed_mixed_error_bound(oracle):
-    """Mixed form against the FP64 oracle: 5000 fixed 1 kpc steps."""
-    rng = np.random.default_rng(16)
-    grid = random_grid(rng, 32, brms=1e-12)
-    spec64 = grid_chain(grid, 5 * U.kpc, bp_fixed(1 * U.kpc), 5 * U.Mpc)
-    spec32 = grid_chain(grid, 5 * U.kpc, bp_fixed(1 * U.kpc), 5 * U.Mpc, precision=_abi.PRECISION_MIXED)
-    c = protons(rng, 256, spread=0.0)
-    a = c.copy()
-    oracle.run(spec64, a)
-    Plan = _engine()
-    b = c.copy()
-    Plan(spec32).run(b)
-    err = rel_pos_err(b, a)
-    assert err.max() <= 1e-6, err.max()
-    np.testing.assert_array_equal(a.trajectory_length, b.trajectory_length)
-    np.testing.assert_array_equal(a.active, b.active)
-
-
-def test_ck_mixed_error(oracle):
-    rng = np.random.default_rng(17)
-    grid = random_grid(rng, 32, brms=1e-12)
-    spec64 = grid_chain(grid, 5 * U.kpc, ck(1e-4, 0.1 * U.kpc, 100 * U.kpc), 5 * U.Mpc)
-    spec32 = grid_chain(grid, 5 * U.kpc, ck(1e-4, 0.1 * U.kpc, 100 * U.kpc), 5 * U.Mpc,
-                        precision=_abi.PRECISION_MIXED)
-    c = protons(rng, 256, spread=0.0)
-    a = c.copy()
-    oracle.run(spec64, a)
-    b = c.copy()
-    _engine()(spec32).run(b)
-    err = rel_pos_err(b, a)
-    # step-size sequences may take a different accept/reject branch where the
-    # error ratio sits within FP32 rounding of 1; the median stays at rounding level
-    assert np.median(err) <= 1e-6, np.median(err)
 
 
 def test_field_eval_fp64_matches_oracle(oracle):
