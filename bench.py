@@ -320,11 +320,11 @@ def main():
     final_64 = d_work.to_host()
 
     # per-candidate error of the mixed form against the FP64 form, beside the
-    # FP64 form's own sensitivity: the same FP64 run started with the x
-    # direction component one ulp larger
+    # FP64 form's own sensitivity: the same FP64 run with every energy one ulp
+    # larger (a 1e-16 change of the gyro-radius applied at every step)
     p_mx, p_64 = final_mx.position(), final_64.position()
     err = np.linalg.norm(p_mx - p_64, axis=1) / np.linalg.norm(p_64, axis=1)
-    d_init.dx.copy_(torch.nextafter(d_init.dx, torch.full_like(d_init.dx, float("inf"))))
+    d_init.energy.copy_(torch.nextafter(d_init.energy, torch.full_like(d_init.energy, float("inf"))))
     one_step(plan_64)
     torch.cuda.synchronize()
     p_ulp = d_work.to_host().position()
@@ -403,10 +403,10 @@ def main():
                      "mixed_over_fp64": value / value_64},
             "mixed_error_vs_fp64": dict(stats(err), measure="|x_mixed - x_fp64| / |x_fp64| per candidate",
                                         well_conditioned={
-                                            "definition": "candidates whose FP64 run with a 1-ulp direction change stays within 1e-12",
+                                            "definition": "candidates whose FP64 run with a 1-ulp energy change stays within 1e-12",
                                             "fraction": float(stable.mean()),
                                             "max_error": float(err[stable].max()) if stable.any() else None}),
-            "fp64_one_ulp_divergence": dict(stats(floor), measure="|x_fp64(dx0 + 1 ulp) - x_fp64(dx0)| / |x_fp64|"),
+            "fp64_one_ulp_divergence": dict(stats(floor), measure="|x_fp64(E + 1 ulp) - x_fp64(E)| / |x_fp64|"),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": d2h, "api": "crp_run (host arrays, pinned)"},
             "roofline": roofline,

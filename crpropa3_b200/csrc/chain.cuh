@@ -168,29 +168,46 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 
 // Add this thread's counts to the run counters, one atomic per warp.
 __device__ __forceinline__ void flush_counters(DevCounters *cnt, unsigned long long steps,
-                                               const StepCount &sc, unsigned long long active) {
-    unsigned long long s = warp_sum(steps), t = warp_sum(sc.tries), e = warp_sum(sc.evals),
-                       a = warp_sum(active);
+                                               const StepCount &sc) {
+    unsigned long long s = warp_sum(steps), t = warp_sum(sc.tries), e = warp_sum(sc.evals);
     if ((threadIdx.x & 31) == 0) {
         if (s) atomicAdd(&cnt->steps, s);
         if (t) atomicAdd(&cnt->tries, t);
         if (e) atomicAdd(&cnt->field_evals, e);
-        if (a) atomicAdd(&cnt->active_left, a);
     }
 }
 
+// Compaction of the candidates that are still active after a launch: the
+// warp's ballot gives each such lane its slot, one atomic per warp reserves
+// the warp's slots in `list` (which may be null: count only).  The count is
+// cnt->active_left.
+__device__ __forceinline__ void append_active(DevCounters *cnt, uint32_t *list, bool still,
+                                              uint32_t index) {
+    const unsigned mask = __ballot_sync(0xffffffffu, still);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(&cnt->active_left, (unsigned long long)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (still && list) list[base + __popc(mask & ((1u << lane) - 1u))] = index;
+}
+
 // One thread per candidate, at most max_steps chain iterations per launch.
-// perm (optional) maps thread -> candidate index.
+// perm_in (optional) maps thread -> candidate index; the candidates still
+// active afterwards are appended to perm_out (optional).
 template <class Prop>
 __device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, uint64_t n,
                                            int max_steps, uint64_t step_cap,
                                            DevCounters *cnt, const DevRecords &rec,
-                                           const uint32_t *perm) {
+                                           const uint32_t *perm_in, uint32_t *perm_out) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     StepCount sc;
-    unsigned long long steps = 0, left = 0;
+    unsigned long long steps = 0;
+    bool still = false;
+    uint64_t i = 0;
     if (t < n) {
-        uint64_t i = perm ? perm[t] : t;
+        i = perm_in ? perm_in[t] : t;
         if (s.active[i]) {
             Cand c;
             load_cand(s, i, c);
@@ -201,11 +218,12 @@ __device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, 
                 k++;
             }
             steps = (unsigned long long)k;
-            left = (c.active && (step_cap == 0 || c.steps < step_cap)) ? 1 : 0;
+            still = c.active && (step_cap == 0 || c.steps < step_cap);
             store_cand(s, c);
         }
     }
-    flush_counters(cnt, steps, sc, left);
+    flush_counters(cnt, steps, sc);
+    append_active(cnt, perm_out, still, (uint32_t)i);
 }
 
 }  // namespace crp

@@ -71,6 +71,9 @@ struct crp_plan {
     void *scratch = nullptr;
     uint64_t rec_cap = 0;
     void *rec_scratch = nullptr;
+    // compaction lists of still-active candidate indices (ping-pong)
+    uint64_t list_cap = 0;
+    uint32_t *lists = nullptr;
     int tuned_block = 0;
 
     ~crp_plan() {
@@ -79,6 +82,7 @@ struct crp_plan {
         if (h_cnt) cudaFreeHost(h_cnt);
         if (scratch) cudaFree(scratch);
         if (rec_scratch) cudaFree(rec_scratch);
+        if (lists) cudaFree(lists);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
@@ -358,20 +362,31 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
         return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE needs step_count (random stream counter)");
     if (o.mode == CRP_MODE_PERSISTENT)
         return fail(CRP_ERR_UNSUPPORTED, "persistent mode is not available in this build");
+    if (n > 0xffffffffull) return fail(CRP_ERR_CAPACITY, "at most 2^32-1 candidates per run");
     cudaStream_t st = (cudaStream_t)o.stream;
     DevState s = to_dev_state(*c);
     DevRecords rec = to_dev_records(o.records);
     int block = o.block_size > 0 ? o.block_size : (p->tuned_block > 0 ? p->tuned_block : 128);
     if (block % 32 || block > 1024) return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d", block);
     int spl = o.steps_per_launch > 0 ? o.steps_per_launch : 4096;
+    if (p->list_cap < n) {
+        if (p->lists) { cudaFree(p->lists); p->lists = nullptr; p->list_cap = 0; }
+        CUDA_TRY(cudaMalloc(&p->lists, sizeof(uint32_t) * 2 * n));
+        p->list_cap = n;
+    }
     double ms_total = 0;
     uint64_t launches = 0;
+    // launch 1 covers every candidate; later launches only the ones the
+    // previous launch left active (compacted index list)
+    uint64_t n_threads = n;
+    const uint32_t *list_in = nullptr;
+    uint32_t *list_out = p->lists;
     for (;;) {
         CUDA_TRY(cudaMemsetAsync(p->d_cnt, 0, sizeof(DevCounters), st));
         CUDA_TRY(cudaEventRecord(p->ev0, st));
         cudaError_t e = (p->precision == CRP_PRECISION_FP64)
-            ? launch_fp64_chunk(p->dev, s, n, spl, o.max_steps, p->d_cnt, rec, nullptr, p->fs, block, st)
-            : launch_mixed_chunk(p->dev, s, n, spl, o.max_steps, p->d_cnt, rec, nullptr, p->fs, block, st);
+            ? launch_fp64_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st)
+            : launch_mixed_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st);
         if (e != cudaSuccess) return cuda_fail(e, "stepping kernel launch");
         CUDA_TRY(cudaEventRecord(p->ev1, st));
         CUDA_TRY(cudaMemcpyAsync(p->h_cnt, p->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
@@ -387,6 +402,9 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
             stats->active_left = p->h_cnt->active_left;
         }
         if (p->h_cnt->active_left == 0) break;
+        n_threads = p->h_cnt->active_left;
+        list_in = list_out;
+        list_out = (list_out == p->lists) ? p->lists + p->list_cap : p->lists;
         if (o.cancel && *o.cancel) {
             if (stats) { stats->launches = launches; stats->device_ms = ms_total; }
             return fail(CRP_ERR_CANCELLED, "run cancelled by the host flag");

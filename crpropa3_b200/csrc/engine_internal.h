@@ -18,16 +18,22 @@ enum FieldSig {
 };
 
 // step_fp64.cu
+// One launch of the chunked stepping kernel: threads t < n advance candidate
+// perm[t] (t without perm) by at most max_steps chain iterations; candidates
+// still active afterwards are appended to perm_out (may be null) and counted
+// in cnt->active_left.
 cudaError_t launch_fp64_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
                               uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
-                              const uint32_t *perm, int fs, int block, cudaStream_t st);
+                              const uint32_t *perm, uint32_t *perm_out, int fs, int block,
+                              cudaStream_t st);
 cudaError_t launch_fp64_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
                               cudaStream_t st);
 
 // step_mixed.cu
 cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
                                uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
-                               const uint32_t *perm, int fs, int block, cudaStream_t st);
+                               const uint32_t *perm, uint32_t *perm_out, int fs, int block,
+                               cudaStream_t st);
 cudaError_t launch_mixed_persistent(const DevPlan &P, const DevState &s, uint64_t n,
                                     uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
                                     int fs, int block, int grid, int refill,

@@ -492,8 +492,8 @@ template <template <int> class Prop, int FS>
 __global__ void __launch_bounds__(128) mixed_chunk_kernel(DevPlan P, DevState s, uint64_t n,
                                                           int max_steps, uint64_t step_cap,
                                                           DevCounters *cnt, DevRecords rec,
-                                                          const uint32_t *perm) {
-    chunk_body<Prop<FS>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+                                                          const uint32_t *perm, uint32_t *perm_out) {
+    chunk_body<Prop<FS>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
 }
 
 __global__ void mixed_field_kernel(DevPlan P, uint64_t n, const double *pos, double *out) {
@@ -506,27 +506,29 @@ __global__ void mixed_field_kernel(DevPlan P, uint64_t n, const double *pos, dou
 template <template <int> class Prop>
 cudaError_t launch_prop(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
                         uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
-                        const uint32_t *perm, int fs, int block, cudaStream_t st) {
+                        const uint32_t *perm, uint32_t *perm_out, int fs, int block,
+                        cudaStream_t st) {
     unsigned grid = (unsigned)((n + block - 1) / block);
     if (fs == FS_GRID)
-        mixed_chunk_kernel<Prop, FS_GRID><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+        mixed_chunk_kernel<Prop, FS_GRID><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
     else if (fs == FS_PLANE_WAVE)
-        mixed_chunk_kernel<Prop, FS_PLANE_WAVE><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+        mixed_chunk_kernel<Prop, FS_PLANE_WAVE><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
     else
-        mixed_chunk_kernel<Prop, FS_GENERIC><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm);
+        mixed_chunk_kernel<Prop, FS_GENERIC><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
-                               uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
-                               const uint32_t *perm, int fs, int block, cudaStream_t st) {
+                              uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
+                              const uint32_t *perm, uint32_t *perm_out, int fs, int block,
+                              cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     int prop = P.modules[P.prop_index].propagator;
-    if (prop == CRP_PROP_BP) return launch_prop<BP>(P, s, n, max_steps, step_cap, cnt, rec, perm, fs, block, st);
-    if (prop == CRP_PROP_CK) return launch_prop<CK>(P, s, n, max_steps, step_cap, cnt, rec, perm, fs, block, st);
-    return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, fs, block, st);
+    if (prop == CRP_PROP_BP) return launch_prop<BP>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    if (prop == CRP_PROP_CK) return launch_prop<CK>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
 }
 
 cudaError_t launch_mixed_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
