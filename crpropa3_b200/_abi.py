@@ -108,6 +108,16 @@ class OutputRows(C.Structure):
                 ("source_position", _dp), ("source_direction", _dp), ("weight", _dp)]
 
 
+class NoAllocGridBpDesc(C.Structure):
+    _fields_ = [("grid_values", C.c_void_p), ("nx", C.c_uint64), ("ny", C.c_uint64),
+                ("nz", C.c_uint64), ("origin", _d * 3), ("spacing", _d * 3),
+                ("reflective", C.c_int32), ("clip_volume", C.c_int32), ("step", _d),
+                ("max_length", _d), ("precision", C.c_int32), ("steps_per_launch", C.c_int32)]
+
+
+NOALLOC_MAX_CANDIDATES = 1 << 20
+
+
 class Candidates(C.Structure):
     _fields_ = [(name, C.POINTER(t)) for name, t in CANDIDATE_FIELDS]
 

@@ -27,6 +27,8 @@ SIGNATURES = {
     "crp_plane_wave_modes": (_i32, [_d, _d, _d, _d, _d, _d, _i32, _i32, _dp, _dp, _dp, _dp, _dp]),
     "crp_source_sample": (_i32, [C.c_void_p, _u32, _u64, _i32p, _dp, _dp]),
     "crp_text_output_write": (_i32, [C.c_char_p, _i32, _i32, C.c_void_p, _u64, C.c_void_p]),
+    "crp_run_device_noalloc": (_i32, [C.POINTER(_abi.NoAllocGridBpDesc), C.POINTER(_abi.Candidates),
+                                      _u64, C.c_void_p, C.POINTER(_abi.RunStats)]),
 }
 
 # entry points added by later parts of the library, declared when present

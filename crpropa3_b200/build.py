@@ -31,6 +31,7 @@ SOURCES = {
     "persistent.cu": [],
     "turbulence.cu": [],
     "crp_engine.cu": [],
+    "noalloc.cu": [],
     "host_tools.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }
 LINK_LIBS = ["-lcufft"]

@@ -261,6 +261,43 @@ crp_status crp_field_eval(crp_plan *plan, uint64_t n, const double *pos_xyz,
                           double *b_xyz, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Allocation-free run
+ * ---------------------------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code inside a CUDA-graph capture region, a process whose device
+ * memory belongs to another allocator, a plugin limited to the buffers its
+ * host hands it -- and so cannot create a crp_plan: a fixed-step
+ * PropagationBP over one Grid3f whose values the caller already holds on the
+ * device, followed by MaximumTrajectoryLength.  Nothing is allocated: the
+ * run's scratch (counters and compaction lists) is a fixed static device
+ * array that every device loading the library holds until exit, so one call
+ * takes at most CRP_NOALLOC_MAX_CANDIDATES candidates (larger n returns
+ * CRP_ERR_CAPACITY).  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture begins.  All calls share the array: calls whose work overlaps on
+ * the GPU race on it.  Results equal crp_run_device with the same chain and
+ * precision. */
+#define CRP_NOALLOC_MAX_CANDIDATES (1u << 20)
+
+typedef struct crp_noalloc_grid_bp_desc {
+    const float *grid_values; /* DEVICE pointer: nx*ny*nz Vector3f cells, Grid.h:338 order */
+    uint64_t nx, ny, nz;
+    double origin[3];
+    double spacing[3];
+    int32_t reflective;
+    int32_t clip_volume;
+    double step;             /* PropagationBP fixed step [m] */
+    double max_length;       /* MaximumTrajectoryLength [m] */
+    int32_t precision;       /* crp_precision */
+    int32_t steps_per_launch; /* 0: default */
+} crp_noalloc_grid_bp_desc;
+
+crp_status crp_run_device_noalloc(const crp_noalloc_grid_bp_desc *desc,
+                                  const crp_candidates *device, uint64_t n, void *stream,
+                                  crp_run_stats *stats);
+
+/* ------------------------------------------------------------------------
  * Host-side set-up and output (no device needed)
  * ---------------------------------------------------------------------- */
 
