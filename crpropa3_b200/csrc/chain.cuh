@@ -25,6 +25,12 @@ struct Cand {
     uint32_t flags;
     int32_t id;
     bool active;
+    // The Grid3f cell the last interpolation read: linear indices of its
+    // first and last corner and the 8 corner vectors.  A candidate stays in
+    // one cell for several steps, so the gathers are skipped while it does;
+    // the values are the grid's own, so results do not change.
+    long long cell0, cell7;
+    float corner[8][3];
 };
 
 __device__ __forceinline__ void load_cand(const DevState &s, uint64_t i, Cand &c) {
@@ -39,6 +45,8 @@ __device__ __forceinline__ void load_cand(const DevState &s, uint64_t i, Cand &c
     c.flags = s.flags[i];
     c.id = s.id[i];
     c.active = s.active[i] != 0;
+    c.cell0 = -1;
+    c.cell7 = -1;
 }
 
 __device__ __forceinline__ void store_cand(const DevState &s, const Cand &c) {

@@ -17,6 +17,10 @@
 #include "crmath.cuh"
 #include "engine_internal.h"
 
+#ifndef CRP_BP_FIXED_MIN_BLOCKS
+#define CRP_BP_FIXED_MIN_BLOCKS 1
+#endif
+
 namespace crp {
 namespace {
 
@@ -37,7 +41,10 @@ __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b 
 __device__ __forceinline__ double clipd(double x, double lo, double hi) { return dmax(lo, dmin(x, hi)); }
 
 // Grid<Vector3f>::interpolate (Grid.h:318) -> trilinearInterpolate (:540).
-__device__ d3 grid_field(const DevGrid &g, d3 pos) {
+// With a cell cache (FS_GRID kernels) the 8 corners are loaded only when the
+// cell changes.
+template <bool CACHE>
+__device__ __forceinline__ d3 grid_field_t(const DevGrid &g, d3 pos, Cand *cc) {
     if (g.clip_volume) {
         bool in = (pos.x >= g.ox) && (pos.x <= g.ex);
         in &= (pos.y >= g.oy) && (pos.y <= g.ey);
@@ -89,10 +96,15 @@ __device__ d3 grid_field(const DevGrid &g, d3 pos) {
     const float *p0 = v + 3 * (b00 + iz0), *p1 = v + 3 * (b10 + iz0), *p2 = v + 3 * (b01 + iz0),
                 *p3 = v + 3 * (b00 + iz1), *p4 = v + 3 * (b10 + iz1), *p5 = v + 3 * (b01 + iz1),
                 *p6 = v + 3 * (b11 + iz0), *p7 = v + 3 * (b11 + iz1);
-    float c[8][3];
+    float lc[8][3];
+    float (*c)[3] = CACHE ? cc->corner : lc;
+    const long long k0 = (long long)(b00 + iz0), k7 = (long long)(b11 + iz1);
+    if (!CACHE || k0 != cc->cell0 || k7 != cc->cell7) {
 #define LD3(k, p) c[k][0] = __ldg(p); c[k][1] = __ldg(p + 1); c[k][2] = __ldg(p + 2);
-    LD3(0, p0) LD3(1, p1) LD3(2, p2) LD3(3, p3) LD3(4, p4) LD3(5, p5) LD3(6, p6) LD3(7, p7)
+        LD3(0, p0) LD3(1, p1) LD3(2, p2) LD3(3, p3) LD3(4, p4) LD3(5, p5) LD3(6, p6) LD3(7, p7)
 #undef LD3
+        if (CACHE) { cc->cell0 = k0; cc->cell7 = k7; }
+    }
     const float wx[8] = {fx1, fx0, fx1, fx1, fx0, fx1, fx0, fx0};
     const float wy[8] = {fy1, fy1, fy0, fy1, fy1, fy0, fy0, fy0};
     const float wz[8] = {fz1, fz1, fz1, fz0, fz0, fz0, fz1, fz0};
@@ -105,6 +117,8 @@ __device__ d3 grid_field(const DevGrid &g, d3 pos) {
     }
     return mk(bx, by, bz);
 }
+
+__device__ d3 grid_field(const DevGrid &g, d3 pos) { return grid_field_t<false>(g, pos, nullptr); }
 
 // PlaneWaveTurbulence::getField, scalar branch (PlaneWaveTurbulence.cpp:233).
 __device__ d3 plane_wave_field(const DevPlaneWave &w, d3 pos) {
@@ -148,8 +162,8 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
 
 // MagneticFieldList::getField (MagneticField.cpp:64) or the single field.
 template <int FS>
-__device__ __forceinline__ d3 field_at(const DevPlan &P, d3 pos) {
-    if (FS == FS_GRID) return grid_field(P.fields[0].grid, pos);
+__device__ __forceinline__ d3 field_at(const DevPlan &P, d3 pos, Cand *cc = nullptr) {
+    if (FS == FS_GRID) return grid_field_t<true>(P.fields[0].grid, pos, cc);
     if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, pos);
     if (P.n_fields == 1) return component_field(P.fields[0], pos);
     d3 b = mk(0, 0, 0);
@@ -167,9 +181,9 @@ __device__ __forceinline__ void set_current_step(Cand &c, double s) {  // Candid
 // ---------------------------------------------------------------- Boris push
 template <int FS>
 __device__ __forceinline__ void bp_dy(const DevPlan &P, d3 &x, d3 &u, double step, double q,
-                                      double m) {
+                                      double m, Cand *cc) {
     x = add(x, divs(muls(u, step), 2.));
-    d3 B = field_at<FS>(P, x);
+    d3 B = field_at<FS>(P, x, cc);
     d3 t = divs(muls(divs(divs(muls(B, q), 2), m), step), kCLight);
     d3 s = divs(muls(t, 2), (1 + dot(t, t)));
     d3 vh = add(u, cross(u, t));
@@ -177,7 +191,7 @@ __device__ __forceinline__ void bp_dy(const DevPlan &P, d3 &x, d3 &u, double ste
     x = add(x, divs(muls(u, step), 2.));
 }
 
-template <int FS>
+template <int FS, int MODE = 0>
 struct BP {
     // PropagationBP::process (PropagationBP.cpp:62)
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
@@ -193,17 +207,17 @@ struct BP {
         double newStep = step;
         double mass = c.E / (kCLight * kCLight);
         d3 xo = mk(c.x, c.y, c.z), uo = mk(c.dx, c.dy, c.dz);
-        if (m.min_step == m.max_step) {
-            bp_dy<FS>(P, xo, uo, step, q, mass);
+        if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
+            bp_dy<FS>(P, xo, uo, step, q, mass, &c);
             sc.tries++; sc.evals++;
         } else {
             step = clipd(c.next, m.min_step, m.max_step);
             newStep = step;
             for (int guard = 0; guard < 4096; guard++) {
                 d3 x1 = mk(c.x, c.y, c.z), u1 = mk(c.dx, c.dy, c.dz), xh = x1, uh = u1;
-                bp_dy<FS>(P, x1, u1, step, q, mass);
-                bp_dy<FS>(P, xh, uh, step / 2, q, mass);
-                bp_dy<FS>(P, xh, uh, step / 2, q, mass);
+                bp_dy<FS>(P, x1, u1, step, q, mass, &c);
+                bp_dy<FS>(P, xh, uh, step / 2, q, mass, &c);
+                bp_dy<FS>(P, xh, uh, step / 2, q, mass, &c);
                 sc.tries++; sc.evals += 3;
                 double S = norm(sub(x1, xh)) / (step * (1 - 1 / 4.));
                 xo = x1; uo = u1;
@@ -247,7 +261,7 @@ __constant__ double ck_bs[6] = {2825. / 27648., 0., 18575. / 48384., 13525. / 55
 
 template <int FS>
 __device__ __forceinline__ void ck_try(const DevPlan &P, d3 x, d3 u, double h, double q, double E,
-                                       d3 &xo, d3 &uo, d3 &eu) {
+                                       d3 &xo, d3 &uo, d3 &eu, Cand *cc) {
     d3 kx[6], ku[6];
     xo = x; uo = u;
     eu = mk(0, 0, 0);
@@ -260,7 +274,7 @@ __device__ __forceinline__ void ck_try(const DevPlan &P, d3 x, d3 u, double h, d
             yu = add(yu, muls(muls(ku[j], ck_a[i * 6 + j]), h));
         }
         d3 vel = muls(unit(yu), kCLight);
-        d3 B = field_at<FS>(P, yx);
+        d3 B = field_at<FS>(P, yx, cc);
         d3 dudt = muls(cross(vel, B), q * kCLight / E);
         kx[i] = vel; ku[i] = dudt;
         xo = add(xo, muls(muls(kx[i], ck_b[i]), h));
@@ -269,7 +283,7 @@ __device__ __forceinline__ void ck_try(const DevPlan &P, d3 x, d3 u, double h, d
     }
 }
 
-template <int FS>
+template <int FS, int MODE = 0>
 struct CK {
     // PropagationCK::process (PropagationCK.cpp:77)
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
@@ -285,14 +299,14 @@ struct CK {
         d3 xo, uo, eu;
         d3 x = mk(c.x, c.y, c.z), u = mk(c.dx, c.dy, c.dz);
         double newStep = step;
-        if (m.min_step == m.max_step) {
-            ck_try<FS>(P, x, u, step / kCLight, c.q, c.E, xo, uo, eu);
+        if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
+            ck_try<FS>(P, x, u, step / kCLight, c.q, c.E, xo, uo, eu, &c);
             sc.tries++; sc.evals += 6;
         } else {
             step = clipd(c.next, m.min_step, m.max_step);
             newStep = step;
             for (int guard = 0; guard < 4096; guard++) {
-                ck_try<FS>(P, x, u, step / kCLight, c.q, c.E, xo, uo, eu);
+                ck_try<FS>(P, x, u, step / kCLight, c.q, c.E, xo, uo, eu, &c);
                 sc.tries++; sc.evals += 6;
                 double r = norm(eu) / m.tolerance;
                 if (r > 1) {
@@ -347,7 +361,7 @@ __device__ __forceinline__ d3 rotated(d3 v, d3 axis, double angle) {  // Vector3
 
 template <int FS>
 __device__ __forceinline__ void sde_try(const DevPlan &P, d3 PosIn, d3 &POut, d3 &PosErr,
-                                        double propStep) {
+                                        double propStep, Cand *cc) {
     d3 k[6];
     POut = PosIn;
 #pragma unroll
@@ -355,7 +369,7 @@ __device__ __forceinline__ void sde_try(const DevPlan &P, d3 PosIn, d3 &POut, d3
         d3 y_n = PosIn;
 #pragma unroll
         for (int j = 0; j < i; j++) y_n = add(y_n, muls(muls(k[j], ck_a[i * 6 + j]), propStep));
-        d3 B = field_at<FS>(P, y_n);
+        d3 B = field_at<FS>(P, y_n, cc);
         k[i] = muls(unit(B), kCLight);
         POut = add(POut, muls(muls(k[i], ck_b[i]), propStep));
         PosErr = add(PosErr, divs(muls(muls(k[i], ck_b[i] - ck_bs[i]), propStep), CRP_KPC));
@@ -388,7 +402,7 @@ struct SDE {
         double r = 42.;
         do {
             d3 PosOut = mk(0, 0, 0), PosErr = mk(0, 0, 0);
-            sde_try<FS>(P, PosIn, PosOut, PosErr, propTime);
+            sde_try<FS>(P, PosIn, PosOut, PosErr, propTime, &c);
             sc.tries++; sc.evals += 6;
             r = norm(PosErr) / m.tolerance;
             propTime *= 0.5;
@@ -398,7 +412,7 @@ struct SDE {
         double allowedTime = TStep * sqrt(h) / kCLight / (double)stepNumber;
         d3 Start = PosIn, PosOut = mk(0, 0, 0), PosErr = mk(0, 0, 0);
         for (unsigned long long j = 0; j < stepNumber; j++) {
-            sde_try<FS>(P, Start, PosOut, PosErr, allowedTime);
+            sde_try<FS>(P, Start, PosOut, PosErr, allowedTime, &c);
             sc.tries++; sc.evals += 6;
             Start = PosOut;
         }
@@ -433,8 +447,19 @@ struct SDE {
     }
 };
 
+// step-mode variants selected by the launcher from min_step == max_step, so
+// that a fixed-step kernel carries no adaptive-controller registers
+template <int FS> using BPFixed = BP<FS, 1>;
+// resident blocks of 128 threads per SM the register budget is sized for:
+// the fixed-step Boris push is latency bound on its gathers and wants warps
+template <class T> struct MinBlocks { static constexpr int value = 1; };
+template <int FS, int MODE> struct MinBlocks<BP<FS, MODE>> { static constexpr int value = MODE == 1 ? CRP_BP_FIXED_MIN_BLOCKS : 1; };
+template <int FS> using BPAdaptive = BP<FS, 2>;
+template <int FS> using CKFixed = CK<FS, 1>;
+template <int FS> using CKAdaptive = CK<FS, 2>;
+
 template <template <int> class Prop, int FS>
-__global__ void __launch_bounds__(128) fp64_chunk_kernel(DevPlan P, DevState s, uint64_t n,
+__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_chunk_kernel(DevPlan P, DevState s, uint64_t n,
                                                          int max_steps, uint64_t step_cap,
                                                          DevCounters *cnt, DevRecords rec,
                                                          const uint32_t *perm, uint32_t *perm_out) {
@@ -471,8 +496,14 @@ cudaError_t launch_fp64_chunk(const DevPlan &P, const DevState &s, uint64_t n, i
                               cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     int prop = P.modules[P.prop_index].propagator;
-    if (prop == CRP_PROP_BP) return launch_prop<BP>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
-    if (prop == CRP_PROP_CK) return launch_prop<CK>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    const DevModule &pm = P.modules[P.prop_index];
+    const bool fixed = pm.min_step == pm.max_step;
+    if (prop == CRP_PROP_BP)
+        return fixed ? launch_prop<BPFixed>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st)
+                     : launch_prop<BPAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    if (prop == CRP_PROP_CK)
+        return fixed ? launch_prop<CKFixed>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st)
+                     : launch_prop<CKAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
     return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
 }
 

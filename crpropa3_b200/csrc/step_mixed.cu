@@ -15,6 +15,10 @@
 #include "chain.cuh"
 #include "engine_internal.h"
 
+#ifndef CRP_BP_FIXED_MIN_BLOCKS
+#define CRP_BP_FIXED_MIN_BLOCKS 1
+#endif
+
 namespace crp {
 namespace {
 
@@ -34,7 +38,10 @@ __device__ __forceinline__ int wrap(int i, int n, bool pow2) {
 
 // Trilinear Grid3f interpolation: FP64 cell coordinates, FP32 weights and
 // values (the reference's own interpolation arithmetic is FP32, Grid.h:571).
-__device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
+// With a cell cache (FS_GRID kernels) the 8 corners are loaded only when the
+// cell changes.
+template <bool CACHE>
+__device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y, double z, Cand *cc) {
     if (g.clip_volume) {
         bool in = (x >= g.ox) && (x <= g.ex) && (y >= g.oy) && (y <= g.ey) && (z >= g.oz) && (z <= g.ez);
         if (!in) return f3mk(0.f, 0.f, 0.f);
@@ -76,32 +83,37 @@ __device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
     const size_t idx[8] = {b00 + iz0, b10 + iz0, b01 + iz0, b00 + iz1, b10 + iz1, b01 + iz1, b11 + iz0, b11 + iz1};
     const float w[8] = {fx1 * fy1 * fz1, fx0 * fy1 * fz1, fx1 * fy0 * fz1, fx1 * fy1 * fz0,
                         fx0 * fy1 * fz0, fx1 * fy0 * fz0, fx0 * fy0 * fz1, fx0 * fy0 * fz0};
+    float lc[8][3];
+    float (*c)[3] = CACHE ? cc->corner : lc;
+    const long long k0 = (long long)idx[0], k7 = (long long)idx[7];
+    if (!CACHE || k0 != cc->cell0 || k7 != cc->cell7) {
+        if (g.values4) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                float4 v = __ldg(g.values4 + idx[k]);
+                c[k][0] = v.x; c[k][1] = v.y; c[k][2] = v.z;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const float *p = g.values + 3 * idx[k];
+                c[k][0] = __ldg(p); c[k][1] = __ldg(p + 1); c[k][2] = __ldg(p + 2);
+            }
+        }
+        if (CACHE) { cc->cell0 = k0; cc->cell7 = k7; }
+    }
     float bx = 0.f, by = 0.f, bz = 0.f;
-    if (g.values4) {
-        float4 c[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) c[k] = __ldg(g.values4 + idx[k]);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            bx = fmaf(c[k].x, w[k], bx);
-            by = fmaf(c[k].y, w[k], by);
-            bz = fmaf(c[k].z, w[k], bz);
-        }
-    } else {
-        float c[8][3];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const float *p = g.values + 3 * idx[k];
-            c[k][0] = __ldg(p); c[k][1] = __ldg(p + 1); c[k][2] = __ldg(p + 2);
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            bx = fmaf(c[k][0], w[k], bx);
-            by = fmaf(c[k][1], w[k], by);
-            bz = fmaf(c[k][2], w[k], bz);
-        }
+    for (int k = 0; k < 8; k++) {
+        bx = fmaf(c[k][0], w[k], bx);
+        by = fmaf(c[k][1], w[k], by);
+        bz = fmaf(c[k][2], w[k], bz);
     }
     return f3mk(bx, by, bz);
+}
+
+__device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
+    return grid_field_t<false>(g, x, y, z, nullptr);
 }
 
 // PlaneWaveTurbulence sum: FP64 phase k*kappa.x + beta, reduced to
@@ -152,8 +164,9 @@ __device__ f3 component_field(const DevComponent &f, double x, double y, double 
 }
 
 template <int FS>
-__device__ __forceinline__ f3 field_at(const DevPlan &P, double x, double y, double z) {
-    if (FS == FS_GRID) return grid_field(P.fields[0].grid, x, y, z);
+__device__ __forceinline__ f3 field_at(const DevPlan &P, double x, double y, double z,
+                                       Cand *cc = nullptr) {
+    if (FS == FS_GRID) return grid_field_t<true>(P.fields[0].grid, x, y, z, cc);
     if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, x, y, z);
     if (P.n_fields == 1) return component_field(P.fields[0], x, y, z);
     f3 b = f3mk(0.f, 0.f, 0.f);
@@ -184,10 +197,10 @@ __device__ __forceinline__ void renorm(double &x, double &y, double &z) {
 // One PropagationBP::dY (PropagationBP.cpp:19) with FP32 rotation increment.
 template <int FS>
 __device__ __forceinline__ void bp_dy(const DevPlan &P, double &x, double &y, double &z, double &ux,
-                                      double &uy, double &uz, double step, float kt) {
+                                      double &uy, double &uz, double step, float kt, Cand *cc) {
     double hh = 0.5 * step;
     x = fma(ux, hh, x); y = fma(uy, hh, y); z = fma(uz, hh, z);
-    f3 B = field_at<FS>(P, x, y, z);
+    f3 B = field_at<FS>(P, x, y, z, cc);
     f3 t = f3mk(B.x * kt, B.y * kt, B.z * kt);   // t = B q step / (2 m c)
     float sf = __fdividef(2.f, 1.f + dot(t, t));
     f3 s = f3mk(t.x * sf, t.y * sf, t.z * sf);
@@ -199,7 +212,7 @@ __device__ __forceinline__ void bp_dy(const DevPlan &P, double &x, double &y, do
     x = fma(ux, hh, x); y = fma(uy, hh, y); z = fma(uz, hh, z);
 }
 
-template <int FS>
+template <int FS, int MODE = 0>
 struct BP {
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
@@ -215,8 +228,8 @@ struct BP {
         // t = B * q / 2 / m * step / c with m = E/c^2  ->  B * (q c step / (2 E))
         const double kq = q * kCLight / (2.0 * c.E);
         double xo = c.x, yo = c.y, zo = c.z, uxo = c.dx, uyo = c.dy, uzo = c.dz;
-        if (m.min_step == m.max_step) {
-            bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, (float)(kq * step));
+        if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
+            bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, (float)(kq * step), &c);
             sc.tries++; sc.evals++;
         } else {
             step = clipd(c.next, m.min_step, m.max_step);
@@ -224,9 +237,9 @@ struct BP {
             for (int guard = 0; guard < 4096; guard++) {
                 double x1 = c.x, y1 = c.y, z1 = c.z, u1x = c.dx, u1y = c.dy, u1z = c.dz;
                 double x2 = c.x, y2 = c.y, z2 = c.z, u2x = c.dx, u2y = c.dy, u2z = c.dz;
-                bp_dy<FS>(P, x1, y1, z1, u1x, u1y, u1z, step, (float)(kq * step));
-                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2));
-                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2));
+                bp_dy<FS>(P, x1, y1, z1, u1x, u1y, u1z, step, (float)(kq * step), &c);
+                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2), &c);
+                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2), &c);
                 sc.tries++; sc.evals += 3;
                 double ex = x1 - x2, ey = y1 - y2, ez = z1 - z2;
                 double S = sqrt(ex * ex + ey * ey + ez * ez) / (step * 0.75);
@@ -272,7 +285,7 @@ __constant__ double ck_eb[6] = {37. / 378. - 2825. / 27648., 0. - 0., 250. / 621
 // FP32, stage positions as FP64 base + FP32 offset, error sum in FP64.
 // Returns the position / direction increments and the direction error norm.
 template <int FS>
-__device__ __forceinline__ double ck_try(const DevPlan &P, const Cand &c, double h, float qc2E,
+__device__ __forceinline__ double ck_try(const DevPlan &P, Cand &c, double h, float qc2E,
                                          double &ddx, double &ddy, double &ddz, double &dux,
                                          double &duy, double &duz) {
     // stage derivative kx_i = c * unit(u_i) (as a unit vector, the factor c
@@ -294,7 +307,7 @@ __device__ __forceinline__ double ck_try(const DevPlan &P, const Cand &c, double
         }
         float inv = rsqrtf(vx * vx + vy * vy + vz * vz);
         f3 vel = f3mk(vx * inv, vy * inv, vz * inv);  // unit velocity
-        f3 B = field_at<FS>(P, c.x + (double)(ox * hc), c.y + (double)(oy * hc), c.z + (double)(oz * hc));
+        f3 B = field_at<FS>(P, c.x + (double)(ox * hc), c.y + (double)(oy * hc), c.z + (double)(oz * hc), &c);
         f3 d = cross(vel, B);
         kx[i] = vel;
         ku[i] = f3mk(d.x * qc2E, d.y * qc2E, d.z * qc2E);  // (q c / E) (c vel x B)
@@ -309,7 +322,7 @@ __device__ __forceinline__ double ck_try(const DevPlan &P, const Cand &c, double
     return sqrt(eux * eux + euy * euy + euz * euz);
 }
 
-template <int FS>
+template <int FS, int MODE = 0>
 struct CK {
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
@@ -324,7 +337,7 @@ struct CK {
         const float qc2E = (float)(c.q * kCLight * kCLight / c.E);
         double ddx, ddy, ddz, dux, duy, duz;
         double newStep = step;
-        if (m.min_step == m.max_step) {
+        if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
             ck_try<FS>(P, c, step / kCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
             sc.tries++; sc.evals += 6;
         } else {
@@ -373,7 +386,7 @@ __device__ __forceinline__ double s_norm(Stream &s) {
 // stage directions in FP32, FP64 base position + FP32 offsets, FP64 error.
 template <int FS>
 __device__ __forceinline__ void sde_try(const DevPlan &P, double x, double y, double z, double t,
-                                        double &ox, double &oy, double &oz, double &err) {
+                                        double &ox, double &oy, double &oz, double &err, Cand *cc) {
     f3 k[6];
     const float tc = (float)(t * kCLight);
     float sx = 0.f, sy = 0.f, sz = 0.f;
@@ -386,7 +399,7 @@ __device__ __forceinline__ void sde_try(const DevPlan &P, double x, double y, do
             float a = ck_af[i * 6 + j];
             ax = fmaf(k[j].x, a, ax); ay = fmaf(k[j].y, a, ay); az = fmaf(k[j].z, a, az);
         }
-        f3 B = field_at<FS>(P, x + (double)(ax * tc), y + (double)(ay * tc), z + (double)(az * tc));
+        f3 B = field_at<FS>(P, x + (double)(ax * tc), y + (double)(ay * tc), z + (double)(az * tc), cc);
         float inv = rsqrtf(B.x * B.x + B.y * B.y + B.z * B.z);
         k[i] = f3mk(B.x * inv, B.y * inv, B.z * inv);
         float b = ck_bf[i];
@@ -421,7 +434,7 @@ struct SDE {
         unsigned counter = 0;
         double r, ox, oy, oz, err;
         do {
-            sde_try<FS>(P, c.x, c.y, c.z, propTime, ox, oy, oz, err);
+            sde_try<FS>(P, c.x, c.y, c.z, propTime, ox, oy, oz, err, &c);
             sc.tries++; sc.evals += 6;
             r = err / m.tolerance;
             propTime *= 0.5;
@@ -431,7 +444,7 @@ struct SDE {
         double allowedTime = TStep * sh / kCLight / (double)stepNumber;
         double sx = c.x, sy = c.y, sz = c.z;
         for (unsigned long long j = 0; j < stepNumber; j++) {
-            sde_try<FS>(P, sx, sy, sz, allowedTime, ox, oy, oz, err);
+            sde_try<FS>(P, sx, sy, sz, allowedTime, ox, oy, oz, err, &c);
             sc.tries++; sc.evals += 6;
             sx = ox; sy = oy; sz = oz;
         }
@@ -488,8 +501,19 @@ struct SDE {
     }
 };
 
+// step-mode variants selected by the launcher from min_step == max_step, so
+// that a fixed-step kernel carries no adaptive-controller registers
+template <int FS> using BPFixed = BP<FS, 1>;
+// resident blocks of 128 threads per SM the register budget is sized for:
+// the fixed-step Boris push is latency bound on its gathers and wants warps
+template <class T> struct MinBlocks { static constexpr int value = 1; };
+template <int FS, int MODE> struct MinBlocks<BP<FS, MODE>> { static constexpr int value = MODE == 1 ? CRP_BP_FIXED_MIN_BLOCKS : 1; };
+template <int FS> using BPAdaptive = BP<FS, 2>;
+template <int FS> using CKFixed = CK<FS, 1>;
+template <int FS> using CKAdaptive = CK<FS, 2>;
+
 template <template <int> class Prop, int FS>
-__global__ void __launch_bounds__(128) mixed_chunk_kernel(DevPlan P, DevState s, uint64_t n,
+__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_chunk_kernel(DevPlan P, DevState s, uint64_t n,
                                                           int max_steps, uint64_t step_cap,
                                                           DevCounters *cnt, DevRecords rec,
                                                           const uint32_t *perm, uint32_t *perm_out) {
@@ -526,8 +550,14 @@ cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, 
                               cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     int prop = P.modules[P.prop_index].propagator;
-    if (prop == CRP_PROP_BP) return launch_prop<BP>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
-    if (prop == CRP_PROP_CK) return launch_prop<CK>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    const DevModule &pm = P.modules[P.prop_index];
+    const bool fixed = pm.min_step == pm.max_step;
+    if (prop == CRP_PROP_BP)
+        return fixed ? launch_prop<BPFixed>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st)
+                     : launch_prop<BPAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    if (prop == CRP_PROP_CK)
+        return fixed ? launch_prop<CKFixed>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st)
+                     : launch_prop<CKAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
     return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
 }
 

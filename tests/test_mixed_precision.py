@@ -3,14 +3,16 @@
 The stated bound: relative final-position error <= 1e-6 against FP64, for
 the fixed-step Boris push (the headline workload).
 
-In a turbulent field low-rigidity trajectories are chaotic: an energy one
-ulp away (a 1e-16 change of the gyro-radius, applied at every step) grows to
-O(1) over a few thousand steps, so no implementation that differs from the
-FP64 form in any rounding can stay within 1e-6 of it there.  The bound is
-therefore tested where the FP64 problem is itself well conditioned, measured
-directly as the FP64 form's own divergence under that one-ulp change: where
-it stays <= 1e-12 (condition number <= 1e4) the mixed form must be within
-1e-6; and it must hold for every candidate of a weakly deflected case.
+In a turbulent field low-rigidity trajectories are chaotic: the FP64 form
+itself amplifies a 1e-12 rad rotation of the initial direction by factors up
+to 1e11 over a few Mpc, so no implementation that differs from the FP64 form
+in any rounding can stay within 1e-6 of it there.  The bound is therefore
+tested where the FP64 problem is well conditioned, measured directly: the
+amplification A = (final-position change / |x|) / 1e-12 of that rotation in
+the FP64 form.  Where A <= 100 the mixed form must be within 1e-6; and it
+must hold for every candidate of a weakly deflected case.  (A one-ulp change
+of the energy is no probe: m = E/c^2 often rounds to the same double and
+the change vanishes.)
 
 For the adaptive Cash-Karp step the comparison is different in kind: FP32
 stage derivatives move the controller's error ratio by ~1e-4 relative, so an
@@ -23,7 +25,7 @@ FP64 at tol and FP64 at tol/10.
 import numpy as np
 import pytest
 
-from helpers import P, U, _abi, bp_fixed, ck, grid_chain, protons, random_grid, rel_pos_err
+from helpers import P, U, _abi, bp_fixed, ck, grid_chain, normalize, protons, random_grid, rel_pos_err
 
 pytestmark = pytest.mark.gpu
 
@@ -35,11 +37,14 @@ def _run(spec, cands):
     return out
 
 
-def _one_ulp(c):
-    """The same candidates with the energy one ulp larger."""
-    d = c.copy()
-    d.energy[:] = np.nextafter(d.energy, np.inf)
-    return d
+def _rotated(c, angle=1e-12):
+    """The same candidates with the initial direction rotated by `angle`."""
+    d = c.direction()
+    perp = np.cross(d, np.array([0.3, -0.5, 0.8]))
+    perp /= np.linalg.norm(perp, axis=1)[:, None]
+    r = c.copy()
+    r.set_direction(normalize(d + angle * perp))
+    return r
 
 
 def _kolmogorov(n, spacing, brms, lmin, lmax):
@@ -63,19 +68,19 @@ def test_bp_mixed_bound_weak_deflection(oracle):
 
 
 def test_bp_mixed_bound_where_fp64_is_well_conditioned(oracle):
-    """Chaotic case: the bound holds wherever FP64 itself is stable to 1 ulp."""
+    """Chaotic case: the bound holds wherever FP64 amplifies a perturbation <= 100x."""
     grid = _kolmogorov(64, 10 * U.kpc, 10 * U.nG, 20 * U.kpc, 200 * U.kpc)
     rng = np.random.default_rng(32)
     c = protons(rng, 2048, emin=1 * U.EeV, emax=100 * U.EeV, spread=0.0)
     s64 = grid_chain(grid, 10 * U.kpc, bp_fixed(1 * U.kpc), 3 * U.Mpc)
     smx = grid_chain(grid, 10 * U.kpc, bp_fixed(1 * U.kpc), 3 * U.Mpc, precision=_abi.PRECISION_MIXED)
     f64 = _run(s64, c)
-    f64_ulp = _run(s64, _one_ulp(c))
+    f64_rot = _run(s64, _rotated(c))
     mixed = _run(smx, c)
-    floor = rel_pos_err(f64_ulp, f64)
+    amplification = rel_pos_err(f64_rot, f64) / 1e-12
     err = rel_pos_err(mixed, f64)
-    stable = floor <= 1e-12
-    assert stable.mean() >= 0.25, stable.mean()
+    stable = amplification <= 100
+    assert stable.mean() >= 0.2, stable.mean()
     assert err[stable].max() <= 1e-6, err[stable].max()
 
 
