@@ -137,9 +137,15 @@ class Records(C.Structure):
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("block_size", C.c_int32), ("ctas_per_sm", C.c_int32),
                 ("steps_per_launch", C.c_int32), ("refill_threshold", C.c_int32),
-                ("_pad0", C.c_int32), ("max_steps", C.c_uint64),
+                ("budget_us", C.c_int32), ("max_steps", C.c_uint64),
                 ("cancel", C.POINTER(C.c_int32)), ("stream", C.c_void_p),
                 ("records", C.POINTER(Records))]
+
+
+class AutotuneResult(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("ctas_per_sm", C.c_int32), ("refill_threshold", C.c_int32),
+                ("burst", C.c_int32), ("trials", C.c_int32), ("_pad0", C.c_int32),
+                ("steps_per_second", _d), ("chunked_steps_per_second", _d)]
 
 
 class RunStats(C.Structure):

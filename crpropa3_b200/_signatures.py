@@ -22,6 +22,8 @@ SIGNATURES = {
     "crp_run_device": (_i32, [_plan_p, C.POINTER(_abi.Candidates), _u64,
                               C.POINTER(_abi.RunOpts), C.POINTER(_abi.RunStats)]),
     "crp_field_eval": (_i32, [_plan_p, _u64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "crp_autotune": (_i32, [_plan_p, C.POINTER(_abi.Candidates), _u64, _u64, _u64, C.c_void_p,
+                            C.POINTER(_abi.AutotuneResult)]),
     "crp_particle_charge": (_i32, [_i32, _dp]),
     "crp_random_draws": (_i32, [_u32, _i32, _u64, _d, _d, _d, _dp]),
     "crp_plane_wave_modes": (_i32, [_d, _d, _d, _d, _d, _d, _i32, _i32, _dp, _dp, _dp, _dp, _dp]),

@@ -234,4 +234,91 @@ __device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, 
     append_active(cnt, perm_out, still, (uint32_t)i);
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Persistent stepping (one launch of SMs x ctas_per_sm CTAs): every lane
+// holds one candidate; a lane whose candidate finishes is refilled from the
+// work queue.  The queue is the virtual list of n_pending indices in
+// pending_in followed by the main index range [main_base, main_base +
+// n_main).  A warp refills once at least `refill` of its lanes are free (the
+// ballot of free lanes ranks them; one atomic per warp reserves their
+// items), runs `burst` chain iterations between refills, and stops after
+// budget_ns of device time: lanes that still hold a candidate then store it
+// and append its index to pending_out (cnt->pending_count), for the next
+// launch.  cnt->queue_head counts the items taken.
+template <class Prop>
+__device__ __forceinline__ void persistent_body(const DevPlan &P, const DevState &s,
+                                                const uint32_t *pending_in, uint64_t n_pending,
+                                                uint64_t main_base, uint64_t n_main,
+                                                uint32_t *pending_out, int burst, int refill,
+                                                unsigned long long budget_ns, uint64_t step_cap,
+                                                DevCounters *cnt, const DevRecords &rec) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint64_t total = n_pending + n_main;
+    const unsigned long long t0 = global_ns();
+    StepCount sc;
+    unsigned long long steps = 0;
+    Cand c;
+    c.cell0 = -1;
+    c.cell7 = -1;
+    bool has = false, exhausted = false;
+    for (;;) {
+        const unsigned freemask = __ballot_sync(full, !has);
+        const int nfree = __popc(freemask);
+        if (!exhausted && nfree > 0 && (nfree >= refill || nfree == 32)) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(&cnt->queue_head, (unsigned long long)nfree);
+            base = __shfl_sync(full, base, 0);
+            if (base + nfree >= total) exhausted = true;
+            if (!has) {
+                const uint64_t t = base + __popc(freemask & ((1u << lane) - 1u));
+                if (t < total) {
+                    const uint64_t i = t < n_pending ? (uint64_t)pending_in[t] : main_base + (t - n_pending);
+                    if (s.active[i] && (step_cap == 0 || (s.steps ? s.steps[i] : 0) < step_cap)) {
+                        load_cand(s, i, c);
+                        has = true;
+                    }
+                }
+            }
+        }
+        if (!__ballot_sync(full, has)) {
+            if (exhausted) break;
+            continue;
+        }
+        if (has) {
+            int k = 0;
+            while (c.active && k < burst && (step_cap == 0 || c.steps < step_cap)) {
+                chain_process<Prop>(P, c, rec, sc);
+                c.steps++;
+                k++;
+            }
+            steps += (unsigned long long)k;
+            if (!c.active || (step_cap != 0 && c.steps >= step_cap)) {
+                store_cand(s, c);
+                has = false;
+            }
+        }
+        bool stop = false;
+        if (lane == 0) stop = global_ns() - t0 > budget_ns;
+        stop = __shfl_sync(full, stop, 0);
+        if (stop) {
+            if (has) store_cand(s, c);
+            const unsigned mask = __ballot_sync(full, has);
+            if (mask) {
+                unsigned long long pb = 0;
+                if (lane == 0) pb = atomicAdd(&cnt->pending_count, (unsigned long long)__popc(mask));
+                pb = __shfl_sync(full, pb, 0);
+                if (has) pending_out[pb + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)c.index;
+            }
+            break;
+        }
+    }
+    flush_counters(cnt, steps, sc);
+}
+
 }  // namespace crp

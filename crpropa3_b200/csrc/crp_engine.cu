@@ -75,6 +75,13 @@ struct crp_plan {
     uint64_t list_cap = 0;
     uint32_t *lists = nullptr;
     int tuned_block = 0;
+    // autotuned launch configuration (crp_autotune); mode 0: not tuned
+    int tuned_mode = 0;
+    int tuned_ctas = 0, tuned_refill = 0, tuned_burst = 0;
+    int num_sms = 0;
+    // device copy of a sample for the autotuner's trials
+    uint64_t trial_n = 0;
+    void *trial = nullptr;
 
     ~crp_plan() {
         for (void *p : owned) cudaFree(p);
@@ -83,6 +90,7 @@ struct crp_plan {
         if (scratch) cudaFree(scratch);
         if (rec_scratch) cudaFree(rec_scratch);
         if (lists) cudaFree(lists);
+        if (trial) cudaFree(trial);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
@@ -336,12 +344,132 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
         p->fs = FS_GENERIC;
     crp_status st = ensure_counters(p);
     if (st) { delete p; return st; }
+    if (cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess)
+        p->num_sms = 148;
     *out = p;
     return CRP_OK;
 }
 
 crp_status crp_plan_destroy(crp_plan *plan) {
     delete plan;
+    return CRP_OK;
+}
+
+// Every array handed to crp_run_device must be reachable from the device:
+// device memory, managed memory, or host memory registered / allocated with
+// CUDA (mapped).  Ordinary host memory would make the kernels fault.
+static crp_status check_device_ptr(const void *ptr, const char *what) {
+    if (!ptr) return CRP_OK;
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CRP_ERR_INVALID_ARGUMENT, "%s: not a CUDA-accessible pointer", what);
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return CRP_OK;
+    if (a.type == cudaMemoryTypeHost && a.devicePointer == ptr) return CRP_OK;
+    return fail(CRP_ERR_INVALID_ARGUMENT,
+                "%s is host memory the device cannot address: pass device arrays to crp_run_device "
+                "(or host arrays to crp_run)", what);
+}
+
+static crp_status check_device_arrays(const crp_candidates *c, const crp_records *r) {
+    const void *const ptrs[] = {c->id, c->charge, c->energy, c->x, c->y, c->z, c->dx, c->dy, c->dz,
+                                c->px, c->py, c->pz, c->trajectory_length, c->time,
+                                c->current_step, c->next_step, c->active, c->flags,
+                                c->max_length, c->step_count};
+    for (const void *q : ptrs) {
+        crp_status st = check_device_ptr(q, "a candidate array");
+        if (st) return st;
+    }
+    if (r) {
+        const void *const rp[] = {r->count, r->index, r->module, r->trajectory_length, r->time,
+                                  r->x, r->y, r->z, r->dx, r->dy, r->dz, r->energy, r->id};
+        for (const void *q : rp) {
+            crp_status st = check_device_ptr(q, "a record array");
+            if (st) return st;
+        }
+    }
+    return CRP_OK;
+}
+
+static crp_status ensure_lists(crp_plan *p, uint64_t n) {
+    if (p->list_cap < n) {
+        if (p->lists) { cudaFree(p->lists); p->lists = nullptr; p->list_cap = 0; }
+        CUDA_TRY(cudaMalloc(&p->lists, sizeof(uint32_t) * 2 * n));
+        p->list_cap = n;
+    }
+    return CRP_OK;
+}
+
+// Persistent mode: bounded launches of SMs x ctas_per_sm CTAs that refill
+// lanes from the device queue; what a launch leaves (lanes still busy at its
+// time budget, queue items not yet taken) is the next launch's queue.
+static crp_status run_persistent(crp_plan *p, const crp_candidates *c, uint64_t n,
+                                 const crp_run_opts &o, crp_run_stats *stats) {
+    cudaStream_t st = (cudaStream_t)o.stream;
+    DevState s = to_dev_state(*c);
+    DevRecords rec = to_dev_records(o.records);
+    const int ctas = o.ctas_per_sm > 0 ? o.ctas_per_sm : (p->tuned_ctas > 0 ? p->tuned_ctas : 2);
+    const int refill = o.refill_threshold > 0 ? o.refill_threshold : (p->tuned_refill > 0 ? p->tuned_refill : 8);
+    const int burst = o.steps_per_launch > 0 ? o.steps_per_launch : (p->tuned_burst > 0 ? p->tuned_burst : 16);
+    if (ctas > 32 || refill > 32) return fail(CRP_ERR_INVALID_ARGUMENT, "ctas_per_sm and refill_threshold must be <= 32");
+    crp_status ls = ensure_lists(p, n);
+    if (ls) return ls;
+    const int grid = p->num_sms * ctas;
+    uint32_t *list_a = p->lists, *list_b = p->lists + p->list_cap;
+    const uint32_t *pending_in = nullptr;
+    uint32_t *pending_out = list_a;
+    uint64_t n_pending = 0, main_base = 0, n_main = n;
+    double ms_total = 0;
+    uint64_t launches = 0;
+    const unsigned long long budget_ns =
+        o.budget_us > 0 ? 1000ull * (unsigned long long)o.budget_us : 200ull * 1000 * 1000;
+    for (;;) {
+        PersistentArgs a{pending_in, n_pending, main_base, n_main, pending_out, burst, refill, budget_ns,
+                         o.max_steps};
+        CUDA_TRY(cudaMemsetAsync(p->d_cnt, 0, sizeof(DevCounters), st));
+        CUDA_TRY(cudaEventRecord(p->ev0, st));
+        cudaError_t e = (p->precision == CRP_PRECISION_FP64)
+            ? launch_fp64_persistent(p->dev, s, a, p->d_cnt, rec, p->fs, grid, st)
+            : launch_mixed_persistent(p->dev, s, a, p->d_cnt, rec, p->fs, grid, st);
+        if (e != cudaSuccess) return cuda_fail(e, "persistent stepping kernel launch");
+        CUDA_TRY(cudaEventRecord(p->ev1, st));
+        CUDA_TRY(cudaMemcpyAsync(p->h_cnt, p->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
+        ms_total += ms;
+        launches++;
+        if (stats) {
+            stats->particle_steps += p->h_cnt->steps;
+            stats->tries += p->h_cnt->tries;
+            stats->field_evaluations += p->h_cnt->field_evals;
+        }
+        const uint64_t total = n_pending + n_main;
+        const uint64_t consumed = p->h_cnt->queue_head < total ? p->h_cnt->queue_head : total;
+        uint64_t next_pending = p->h_cnt->pending_count;
+        if (consumed < n_pending) {
+            // pending items nobody took move behind the new pending list
+            const uint64_t rest = n_pending - consumed;
+            CUDA_TRY(cudaMemcpyAsync(pending_out + next_pending, pending_in + consumed,
+                                     sizeof(uint32_t) * rest, cudaMemcpyDeviceToDevice, st));
+            next_pending += rest;
+        } else {
+            main_base += consumed - n_pending;
+            n_main -= consumed - n_pending;
+        }
+        n_pending = next_pending;
+        pending_in = pending_out;
+        pending_out = (pending_out == list_a) ? list_b : list_a;
+        if (stats) stats->active_left = n_pending + n_main;
+        if (n_pending == 0 && n_main == 0) break;
+        if (o.cancel && *o.cancel) {
+            if (stats) { stats->launches = launches; stats->device_ms = ms_total; }
+            return fail(CRP_ERR_CANCELLED, "run cancelled by the host flag");
+        }
+    }
+    if (stats) { stats->launches = launches; stats->device_ms = ms_total; stats->active_left = 0; }
     return CRP_OK;
 }
 
@@ -360,20 +488,20 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
         return fail(CRP_ERR_INVALID_ARGUMENT, "per-candidate MaximumTrajectoryLength needs max_length");
     if (needs_step_count(p) && !c->step_count)
         return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE needs step_count (random stream counter)");
-    if (o.mode == CRP_MODE_PERSISTENT)
-        return fail(CRP_ERR_UNSUPPORTED, "persistent mode is not available in this build");
     if (n > 0xffffffffull) return fail(CRP_ERR_CAPACITY, "at most 2^32-1 candidates per run");
+    crp_status ps = check_device_arrays(c, o.records);
+    if (ps) return ps;
+    int mode = o.mode;
+    if (mode == CRP_MODE_AUTO) mode = p->tuned_mode ? p->tuned_mode : CRP_MODE_CHUNKED;
+    if (mode == CRP_MODE_PERSISTENT) return run_persistent(p, c, n, o, stats);
     cudaStream_t st = (cudaStream_t)o.stream;
     DevState s = to_dev_state(*c);
     DevRecords rec = to_dev_records(o.records);
     int block = o.block_size > 0 ? o.block_size : (p->tuned_block > 0 ? p->tuned_block : 128);
     if (block % 32 || block > 1024) return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d", block);
     int spl = o.steps_per_launch > 0 ? o.steps_per_launch : 4096;
-    if (p->list_cap < n) {
-        if (p->lists) { cudaFree(p->lists); p->lists = nullptr; p->list_cap = 0; }
-        CUDA_TRY(cudaMalloc(&p->lists, sizeof(uint32_t) * 2 * n));
-        p->list_cap = n;
-    }
+    crp_status ls = ensure_lists(p, n);
+    if (ls) return ls;
     double ms_total = 0;
     uint64_t launches = 0;
     // launch 1 covers every candidate; later launches only the ones the
@@ -503,6 +631,85 @@ crp_status crp_run(crp_plan *p, const crp_candidates *h, uint64_t n, const crp_r
 #undef D2H
     CUDA_TRY(cudaStreamSynchronize(st));
     return rs;
+}
+
+crp_status crp_autotune(crp_plan *p, const crp_candidates *c, uint64_t n, uint64_t sample_n,
+                        uint64_t steps_per_candidate, void *stream, crp_autotune_result *res) {
+    if (!p || !c || !res) return fail(CRP_ERR_INVALID_ARGUMENT, "NULL argument");
+    memset(res, 0, sizeof(*res));
+    if (n == 0) return CRP_OK;
+    const uint64_t m = sample_n == 0 || sample_n > n ? n : sample_n;
+    const uint64_t cap = steps_per_candidate ? steps_per_candidate : 256;
+    cudaStream_t st = (cudaStream_t)stream;
+    // one device block for the trial copy: 17 double / u64 arrays, id, flags, active
+    if (p->trial_n < m) {
+        if (p->trial) { cudaFree(p->trial); p->trial = nullptr; p->trial_n = 0; }
+        CUDA_TRY(cudaMalloc(&p->trial, (17 * 8 + 9) * m + 32 * 256));
+        p->trial_n = m;
+    }
+    char *base = static_cast<char *>(p->trial);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { void *r = base + off; off += (bytes + 255) / 256 * 256; return r; };
+    crp_candidates t{};
+    double **dmem[] = {&t.charge, &t.energy, &t.x, &t.y, &t.z, &t.dx, &t.dy, &t.dz, &t.px, &t.py, &t.pz,
+                       &t.trajectory_length, &t.time, &t.current_step, &t.next_step, &t.max_length};
+    for (double **d : dmem) *d = (double *)take(8 * m);
+    t.step_count = (uint64_t *)take(8 * m);
+    t.id = (int32_t *)take(4 * m);
+    t.flags = (uint32_t *)take(4 * m);
+    t.active = (uint8_t *)take(m);
+    auto reset = [&]() -> crp_status {
+        const double *const src[] = {c->charge, c->energy, c->x, c->y, c->z, c->dx, c->dy, c->dz,
+                                     c->px, c->py, c->pz, c->trajectory_length, c->time,
+                                     c->current_step, c->next_step, c->max_length};
+        for (int k = 0; k < 16; k++) {
+            if (src[k]) CUDA_TRY(cudaMemcpyAsync(*dmem[k], src[k], 8 * m, cudaMemcpyDeviceToDevice, st));
+            else CUDA_TRY(cudaMemsetAsync(*dmem[k], 0, 8 * m, st));
+        }
+        CUDA_TRY(cudaMemsetAsync(t.step_count, 0, 8 * m, st));
+        CUDA_TRY(cudaMemcpyAsync(t.id, c->id, 4 * m, cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(t.flags, c->flags, 4 * m, cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(t.active, c->active, m, cudaMemcpyDeviceToDevice, st));
+        return CRP_OK;
+    };
+    struct Cfg { int mode, ctas, refill, burst; };
+    std::vector<Cfg> cfgs = {{CRP_MODE_CHUNKED, 0, 0, 0}};
+    for (int ctas : {1, 2, 3, 4})
+        for (int refill : {1, 8, 16, 32})
+            for (int burst : {4, 16, 64}) cfgs.push_back({CRP_MODE_PERSISTENT, ctas, refill, burst});
+    double best = -1, chunked = 0;
+    Cfg bestc = cfgs[0];
+    int trials = 0;
+    for (const Cfg &g : cfgs) {
+        crp_status rs = reset();
+        if (rs) return rs;
+        crp_run_opts o{};
+        o.mode = g.mode;
+        o.ctas_per_sm = g.ctas;
+        o.refill_threshold = g.refill;
+        o.steps_per_launch = g.mode == CRP_MODE_PERSISTENT ? g.burst : 0;
+        o.max_steps = cap;
+        o.stream = stream;
+        crp_run_stats rstats{};
+        rs = crp_run_device(p, &t, m, &o, &rstats);
+        if (rs) return rs;
+        trials++;
+        const double rate = rstats.device_ms > 0 ? rstats.particle_steps / (rstats.device_ms * 1e-3) : 0;
+        if (g.mode == CRP_MODE_CHUNKED) chunked = rate;
+        if (rate > best) { best = rate; bestc = g; }
+    }
+    p->tuned_mode = bestc.mode;
+    p->tuned_ctas = bestc.ctas;
+    p->tuned_refill = bestc.refill;
+    p->tuned_burst = bestc.burst;
+    res->mode = bestc.mode;
+    res->ctas_per_sm = bestc.ctas;
+    res->refill_threshold = bestc.refill;
+    res->burst = bestc.burst;
+    res->trials = trials;
+    res->steps_per_second = best;
+    res->chunked_steps_per_second = chunked;
+    return CRP_OK;
 }
 
 crp_status crp_field_eval(crp_plan *p, uint64_t n, const double *pos, double *out, void *stream) {

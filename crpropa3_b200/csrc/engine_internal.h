@@ -17,6 +17,21 @@ enum FieldSig {
     FS_PLANE_WAVE = 2  // one PlaneWaveTurbulence, not wrapped
 };
 
+// Persistent stepping launch (chain.cuh persistent_body): `grid` CTAs of 128
+// threads take work from the virtual queue pending_in[0..n_pending) followed
+// by [main_base, main_base + n_main) until it is empty or budget_ns of
+// device time have passed.
+struct PersistentArgs {
+    const uint32_t *pending_in;
+    uint64_t n_pending;
+    uint64_t main_base;
+    uint64_t n_main;
+    uint32_t *pending_out;
+    int burst;
+    int refill;
+    unsigned long long budget_ns;
+    uint64_t step_cap;
+};
 // step_fp64.cu
 // One launch of the chunked stepping kernel: threads t < n advance candidate
 // perm[t] (t without perm) by at most max_steps chain iterations; candidates
@@ -28,17 +43,17 @@ cudaError_t launch_fp64_chunk(const DevPlan &P, const DevState &s, uint64_t n, i
                               cudaStream_t st);
 cudaError_t launch_fp64_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
                               cudaStream_t st);
+cudaError_t launch_fp64_persistent(const DevPlan &P, const DevState &s, const PersistentArgs &a,
+                                   DevCounters *cnt, const DevRecords &rec, int fs, int grid,
+                                   cudaStream_t st);
 
 // step_mixed.cu
 cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
                                uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
                                const uint32_t *perm, uint32_t *perm_out, int fs, int block,
                                cudaStream_t st);
-cudaError_t launch_mixed_persistent(const DevPlan &P, const DevState &s, uint64_t n,
-                                    uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
-                                    int fs, int block, int grid, int refill,
-                                    unsigned long long deadline_ns, uint32_t *pending_in,
-                                    uint64_t n_pending_in, uint32_t *pending_out,
+cudaError_t launch_mixed_persistent(const DevPlan &P, const DevState &s, const PersistentArgs &a,
+                                    DevCounters *cnt, const DevRecords &rec, int fs, int grid,
                                     cudaStream_t st);
 cudaError_t launch_mixed_field(const DevPlan &P, uint64_t n, const double *pos, double *out,
                                cudaStream_t st);

@@ -466,6 +466,28 @@ __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_chunk_ke
     chunk_body<Prop<FS>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
 }
 
+template <template <int> class Prop, int FS>
+__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_persistent_kernel(
+    DevPlan P, DevState s, const uint32_t *pending_in, uint64_t n_pending, uint64_t main_base,
+    uint64_t n_main, uint32_t *pending_out, int burst, int refill, unsigned long long budget_ns,
+    uint64_t step_cap, DevCounters *cnt, DevRecords rec) {
+    persistent_body<Prop<FS>>(P, s, pending_in, n_pending, main_base, n_main, pending_out, burst,
+                              refill, budget_ns, step_cap, cnt, rec);
+}
+
+template <template <int> class Prop>
+cudaError_t launch_persistent_prop(const DevPlan &P, const DevState &s, const PersistentArgs &a,
+                                   DevCounters *cnt, const DevRecords &rec, int fs, int grid,
+                                   cudaStream_t st) {
+#define CRP_PERSIST(FSV) fp64_persistent_kernel<Prop, FSV><<<grid, 128, 0, st>>>(P, s, a.pending_in, \
+        a.n_pending, a.main_base, a.n_main, a.pending_out, a.burst, a.refill, a.budget_ns, a.step_cap, cnt, rec)
+    if (fs == FS_GRID) CRP_PERSIST(FS_GRID);
+    else if (fs == FS_PLANE_WAVE) CRP_PERSIST(FS_PLANE_WAVE);
+    else CRP_PERSIST(FS_GENERIC);
+#undef CRP_PERSIST
+    return cudaGetLastError();
+}
+
 __global__ void fp64_field_kernel(DevPlan P, uint64_t n, const double *pos, double *out) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -505,6 +527,20 @@ cudaError_t launch_fp64_chunk(const DevPlan &P, const DevState &s, uint64_t n, i
         return fixed ? launch_prop<CKFixed>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st)
                      : launch_prop<CKAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
     return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+}
+
+cudaError_t launch_fp64_persistent(const DevPlan &P, const DevState &s, const PersistentArgs &a,
+                                   DevCounters *cnt, const DevRecords &rec, int fs, int grid,
+                                   cudaStream_t st) {
+    const DevModule &pm = P.modules[P.prop_index];
+    const bool fixed = pm.min_step == pm.max_step;
+    if (pm.propagator == CRP_PROP_BP)
+        return fixed ? launch_persistent_prop<BPFixed>(P, s, a, cnt, rec, fs, grid, st)
+                     : launch_persistent_prop<BPAdaptive>(P, s, a, cnt, rec, fs, grid, st);
+    if (pm.propagator == CRP_PROP_CK)
+        return fixed ? launch_persistent_prop<CKFixed>(P, s, a, cnt, rec, fs, grid, st)
+                     : launch_persistent_prop<CKAdaptive>(P, s, a, cnt, rec, fs, grid, st);
+    return launch_persistent_prop<SDE>(P, s, a, cnt, rec, fs, grid, st);
 }
 
 cudaError_t launch_fp64_field(const DevPlan &P, uint64_t n, const double *pos, double *out,

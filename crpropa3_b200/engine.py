@@ -47,10 +47,11 @@ class Plan:
     @staticmethod
     def _opts(mode=_abi.MODE_AUTO, block_size=0, steps_per_launch=0, max_steps=0, stream=None,
               records: Optional[RecordArrays] = None, cancel=None, ctas_per_sm=0,
-              refill_threshold=0):
+              refill_threshold=0, budget_us=0):
         o = _abi.RunOpts()
         o.mode, o.block_size, o.steps_per_launch = mode, block_size, steps_per_launch
         o.max_steps, o.ctas_per_sm, o.refill_threshold = max_steps, ctas_per_sm, refill_threshold
+        o.budget_us = budget_us
         o.stream = stream
         keep = []
         if records is not None:
@@ -70,6 +71,16 @@ class Plan:
         _abi.check(fn(self.handle, C.byref(s), cands.n, C.byref(o), C.byref(stats)))
         del keep
         return stats
+
+    def autotune(self, device_cands: CandidateArrays, sample_n=1 << 17, steps_per_candidate=256,
+                 stream=None) -> _abi.AutotuneResult:
+        """Time launch configurations on a sample of device candidates; the
+        best is used by later runs in MODE_AUTO (crp_autotune)."""
+        res = _abi.AutotuneResult()
+        s = device_cands.struct()
+        _abi.check(self.lib.crp_autotune(self.handle, C.byref(s), device_cands.n, sample_n,
+                                         steps_per_candidate, stream, C.byref(res)))
+        return res
 
     def field(self, pos) -> np.ndarray:
         """Field of the plan at positions (n, 3) [m] -> (n, 3) [T], on the device."""

@@ -109,9 +109,9 @@ def grid_turbulence(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.
         if use_torch:
             import torch
             t = torch.from_numpy(arr).to(device)
-            comps.append(torch.fft.irfftn(t, s=(n, n, n)).cpu().numpy().astype(np.float32))
+            comps.append(torch.fft.irfftn(t, s=(n, n, n), dim=(0, 1, 2)).cpu().numpy().astype(np.float32))
         else:
-            comps.append(np.fft.irfftn(arr, s=(n, n, n)).astype(np.float32))
+            comps.append(np.fft.irfftn(arr, s=(n, n, n), axes=(0, 1, 2)).astype(np.float32))
     g = np.stack(comps, axis=-1).astype(np.float32)
     g64 = g.astype(np.float64)
     rms = math.sqrt(float((g64 * g64).sum()) / (n * n * n))

@@ -216,7 +216,7 @@ typedef struct crp_run_opts {
     int32_t ctas_per_sm;       /* 0: autotuned (persistent mode) */
     int32_t steps_per_launch;  /* 0: default (chunked mode) */
     int32_t refill_threshold;  /* persistent: lanes idle before a warp refills, 0: autotuned */
-    int32_t _pad0;
+    int32_t budget_us;         /* persistent: device time per launch [us], 0: 200 ms */
     uint64_t max_steps;        /* per-candidate cap on accepted steps, 0: none */
     volatile int32_t *cancel;  /* host flag polled between launches, may be NULL */
     void *stream;              /* cudaStream_t, NULL: the legacy default stream */
@@ -254,6 +254,28 @@ crp_status crp_run(crp_plan *plan, const crp_candidates *host, uint64_t n,
  * only where stats is NULL and no cancel flag is given. */
 crp_status crp_run_device(crp_plan *plan, const crp_candidates *device, uint64_t n,
                           const crp_run_opts *opts, crp_run_stats *stats);
+
+/* Launch-configuration autotuner.  Times short trials (at most
+ * steps_per_candidate chain iterations each) on up to sample_n candidates
+ * copied from the device arrays `device` (which stay unchanged): the chunked
+ * launch, and persistent launches over CTAs per SM, refill threshold and
+ * burst length.  The fastest is stored in the plan and used by runs whose
+ * mode is CRP_MODE_AUTO; *result reports it.  No reference counterpart (the
+ * reference's OpenMP schedule is fixed at build time, CMakeLists.txt:206). */
+typedef struct crp_autotune_result {
+    int32_t mode;              /* crp_run_mode chosen */
+    int32_t ctas_per_sm;
+    int32_t refill_threshold;
+    int32_t burst;             /* chain iterations between refills */
+    int32_t trials;
+    int32_t _pad0;
+    double steps_per_second;   /* of the chosen configuration on the sample */
+    double chunked_steps_per_second;
+} crp_autotune_result;
+
+crp_status crp_autotune(crp_plan *plan, const crp_candidates *device, uint64_t n,
+                        uint64_t sample_n, uint64_t steps_per_candidate, void *stream,
+                        crp_autotune_result *result);
 
 /* Field of the plan (sum of its components) at n positions (device arrays,
  * planar x[n] y[n] z[n] in and out).  MagneticField::getField. */

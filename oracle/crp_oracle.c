@@ -769,3 +769,167 @@ int oracle_run(const crp_plan_desc *d, const crp_candidates *a, uint64_t n, crp_
     if (tries_out) *tries_out = tries;
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Adjoint of the fixed-step Boris push (no reference counterpart)
+ *
+ * Forward model (the differentiable one): PropagationBP::dY
+ * (PropagationBP.cpp:19) with the Grid3f values taken as doubles and the
+ * trilinear weights in double (the corner order of Grid.h:571), then the
+ * direction normalised.  Loss per candidate: 1 - u_final . target.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    const float *g;
+    int nx, ny, nz;
+    double go[3], s[3];
+} adj_grid_t;
+
+static void adj_cell(const adj_grid_t *G, v3 x, size_t idx[8], double w[8], double dw[8][3]) {
+    double r[3] = {(x.x - G->go[0]) / G->s[0], (x.y - G->go[1]) / G->s[1], (x.z - G->go[2]) / G->s[2]};
+    int n[3] = {G->nx, G->ny, G->nz}, lo[3], hi[3];
+    double f0[3], f1[3];
+    for (int a = 0; a < 3; a++) {
+        double fl = floor(r[a]);
+        lo[a] = (((int)fl % n[a]) + n[a]) % n[a];
+        hi[a] = (lo[a] + 1) % n[a];
+        f0[a] = r[a] - fl;
+        f1[a] = 1 - f0[a];
+    }
+    const int sel[8][3] = {{0,0,0},{1,0,0},{0,1,0},{0,0,1},{1,0,1},{0,1,1},{1,1,0},{1,1,1}};
+    for (int k = 0; k < 8; k++) {
+        int ix = sel[k][0] ? hi[0] : lo[0], iy = sel[k][1] ? hi[1] : lo[1], iz = sel[k][2] ? hi[2] : lo[2];
+        idx[k] = ((size_t)ix * G->ny + (size_t)iy) * G->nz + (size_t)iz;
+        double wx = sel[k][0] ? f0[0] : f1[0], wy = sel[k][1] ? f0[1] : f1[1], wz = sel[k][2] ? f0[2] : f1[2];
+        double sx = (sel[k][0] ? 1.0 : -1.0) / G->s[0], sy = (sel[k][1] ? 1.0 : -1.0) / G->s[1],
+               sz = (sel[k][2] ? 1.0 : -1.0) / G->s[2];
+        w[k] = wx * wy * wz;
+        dw[k][0] = sx * wy * wz;
+        dw[k][1] = wx * sy * wz;
+        dw[k][2] = wx * wy * sz;
+    }
+}
+
+static v3 adj_field(const adj_grid_t *G, v3 x) {
+    size_t idx[8];
+    double w[8], dw[8][3];
+    adj_cell(G, x, idx, w, dw);
+    v3 B = mk(0, 0, 0);
+    for (int k = 0; k < 8; k++) {
+        const float *c = G->g + 3 * idx[k];
+        B.x += w[k] * (double)c[0];
+        B.y += w[k] * (double)c[1];
+        B.z += w[k] * (double)c[2];
+    }
+    return B;
+}
+
+static void adj_step(const adj_grid_t *G, v3 *x, v3 *u, double hh, double kappa) {
+    v3 x1 = add(*x, muls(*u, hh));
+    v3 B = adj_field(G, x1);
+    v3 t = muls(B, kappa);
+    double D = 1 + dot(t, t);
+    v3 s = muls(t, 2 / D);
+    v3 v = add(*u, cross(*u, t));
+    v3 u2 = add(*u, cross(v, s));
+    *x = add(x1, muls(u2, hh));
+    *u = divs(u2, norm(u2));
+}
+
+/* Loss and gradients for n candidates (position, direction, energy,
+ * charge, target interleaved xyz): fixed step h, n_steps steps.  grad_grid
+ * (3 doubles per cell) is accumulated (+=), may be NULL. */
+int oracle_bp_adjoint(const float *grid, int nx, int ny, int nz, const double *origin,
+                      const double *spacing, double h, int n_steps, uint64_t n, const double *pos,
+                      const double *dir, const double *energy, const double *charge,
+                      const double *target, double *loss, double *grad_dir, double *grad_energy,
+                      double *grad_grid) {
+    adj_grid_t G = {grid, nx, ny, nz,
+                    {origin[0] + spacing[0] / 2, origin[1] + spacing[1] / 2, origin[2] + spacing[2] / 2},
+                    {spacing[0], spacing[1], spacing[2]}};
+    const double hh = h / 2;
+    v3 *xs = (v3 *)malloc(sizeof(v3) * (size_t)(n_steps + 1));
+    v3 *us = (v3 *)malloc(sizeof(v3) * (size_t)(n_steps + 1));
+    if (!xs || !us) { free(xs); free(us); return 1; }
+    for (uint64_t i = 0; i < n; i++) {
+        double kappa = charge[i] * h * c_light / (2 * energy[i]);
+        xs[0] = mk(pos[3*i], pos[3*i+1], pos[3*i+2]);
+        us[0] = mk(dir[3*i], dir[3*i+1], dir[3*i+2]);
+        for (int k = 0; k < n_steps; k++) {
+            xs[k + 1] = xs[k]; us[k + 1] = us[k];
+            adj_step(&G, &xs[k + 1], &us[k + 1], hh, kappa);
+        }
+        v3 tg = mk(target[3*i], target[3*i+1], target[3*i+2]);
+        if (loss) loss[i] = 1 - dot(us[n_steps], tg);
+        v3 xb = mk(0, 0, 0), ub = muls(tg, -1.0);
+        double kb = 0;
+        for (int k = n_steps - 1; k >= 0; k--) {
+            v3 x = xs[k], u = us[k];
+            /* recompute the step's intermediates */
+            v3 x1 = add(x, muls(u, hh));
+            size_t idx[8];
+            double w[8], dw[8][3];
+            adj_cell(&G, x1, idx, w, dw);
+            v3 B = mk(0, 0, 0);
+            for (int q = 0; q < 8; q++) {
+                const float *c = G.g + 3 * idx[q];
+                B.x += w[q] * (double)c[0]; B.y += w[q] * (double)c[1]; B.z += w[q] * (double)c[2];
+            }
+            v3 t = muls(B, kappa);
+            double D = 1 + dot(t, t);
+            v3 s = muls(t, 2 / D);
+            v3 v = add(u, cross(u, t));
+            v3 u2 = add(u, cross(v, s));
+            double nn = norm(u2);
+            v3 un = divs(u2, nn);
+            /* reverse */
+            v3 u2b = divs(sub(ub, muls(un, dot(un, ub))), nn);
+            v3 x1b = xb;
+            u2b = add(u2b, muls(xb, hh));
+            v3 ubar = u2b;
+            v3 vb = cross(s, u2b);
+            v3 sb = cross(u2b, v);
+            ubar = add(ubar, add(vb, cross(t, vb)));
+            v3 tb = cross(vb, u);
+            tb = add(tb, sub(muls(sb, 2 / D), muls(t, 4 * dot(t, sb) / (D * D))));
+            v3 Bb = muls(tb, kappa);
+            kb += dot(tb, B);
+            for (int q = 0; q < 8; q++) {
+                const float *c = G.g + 3 * idx[q];
+                double gdot = Bb.x * (double)c[0] + Bb.y * (double)c[1] + Bb.z * (double)c[2];
+                x1b.x += gdot * dw[q][0]; x1b.y += gdot * dw[q][1]; x1b.z += gdot * dw[q][2];
+                if (grad_grid) {
+                    grad_grid[3 * idx[q]] += w[q] * Bb.x;
+                    grad_grid[3 * idx[q] + 1] += w[q] * Bb.y;
+                    grad_grid[3 * idx[q] + 2] += w[q] * Bb.z;
+                }
+            }
+            xb = x1b;
+            ubar = add(ubar, muls(x1b, hh));
+            ub = ubar;
+        }
+        grad_dir[3*i] = ub.x; grad_dir[3*i+1] = ub.y; grad_dir[3*i+2] = ub.z;
+        /* kappa = q h c / (2E): d kappa / dE = -kappa / E */
+        grad_energy[i] = kb * (-kappa / energy[i]);
+    }
+    free(xs);
+    free(us);
+    return 0;
+}
+
+/* Loss only, same forward model (for central finite differences). */
+double oracle_bp_loss(const float *grid, int nx, int ny, int nz, const double *origin,
+                      const double *spacing, double h, int n_steps, uint64_t n, const double *pos,
+                      const double *dir, const double *energy, const double *charge,
+                      const double *target) {
+    adj_grid_t G = {grid, nx, ny, nz,
+                    {origin[0] + spacing[0] / 2, origin[1] + spacing[1] / 2, origin[2] + spacing[2] / 2},
+                    {spacing[0], spacing[1], spacing[2]}};
+    double L = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        double kappa = charge[i] * h * c_light / (2 * energy[i]);
+        v3 x = mk(pos[3*i], pos[3*i+1], pos[3*i+2]), u = mk(dir[3*i], dir[3*i+1], dir[3*i+2]);
+        for (int k = 0; k < n_steps; k++) adj_step(&G, &x, &u, h / 2, kappa);
+        L += 1 - dot(u, mk(target[3*i], target[3*i+1], target[3*i+2]));
+    }
+    return L;
+}
