@@ -222,6 +222,55 @@ def run_reference_arm(args):
     return 0
 
 
+def adjoint_cost(dev, args):
+    """Adjoint of the fixed-step Boris push, backtracking workload: 10^5
+    antiprotons, log-uniform 5-50 EeV, through a 128^3 Kolmogorov Grid3f (10
+    kpc, periodic, Brms 3 nG), 2000 steps of 1 kpc, checkpoints every 100
+    steps; loss sum(1 - cos) to seeded random targets; gradients w.r.t. the
+    initial momenta and all grid values.  Cost = (adjoint call) / (forward
+    call), both CUDA-event timed, best of 3 after a warm-up."""
+    import torch
+    from crpropa3_b200 import units as U
+    from crpropa3_b200.adjoint import bp_adjoint_backward, bp_adjoint_forward, bp_forward_loss
+    from crpropa3_b200.turbulence import grid_turbulence
+    n, steps, k = 100_000, 2000, 100
+    rng = np.random.default_rng(4)
+    grid = torch.from_numpy(grid_turbulence(128, 10 * U.kpc, 3 * U.nG, 20 * U.kpc, 1280 * U.kpc,
+                                            seed=42, device=dev)).to(dev)
+    u0 = rng.standard_normal((n, 3))
+    u0 /= np.linalg.norm(u0, axis=1)[:, None]
+    tg = rng.standard_normal((n, 3))
+    tg /= np.linalg.norm(tg, axis=1)[:, None]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    e = t(np.exp(rng.uniform(np.log(5), np.log(50), n)) * U.EeV)
+    q = t(np.full(n, -U.eplus))
+    pos, u0, tg = t(np.zeros((n, 3))), t(u0), t(tg)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()
+        best = None
+        for _ in range(3):
+            torch.cuda.synchronize()
+            ev0.record()
+            fn()
+            ev1.record()
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            best = ms if best is None else min(best, ms)
+        return best
+    args6 = (grid, (0, 0, 0), 10 * U.kpc, U.kpc, steps, pos, u0, e, q, tg)
+    f_ms = timed(lambda: bp_forward_loss(*args6))
+    fc_ms = timed(lambda: bp_adjoint_forward(*args6, k))
+    tape = bp_adjoint_forward(*args6, k)
+    b_ms = timed(lambda: bp_adjoint_backward(tape))
+    return {"workload": "10^5 antiprotons 5-50 EeV, 128^3 Grid3f 3 nG 10 kpc, 2000 x 1 kpc Boris, K=100",
+            "forward_ms": f_ms, "forward_checkpointed_ms": fc_ms, "backward_ms": b_ms,
+            "cost_ratio": b_ms / f_ms, "cost_ratio_with_checkpointed_forward": (fc_ms + b_ms) / f_ms,
+            "definition": "cost_ratio = reverse pass (recompute from checkpoints + adjoint) / plain forward",
+            "forward_particle_steps_per_s": n * steps / (f_ms / 1e3)}
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -235,6 +284,7 @@ def main():
     ap.add_argument("--track", type=int, default=5000, help="steps per candidate (1 kpc each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=0)
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--uniform-start", action="store_true",
                     help="start candidates uniformly over the grid volume (profiling case)")
     args = ap.parse_args()
@@ -384,6 +434,8 @@ def main():
                 "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
                 "basis": "96 B (8 corners x 12 B) per particle-step over the stepping kernel time"}
 
+    adjoint = None if args.no_adjoint else adjoint_cost(dev, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = cpu_threads()
@@ -420,6 +472,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": d2h, "api": "crp_run (host arrays, pinned)"},
             "roofline": roofline,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),

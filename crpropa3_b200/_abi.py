@@ -142,6 +142,18 @@ class RunOpts(C.Structure):
                 ("records", C.POINTER(Records))]
 
 
+class AdjointDesc(C.Structure):
+    _fields_ = [("grid_values", C.c_void_p), ("nx", C.c_uint64), ("ny", C.c_uint64),
+                ("nz", C.c_uint64), ("origin", _d * 3), ("spacing", _d * 3), ("step", _d),
+                ("n_steps", C.c_int32), ("checkpoint_every", C.c_int32)]
+
+
+class AdjointIO(C.Structure):
+    _fields_ = [("n", C.c_uint64)] + [(k, C.c_void_p) for k in (
+        "x", "y", "z", "dx", "dy", "dz", "energy", "charge", "tx", "ty", "tz", "loss", "ux", "uy",
+        "uz", "grad_dx", "grad_dy", "grad_dz", "grad_energy", "grad_grid")]
+
+
 class AutotuneResult(C.Structure):
     _fields_ = [("mode", C.c_int32), ("ctas_per_sm", C.c_int32), ("refill_threshold", C.c_int32),
                 ("burst", C.c_int32), ("trials", C.c_int32), ("_pad0", C.c_int32),

@@ -25,6 +25,14 @@ SIGNATURES = {
     "crp_autotune": (_i32, [_plan_p, C.POINTER(_abi.Candidates), _u64, _u64, _u64, C.c_void_p,
                             C.POINTER(_abi.AutotuneResult)]),
     "crp_particle_charge": (_i32, [_i32, _dp]),
+    "crp_bp_adjoint_workspace": (_i32, [C.POINTER(_abi.AdjointDesc), _u64, C.POINTER(C.c_size_t)]),
+    "crp_bp_forward_loss": (_i32, [C.POINTER(_abi.AdjointDesc), C.POINTER(_abi.AdjointIO), C.c_void_p]),
+    "crp_bp_adjoint": (_i32, [C.POINTER(_abi.AdjointDesc), C.POINTER(_abi.AdjointIO), C.c_void_p,
+                              C.c_size_t, C.c_void_p]),
+    "crp_bp_adjoint_forward": (_i32, [C.POINTER(_abi.AdjointDesc), C.POINTER(_abi.AdjointIO),
+                                      C.c_void_p, C.c_size_t, C.c_void_p]),
+    "crp_bp_adjoint_backward": (_i32, [C.POINTER(_abi.AdjointDesc), C.POINTER(_abi.AdjointIO),
+                                       C.c_void_p, C.c_size_t, C.c_void_p]),
     "crp_random_draws": (_i32, [_u32, _i32, _u64, _d, _d, _d, _dp]),
     "crp_plane_wave_modes": (_i32, [_d, _d, _d, _d, _d, _d, _i32, _i32, _dp, _dp, _dp, _dp, _dp]),
     "crp_source_sample": (_i32, [C.c_void_p, _u32, _u64, _i32p, _dp, _dp]),

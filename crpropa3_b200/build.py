@@ -27,7 +27,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUD
 SOURCES = {
     "step_fp64.cu": ["-fmad=false"],
     "step_mixed.cu": [],
-    "adjoint.cu": ["-fmad=false"],
+    "adjoint.cu": [],
     "persistent.cu": [],
     "turbulence.cu": [],
     "crp_engine.cu": [],

@@ -283,6 +283,58 @@ crp_status crp_field_eval(crp_plan *plan, uint64_t n, const double *pos_xyz,
                           double *b_xyz, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Adjoint of the fixed-step Boris push (no reference counterpart)
+ * ---------------------------------------------------------------------- */
+
+/* Forward model: PropagationBP::dY (PropagationBP.cpp:19) with fixed step
+ * `step` over one periodic Grid3f, the grid values taken as doubles with
+ * double trilinear weights (the corner order of Grid.h:571), the direction
+ * normalised after each step; n_steps steps.  Loss per candidate:
+ * 1 - u_final . target.  The adjoint recomputes segments of
+ * checkpoint_every (<= 128) steps from FP64 checkpoints. */
+typedef struct crp_adjoint_desc {
+    const float *grid_values; /* DEVICE pointer, Vector3f cells */
+    uint64_t nx, ny, nz;
+    double origin[3];
+    double spacing[3];
+    double step;              /* [m] */
+    int32_t n_steps;
+    int32_t checkpoint_every;
+} crp_adjoint_desc;
+
+/* Device arrays of n candidates (planar components). */
+typedef struct crp_adjoint_io {
+    uint64_t n;
+    const double *x, *y, *z;       /* initial position [m] */
+    const double *dx, *dy, *dz;    /* initial direction (unit) */
+    const double *energy, *charge; /* [J], [C] */
+    const double *tx, *ty, *tz;    /* target directions */
+    double *loss;                  /* out: 1 - u_final . target */
+    double *ux, *uy, *uz;          /* out: final direction (may be NULL) */
+    double *grad_dx, *grad_dy, *grad_dz; /* out: dL/du0 */
+    double *grad_energy;           /* out: dL/dE */
+    double *grad_grid;             /* out: dL/d(grid value), nx*ny*nz*3, may be NULL */
+} crp_adjoint_io;
+
+/* Bytes of device workspace crp_bp_adjoint needs for n candidates. */
+crp_status crp_bp_adjoint_workspace(const crp_adjoint_desc *desc, uint64_t n, size_t *bytes);
+/* Forward pass only: loss (and final directions). */
+crp_status crp_bp_forward_loss(const crp_adjoint_desc *desc, const crp_adjoint_io *io, void *stream);
+/* Forward pass with checkpoints, then the reverse pass: loss and gradients.
+ * The grid gradient is summed with 64-bit fixed-point atomics (unit
+ * 2^-36 max|kappa|, kappa = q step c / 2E), so it is the same bits on every
+ * run. */
+crp_status crp_bp_adjoint(const crp_adjoint_desc *desc, const crp_adjoint_io *io, void *workspace,
+                          size_t workspace_bytes, void *stream);
+/* The two halves of crp_bp_adjoint: the forward pass that writes loss and
+ * checkpoints into the workspace, and the reverse pass that reads them (same
+ * desc, inputs and workspace, nothing changed in between). */
+crp_status crp_bp_adjoint_forward(const crp_adjoint_desc *desc, const crp_adjoint_io *io,
+                                  void *workspace, size_t workspace_bytes, void *stream);
+crp_status crp_bp_adjoint_backward(const crp_adjoint_desc *desc, const crp_adjoint_io *io,
+                                   void *workspace, size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
  * Allocation-free run
  * ---------------------------------------------------------------------- */
 

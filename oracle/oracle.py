@@ -62,6 +62,12 @@ class Oracle:
                                              C.POINTER(C.c_int32), _dp, C.c_double, C.c_double,
                                              C.c_double, C.POINTER(C.c_int32), _dp, _dp]
         lib.oracle_philox_block.argtypes = [C.POINTER(C.c_uint32)] * 3
+        adj = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_int,
+               C.c_uint64, _dp, _dp, _dp, _dp, _dp]
+        lib.oracle_bp_adjoint.argtypes = adj + [_dp, _dp, _dp, _dp]
+        lib.oracle_bp_adjoint.restype = C.c_int
+        lib.oracle_bp_loss.argtypes = adj
+        lib.oracle_bp_loss.restype = C.c_double
         self.lib = lib
 
     def run(self, spec, cands: CandidateArrays, records: RecordArrays = None, threads=0,
@@ -105,6 +111,27 @@ class Oracle:
                                              out_id.ctypes.data_as(C.POINTER(C.c_int32)),
                                              _dptr(e), _dptr(d)) == 0
         return out_id, e, d.reshape(n, 3)
+
+    def _adj_args(self, grid, origin, spacing, step, n_steps, pos, u0, energy, charge, target):
+        g = np.ascontiguousarray(grid, dtype=np.float32)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (origin, (spacing,) * 3, pos, u0, energy, charge, target)]
+        self._keep = (g, arrs)
+        o, sp, p, u, e, q, t = arrs
+        return (g.ctypes.data_as(C.POINTER(C.c_float)), g.shape[0], g.shape[1], g.shape[2], _dptr(o), _dptr(sp),
+                float(step), int(n_steps), len(e), _dptr(p), _dptr(u), _dptr(e), _dptr(q), _dptr(t))
+
+    def bp_adjoint(self, grid, origin, spacing, step, n_steps, pos, u0, energy, charge, target):
+        """CPU reference adjoint: (loss per candidate, dL/du0, dL/dE, dL/dgrid)."""
+        n = len(energy)
+        loss, gu, ge = np.zeros(n), np.zeros(3 * n), np.zeros(n)
+        gg = np.zeros(np.asarray(grid).shape, dtype=np.float64)
+        args = self._adj_args(grid, origin, spacing, step, n_steps, pos, u0, energy, charge, target)
+        assert self.lib.oracle_bp_adjoint(*args, _dptr(loss), _dptr(gu), _dptr(ge), _dptr(gg)) == 0
+        return loss, gu.reshape(n, 3), ge, gg
+
+    def bp_loss(self, grid, origin, spacing, step, n_steps, pos, u0, energy, charge, target):
+        return self.lib.oracle_bp_loss(*self._adj_args(grid, origin, spacing, step, n_steps, pos, u0,
+                                                       energy, charge, target))
 
     def philox(self, ctr, key):
         c = (C.c_uint32 * 4)(*ctr)
