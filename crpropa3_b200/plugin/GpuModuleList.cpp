@@ -1,0 +1,791 @@
+// GpuModuleList.cpp -- chain translation, candidate packing, device run
+// through crp_gpu.h, write-back and host replay of the chain's actions.
+#include "GpuModuleList.h"
+
+#include "crp_gpu.h"
+
+#include "crpropa/Geometry.h"
+#include "crpropa/Grid.h"
+#include "crpropa/magneticField/MagneticFieldGrid.h"
+#include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
+#include "crpropa/module/BreakCondition.h"
+#include "crpropa/module/DiffusionSDE.h"
+#include "crpropa/module/Observer.h"
+#include "crpropa/module/PropagationBP.h"
+#include "crpropa/module/PropagationCK.h"
+
+#include <cxxabi.h>
+#include <signal.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <sstream>
+#include <stdexcept>
+#include <typeinfo>
+#include <vector>
+
+using namespace crpropa;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Members the reference keeps private or protected without a getter.  An
+// explicit instantiation may name any member regardless of access
+// ([temp.explicit]); the friend function it defines hands out the member
+// pointer.  Each use names the member exactly as the reference header
+// declares it, so a change there fails this build instead of misreading.
+template <typename Tag, typename Tag::type M>
+struct Expose {
+    friend typename Tag::type member(Tag) { return M; }
+};
+
+#define CRPGPU_MEMBER(TAG, CLASS, TYPE, NAME)      \
+    struct TAG {                                    \
+        typedef TYPE CLASS::*type;                  \
+        friend type member(TAG);                    \
+    };                                              \
+    template struct Expose<TAG, &CLASS::NAME>
+
+typedef std::vector<ref_ptr<ObserverFeature> > FeatureList;
+typedef std::vector<ref_ptr<MagneticField> > FieldVector;
+
+CRPGPU_MEMBER(ObserverFeatures, Observer, FeatureList, features);       // Observer.h:48
+CRPGPU_MEMBER(ObserverAction, Observer, ref_ptr<Module>, detectionAction);
+CRPGPU_MEMBER(ObserverClone, Observer, bool, clone);
+CRPGPU_MEMBER(ObserverInactive, Observer, bool, makeInactive);
+CRPGPU_MEMBER(ObserverFlagKey, Observer, std::string, flagKey);         // Observer.h:45
+CRPGPU_MEMBER(ObserverFlagValue, Observer, std::string, flagValue);
+CRPGPU_MEMBER(SurfaceOf, ObserverSurface, ref_ptr<Surface>, surface);  // Observer.h:92
+CRPGPU_MEMBER(SphereCenter, Sphere, Vector3d, center);                 // Geometry.h:61
+CRPGPU_MEMBER(SphereRadius, Sphere, double, radius);
+CRPGPU_MEMBER(ListFields, MagneticFieldList, FieldVector, fields);     // MagneticField.h:82
+CRPGPU_MEMBER(PeriodicInner, PeriodicMagneticField, ref_ptr<MagneticField>, field);  // :48
+CRPGPU_MEMBER(WavesNm, PlaneWaveTurbulence, int, Nm);                  // PlaneWaveTurbulence.h:93
+CRPGPU_MEMBER(WavesXi, PlaneWaveTurbulence, std::vector<Vector3d>, xi);
+CRPGPU_MEMBER(WavesKappa, PlaneWaveTurbulence, std::vector<Vector3d>, kappa);
+CRPGPU_MEMBER(WavesBeta, PlaneWaveTurbulence, std::vector<double>, beta);
+CRPGPU_MEMBER(WavesAk, PlaneWaveTurbulence, std::vector<double>, Ak);
+CRPGPU_MEMBER(WavesK, PlaneWaveTurbulence, std::vector<double>, k);
+CRPGPU_MEMBER(RejectAction, AbstractCondition, ref_ptr<Module>, rejectAction);  // Module.h:39
+CRPGPU_MEMBER(RejectInactive, AbstractCondition, bool, makeRejectedInactive);
+CRPGPU_MEMBER(RejectKey, AbstractCondition, std::string, rejectFlagKey);
+CRPGPU_MEMBER(RejectValue, AbstractCondition, std::string, rejectFlagValue);
+// ParticleState::setDirection normalises (ParticleState.cpp:30); the device
+// already wrote the normalised direction the reference would hold, and a
+// second normalisation can move its last bit.
+CRPGPU_MEMBER(StateDirection, ParticleState, Vector3d, direction);     // ParticleState.h:27
+
+#undef CRPGPU_MEMBER
+
+static_assert(sizeof(Vector3f) == 12, "Grid3f cells must be three packed floats (crp_grid3f_desc)");
+
+struct Unsupported : std::runtime_error {
+    explicit Unsupported(const std::string &m) : std::runtime_error(m) {}
+};
+
+std::string type_name(const void *obj, const std::type_info &ti) {
+    (void)obj;
+    int st = 0;
+    char *d = abi::__cxa_demangle(ti.name(), 0, 0, &st);
+    std::string s = (st == 0 && d) ? d : ti.name();
+    free(d);
+    return s;
+}
+
+template <class T>
+std::string name_of(const T *obj) {
+    return type_name(obj, typeid(*obj));
+}
+
+std::string crp_error(crp_status st) {
+    char buf[512];
+    buf[0] = 0;
+    crp_last_error(buf, sizeof(buf));
+    std::ostringstream os;
+    os << "GpuModuleList: device path failed (status " << int(st) << "): " << buf;
+    return os.str();
+}
+
+void check(crp_status st) {
+    if (st != CRP_OK) throw std::runtime_error(crp_error(st));
+}
+
+// One chain module's host-side actions, replayed from the device's records.
+struct Action {
+    int kind;  // CRP_MODULE_MAX_TRAJECTORY_LENGTH or CRP_MODULE_OBSERVER
+    const AbstractCondition *condition;
+    const Observer *observer;
+};
+
+struct PeriodicWrap {
+    Vector3d origin, extends;
+    bool reflective;
+};
+
+// 64-bit FNV-1a over bytes, and a word-wise mix for large payloads.
+struct Fingerprint {
+    uint64_t h;
+    Fingerprint() : h(1469598103934665603ull) {}
+    void bytes(const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        for (size_t i = 0; i < n; i++) h = (h ^ c[i]) * 1099511628211ull;
+    }
+    template <class T>
+    void value(const T &v) { bytes(&v, sizeof(v)); }
+    void words(const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        size_t w = n / 8;
+        uint64_t a = h;
+        for (size_t i = 0; i < w; i++) {
+            uint64_t x;
+            std::memcpy(&x, c + 8 * i, 8);
+            a = (a ^ x) * 0x9E3779B97F4A7C15ull;
+            a ^= a >> 29;
+        }
+        h = a;
+        bytes(c + 8 * w, n - 8 * w);
+    }
+};
+
+struct Translation {
+    std::vector<crp_field_component> fields;
+    std::vector<crp_module_desc> modules;
+    std::vector<Action> actions;  // one per modules[] entry
+    std::deque<std::vector<double> > storage;  // push_back keeps references valid
+    std::string perCandidateKey;
+    bool hasPropagation;
+    bool needsStepCount;
+    Fingerprint fp;
+    std::ostringstream text;
+
+    Translation() : hasPropagation(false), needsStepCount(false) {}
+
+    void addField(const MagneticField *f, const PeriodicWrap *wrap) {
+        if (!f) throw Unsupported("a propagation module has no magnetic field");
+        if (const MagneticFieldList *l = dynamic_cast<const MagneticFieldList *>(f)) {
+            const FieldVector &v = l->*member(ListFields());
+            for (size_t i = 0; i < v.size(); i++) addField(v[i].get(), wrap);
+            return;
+        }
+        if (const PeriodicMagneticField *p = dynamic_cast<const PeriodicMagneticField *>(f)) {
+            if (wrap) throw Unsupported("PeriodicMagneticField inside a PeriodicMagneticField");
+            PeriodicMagneticField *q = const_cast<PeriodicMagneticField *>(p);
+            PeriodicWrap w = {q->getOrigin(), q->getExtends(), q->isReflective()};
+            addField((p->*member(PeriodicInner())).get(), &w);
+            return;
+        }
+        crp_field_component c;
+        std::memset(&c, 0, sizeof(c));
+        if (wrap) {
+            c.periodic = 1;
+            c.periodic_reflective = wrap->reflective ? 1 : 0;
+            for (int a = 0; a < 3; a++) {
+                c.periodic_origin[a] = wrap->origin.data[a];
+                c.periodic_extends[a] = wrap->extends.data[a];
+            }
+        }
+        if (const MagneticFieldGrid *g = dynamic_cast<const MagneticFieldGrid *>(f)) {
+            ref_ptr<Grid3f> grid = const_cast<MagneticFieldGrid *>(g)->getGrid();
+            if (!grid.valid()) throw Unsupported("MagneticFieldGrid without a grid");
+            if (grid->getInterpolationType() != TRILINEAR)
+                throw Unsupported("Grid3f interpolation " + grid->getInterpolationTypeName() +
+                                  " (the device path interpolates trilinearly)");
+            std::vector<Vector3f> &v = grid->getGrid();
+            c.kind = CRP_FIELD_GRID;
+            c.grid.values = reinterpret_cast<const float *>(&v[0]);
+            c.grid.nx = grid->getNx();
+            c.grid.ny = grid->getNy();
+            c.grid.nz = grid->getNz();
+            Vector3d o = grid->getOrigin(), s = grid->getSpacing();
+            for (int a = 0; a < 3; a++) {
+                c.grid.origin[a] = o.data[a];
+                c.grid.spacing[a] = s.data[a];
+            }
+            c.grid.reflective = grid->isReflective() ? 1 : 0;
+            c.grid.clip_volume = grid->getClipVolume() ? 1 : 0;
+            fp.words(c.grid.values, sizeof(float) * 3 * v.size());
+            text << "  field: Grid3f " << c.grid.nx << "x" << c.grid.ny << "x" << c.grid.nz
+                 << " spacing " << s.x << " reflective " << c.grid.reflective << " clipVolume "
+                 << c.grid.clip_volume;
+        } else if (const PlaneWaveTurbulence *w = dynamic_cast<const PlaneWaveTurbulence *>(f)) {
+            const int nm = w->*member(WavesNm());
+            const std::vector<Vector3d> &xi = w->*member(WavesXi());
+            const std::vector<Vector3d> &kap = w->*member(WavesKappa());
+            storage.push_back(std::vector<double>(3 * nm));
+            std::vector<double> &xs = storage.back();
+            storage.push_back(std::vector<double>(3 * nm));
+            std::vector<double> &ks = storage.back();
+            for (int i = 0; i < nm; i++)
+                for (int a = 0; a < 3; a++) {
+                    xs[3 * i + a] = xi[i].data[a];
+                    ks[3 * i + a] = kap[i].data[a];
+                }
+            storage.push_back(w->*member(WavesK()));
+            const std::vector<double> &kk = storage.back();
+            storage.push_back(w->*member(WavesBeta()));
+            const std::vector<double> &bb = storage.back();
+            storage.push_back(w->*member(WavesAk()));
+            const std::vector<double> &aa = storage.back();
+            c.kind = CRP_FIELD_PLANE_WAVE;
+            c.plane_wave.n_modes = nm;
+            c.plane_wave.xi = &xs[0];
+            c.plane_wave.kappa = &ks[0];
+            c.plane_wave.k = &kk[0];
+            c.plane_wave.beta = &bb[0];
+            c.plane_wave.ak = &aa[0];
+            fp.words(&xs[0], 8 * xs.size());
+            fp.words(&ks[0], 8 * ks.size());
+            fp.words(&kk[0], 8 * kk.size());
+            fp.words(&bb[0], 8 * bb.size());
+            fp.words(&aa[0], 8 * aa.size());
+            text << "  field: PlaneWaveTurbulence " << nm << " modes";
+        } else if (const UniformMagneticField *u = dynamic_cast<const UniformMagneticField *>(f)) {
+            Vector3d b = u->getField(Vector3d(0.));
+            c.kind = CRP_FIELD_UNIFORM;
+            for (int a = 0; a < 3; a++) c.uniform[a] = b.data[a];
+            text << "  field: UniformMagneticField " << b.x << " " << b.y << " " << b.z;
+        } else if (const crpgpu::ToroidalMagneticField *t =
+                       dynamic_cast<const crpgpu::ToroidalMagneticField *>(f)) {
+            c.kind = CRP_FIELD_TOROIDAL;
+            c.toroidal_b0 = t->getB0();
+            text << "  field: ToroidalMagneticField b0 " << c.toroidal_b0;
+        } else {
+            throw Unsupported("magnetic field " + name_of(f) + " has no device form");
+        }
+        if (wrap)
+            text << " in PeriodicMagneticField extends " << wrap->extends.x << " reflective "
+                 << wrap->reflective;
+        text << "\n";
+        fields.push_back(c);
+    }
+
+    void setField(const MagneticField *f) {
+        if (hasPropagation) throw Unsupported("more than one propagation module");
+        hasPropagation = true;
+        addField(f, 0);
+    }
+
+    static crp_module_desc blank(int kind) {
+        crp_module_desc m;
+        std::memset(&m, 0, sizeof(m));
+        m.kind = kind;
+        m.deactivate_on_detection = 1;
+        return m;
+    }
+
+    void addModule(const Module *m) {
+        if (const PropagationBP *p = dynamic_cast<const PropagationBP *>(m)) {
+            crp_module_desc d = blank(CRP_MODULE_PROPAGATION);
+            d.propagator = CRP_PROP_BP;
+            d.tolerance = p->getTolerance();
+            d.min_step = p->getMinimumStep();
+            d.max_step = p->getMaximumStep();
+            text << "  module: PropagationBP tolerance " << d.tolerance << " minStep " << d.min_step
+                 << " maxStep " << d.max_step << "\n";
+            setField(p->getField().get());
+            push(d, Action());
+        } else if (const PropagationCK *p = dynamic_cast<const PropagationCK *>(m)) {
+            crp_module_desc d = blank(CRP_MODULE_PROPAGATION);
+            d.propagator = CRP_PROP_CK;
+            d.tolerance = p->getTolerance();
+            d.min_step = p->getMinimumStep();
+            d.max_step = p->getMaximumStep();
+            text << "  module: PropagationCK tolerance " << d.tolerance << " minStep " << d.min_step
+                 << " maxStep " << d.max_step << "\n";
+            setField(p->getField().get());
+            push(d, Action());
+        } else if (const DiffusionSDE *p = dynamic_cast<const DiffusionSDE *>(m)) {
+            if (p->getAdvectionField().valid())
+                throw Unsupported("DiffusionSDE with an advection field");
+            crp_module_desc d = blank(CRP_MODULE_PROPAGATION);
+            d.propagator = CRP_PROP_SDE;
+            d.tolerance = p->getTolerance();
+            d.min_step = p->getMinimumStep();
+            d.max_step = p->getMaximumStep();
+            d.sde_epsilon = p->getEpsilon();
+            d.sde_alpha = p->getAlpha();
+            d.sde_scale = p->getScale();
+            text << "  module: DiffusionSDE tolerance " << d.tolerance << " minStep " << d.min_step
+                 << " maxStep " << d.max_step << " epsilon " << d.sde_epsilon << " alpha "
+                 << d.sde_alpha << " scale " << d.sde_scale << "\n";
+            setField(p->getMagneticField().get());
+            needsStepCount = true;
+            push(d, Action());
+        } else if (const crpgpu::CandidateMaximumTrajectoryLength *c =
+                       dynamic_cast<const crpgpu::CandidateMaximumTrajectoryLength *>(m)) {
+            if (!perCandidateKey.empty() && perCandidateKey != c->getPropertyKey())
+                throw Unsupported("two CandidateMaximumTrajectoryLength modules with different keys");
+            perCandidateKey = c->getPropertyKey();
+            crp_module_desc d = blank(CRP_MODULE_MAX_TRAJECTORY_LENGTH);
+            d.per_candidate_length = 1;
+            d.record = 1;
+            condition(c);
+            text << "  module: CandidateMaximumTrajectoryLength key " << perCandidateKey << "\n";
+            Action a = {CRP_MODULE_MAX_TRAJECTORY_LENGTH, c, 0};
+            push(d, a);
+        } else if (const MaximumTrajectoryLength *c = dynamic_cast<const MaximumTrajectoryLength *>(m)) {
+            if (!c->getObserverPositions().empty())
+                throw Unsupported("MaximumTrajectoryLength with observer positions");
+            crp_module_desc d = blank(CRP_MODULE_MAX_TRAJECTORY_LENGTH);
+            d.max_length = c->getMaximumTrajectoryLength();
+            d.record = 1;
+            condition(c);
+            text << "  module: MaximumTrajectoryLength " << d.max_length << "\n";
+            Action a = {CRP_MODULE_MAX_TRAJECTORY_LENGTH, c, 0};
+            push(d, a);
+        } else if (const Observer *o = dynamic_cast<const Observer *>(m)) {
+            const FeatureList &fs = o->*member(ObserverFeatures());
+            if (fs.empty()) {
+                text << "  module: Observer without features (never detects; dropped)\n";
+                return;
+            }
+            if (fs.size() > 1) throw Unsupported("Observer with more than one feature");
+            crp_module_desc d = blank(CRP_MODULE_OBSERVER);
+            const ObserverFeature *f = fs[0].get();
+            if (const ObserverSurface *s = dynamic_cast<const ObserverSurface *>(f)) {
+                const Surface *surf = (s->*member(SurfaceOf())).get();
+                const Sphere *sp = dynamic_cast<const Sphere *>(surf);
+                if (!sp) throw Unsupported("ObserverSurface over " + name_of(surf));
+                const Vector3d &c = sp->*member(SphereCenter());
+                d.observer_feature = CRP_OBSERVER_SURFACE_SPHERE;
+                for (int a = 0; a < 3; a++) d.sphere_center[a] = c.data[a];
+                d.sphere_radius = sp->*member(SphereRadius());
+                text << "  module: Observer ObserverSurface(Sphere center " << c.x << " " << c.y
+                     << " " << c.z << " radius " << d.sphere_radius << ")";
+            } else if (typeid(*f) == typeid(ObserverDetectAll)) {
+                d.observer_feature = CRP_OBSERVER_DETECT_ALL;
+                text << "  module: Observer ObserverDetectAll";
+            } else {
+                throw Unsupported("observer feature " + name_of(f) + " has no device form");
+            }
+            d.deactivate_on_detection = (o->*member(ObserverInactive())) ? 1 : 0;
+            d.record = 1;
+            const Module *act = (o->*member(ObserverAction())).get();
+            text << " deactivate " << d.deactivate_on_detection << " action "
+                 << (act ? name_of(act) : std::string("none")) << "\n";
+            Action a = {CRP_MODULE_OBSERVER, 0, o};
+            push(d, a);
+        } else {
+            throw Unsupported("module " + name_of(m) + " has no device form");
+        }
+    }
+
+    void condition(const AbstractCondition *c) {
+        if (!(c->*member(RejectInactive())))
+            throw Unsupported(name_of(c) + " with setMakeRejectedInactive(false)");
+    }
+
+    void push(const crp_module_desc &d, const Action &a) {
+        modules.push_back(d);
+        actions.push_back(a);
+        fp.value(d);
+    }
+
+    void finish(int precision, uint64_t seed) {
+        if (!hasPropagation) throw Unsupported("no propagation module");
+        fp.value(precision);
+        fp.value(seed);
+        for (size_t i = 0; i < fields.size(); i++) {
+            crp_field_component c = fields[i];
+            c.grid.values = 0;  // content hashed above
+            c.plane_wave.xi = c.plane_wave.kappa = c.plane_wave.k = c.plane_wave.beta =
+                c.plane_wave.ak = 0;
+            fp.value(c);
+        }
+    }
+};
+
+volatile int32_t g_cancel = 0;
+
+extern "C" void crpgpu_on_signal(int sig) { g_cancel = sig; }
+
+struct SignalScope {
+    struct sigaction old_int, old_term;
+    SignalScope() {
+        g_cancel = 0;
+        struct sigaction sa;
+        std::memset(&sa, 0, sizeof(sa));
+        sa.sa_handler = crpgpu_on_signal;
+        sigaction(SIGINT, &sa, &old_int);
+        sigaction(SIGTERM, &sa, &old_term);
+    }
+    ~SignalScope() {
+        sigaction(SIGINT, &old_int, 0);
+        sigaction(SIGTERM, &old_term, 0);
+    }
+};
+
+// Host structure-of-arrays of one batch.
+struct Batch {
+    std::vector<int32_t> id;
+    std::vector<double> charge, energy, x, y, z, dx, dy, dz, px, py, pz, length, time, cur, next,
+        max_length;
+    std::vector<uint8_t> active;
+    std::vector<uint32_t> flags;
+    std::vector<uint64_t> steps;
+
+    void resize(size_t n, bool per, bool sc) {
+        id.resize(n);
+        std::vector<double> *d[] = {&charge, &energy, &x, &y, &z, &dx, &dy, &dz, &px, &py, &pz,
+                                    &length, &time, &cur, &next};
+        for (size_t i = 0; i < sizeof(d) / sizeof(d[0]); i++) d[i]->resize(n);
+        max_length.resize(per ? n : 0);
+        active.resize(n);
+        flags.resize(n);
+        steps.resize(sc ? n : 0);
+    }
+
+    crp_candidates view() {
+        crp_candidates c;
+        std::memset(&c, 0, sizeof(c));
+        c.id = &id[0];
+        c.charge = &charge[0];
+        c.energy = &energy[0];
+        c.x = &x[0]; c.y = &y[0]; c.z = &z[0];
+        c.dx = &dx[0]; c.dy = &dy[0]; c.dz = &dz[0];
+        c.px = &px[0]; c.py = &py[0]; c.pz = &pz[0];
+        c.trajectory_length = &length[0];
+        c.time = &time[0];
+        c.current_step = &cur[0];
+        c.next_step = &next[0];
+        c.active = &active[0];
+        c.flags = &flags[0];
+        c.max_length = max_length.empty() ? 0 : &max_length[0];
+        c.step_count = steps.empty() ? 0 : &steps[0];
+        return c;
+    }
+};
+
+struct Records {
+    uint64_t count;
+    std::vector<uint64_t> index;
+    std::vector<int32_t> module, id;
+    std::vector<double> length, time, x, y, z, dx, dy, dz, energy;
+
+    crp_records view(uint64_t cap) {
+        index.resize(cap); module.resize(cap); id.resize(cap);
+        std::vector<double> *d[] = {&length, &time, &x, &y, &z, &dx, &dy, &dz, &energy};
+        for (size_t i = 0; i < sizeof(d) / sizeof(d[0]); i++) d[i]->resize(cap);
+        crp_records r;
+        std::memset(&r, 0, sizeof(r));
+        count = 0;
+        r.capacity = cap;
+        r.count = &count;
+        r.index = &index[0]; r.module = &module[0]; r.id = &id[0];
+        r.trajectory_length = &length[0]; r.time = &time[0];
+        r.x = &x[0]; r.y = &y[0]; r.z = &z[0];
+        r.dx = &dx[0]; r.dy = &dy[0]; r.dz = &dz[0];
+        r.energy = &energy[0];
+        return r;
+    }
+};
+
+void set_direction_exact(ParticleState &s, double x, double y, double z) {
+    s.*member(StateDirection()) = Vector3d(x, y, z);
+}
+
+}  // namespace
+
+namespace crpgpu {
+
+// ---------------------------------------------------------------------------
+ToroidalMagneticField::ToroidalMagneticField(double b0) : b0(b0) {}
+
+Vector3d ToroidalMagneticField::getField(const Vector3d &p) const {
+    double r = std::sqrt(p.x * p.x + p.y * p.y);
+    return Vector3d(-p.y, p.x, 0.) * (b0 / r);
+}
+
+double ToroidalMagneticField::getB0() const { return b0; }
+
+CandidateMaximumTrajectoryLength::CandidateMaximumTrajectoryLength(const std::string &key)
+    : key(key) {}
+
+void CandidateMaximumTrajectoryLength::process(Candidate *c) const {
+    double maxLength = c->getProperty(key).asDouble();
+    double length = c->getTrajectoryLength();
+    if (length >= maxLength)
+        reject(c);
+    else
+        c->limitNextStep(maxLength - length);
+}
+
+std::string CandidateMaximumTrajectoryLength::getPropertyKey() const { return key; }
+
+std::string CandidateMaximumTrajectoryLength::getDescription() const {
+    return "Maximum trajectory length from candidate property " + key;
+}
+
+// ---------------------------------------------------------------------------
+struct GpuModuleList::Impl {
+    int precision;
+    uint64_t seed;
+    size_t batch;
+    bool cpuFallback;
+    crp_plan *plan;
+    uint64_t planFingerprint;
+    crp_run_stats stats;
+    uint64_t events;
+
+    Impl() : precision(CRP_PRECISION_FP64), seed(0), batch(size_t(1) << 20), cpuFallback(false),
+             plan(0), planFingerprint(0), events(0) {
+        std::memset(&stats, 0, sizeof(stats));
+    }
+    ~Impl() {
+        if (plan) crp_plan_destroy(plan);
+    }
+};
+
+GpuModuleList::GpuModuleList() : impl(new Impl()) {}
+
+GpuModuleList::~GpuModuleList() { delete impl; }
+
+void GpuModuleList::setPrecision(Precision p) { impl->precision = p; }
+
+GpuModuleList::Precision GpuModuleList::getPrecision() const {
+    return impl->precision == CRP_PRECISION_MIXED ? MIXED : FP64;
+}
+
+void GpuModuleList::setSeed(uint64_t seed) { impl->seed = seed; }
+
+void GpuModuleList::setBatchSize(size_t n) {
+    if (n == 0) throw std::runtime_error("GpuModuleList: batch size must be positive");
+    impl->batch = n;
+}
+
+void GpuModuleList::setCpuFallback(bool allow) { impl->cpuFallback = allow; }
+
+const crp_run_stats &GpuModuleList::getLastRunStats() const { return impl->stats; }
+
+uint64_t GpuModuleList::getLastRunEvents() const { return impl->events; }
+
+static void translate(const ModuleList &ml, int precision, uint64_t seed, Translation &t) {
+    for (ModuleList::const_iterator it = ml.begin(); it != ml.end(); ++it) t.addModule(it->get());
+    t.finish(precision, seed);
+}
+
+bool GpuModuleList::isSupported(std::string *reason) const {
+    try {
+        Translation t;
+        translate(*this, impl->precision, impl->seed, t);
+        return true;
+    } catch (Unsupported &e) {
+        if (reason) *reason = e.what();
+        return false;
+    }
+}
+
+std::string GpuModuleList::describePlan() const {
+    Translation t;
+    try {
+        translate(*this, impl->precision, impl->seed, t);
+    } catch (Unsupported &e) {
+        throw std::runtime_error(std::string("GpuModuleList: ") + e.what());
+    }
+    std::ostringstream os;
+    os << "GpuModuleList plan (" << (impl->precision == CRP_PRECISION_MIXED ? "mixed" : "fp64")
+       << ", seed " << impl->seed << ")\n"
+       << t.text.str();
+    return os.str();
+}
+
+std::string GpuModuleList::getDescription() const {
+    return "GpuModuleList (device stepping path)\n" + ModuleList::getDescription();
+}
+
+void GpuModuleList::run(Candidate *candidate, bool recursive, bool secondariesFirst) {
+    candidate_vector_t v(1, ref_ptr<Candidate>(candidate));
+    run(&v, recursive, secondariesFirst);
+}
+
+void GpuModuleList::run(ref_ptr<Candidate> candidate, bool recursive, bool secondariesFirst) {
+    run(candidate.get(), recursive, secondariesFirst);
+}
+
+void GpuModuleList::run(const candidate_vector_t *candidates, bool recursive,
+                        bool secondariesFirst) {
+    std::string why;
+    if (!isSupported(&why)) {
+        if (impl->cpuFallback) {
+            ModuleList::run(candidates, recursive, secondariesFirst);
+            return;
+        }
+        throw std::runtime_error("GpuModuleList: chain is not on the device path: " + why);
+    }
+    runDevice(*candidates);
+}
+
+void GpuModuleList::run(SourceInterface *source, size_t count, bool recursive,
+                        bool secondariesFirst) {
+    std::string why;
+    if (!isSupported(&why)) {
+        if (impl->cpuFallback) {
+            ModuleList::run(source, count, recursive, secondariesFirst);
+            return;
+        }
+        throw std::runtime_error("GpuModuleList: chain is not on the device path: " + why);
+    }
+    crp_run_stats total;
+    std::memset(&total, 0, sizeof(total));
+    uint64_t events = 0;
+    for (size_t done = 0; done < count;) {
+        size_t n = std::min(impl->batch, count - done);
+        candidate_vector_t v;
+        v.reserve(n);
+        for (size_t i = 0; i < n; i++) v.push_back(source->getCandidate());
+        runDevice(v);
+        total.particle_steps += impl->stats.particle_steps;
+        total.tries += impl->stats.tries;
+        total.field_evaluations += impl->stats.field_evaluations;
+        total.launches += impl->stats.launches;
+        total.device_ms += impl->stats.device_ms;
+        events += impl->events;
+        done += n;
+    }
+    impl->stats = total;
+    impl->events = events;
+}
+
+void GpuModuleList::runDevice(const candidate_vector_t &cands) {
+    Translation t;
+    translate(*this, impl->precision, impl->seed, t);
+    std::memset(&impl->stats, 0, sizeof(impl->stats));
+    impl->events = 0;
+    const size_t n = cands.size();
+    if (n == 0) return;
+
+    // plan: rebuilt when the chain, its parameters or its field payload changed
+    if (!impl->plan || impl->planFingerprint != t.fp.h) {
+        if (impl->plan) {
+            crp_plan_destroy(impl->plan);
+            impl->plan = 0;
+        }
+        crp_plan_desc d;
+        std::memset(&d, 0, sizeof(d));
+        d.abi_version = CRP_ABI_VERSION;
+        d.precision = impl->precision;
+        d.fields = &t.fields[0];
+        d.n_fields = int32_t(t.fields.size());
+        d.modules = &t.modules[0];
+        d.n_modules = int32_t(t.modules.size());
+        d.seed = impl->seed;
+        check(crp_plan_create(&d, &impl->plan));
+        impl->planFingerprint = t.fp.h;
+    }
+
+    const bool per = !t.perCandidateKey.empty();
+    Batch b;
+    b.resize(n, per, t.needsStepCount);
+    for (size_t i = 0; i < n; i++) {
+        const Candidate *c = cands[i].get();
+        const ParticleState &s = c->current;
+        b.id[i] = s.getId();
+        b.charge[i] = s.getCharge();
+        b.energy[i] = s.getEnergy();
+        const Vector3d &p = s.getPosition(), &u = s.getDirection(),
+                       &q = c->previous.getPosition();
+        b.x[i] = p.x; b.y[i] = p.y; b.z[i] = p.z;
+        b.dx[i] = u.x; b.dy[i] = u.y; b.dz[i] = u.z;
+        b.px[i] = q.x; b.py[i] = q.y; b.pz[i] = q.z;
+        b.length[i] = c->getTrajectoryLength();
+        b.time[i] = c->getTime();
+        b.cur[i] = c->getCurrentStep();
+        b.next[i] = c->getNextStep();
+        b.active[i] = c->isActive() ? 1 : 0;
+        b.flags[i] = 0;
+        if (per) b.max_length[i] = c->getProperty(t.perCandidateKey).asDouble();
+        if (t.needsStepCount) b.steps[i] = 0;
+    }
+
+    // every recording module fires at most once per candidate when it
+    // deactivates; observers that keep candidates active may fire more often
+    // (the run is repeated with the exact count then: the inputs are intact)
+    size_t nrec = 0;
+    for (size_t m = 0; m < t.modules.size(); m++) nrec += t.modules[m].record ? 1 : 0;
+    Records rec;
+    uint64_t cap = uint64_t(n) * std::max<size_t>(nrec, 1) + 1024;
+    for (int attempt = 0;; attempt++) {
+        Batch work = b;
+        crp_candidates view = work.view();
+        crp_records rv = rec.view(cap);
+        crp_run_opts o;
+        std::memset(&o, 0, sizeof(o));
+        o.mode = CRP_MODE_AUTO;
+        o.cancel = &g_cancel;
+        o.records = nrec ? &rv : 0;
+        crp_status st;
+        {
+            SignalScope sig;
+            st = crp_run(impl->plan, &view, n, &o, &impl->stats);
+        }
+        if (st == CRP_ERR_CANCELLED)
+            throw std::runtime_error("GpuModuleList: run interrupted by a signal; candidates unchanged");
+        check(st);
+        if (rec.count > cap) {
+            if (attempt > 0) throw std::runtime_error("GpuModuleList: record count changed between runs");
+            cap = rec.count;
+            continue;
+        }
+        std::swap(b, work);  // keep the results
+        break;
+    }
+
+    // events per candidate in the order the device wrote them (one thread
+    // writes all of a candidate's records, so slot order is time order)
+    const uint64_t ne = nrec ? rec.count : 0;
+    std::vector<uint64_t> order(ne);
+    for (uint64_t e = 0; e < ne; e++) order[e] = e;
+    std::stable_sort(order.begin(), order.end(),
+                     [&rec](uint64_t a, uint64_t c) { return rec.index[a] < rec.index[c]; });
+    impl->events = ne;
+
+    size_t e = 0;
+    for (size_t i = 0; i < n; i++) {
+        Candidate *c = cands[i].get();
+        for (; e < ne && rec.index[order[e]] == i; e++) {
+            const uint64_t r = order[e];
+            const int mi = rec.module[r];
+            if (mi < 0 || size_t(mi) >= t.actions.size())
+                throw std::runtime_error("GpuModuleList: record of an unknown module");
+            c->current.setPosition(Vector3d(rec.x[r], rec.y[r], rec.z[r]));
+            set_direction_exact(c->current, rec.dx[r], rec.dy[r], rec.dz[r]);
+            c->setTrajectoryLength(rec.length[r]);
+            c->setTime(rec.time[r]);
+            const Action &a = t.actions[mi];
+            if (a.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
+                // AbstractCondition::reject (Module.cpp:25-37)
+                const ref_ptr<Module> &act = a.condition->*member(RejectAction());
+                if (act.valid()) act->process(c);
+                const std::string &k = a.condition->*member(RejectKey());
+                if (!k.empty()) c->setProperty(k, a.condition->*member(RejectValue()));
+            } else if (a.kind == CRP_MODULE_OBSERVER) {
+                // Observer::process after a detection (Observer.cpp:37-52)
+                const FeatureList &fs = a.observer->*member(ObserverFeatures());
+                for (size_t f = 0; f < fs.size(); f++) fs[f]->onDetection(c);
+                const ref_ptr<Module> &act = a.observer->*member(ObserverAction());
+                if (act.valid()) {
+                    if (a.observer->*member(ObserverClone()))
+                        act->process(c->clone(false));
+                    else
+                        act->process(c);
+                }
+                const std::string &k = a.observer->*member(ObserverFlagKey());
+                if (!k.empty()) c->setProperty(k, a.observer->*member(ObserverFlagValue()));
+            }
+        }
+        // final state
+        c->current.setPosition(Vector3d(b.x[i], b.y[i], b.z[i]));
+        set_direction_exact(c->current, b.dx[i], b.dy[i], b.dz[i]);
+        c->previous.setPosition(Vector3d(b.px[i], b.py[i], b.pz[i]));
+        c->setCurrentStep(b.cur[i]);  // also adds to length and time: both set next
+        c->setTrajectoryLength(b.length[i]);
+        c->setTime(b.time[i]);
+        c->setNextStep(b.next[i]);
+        c->setActive(b.active[i] != 0);
+    }
+}
+
+}  // namespace crpgpu

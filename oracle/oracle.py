@@ -5,6 +5,9 @@
 * `Reference` wraps oracle/_ref/libcrp_ref.so, the reference itself compiled
   from its sources with the shim ref_shim.cpp (oracle/Makefile), when it has
   been built (it needs the reference checkout at build time only).
+* `PluginHarness` wraps oracle/_ref/libcrp_ref_gpu.so: the reference's own
+  chain objects run through the product's C++ plugin GpuModuleList
+  (crpropa3_b200/plugin), the drop-in for ModuleList::run.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU legs use this module;
 the product never imports it.
@@ -25,6 +28,7 @@ ORACLE_LIB = os.path.join(HERE, "_build", "libcrp_oracle.so")
 ORACLE_CRPOW_LIB = os.path.join(HERE, "_build", "libcrp_oracle_crpow.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcrp_ref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libcrp_ref_fast.so")
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libcrp_ref_gpu.so")
 
 _dp = C.POINTER(C.c_double)
 
@@ -81,6 +85,13 @@ class Oracle:
                                 C.byref(steps), C.byref(tries))
         assert r == 0
         return steps.value, tries.value
+
+    def run_textout(self, spec, cands: CandidateArrays, path, output_type, threads=1, seed=0,
+                    serial0=1):
+        """Run with TextOutput(path, output_type) as every observer's action."""
+        self._check(self.lib.ref_run_textout(C.byref(spec.desc()), C.byref(cands.struct()),
+                                             cands.n, str(path).encode(), output_type, threads,
+                                             seed, serial0))
 
     def field(self, spec, pos):
         pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).T)
@@ -166,6 +177,9 @@ class Reference:
         lib.ref_charge.restype = C.c_double
         lib.ref_charge.argtypes = [C.c_int32]
         lib.ref_last_error.restype = C.c_char_p
+        lib.ref_run_textout.argtypes = [C.POINTER(_abi.PlanDesc), C.POINTER(_abi.Candidates),
+                                        C.c_uint64, C.c_char_p, C.c_int, C.c_int, C.c_uint32,
+                                        C.c_uint64]
         lib.ref_text_output.argtypes = [C.c_char_p, C.c_int, C.c_uint64, C.POINTER(C.c_uint64),
                                         C.POINTER(C.c_int32), _dp, _dp, _dp, _dp,
                                         C.POINTER(C.c_int32), _dp, _dp, _dp]
@@ -184,6 +198,13 @@ class Reference:
                                      C.byref(rs) if rs is not None else None, threads, seed,
                                      C.byref(steps), C.byref(secs)))
         return steps.value, secs.value
+
+    def run_textout(self, spec, cands: CandidateArrays, path, output_type, threads=1, seed=0,
+                    serial0=1):
+        """Run with TextOutput(path, output_type) as every observer's action."""
+        self._check(self.lib.ref_run_textout(C.byref(spec.desc()), C.byref(cands.struct()),
+                                             cands.n, str(path).encode(), output_type, threads,
+                                             seed, serial0))
 
     def field(self, spec, pos):
         pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).T)
@@ -224,3 +245,74 @@ class Reference:
             ids.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(energy), _dptr(pos), _dptr(dirs),
             _dptr(length), src_id.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(src_e),
             _dptr(src_pos), _dptr(src_dir)))
+
+
+def plugin_harness_available() -> bool:
+    return os.path.exists(REF_GPU_LIB)
+
+
+class PluginHarness:
+    """The reference's chain objects run through the C++ plugin GpuModuleList
+    (ref_gpu_shim.cpp).  describe() and unsupported chains need no device."""
+
+    def __init__(self):
+        if not os.path.exists(REF_GPU_LIB):
+            raise RuntimeError(f"{REF_GPU_LIB} is not built (make -C oracle ref-gpu)")
+        lib = C.CDLL(REF_GPU_LIB)
+        pd, cd = C.POINTER(_abi.PlanDesc), C.POINTER(_abi.Candidates)
+        lib.ref_gpu_last_error.restype = C.c_char_p
+        lib.ref_gpu_run.argtypes = [pd, cd, C.c_uint64, C.POINTER(_abi.Records), C.c_int,
+                                    C.c_uint64, C.POINTER(_abi.RunStats), C.POINTER(C.c_uint64)]
+        lib.ref_gpu_run_textout.argtypes = [pd, cd, C.c_uint64, C.c_char_p, C.c_int, C.c_int,
+                                            C.c_uint64, C.c_uint64]
+        lib.ref_run_source_textout.argtypes = [pd, C.c_int, C.c_int, _dp, C.c_int32, C.c_double,
+                                               C.c_double, C.c_double, C.c_uint64, C.c_uint64,
+                                               C.c_char_p, C.c_int, C.c_uint32, C.c_uint64,
+                                               C.POINTER(_abi.RunStats)]
+        lib.ref_gpu_describe.argtypes = [pd, C.c_int, C.c_char_p, C.c_size_t]
+        lib.ref_gpu_unsupported_throws.argtypes = [pd, C.c_char_p, C.c_size_t]
+        self.lib = lib
+
+    def _check(self, r):
+        if r != 0:
+            raise RuntimeError(self.lib.ref_gpu_last_error().decode())
+
+    def run(self, spec, cands: CandidateArrays, records: RecordArrays = None, precision=0, seed=0):
+        """GpuModuleList::run(candidate_vector_t*): (run stats, events replayed)."""
+        rs = records.struct() if records is not None else None
+        stats, events = _abi.RunStats(), C.c_uint64()
+        self._check(self.lib.ref_gpu_run(C.byref(spec.desc()), C.byref(cands.struct()), cands.n,
+                                         C.byref(rs) if rs is not None else None, precision, seed,
+                                         C.byref(stats), C.byref(events)))
+        return stats, events.value
+
+    def run_textout(self, spec, cands: CandidateArrays, path, output_type, precision=0, seed=0,
+                    serial0=1):
+        self._check(self.lib.ref_gpu_run_textout(C.byref(spec.desc()), C.byref(cands.struct()),
+                                                 cands.n, str(path).encode(), output_type,
+                                                 precision, seed, serial0))
+
+    def run_source_textout(self, spec, gpu, position, pid, emin, emax, index, count, path,
+                           output_type, seed=1, serial0=1, batch=0, precision=0):
+        """run(source, count) of SourcePosition + SourceParticleType +
+        SourcePowerLawSpectrum + SourceIsotropicEmission, on the plugin (gpu)
+        or on the reference's ModuleList with one thread."""
+        pos = np.ascontiguousarray(position, dtype=np.float64)
+        stats = _abi.RunStats()
+        self._check(self.lib.ref_run_source_textout(
+            C.byref(spec.desc()), 1 if gpu else 0, precision, _dptr(pos), pid, emin, emax, index,
+            count, batch, str(path).encode(), output_type, seed, serial0, C.byref(stats)))
+        return stats
+
+    def describe(self, spec, extra=0):
+        """(on the device path?, plan text or reason) without a device."""
+        buf = C.create_string_buffer(1 << 16)
+        r = self.lib.ref_gpu_describe(C.byref(spec.desc()), extra, buf, len(buf))
+        if r < 0:
+            raise RuntimeError(buf.value.decode())
+        return r == 1, buf.value.decode()
+
+    def unsupported_run_message(self, spec):
+        buf = C.create_string_buffer(4096)
+        r = self.lib.ref_gpu_unsupported_throws(C.byref(spec.desc()), buf, len(buf))
+        return (buf.value.decode() if r == 1 else None)

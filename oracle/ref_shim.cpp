@@ -26,6 +26,7 @@
  *   StepCounter           counts process() calls of the chain = steps
  */
 #include "crp_gpu.h"
+#include "ref_chain.h"
 
 #include "crpropa/Candidate.h"
 #include "crpropa/Grid.h"
@@ -59,8 +60,10 @@
 using namespace crpropa;
 
 namespace {
-
 std::string g_error;
+}
+
+namespace crp_ref {
 
 /* The mass table is read on the first ParticleState::setId of a nucleus
  * (ParticleMass.cpp:24); the stepping path never uses the mass.  Point
@@ -125,26 +128,16 @@ public:
     }
 };
 
-class StepCounter : public Module {
-public:
-    mutable std::vector<uint64_t> perThread;
-    StepCounter() : perThread(256 * 8, 0) {}
-    void process(Candidate *c) const { perThread[omp_get_thread_num() * 8]++; }
-    uint64_t total() const {
-        uint64_t s = 0;
-        for (size_t i = 0; i < perThread.size(); i += 8) s += perThread[i];
-        return s;
-    }
-};
+StepCounter::StepCounter() : perThread(256 * 8, 0) {}
+void StepCounter::process(Candidate *c) const { perThread[omp_get_thread_num() * 8]++; }
+uint64_t StepCounter::total() const {
+    uint64_t s = 0;
+    for (size_t i = 0; i < perThread.size(); i += 8) s += perThread[i];
+    return s;
+}
 
-struct Built {
-    ref_ptr<ModuleList> sim;
-    ref_ptr<MagneticField> field;
-    std::vector<ref_ptr<Referenced> > keep;  // spectra, grids
-    ref_ptr<StepCounter> counter;
-};
-
-ref_ptr<MagneticField> build_component(const crp_field_component &f, Built &b) {
+static ref_ptr<MagneticField> build_component(const crp_field_component &f, Built &b,
+                                              const Helpers *h) {
     ref_ptr<MagneticField> m;
     if (f.kind == CRP_FIELD_GRID) {
         const crp_grid3f_desc &g = f.grid;
@@ -166,7 +159,7 @@ ref_ptr<MagneticField> build_component(const crp_field_component &f, Built &b) {
     } else if (f.kind == CRP_FIELD_UNIFORM) {
         m = new UniformMagneticField(Vector3d(f.uniform[0], f.uniform[1], f.uniform[2]));
     } else if (f.kind == CRP_FIELD_TOROIDAL) {
-        m = new ToroidalField(f.toroidal_b0);
+        m = h ? h->toroidal(f.toroidal_b0) : new ToroidalField(f.toroidal_b0);
     } else {
         throw std::runtime_error("ref_shim: unknown field kind");
     }
@@ -179,18 +172,19 @@ ref_ptr<MagneticField> build_component(const crp_field_component &f, Built &b) {
     return m;
 }
 
-ref_ptr<MagneticField> build_field(const crp_plan_desc *d, Built &b) {
+static ref_ptr<MagneticField> build_field(const crp_plan_desc *d, Built &b, const Helpers *h) {
     if (d->n_fields == 1)
-        return build_component(d->fields[0], b);
+        return build_component(d->fields[0], b, h);
     ref_ptr<MagneticFieldList> list = new MagneticFieldList();
     for (int i = 0; i < d->n_fields; i++)
-        list->addField(build_component(d->fields[i], b));
+        list->addField(build_component(d->fields[i], b, h));
     return list;
 }
 
-void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b) {
-    b.field = build_field(d, b);
-    b.sim = new ModuleList();
+void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpers *h,
+                 ModuleList *sim, bool count_steps, const char *text_output, int text_type) {
+    b.field = build_field(d, b, h);
+    b.sim = sim ? sim : new ModuleList();
     for (int i = 0; i < d->n_modules; i++) {
         const crp_module_desc &m = d->modules[i];
         if (m.kind == CRP_MODULE_PROPAGATION) {
@@ -213,7 +207,7 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b) {
         } else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
             AbstractCondition *c;
             if (m.per_candidate_length)
-                c = new PerCandidateLength();
+                c = h ? h->perCandidateLength() : new PerCandidateLength();
             else
                 c = new MaximumTrajectoryLength(m.max_length);
             if (m.record) c->onReject(new RecordAction(rec, i));
@@ -228,17 +222,64 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b) {
                 o->add(new ObserverDetectAll());
             o->setDeactivateOnDetection(m.deactivate_on_detection != 0);
             o->setFlag("Detected", "Detected");
-            if (m.record) o->onDetection(new RecordAction(rec, i));
+            if (text_output)
+                o->onDetection(new TextOutput(text_output, (Output::OutputType)text_type));
+            else if (m.record)
+                o->onDetection(new RecordAction(rec, i));
             b.sim->add(o);
         } else {
             throw std::runtime_error("ref_shim: unknown module kind");
         }
     }
-    b.counter = new StepCounter();
-    b.sim->add(b.counter.get());
+    if (count_steps) {
+        b.counter = new StepCounter();
+        b.sim->add(b.counter.get());
+    }
 }
 
-}  // namespace
+void load_candidates(const crp_candidates *c, uint64_t n, ModuleList::candidate_vector_t &cands) {
+    cands.clear();
+    cands.reserve(n);
+    for (uint64_t i = 0; i < n; i++) {
+        ref_ptr<Candidate> cand = new Candidate(
+            c->id[i], c->energy[i], Vector3d(c->x[i], c->y[i], c->z[i]),
+            Vector3d(c->dx[i], c->dy[i], c->dz[i]));
+        cand->previous.setPosition(Vector3d(c->px[i], c->py[i], c->pz[i]));
+        cand->setTrajectoryLength(c->trajectory_length[i]);
+        cand->setTime(c->time[i]);
+        cand->setNextStep(c->next_step[i]);
+        cand->setActive(c->active[i] != 0);
+        cand->setProperty("CrpIndex", Variant((uint64_t)i));
+        if (c->max_length)
+            cand->setProperty("CrpMaxLength", Variant(c->max_length[i]));
+        cands.push_back(cand);
+    }
+}
+
+void store_candidates(const ModuleList::candidate_vector_t &cands, const crp_candidates *c) {
+    for (uint64_t i = 0; i < cands.size(); i++) {
+        Candidate *cand = cands[i];
+        const Vector3d &p = cand->current.getPosition();
+        const Vector3d &d = cand->current.getDirection();
+        const Vector3d &q = cand->previous.getPosition();
+        c->x[i] = p.x; c->y[i] = p.y; c->z[i] = p.z;
+        c->dx[i] = d.x; c->dy[i] = d.y; c->dz[i] = d.z;
+        c->px[i] = q.x; c->py[i] = q.y; c->pz[i] = q.z;
+        c->trajectory_length[i] = cand->getTrajectoryLength();
+        c->time[i] = cand->getTime();
+        c->current_step[i] = cand->getCurrentStep();
+        c->next_step[i] = cand->getNextStep();
+        c->active[i] = cand->isActive() ? 1 : 0;
+        uint32_t fl = 0;
+        if (cand->hasProperty("Rejected")) fl |= CRP_FLAG_REJECTED;
+        if (cand->hasProperty("Detected")) fl |= CRP_FLAG_DETECTED;
+        c->flags[i] = fl;
+    }
+}
+
+}  // namespace crp_ref
+
+using namespace crp_ref;
 
 extern "C" {
 
@@ -254,23 +295,9 @@ int ref_run(const crp_plan_desc *desc, const crp_candidates *c, uint64_t n,
     try {
         ensure_data_path();
         Built b;
-        build_chain(desc, rec, b);
+        build_chain(desc, rec, b, 0, 0, true, 0, 0);
         ModuleList::candidate_vector_t cands;
-        cands.reserve(n);
-        for (uint64_t i = 0; i < n; i++) {
-            ref_ptr<Candidate> cand = new Candidate(
-                c->id[i], c->energy[i], Vector3d(c->x[i], c->y[i], c->z[i]),
-                Vector3d(c->dx[i], c->dy[i], c->dz[i]));
-            cand->previous.setPosition(Vector3d(c->px[i], c->py[i], c->pz[i]));
-            cand->setTrajectoryLength(c->trajectory_length[i]);
-            cand->setTime(c->time[i]);
-            cand->setNextStep(c->next_step[i]);
-            cand->setActive(c->active[i] != 0);
-            cand->setProperty("CrpIndex", Variant((uint64_t)i));
-            if (c->max_length)
-                cand->setProperty("CrpMaxLength", Variant(c->max_length[i]));
-            cands.push_back(cand);
-        }
+        load_candidates(c, n, cands);
         if (nthreads > 0) omp_set_num_threads(nthreads);
         Random::seedThreads(seed);
         // ModuleList::run prints a thread-count banner on stdout; keep
@@ -284,24 +311,38 @@ int ref_run(const crp_plan_desc *desc, const crp_candidates *c, uint64_t n,
         std::cout.rdbuf(old);
         if (seconds) *seconds = t1 - t0;
         if (steps) *steps = b.counter->total();
-        for (uint64_t i = 0; i < n; i++) {
-            Candidate *cand = cands[i];
-            const Vector3d &p = cand->current.getPosition();
-            const Vector3d &d = cand->current.getDirection();
-            const Vector3d &q = cand->previous.getPosition();
-            c->x[i] = p.x; c->y[i] = p.y; c->z[i] = p.z;
-            c->dx[i] = d.x; c->dy[i] = d.y; c->dz[i] = d.z;
-            c->px[i] = q.x; c->py[i] = q.y; c->pz[i] = q.z;
-            c->trajectory_length[i] = cand->getTrajectoryLength();
-            c->time[i] = cand->getTime();
-            c->current_step[i] = cand->getCurrentStep();
-            c->next_step[i] = cand->getNextStep();
-            c->active[i] = cand->isActive() ? 1 : 0;
-            uint32_t fl = 0;
-            if (cand->hasProperty("Rejected")) fl |= CRP_FLAG_REJECTED;
-            if (cand->hasProperty("Detected")) fl |= CRP_FLAG_DETECTED;
-            c->flags[i] = fl;
+        store_candidates(cands, c);
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/* The same run with a TextOutput(path, output_type) as every observer's
+ * detection action (Observer::onDetection, Observer.cpp:22) instead of the
+ * record action; serial numbers start at serial0 (Candidate.h:170). */
+int ref_run_textout(const crp_plan_desc *desc, const crp_candidates *c, uint64_t n,
+                    const char *path, int output_type, int nthreads, uint32_t seed,
+                    uint64_t serial0) {
+    try {
+        ensure_data_path();
+        Built b;
+        {
+            build_chain(desc, 0, b, 0, 0, false, path, output_type);
+            Candidate::setNextSerialNumber(serial0);
+            ModuleList::candidate_vector_t cands;
+            load_candidates(c, n, cands);
+            if (nthreads > 0) omp_set_num_threads(nthreads);
+            Random::seedThreads(seed);
+            std::streambuf *old = std::cout.rdbuf();
+            std::ostringstream sink;
+            std::cout.rdbuf(sink.rdbuf());
+            b.sim->run(&cands, true, false);
+            std::cout.rdbuf(old);
+            store_candidates(cands, c);
         }
+        b.sim = 0;  // closes the TextOutput files
         return 0;
     } catch (std::exception &e) {
         g_error = e.what();
@@ -314,7 +355,7 @@ int ref_field_eval(const crp_plan_desc *desc, uint64_t n, const double *pos, dou
     try {
         ensure_data_path();
         Built b;
-        ref_ptr<MagneticField> f = build_field(desc, b);
+        ref_ptr<MagneticField> f = build_field(desc, b, 0);
         for (uint64_t i = 0; i < n; i++) {
             Vector3d B = f->getField(Vector3d(pos[i], pos[n + i], pos[2 * n + i]));
             out[i] = B.x; out[n + i] = B.y; out[2 * n + i] = B.z;
