@@ -178,10 +178,14 @@ __device__ __forceinline__ f3 field_at(const DevPlan &P, double x, double y, dou
     return b;
 }
 
+// Candidate::setCurrentStep (Candidate.cpp:92): the time increment s / c is
+// taken as s times the correctly rounded 1 / c (within one ulp of the
+// increment; the FP64 form divides).
+constexpr double kInvCLight = 1.0 / kCLight;
 __device__ __forceinline__ void set_current_step(Cand &c, double s) {
     c.cur = s;
     c.len += s;
-    c.time += s / kCLight;
+    c.time = fma(s, kInvCLight, c.time);
 }
 
 // Renormalise an FP64 direction that is within rounding of unit length:
@@ -225,11 +229,12 @@ struct BP {
             return;
         }
         double newStep = step;
-        // t = B * q / 2 / m * step / c with m = E/c^2  ->  B * (q c step / (2 E))
-        const double kq = q * kCLight / (2.0 * c.E);
+        // t = B * q / 2 / m * step / c with m = E/c^2  ->  B * (q c step / (2 E)),
+        // formed in FP32 like the rotation it scales
+        const float kq = __fdividef((float)(q * (0.5 * kCLight)), (float)c.E);
         double xo = c.x, yo = c.y, zo = c.z, uxo = c.dx, uyo = c.dy, uzo = c.dz;
         if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
-            bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, (float)(kq * step), &c);
+            bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, kq * (float)step, &c);
             sc.tries++; sc.evals++;
         } else {
             step = clipd(c.next, m.min_step, m.max_step);
@@ -237,9 +242,10 @@ struct BP {
             for (int guard = 0; guard < 4096; guard++) {
                 double x1 = c.x, y1 = c.y, z1 = c.z, u1x = c.dx, u1y = c.dy, u1z = c.dz;
                 double x2 = c.x, y2 = c.y, z2 = c.z, u2x = c.dx, u2y = c.dy, u2z = c.dz;
-                bp_dy<FS>(P, x1, y1, z1, u1x, u1y, u1z, step, (float)(kq * step), &c);
-                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2), &c);
-                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, (float)(kq * step / 2), &c);
+                const float kts = kq * (float)step;
+                bp_dy<FS>(P, x1, y1, z1, u1x, u1y, u1z, step, kts, &c);
+                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, 0.5f * kts, &c);
+                bp_dy<FS>(P, x2, y2, z2, u2x, u2y, u2z, step / 2, 0.5f * kts, &c);
                 sc.tries++; sc.evals += 3;
                 double ex = x1 - x2, ey = y1 - y2, ez = z1 - z2;
                 double S = sqrt(ex * ex + ey * ey + ez * ez) / (step * 0.75);
@@ -334,17 +340,17 @@ struct CK {
             c.next = m.max_step;
             return;
         }
-        const float qc2E = (float)(c.q * kCLight * kCLight / c.E);
+        const float qc2E = __fdividef((float)(c.q * (kCLight * kCLight)), (float)c.E);
         double ddx, ddy, ddz, dux, duy, duz;
         double newStep = step;
         if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
-            ck_try<FS>(P, c, step / kCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
+            ck_try<FS>(P, c, step * kInvCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
             sc.tries++; sc.evals += 6;
         } else {
             step = clipd(c.next, m.min_step, m.max_step);
             newStep = step;
             for (int guard = 0; guard < 4096; guard++) {
-                double err = ck_try<FS>(P, c, step / kCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
+                double err = ck_try<FS>(P, c, step * kInvCLight, qc2E, ddx, ddy, ddz, dux, duy, duz);
                 sc.tries++; sc.evals += 6;
                 double r = err / m.tolerance;
                 if (r > 1) {
@@ -416,7 +422,7 @@ template <int FS>
 struct SDE {
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
-        double h = clipd(c.next, m.min_step, m.max_step) / kCLight;
+        double h = clipd(c.next, m.min_step, m.max_step) * kInvCLight;
         if (c.q == 0) {
             c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
             set_current_step(c, h * kCLight);
@@ -430,7 +436,7 @@ struct SDE {
         double eta0 = s_norm(s), eta1 = s_norm(s), eta2 = s_norm(s);
         double TStep = BT0 * eta0, NStep = BT4 * eta1, BStep = BT4 * eta2;
         double sh = sqrt(h);
-        double propTime = TStep * sh / kCLight;
+        double propTime = TStep * sh * kInvCLight;
         unsigned counter = 0;
         double r, ox, oy, oz, err;
         do {
@@ -439,9 +445,9 @@ struct SDE {
             r = err / m.tolerance;
             propTime *= 0.5;
             counter += 1;
-        } while (r > 1 && fabs(propTime) >= m.min_step / kCLight && counter < 60);
+        } while (r > 1 && fabs(propTime) >= m.min_step * kInvCLight && counter < 60);
         unsigned long long stepNumber = 1ull << (counter - 1);
-        double allowedTime = TStep * sh / kCLight / (double)stepNumber;
+        double allowedTime = TStep * sh * kInvCLight / (double)stepNumber;
         double sx = c.x, sy = c.y, sz = c.z;
         for (unsigned long long j = 0; j < stepNumber; j++) {
             sde_try<FS>(P, sx, sy, sz, allowedTime, ox, oy, oz, err, &c);
