@@ -34,6 +34,7 @@ import numpy as np  # noqa: E402
 METRIC = "particle-steps/s, 1 B200: mixed-prec vs FP64 at stated error; adjoint cost/fwd"
 UNIT = "particle-steps/s"
 ALGO_BYTES_PER_STEP = 96  # 8 corners x 12 B Grid3f payload per field evaluation
+TRAFFIC_B_PER_STEP = 27.3  # DRAM read+write per particle-step of the mixed kernel (ncu)
 
 
 def log(*a):
@@ -50,8 +51,13 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons during the timed region:
+    NVML polled every 20 ms from a thread (nvidia-smi -lms 200 if NVML is
+    unavailable)."""
 
+    # nvmlClocksEventReason* bits
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -59,8 +65,46 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.samples, self.max_mhz, self.reasons = [], None, set()
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self):
+        nv, h = self._nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for b, name in self.REASONS.items():
+                    if bits & b:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.02)
 
     def __enter__(self):
+        try:
+            self._nvml = self._handle()
+            nv, h = self._nvml
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+            return self
+        except Exception:
+            self._nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
@@ -71,7 +115,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -79,25 +125,25 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for l in out.splitlines():
+                f = [x.strip() for x in l.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.samples.append(float(f[1]))
+                    self.max_mhz = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        self.reasons.add(n)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = self.samples
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(sm),
+                "source": "nvml 20 ms" if self._nvml else "nvidia-smi 200 ms"}
 
 
 def setup_dist(args):
@@ -115,12 +161,34 @@ def setup_dist(args):
 
 
 def max_over_ranks(x, world):
+    """Max of a per-rank scalar over the process group (NCCL: on the GPU;
+    gloo: on the host)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_local, ms_local, world):
+    """Whole-job rate of N independent replicas (weak scaling): the units all
+    ranks processed over the slowest rank's device time."""
+    ms_max = max_over_ranks(ms_local, world)
+    units = units_local if world == 1 else int(round(sum_over_ranks(units_local, world)))
+    return units / (ms_max / 1e3), ms_max, units
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -271,6 +339,117 @@ def adjoint_cost(dev, args):
             "forward_particle_steps_per_s": n * steps / (f_ms / 1e3)}
 
 
+def _timed_runs(plan, d_init, d_work, repeats, **kw):
+    """Reset the device state from d_init and run the plan `repeats` times
+    after one warm-up; device time of the stepping launches (CUDA events
+    inside crp_run_device), totals over the timed runs."""
+    def once():
+        for name in d_work.MEMBERS:
+            a = getattr(d_work, name)
+            if a is not None:
+                a.copy_(getattr(d_init, name))
+        return plan.run(d_work, **kw)
+    once()
+    tot = {"particle_steps": 0, "tries": 0, "field_evaluations": 0, "launches": 0, "device_ms": 0.0}
+    for _ in range(repeats):
+        st = once()
+        for k in tot:
+            tot[k] += getattr(st, k)
+    return tot
+
+
+def secondary_configs(dev, peaks):
+    """The other stepping configurations, each timed on the device after a
+    warm-up, on bounded samples of the workload where a full run is out of
+    reach (per-candidate step caps, stated).  Roofline bases: 576 B of Grid3f
+    payload per Cash-Karp try (6 evaluations x 8 corners x 12 B) against the
+    measured L2 bandwidth for the L2-resident 64^3 grid; for plane-wave
+    stepping one hardware cosine per mode per field evaluation against the
+    measured cosine throughput."""
+    out = {}
+    out.update(cfg_grid_ck_64(dev, peaks))
+    out.update(cfg_grid_ck_nuclei(dev, peaks))
+    out.update(cfg_sde_galactic(dev, peaks))
+    return out
+
+
+def cfg_grid_ck_64(dev, peaks, n=10_000):
+    """PropagationCK over the 64^3 grid (3.1 MB, L2-resident), full runs."""
+    from crpropa3_b200 import _abi, engine, workloads as W
+    out = {}
+    for prec, name in ((_abi.PRECISION_FP64, "fp64"), (_abi.PRECISION_MIXED, "mixed")):
+        spec, cands, grid = W.grid_ck_64(n=n, precision=prec, device=dev)
+        plan = engine.Plan(spec)
+        t = _timed_runs(plan, cands.to_device(dev), cands.to_device(dev), 3)
+        tries_s = t["tries"] / (t["device_ms"] / 1e3)
+        gbs = 576 * tries_s / 1e9
+        out.setdefault("grid_ck_64", {
+            "workload": f"{n} protons 1-100 EeV, 64^3 Grid3f 1 nG 10 kpc, PropagationCK 1e-4 "
+                        "0.1-10 kpc, MaximumTrajectoryLength 10 Mpc, full runs",
+            "note": "10^4 candidates fill 79 of the 148 SMs (one thread per candidate)"})[name] = {
+            "tries_per_s": tries_s, "particle_steps_per_s": t["particle_steps"] / (t["device_ms"] / 1e3),
+            "ms_per_run": t["device_ms"] / 3,
+            "roofline": {"bound": "l2", "achieved": gbs, "peak": peaks.get("l2_gbs"), "unit": "GB/s",
+                         "frac": gbs / peaks["l2_gbs"] if peaks.get("l2_gbs") else None,
+                         "basis": "576 B per Cash-Karp try"}}
+        plan.close()
+        del grid
+    return out
+
+
+def cfg_grid_ck_nuclei(dev, peaks, n3=4_000_000, cap3=512):
+    """PropagationCK, 4 species, E^-2, per-candidate lengths, 256^3 grid:
+    chunked launches vs the autotuned persistent refill kernel."""
+    from crpropa3_b200 import _abi, engine, workloads as W
+    out = {}
+    spec, cands, grid = W.grid_ck_nuclei(n=n3, device=dev)
+    plan = engine.Plan(spec)
+    d_init, d_work = cands.to_device(dev), cands.to_device(dev)
+    chunked = _timed_runs(plan, d_init, d_work, 2, mode=_abi.MODE_CHUNKED, max_steps=cap3)
+    tune = plan.autotune(d_init, sample_n=1 << 18, steps_per_candidate=128)
+    auto = _timed_runs(plan, d_init, d_work, 2, mode=_abi.MODE_AUTO, max_steps=cap3)
+    rate = lambda t: t["tries"] / (t["device_ms"] / 1e3)
+    out["grid_ck_nuclei"] = {
+        "workload": f"{n3} candidates (H, He-4, N-14, Fe-56), E^-2 0.1-100 EeV, 256^3 Grid3f, "
+                    f"PropagationCK 1e-4 0.1-100 kpc, lengths U[1,50] Mpc; at most {cap3} steps "
+                    "per candidate (full runs reach 5e5 steps)",
+        "chunked_tries_per_s": rate(chunked),
+        "autotuned_tries_per_s": rate(auto),
+        "autotuned": {"mode": int(tune.mode), "ctas_per_sm": int(tune.ctas_per_sm),
+                      "refill_threshold": int(tune.refill_threshold), "burst": int(tune.burst)},
+        "roofline": {"bound": "hbm", "achieved": 576 * rate(auto) / 1e9, "unit": "GB/s",
+                     "basis": "576 B per Cash-Karp try"}}
+    plan.close()
+    del d_init, d_work, grid
+    return out
+
+
+def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
+    """DiffusionSDE, toroidal field + 1024-mode plane waves."""
+    import torch
+    from crpropa3_b200 import engine, workloads as W
+    out = {}
+    spec, cands = W.sde_galactic(n=n5)
+    plan = engine.Plan(spec)
+    t = _timed_runs(plan, cands.to_device(dev), cands.to_device(dev), 2, max_steps=cap5)
+    secs = t["device_ms"] / 1e3
+    mode_evals = t["field_evaluations"] * 1024
+    cos_s = mode_evals / secs
+    out["sde_galactic"] = {
+        "workload": f"{n5} protons 1 TeV-1 PeV, DiffusionSDE (1e-4, 0.1-100 pc, eps 0.1), "
+                    f"1 muG toroidal + PlaneWaveTurbulence 1024 modes 0.5 muG 1-100 pc, "
+                    f"absorbing sphere 20 kpc; {cap5} steps per candidate (full runs ~1e5)",
+        "particle_steps_per_s": t["particle_steps"] / secs,
+        "field_evaluations_per_s": t["field_evaluations"] / secs,
+        "mode_evaluations_per_s": cos_s,
+        "roofline": {"bound": "sfu", "achieved": cos_s / 1e9, "peak": peaks.get("cos_gops"),
+                     "unit": "Gcos/s", "frac": cos_s / 1e9 / peaks["cos_gops"] if peaks.get("cos_gops") else None,
+                     "basis": "one hardware cosine per mode per field evaluation"}}
+    plan.close()
+    torch.cuda.synchronize()
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -285,6 +464,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=0)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the secondary configurations")
     ap.add_argument("--uniform-start", action="store_true",
                     help="start candidates uniformly over the grid volume (profiling case)")
     args = ap.parse_args()
@@ -296,6 +476,20 @@ def main():
     torch.cuda.set_device(local)
     from crpropa3_b200 import _abi, engine, units as U, workloads as W
     from crpropa3_b200.state import CandidateArrays
+
+    if args.workload != "grid_bp_256":
+        # one secondary configuration alone (profiling runs), one JSON line
+        dev = f"cuda:{local}"
+        runs = {"grid_ck_64": lambda: cfg_grid_ck_64(dev, {}, n=args.n or 10_000),
+                "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or 4_000_000),
+                "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20))}
+        if args.workload not in runs:
+            log(f"unknown workload {args.workload}")
+            return 2
+        res = runs[args.workload]()
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, **res}))
+        return 0
 
     n = args.n or 1_000_000
     dev = f"cuda:{local}"
@@ -320,9 +514,17 @@ def main():
             if a is not None:
                 a.copy_(getattr(d_init, name))
 
+    # every stepping launch of the process, per form, for comparison with the
+    # ncu launch list of the same command (profiles/launches_grid_bp_256.md)
+    kernel_time = {"mixed_chunk_kernel<BPFixed>": [0, 0.0], "fp64_chunk_kernel<BPFixed>": [0, 0.0]}
+
     def one_step(plan):
         reset()
-        return plan.run(d_work)
+        st = plan.run(d_work)
+        k = kernel_time["mixed_chunk_kernel<BPFixed>" if plan is plan_mx else "fp64_chunk_kernel<BPFixed>"]
+        k[0] += st.launches
+        k[1] += st.device_ms
+        return st
 
     # warm-up (both forms)
     for _ in range(args.warmup):
@@ -347,9 +549,7 @@ def main():
         torch.cuda.synchronize()
     barrier(world)
     ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms, world)
-    total_steps = steps_mx * world  # weak scaling: each rank its own batch
-    value = total_steps / (ms_max / 1e3)
+    value, ms_max, total_steps = replica_rate(steps_mx, ms, world)
     final_mx = d_work.to_host()
 
     # ---- FP64 form
@@ -365,8 +565,7 @@ def main():
         kernel64_ms += st.device_ms
     ev1.record()
     torch.cuda.synchronize()
-    ms64 = max_over_ranks(ev0.elapsed_time(ev1), world)
-    value_64 = steps_64 * world / (ms64 / 1e3)
+    value_64, ms64, _ = replica_rate(steps_64, ev0.elapsed_time(ev1), world)
     final_64 = d_work.to_host()
 
     # per-candidate error of the mixed form against the FP64 form, beside the
@@ -418,10 +617,11 @@ def main():
         t1 = time.perf_counter()
         st = plan_mx.run(h_work)
         t2 = time.perf_counter()
+        kernel_time["mixed_chunk_kernel<BPFixed>"][0] += st.launches
+        kernel_time["mixed_chunk_kernel<BPFixed>"][1] += st.device_ms
         e2e_steps += st.particle_steps
         e2e_s += t2 - t1
-    e2e_s = max_over_ranks(e2e_s, world)
-    e2e_value = e2e_steps * world / e2e_s
+    e2e_value, _, _ = replica_rate(e2e_steps, e2e_s * 1e3, world)
     # inputs: every member; outputs: the members crp_run copies back
     out_members = ["x", "y", "z", "dx", "dy", "dz", "px", "py", "pz", "trajectory_length", "time",
                    "current_step", "next_step", "flags", "active"]
@@ -430,11 +630,25 @@ def main():
     # ---- roofline of the stepping kernel (device_ms = CUDA events around its launches)
     peak, peak_kind = measured_peaks()
     achieved = ALGO_BYTES_PER_STEP * steps_mx / (kernel_ms / 1e3) / 1e9
+    # DRAM bytes per particle-step of this kernel from ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum), scaled to the steps of an average timed launch
+    traffic = TRAFFIC_B_PER_STEP * steps_mx / max(launches, 1)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                "basis": "96 B (8 corners x 12 B) per particle-step over the stepping kernel time"}
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "basis": "96 B (8 corners x 12 B) per particle-step over the stepping kernel time",
+                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step measured by ncu "
+                                 "(profiles/mixed_chunk_kernel_bp_fixed_grid256_n131072.md) x "
+                                 "particle-steps per timed launch"}
 
     adjoint = None if args.no_adjoint else adjoint_cost(dev, args)
+
+    peaks = {}
+    try:
+        from crpropa3_b200 import peaks as PK
+        peaks = PK.measure()
+    except Exception as e:  # the headline does not depend on these
+        log(f"[bench] peaks not measured: {e}")
+    configs = None if (args.no_configs or world > 1) else secondary_configs(dev, peaks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -473,8 +687,11 @@ def main():
                     "d2h_bytes_per_step": d2h, "api": "crp_run (host arrays, pinned)"},
             "roofline": roofline,
             "adjoint": adjoint,
+            "configs": configs,
+            "measured_peaks": dict(peaks, hbm_gbs=peak, hbm_source=peak_kind) if peaks else None,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
+            "kernel_time": {k: {"launches": v[0], "device_ms": v[1]} for k, v in kernel_time.items()},
             "clocks": clk.summary(),
         }
         print(json.dumps(line))

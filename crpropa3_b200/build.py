@@ -19,6 +19,8 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OBJ = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "lib", "libcrp_b200.so")
+# microbenchmarks of the roofline denominators (benchmark only)
+PEAKS_LIB = os.path.join(PKG, "lib", "libcrp_peaks.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
@@ -34,6 +36,7 @@ SOURCES = {
     "noalloc.cu": [],
     "host_tools.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }
+PEAKS_SOURCES = {"peaks.cu": []}
 LINK_LIBS = ["-lcufft"]
 
 
@@ -72,13 +75,19 @@ def build(verbose: bool = False) -> str:
     present = {s: f for s, f in SOURCES.items() if os.path.exists(os.path.join(CSRC, s))}
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda kv: _compile(nvcc, kv[0], kv[1], verbose), present.items()))
-    if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
-        return LIB
-    cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-L/usr/local/cuda/lib64"] + LINK_LIBS
+        pobjs = list(ex.map(lambda kv: _compile(nvcc, kv[0], kv[1], verbose), PEAKS_SOURCES.items()))
+    _link(nvcc, LIB, objs, LINK_LIBS)
+    _link(nvcc, PEAKS_LIB, pobjs, [])
+    return LIB
+
+
+def _link(nvcc, lib, objs, libs):
+    if os.path.exists(lib) and all(os.path.getmtime(lib) >= os.path.getmtime(o) for o in objs):
+        return
+    cmd = [nvcc] + ARCH + ["-shared", "-o", lib] + objs + ["-L/usr/local/cuda/lib64"] + libs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"link failed:\n{r.stderr[-6000:]}")
-    return LIB
+        raise RuntimeError(f"link of {os.path.basename(lib)} failed:\n{r.stderr[-6000:]}")
 
 
 if __name__ == "__main__":

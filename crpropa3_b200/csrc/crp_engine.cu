@@ -66,6 +66,12 @@ struct crp_plan {
     DevCounters *d_cnt = nullptr;
     DevCounters *h_cnt = nullptr;  // pinned
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // persistent mode: device work queue, its pinned host mirror, and the
+    // stream the launch graphs are captured on and run in
+    DevQueue *d_queue = nullptr;
+    DevQueue *h_queue = nullptr;
+    cudaStream_t gstream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     // device copies for crp_run() on host arrays
     uint64_t scratch_n = 0;
     void *scratch = nullptr;
@@ -93,6 +99,11 @@ struct crp_plan {
         if (trial) cudaFree(trial);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (d_queue) cudaFree(d_queue);
+        if (h_queue) cudaFreeHost(h_queue);
+        if (gstream) cudaStreamDestroy(gstream);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
     }
 };
 
@@ -405,6 +416,58 @@ static crp_status ensure_lists(crp_plan *p, uint64_t n) {
 // Persistent mode: bounded launches of SMs x ctas_per_sm CTAs that refill
 // lanes from the device queue; what a launch leaves (lanes still busy at its
 // time budget, queue items not yet taken) is the next launch's queue.
+// Bookkeeping between two persistent launches, captured with them: pending
+// items no lane took are appended behind the launch's new pending list
+// (carry_kernel, all threads), then the queue advances and the launch's
+// counters are added to the run totals and cleared (advance_kernel, one
+// thread).
+__global__ void carry_kernel(const DevQueue *q, const DevCounters *cnt, uint32_t *la, uint32_t *lb) {
+    const unsigned long long total = q->n_pending + q->n_main;
+    const unsigned long long consumed = cnt->queue_head < total ? cnt->queue_head : total;
+    if (consumed >= q->n_pending) return;
+    const unsigned long long rest = q->n_pending - consumed, base = cnt->pending_count;
+    const uint32_t *pin = q->cur ? lb : la;
+    uint32_t *pout = q->cur ? la : lb;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < rest; i += stride)
+        pout[base + i] = pin[consumed + i];
+}
+
+__global__ void advance_kernel(DevQueue *q, DevCounters *cnt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const unsigned long long total = q->n_pending + q->n_main;
+    const unsigned long long consumed = cnt->queue_head < total ? cnt->queue_head : total;
+    unsigned long long next_pending = cnt->pending_count;
+    if (consumed < q->n_pending) {
+        next_pending += q->n_pending - consumed;
+    } else {
+        q->main_base += consumed - q->n_pending;
+        q->n_main -= consumed - q->n_pending;
+    }
+    q->n_pending = next_pending;
+    q->cur ^= 1u;
+    q->remaining = q->n_pending + q->n_main;
+    q->steps += cnt->steps;
+    q->tries += cnt->tries;
+    q->field_evals += cnt->field_evals;
+    if (total > 0) q->launches++;
+    cnt->steps = cnt->tries = cnt->field_evals = 0;
+    cnt->queue_head = cnt->pending_count = cnt->active_left = 0;
+}
+
+static crp_status ensure_graph_resources(crp_plan *p) {
+    if (!p->d_queue) CUDA_TRY(cudaMalloc(&p->d_queue, sizeof(DevQueue)));
+    if (!p->h_queue) CUDA_TRY(cudaMallocHost(&p->h_queue, sizeof(DevQueue)));
+    if (!p->gstream) CUDA_TRY(cudaStreamCreateWithFlags(&p->gstream, cudaStreamNonBlocking));
+    if (!p->ev_in) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
+    if (!p->ev_out) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+    return CRP_OK;
+}
+
+// Persistent launches of this many rounds (launch, carry, advance) form one
+// CUDA graph; the host looks at the queue once per graph.
+constexpr int kRoundsPerGraph = 8;
+
 static crp_status run_persistent(crp_plan *p, const crp_candidates *c, uint64_t n,
                                  const crp_run_opts &o, crp_run_stats *stats) {
     cudaStream_t st = (cudaStream_t)o.stream;
@@ -416,61 +479,76 @@ static crp_status run_persistent(crp_plan *p, const crp_candidates *c, uint64_t 
     if (ctas > 32 || refill > 32) return fail(CRP_ERR_INVALID_ARGUMENT, "ctas_per_sm and refill_threshold must be <= 32");
     crp_status ls = ensure_lists(p, n);
     if (ls) return ls;
+    ls = ensure_graph_resources(p);
+    if (ls) return ls;
     const int grid = p->num_sms * ctas;
-    uint32_t *list_a = p->lists, *list_b = p->lists + p->list_cap;
-    const uint32_t *pending_in = nullptr;
-    uint32_t *pending_out = list_a;
-    uint64_t n_pending = 0, main_base = 0, n_main = n;
-    double ms_total = 0;
-    uint64_t launches = 0;
     const unsigned long long budget_ns =
-        o.budget_us > 0 ? 1000ull * (unsigned long long)o.budget_us : 200ull * 1000 * 1000;
-    for (;;) {
-        PersistentArgs a{pending_in, n_pending, main_base, n_main, pending_out, burst, refill, budget_ns,
-                         o.max_steps};
-        CUDA_TRY(cudaMemsetAsync(p->d_cnt, 0, sizeof(DevCounters), st));
-        CUDA_TRY(cudaEventRecord(p->ev0, st));
-        cudaError_t e = (p->precision == CRP_PRECISION_FP64)
-            ? launch_fp64_persistent(p->dev, s, a, p->d_cnt, rec, p->fs, grid, st)
-            : launch_mixed_persistent(p->dev, s, a, p->d_cnt, rec, p->fs, grid, st);
-        if (e != cudaSuccess) return cuda_fail(e, "persistent stepping kernel launch");
-        CUDA_TRY(cudaEventRecord(p->ev1, st));
-        CUDA_TRY(cudaMemcpyAsync(p->h_cnt, p->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-        float ms = 0;
-        CUDA_TRY(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
-        ms_total += ms;
-        launches++;
-        if (stats) {
-            stats->particle_steps += p->h_cnt->steps;
-            stats->tries += p->h_cnt->tries;
-            stats->field_evaluations += p->h_cnt->field_evals;
-        }
-        const uint64_t total = n_pending + n_main;
-        const uint64_t consumed = p->h_cnt->queue_head < total ? p->h_cnt->queue_head : total;
-        uint64_t next_pending = p->h_cnt->pending_count;
-        if (consumed < n_pending) {
-            // pending items nobody took move behind the new pending list
-            const uint64_t rest = n_pending - consumed;
-            CUDA_TRY(cudaMemcpyAsync(pending_out + next_pending, pending_in + consumed,
-                                     sizeof(uint32_t) * rest, cudaMemcpyDeviceToDevice, st));
-            next_pending += rest;
-        } else {
-            main_base += consumed - n_pending;
-            n_main -= consumed - n_pending;
-        }
-        n_pending = next_pending;
-        pending_in = pending_out;
-        pending_out = (pending_out == list_a) ? list_b : list_a;
-        if (stats) stats->active_left = n_pending + n_main;
-        if (n_pending == 0 && n_main == 0) break;
-        if (o.cancel && *o.cancel) {
-            if (stats) { stats->launches = launches; stats->device_ms = ms_total; }
-            return fail(CRP_ERR_CANCELLED, "run cancelled by the host flag");
+        o.budget_us > 0 ? 1000ull * (unsigned long long)o.budget_us : 25ull * 1000 * 1000;
+    cudaStream_t gs = p->gstream;
+    // the graph stream follows the caller's stream
+    CUDA_TRY(cudaEventRecord(p->ev_in, st));
+    CUDA_TRY(cudaStreamWaitEvent(gs, p->ev_in, 0));
+    *p->h_queue = DevQueue{};
+    p->h_queue->n_main = n;
+    p->h_queue->remaining = n;
+    CUDA_TRY(cudaMemcpyAsync(p->d_queue, p->h_queue, sizeof(DevQueue), cudaMemcpyHostToDevice, gs));
+    CUDA_TRY(cudaMemsetAsync(p->d_cnt, 0, sizeof(DevCounters), gs));
+    CUDA_TRY(cudaStreamSynchronize(gs));  // h_queue is rewritten below
+
+    PersistentArgs a{p->d_queue, p->lists, p->lists + p->list_cap, burst, refill, budget_ns,
+                     o.max_steps};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaSuccess;
+    for (int r = 0; r < kRoundsPerGraph && ce == cudaSuccess; r++) {
+        ce = (p->precision == CRP_PRECISION_FP64)
+            ? launch_fp64_persistent(p->dev, s, a, p->d_cnt, rec, p->fs, grid, gs)
+            : launch_mixed_persistent(p->dev, s, a, p->d_cnt, rec, p->fs, grid, gs);
+        if (ce == cudaSuccess) {
+            carry_kernel<<<p->num_sms * 2, 256, 0, gs>>>(p->d_queue, p->d_cnt, a.list_a, a.list_b);
+            advance_kernel<<<1, 32, 0, gs>>>(p->d_queue, p->d_cnt);
+            ce = cudaGetLastError();
         }
     }
-    if (stats) { stats->launches = launches; stats->device_ms = ms_total; stats->active_left = 0; }
-    return CRP_OK;
+    cudaError_t ee = cudaStreamEndCapture(gs, &graph);
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(ce != cudaSuccess ? ce : ee, "capture of the persistent launch graph");
+    }
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_fail(ce, "instantiation of the persistent launch graph");
+
+    double ms_total = 0;
+    crp_status result = CRP_OK;
+    for (;;) {
+        cudaError_t e = cudaEventRecord(p->ev0, gs);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, gs);
+        if (e == cudaSuccess) e = cudaEventRecord(p->ev1, gs);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(p->h_queue, p->d_queue, sizeof(DevQueue), cudaMemcpyDeviceToHost, gs);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(gs);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+        if (e != cudaSuccess) { result = cuda_fail(e, "persistent launch graph"); break; }
+        ms_total += ms;
+        if (p->h_queue->remaining == 0) break;
+        if (o.cancel && *o.cancel) { result = fail(CRP_ERR_CANCELLED, "run cancelled by the host flag"); break; }
+    }
+    cudaGraphExecDestroy(exec);
+    if (stats) {
+        stats->particle_steps = p->h_queue->steps;
+        stats->tries = p->h_queue->tries;
+        stats->field_evaluations = p->h_queue->field_evals;
+        stats->launches = p->h_queue->launches;
+        stats->active_left = p->h_queue->remaining;
+        stats->device_ms = ms_total;
+    }
+    // the caller's stream follows the graph stream
+    CUDA_TRY(cudaEventRecord(p->ev_out, gs));
+    CUDA_TRY(cudaStreamWaitEvent(st, p->ev_out, 0));
+    return result;
 }
 
 crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,

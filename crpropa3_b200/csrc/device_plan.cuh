@@ -91,6 +91,19 @@ struct DevRecords {
 };
 
 // Run counters, accumulated with one atomic per warp.
+// Work queue of the persistent mode, in device memory so that a sequence of
+// persistent launches with their bookkeeping can be captured in one CUDA
+// graph: the pending list (candidates a launch left unfinished when its
+// time budget ran out) is list `cur` (0: a, 1: b); the untouched main range
+// is [main_base, main_base + n_main).  advance_kernel updates it between
+// launches and accumulates the run totals.
+struct DevQueue {
+    unsigned long long n_pending, main_base, n_main, remaining;
+    unsigned long long steps, tries, field_evals, launches;
+    unsigned int cur, pad;
+    unsigned long long pad2;
+};
+
 struct DevCounters {
     unsigned long long steps;
     unsigned long long tries;

@@ -18,20 +18,21 @@ enum FieldSig {
 };
 
 // Persistent stepping launch (chain.cuh persistent_body): `grid` CTAs of 128
-// threads take work from the virtual queue pending_in[0..n_pending) followed
-// by [main_base, main_base + n_main) until it is empty or budget_ns of
-// device time have passed.
+// threads take work from the virtual queue described by *q -- its pending
+// list (list_a or list_b, by q->cur) followed by its main range -- until it
+// is empty or budget_ns of device time have passed; unfinished candidates
+// go to the other list.  Kernel parameters are fixed for a whole run, so
+// the launches can be captured in a CUDA graph.
 struct PersistentArgs {
-    const uint32_t *pending_in;
-    uint64_t n_pending;
-    uint64_t main_base;
-    uint64_t n_main;
-    uint32_t *pending_out;
+    const DevQueue *q;
+    uint32_t *list_a;
+    uint32_t *list_b;
     int burst;
     int refill;
     unsigned long long budget_ns;
     uint64_t step_cap;
 };
+
 // step_fp64.cu
 // One launch of the chunked stepping kernel: threads t < n advance candidate
 // perm[t] (t without perm) by at most max_steps chain iterations; candidates

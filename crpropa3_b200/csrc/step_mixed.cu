@@ -528,19 +528,20 @@ __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_chunk_k
 
 template <template <int> class Prop, int FS>
 __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_persistent_kernel(
-    DevPlan P, DevState s, const uint32_t *pending_in, uint64_t n_pending, uint64_t main_base,
-    uint64_t n_main, uint32_t *pending_out, int burst, int refill, unsigned long long budget_ns,
-    uint64_t step_cap, DevCounters *cnt, DevRecords rec) {
-    persistent_body<Prop<FS>>(P, s, pending_in, n_pending, main_base, n_main, pending_out, burst,
-                              refill, budget_ns, step_cap, cnt, rec);
+    DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
+    // the queue is written only between launches (advance_kernel)
+    const DevQueue q = *a.q;
+    const uint32_t *pending_in = q.cur ? a.list_b : a.list_a;
+    uint32_t *pending_out = q.cur ? a.list_a : a.list_b;
+    persistent_body<Prop<FS>>(P, s, pending_in, q.n_pending, q.main_base, q.n_main, pending_out,
+                              a.burst, a.refill, a.budget_ns, a.step_cap, cnt, rec);
 }
 
 template <template <int> class Prop>
 cudaError_t launch_persistent_prop(const DevPlan &P, const DevState &s, const PersistentArgs &a,
                                    DevCounters *cnt, const DevRecords &rec, int fs, int grid,
                                    cudaStream_t st) {
-#define CRP_PERSIST(FSV) mixed_persistent_kernel<Prop, FSV><<<grid, 128, 0, st>>>(P, s, a.pending_in, \
-        a.n_pending, a.main_base, a.n_main, a.pending_out, a.burst, a.refill, a.budget_ns, a.step_cap, cnt, rec)
+#define CRP_PERSIST(FSV) mixed_persistent_kernel<Prop, FSV><<<grid, 128, 0, st>>>(P, s, a, cnt, rec)
     if (fs == FS_GRID) CRP_PERSIST(FS_GRID);
     else if (fs == FS_PLANE_WAVE) CRP_PERSIST(FS_PLANE_WAVE);
     else CRP_PERSIST(FS_GENERIC);

@@ -100,3 +100,37 @@ def grid_ck_nuclei(n=10_000_000, grid=None, precision=_abi.PRECISION_MIXED, devi
     rng = np.random.default_rng(seed)
     cands.max_length[:] = rng.uniform(1, 50, n) * U.Mpc
     return spec, cands, grid
+
+
+def plane_wave_modes(brms, lmin, lmax, lbendover, sindex, qindex, n_modes, seed):
+    """Wave modes of PlaneWaveTurbulence(TurbulenceSpectrum(...), n_modes, seed)
+    (PlaneWaveTurbulence.cpp:79) via crp_plane_wave_modes: xi, kappa (n, 3),
+    k, beta, Ak (n,)."""
+    lib = _abi.load()
+    xi, kappa = np.zeros(3 * n_modes), np.zeros(3 * n_modes)
+    k, beta, ak = np.zeros(n_modes), np.zeros(n_modes), np.zeros(n_modes)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    _abi.check(lib.crp_plane_wave_modes(brms, lmin, lmax, lbendover, sindex, qindex, n_modes, seed,
+                                        dp(xi), dp(kappa), dp(k), dp(beta), dp(ak)))
+    return xi.reshape(n_modes, 3), kappa.reshape(n_modes, 3), k, beta, ak
+
+
+def sde_galactic(n=10_000_000, n_modes=1024, precision=_abi.PRECISION_MIXED, seed=5,
+                 source=(8.5 * U.kpc, 0.0, 0.0)):
+    """DiffusionSDE (tolerance 1e-4, steps 0.1-100 pc, epsilon 0.1, alpha 1/3,
+    scale 1) in B = 1 muG (-y, x, 0)/r plus PlaneWaveTurbulence (n_modes
+    modes, Brms 0.5 muG, lMin 1 pc, lMax 100 pc, lBendover 1 pc, Kolmogorov,
+    mode seed 11); protons log-uniform 1 TeV - 1 PeV from `source`, absorbed
+    by an Observer sphere of 20 kpc around the origin."""
+    spectrum = (0.5 * U.muG, 1 * U.pc, 100 * U.pc, 1 * U.pc, 5.0 / 3.0, 4.0)
+    xi, kappa, k, beta, ak = plane_wave_modes(*spectrum, n_modes, 11)
+    fields = [P.ToroidalField(1 * U.muG),
+              P.PlaneWaveField(xi, kappa, k, beta, ak, spectrum=spectrum, seed=11)]
+    spec = P.ChainSpec(fields,
+                       [P.Propagation(_abi.PROP_SDE, 1e-4, 0.1 * U.pc, 100 * U.pc, epsilon=0.1,
+                                      alpha=1.0 / 3.0, scale=1.0),
+                        P.ObserverSpec(_abi.OBSERVER_SURFACE_SPHERE, (0.0, 0.0, 0.0), 20 * U.kpc,
+                                       True, False)],
+                       precision=precision, seed=seed)
+    cands = source_candidates(n, [IDS["H"]], 1 * U.TeV, 1000 * U.TeV, -1.0, seed, position=source)
+    return spec, cands

@@ -121,3 +121,27 @@ def test_autotune_then_auto_run():
     got = d.to_host()
     for m in STATE:
         np.testing.assert_array_equal(getattr(got, m), getattr(ref, m), err_msg=m)
+
+
+def test_persistent_graph_rounds_and_cancel():
+    """Persistent launches run as captured CUDA graphs of several rounds
+    (launch, carry-over, queue advance); the host flag is polled between
+    graphs: a raised flag ends the run with CRP_ERR_CANCELLED and the
+    candidates still to do are reported."""
+    import ctypes as C
+    from crpropa3_b200.engine import Plan
+    grid = random_grid(np.random.default_rng(68), 32, brms=1e-12)
+    c = _nuclei(20000, 69)
+    spec = _spec(grid, _abi.PRECISION_MIXED)
+    # many short rounds: a 50 us budget cuts every launch
+    got, st = _run(spec, c, mode=_abi.MODE_PERSISTENT, budget_us=50, ctas_per_sm=1)
+    ref, st0 = _run(spec, c, mode=_abi.MODE_CHUNKED)
+    for m in STATE:
+        np.testing.assert_array_equal(getattr(got, m), getattr(ref, m), err_msg=m)
+    assert st.launches > 8  # more than one graph of rounds
+    flag = C.c_int32(1)
+    plan = Plan(spec)
+    d = c.to_device("cuda")
+    with pytest.raises(_abi.CrpError) as e:
+        plan.run(d, mode=_abi.MODE_PERSISTENT, budget_us=50, ctas_per_sm=1, cancel=C.pointer(flag))
+    assert e.value.status == _abi.ERR_CANCELLED
