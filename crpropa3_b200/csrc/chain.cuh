@@ -93,6 +93,16 @@ struct Stream {
         default: return block.w;
         }
     }
+    // continue the stream at word w (as if w words had been drawn)
+    __device__ void seek(int w) {
+        cursor = w;
+        if (w & 3) {
+            uint64_t c = step * 4 + (uint64_t)(w >> 2);
+            block = philox4x32_10(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)cand,
+                                             (uint32_t)(cand >> 32)),
+                                  (uint32_t)seed, (uint32_t)(seed >> 32));
+        }
+    }
 };
 
 __device__ __forceinline__ void write_record(const DevRecords &rec, const Cand &c, int module) {

@@ -57,6 +57,8 @@ namespace crp {
 void set_last_error(const char *msg) { g_error = msg; }
 }  // namespace crp
 
+constexpr double kInv2Pi = 0.15915494309189533577;  // 1 / (2 pi)
+
 struct crp_plan {
     int device = 0;
     int precision = CRP_PRECISION_FP64;
@@ -211,12 +213,13 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             for (int a = 0; a < 3; a++) {
                 m9[9 * i + a] = w.xi[3 * i + a];
                 m9[9 * i + 3 + a] = w.kappa[3 * i + a];
-                kk[4 * i + a] = w.k[i] * w.kappa[3 * i + a];
+                // mixed form: phase in turns, k kappa / 2 pi
+                kk[4 * i + a] = w.k[i] * w.kappa[3 * i + a] * kInv2Pi;
             }
             m9[9 * i + 6] = w.k[i];
             m9[9 * i + 7] = w.beta[i];
             m9[9 * i + 8] = w.ak[i];
-            kk[4 * i + 3] = w.beta[i];
+            kk[4 * i + 3] = w.beta[i] * kInv2Pi;
             a32[i] = make_float4((float)(w.ak[i] * w.xi[3 * i]), (float)(w.ak[i] * w.xi[3 * i + 1]),
                                  (float)(w.ak[i] * w.xi[3 * i + 2]), 0.f);
         }

@@ -28,7 +28,7 @@ struct DevGrid {
 struct DevPlaneWave {
     const double *modes;   // FP64 form: per mode {xi x y z, kappa x y z, k, beta, Ak} (9 doubles)
     const float4 *modes32; // mixed form: per mode {k*kappa (FP64 split), Ak*xi} (see step_mixed.cu)
-    const double *kk;      // mixed form: per mode k*kappa as 3 doubles + beta (4 doubles)
+    const double *kk;      // mixed form: per mode k*kappa and beta in turns (over 2 pi), 4 doubles
     int n;
 };
 

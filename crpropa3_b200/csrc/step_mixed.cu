@@ -116,35 +116,46 @@ __device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
     return grid_field_t<false>(g, x, y, z, nullptr);
 }
 
-// PlaneWaveTurbulence sum: FP64 phase k*kappa.x + beta, reduced to
-// [-pi, pi] in FP64 (two-constant Cody-Waite), then FP32 hardware cosine
-// and FP32 accumulation.  Table per mode: kk = {k kappa_x, k kappa_y,
-// k kappa_z, beta} (FP64), modes32 = {Ak xi_x, Ak xi_y, Ak xi_z, 0} (FP32).
+// PlaneWaveTurbulence sum (PlaneWaveTurbulence.cpp:231).  The phase is
+// taken in turns, p = (k kappa . x + beta) / 2 pi, in FP64 (|p| reaches 1e4
+// turns at kpc distances and pc wavelengths, where FP32 would keep no
+// fraction); its fraction f = p - rint(p) is exact in FP64, and the FP32
+// hardware cosine takes 2 pi f.  Amplitudes A xi and the sums are FP32.
+// Table per mode: kk = {k kappa / 2 pi, beta / 2 pi} (FP64), modes32 =
+// {A xi, 0} (FP32).  Two accumulator sets halve the dependence chain of the
+// sums.
 __device__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double z) {
-    const double inv2pi = 0.15915494309189533577;
-    const double twopi_hi = 6.28318530717958623200, twopi_lo = 2.44929359829470635445e-16;
-    float bx = 0.f, by = 0.f, bz = 0.f;
+    const float twopi = 6.28318530717958647692f;
+    float bx0 = 0.f, by0 = 0.f, bz0 = 0.f, bx1 = 0.f, by1 = 0.f, bz1 = 0.f;
     const double2 *kk = reinterpret_cast<const double2 *>(w.kk);
+    const int n2 = w.n & ~1;
 #pragma unroll 4
-    for (int i = 0; i < w.n; i++) {
-        double2 m0 = __ldg(kk + 2 * i), m1 = __ldg(kk + 2 * i + 1);
-        float4 a = __ldg(w.modes32 + i);
-        double ph = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
-        double nr = rint(ph * inv2pi);
-        double red = fma(-nr, twopi_lo, fma(-nr, twopi_hi, ph));
-        float c = __cosf((float)red);
-        bx = fmaf(a.x, c, bx);
-        by = fmaf(a.y, c, by);
-        bz = fmaf(a.z, c, bz);
+    for (int i = 0; i < n2; i += 2) {
+        const double2 m0 = __ldg(kk + 2 * i), m1 = __ldg(kk + 2 * i + 1);
+        const double2 m2 = __ldg(kk + 2 * i + 2), m3 = __ldg(kk + 2 * i + 3);
+        const float4 a = __ldg(w.modes32 + i), b = __ldg(w.modes32 + i + 1);
+        const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
+        const double p1 = fma(m2.x, x, fma(m2.y, y, fma(m3.x, z, m3.y)));
+        const float c0 = __cosf(twopi * (float)(p0 - rint(p0)));
+        const float c1 = __cosf(twopi * (float)(p1 - rint(p1)));
+        bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
+        bx1 = fmaf(b.x, c1, bx1); by1 = fmaf(b.y, c1, by1); bz1 = fmaf(b.z, c1, bz1);
     }
-    return f3mk(bx, by, bz);
+    if (n2 < w.n) {
+        const double2 m0 = __ldg(kk + 2 * n2), m1 = __ldg(kk + 2 * n2 + 1);
+        const float4 a = __ldg(w.modes32 + n2);
+        const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
+        const float c0 = __cosf(twopi * (float)(p0 - rint(p0)));
+        bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
+    }
+    return f3mk(bx0 + bx1, by0 + by1, bz0 + bz1);
 }
 
 __device__ f3 component_field(const DevComponent &f, double x, double y, double z) {
     if (f.periodic) {
         double qx = x - f.po[0], qy = y - f.po[1], qz = z - f.po[2];
         double nx = floor(qx / f.pe[0]), ny = floor(qy / f.pe[1]), nz = floor(qz / f.pe[2]);
-        x = qx - nx * f.pe[0]; y = qy - ny * f.pe[1]; z = qz - nz * f.pe[2];
+        x = fma(-nx, f.pe[0], qx); y = fma(-ny, f.pe[1], qy); z = fma(-nz, f.pe[2], qz);
         if (f.periodic_reflective) {
             if ((long long)fabs(nx) % 2 == 1) x = f.pe[0] - x;
             if ((long long)fabs(ny) % 2 == 1) y = f.pe[1] - y;
@@ -156,7 +167,7 @@ __device__ f3 component_field(const DevComponent &f, double x, double y, double 
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z);
     case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
     default: {
-        double r = sqrt(x * x + y * y);
+        double r = sqrt(fma(x, x, y * y));
         double s = f.b0 / r;
         return f3mk((float)(-y * s), (float)(x * s), 0.f);
     }
@@ -380,7 +391,7 @@ struct CK {
 
 // ------------------------------------------------------------ DiffusionSDE
 __device__ __forceinline__ double s_rand(Stream &s) { return (double)s.next_u32() * (1.0 / 4294967295.0); }
-__device__ __forceinline__ double s_uniform(Stream &s, double a, double b) { return a + (b - a) * s_rand(s); }
+__device__ __forceinline__ double s_uniform(Stream &s, double a, double b) { return fma(b - a, s_rand(s), a); }
 __device__ __forceinline__ double s_norm(Stream &s) {
     double dblexc = ((double)s.next_u32() + 0.5) * (1.0 / 4294967296.0);
     double r = sqrt(-2.0 * log(1.0 - dblexc));
@@ -388,124 +399,283 @@ __device__ __forceinline__ double s_norm(Stream &s) {
     return r * cos(phi);
 }
 
-// Field-line trace of DiffusionSDE::tryStep (DiffusionSDE.cpp:233): unit B
-// stage directions in FP32, FP64 base position + FP32 offsets, FP64 error.
-template <int FS>
-__device__ __forceinline__ void sde_try(const DevPlan &P, double x, double y, double z, double t,
-                                        double &ox, double &oy, double &oz, double &err, Cand *cc) {
-    f3 k[6];
-    const float tc = (float)(t * kCLight);
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    double ex = 0, ey = 0, ez = 0;
-#pragma unroll
-    for (int i = 0; i < 6; i++) {
-        float ax = 0.f, ay = 0.f, az = 0.f;
-#pragma unroll
-        for (int j = 0; j < i; j++) {
-            float a = ck_af[i * 6 + j];
-            ax = fmaf(k[j].x, a, ax); ay = fmaf(k[j].y, a, ay); az = fmaf(k[j].z, a, az);
-        }
-        f3 B = field_at<FS>(P, x + (double)(ax * tc), y + (double)(ay * tc), z + (double)(az * tc), cc);
-        float inv = rsqrtf(B.x * B.x + B.y * B.y + B.z * B.z);
-        k[i] = f3mk(B.x * inv, B.y * inv, B.z * inv);
-        float b = ck_bf[i];
-        sx = fmaf(k[i].x, b, sx); sy = fmaf(k[i].y, b, sy); sz = fmaf(k[i].z, b, sz);
-        double e = ck_eb[i];
-        ex = fma((double)k[i].x, e, ex); ey = fma((double)k[i].y, e, ey); ez = fma((double)k[i].z, e, ez);
-    }
-    const double tcd = t * kCLight;
-    ox = x + (double)sx * tcd; oy = y + (double)sy * tcd; oz = z + (double)sz * tcd;
-    err = sqrt(ex * ex + ey * ey + ez * ez) * fabs(tcd) / CRP_KPC;
+// Explicit multiply-adds: the coroutine below is inlined into two kernels,
+// and contraction left to the compiler can differ between them.
+__device__ __forceinline__ double ddot(double ax, double ay, double az, double bx, double by, double bz) {
+    return fma(ax, bx, fma(ay, by, az * bz));
+}
+__device__ __forceinline__ double dcross_c(double a1, double b2, double a2, double b1) {
+    return fma(a1, b2, -(a2 * b1));  // a1 b2 - a2 b1
 }
 
+// ------------------------------------------------------------ DiffusionSDE
+// DiffusionSDE::process (DiffusionSDE.cpp:47) written as a coroutine that
+// stops at every field evaluation: the step-size halving tries of the
+// field-line trace (DiffusionSDE::tryStep, :233, Cash-Karp stages of the unit
+// field direction in FP32, FP64 base position and error), the 2^n sub-steps,
+// then the perpendicular and drift displacements (:120-200).  Every lane
+// runs its own number of six-stage traces, so a warp that evaluated fields
+// lane by lane would spend most of its time with one or a few lanes inside a
+// plane-wave mode sum; mixed_sde_coop_kernel instead evaluates the field
+// for all lanes waiting for one in a single converged pass, and a lane whose
+// step is done starts its next chain iteration at once.  SDE<FS> (the
+// persistent kernels) runs the same coroutine lane by lane, so both give
+// the same bits.  Stage i's offset gets a_ij k_j as soon as k_j is known.
+struct SdeCo {
+    double h, sh, TStep, NStep, BStep;
+    double propTime, allowedTime;
+    unsigned long long stepNumber, j;
+    unsigned counter;
+    int phase;                 // 0: step-halving tries, 1: sub-steps
+    int stage;                 // next stage of the current try
+    double bx, by, bz;         // base position of the current try
+    double t;                  // time of the current try
+    float tc;
+    f3 a1, a2, a3, a4, a5;     // offsets of stages 1..5 (units of tc)
+    float sx, sy, sz;
+    double ex, ey, ez;
+    double ox, oy, oz;         // end point of the last finished try
+    double qx, qy, qz;         // position the lane waits for a field at
+};
+
+__device__ __forceinline__ void sde_co_start_try(SdeCo &co, double x, double y, double z, double t) {
+    co.bx = x; co.by = y; co.bz = z;
+    co.t = t;
+    co.tc = (float)(t * kCLight);
+    co.stage = 0;
+    co.a1 = co.a2 = co.a3 = co.a4 = co.a5 = f3mk(0.f, 0.f, 0.f);
+    co.sx = co.sy = co.sz = 0.f;
+    co.ex = co.ey = co.ez = 0.0;
+    co.qx = x; co.qy = y; co.qz = z;
+}
+
+// First part of SDE::process up to the first field evaluation.  Returns
+// false when the step needs no field (neutral candidate): it is then done.
+template <int FS>
+__device__ __forceinline__ bool sde_co_begin(const DevPlan &P, const DevModule &m, Cand &c, SdeCo &co) {
+    c.px = c.x; c.py = c.y; c.pz = c.z;
+    const double h = clipd(c.next, m.min_step, m.max_step) * kInvCLight;
+    if (c.q == 0) {
+        c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+        set_current_step(c, h * kCLight);
+        c.next = m.max_step;
+        return false;
+    }
+    const double rig = c.E / c.q;
+    const double D = m.scale * 6.1e24 * pow(fabs(rig) / 4.0e9, m.alpha);
+    const double BT0 = sqrt(2 * D), BT4 = sqrt(2 * m.eps * D);
+    Stream s{P.seed, c.index, c.steps, make_uint4(0, 0, 0, 0), 0};
+    const double eta0 = s_norm(s), eta1 = s_norm(s), eta2 = s_norm(s);
+    co.h = h;
+    co.TStep = BT0 * eta0; co.NStep = BT4 * eta1; co.BStep = BT4 * eta2;
+    co.sh = sqrt(h);
+    co.propTime = co.TStep * co.sh * kInvCLight;
+    co.counter = 0;
+    co.phase = 0;
+    sde_co_start_try(co, c.x, c.y, c.z, co.propTime);
+    return true;
+}
+
+// Rest of SDE::process after the last field-line trace (o = its end point).
+__device__ __forceinline__ void sde_co_finish(const DevPlan &P, const DevModule &m, Cand &c, const SdeCo &co) {
+    const double h = co.h, sh = co.sh;
+    double tx = co.ox - c.x, ty = co.oy - c.y, tz = co.oz - c.z;
+    double tn = sqrt(ddot(tx, ty, tz, tx, ty, tz));
+    tx /= tn; ty /= tn; tz /= tn;
+    if (!(tn == tn) || tn == 0.0) {
+        c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+        set_current_step(c, h * kCLight);
+        c.next = clipd(5 * h * kCLight, m.min_step, m.max_step);
+        return;
+    }
+    Stream s{P.seed, c.index, c.steps, make_uint4(0, 0, 0, 0), 0};
+    s.seek(6);  // the three normals took words 0-5
+    double nx = 0, ny = 0, nz = 0;
+    for (int guard = 0; nx == 0 && ny == 0 && nz == 0 && guard < 3; guard++) {
+        double zr = s_uniform(s, -1.0, 1.0), tr = s_uniform(s, -kPi, kPi);
+        double rr = sqrt(fma(-zr, zr, 1.0)), sn, cs;
+        sincos(tr, &sn, &cs);
+        double rx = rr * cs, ry = rr * sn, rz = zr;
+        nx = dcross_c(ty, rz, ry, tz); ny = dcross_c(tz, rx, rz, tx); nz = dcross_c(tx, ry, rx, ty);
+    }
+    double nn = sqrt(ddot(nx, ny, nz, nx, ny, nz));
+    if (nn == 0.0) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
+    nx /= nn; ny /= nn; nz /= nn;
+    double bx = dcross_c(ty, nz, ny, tz), by = dcross_c(tz, nx, nz, tx), bz = dcross_c(tx, ny, nx, ty);
+    double bn = sqrt(ddot(bx, by, bz, bx, by, bz));
+    bx /= bn; by /= bn; bz /= bn;
+    double POx = fma(fma(nx, co.NStep, bx * co.BStep), sh, co.ox);
+    double POy = fma(fma(ny, co.NStep, by * co.BStep), sh, co.oy);
+    double POz = fma(fma(nz, co.NStep, bz * co.BStep), sh, co.oz);
+    if (isnan(POx + POy + POz)) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
+    s.cursor = 12;
+    double theta = acos(s_uniform(s, 1, cos(kPi / 2.)));
+    double zr = s_uniform(s, -1.0, 1.0), tr = s_uniform(s, -kPi, kPi);
+    double rr = sqrt(fma(-zr, zr, 1.0)), sn, cs;
+    sincos(tr, &sn, &cs);
+    double rx = rr * cs, ry = rr * sn, rz = zr;
+    double ax = dcross_c(ty, rz, ry, tz), ay = dcross_c(tz, rx, rz, tx), az = dcross_c(tx, ry, rx, ty);
+    double an = sqrt(ddot(ax, ay, az, ax, ay, az));
+    if (an != 0.) { ax /= an; ay /= an; az /= an; }
+    double st, ct;
+    sincos(theta, &st, &ct);
+    double adt = ddot(ax, ay, az, tx, ty, tz);
+    double cx_ = dcross_c(ay, tz, az, ty), cy_ = dcross_c(az, tx, ax, tz), cz_ = dcross_c(ax, ty, ay, tx);
+    const double omc = 1 - ct;
+    double dx = fma(tx, ct, fma(cx_, st, (ax * adt) * omc));
+    double dy = fma(ty, ct, fma(cy_, st, (ay * adt) * omc));
+    double dz = fma(tz, ct, fma(cz_, st, (az * adt) * omc));
+    double dn = 1.0 / sqrt(ddot(dx, dy, dz, dx, dy, dz));
+    c.x = POx; c.y = POy; c.z = POz;
+    c.dx = dx * dn; c.dy = dy * dn; c.dz = dz * dn;
+    set_current_step(c, h * kCLight);
+    c.next = (co.stepNumber > 1) ? h / ((double)co.stepNumber * (double)co.stepNumber) * kCLight
+                                 : 4 * h * kCLight;
+}
+
+// Take the field at co.q for the current stage.  Returns true while the
+// step waits for another field (co.q set), false when the step is done.
+__device__ __forceinline__ bool sde_co_consume(const DevPlan &P, const DevModule &m, Cand &c, SdeCo &co,
+                                               f3 B, StepCount &sc) {
+    const int jst = co.stage;
+    const float inv = rsqrtf(dot(B, B));
+    const f3 k = f3mk(B.x * inv, B.y * inv, B.z * inv);
+    const float b = ck_bf[jst];
+    co.sx = fmaf(k.x, b, co.sx); co.sy = fmaf(k.y, b, co.sy); co.sz = fmaf(k.z, b, co.sz);
+    const double e = ck_eb[jst];
+    co.ex = fma((double)k.x, e, co.ex); co.ey = fma((double)k.y, e, co.ey); co.ez = fma((double)k.z, e, co.ez);
+    // stage i's offset gets a_ij k_j for every later stage i
+    auto add = [&](f3 &acc, int i) {
+        const float a = ck_af[i * 6 + jst];
+        acc.x = fmaf(k.x, a, acc.x); acc.y = fmaf(k.y, a, acc.y); acc.z = fmaf(k.z, a, acc.z);
+    };
+    if (jst < 1) add(co.a1, 1);
+    if (jst < 2) add(co.a2, 2);
+    if (jst < 3) add(co.a3, 3);
+    if (jst < 4) add(co.a4, 4);
+    if (jst < 5) add(co.a5, 5);
+    co.stage = jst + 1;
+    if (co.stage < 6) {
+        const int st = co.stage;
+        const f3 a = st == 1 ? co.a1 : st == 2 ? co.a2 : st == 3 ? co.a3 : st == 4 ? co.a4 : co.a5;
+        co.qx = co.bx + (double)(a.x * co.tc);
+        co.qy = co.by + (double)(a.y * co.tc);
+        co.qz = co.bz + (double)(a.z * co.tc);
+        return true;
+    }
+    // the try is complete: end point and error of the trace
+    sc.tries++;
+    sc.evals += 6;
+    const double tcd = co.t * kCLight;
+    co.ox = fma((double)co.sx, tcd, co.bx); co.oy = fma((double)co.sy, tcd, co.by); co.oz = fma((double)co.sz, tcd, co.bz);
+    const double err = sqrt(ddot(co.ex, co.ey, co.ez, co.ex, co.ey, co.ez)) * fabs(tcd) / CRP_KPC;
+    if (co.phase == 0) {
+        const double r = err / m.tolerance;
+        co.propTime *= 0.5;
+        co.counter += 1;
+        if (r > 1 && fabs(co.propTime) >= m.min_step * kInvCLight && co.counter < 60) {
+            sde_co_start_try(co, c.x, c.y, c.z, co.propTime);
+            return true;
+        }
+        co.stepNumber = 1ull << (co.counter - 1);
+        co.allowedTime = co.TStep * co.sh * kInvCLight / (double)co.stepNumber;
+        co.phase = 1;
+        co.j = 0;
+        sde_co_start_try(co, c.x, c.y, c.z, co.allowedTime);
+        return true;
+    }
+    co.j++;
+    if (co.j < co.stepNumber) {
+        sde_co_start_try(co, co.ox, co.oy, co.oz, co.allowedTime);
+        return true;
+    }
+    sde_co_finish(P, m, c, co);
+    return false;
+}
+
+// DiffusionSDE::process (DiffusionSDE.cpp:47) for one lane: the coroutine
+// run to completion, field evaluations in place.
 template <int FS>
 struct SDE {
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
-        c.px = c.x; c.py = c.y; c.pz = c.z;
-        double h = clipd(c.next, m.min_step, m.max_step) * kInvCLight;
-        if (c.q == 0) {
-            c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
-            set_current_step(c, h * kCLight);
-            c.next = m.max_step;
-            return;
+        SdeCo co;
+        if (!sde_co_begin<FS>(P, m, c, co)) return;
+        while (sde_co_consume(P, m, c, co, field_at<FS>(P, co.qx, co.qy, co.qz, &c), sc)) {
         }
-        double rig = c.E / c.q;
-        double D = m.scale * 6.1e24 * pow(fabs(rig) / 4.0e9, m.alpha);
-        double BT0 = sqrt(2 * D), BT4 = sqrt(2 * m.eps * D);
-        Stream s{P.seed, c.index, c.steps, make_uint4(0, 0, 0, 0), 0};
-        double eta0 = s_norm(s), eta1 = s_norm(s), eta2 = s_norm(s);
-        double TStep = BT0 * eta0, NStep = BT4 * eta1, BStep = BT4 * eta2;
-        double sh = sqrt(h);
-        double propTime = TStep * sh * kInvCLight;
-        unsigned counter = 0;
-        double r, ox, oy, oz, err;
-        do {
-            sde_try<FS>(P, c.x, c.y, c.z, propTime, ox, oy, oz, err, &c);
-            sc.tries++; sc.evals += 6;
-            r = err / m.tolerance;
-            propTime *= 0.5;
-            counter += 1;
-        } while (r > 1 && fabs(propTime) >= m.min_step * kInvCLight && counter < 60);
-        unsigned long long stepNumber = 1ull << (counter - 1);
-        double allowedTime = TStep * sh * kInvCLight / (double)stepNumber;
-        double sx = c.x, sy = c.y, sz = c.z;
-        for (unsigned long long j = 0; j < stepNumber; j++) {
-            sde_try<FS>(P, sx, sy, sz, allowedTime, ox, oy, oz, err, &c);
-            sc.tries++; sc.evals += 6;
-            sx = ox; sy = oy; sz = oz;
-        }
-        double tx = ox - c.x, ty = oy - c.y, tz = oz - c.z;
-        double tn = sqrt(tx * tx + ty * ty + tz * tz);
-        tx /= tn; ty /= tn; tz /= tn;
-        if (!(tn == tn) || tn == 0.0) {
-            c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
-            set_current_step(c, h * kCLight);
-            c.next = clipd(5 * h * kCLight, m.min_step, m.max_step);
-            return;
-        }
-        double nx = 0, ny = 0, nz = 0;
-        for (int guard = 0; nx == 0 && ny == 0 && nz == 0 && guard < 3; guard++) {
-            double zr = s_uniform(s, -1.0, 1.0), tr = s_uniform(s, -kPi, kPi);
-            double rr = sqrt(1 - zr * zr), sn, cs;
-            sincos(tr, &sn, &cs);
-            double rx = rr * cs, ry = rr * sn, rz = zr;
-            nx = ty * rz - ry * tz; ny = tz * rx - rz * tx; nz = tx * ry - rx * ty;
-        }
-        double nn = sqrt(nx * nx + ny * ny + nz * nz);
-        if (nn == 0.0) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
-        nx /= nn; ny /= nn; nz /= nn;
-        double bx = ty * nz - ny * tz, by = tz * nx - nz * tx, bz = tx * ny - nx * ty;
-        double bn = sqrt(bx * bx + by * by + bz * bz);
-        bx /= bn; by /= bn; bz /= bn;
-        double POx = ox + (nx * NStep + bx * BStep) * sh;
-        double POy = oy + (ny * NStep + by * BStep) * sh;
-        double POz = oz + (nz * NStep + bz * BStep) * sh;
-        if (isnan(POx + POy + POz)) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
-        // randConeVector(T, pi/2) (Random.cpp:159): rotate T by theta about T x randVector
-        s.cursor = 12;
-        double theta = acos(s_uniform(s, 1, cos(kPi / 2.)));
-        double zr = s_uniform(s, -1.0, 1.0), tr = s_uniform(s, -kPi, kPi);
-        double rr = sqrt(1 - zr * zr), sn, cs;
-        sincos(tr, &sn, &cs);
-        double rx = rr * cs, ry = rr * sn, rz = zr;
-        double ax = ty * rz - ry * tz, ay = tz * rx - rz * tx, az = tx * ry - rx * ty;
-        double an = sqrt(ax * ax + ay * ay + az * az);
-        if (an != 0.) { ax /= an; ay /= an; az /= an; }
-        double st, ct;
-        sincos(theta, &st, &ct);
-        // Rodrigues rotation of T about the unit axis a
-        double adt = ax * tx + ay * ty + az * tz;
-        double cx_ = ay * tz - az * ty, cy_ = az * tx - ax * tz, cz_ = ax * ty - ay * tx;
-        double dx = tx * ct + cx_ * st + ax * adt * (1 - ct);
-        double dy = ty * ct + cy_ * st + ay * adt * (1 - ct);
-        double dz = tz * ct + cz_ * st + az * adt * (1 - ct);
-        double dn = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
-        c.x = POx; c.y = POy; c.z = POz;
-        c.dx = dx * dn; c.dy = dy * dn; c.dz = dz * dn;
-        set_current_step(c, h * kCLight);
-        c.next = (stepNumber > 1) ? h / ((double)stepNumber * (double)stepNumber) * kCLight : 4 * h * kCLight;
     }
 };
+
+
+// The non-propagation modules mi in [from, to) of one chain iteration.
+__device__ __forceinline__ void chain_part(const DevPlan &P, Cand &c, const DevRecords &rec, int from, int to) {
+#pragma unroll 1
+    for (int mi = from; mi < to; mi++) {
+        const DevModule &m = P.modules[mi];
+        if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) max_trajectory_length(m, c, rec, mi);
+        else if (m.kind == CRP_MODULE_OBSERVER) observer(m, c, rec, mi);
+    }
+}
+
+// Chunked launch of a DiffusionSDE chain in coroutine form (the loop of
+// chunk_body, every module of the chain in order, each iteration).
+#ifndef CRP_SDE_COOP_MIN_BLOCKS
+#define CRP_SDE_COOP_MIN_BLOCKS 1
+#endif
+template <int FS>
+__global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_kernel(DevPlan P, DevState s, uint64_t n,
+                                                               int max_steps, uint64_t step_cap,
+                                                               DevCounters *cnt, DevRecords rec,
+                                                               const uint32_t *perm, uint32_t *perm_out) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pi = P.prop_index;
+    const DevModule &pm = P.modules[pi];
+    StepCount sc;
+    Cand c;
+    SdeCo co;
+    uint64_t i = 0;
+    bool loaded = false, live = false, want = false;
+    int k = 0;
+    if (t < n) {
+        i = perm ? perm[t] : t;
+        if (s.active[i]) {
+            load_cand(s, i, c);
+            loaded = live = true;
+        }
+    }
+    for (;;) {
+        while (live && !want) {
+            if (!(c.active && k < max_steps && (step_cap == 0 || c.steps < step_cap))) {
+                live = false;
+                break;
+            }
+            chain_part(P, c, rec, 0, pi);
+            if (sde_co_begin<FS>(P, pm, c, co)) {
+                want = true;
+            } else {
+                chain_part(P, c, rec, pi + 1, P.n_modules);
+                c.steps++;
+                k++;
+            }
+        }
+        if (!__any_sync(0xffffffffu, want)) break;
+        if (want) {
+            const f3 B = field_at<FS>(P, co.qx, co.qy, co.qz, &c);
+            if (!sde_co_consume(P, pm, c, co, B, sc)) {
+                want = false;
+                chain_part(P, c, rec, pi + 1, P.n_modules);
+                c.steps++;
+                k++;
+            }
+        }
+    }
+    bool still = false;
+    if (loaded) {
+        still = c.active && (step_cap == 0 || c.steps < step_cap);
+        store_cand(s, c);
+    }
+    flush_counters(cnt, (unsigned long long)k, sc);
+    append_active(cnt, perm_out, still, (uint32_t)i);
+}
 
 // step-mode variants selected by the launcher from min_step == max_step, so
 // that a fixed-step kernel carries no adaptive-controller registers
@@ -587,7 +757,15 @@ cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, 
     if (prop == CRP_PROP_CK)
         return fixed ? launch_prop<CKFixed>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st)
                      : launch_prop<CKAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
-    return launch_prop<SDE>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
+    if (block > 128) block = 128;
+    const unsigned grid = (unsigned)((n + block - 1) / block);
+    if (fs == FS_GRID)
+        mixed_sde_coop_kernel<FS_GRID><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+    else if (fs == FS_PLANE_WAVE)
+        mixed_sde_coop_kernel<FS_PLANE_WAVE><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+    else
+        mixed_sde_coop_kernel<FS_GENERIC><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_mixed_persistent(const DevPlan &P, const DevState &s, const PersistentArgs &a,

@@ -122,3 +122,35 @@ def test_sde_exit_distributions_match_reference(oracle, reference):
     gz = g["z"] / np.sqrt(g["x"] ** 2 + g["y"] ** 2 + g["z"] ** 2)
     rz = r["z"] / np.sqrt(r["x"] ** 2 + r["y"] ** 2 + r["z"] ** 2)
     assert stats.ks_2samp(gz, rz).pvalue > 1e-4
+
+
+@pytest.mark.parametrize("field", ["plane_wave", "toroidal_plus_waves", "grid"])
+def test_sde_mixed_coroutine_kernel_equals_per_lane_kernel(oracle, field):
+    """The mixed form's chunked launches run DiffusionSDE as a coroutine
+    (converged field passes for all waiting lanes); its persistent launches
+    run the per-lane step.  Same arithmetic, so bit-identical results."""
+    from helpers import random_grid
+    from crpropa3_b200.engine import Plan
+    xi, kappa, k, beta, ak = oracle.plane_wave_modes(0.5 * U.muG, 1 * U.pc, 100 * U.pc, 1.0, 5 / 3, 4.0, 64, 11)
+    pw = P.PlaneWaveField(xi, kappa, k, beta, ak, spectrum=(0.5 * U.muG, 1 * U.pc, 100 * U.pc, 1.0, 5 / 3, 4.0),
+                          seed=11)
+    fields = {"plane_wave": [pw],
+              "toroidal_plus_waves": [P.ToroidalField(1 * U.muG), pw],
+              "grid": [P.GridField(random_grid(np.random.default_rng(5), 16, brms=1e-10),
+                                   (-8 * U.pc,) * 3, (1 * U.pc,) * 3)]}[field]
+    obs = P.ObserverSpec(_abi.OBSERVER_SURFACE_SPHERE, (0, 0, 0), 300 * U.pc, True, True)
+    spec = _sde_chain(fields, min_step=0.1 * U.pc, max_step=100 * U.pc, eps=0.1, length=2 * U.kpc,
+                      precision=_abi.PRECISION_MIXED, observer=obs)
+    rng = np.random.default_rng(46)
+    c = _cands(3000, 1.0, pos=(150 * U.pc, 0, 0), rng=rng)
+    c.energy[:] = np.exp(rng.uniform(np.log(10 * U.TeV), np.log(1 * U.PeV), c.n))
+    a, b = c.to_device("cuda"), c.to_device("cuda")
+    plan = Plan(spec)
+    sa = plan.run(a, mode=_abi.MODE_CHUNKED, steps_per_launch=40)
+    sb = plan.run(b, mode=_abi.MODE_PERSISTENT, ctas_per_sm=2, steps_per_launch=8)
+    ha, hb = a.to_host(), b.to_host()
+    for m in ("x", "y", "z", "dx", "dy", "dz", "trajectory_length", "time", "next_step", "active",
+              "flags", "step_count"):
+        np.testing.assert_array_equal(getattr(ha, m), getattr(hb, m), err_msg=m)
+    assert sa.particle_steps == sb.particle_steps and sa.tries == sb.tries
+    assert sa.launches > 1
