@@ -123,17 +123,32 @@ __device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
 // hardware cosine takes 2 pi f.  Amplitudes A xi and the sums are FP32.
 // Table per mode: kk = {k kappa / 2 pi, beta / 2 pi} (FP64), modes32 =
 // {A xi, 0} (FP32).  Two accumulator sets halve the dependence chain of the
-// sums.
-__device__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double z) {
+// sums.  The table is read from global memory (read-only path) or from a
+// copy a kernel staged in shared memory.
+struct PwTab {
+    const double2 *kk;
+    const float4 *a;
+    int n;
+};
+
+template <bool SHARED>
+__device__ __forceinline__ f3 pw_sum(const double2 *kk, const float4 *am, int n, double x, double y,
+                                     double z) {
     const float twopi = 6.28318530717958647692f;
     float bx0 = 0.f, by0 = 0.f, bz0 = 0.f, bx1 = 0.f, by1 = 0.f, bz1 = 0.f;
-    const double2 *kk = reinterpret_cast<const double2 *>(w.kk);
-    const int n2 = w.n & ~1;
+    const int n2 = n & ~1;
 #pragma unroll 4
     for (int i = 0; i < n2; i += 2) {
-        const double2 m0 = __ldg(kk + 2 * i), m1 = __ldg(kk + 2 * i + 1);
-        const double2 m2 = __ldg(kk + 2 * i + 2), m3 = __ldg(kk + 2 * i + 3);
-        const float4 a = __ldg(w.modes32 + i), b = __ldg(w.modes32 + i + 1);
+        double2 m0, m1, m2, m3;
+        float4 a, b;
+        if (SHARED) {
+            m0 = kk[2 * i]; m1 = kk[2 * i + 1]; m2 = kk[2 * i + 2]; m3 = kk[2 * i + 3];
+            a = am[i]; b = am[i + 1];
+        } else {
+            m0 = __ldg(kk + 2 * i); m1 = __ldg(kk + 2 * i + 1);
+            m2 = __ldg(kk + 2 * i + 2); m3 = __ldg(kk + 2 * i + 3);
+            a = __ldg(am + i); b = __ldg(am + i + 1);
+        }
         const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
         const double p1 = fma(m2.x, x, fma(m2.y, y, fma(m3.x, z, m3.y)));
         const float c0 = __cosf(twopi * (float)(p0 - rint(p0)));
@@ -141,9 +156,10 @@ __device__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double
         bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
         bx1 = fmaf(b.x, c1, bx1); by1 = fmaf(b.y, c1, by1); bz1 = fmaf(b.z, c1, bz1);
     }
-    if (n2 < w.n) {
-        const double2 m0 = __ldg(kk + 2 * n2), m1 = __ldg(kk + 2 * n2 + 1);
-        const float4 a = __ldg(w.modes32 + n2);
+    if (n2 < n) {
+        const double2 m0 = SHARED ? kk[2 * n2] : __ldg(kk + 2 * n2);
+        const double2 m1 = SHARED ? kk[2 * n2 + 1] : __ldg(kk + 2 * n2 + 1);
+        const float4 a = SHARED ? am[n2] : __ldg(am + n2);
         const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
         const float c0 = __cosf(twopi * (float)(p0 - rint(p0)));
         bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
@@ -151,7 +167,17 @@ __device__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double
     return f3mk(bx0 + bx1, by0 + by1, bz0 + bz1);
 }
 
-__device__ f3 component_field(const DevComponent &f, double x, double y, double z) {
+__device__ __forceinline__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double z,
+                                               const PwTab *sh = nullptr) {
+    if (sh) return pw_sum<true>(sh->kk, sh->a, sh->n, x, y, z);
+    return pw_sum<false>(reinterpret_cast<const double2 *>(w.kk), w.modes32, w.n, x, y, z);
+}
+
+// Multiply-adds here are written out (fma) so that the result does not
+// depend on how the compiler contracts the expression in each kernel that
+// inlines it: the chunked and persistent launches must agree bit for bit.
+__device__ __forceinline__ f3 component_field(const DevComponent &f, double x, double y, double z,
+                                             const PwTab *sh = nullptr) {
     if (f.periodic) {
         double qx = x - f.po[0], qy = y - f.po[1], qz = z - f.po[2];
         double nx = floor(qx / f.pe[0]), ny = floor(qy / f.pe[1]), nz = floor(qz / f.pe[2]);
@@ -164,7 +190,7 @@ __device__ f3 component_field(const DevComponent &f, double x, double y, double 
     }
     switch (f.kind) {
     case CRP_FIELD_GRID: return grid_field(f.grid, x, y, z);
-    case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z);
+    case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z, sh);
     case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
     default: {
         double r = sqrt(fma(x, x, y * y));
@@ -174,16 +200,18 @@ __device__ f3 component_field(const DevComponent &f, double x, double y, double 
     }
 }
 
+// sh: the plan's plane-wave table staged in shared memory (at most one
+// plane-wave component), or null.
 template <int FS>
 __device__ __forceinline__ f3 field_at(const DevPlan &P, double x, double y, double z,
-                                       Cand *cc = nullptr) {
+                                       Cand *cc = nullptr, const PwTab *sh = nullptr) {
     if (FS == FS_GRID) return grid_field_t<true>(P.fields[0].grid, x, y, z, cc);
-    if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, x, y, z);
-    if (P.n_fields == 1) return component_field(P.fields[0], x, y, z);
+    if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, x, y, z, sh);
+    if (P.n_fields == 1) return component_field(P.fields[0], x, y, z, sh);
     f3 b = f3mk(0.f, 0.f, 0.f);
 #pragma unroll 1
     for (int i = 0; i < P.n_fields; i++) {
-        f3 c = component_field(P.fields[i], x, y, z);
+        f3 c = component_field(P.fields[i], x, y, z, sh);
         b.x += c.x; b.y += c.y; b.z += c.z;
     }
     return b;
@@ -621,11 +649,27 @@ __device__ __forceinline__ void chain_part(const DevPlan &P, Cand &c, const DevR
 #ifndef CRP_SDE_COOP_MIN_BLOCKS
 #define CRP_SDE_COOP_MIN_BLOCKS 1
 #endif
+// pw_field >= 0: index of the plan's plane-wave component, whose mode
+// table the block stages in shared memory (dynamic, 48 B per mode) first.
 template <int FS>
 __global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_kernel(DevPlan P, DevState s, uint64_t n,
                                                                int max_steps, uint64_t step_cap,
                                                                DevCounters *cnt, DevRecords rec,
-                                                               const uint32_t *perm, uint32_t *perm_out) {
+                                                               const uint32_t *perm, uint32_t *perm_out,
+                                                               int pw_field) {
+    extern __shared__ __align__(16) unsigned char pw_smem[];
+    PwTab tab{nullptr, nullptr, 0};
+    if (pw_field >= 0) {
+        const DevPlaneWave &w = P.fields[pw_field].pw;
+        double2 *kk = reinterpret_cast<double2 *>(pw_smem);
+        float4 *am = reinterpret_cast<float4 *>(pw_smem + (size_t)w.n * 32);
+        const double2 *gk = reinterpret_cast<const double2 *>(w.kk);
+        for (int q = threadIdx.x; q < 2 * w.n; q += blockDim.x) kk[q] = __ldg(gk + q);
+        for (int q = threadIdx.x; q < w.n; q += blockDim.x) am[q] = __ldg(w.modes32 + q);
+        __syncthreads();
+        tab = PwTab{kk, am, w.n};
+    }
+    const PwTab *sh = pw_field >= 0 ? &tab : nullptr;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int pi = P.prop_index;
     const DevModule &pm = P.modules[pi];
@@ -659,7 +703,7 @@ __global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_k
         }
         if (!__any_sync(0xffffffffu, want)) break;
         if (want) {
-            const f3 B = field_at<FS>(P, co.qx, co.qy, co.qz, &c);
+            const f3 B = field_at<FS>(P, co.qx, co.qy, co.qz, &c, sh);
             if (!sde_co_consume(P, pm, c, co, B, sc)) {
                 want = false;
                 chain_part(P, c, rec, pi + 1, P.n_modules);
@@ -759,12 +803,28 @@ cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, 
                      : launch_prop<CKAdaptive>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out, fs, block, st);
     if (block > 128) block = 128;
     const unsigned grid = (unsigned)((n + block - 1) / block);
-    if (fs == FS_GRID)
-        mixed_sde_coop_kernel<FS_GRID><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
-    else if (fs == FS_PLANE_WAVE)
-        mixed_sde_coop_kernel<FS_PLANE_WAVE><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+    // stage the plane-wave table in shared memory when there is exactly one
+    // plane-wave component and its table fits in 96 KB (two blocks per SM)
+    int pw_field = -1, n_pw = 0;
+    for (int f = 0; f < P.n_fields; f++)
+        if (P.fields[f].kind == CRP_FIELD_PLANE_WAVE) { pw_field = f; n_pw++; }
+    size_t smem = 0;
+    if (n_pw == 1 && (size_t)P.fields[pw_field].pw.n * 48 <= 96 * 1024)
+        smem = (size_t)P.fields[pw_field].pw.n * 48;
     else
-        mixed_sde_coop_kernel<FS_GENERIC><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+        pw_field = -1;
+#define CRP_SDE_COOP(FSV)                                                                              \
+    do {                                                                                               \
+        if (smem > 48 * 1024)                                                                          \
+            cudaFuncSetAttribute(mixed_sde_coop_kernel<FSV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)smem);                                                           \
+        mixed_sde_coop_kernel<FSV><<<grid, block, smem, st>>>(P, s, n, max_steps, step_cap, cnt, rec,  \
+                                                              perm, perm_out, pw_field);               \
+    } while (0)
+    if (fs == FS_GRID) CRP_SDE_COOP(FS_GRID);
+    else if (fs == FS_PLANE_WAVE) CRP_SDE_COOP(FS_PLANE_WAVE);
+    else CRP_SDE_COOP(FS_GENERIC);
+#undef CRP_SDE_COOP
     return cudaGetLastError();
 }
 
