@@ -394,10 +394,23 @@ def cfg_grid_ck_64(dev, peaks, n=10_000):
                          "basis": "576 B per Cash-Karp try"}}
         plan.close()
         del grid
+    # the same L2-resident grid with enough candidates to fill the GPU
+    n_big = 1 << 20
+    spec, cands, grid = W.grid_ck_64(n=n_big, precision=_abi.PRECISION_MIXED, device=dev)
+    plan = engine.Plan(spec)
+    t = _timed_runs(plan, cands.to_device(dev), cands.to_device(dev), 2)
+    tries_s = t["tries"] / (t["device_ms"] / 1e3)
+    gbs = 576 * tries_s / 1e9
+    out["grid_ck_64"]["mixed_1M"] = {
+        "candidates": n_big, "tries_per_s": tries_s, "ms_per_run": t["device_ms"] / 2,
+        "roofline": {"bound": "l2", "achieved": gbs, "peak": peaks.get("l2_gbs"), "unit": "GB/s",
+                     "frac": gbs / peaks["l2_gbs"] if peaks.get("l2_gbs") else None,
+                     "basis": "576 B per Cash-Karp try"}}
+    plan.close()
     return out
 
 
-def cfg_grid_ck_nuclei(dev, peaks, n3=4_000_000, cap3=512):
+def cfg_grid_ck_nuclei(dev, peaks, n3=1 << 20, cap3=2048):
     """PropagationCK, 4 species, E^-2, per-candidate lengths, 256^3 grid:
     chunked launches vs the autotuned persistent refill kernel."""
     from crpropa3_b200 import _abi, engine, workloads as W
@@ -406,7 +419,8 @@ def cfg_grid_ck_nuclei(dev, peaks, n3=4_000_000, cap3=512):
     plan = engine.Plan(spec)
     d_init, d_work = cands.to_device(dev), cands.to_device(dev)
     chunked = _timed_runs(plan, d_init, d_work, 2, mode=_abi.MODE_CHUNKED, max_steps=cap3)
-    tune = plan.autotune(d_init, sample_n=1 << 18, steps_per_candidate=128)
+    persistent = _timed_runs(plan, d_init, d_work, 2, mode=_abi.MODE_PERSISTENT, max_steps=cap3)
+    tune = plan.autotune(d_init, sample_n=1 << 18, steps_per_candidate=256)
     auto = _timed_runs(plan, d_init, d_work, 2, mode=_abi.MODE_AUTO, max_steps=cap3)
     rate = lambda t: t["tries"] / (t["device_ms"] / 1e3)
     out["grid_ck_nuclei"] = {
@@ -414,6 +428,7 @@ def cfg_grid_ck_nuclei(dev, peaks, n3=4_000_000, cap3=512):
                     f"PropagationCK 1e-4 0.1-100 kpc, lengths U[1,50] Mpc; at most {cap3} steps "
                     "per candidate (full runs reach 5e5 steps)",
         "chunked_tries_per_s": rate(chunked),
+        "persistent_default_tries_per_s": rate(persistent),
         "autotuned_tries_per_s": rate(auto),
         "autotuned": {"mode": int(tune.mode), "ctas_per_sm": int(tune.ctas_per_sm),
                       "refill_threshold": int(tune.refill_threshold), "burst": int(tune.burst)},
@@ -481,7 +496,7 @@ def main():
         # one secondary configuration alone (profiling runs), one JSON line
         dev = f"cuda:{local}"
         runs = {"grid_ck_64": lambda: cfg_grid_ck_64(dev, {}, n=args.n or 10_000),
-                "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or 4_000_000),
+                "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or (1 << 20)),
                 "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20))}
         if args.workload not in runs:
             log(f"unknown workload {args.workload}")
