@@ -165,10 +165,18 @@ __device__ __forceinline__ void observer(const DevModule &m, Cand &c, const DevR
 }
 
 // ModuleList::process (ModuleList.cpp.in:54): every module of the chain, in
-// order, whether or not an earlier module deactivated the candidate.
-template <class Prop>
+// order, whether or not an earlier module deactivated the candidate; a
+// compiled module sequence for the chain shapes of device_plan.cuh, else the
+// module list walked in order.
+template <class Prop, int CS = CS_GENERIC>
 __device__ __forceinline__ void chain_process(const DevPlan &P, Cand &c, const DevRecords &rec,
                                               StepCount &sc) {
+    if (CS == CS_PM || CS == CS_PMO) {
+        Prop::process(P, P.modules[0], c, sc);
+        max_trajectory_length(P.modules[1], c, rec, 1);
+        if (CS == CS_PMO) observer(P.modules[2], c, rec, 2);
+        return;
+    }
 #pragma unroll 1
     for (int mi = 0; mi < P.n_modules; mi++) {
         const DevModule &m = P.modules[mi];
@@ -214,7 +222,7 @@ __device__ __forceinline__ void append_active(DevCounters *cnt, uint32_t *list, 
 // One thread per candidate, at most max_steps chain iterations per launch.
 // perm_in (optional) maps thread -> candidate index; the candidates still
 // active afterwards are appended to perm_out (optional).
-template <class Prop>
+template <class Prop, int CS = CS_GENERIC>
 __device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, uint64_t n,
                                            int max_steps, uint64_t step_cap,
                                            DevCounters *cnt, const DevRecords &rec,
@@ -231,7 +239,7 @@ __device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, 
             load_cand(s, i, c);
             int k = 0;
             while (c.active && k < max_steps && (step_cap == 0 || c.steps < step_cap)) {
-                chain_process<Prop>(P, c, rec, sc);
+                chain_process<Prop, CS>(P, c, rec, sc);
                 c.steps++;
                 k++;
             }

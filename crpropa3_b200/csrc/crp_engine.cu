@@ -334,6 +334,14 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
     d.n_modules = desc->n_modules;
     d.prop_index = prop_index;
     d.seed = desc->seed;
+    // module sequences with compiled kernels (chain.cuh ChainShape)
+    const auto kind = [&](int i) { return desc->modules[i].kind; };
+    d.shape = CS_GENERIC;
+    if (desc->n_modules == 2 && kind(0) == CRP_MODULE_PROPAGATION && kind(1) == CRP_MODULE_MAX_TRAJECTORY_LENGTH)
+        d.shape = CS_PM;
+    else if (desc->n_modules == 3 && kind(0) == CRP_MODULE_PROPAGATION &&
+             kind(1) == CRP_MODULE_MAX_TRAJECTORY_LENGTH && kind(2) == CRP_MODULE_OBSERVER)
+        d.shape = CS_PMO;
     for (int i = 0; i < desc->n_fields; i++) {
         crp_status st = build_component(p, desc->fields[i], d.fields[i]);
         if (st) { delete p; return st; }

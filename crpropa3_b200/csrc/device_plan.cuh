@@ -57,11 +57,17 @@ struct DevModule {
     int record;
 };
 
+// Module sequences the stepping kernels are compiled for: CS_PM =
+// [propagation, MaximumTrajectoryLength], CS_PMO = [propagation,
+// MaximumTrajectoryLength, Observer]; any other chain walks the module list
+// (CS_GENERIC).  The plan records which one its chain matches.
+enum ChainShape { CS_GENERIC = 0, CS_PM = 1, CS_PMO = 2 };
+
 struct DevPlan {
     int n_fields;
     int n_modules;
     int prop_index;  // position of the propagation module in the chain
-    int pad;
+    int shape;       // ChainShape (chain.cuh) the module sequence matches
     uint64_t seed;
     DevComponent fields[kMaxFields];
     DevModule modules[kMaxModules];

@@ -732,12 +732,12 @@ template <int FS> using BPAdaptive = BP<FS, 2>;
 template <int FS> using CKFixed = CK<FS, 1>;
 template <int FS> using CKAdaptive = CK<FS, 2>;
 
-template <template <int> class Prop, int FS>
+template <template <int> class Prop, int FS, int CS>
 __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_chunk_kernel(DevPlan P, DevState s, uint64_t n,
                                                           int max_steps, uint64_t step_cap,
                                                           DevCounters *cnt, DevRecords rec,
                                                           const uint32_t *perm, uint32_t *perm_out) {
-    chunk_body<Prop<FS>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+    chunk_body<Prop<FS>, CS>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
 }
 
 template <template <int> class Prop, int FS>
@@ -776,12 +776,22 @@ cudaError_t launch_prop(const DevPlan &P, const DevState &s, uint64_t n, int max
                         const uint32_t *perm, uint32_t *perm_out, int fs, int block,
                         cudaStream_t st) {
     unsigned grid = (unsigned)((n + block - 1) / block);
-    if (fs == FS_GRID)
-        mixed_chunk_kernel<Prop, FS_GRID><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
-    else if (fs == FS_PLANE_WAVE)
-        mixed_chunk_kernel<Prop, FS_PLANE_WAVE><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
-    else
-        mixed_chunk_kernel<Prop, FS_GENERIC><<<grid, block, 0, st>>>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
+#define CRP_CHUNK(FSV, CSV) mixed_chunk_kernel<Prop, FSV, CSV><<<grid, block, 0, st>>>(P, s, n, max_steps, \
+        step_cap, cnt, rec, perm, perm_out)
+    // compiled chain shapes for the single-field signatures; the generic
+    // field sum walks the module list
+    if (fs == FS_GRID) {
+        if (P.shape == CS_PM) CRP_CHUNK(FS_GRID, CS_PM);
+        else if (P.shape == CS_PMO) CRP_CHUNK(FS_GRID, CS_PMO);
+        else CRP_CHUNK(FS_GRID, CS_GENERIC);
+    } else if (fs == FS_PLANE_WAVE) {
+        if (P.shape == CS_PM) CRP_CHUNK(FS_PLANE_WAVE, CS_PM);
+        else if (P.shape == CS_PMO) CRP_CHUNK(FS_PLANE_WAVE, CS_PMO);
+        else CRP_CHUNK(FS_PLANE_WAVE, CS_GENERIC);
+    } else {
+        CRP_CHUNK(FS_GENERIC, CS_GENERIC);
+    }
+#undef CRP_CHUNK
     return cudaGetLastError();
 }
 
