@@ -268,7 +268,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // budget_ns of device time: lanes that still hold a candidate then store it
 // and append its index to pending_out (cnt->pending_count), for the next
 // launch.  cnt->queue_head counts the items taken.
-template <class Prop>
+template <class Prop, int CS = CS_GENERIC>
 __device__ __forceinline__ void persistent_body(const DevPlan &P, const DevState &s,
                                                 const uint32_t *pending_in, uint64_t n_pending,
                                                 uint64_t main_base, uint64_t n_main,
@@ -311,7 +311,7 @@ __device__ __forceinline__ void persistent_body(const DevPlan &P, const DevState
         if (has) {
             int k = 0;
             while (c.active && k < burst && (step_cap == 0 || c.steps < step_cap)) {
-                chain_process<Prop>(P, c, rec, sc);
+                chain_process<Prop, CS>(P, c, rec, sc);
                 c.steps++;
                 k++;
             }

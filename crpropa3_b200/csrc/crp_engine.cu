@@ -358,8 +358,11 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
         dm.radius = m.sphere_radius;
         dm.deactivate = m.deactivate_on_detection; dm.record = m.record;
     }
-    if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_GRID)
-        p->fs = FS_GRID;
+    if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_GRID) {
+        const DevGrid &g = d.fields[0].grid;
+        const bool padded = p->precision != CRP_PRECISION_MIXED || g.values4 != nullptr;
+        p->fs = (!g.reflective && !g.clip_volume && g.pow2 && padded) ? FS_GRID_PERIODIC : FS_GRID;
+    }
     else if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_PLANE_WAVE)
         p->fs = FS_PLANE_WAVE;
     else

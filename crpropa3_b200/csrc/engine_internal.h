@@ -14,7 +14,9 @@ namespace crp {
 enum FieldSig {
     FS_GENERIC = 0,    // any sum of (possibly periodic) components
     FS_GRID = 1,       // one MagneticFieldGrid, not wrapped
-    FS_PLANE_WAVE = 2  // one PlaneWaveTurbulence, not wrapped
+    FS_PLANE_WAVE = 2, // one PlaneWaveTurbulence, not wrapped
+    FS_GRID_PERIODIC = 3  // FS_GRID with a periodic grid of power-of-two dimensions, no
+                          // clipVolume (and the padded copy, mixed form): no runtime checks
 };
 
 // Persistent stepping launch (chain.cuh persistent_body): `grid` CTAs of 128

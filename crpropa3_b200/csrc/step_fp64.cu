@@ -43,9 +43,12 @@ __device__ __forceinline__ double clipd(double x, double lo, double hi) { return
 // Grid<Vector3f>::interpolate (Grid.h:318) -> trilinearInterpolate (:540).
 // With a cell cache (FS_GRID kernels) the 8 corners are loaded only when the
 // cell changes.
-template <bool CACHE>
+// PER: the grid is periodic with power-of-two dimensions and has no
+// clipVolume (FS_GRID_PERIODIC): those branches are compiled out and the
+// periodic clamp is a mask (equal to the double modulo of Grid.h:31 there).
+template <bool CACHE, bool PER = false>
 __device__ __forceinline__ d3 grid_field_t(const DevGrid &g, d3 pos, Cand *cc) {
-    if (g.clip_volume) {
+    if (!PER && g.clip_volume) {
         bool in = (pos.x >= g.ox) && (pos.x <= g.ex);
         in &= (pos.y >= g.oy) && (pos.y <= g.ey);
         in &= (pos.z >= g.oz) && (pos.z <= g.ez);
@@ -56,7 +59,7 @@ __device__ __forceinline__ d3 grid_field_t(const DevGrid &g, d3 pos, Cand *cc) {
     double rz = (pos.z - g.goz) / g.sz;
     int ix0, ix1, iy0, iy1, iz0, iz1;
     double fX0, fY0, fZ0;
-    if (g.reflective) {  // reflectiveClamp (Grid.h:49)
+    if (!PER && g.reflective) {  // reflectiveClamp (Grid.h:49)
         double r[3] = {rx, ry, rz}, res[3];
         int n[3] = {g.nx, g.ny, g.nz}, lo[3], hi[3];
 #pragma unroll
@@ -78,6 +81,13 @@ __device__ __forceinline__ d3 grid_field_t(const DevGrid &g, d3 pos, Cand *cc) {
         fX0 = res[0] - floor(res[0]);
         fY0 = res[1] - floor(res[1]);
         fZ0 = res[2] - floor(res[2]);
+    } else if (PER) {  // periodicClamp (Grid.h:31), power-of-two dimensions
+        ix0 = (int)floor(rx) & (g.nx - 1); ix1 = (ix0 + 1) & (g.nx - 1);
+        iy0 = (int)floor(ry) & (g.ny - 1); iy1 = (iy0 + 1) & (g.ny - 1);
+        iz0 = (int)floor(rz) & (g.nz - 1); iz1 = (iz0 + 1) & (g.nz - 1);
+        fX0 = rx - floor(rx);
+        fY0 = ry - floor(ry);
+        fZ0 = rz - floor(rz);
     } else {  // periodicClamp (Grid.h:31)
         ix0 = (((int)floor(rx) % g.nx) + g.nx) % g.nx; ix1 = (ix0 + 1) % g.nx;
         iy0 = (((int)floor(ry) % g.ny) + g.ny) % g.ny; iy1 = (iy0 + 1) % g.ny;
@@ -164,6 +174,7 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
 template <int FS>
 __device__ __forceinline__ d3 field_at(const DevPlan &P, d3 pos, Cand *cc = nullptr) {
     if (FS == FS_GRID) return grid_field_t<true>(P.fields[0].grid, pos, cc);
+    if (FS == FS_GRID_PERIODIC) return grid_field_t<true, true>(P.fields[0].grid, pos, cc);
     if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, pos);
     if (P.n_fields == 1) return component_field(P.fields[0], pos);
     d3 b = mk(0, 0, 0);
@@ -466,14 +477,14 @@ __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_chunk_ke
     chunk_body<Prop<FS>, CS>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
 }
 
-template <template <int> class Prop, int FS>
+template <template <int> class Prop, int FS, int CS>
 __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_persistent_kernel(
     DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
     // the queue is written only between launches (advance_kernel)
     const DevQueue q = *a.q;
     const uint32_t *pending_in = q.cur ? a.list_b : a.list_a;
     uint32_t *pending_out = q.cur ? a.list_a : a.list_b;
-    persistent_body<Prop<FS>>(P, s, pending_in, q.n_pending, q.main_base, q.n_main, pending_out,
+    persistent_body<Prop<FS>, CS>(P, s, pending_in, q.n_pending, q.main_base, q.n_main, pending_out,
                               a.burst, a.refill, a.budget_ns, a.step_cap, cnt, rec);
 }
 
@@ -481,10 +492,20 @@ template <template <int> class Prop>
 cudaError_t launch_persistent_prop(const DevPlan &P, const DevState &s, const PersistentArgs &a,
                                    DevCounters *cnt, const DevRecords &rec, int fs, int grid,
                                    cudaStream_t st) {
-#define CRP_PERSIST(FSV) fp64_persistent_kernel<Prop, FSV><<<grid, 128, 0, st>>>(P, s, a, cnt, rec)
-    if (fs == FS_GRID) CRP_PERSIST(FS_GRID);
-    else if (fs == FS_PLANE_WAVE) CRP_PERSIST(FS_PLANE_WAVE);
-    else CRP_PERSIST(FS_GENERIC);
+#define CRP_PERSIST(FSV, CSV) fp64_persistent_kernel<Prop, FSV, CSV><<<grid, 128, 0, st>>>(P, s, a, cnt, rec)
+    if (fs == FS_GRID_PERIODIC) {
+        if (P.shape == CS_PM) CRP_PERSIST(FS_GRID_PERIODIC, CS_PM);
+        else if (P.shape == CS_PMO) CRP_PERSIST(FS_GRID_PERIODIC, CS_PMO);
+        else CRP_PERSIST(FS_GRID_PERIODIC, CS_GENERIC);
+    } else if (fs == FS_GRID) {
+        CRP_PERSIST(FS_GRID, CS_GENERIC);
+    } else if (fs == FS_PLANE_WAVE) {
+        if (P.shape == CS_PM) CRP_PERSIST(FS_PLANE_WAVE, CS_PM);
+        else if (P.shape == CS_PMO) CRP_PERSIST(FS_PLANE_WAVE, CS_PMO);
+        else CRP_PERSIST(FS_PLANE_WAVE, CS_GENERIC);
+    } else {
+        CRP_PERSIST(FS_GENERIC, CS_GENERIC);
+    }
 #undef CRP_PERSIST
     return cudaGetLastError();
 }
@@ -506,10 +527,12 @@ cudaError_t launch_prop(const DevPlan &P, const DevState &s, uint64_t n, int max
         step_cap, cnt, rec, perm, perm_out)
     // compiled chain shapes for the single-field signatures; the generic
     // field sum walks the module list
-    if (fs == FS_GRID) {
-        if (P.shape == CS_PM) CRP_CHUNK(FS_GRID, CS_PM);
-        else if (P.shape == CS_PMO) CRP_CHUNK(FS_GRID, CS_PMO);
-        else CRP_CHUNK(FS_GRID, CS_GENERIC);
+    if (fs == FS_GRID_PERIODIC) {
+        if (P.shape == CS_PM) CRP_CHUNK(FS_GRID_PERIODIC, CS_PM);
+        else if (P.shape == CS_PMO) CRP_CHUNK(FS_GRID_PERIODIC, CS_PMO);
+        else CRP_CHUNK(FS_GRID_PERIODIC, CS_GENERIC);
+    } else if (fs == FS_GRID) {
+        CRP_CHUNK(FS_GRID, CS_GENERIC);
     } else if (fs == FS_PLANE_WAVE) {
         if (P.shape == CS_PM) CRP_CHUNK(FS_PLANE_WAVE, CS_PM);
         else if (P.shape == CS_PMO) CRP_CHUNK(FS_PLANE_WAVE, CS_PMO);

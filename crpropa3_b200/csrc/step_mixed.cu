@@ -40,9 +40,11 @@ __device__ __forceinline__ int wrap(int i, int n, bool pow2) {
 // values (the reference's own interpolation arithmetic is FP32, Grid.h:571).
 // With a cell cache (FS_GRID kernels) the 8 corners are loaded only when the
 // cell changes.
-template <bool CACHE>
+// PER: the grid is periodic with power-of-two dimensions, has no clipVolume
+// and has the padded copy (FS_GRID_PERIODIC): those branches are compiled out.
+template <bool CACHE, bool PER = false>
 __device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y, double z, Cand *cc) {
-    if (g.clip_volume) {
+    if (!PER && g.clip_volume) {
         bool in = (x >= g.ox) && (x <= g.ex) && (y >= g.oy) && (y <= g.ey) && (z >= g.oz) && (z <= g.ez);
         if (!in) return f3mk(0.f, 0.f, 0.f);
     }
@@ -50,7 +52,7 @@ __device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y,
     double flx = floor(rx), fly = floor(ry), flz = floor(rz);
     float fx0 = (float)(rx - flx), fy0 = (float)(ry - fly), fz0 = (float)(rz - flz);
     int ix0, ix1, iy0, iy1, iz0, iz1;
-    if (g.reflective) {
+    if (!PER && g.reflective) {
         double r[3] = {rx, ry, rz};
         int n[3] = {g.nx, g.ny, g.nz}, lo[3], hi[3];
         float f[3];
@@ -71,7 +73,7 @@ __device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y,
         ix0 = lo[0]; ix1 = hi[0]; iy0 = lo[1]; iy1 = hi[1]; iz0 = lo[2]; iz1 = hi[2];
         fx0 = f[0]; fy0 = f[1]; fz0 = f[2];
     } else {
-        bool p2 = g.pow2 != 0;
+        bool p2 = PER || g.pow2 != 0;
         ix0 = wrap((int)flx, g.nx, p2); ix1 = (ix0 + 1 == g.nx) ? 0 : ix0 + 1;
         iy0 = wrap((int)fly, g.ny, p2); iy1 = (iy0 + 1 == g.ny) ? 0 : iy0 + 1;
         iz0 = wrap((int)flz, g.nz, p2); iz1 = (iz0 + 1 == g.nz) ? 0 : iz0 + 1;
@@ -87,7 +89,7 @@ __device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y,
     float (*c)[3] = CACHE ? cc->corner : lc;
     const long long k0 = (long long)idx[0], k7 = (long long)idx[7];
     if (!CACHE || k0 != cc->cell0 || k7 != cc->cell7) {
-        if (g.values4) {
+        if (PER || g.values4) {
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 float4 v = __ldg(g.values4 + idx[k]);
@@ -206,6 +208,7 @@ template <int FS>
 __device__ __forceinline__ f3 field_at(const DevPlan &P, double x, double y, double z,
                                        Cand *cc = nullptr, const PwTab *sh = nullptr) {
     if (FS == FS_GRID) return grid_field_t<true>(P.fields[0].grid, x, y, z, cc);
+    if (FS == FS_GRID_PERIODIC) return grid_field_t<true, true>(P.fields[0].grid, x, y, z, cc);
     if (FS == FS_PLANE_WAVE) return plane_wave_field(P.fields[0].pw, x, y, z, sh);
     if (P.n_fields == 1) return component_field(P.fields[0], x, y, z, sh);
     f3 b = f3mk(0.f, 0.f, 0.f);
@@ -740,14 +743,14 @@ __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_chunk_k
     chunk_body<Prop<FS>, CS>(P, s, n, max_steps, step_cap, cnt, rec, perm, perm_out);
 }
 
-template <template <int> class Prop, int FS>
+template <template <int> class Prop, int FS, int CS>
 __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_persistent_kernel(
     DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
     // the queue is written only between launches (advance_kernel)
     const DevQueue q = *a.q;
     const uint32_t *pending_in = q.cur ? a.list_b : a.list_a;
     uint32_t *pending_out = q.cur ? a.list_a : a.list_b;
-    persistent_body<Prop<FS>>(P, s, pending_in, q.n_pending, q.main_base, q.n_main, pending_out,
+    persistent_body<Prop<FS>, CS>(P, s, pending_in, q.n_pending, q.main_base, q.n_main, pending_out,
                               a.burst, a.refill, a.budget_ns, a.step_cap, cnt, rec);
 }
 
@@ -755,10 +758,20 @@ template <template <int> class Prop>
 cudaError_t launch_persistent_prop(const DevPlan &P, const DevState &s, const PersistentArgs &a,
                                    DevCounters *cnt, const DevRecords &rec, int fs, int grid,
                                    cudaStream_t st) {
-#define CRP_PERSIST(FSV) mixed_persistent_kernel<Prop, FSV><<<grid, 128, 0, st>>>(P, s, a, cnt, rec)
-    if (fs == FS_GRID) CRP_PERSIST(FS_GRID);
-    else if (fs == FS_PLANE_WAVE) CRP_PERSIST(FS_PLANE_WAVE);
-    else CRP_PERSIST(FS_GENERIC);
+#define CRP_PERSIST(FSV, CSV) mixed_persistent_kernel<Prop, FSV, CSV><<<grid, 128, 0, st>>>(P, s, a, cnt, rec)
+    if (fs == FS_GRID_PERIODIC) {
+        if (P.shape == CS_PM) CRP_PERSIST(FS_GRID_PERIODIC, CS_PM);
+        else if (P.shape == CS_PMO) CRP_PERSIST(FS_GRID_PERIODIC, CS_PMO);
+        else CRP_PERSIST(FS_GRID_PERIODIC, CS_GENERIC);
+    } else if (fs == FS_GRID) {
+        CRP_PERSIST(FS_GRID, CS_GENERIC);
+    } else if (fs == FS_PLANE_WAVE) {
+        if (P.shape == CS_PM) CRP_PERSIST(FS_PLANE_WAVE, CS_PM);
+        else if (P.shape == CS_PMO) CRP_PERSIST(FS_PLANE_WAVE, CS_PMO);
+        else CRP_PERSIST(FS_PLANE_WAVE, CS_GENERIC);
+    } else {
+        CRP_PERSIST(FS_GENERIC, CS_GENERIC);
+    }
 #undef CRP_PERSIST
     return cudaGetLastError();
 }
@@ -780,10 +793,12 @@ cudaError_t launch_prop(const DevPlan &P, const DevState &s, uint64_t n, int max
         step_cap, cnt, rec, perm, perm_out)
     // compiled chain shapes for the single-field signatures; the generic
     // field sum walks the module list
-    if (fs == FS_GRID) {
-        if (P.shape == CS_PM) CRP_CHUNK(FS_GRID, CS_PM);
-        else if (P.shape == CS_PMO) CRP_CHUNK(FS_GRID, CS_PMO);
-        else CRP_CHUNK(FS_GRID, CS_GENERIC);
+    if (fs == FS_GRID_PERIODIC) {
+        if (P.shape == CS_PM) CRP_CHUNK(FS_GRID_PERIODIC, CS_PM);
+        else if (P.shape == CS_PMO) CRP_CHUNK(FS_GRID_PERIODIC, CS_PMO);
+        else CRP_CHUNK(FS_GRID_PERIODIC, CS_GENERIC);
+    } else if (fs == FS_GRID) {
+        CRP_CHUNK(FS_GRID, CS_GENERIC);
     } else if (fs == FS_PLANE_WAVE) {
         if (P.shape == CS_PM) CRP_CHUNK(FS_PLANE_WAVE, CS_PM);
         else if (P.shape == CS_PMO) CRP_CHUNK(FS_PLANE_WAVE, CS_PMO);
@@ -831,7 +846,7 @@ cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, 
         mixed_sde_coop_kernel<FSV><<<grid, block, smem, st>>>(P, s, n, max_steps, step_cap, cnt, rec,  \
                                                               perm, perm_out, pw_field);               \
     } while (0)
-    if (fs == FS_GRID) CRP_SDE_COOP(FS_GRID);
+    if (fs == FS_GRID || fs == FS_GRID_PERIODIC) CRP_SDE_COOP(FS_GRID);
     else if (fs == FS_PLANE_WAVE) CRP_SDE_COOP(FS_PLANE_WAVE);
     else CRP_SDE_COOP(FS_GENERIC);
 #undef CRP_SDE_COOP
