@@ -654,6 +654,9 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "basis": "96 B (8 corners x 12 B) per particle-step over the stepping kernel time",
+                "note": "the register cell cache reloads corners only on a cell change, so DRAM "
+                        "traffic per step (traffic) is below the 96 B basis and frac can exceed 1; "
+                        "ncu shows the kernel issue/latency bound, not HBM bound",
                 "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step measured by ncu "
                                  "(profiles/mixed_chunk_kernel_bp_fixed_grid256_n131072.md) x "
                                  "particle-steps per timed launch"}

@@ -119,9 +119,11 @@ __device__ __forceinline__ void write_record(const DevRecords &rec, const Cand &
     rec.id[slot] = c.id;
 }
 
+// Per-thread counts of one launch (32-bit: a launch is bounded in steps or
+// device time), added to the run counters once per warp at its end.
 struct StepCount {
-    unsigned long long tries = 0;
-    unsigned long long evals = 0;
+    unsigned tries = 0;
+    unsigned evals = 0;
 };
 
 // MaximumTrajectoryLength::process (BreakCondition.cpp:42) and
@@ -195,7 +197,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // Add this thread's counts to the run counters, one atomic per warp.
 __device__ __forceinline__ void flush_counters(DevCounters *cnt, unsigned long long steps,
                                                const StepCount &sc) {
-    unsigned long long s = warp_sum(steps), t = warp_sum(sc.tries), e = warp_sum(sc.evals);
+    unsigned long long s = warp_sum(steps), t = warp_sum((unsigned long long)sc.tries),
+                       e = warp_sum((unsigned long long)sc.evals);
     if ((threadIdx.x & 31) == 0) {
         if (s) atomicAdd(&cnt->steps, s);
         if (t) atomicAdd(&cnt->tries, t);
@@ -237,12 +240,21 @@ __device__ __forceinline__ void chunk_body(const DevPlan &P, const DevState &s, 
         if (s.active[i]) {
             Cand c;
             load_cand(s, i, c);
+            // iterations this launch may take: max_steps, and what the
+            // per-candidate cap leaves; c.steps is kept current inside the
+            // loop only for modules that read it (Prop::kReadsStepCount)
+            int kmax = max_steps;
+            if (step_cap) {
+                const uint64_t left = step_cap > c.steps ? step_cap - c.steps : 0;
+                kmax = left < (uint64_t)kmax ? (int)left : kmax;
+            }
             int k = 0;
-            while (c.active && k < max_steps && (step_cap == 0 || c.steps < step_cap)) {
+            while (c.active && k < kmax) {
                 chain_process<Prop, CS>(P, c, rec, sc);
-                c.steps++;
+                if (Prop::kReadsStepCount) c.steps++;
                 k++;
             }
+            if (!Prop::kReadsStepCount) c.steps += (uint64_t)k;
             steps = (unsigned long long)k;
             still = c.active && (step_cap == 0 || c.steps < step_cap);
             store_cand(s, c);
@@ -309,12 +321,18 @@ __device__ __forceinline__ void persistent_body(const DevPlan &P, const DevState
             continue;
         }
         if (has) {
+            int kmax = burst;
+            if (step_cap) {
+                const uint64_t left = step_cap > c.steps ? step_cap - c.steps : 0;
+                kmax = left < (uint64_t)kmax ? (int)left : kmax;
+            }
             int k = 0;
-            while (c.active && k < burst && (step_cap == 0 || c.steps < step_cap)) {
+            while (c.active && k < kmax) {
                 chain_process<Prop, CS>(P, c, rec, sc);
-                c.steps++;
+                if (Prop::kReadsStepCount) c.steps++;
                 k++;
             }
+            if (!Prop::kReadsStepCount) c.steps += (uint64_t)k;
             steps += (unsigned long long)k;
             if (!c.active || (step_cap != 0 && c.steps >= step_cap)) {
                 store_cand(s, c);

@@ -361,7 +361,8 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
     if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_GRID) {
         const DevGrid &g = d.fields[0].grid;
         const bool padded = p->precision != CRP_PRECISION_MIXED || g.values4 != nullptr;
-        p->fs = (!g.reflective && !g.clip_volume && g.pow2 && padded) ? FS_GRID_PERIODIC : FS_GRID;
+        const bool small = (uint64_t)g.nx * g.ny * g.nz < (1ull << 31);  // 32-bit cell indices
+        p->fs = (!g.reflective && !g.clip_volume && g.pow2 && padded && small) ? FS_GRID_PERIODIC : FS_GRID;
     }
     else if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_PLANE_WAVE)
         p->fs = FS_PLANE_WAVE;

@@ -13,6 +13,8 @@
 // correctly rounded, which agrees with glibc's pow except where glibc itself
 // misrounds (about 1e-3 of inputs); cos in the wave sum and log/cos in the
 // normal draws are CUDA's, within a few ulp of glibc's.
+#include <type_traits>
+
 #include "chain.cuh"
 #include "crmath.cuh"
 #include "engine_internal.h"
@@ -98,14 +100,17 @@ __device__ __forceinline__ d3 grid_field_t(const DevGrid &g, d3 pos, Cand *cc) {
     }
     const float fx1 = (float)(1 - fX0), fy1 = (float)(1 - fY0), fz1 = (float)(1 - fZ0);
     const float fx0 = (float)fX0, fy0 = (float)fY0, fz0 = (float)fZ0;
-    const size_t sy = (size_t)g.nz, sx = (size_t)g.ny * (size_t)g.nz;
+    // cell indices: 32-bit for FS_GRID_PERIODIC grids (fewer than 2^31 cells)
+    using Index = typename std::conditional<PER, unsigned, size_t>::type;
+    const Index sy = (Index)g.nz, sx = (Index)g.ny * (Index)g.nz;
     const float *v = g.values;
-    const size_t b00 = (size_t)ix0 * sx + (size_t)iy0 * sy, b10 = (size_t)ix1 * sx + (size_t)iy0 * sy;
-    const size_t b01 = (size_t)ix0 * sx + (size_t)iy1 * sy, b11 = (size_t)ix1 * sx + (size_t)iy1 * sy;
+    const Index b00 = (Index)ix0 * sx + (Index)iy0 * sy, b10 = (Index)ix1 * sx + (Index)iy0 * sy;
+    const Index b01 = (Index)ix0 * sx + (Index)iy1 * sy, b11 = (Index)ix1 * sx + (Index)iy1 * sy;
     // the corner order of Grid.h:571-578
-    const float *p0 = v + 3 * (b00 + iz0), *p1 = v + 3 * (b10 + iz0), *p2 = v + 3 * (b01 + iz0),
-                *p3 = v + 3 * (b00 + iz1), *p4 = v + 3 * (b10 + iz1), *p5 = v + 3 * (b01 + iz1),
-                *p6 = v + 3 * (b11 + iz0), *p7 = v + 3 * (b11 + iz1);
+    const float *p0 = v + 3 * (size_t)(b00 + iz0), *p1 = v + 3 * (size_t)(b10 + iz0),
+                *p2 = v + 3 * (size_t)(b01 + iz0), *p3 = v + 3 * (size_t)(b00 + iz1),
+                *p4 = v + 3 * (size_t)(b10 + iz1), *p5 = v + 3 * (size_t)(b01 + iz1),
+                *p6 = v + 3 * (size_t)(b11 + iz0), *p7 = v + 3 * (size_t)(b11 + iz1);
     float lc[8][3];
     float (*c)[3] = CACHE ? cc->corner : lc;
     const long long k0 = (long long)(b00 + iz0), k7 = (long long)(b11 + iz1);
@@ -204,6 +209,7 @@ __device__ __forceinline__ void bp_dy(const DevPlan &P, d3 &x, d3 &u, double ste
 
 template <int FS, int MODE = 0>
 struct BP {
+    static constexpr bool kReadsStepCount = false;
     // PropagationBP::process (PropagationBP.cpp:62)
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
@@ -296,6 +302,7 @@ __device__ __forceinline__ void ck_try(const DevPlan &P, d3 x, d3 u, double h, d
 
 template <int FS, int MODE = 0>
 struct CK {
+    static constexpr bool kReadsStepCount = false;
     // PropagationCK::process (PropagationCK.cpp:77)
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
@@ -389,6 +396,7 @@ __device__ __forceinline__ void sde_try(const DevPlan &P, d3 PosIn, d3 &POut, d3
 
 template <int FS>
 struct SDE {
+    static constexpr bool kReadsStepCount = true;  // the Philox counter
     // DiffusionSDE::process (DiffusionSDE.cpp:47), without advection field.
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;

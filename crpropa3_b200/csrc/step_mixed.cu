@@ -12,6 +12,8 @@
 // against the FP64 quantities they are added to, which keeps the
 // accumulated error of 10^3-10^6 steps at the FP64 level of the increments'
 // relative error times their size.
+#include <type_traits>
+
 #include "chain.cuh"
 #include "engine_internal.h"
 
@@ -79,10 +81,12 @@ __device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y,
         iz0 = wrap((int)flz, g.nz, p2); iz1 = (iz0 + 1 == g.nz) ? 0 : iz0 + 1;
     }
     const float fx1 = 1.f - fx0, fy1 = 1.f - fy0, fz1 = 1.f - fz0;
-    const size_t sy = (size_t)g.nz, sx = (size_t)g.ny * (size_t)g.nz;
-    const size_t b00 = (size_t)ix0 * sx + (size_t)iy0 * sy, b10 = (size_t)ix1 * sx + (size_t)iy0 * sy;
-    const size_t b01 = (size_t)ix0 * sx + (size_t)iy1 * sy, b11 = (size_t)ix1 * sx + (size_t)iy1 * sy;
-    const size_t idx[8] = {b00 + iz0, b10 + iz0, b01 + iz0, b00 + iz1, b10 + iz1, b01 + iz1, b11 + iz0, b11 + iz1};
+    // cell indices: 32-bit for FS_GRID_PERIODIC grids (fewer than 2^31 cells)
+    using Index = typename std::conditional<PER, unsigned, size_t>::type;
+    const Index sy = (Index)g.nz, sx = (Index)g.ny * (Index)g.nz;
+    const Index b00 = (Index)ix0 * sx + (Index)iy0 * sy, b10 = (Index)ix1 * sx + (Index)iy0 * sy;
+    const Index b01 = (Index)ix0 * sx + (Index)iy1 * sy, b11 = (Index)ix1 * sx + (Index)iy1 * sy;
+    const Index idx[8] = {b00 + iz0, b10 + iz0, b01 + iz0, b00 + iz1, b10 + iz1, b01 + iz1, b11 + iz0, b11 + iz1};
     const float w[8] = {fx1 * fy1 * fz1, fx0 * fy1 * fz1, fx1 * fy0 * fz1, fx1 * fy1 * fz0,
                         fx0 * fy1 * fz0, fx1 * fy0 * fz0, fx0 * fy0 * fz1, fx0 * fy0 * fz0};
     float lc[8][3];
@@ -260,6 +264,7 @@ __device__ __forceinline__ void bp_dy(const DevPlan &P, double &x, double &y, do
 
 template <int FS, int MODE = 0>
 struct BP {
+    static constexpr bool kReadsStepCount = false;
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
         double q = c.q, step = m.max_step;
@@ -372,6 +377,7 @@ __device__ __forceinline__ double ck_try(const DevPlan &P, Cand &c, double h, fl
 
 template <int FS, int MODE = 0>
 struct CK {
+    static constexpr bool kReadsStepCount = false;
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
         double step = m.max_step;
@@ -628,6 +634,7 @@ __device__ __forceinline__ bool sde_co_consume(const DevPlan &P, const DevModule
 // run to completion, field evaluations in place.
 template <int FS>
 struct SDE {
+    static constexpr bool kReadsStepCount = true;  // the Philox counter
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         SdeCo co;
         if (!sde_co_begin<FS>(P, m, c, co)) return;
