@@ -34,7 +34,7 @@ import numpy as np  # noqa: E402
 METRIC = "particle-steps/s, 1 B200: mixed-prec vs FP64 at stated error; adjoint cost/fwd"
 UNIT = "particle-steps/s"
 ALGO_BYTES_PER_STEP = 96  # 8 corners x 12 B Grid3f payload per field evaluation
-TRAFFIC_B_PER_STEP = 27.3  # DRAM read+write per particle-step of the mixed kernel (ncu)
+TRAFFIC_B_PER_STEP = 32.6  # DRAM read+write per particle-step of the mixed kernel (ncu, full size)
 
 
 def log(*a):
@@ -657,8 +657,8 @@ def main():
                 "note": "the register cell cache reloads corners only on a cell change, so DRAM "
                         "traffic per step (traffic) is below the 96 B basis and frac can exceed 1; "
                         "ncu shows the kernel issue/latency bound, not HBM bound",
-                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step measured by ncu "
-                                 "(profiles/mixed_chunk_kernel_bp_fixed_grid256_n131072.md) x "
+                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step measured by ncu on a "
+                                 "full-size launch (profiles/launches_grid_bp_256.md) x "
                                  "particle-steps per timed launch"}
 
     adjoint = None if args.no_adjoint else adjoint_cost(dev, args)

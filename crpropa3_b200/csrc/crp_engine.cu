@@ -767,7 +767,7 @@ crp_status crp_autotune(crp_plan *p, const crp_candidates *c, uint64_t n, uint64
     };
     struct Cfg { int mode, ctas, refill, burst; };
     std::vector<Cfg> cfgs = {{CRP_MODE_CHUNKED, 0, 0, 0}};
-    for (int ctas : {1, 2, 3, 4})
+    for (int ctas : {1, 2, 3, 4, 6})
         for (int refill : {1, 8, 16, 32})
             for (int burst : {4, 16, 64}) cfgs.push_back({CRP_MODE_PERSISTENT, ctas, refill, burst});
     double best = -1, chunked = 0;

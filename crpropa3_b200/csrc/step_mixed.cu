@@ -17,8 +17,15 @@
 #include "chain.cuh"
 #include "engine_internal.h"
 
+// Resident blocks of 128 threads per SM the register budget of the
+// fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
+// grid workloads: both are bound by gather latency, and more warps in
+// flight pay until spills set in).
 #ifndef CRP_BP_FIXED_MIN_BLOCKS
-#define CRP_BP_FIXED_MIN_BLOCKS 1
+#define CRP_BP_FIXED_MIN_BLOCKS 6
+#endif
+#ifndef CRP_CK_MIN_BLOCKS
+#define CRP_CK_MIN_BLOCKS 3
 #endif
 
 namespace crp {
@@ -738,6 +745,7 @@ template <int FS> using BPFixed = BP<FS, 1>;
 // the fixed-step Boris push is latency bound on its gathers and wants warps
 template <class T> struct MinBlocks { static constexpr int value = 1; };
 template <int FS, int MODE> struct MinBlocks<BP<FS, MODE>> { static constexpr int value = MODE == 1 ? CRP_BP_FIXED_MIN_BLOCKS : 1; };
+template <int FS, int MODE> struct MinBlocks<CK<FS, MODE>> { static constexpr int value = CRP_CK_MIN_BLOCKS; };
 template <int FS> using BPAdaptive = BP<FS, 2>;
 template <int FS> using CKFixed = CK<FS, 1>;
 template <int FS> using CKAdaptive = CK<FS, 2>;
