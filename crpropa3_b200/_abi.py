@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # crp_status
 OK = 0
@@ -34,9 +34,13 @@ STATUS_NAMES = {
 }
 
 FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL = 1, 2, 3, 4
-MODULE_PROPAGATION, MODULE_MAX_TRAJECTORY_LENGTH, MODULE_OBSERVER = 1, 2, 3
+MODULE_PROPAGATION, MODULE_MAX_TRAJECTORY_LENGTH, MODULE_OBSERVER, MODULE_BOUNDARY = 1, 2, 3, 4
 PROP_CK, PROP_BP, PROP_SDE = 1, 2, 3
-OBSERVER_SURFACE_SPHERE, OBSERVER_DETECT_ALL = 1, 2
+OBSERVER_SURFACE_SPHERE, OBSERVER_DETECT_ALL, OBSERVER_SURFACE_PLANE, OBSERVER_SURFACE_BOX = 1, 2, 3, 4
+OBSERVER_TRACKING, OBSERVER_1D, OBSERVER_INACTIVE_VETO, OBSERVER_NUCLEUS_VETO = 5, 6, 7, 8
+OBSERVER_NEUTRINO_VETO, OBSERVER_PHOTON_VETO, OBSERVER_ELECTRON_VETO, OBSERVER_PARTICLE_ID_VETO = 9, 10, 11, 12
+MAX_OBSERVER_FEATURES = 4
+BOUNDARY_SPHERICAL, BOUNDARY_CUBIC, BOUNDARY_ELLIPSOIDAL, BOUNDARY_CYLINDRICAL = 1, 2, 3, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 FLAG_REJECTED, FLAG_DETECTED, FLAG_NAN = 1, 2, 4
 MODE_AUTO, MODE_CHUNKED, MODE_PERSISTENT = 0, 1, 2
@@ -65,13 +69,21 @@ class FieldComponent(C.Structure):
                 ("toroidal_b0", _d)]
 
 
+class FeatureDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("particle_id", C.c_int32), ("a", _d * 3), ("b", _d * 3),
+                ("r", _d), ("step", _d)]
+
+
 class ModuleDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("propagator", C.c_int32), ("tolerance", _d),
                 ("min_step", _d), ("max_step", _d), ("sde_epsilon", _d), ("sde_alpha", _d),
                 ("sde_scale", _d), ("max_length", _d), ("per_candidate_length", C.c_int32),
                 ("observer_feature", C.c_int32), ("sphere_center", _d * 3),
                 ("sphere_radius", _d), ("deactivate_on_detection", C.c_int32),
-                ("record", C.c_int32)]
+                ("record", C.c_int32), ("n_features", C.c_int32), ("boundary", C.c_int32),
+                ("features", FeatureDesc * 4), ("boundary_a", _d * 3), ("boundary_b", _d * 3),
+                ("boundary_size", _d), ("boundary_radius", _d), ("boundary_margin", _d),
+                ("boundary_limit_step", C.c_int32), ("_pad1", C.c_int32)]
 
 
 class PlanDesc(C.Structure):

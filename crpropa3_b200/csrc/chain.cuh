@@ -141,28 +141,149 @@ __device__ __forceinline__ void max_trajectory_length(const DevModule &m, Cand &
     }
 }
 
-// Observer::process (Observer.cpp:27) with ObserverSurface(Sphere)
-// (Observer.cpp:394, Geometry.cpp:41) or ObserverDetectAll (Observer.cpp:93).
-__device__ __forceinline__ void observer(const DevModule &m, Cand &c, const DevRecords &rec,
-                                         int mi) {
-    bool detected;
-    if (m.observer == CRP_OBSERVER_SURFACE_SPHERE) {
-        double ax = c.x - m.cx, ay = c.y - m.cy, az = c.z - m.cz;
-        double bx = c.px - m.cx, by = c.py - m.cy, bz = c.pz - m.cz;
-        double cd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)), __dmul_rn(az, az))) - m.radius;
-        double pd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz))) - m.radius;
-        double lim = fabs(cd);
-        c.next = (lim < c.next) ? lim : c.next;
-        if (cd * pd > 0) detected = false;
-        else if (pd == 0) detected = false;
-        else detected = true;
-    } else {
-        detected = true;
+// Arithmetic of the reference's geometry in double precision without
+// contraction (this header is also compiled where multiply-adds are fused):
+// |v| = sqrt(x*x + y*y + z*z) (Vector3::getR), n.v = x*v.x + y*v.y + z*v.z.
+__device__ __forceinline__ double nc_norm(double x, double y, double z) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+__device__ __forceinline__ double nc_dot(double ax, double ay, double az, double bx, double by, double bz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
+}
+__device__ __forceinline__ double dmin_std(double a, double b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ double dmax_std(double a, double b) { return (a < b) ? b : a; }  // std::max
+// Candidate::limitNextStep (Candidate.cpp:102)
+__device__ __forceinline__ void limit_next(Cand &c, double step) { c.next = (step < c.next) ? step : c.next; }
+
+// ParticleID.cpp:37 isNucleus (neutron counted) with HepPID::isNucleus
+// (ParticleIDMethods.cc:242): proton, or +/-10LZZZAAAI with A >= Z.
+__device__ __forceinline__ bool is_nucleus(int id) {
+    if (id == 2112) return true;
+    const int a = id < 0 ? -id : id;
+    if (a == 2212) return true;
+    if ((a / 1000000000) % 10 == 1 && (a / 100000000) % 10 == 0)
+        return (a / 10) % 1000 >= (a / 10000) % 1000;
+    return false;
+}
+
+// Surface::distance of the observer surfaces (Geometry.cpp:19, 41, 64).
+__device__ __forceinline__ double surface_distance(const DevFeature &f, double x, double y, double z) {
+    if (f.kind == CRP_OBSERVER_SURFACE_SPHERE)
+        return __dsub_rn(nc_norm(__dsub_rn(x, f.ax), __dsub_rn(y, f.ay), __dsub_rn(z, f.az)), f.r);
+    if (f.kind == CRP_OBSERVER_SURFACE_PLANE)
+        return nc_dot(f.bx, f.by, f.bz, __dsub_rn(x, f.ax), __dsub_rn(y, f.ay), __dsub_rn(z, f.az));
+    // ParaxialBox: X = point - corner - size / 2
+    const double hx = f.bx / 2., hy = f.by / 2., hz = f.bz / 2.;
+    const double X = __dsub_rn(__dsub_rn(x, f.ax), hx), Y = __dsub_rn(__dsub_rn(y, f.ay), hy),
+                 Z = __dsub_rn(__dsub_rn(z, f.az), hz);
+    if ((fabs(X) <= hx) && (fabs(Y) <= hy) && (fabs(Z) <= hz)) {
+        const double d = dmin_std(__dsub_rn(hx, fabs(X)), dmin_std(__dsub_rn(hy, fabs(Y)), __dsub_rn(hz, fabs(Z))));
+        return -1. * d;
     }
-    if (detected) {
+    const double a = dmax_std(0., __dsub_rn(fabs(X), hx)), b = dmax_std(0., __dsub_rn(fabs(Y), hy)),
+                 cc = dmax_std(0., __dsub_rn(fabs(Z), hz));
+    return nc_norm(a, b, cc);
+}
+
+enum { DET_NOTHING = 0, DET_DETECTED = 1, DET_VETO = 2 };
+
+// ObserverFeature::checkDetection of each feature (Observer.cpp:93-394).
+__device__ __forceinline__ int check_feature(const DevFeature &f, Cand &c) {
+    switch (f.kind) {
+    case CRP_OBSERVER_SURFACE_SPHERE:
+    case CRP_OBSERVER_SURFACE_PLANE:
+    case CRP_OBSERVER_SURFACE_BOX: {  // ObserverSurface (Observer.cpp:394)
+        const double cd = surface_distance(f, c.x, c.y, c.z);
+        const double pd = surface_distance(f, c.px, c.py, c.pz);
+        limit_next(c, fabs(cd));
+        if (__dmul_rn(cd, pd) > 0) return DET_NOTHING;
+        if (pd == 0) return DET_NOTHING;
+        return DET_DETECTED;
+    }
+    case CRP_OBSERVER_DETECT_ALL: return DET_DETECTED;
+    case CRP_OBSERVER_TRACKING: {
+        const double d = nc_norm(__dsub_rn(c.x, f.ax), __dsub_rn(c.y, f.ay), __dsub_rn(c.z, f.az));
+        if (d > f.r) {
+            limit_next(c, fabs(__dsub_rn(d, f.r)));
+            return DET_NOTHING;
+        }
+        limit_next(c, f.step);
+        return DET_DETECTED;
+    }
+    case CRP_OBSERVER_1D:
+        if (c.x > 0) {
+            limit_next(c, c.x);
+            return DET_NOTHING;
+        }
+        return DET_DETECTED;
+    case CRP_OBSERVER_INACTIVE_VETO: return c.active ? DET_NOTHING : DET_VETO;
+    case CRP_OBSERVER_NUCLEUS_VETO: return is_nucleus(c.id) ? DET_VETO : DET_NOTHING;
+    case CRP_OBSERVER_NEUTRINO_VETO: {
+        const int a = c.id < 0 ? -c.id : c.id;
+        return (a == 12 || a == 14 || a == 16) ? DET_VETO : DET_NOTHING;
+    }
+    case CRP_OBSERVER_PHOTON_VETO: return c.id == 22 ? DET_VETO : DET_NOTHING;
+    case CRP_OBSERVER_ELECTRON_VETO: return (c.id == 11 || c.id == -11) ? DET_VETO : DET_NOTHING;
+    default: return c.id == f.pid ? DET_VETO : DET_NOTHING;  // CRP_OBSERVER_PARTICLE_ID_VETO
+    }
+}
+
+// Observer::process (Observer.cpp:27): every feature checked in order (each
+// may limit the next step); detected when one detects and none vetoes.
+__device__ __forceinline__ void observer(const DevPlan &P, const DevModule &m, Cand &c,
+                                         const DevRecords &rec, int mi) {
+    int state = DET_NOTHING;
+#pragma unroll 1
+    for (int f = 0; f < m.nfeat; f++) {
+        const int st = check_feature(P.feat[m.feat0 + f], c);
+        if (st == DET_VETO) state = DET_VETO;
+        else if (st == DET_DETECTED && state != DET_VETO) state = DET_DETECTED;
+    }
+    if (state == DET_DETECTED) {
         if (m.record) write_record(rec, c, mi);
         c.flags |= CRP_FLAG_DETECTED;
         if (m.deactivate) c.active = false;
+    }
+}
+
+// AbstractCondition::reject (Module.cpp:25) of a boundary.
+__device__ __forceinline__ void reject(const DevModule &m, Cand &c, const DevRecords &rec, int mi) {
+    if (m.record) write_record(rec, c, mi);
+    c.flags |= CRP_FLAG_REJECTED;
+    c.active = false;
+}
+
+// CubicBoundary, SphericalBoundary, EllipsoidalBoundary, CylindricalBoundary
+// ::process (Boundary.cpp:171, 216, 259, 303).
+__device__ __forceinline__ void boundary(const DevModule &m, Cand &c, const DevRecords &rec, int mi) {
+    if (m.boundary == CRP_BOUNDARY_CUBIC) {
+        const double rx = __dsub_rn(c.x, m.cx), ry = __dsub_rn(c.y, m.cy), rz = __dsub_rn(c.z, m.cz);
+        const double lo = dmin_std(rx, dmin_std(ry, rz)), hi = dmax_std(rx, dmax_std(ry, rz));
+        if ((lo <= 0) || (hi >= m.bsize)) reject(m, c, rec, mi);
+        if (m.limit_step) {
+            limit_next(c, __dadd_rn(lo, m.margin));
+            limit_next(c, __dadd_rn(__dsub_rn(m.bsize, hi), m.margin));
+        }
+    } else if (m.boundary == CRP_BOUNDARY_SPHERICAL) {
+        const double d = nc_norm(__dsub_rn(c.x, m.cx), __dsub_rn(c.y, m.cy), __dsub_rn(c.z, m.cz));
+        if (d >= m.bsize) reject(m, c, rec, mi);
+        if (m.limit_step) limit_next(c, __dadd_rn(__dsub_rn(m.bsize, d), m.margin));
+    } else if (m.boundary == CRP_BOUNDARY_ELLIPSOIDAL) {
+        const double d = __dadd_rn(nc_norm(__dsub_rn(c.x, m.cx), __dsub_rn(c.y, m.cy), __dsub_rn(c.z, m.cz)),
+                                   nc_norm(__dsub_rn(c.x, m.bx), __dsub_rn(c.y, m.by), __dsub_rn(c.z, m.bz)));
+        if (d >= m.bsize) reject(m, c, rec, mi);
+        if (m.limit_step) limit_next(c, __dadd_rn(__dsub_rn(m.bsize, d), m.margin));
+    } else {  // CRP_BOUNDARY_CYLINDRICAL; pow(v, 2.) and pow(v, 0.5) as v*v and sqrt(v)
+        const double dx = __dsub_rn(c.x, m.cx), dy = __dsub_rn(c.y, m.cy), dz = __dsub_rn(c.z, m.cz);
+        const double R2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+        const double Z = fabs(dz);
+        if (R2 < __dmul_rn(m.bradius, m.bradius) && Z < m.bsize / 2.) {
+            if (m.limit_step)
+                limit_next(c, __dadd_rn(dmin_std(__dsub_rn(m.bradius, __dsqrt_rn(R2)), __dsub_rn(m.bsize / 2., Z)),
+                                        m.margin));
+            return;
+        }
+        reject(m, c, rec, mi);
     }
 }
 
@@ -176,7 +297,7 @@ __device__ __forceinline__ void chain_process(const DevPlan &P, Cand &c, const D
     if (CS == CS_PM || CS == CS_PMO) {
         Prop::process(P, P.modules[0], c, sc);
         max_trajectory_length(P.modules[1], c, rec, 1);
-        if (CS == CS_PMO) observer(P.modules[2], c, rec, 2);
+        if (CS == CS_PMO) observer(P, P.modules[2], c, rec, 2);
         return;
     }
 #pragma unroll 1
@@ -184,7 +305,8 @@ __device__ __forceinline__ void chain_process(const DevPlan &P, Cand &c, const D
         const DevModule &m = P.modules[mi];
         if (m.kind == CRP_MODULE_PROPAGATION) Prop::process(P, m, c, sc);
         else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) max_trajectory_length(m, c, rec, mi);
-        else observer(m, c, rec, mi);
+        else if (m.kind == CRP_MODULE_OBSERVER) observer(P, m, c, rec, mi);
+        else boundary(m, c, rec, mi);
     }
 }
 

@@ -145,8 +145,19 @@ crp_status validate_module(const crp_module_desc &m) {
         }
     } else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
     } else if (m.kind == CRP_MODULE_OBSERVER) {
-        if (m.observer_feature != CRP_OBSERVER_SURFACE_SPHERE && m.observer_feature != CRP_OBSERVER_DETECT_ALL)
-            return fail(CRP_ERR_UNSUPPORTED, "unsupported observer feature %d", m.observer_feature);
+        if (m.n_features < 0 || m.n_features > CRP_MAX_OBSERVER_FEATURES)
+            return fail(CRP_ERR_UNSUPPORTED, "at most %d observer features (got %d)", CRP_MAX_OBSERVER_FEATURES,
+                        m.n_features);
+        if (m.n_features == 0) {
+            if (m.observer_feature != CRP_OBSERVER_SURFACE_SPHERE && m.observer_feature != CRP_OBSERVER_DETECT_ALL)
+                return fail(CRP_ERR_UNSUPPORTED, "unsupported observer feature %d", m.observer_feature);
+        }
+        for (int f = 0; f < m.n_features; f++)
+            if (m.features[f].kind < CRP_OBSERVER_SURFACE_SPHERE || m.features[f].kind > CRP_OBSERVER_PARTICLE_ID_VETO)
+                return fail(CRP_ERR_UNSUPPORTED, "unsupported observer feature %d", m.features[f].kind);
+    } else if (m.kind == CRP_MODULE_BOUNDARY) {
+        if (m.boundary < CRP_BOUNDARY_SPHERICAL || m.boundary > CRP_BOUNDARY_CYLINDRICAL)
+            return fail(CRP_ERR_UNSUPPORTED, "unsupported boundary %d", m.boundary);
     } else {
         return fail(CRP_ERR_UNSUPPORTED, "unsupported module kind %d", m.kind);
     }
@@ -346,6 +357,7 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
         crp_status st = build_component(p, desc->fields[i], d.fields[i]);
         if (st) { delete p; return st; }
     }
+    int nfeat_total = 0;
     for (int i = 0; i < desc->n_modules; i++) {
         const crp_module_desc &m = desc->modules[i];
         DevModule &dm = d.modules[i];
@@ -357,6 +369,36 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
         dm.cx = m.sphere_center[0]; dm.cy = m.sphere_center[1]; dm.cz = m.sphere_center[2];
         dm.radius = m.sphere_radius;
         dm.deactivate = m.deactivate_on_detection; dm.record = m.record;
+        if (m.kind == CRP_MODULE_OBSERVER) {
+            // the single legacy feature becomes a one-entry feature list
+            crp_observer_feature_desc legacy{};
+            legacy.kind = m.observer_feature;
+            for (int a = 0; a < 3; a++) legacy.a[a] = m.sphere_center[a];
+            legacy.r = m.sphere_radius;
+            const crp_observer_feature_desc *fs = m.n_features > 0 ? m.features : &legacy;
+            const int nf = m.n_features > 0 ? m.n_features : 1;
+            if (nfeat_total + nf > kMaxFeatures) {
+                delete p;
+                return fail(CRP_ERR_UNSUPPORTED, "at most %d observer features per chain", kMaxFeatures);
+            }
+            dm.feat0 = nfeat_total;
+            dm.nfeat = nf;
+            for (int f = 0; f < nf; f++) {
+                DevFeature &df = d.feat[nfeat_total++];
+                df.kind = fs[f].kind;
+                df.pid = fs[f].particle_id;
+                df.ax = fs[f].a[0]; df.ay = fs[f].a[1]; df.az = fs[f].a[2];
+                df.bx = fs[f].b[0]; df.by = fs[f].b[1]; df.bz = fs[f].b[2];
+                df.r = fs[f].r; df.step = fs[f].step;
+            }
+        }
+        if (m.kind == CRP_MODULE_BOUNDARY) {
+            dm.boundary = m.boundary;
+            dm.limit_step = m.boundary_limit_step;
+            dm.cx = m.boundary_a[0]; dm.cy = m.boundary_a[1]; dm.cz = m.boundary_a[2];
+            dm.bx = m.boundary_b[0]; dm.by = m.boundary_b[1]; dm.bz = m.boundary_b[2];
+            dm.bsize = m.boundary_size; dm.bradius = m.boundary_radius; dm.margin = m.boundary_margin;
+        }
     }
     if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_GRID) {
         const DevGrid &g = d.fields[0].grid;

@@ -10,6 +10,7 @@ namespace crp {
 
 constexpr int kMaxFields = 4;
 constexpr int kMaxModules = 8;
+constexpr int kMaxFeatures = 8;  // observer features of all modules of a plan
 
 struct DevGrid {
     const float *values;   // packed Vector3f cells, 12 B each (Grid.h:338 order)
@@ -55,6 +56,20 @@ struct DevModule {
     double cx, cy, cz, radius;
     int deactivate;
     int record;
+    int feat0, nfeat;      // observer: features feat0 .. feat0 + nfeat - 1 of DevPlan::feat
+    int boundary;          // crp_boundary_kind
+    int limit_step;        // boundary setLimitStep
+    double bx, by, bz;     // boundary: a = (cx, cy, cz), b
+    double bsize, bradius, margin;
+};
+
+// One observer feature (crp_observer_feature_desc).
+struct DevFeature {
+    int kind;
+    int pid;
+    double ax, ay, az;
+    double bx, by, bz;
+    double r, step;
 };
 
 // Module sequences the stepping kernels are compiled for: CS_PM =
@@ -71,6 +86,7 @@ struct DevPlan {
     uint64_t seed;
     DevComponent fields[kMaxFields];
     DevModule modules[kMaxModules];
+    DevFeature feat[kMaxFeatures];
 };
 
 // Candidate arrays (include/crp_gpu.h crp_candidates), device pointers.

@@ -657,7 +657,8 @@ __device__ __forceinline__ void chain_part(const DevPlan &P, Cand &c, const DevR
     for (int mi = from; mi < to; mi++) {
         const DevModule &m = P.modules[mi];
         if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) max_trajectory_length(m, c, rec, mi);
-        else if (m.kind == CRP_MODULE_OBSERVER) observer(m, c, rec, mi);
+        else if (m.kind == CRP_MODULE_OBSERVER) observer(P, m, c, rec, mi);
+        else if (m.kind == CRP_MODULE_BOUNDARY) boundary(m, c, rec, mi);
     }
 }
 

@@ -78,11 +78,41 @@ class MaxTrajectoryLength:
 
 
 @dataclass
+class Feature:
+    """One observer feature (crp_observer_feature_desc): a, b, r, step and
+    particle_id as the feature kind uses them."""
+    kind: int
+    a: Sequence[float] = (0.0, 0.0, 0.0)
+    b: Sequence[float] = (0.0, 0.0, 0.0)
+    r: float = 0.0
+    step: float = 0.0
+    particle_id: int = 0
+
+
+@dataclass
 class ObserverSpec:
+    """Observer (Observer.cpp:27): the single sphere/detect-all feature given
+    by feature/center/radius, or the list `features` (at most 4)."""
     feature: int = _abi.OBSERVER_SURFACE_SPHERE
     center: Sequence[float] = (0.0, 0.0, 0.0)
     radius: float = 0.0
     deactivate: bool = True
+    record: bool = False
+    features: Optional[List[Feature]] = None
+
+
+@dataclass
+class BoundarySpec:
+    """Spherical/Cubic/Ellipsoidal/CylindricalBoundary (Boundary.cpp:171-303):
+    a = centre / origin / first focal point, b = second focal point, size =
+    radius / edge / major axis / height, radius = cylinder radius."""
+    kind: int
+    a: Sequence[float] = (0.0, 0.0, 0.0)
+    b: Sequence[float] = (0.0, 0.0, 0.0)
+    size: float = 0.0
+    radius: float = 0.0
+    margin: float = 0.1 * 3.0856775814913673e19  # 0.1 kpc, the reference default
+    limit_step: bool = True
     record: bool = False
 
 
@@ -176,6 +206,23 @@ class ChainSpec:
             d.sphere_center[:] = _v3(m.center)
             d.sphere_radius = float(m.radius)
             d.deactivate_on_detection = int(bool(m.deactivate))
+            d.record = int(bool(m.record))
+            feats = m.features or []
+            if len(feats) > _abi.MAX_OBSERVER_FEATURES:
+                raise ValueError(f"at most {_abi.MAX_OBSERVER_FEATURES} observer features")
+            d.n_features = len(feats)
+            for i, f in enumerate(feats):
+                fd = d.features[i]
+                fd.kind, fd.particle_id = int(f.kind), int(f.particle_id)
+                fd.a[:], fd.b[:] = _v3(f.a), _v3(f.b)
+                fd.r, fd.step = float(f.r), float(f.step)
+        elif isinstance(m, BoundarySpec):
+            d.kind = _abi.MODULE_BOUNDARY
+            d.boundary = int(m.kind)
+            d.boundary_a[:], d.boundary_b[:] = _v3(m.a), _v3(m.b)
+            d.boundary_size, d.boundary_radius = float(m.size), float(m.radius)
+            d.boundary_margin = float(m.margin)
+            d.boundary_limit_step = int(bool(m.limit_step))
             d.record = int(bool(m.record))
         else:
             raise TypeError(f"unsupported module {type(m).__name__}")

@@ -8,6 +8,7 @@
 #include "crpropa/Grid.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
+#include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
 #include "crpropa/module/Observer.h"
@@ -73,6 +74,32 @@ CRPGPU_MEMBER(RejectAction, AbstractCondition, ref_ptr<Module>, rejectAction);  
 CRPGPU_MEMBER(RejectInactive, AbstractCondition, bool, makeRejectedInactive);
 CRPGPU_MEMBER(RejectKey, AbstractCondition, std::string, rejectFlagKey);
 CRPGPU_MEMBER(RejectValue, AbstractCondition, std::string, rejectFlagValue);
+CRPGPU_MEMBER(PlaneX0, Plane, Vector3d, x0);                           // Geometry.h:45
+CRPGPU_MEMBER(PlaneN, Plane, Vector3d, n);
+CRPGPU_MEMBER(BoxCorner, ParaxialBox, Vector3d, corner);               // Geometry.h:77
+CRPGPU_MEMBER(BoxSize, ParaxialBox, Vector3d, size);
+CRPGPU_MEMBER(TrackCenter, ObserverTracking, Vector3d, center);        // Observer.h:109
+CRPGPU_MEMBER(TrackRadius, ObserverTracking, double, radius);
+CRPGPU_MEMBER(TrackStep, ObserverTracking, double, stepSize);
+CRPGPU_MEMBER(VetoId, ObserverParticleIdVeto, int, vetoParticleId);    // Observer.h:226
+CRPGPU_MEMBER(CubeOrigin, CubicBoundary, Vector3d, origin);            // Boundary.h:104
+CRPGPU_MEMBER(CubeSize, CubicBoundary, double, size);
+CRPGPU_MEMBER(CubeMargin, CubicBoundary, double, margin);
+CRPGPU_MEMBER(CubeLimit, CubicBoundary, bool, limitStep);
+CRPGPU_MEMBER(SphCenter, SphericalBoundary, Vector3d, center);         // Boundary.h:136
+CRPGPU_MEMBER(SphRadius, SphericalBoundary, double, radius);
+CRPGPU_MEMBER(SphMargin, SphericalBoundary, double, margin);
+CRPGPU_MEMBER(SphLimit, SphericalBoundary, bool, limitStep);
+CRPGPU_MEMBER(EllF1, EllipsoidalBoundary, Vector3d, focalPoint1);      // Boundary.h:169
+CRPGPU_MEMBER(EllF2, EllipsoidalBoundary, Vector3d, focalPoint2);
+CRPGPU_MEMBER(EllAxis, EllipsoidalBoundary, double, majorAxis);
+CRPGPU_MEMBER(EllMargin, EllipsoidalBoundary, double, margin);
+CRPGPU_MEMBER(EllLimit, EllipsoidalBoundary, bool, limitStep);
+CRPGPU_MEMBER(CylOrigin, CylindricalBoundary, Vector3d, origin);       // Boundary.h:204
+CRPGPU_MEMBER(CylHeight, CylindricalBoundary, double, height);
+CRPGPU_MEMBER(CylRadius, CylindricalBoundary, double, radius);
+CRPGPU_MEMBER(CylMargin, CylindricalBoundary, double, margin);
+CRPGPU_MEMBER(CylLimit, CylindricalBoundary, bool, limitStep);
 // ParticleState::setDirection normalises (ParticleState.cpp:30); the device
 // already wrote the normalised direction the reference would hold, and a
 // second normalisation can move its last bit.
@@ -115,7 +142,7 @@ void check(crp_status st) {
 
 // One chain module's host-side actions, replayed from the device's records.
 struct Action {
-    int kind;  // CRP_MODULE_MAX_TRAJECTORY_LENGTH or CRP_MODULE_OBSERVER
+    int kind;  // CRP_MODULE_MAX_TRAJECTORY_LENGTH, CRP_MODULE_BOUNDARY or CRP_MODULE_OBSERVER
     const AbstractCondition *condition;
     const Observer *observer;
 };
@@ -342,34 +369,144 @@ struct Translation {
                 text << "  module: Observer without features (never detects; dropped)\n";
                 return;
             }
-            if (fs.size() > 1) throw Unsupported("Observer with more than one feature");
+            if (fs.size() > CRP_MAX_OBSERVER_FEATURES)
+                throw Unsupported("Observer with more than 4 features");
             crp_module_desc d = blank(CRP_MODULE_OBSERVER);
-            const ObserverFeature *f = fs[0].get();
-            if (const ObserverSurface *s = dynamic_cast<const ObserverSurface *>(f)) {
-                const Surface *surf = (s->*member(SurfaceOf())).get();
-                const Sphere *sp = dynamic_cast<const Sphere *>(surf);
-                if (!sp) throw Unsupported("ObserverSurface over " + name_of(surf));
-                const Vector3d &c = sp->*member(SphereCenter());
-                d.observer_feature = CRP_OBSERVER_SURFACE_SPHERE;
-                for (int a = 0; a < 3; a++) d.sphere_center[a] = c.data[a];
-                d.sphere_radius = sp->*member(SphereRadius());
-                text << "  module: Observer ObserverSurface(Sphere center " << c.x << " " << c.y
-                     << " " << c.z << " radius " << d.sphere_radius << ")";
-            } else if (typeid(*f) == typeid(ObserverDetectAll)) {
-                d.observer_feature = CRP_OBSERVER_DETECT_ALL;
-                text << "  module: Observer ObserverDetectAll";
-            } else {
-                throw Unsupported("observer feature " + name_of(f) + " has no device form");
+            d.n_features = int32_t(fs.size());
+            text << "  module: Observer";
+            for (size_t k = 0; k < fs.size(); k++) {
+                feature(fs[k].get(), d.features[k]);
+                text << (k ? ", " : " ");
             }
             d.deactivate_on_detection = (o->*member(ObserverInactive())) ? 1 : 0;
             d.record = 1;
             const Module *act = (o->*member(ObserverAction())).get();
             text << " deactivate " << d.deactivate_on_detection << " action "
                  << (act ? name_of(act) : std::string("none")) << "\n";
-            Action a = {CRP_MODULE_OBSERVER, 0, o};
-            push(d, a);
+            Action ac = {CRP_MODULE_OBSERVER, 0, o};
+            push(d, ac);
+        } else if (dynamic_cast<const CubicBoundary *>(m) || dynamic_cast<const SphericalBoundary *>(m) ||
+                   dynamic_cast<const EllipsoidalBoundary *>(m) || dynamic_cast<const CylindricalBoundary *>(m)) {
+            const AbstractCondition *c = dynamic_cast<const AbstractCondition *>(m);
+            crp_module_desc d = blank(CRP_MODULE_BOUNDARY);
+            d.record = 1;
+            condition(c);
+            Vector3d a0, b0;
+            if (const CubicBoundary *q = dynamic_cast<const CubicBoundary *>(m)) {
+                d.boundary = CRP_BOUNDARY_CUBIC;
+                a0 = q->*member(CubeOrigin());
+                d.boundary_size = q->*member(CubeSize());
+                d.boundary_margin = q->*member(CubeMargin());
+                d.boundary_limit_step = (q->*member(CubeLimit())) ? 1 : 0;
+                text << "  module: CubicBoundary size " << d.boundary_size;
+            } else if (const SphericalBoundary *q = dynamic_cast<const SphericalBoundary *>(m)) {
+                d.boundary = CRP_BOUNDARY_SPHERICAL;
+                a0 = q->*member(SphCenter());
+                d.boundary_size = q->*member(SphRadius());
+                d.boundary_margin = q->*member(SphMargin());
+                d.boundary_limit_step = (q->*member(SphLimit())) ? 1 : 0;
+                text << "  module: SphericalBoundary radius " << d.boundary_size;
+            } else if (const EllipsoidalBoundary *q = dynamic_cast<const EllipsoidalBoundary *>(m)) {
+                d.boundary = CRP_BOUNDARY_ELLIPSOIDAL;
+                a0 = q->*member(EllF1());
+                b0 = q->*member(EllF2());
+                d.boundary_size = q->*member(EllAxis());
+                d.boundary_margin = q->*member(EllMargin());
+                d.boundary_limit_step = (q->*member(EllLimit())) ? 1 : 0;
+                text << "  module: EllipsoidalBoundary major axis " << d.boundary_size;
+            } else {
+                const CylindricalBoundary *cy = dynamic_cast<const CylindricalBoundary *>(m);
+                d.boundary = CRP_BOUNDARY_CYLINDRICAL;
+                a0 = cy->*member(CylOrigin());
+                d.boundary_size = cy->*member(CylHeight());
+                d.boundary_radius = cy->*member(CylRadius());
+                d.boundary_margin = cy->*member(CylMargin());
+                d.boundary_limit_step = (cy->*member(CylLimit())) ? 1 : 0;
+                text << "  module: CylindricalBoundary height " << d.boundary_size << " radius "
+                     << d.boundary_radius;
+            }
+            for (int k = 0; k < 3; k++) {
+                d.boundary_a[k] = a0.data[k];
+                d.boundary_b[k] = b0.data[k];
+            }
+            text << " margin " << d.boundary_margin << " limitStep " << d.boundary_limit_step << "\n";
+            Action ac = {CRP_MODULE_BOUNDARY, c, 0};
+            push(d, ac);
         } else {
             throw Unsupported("module " + name_of(m) + " has no device form");
+        }
+    }
+
+    // One ObserverFeature; exact classes only (a subclass may override checkDetection).
+    void feature(const ObserverFeature *f, crp_observer_feature_desc &fd) {
+        std::memset(&fd, 0, sizeof(fd));
+        const std::type_info &ti = typeid(*f);
+        if (const ObserverSurface *sf = dynamic_cast<const ObserverSurface *>(f)) {
+            if (ti != typeid(ObserverSurface)) throw Unsupported("observer feature " + name_of(f) + " has no device form");
+            const Surface *surf = (sf->*member(SurfaceOf())).get();
+            Vector3d a, b;
+            double r = 0;
+            if (surf && typeid(*surf) == typeid(Sphere)) {
+                const Sphere *sp = static_cast<const Sphere *>(surf);
+                fd.kind = CRP_OBSERVER_SURFACE_SPHERE;
+                a = sp->*member(SphereCenter());
+                r = sp->*member(SphereRadius());
+                text << "ObserverSurface(Sphere center " << a.x << " " << a.y << " " << a.z << " radius " << r << ")";
+            } else if (surf && typeid(*surf) == typeid(Plane)) {
+                const Plane *pl = static_cast<const Plane *>(surf);
+                fd.kind = CRP_OBSERVER_SURFACE_PLANE;
+                a = pl->*member(PlaneX0());
+                b = pl->*member(PlaneN());
+                text << "ObserverSurface(Plane)";
+            } else if (surf && typeid(*surf) == typeid(ParaxialBox)) {
+                const ParaxialBox *bx = static_cast<const ParaxialBox *>(surf);
+                fd.kind = CRP_OBSERVER_SURFACE_BOX;
+                a = bx->*member(BoxCorner());
+                b = bx->*member(BoxSize());
+                text << "ObserverSurface(ParaxialBox)";
+            } else {
+                throw Unsupported("ObserverSurface over " + (surf ? name_of(surf) : std::string("nothing")));
+            }
+            for (int k = 0; k < 3; k++) {
+                fd.a[k] = a.data[k];
+                fd.b[k] = b.data[k];
+            }
+            fd.r = r;
+        } else if (ti == typeid(ObserverDetectAll)) {
+            fd.kind = CRP_OBSERVER_DETECT_ALL;
+            text << "ObserverDetectAll";
+        } else if (ti == typeid(ObserverTracking)) {
+            const ObserverTracking *t = static_cast<const ObserverTracking *>(f);
+            fd.kind = CRP_OBSERVER_TRACKING;
+            const Vector3d &c = t->*member(TrackCenter());
+            for (int k = 0; k < 3; k++) fd.a[k] = c.data[k];
+            fd.r = t->*member(TrackRadius());
+            fd.step = t->*member(TrackStep());
+            text << "ObserverTracking";
+        } else if (ti == typeid(Observer1D)) {
+            fd.kind = CRP_OBSERVER_1D;
+            text << "Observer1D";
+        } else if (ti == typeid(ObserverInactiveVeto)) {
+            fd.kind = CRP_OBSERVER_INACTIVE_VETO;
+            text << "ObserverInactiveVeto";
+        } else if (ti == typeid(ObserverNucleusVeto)) {
+            fd.kind = CRP_OBSERVER_NUCLEUS_VETO;
+            text << "ObserverNucleusVeto";
+        } else if (ti == typeid(ObserverNeutrinoVeto)) {
+            fd.kind = CRP_OBSERVER_NEUTRINO_VETO;
+            text << "ObserverNeutrinoVeto";
+        } else if (ti == typeid(ObserverPhotonVeto)) {
+            fd.kind = CRP_OBSERVER_PHOTON_VETO;
+            text << "ObserverPhotonVeto";
+        } else if (ti == typeid(ObserverElectronVeto)) {
+            fd.kind = CRP_OBSERVER_ELECTRON_VETO;
+            text << "ObserverElectronVeto";
+        } else if (ti == typeid(ObserverParticleIdVeto)) {
+            fd.kind = CRP_OBSERVER_PARTICLE_ID_VETO;
+            fd.particle_id = static_cast<const ObserverParticleIdVeto *>(f)->*member(VetoId());
+            text << "ObserverParticleIdVeto " << fd.particle_id;
+        } else {
+            throw Unsupported("observer feature " + name_of(f) + " has no device form");
         }
     }
 
@@ -755,7 +892,7 @@ void GpuModuleList::runDevice(const candidate_vector_t &cands) {
             c->setTrajectoryLength(rec.length[r]);
             c->setTime(rec.time[r]);
             const Action &a = t.actions[mi];
-            if (a.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
+            if (a.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH || a.kind == CRP_MODULE_BOUNDARY) {
                 // AbstractCondition::reject (Module.cpp:25-37)
                 const ref_ptr<Module> &act = a.condition->*member(RejectAction());
                 if (act.valid()) act->process(c);

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 1u
+#define CRP_ABI_VERSION 2u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -108,7 +108,9 @@ typedef struct crp_field_component {
 enum crp_module_kind {
     CRP_MODULE_PROPAGATION = 1,
     CRP_MODULE_MAX_TRAJECTORY_LENGTH = 2, /* MaximumTrajectoryLength (BreakCondition.cpp:42) */
-    CRP_MODULE_OBSERVER = 3               /* Observer (Observer.cpp:27) */
+    CRP_MODULE_OBSERVER = 3,              /* Observer (Observer.cpp:27) */
+    CRP_MODULE_BOUNDARY = 4               /* SphericalBoundary, CubicBoundary, EllipsoidalBoundary,
+                                             CylindricalBoundary (Boundary.cpp:171-320) */
 };
 
 enum crp_propagator {
@@ -118,8 +120,39 @@ enum crp_propagator {
 };
 
 enum crp_observer_feature {
-    CRP_OBSERVER_SURFACE_SPHERE = 1, /* ObserverSurface(Sphere) (Observer.cpp:394, Geometry.cpp:41) */
-    CRP_OBSERVER_DETECT_ALL = 2      /* ObserverDetectAll (Observer.cpp:93) */
+    CRP_OBSERVER_SURFACE_SPHERE = 1,   /* ObserverSurface(Sphere) (Observer.cpp:394, Geometry.cpp:41) */
+    CRP_OBSERVER_DETECT_ALL = 2,       /* ObserverDetectAll (Observer.cpp:93) */
+    CRP_OBSERVER_SURFACE_PLANE = 3,    /* ObserverSurface(Plane) (Geometry.cpp:19): a = x0, b = n */
+    CRP_OBSERVER_SURFACE_BOX = 4,      /* ObserverSurface(ParaxialBox) (Geometry.cpp:64): a = corner, b = size */
+    CRP_OBSERVER_TRACKING = 5,         /* ObserverTracking (Observer.cpp:109): a = centre, r, step */
+    CRP_OBSERVER_1D = 6,               /* Observer1D (Observer.cpp:137) */
+    CRP_OBSERVER_INACTIVE_VETO = 7,    /* ObserverInactiveVeto (Observer.cpp:174) */
+    CRP_OBSERVER_NUCLEUS_VETO = 8,     /* ObserverNucleusVeto (Observer.cpp:185) */
+    CRP_OBSERVER_NEUTRINO_VETO = 9,    /* ObserverNeutrinoVeto (Observer.cpp:196) */
+    CRP_OBSERVER_PHOTON_VETO = 10,     /* ObserverPhotonVeto (Observer.cpp:208) */
+    CRP_OBSERVER_ELECTRON_VETO = 11,   /* ObserverElectronVeto (Observer.cpp:219) */
+    CRP_OBSERVER_PARTICLE_ID_VETO = 12 /* ObserverParticleIdVeto (Observer.cpp:234): particle_id */
+};
+
+/* One feature of an Observer; the observer detects when a feature detects
+ * and none vetoes (Observer.cpp:27-35), every feature limiting the next step
+ * as its checkDetection does. */
+typedef struct crp_observer_feature_desc {
+    int32_t kind;        /* crp_observer_feature */
+    int32_t particle_id; /* CRP_OBSERVER_PARTICLE_ID_VETO */
+    double a[3];
+    double b[3];
+    double r;
+    double step;
+} crp_observer_feature_desc;
+
+#define CRP_MAX_OBSERVER_FEATURES 4
+
+enum crp_boundary_kind {
+    CRP_BOUNDARY_SPHERICAL = 1,  /* SphericalBoundary (Boundary.cpp:216): a = centre, size = radius */
+    CRP_BOUNDARY_CUBIC = 2,      /* CubicBoundary (Boundary.cpp:171): a = origin, size */
+    CRP_BOUNDARY_ELLIPSOIDAL = 3,/* EllipsoidalBoundary (Boundary.cpp:259): a, b = focal points, size = major axis */
+    CRP_BOUNDARY_CYLINDRICAL = 4 /* CylindricalBoundary (Boundary.cpp:303): a = origin, size = height, radius */
 };
 
 typedef struct crp_module_desc {
@@ -141,6 +174,19 @@ typedef struct crp_module_desc {
     double sphere_radius;
     int32_t deactivate_on_detection; /* Observer::setDeactivateOnDetection, default 1 */
     int32_t record;                  /* the detection (or rejection) action writes a record */
+    /* CRP_MODULE_OBSERVER with several features: n_features > 0 replaces
+     * observer_feature and sphere_* above */
+    int32_t n_features;
+    /* CRP_MODULE_BOUNDARY */
+    int32_t boundary;                /* crp_boundary_kind */
+    crp_observer_feature_desc features[CRP_MAX_OBSERVER_FEATURES];
+    double boundary_a[3];
+    double boundary_b[3];
+    double boundary_size;
+    double boundary_radius;
+    double boundary_margin;          /* setMargin, default 0.1 kpc (0 cylindrical) */
+    int32_t boundary_limit_step;     /* setLimitStep, default 1 (0 cylindrical) */
+    int32_t _pad1;
 } crp_module_desc;
 
 enum crp_precision {

@@ -687,6 +687,142 @@ static void write_record(crp_records *rec, const cand_t *c, int module) {
     rec->id[slot] = c->id;
 }
 
+static double std_min(double a, double b) { return (b < a) ? b : a; } /* std::min */
+static double std_max(double a, double b) { return (a < b) ? b : a; } /* std::max */
+
+/* ParticleID.cpp:37 isNucleus: the neutron, and HepPID::isNucleus
+ * (ParticleIDMethods.cc:242): the proton, or +/-10LZZZAAAI with A >= Z. */
+static int is_nucleus(int id) {
+    if (id == 2112) return 1;
+    int a = id < 0 ? -id : id;
+    if (a == 2212) return 1;
+    if ((a / 1000000000) % 10 == 1 && (a / 100000000) % 10 == 0)
+        return (a / 10) % 1000 >= (a / 10000) % 1000;
+    return 0;
+}
+
+/* Sphere / Plane / ParaxialBox ::distance (Geometry.cpp:41, 19, 64). */
+static double surface_distance(const crp_observer_feature_desc *f, v3 p) {
+    v3 a = mk(f->a[0], f->a[1], f->a[2]);
+    if (f->kind == CRP_OBSERVER_SURFACE_SPHERE) return norm(sub(p, a)) - f->r;
+    v3 dX = sub(p, a);
+    if (f->kind == CRP_OBSERVER_SURFACE_PLANE) return f->b[0] * dX.x + f->b[1] * dX.y + f->b[2] * dX.z;
+    double hx = f->b[0] / 2., hy = f->b[1] / 2., hz = f->b[2] / 2.;
+    double X = dX.x - hx, Y = dX.y - hy, Z = dX.z - hz;
+    if ((fabs(X) <= hx) && (fabs(Y) <= hy) && (fabs(Z) <= hz)) {
+        double d = std_min(hx - fabs(X), std_min(hy - fabs(Y), hz - fabs(Z)));
+        return -1. * d;
+    }
+    double qa = std_max(0., fabs(X) - hx), qb = std_max(0., fabs(Y) - hy), qc = std_max(0., fabs(Z) - hz);
+    return sqrt(qa * qa + qb * qb + qc * qc);
+}
+
+enum { DET_NOTHING = 0, DET_DETECTED = 1, DET_VETO = 2 };
+
+/* ObserverFeature::checkDetection of each feature (Observer.cpp:93-394). */
+static int check_feature(const crp_observer_feature_desc *f, cand_t *c) {
+    int a;
+    switch (f->kind) {
+    case CRP_OBSERVER_SURFACE_SPHERE:
+    case CRP_OBSERVER_SURFACE_PLANE:
+    case CRP_OBSERVER_SURFACE_BOX: { /* ObserverSurface, Observer.cpp:394 */
+        double cd = surface_distance(f, c->pos), pd = surface_distance(f, c->prev);
+        limit_next_step(c, fabs(cd));
+        if (cd * pd > 0) return DET_NOTHING;
+        if (pd == 0) return DET_NOTHING;
+        return DET_DETECTED;
+    }
+    case CRP_OBSERVER_DETECT_ALL: return DET_DETECTED; /* :93 */
+    case CRP_OBSERVER_TRACKING: { /* :109 */
+        double d = norm(sub(c->pos, mk(f->a[0], f->a[1], f->a[2])));
+        if (d > f->r) {
+            limit_next_step(c, fabs(d - f->r));
+            return DET_NOTHING;
+        }
+        limit_next_step(c, f->step);
+        return DET_DETECTED;
+    }
+    case CRP_OBSERVER_1D: /* :137 */
+        if (c->pos.x > 0) {
+            limit_next_step(c, c->pos.x);
+            return DET_NOTHING;
+        }
+        return DET_DETECTED;
+    case CRP_OBSERVER_INACTIVE_VETO: return c->active ? DET_NOTHING : DET_VETO; /* :174 */
+    case CRP_OBSERVER_NUCLEUS_VETO: return is_nucleus(c->id) ? DET_VETO : DET_NOTHING; /* :185 */
+    case CRP_OBSERVER_NEUTRINO_VETO: /* :196 */
+        a = c->id < 0 ? -c->id : c->id;
+        return (a == 12 || a == 14 || a == 16) ? DET_VETO : DET_NOTHING;
+    case CRP_OBSERVER_PHOTON_VETO: return c->id == 22 ? DET_VETO : DET_NOTHING; /* :208 */
+    case CRP_OBSERVER_ELECTRON_VETO: return (c->id == 11 || c->id == -11) ? DET_VETO : DET_NOTHING;
+    default: return c->id == f->particle_id ? DET_VETO : DET_NOTHING; /* :234 */
+    }
+}
+
+/* Observer::process (Observer.cpp:27-52); the single legacy feature when
+ * n_features is 0. */
+static void observer_process(const crp_module_desc *m, cand_t *c, crp_records *rec, int i) {
+    crp_observer_feature_desc legacy;
+    memset(&legacy, 0, sizeof(legacy));
+    legacy.kind = m->observer_feature;
+    memcpy(legacy.a, m->sphere_center, sizeof(legacy.a));
+    legacy.r = m->sphere_radius;
+    const crp_observer_feature_desc *fs = m->n_features > 0 ? m->features : &legacy;
+    int nf = m->n_features > 0 ? m->n_features : 1;
+    int state = DET_NOTHING;
+    for (int f = 0; f < nf; f++) {
+        int st = check_feature(&fs[f], c);
+        if (st == DET_VETO) state = DET_VETO;
+        else if (st == DET_DETECTED && state != DET_VETO) state = DET_DETECTED;
+    }
+    if (state == DET_DETECTED) {
+        if (m->record) write_record(rec, c, i);
+        c->flags |= CRP_FLAG_DETECTED;
+        if (m->deactivate_on_detection) c->active = 0;
+    }
+}
+
+static void reject_candidate(const crp_module_desc *m, cand_t *c, crp_records *rec, int i) {
+    if (m->record) write_record(rec, c, i); /* AbstractCondition::reject, Module.cpp:25 */
+    c->flags |= CRP_FLAG_REJECTED;
+    c->active = 0;
+}
+
+/* CubicBoundary / SphericalBoundary / EllipsoidalBoundary /
+ * CylindricalBoundary ::process (Boundary.cpp:171, 216, 259, 303). */
+static void boundary_process(const crp_module_desc *m, cand_t *c, crp_records *rec, int i) {
+    v3 a = mk(m->boundary_a[0], m->boundary_a[1], m->boundary_a[2]);
+    if (m->boundary == CRP_BOUNDARY_CUBIC) {
+        v3 r = sub(c->pos, a);
+        double lo = std_min(r.x, std_min(r.y, r.z)), hi = std_max(r.x, std_max(r.y, r.z));
+        if ((lo <= 0) || (hi >= m->boundary_size)) reject_candidate(m, c, rec, i);
+        if (m->boundary_limit_step) {
+            limit_next_step(c, lo + m->boundary_margin);
+            limit_next_step(c, m->boundary_size - hi + m->boundary_margin);
+        }
+    } else if (m->boundary == CRP_BOUNDARY_SPHERICAL) {
+        double d = norm(sub(c->pos, a));
+        if (d >= m->boundary_size) reject_candidate(m, c, rec, i);
+        if (m->boundary_limit_step) limit_next_step(c, m->boundary_size - d + m->boundary_margin);
+    } else if (m->boundary == CRP_BOUNDARY_ELLIPSOIDAL) {
+        v3 b = mk(m->boundary_b[0], m->boundary_b[1], m->boundary_b[2]);
+        double d = norm(sub(c->pos, a)) + norm(sub(c->pos, b));
+        if (d >= m->boundary_size) reject_candidate(m, c, rec, i);
+        if (m->boundary_limit_step) limit_next_step(c, m->boundary_size - d + m->boundary_margin);
+    } else {
+        v3 d = sub(c->pos, a);
+        double R2 = ORACLE_POW(d.x, 2.) + ORACLE_POW(d.y, 2.);
+        double Z = fabs(d.z);
+        if (R2 < ORACLE_POW(m->boundary_radius, 2.) && Z < m->boundary_size / 2.) {
+            if (m->boundary_limit_step)
+                limit_next_step(c, std_min(m->boundary_radius - ORACLE_POW(R2, 0.5), m->boundary_size / 2. - Z) +
+                                       m->boundary_margin);
+            return;
+        }
+        reject_candidate(m, c, rec, i);
+    }
+}
+
 /* One ModuleList::process (ModuleList.cpp.in:54): every module in order. */
 static void chain_process(const crp_plan_desc *d, cand_t *c, crp_records *rec, uint64_t *tries) {
     for (int i = 0; i < d->n_modules; i++) {
@@ -705,23 +841,9 @@ static void chain_process(const crp_plan_desc *d, cand_t *c, crp_records *rec, u
                 limit_next_step(c, maxLength - c->len);
             }
         } else if (m->kind == CRP_MODULE_OBSERVER) { /* Observer.cpp:27 */
-            int detected;
-            if (m->observer_feature == CRP_OBSERVER_SURFACE_SPHERE) { /* Observer.cpp:394 */
-                v3 ctr = mk(m->sphere_center[0], m->sphere_center[1], m->sphere_center[2]);
-                double cd = norm(sub(c->pos, ctr)) - m->sphere_radius;
-                double pd = norm(sub(c->prev, ctr)) - m->sphere_radius;
-                limit_next_step(c, fabs(cd));
-                if (cd * pd > 0) detected = 0;
-                else if (pd == 0) detected = 0;
-                else detected = 1;
-            } else {
-                detected = 1;
-            }
-            if (detected) {
-                if (m->record) write_record(rec, c, i);
-                c->flags |= CRP_FLAG_DETECTED;
-                if (m->deactivate_on_detection) c->active = 0;
-            }
+            observer_process(m, c, rec, i);
+        } else if (m->kind == CRP_MODULE_BOUNDARY) {
+            boundary_process(m, c, rec, i);
         }
     }
 }

@@ -38,6 +38,7 @@
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/magneticField/turbulentField/TurbulentField.h"
+#include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
 #include "crpropa/module/Observer.h"
@@ -181,6 +182,26 @@ static ref_ptr<MagneticField> build_field(const crp_plan_desc *d, Built &b, cons
     return list;
 }
 
+// The reference's observer feature for a crp_observer_feature_desc.
+static ObserverFeature *build_feature(const crp_observer_feature_desc &f) {
+    const Vector3d a(f.a[0], f.a[1], f.a[2]), bv(f.b[0], f.b[1], f.b[2]);
+    switch (f.kind) {
+    case CRP_OBSERVER_SURFACE_SPHERE: return new ObserverSurface(new Sphere(a, f.r));
+    case CRP_OBSERVER_DETECT_ALL: return new ObserverDetectAll();
+    case CRP_OBSERVER_SURFACE_PLANE: return new ObserverSurface(new Plane(a, bv));
+    case CRP_OBSERVER_SURFACE_BOX: return new ObserverSurface(new ParaxialBox(a, bv));
+    case CRP_OBSERVER_TRACKING: return new ObserverTracking(a, f.r, f.step);
+    case CRP_OBSERVER_1D: return new Observer1D();
+    case CRP_OBSERVER_INACTIVE_VETO: return new ObserverInactiveVeto();
+    case CRP_OBSERVER_NUCLEUS_VETO: return new ObserverNucleusVeto();
+    case CRP_OBSERVER_NEUTRINO_VETO: return new ObserverNeutrinoVeto();
+    case CRP_OBSERVER_PHOTON_VETO: return new ObserverPhotonVeto();
+    case CRP_OBSERVER_ELECTRON_VETO: return new ObserverElectronVeto();
+    case CRP_OBSERVER_PARTICLE_ID_VETO: return new ObserverParticleIdVeto(f.particle_id);
+    }
+    throw std::runtime_error("ref_shim: unknown observer feature");
+}
+
 void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpers *h,
                  ModuleList *sim, bool count_steps, const char *text_output, int text_type) {
     b.field = build_field(d, b, h);
@@ -214,12 +235,15 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpe
             b.sim->add(c);
         } else if (m.kind == CRP_MODULE_OBSERVER) {
             Observer *o = new Observer();
-            if (m.observer_feature == CRP_OBSERVER_SURFACE_SPHERE)
-                o->add(new ObserverSurface(new Sphere(
-                    Vector3d(m.sphere_center[0], m.sphere_center[1], m.sphere_center[2]),
-                    m.sphere_radius)));
-            else
-                o->add(new ObserverDetectAll());
+            if (m.n_features == 0) {
+                if (m.observer_feature == CRP_OBSERVER_SURFACE_SPHERE)
+                    o->add(new ObserverSurface(new Sphere(
+                        Vector3d(m.sphere_center[0], m.sphere_center[1], m.sphere_center[2]),
+                        m.sphere_radius)));
+                else
+                    o->add(new ObserverDetectAll());
+            }
+            for (int f = 0; f < m.n_features; f++) o->add(build_feature(m.features[f]));
             o->setDeactivateOnDetection(m.deactivate_on_detection != 0);
             o->setFlag("Detected", "Detected");
             if (text_output)
@@ -227,6 +251,33 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpe
             else if (m.record)
                 o->onDetection(new RecordAction(rec, i));
             b.sim->add(o);
+        } else if (m.kind == CRP_MODULE_BOUNDARY) {
+            const Vector3d a(m.boundary_a[0], m.boundary_a[1], m.boundary_a[2]);
+            AbstractCondition *c;
+            if (m.boundary == CRP_BOUNDARY_SPHERICAL) {
+                SphericalBoundary *bnd = new SphericalBoundary(a, m.boundary_size);
+                bnd->setMargin(m.boundary_margin);
+                bnd->setLimitStep(m.boundary_limit_step != 0);
+                c = bnd;
+            } else if (m.boundary == CRP_BOUNDARY_CUBIC) {
+                CubicBoundary *bnd = new CubicBoundary(a, m.boundary_size);
+                bnd->setMargin(m.boundary_margin);
+                bnd->setLimitStep(m.boundary_limit_step != 0);
+                c = bnd;
+            } else if (m.boundary == CRP_BOUNDARY_ELLIPSOIDAL) {
+                EllipsoidalBoundary *bnd = new EllipsoidalBoundary(
+                    a, Vector3d(m.boundary_b[0], m.boundary_b[1], m.boundary_b[2]), m.boundary_size);
+                bnd->setMargin(m.boundary_margin);
+                bnd->setLimitStep(m.boundary_limit_step != 0);
+                c = bnd;
+            } else {
+                CylindricalBoundary *bnd = new CylindricalBoundary(a, m.boundary_size, m.boundary_radius);
+                bnd->setMargin(m.boundary_margin);
+                bnd->setLimitStep(m.boundary_limit_step != 0);
+                c = bnd;
+            }
+            if (m.record) c->onReject(new RecordAction(rec, i));
+            b.sim->add(c);
         } else {
             throw std::runtime_error("ref_shim: unknown module kind");
         }

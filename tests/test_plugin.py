@@ -200,3 +200,38 @@ def test_plugin_mixed_precision_within_bound(plugin, reference):
     plugin.run(spec_mx, b, precision=_abi.PRECISION_MIXED)
     rel = np.linalg.norm(a.position() - b.position(), axis=1) / np.linalg.norm(a.position(), axis=1)
     assert rel.max() <= 1e-6, rel.max()
+
+
+def _ob_chains():
+    import test_observers_boundaries as T
+    return T
+
+
+@pytest.mark.parametrize("name", ["plane", "box", "tracking", "observer1d", "vetoes", "spherical", "cubic",
+                                  "ellipsoidal", "cylindrical", "boundary_and_observer"])
+def test_plugin_translates_observer_features_and_boundaries(plugin, name):
+    T = _ob_chains()
+    ok, text = plugin.describe(T._spec(name))
+    assert ok, text
+    expect = {"plane": "ObserverSurface(Plane)", "box": "ObserverSurface(ParaxialBox)",
+              "tracking": "ObserverTracking", "observer1d": "Observer1D",
+              "vetoes": "ObserverParticleIdVeto 1000020040", "spherical": "SphericalBoundary",
+              "cubic": "CubicBoundary", "ellipsoidal": "EllipsoidalBoundary",
+              "cylindrical": "CylindricalBoundary", "boundary_and_observer": "SphericalBoundary"}[name]
+    assert expect in text, text
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["vetoes", "box", "tracking", "cubic", "cylindrical", "boundary_and_observer"])
+def test_plugin_observer_features_and_boundaries_bitwise(plugin, reference, name):
+    """The reference's Observer features and boundary modules, run through
+    GpuModuleList (FP64 form), against ModuleList::run: same state, flags and
+    replayed records."""
+    T = _ob_chains()
+    spec = T._spec(name)
+    c = T._cands()
+    a, b = c.copy(), c.copy()
+    ra, rb = RecordArrays(200_000), RecordArrays(200_000)
+    reference.run(spec, a, ra, threads=2)
+    plugin.run(spec, b, rb)
+    T._compare(a, b, ra, rb)
