@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # crp_status
 OK = 0
@@ -33,7 +33,8 @@ STATUS_NAMES = {
     ERR_NO_DEVICE: "CRP_ERR_NO_DEVICE",
 }
 
-FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL = 1, 2, 3, 4
+FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID = 1, 2, 3, 4, 5
+INTERPOLATION_TRILINEAR, INTERPOLATION_TRICUBIC, INTERPOLATION_NEAREST_NEIGHBOUR = 0, 1, 2
 MODULE_PROPAGATION, MODULE_MAX_TRAJECTORY_LENGTH, MODULE_OBSERVER, MODULE_BOUNDARY = 1, 2, 3, 4
 PROP_CK, PROP_BP, PROP_SDE = 1, 2, 3
 OBSERVER_SURFACE_SPHERE, OBSERVER_DETECT_ALL, OBSERVER_SURFACE_PLANE, OBSERVER_SURFACE_BOX = 1, 2, 3, 4
@@ -53,7 +54,7 @@ _fp = C.POINTER(C.c_float)
 class GridDesc(C.Structure):
     _fields_ = [("values", _fp), ("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64),
                 ("origin", _d * 3), ("spacing", _d * 3), ("reflective", C.c_int32),
-                ("clip_volume", C.c_int32)]
+                ("clip_volume", C.c_int32), ("interpolation", C.c_int32), ("_pad", C.c_int32)]
 
 
 class PlaneWaveDesc(C.Structure):
@@ -66,7 +67,7 @@ class FieldComponent(C.Structure):
     _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
                 ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
                 ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
-                ("toroidal_b0", _d)]
+                ("toroidal_b0", _d), ("modulation", GridDesc)]
 
 
 class FeatureDesc(C.Structure):

@@ -164,6 +164,47 @@ crp_status validate_module(const crp_module_desc &m) {
     return CRP_OK;
 }
 
+// A Grid3f (comps 3) or Grid1f (comps 1) on the device: the cell values, the
+// padded copy of a Grid3f for the mixed form, and GridProperties (Grid.h:75).
+crp_status build_grid(crp_plan *p, const crp_grid3f_desc &g, int comps, DevGrid &dg) {
+    const char *name = comps == 3 ? "Grid3f" : "Grid1f";
+    if (!g.values || g.nx == 0 || g.ny == 0 || g.nz == 0)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "%s: empty grid", name);
+    if (g.nx > (1u << 20) || g.ny > (1u << 20) || g.nz > (1u << 20))
+        return fail(CRP_ERR_CAPACITY, "%s: a dimension beyond 2^20 cells", name);
+    if (g.interpolation < CRP_INTERPOLATION_TRILINEAR || g.interpolation > CRP_INTERPOLATION_NEAREST_NEIGHBOUR)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "%s: interpolation type not understood", name);
+    size_t cells = (size_t)g.nx * g.ny * g.nz;
+    crp_status st = upload(p, g.values, cells * comps, &dg.values);
+    if (st) return st;
+    dg.values4 = nullptr;
+    if (comps == 3 && p->precision == CRP_PRECISION_MIXED) {
+        // 16-byte cells: one aligned 128-bit load per corner
+        std::vector<float4> pad(cells);
+        for (size_t i = 0; i < cells; i++)
+            pad[i] = make_float4(g.values[3 * i], g.values[3 * i + 1], g.values[3 * i + 2], 0.f);
+        st = upload(p, pad.data(), cells, &dg.values4);
+        if (st) return st;
+    }
+    dg.nx = (int)g.nx; dg.ny = (int)g.ny; dg.nz = (int)g.nz;
+    dg.reflective = g.reflective;
+    dg.clip_volume = g.clip_volume;
+    dg.interp = g.interpolation;
+    dg.pow2 = is_pow2(g.nx) && is_pow2(g.ny) && is_pow2(g.nz);
+    // Grid::setOrigin (Grid.h:225): gridOrigin = origin + spacing/2
+    dg.gox = g.origin[0] + g.spacing[0] / 2;
+    dg.goy = g.origin[1] + g.spacing[1] / 2;
+    dg.goz = g.origin[2] + g.spacing[2] / 2;
+    dg.sx = g.spacing[0]; dg.sy = g.spacing[1]; dg.sz = g.spacing[2];
+    dg.inv_sx = 1.0 / g.spacing[0]; dg.inv_sy = 1.0 / g.spacing[1]; dg.inv_sz = 1.0 / g.spacing[2];
+    dg.ox = g.origin[0]; dg.oy = g.origin[1]; dg.oz = g.origin[2];
+    // edge = origin + Vector3d(Nx, Ny, Nz) * spacing (Grid.h:322)
+    dg.ex = g.origin[0] + (double)g.nx * g.spacing[0];
+    dg.ey = g.origin[1] + (double)g.ny * g.spacing[1];
+    dg.ez = g.origin[2] + (double)g.nz * g.spacing[2];
+    return CRP_OK;
+}
+
 crp_status build_component(crp_plan *p, const crp_field_component &f, DevComponent &d) {
     d.kind = f.kind;
     d.periodic = f.periodic;
@@ -176,40 +217,13 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
     d.b0 = f.toroidal_b0;
     if (f.periodic && !(f.periodic_extends[0] > 0 && f.periodic_extends[1] > 0 && f.periodic_extends[2] > 0))
         return fail(CRP_ERR_INVALID_ARGUMENT, "PeriodicMagneticField: extends must be > 0");
-    if (f.kind == CRP_FIELD_GRID) {
-        const crp_grid3f_desc &g = f.grid;
-        if (!g.values || g.nx == 0 || g.ny == 0 || g.nz == 0)
-            return fail(CRP_ERR_INVALID_ARGUMENT, "Grid3f: empty grid");
-        if (g.nx > (1u << 20) || g.ny > (1u << 20) || g.nz > (1u << 20))
-            return fail(CRP_ERR_CAPACITY, "Grid3f: a dimension beyond 2^20 cells");
-        size_t cells = (size_t)g.nx * g.ny * g.nz;
-        DevGrid &dg = d.grid;
-        crp_status st = upload(p, g.values, cells * 3, &dg.values);
+    if (f.kind == CRP_FIELD_GRID || f.kind == CRP_FIELD_MODULATED_GRID) {
+        crp_status st = build_grid(p, f.grid, 3, d.grid);
         if (st) return st;
-        dg.values4 = nullptr;
-        if (p->precision == CRP_PRECISION_MIXED) {
-            // 16-byte cells: one aligned 128-bit load per corner
-            std::vector<float4> pad(cells);
-            for (size_t i = 0; i < cells; i++)
-                pad[i] = make_float4(g.values[3 * i], g.values[3 * i + 1], g.values[3 * i + 2], 0.f);
-            st = upload(p, pad.data(), cells, &dg.values4);
+        if (f.kind == CRP_FIELD_MODULATED_GRID) {
+            st = build_grid(p, f.modulation, 1, d.mod);
             if (st) return st;
         }
-        dg.nx = (int)g.nx; dg.ny = (int)g.ny; dg.nz = (int)g.nz;
-        dg.reflective = g.reflective;
-        dg.clip_volume = g.clip_volume;
-        dg.pow2 = is_pow2(g.nx) && is_pow2(g.ny) && is_pow2(g.nz);
-        // Grid::setOrigin (Grid.h:225): gridOrigin = origin + spacing/2
-        dg.gox = g.origin[0] + g.spacing[0] / 2;
-        dg.goy = g.origin[1] + g.spacing[1] / 2;
-        dg.goz = g.origin[2] + g.spacing[2] / 2;
-        dg.sx = g.spacing[0]; dg.sy = g.spacing[1]; dg.sz = g.spacing[2];
-        dg.inv_sx = 1.0 / g.spacing[0]; dg.inv_sy = 1.0 / g.spacing[1]; dg.inv_sz = 1.0 / g.spacing[2];
-        dg.ox = g.origin[0]; dg.oy = g.origin[1]; dg.oz = g.origin[2];
-        // edge = origin + Vector3d(Nx, Ny, Nz) * spacing (Grid.h:322)
-        dg.ex = g.origin[0] + (double)g.nx * g.spacing[0];
-        dg.ey = g.origin[1] + (double)g.ny * g.spacing[1];
-        dg.ez = g.origin[2] + (double)g.nz * g.spacing[2];
     } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
         const crp_plane_wave_desc &w = f.plane_wave;
         if (w.n_modes <= 1)
@@ -404,7 +418,9 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
         const DevGrid &g = d.fields[0].grid;
         const bool padded = p->precision != CRP_PRECISION_MIXED || g.values4 != nullptr;
         const bool small = (uint64_t)g.nx * g.ny * g.nz < (1ull << 31);  // 32-bit cell indices
-        p->fs = (!g.reflective && !g.clip_volume && g.pow2 && padded && small) ? FS_GRID_PERIODIC : FS_GRID;
+        const bool trilinear = g.interp == CRP_INTERPOLATION_TRILINEAR;
+        p->fs = (!g.reflective && !g.clip_volume && g.pow2 && padded && small && trilinear) ? FS_GRID_PERIODIC
+                                                                                           : FS_GRID;
     }
     else if (d.n_fields == 1 && !desc->fields[0].periodic && desc->fields[0].kind == CRP_FIELD_PLANE_WAVE)
         p->fs = FS_PLANE_WAVE;

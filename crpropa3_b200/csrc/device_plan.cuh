@@ -24,6 +24,8 @@ struct DevGrid {
     double inv_sx, inv_sy, inv_sz;  // 1/spacing (mixed form only)
     double ox, oy, oz;     // origin (clipVolume test)
     double ex, ey, ez;     // origin + N*spacing (clipVolume test, Grid.h:322)
+    int interp;            // crp_interpolation
+    int pad_;
 };
 
 struct DevPlaneWave {
@@ -43,6 +45,7 @@ struct DevComponent {
     DevPlaneWave pw;
     double uniform[3];
     double b0;
+    DevGrid mod;    // CRP_FIELD_MODULATED_GRID: the Grid1f modulation (values: one float per cell)
 };
 
 struct DevModule {

@@ -18,6 +18,7 @@
 #include "chain.cuh"
 #include "crmath.cuh"
 #include "engine_internal.h"
+#include "grid_interp.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -57,6 +58,10 @@ __device__ __forceinline__ double clipd(double x, double lo, double hi) { return
 // periodic clamp is a mask (equal to the double modulo of Grid.h:31 there).
 template <bool CACHE, bool PER = false>
 __device__ __forceinline__ d3 grid_field_t(const DevGrid &g, d3 pos, Cand *cc) {
+    if (!PER && g.interp != CRP_INTERPOLATION_TRILINEAR) {  // tricubic, nearest (Grid.h:328-331)
+        const gi3 v = gi_vector_other(g, pos.x, pos.y, pos.z);
+        return mk(v.x, v.y, v.z);
+    }
     if (!PER && g.clip_volume) {
         bool in = (pos.x >= g.ox) && (pos.x <= g.ex);
         in &= (pos.y >= g.oy) && (pos.y <= g.ey);
@@ -173,6 +178,10 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
     }
     switch (f.kind) {
     case CRP_FIELD_GRID: return grid_field(f.grid, pos);
+    case CRP_FIELD_MODULATED_GRID: {  // ModulatedMagneticFieldGrid::getField (MagneticFieldGrid.cpp:51)
+        const float m = gi_scalar(f.mod, pos.x, pos.y, pos.z);
+        return muls(grid_field(f.grid, pos), (double)m);
+    }
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, pos);
     case CRP_FIELD_UNIFORM: return mk(f.uniform[0], f.uniform[1], f.uniform[2]);
     default: {

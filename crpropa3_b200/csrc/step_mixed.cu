@@ -16,6 +16,7 @@
 
 #include "chain.cuh"
 #include "engine_internal.h"
+#include "grid_interp.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -53,6 +54,10 @@ __device__ __forceinline__ int wrap(int i, int n, bool pow2) {
 // and has the padded copy (FS_GRID_PERIODIC): those branches are compiled out.
 template <bool CACHE, bool PER = false>
 __device__ __forceinline__ f3 grid_field_t(const DevGrid &g, double x, double y, double z, Cand *cc) {
+    if (!PER && g.interp != CRP_INTERPOLATION_TRILINEAR) {  // tricubic, nearest (Grid.h:328-331)
+        const gi3 v = gi_vector_other(g, x, y, z);
+        return f3mk(v.x, v.y, v.z);
+    }
     if (!PER && g.clip_volume) {
         bool in = (x >= g.ox) && (x <= g.ex) && (y >= g.oy) && (y <= g.ey) && (z >= g.oz) && (z <= g.ez);
         if (!in) return f3mk(0.f, 0.f, 0.f);
@@ -203,6 +208,11 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     }
     switch (f.kind) {
     case CRP_FIELD_GRID: return grid_field(f.grid, x, y, z);
+    case CRP_FIELD_MODULATED_GRID: {  // MagneticFieldGrid.cpp:51
+        const float m = gi_scalar(f.mod, x, y, z);
+        const f3 b = grid_field(f.grid, x, y, z);
+        return f3mk(b.x * m, b.y * m, b.z * m);
+    }
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z, sh);
     case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
     default: {

@@ -31,6 +31,29 @@ class GridField:
     reflective: bool = False
     clip_volume: bool = False
     periodic: Optional[tuple] = None  # (origin, extends, reflective) PeriodicMagneticField
+    interpolation: int = _abi.INTERPOLATION_TRILINEAR  # Grid::setInterpolationType (Grid.h:255)
+
+
+@dataclass
+class ScalarGrid:
+    """A Grid1f (Grid.h:587): values (nx, ny, nz) float32, z fastest."""
+    values: np.ndarray
+    origin: Sequence[float] = (0.0, 0.0, 0.0)
+    spacing: Sequence[float] = (1.0, 1.0, 1.0)
+    reflective: bool = True  # what ModulatedMagneticFieldGrid's constructor sets (MagneticFieldGrid.cpp:23)
+    clip_volume: bool = False
+    interpolation: int = _abi.INTERPOLATION_TRILINEAR
+
+
+@dataclass
+class ModulatedGridField:
+    """ModulatedMagneticFieldGrid (MagneticFieldGrid.cpp:51): the Grid3f field
+    times the interpolated Grid1f modulation.  The constructor makes the
+    Grid3f periodic and the modulation reflective (MagneticFieldGrid.cpp:22-23);
+    setReflective(grid, modulation) is the two grids' own flags here."""
+    grid: GridField
+    modulation: ScalarGrid
+    periodic: Optional[tuple] = None
 
 
 @dataclass
@@ -158,16 +181,12 @@ class ChainSpec:
             c.periodic_extends[:] = _v3(e)
             c.periodic_reflective = int(bool(refl))
         if isinstance(f, GridField):
-            v = np.ascontiguousarray(f.values, dtype=np.float32)
-            if v.ndim != 4 or v.shape[3] != 3:
-                raise ValueError("grid values must have shape (nx, ny, nz, 3)")
             c.kind = _abi.FIELD_GRID
-            c.grid.values = self._arr(v, np.float32)
-            c.grid.nx, c.grid.ny, c.grid.nz = v.shape[:3]
-            c.grid.origin[:] = _v3(f.origin)
-            c.grid.spacing[:] = _v3(f.spacing)
-            c.grid.reflective = int(bool(f.reflective))
-            c.grid.clip_volume = int(bool(f.clip_volume))
+            self._fill_grid(c.grid, f, 3)
+        elif isinstance(f, ModulatedGridField):
+            c.kind = _abi.FIELD_MODULATED_GRID
+            self._fill_grid(c.grid, f.grid, 3)
+            self._fill_grid(c.modulation, f.modulation, 1)
         elif isinstance(f, PlaneWaveField):
             c.kind = _abi.FIELD_PLANE_WAVE
             w = c.plane_wave
@@ -187,6 +206,20 @@ class ChainSpec:
             c.toroidal_b0 = float(f.b0)
         else:
             raise TypeError(f"unsupported field component {type(f).__name__}")
+
+    def _fill_grid(self, g, f, comps):
+        v = np.ascontiguousarray(f.values, dtype=np.float32)
+        if comps == 3 and (v.ndim != 4 or v.shape[3] != 3):
+            raise ValueError("grid values must have shape (nx, ny, nz, 3)")
+        if comps == 1 and v.ndim != 3:
+            raise ValueError("scalar grid values must have shape (nx, ny, nz)")
+        g.values = self._arr(v, np.float32)
+        g.nx, g.ny, g.nz = v.shape[:3]
+        g.origin[:] = _v3(f.origin)
+        g.spacing[:] = _v3(f.spacing)
+        g.reflective = int(bool(f.reflective))
+        g.clip_volume = int(bool(f.clip_volume))
+        g.interpolation = int(f.interpolation)
 
     @staticmethod
     def _fill_module(d, m):

@@ -108,6 +108,7 @@ CRPGPU_MEMBER(StateDirection, ParticleState, Vector3d, direction);     // Partic
 #undef CRPGPU_MEMBER
 
 static_assert(sizeof(Vector3f) == 12, "Grid3f cells must be three packed floats (crp_grid3f_desc)");
+static_assert(sizeof(float) == 4, "Grid1f cells must be single floats (crp_grid3f_desc)");
 
 struct Unsupported : std::runtime_error {
     explicit Unsupported(const std::string &m) : std::runtime_error(m) {}
@@ -217,26 +218,21 @@ struct Translation {
         if (const MagneticFieldGrid *g = dynamic_cast<const MagneticFieldGrid *>(f)) {
             ref_ptr<Grid3f> grid = const_cast<MagneticFieldGrid *>(g)->getGrid();
             if (!grid.valid()) throw Unsupported("MagneticFieldGrid without a grid");
-            if (grid->getInterpolationType() != TRILINEAR)
-                throw Unsupported("Grid3f interpolation " + grid->getInterpolationTypeName() +
-                                  " (the device path interpolates trilinearly)");
-            std::vector<Vector3f> &v = grid->getGrid();
             c.kind = CRP_FIELD_GRID;
-            c.grid.values = reinterpret_cast<const float *>(&v[0]);
-            c.grid.nx = grid->getNx();
-            c.grid.ny = grid->getNy();
-            c.grid.nz = grid->getNz();
-            Vector3d o = grid->getOrigin(), s = grid->getSpacing();
-            for (int a = 0; a < 3; a++) {
-                c.grid.origin[a] = o.data[a];
-                c.grid.spacing[a] = s.data[a];
-            }
-            c.grid.reflective = grid->isReflective() ? 1 : 0;
-            c.grid.clip_volume = grid->getClipVolume() ? 1 : 0;
-            fp.words(c.grid.values, sizeof(float) * 3 * v.size());
-            text << "  field: Grid3f " << c.grid.nx << "x" << c.grid.ny << "x" << c.grid.nz
-                 << " spacing " << s.x << " reflective " << c.grid.reflective << " clipVolume "
-                 << c.grid.clip_volume;
+            text << "  field: ";
+            fillGrid(*grid, 3, c.grid);
+        } else if (const ModulatedMagneticFieldGrid *g =
+                       dynamic_cast<const ModulatedMagneticFieldGrid *>(f)) {
+            ModulatedMagneticFieldGrid *q = const_cast<ModulatedMagneticFieldGrid *>(g);
+            ref_ptr<Grid3f> grid = q->getGrid();
+            ref_ptr<Grid1f> mod = q->getModulationGrid();
+            if (!grid.valid() || !mod.valid())
+                throw Unsupported("ModulatedMagneticFieldGrid without a grid");
+            c.kind = CRP_FIELD_MODULATED_GRID;
+            text << "  field: ModulatedMagneticFieldGrid ";
+            fillGrid(*grid, 3, c.grid);
+            text << " modulation ";
+            fillGrid(*mod, 1, c.modulation);
         } else if (const PlaneWaveTurbulence *w = dynamic_cast<const PlaneWaveTurbulence *>(f)) {
             const int nm = w->*member(WavesNm());
             const std::vector<Vector3d> &xi = w->*member(WavesXi());
@@ -287,6 +283,34 @@ struct Translation {
                  << wrap->reflective;
         text << "\n";
         fields.push_back(c);
+    }
+
+    // A Grid3f (width 3) or Grid1f (width 1) as a crp_grid3f_desc over the
+    // grid's own storage (Grid.h:161-336: origin, spacing, boundary flags,
+    // interpolation type).
+    template <typename T>
+    void fillGrid(Grid<T> &grid, int width, crp_grid3f_desc &d) {
+        std::vector<T> &v = grid.getGrid();
+        if (v.empty()) throw Unsupported("empty grid");
+        const interpolationType ip = grid.getInterpolationType();
+        if (ip != TRILINEAR && ip != TRICUBIC && ip != NEAREST_NEIGHBOUR)
+            throw Unsupported("grid interpolation " + grid.getInterpolationTypeName());
+        d.values = reinterpret_cast<const float *>(&v[0]);
+        d.nx = grid.getNx();
+        d.ny = grid.getNy();
+        d.nz = grid.getNz();
+        Vector3d o = grid.getOrigin(), s = grid.getSpacing();
+        for (int a = 0; a < 3; a++) {
+            d.origin[a] = o.data[a];
+            d.spacing[a] = s.data[a];
+        }
+        d.reflective = grid.isReflective() ? 1 : 0;
+        d.clip_volume = grid.getClipVolume() ? 1 : 0;
+        d.interpolation = (int32_t)ip;
+        fp.words(d.values, sizeof(float) * width * v.size());
+        text << (width == 3 ? "Grid3f " : "Grid1f ") << d.nx << "x" << d.ny << "x" << d.nz << " spacing "
+             << s.x << " reflective " << d.reflective << " clipVolume " << d.clip_volume << " "
+             << grid.getInterpolationTypeName();
     }
 
     void setField(const MagneticField *f) {
@@ -527,7 +551,7 @@ struct Translation {
         fp.value(seed);
         for (size_t i = 0; i < fields.size(); i++) {
             crp_field_component c = fields[i];
-            c.grid.values = 0;  // content hashed above
+            c.grid.values = c.modulation.values = 0;  // content hashed above
             c.plane_wave.xi = c.plane_wave.kappa = c.plane_wave.k = c.plane_wave.beta =
                 c.plane_wave.ak = 0;
             fp.value(c);

@@ -6,14 +6,19 @@
 //
 //   propagation   PropagationBP (fixed or adaptive), PropagationCK,
 //                 DiffusionSDE (no advection field)
-//   fields        MagneticFieldGrid over a trilinear Grid3f,
+//   fields        MagneticFieldGrid over a Grid3f (trilinear, tricubic or
+//                 nearest-neighbour), ModulatedMagneticFieldGrid,
 //                 PeriodicMagneticField, MagneticFieldList,
 //                 UniformMagneticField, PlaneWaveTurbulence,
 //                 ToroidalMagneticField (below)
 //   conditions    MaximumTrajectoryLength (no observer positions),
-//                 CandidateMaximumTrajectoryLength (below)
-//   observers     Observer with ObserverSurface(Sphere) or
-//                 ObserverDetectAll; any detection action
+//                 CandidateMaximumTrajectoryLength (below),
+//                 SphericalBoundary, CubicBoundary, EllipsoidalBoundary,
+//                 CylindricalBoundary
+//   observers     Observer with up to four features: ObserverSurface over a
+//                 Sphere, Plane or ParaxialBox, ObserverDetectAll,
+//                 ObserverTracking, Observer1D and the particle vetoes;
+//                 any detection action
 //
 // The user's chain objects are read, not replaced: the same ModuleList code
 // that builds a CPU simulation builds this one.  run() packs the candidates

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 2u
+#define CRP_ABI_VERSION 3u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -55,7 +55,16 @@ enum crp_field_kind {
     CRP_FIELD_GRID = 1,       /* MagneticFieldGrid over Grid3f (MagneticFieldGrid.cpp:17) */
     CRP_FIELD_PLANE_WAVE = 2, /* PlaneWaveTurbulence (PlaneWaveTurbulence.cpp:231) */
     CRP_FIELD_UNIFORM = 3,    /* UniformMagneticField (MagneticField.h:109) */
-    CRP_FIELD_TOROIDAL = 4    /* B = b0 * (-y, x, 0) / r, r = sqrt(x^2 + y^2) */
+    CRP_FIELD_TOROIDAL = 4,   /* B = b0 * (-y, x, 0) / r, r = sqrt(x^2 + y^2) */
+    CRP_FIELD_MODULATED_GRID = 5 /* ModulatedMagneticFieldGrid: Grid3f times a Grid1f
+                                    modulation (MagneticFieldGrid.cpp:51) */
+};
+
+/* Grid::setInterpolationType (Grid.h:255; enum interpolationType, Grid.h:24). */
+enum crp_interpolation {
+    CRP_INTERPOLATION_TRILINEAR = 0,        /* Grid.h:539 */
+    CRP_INTERPOLATION_TRICUBIC = 1,         /* Grid.h:459 (Vector3f: the SIMD form), Grid.h:504 */
+    CRP_INTERPOLATION_NEAREST_NEIGHBOUR = 2 /* closestValue, Grid.h:383 */
 };
 
 /* Grid3f payload and GridProperties (Grid.h:75).  values holds Nx*Ny*Nz
@@ -68,6 +77,8 @@ typedef struct crp_grid3f_desc {
     double spacing[3];
     int32_t reflective;  /* Grid::setReflective */
     int32_t clip_volume; /* Grid::setClipVolume */
+    int32_t interpolation; /* crp_interpolation */
+    int32_t _pad;
 } crp_grid3f_desc;
 
 /* Wave modes of a PlaneWaveTurbulence (PlaneWaveTurbulence.cpp:79-229),
@@ -99,6 +110,9 @@ typedef struct crp_field_component {
     crp_plane_wave_desc plane_wave;
     double uniform[3];
     double toroidal_b0;
+    /* CRP_FIELD_MODULATED_GRID: the Grid1f modulation, one float per cell
+     * (values: nx*ny*nz floats in the same order as a Grid3f's cells) */
+    crp_grid3f_desc modulation;
 } crp_field_component;
 
 /* ------------------------------------------------------------------------

@@ -264,16 +264,158 @@ static v3 stream_cone(stream_t *s, v3 mean, double radius) { /* Random.cpp:159, 
 /* Grid<Vector3f>::interpolate / trilinearInterpolate (Grid.h:318, :540),
  * values and weights in float as Vector3f * double converts the weight to
  * float (Vector3.h:305). */
+/* periodicBoundary / reflectiveBoundary of a cell index (Grid.h:37-46) and
+ * the symmetrical round (Grid.h:61). */
+static int periodic_boundary(int i, int n) { return ((i % n) + n) % n; }
+static int reflective_boundary(int i, int n) {
+    while ((i < -0.5) || (i > (n - 0.5))) i = 2 * n * (i > (n - 0.5)) - i - 1;
+    return i;
+}
+static double sym_round(double r) { return (r > 0.0) ? floor(r + 0.5) : ceil(r - 0.5); }
+
+static size_t grid_cell(const crp_grid3f_desc *g, int ix, int iy, int iz) {
+    return ((size_t)ix * (size_t)g->ny + (size_t)iy) * (size_t)g->nz + (size_t)iz;
+}
+static size_t grid_cell_bc(const crp_grid3f_desc *g, int ix, int iy, int iz) {
+    int nx = (int)g->nx, ny = (int)g->ny, nz = (int)g->nz;
+    if (g->reflective)
+        return grid_cell(g, reflective_boundary(ix, nx), reflective_boundary(iy, ny), reflective_boundary(iz, nz));
+    return grid_cell(g, periodic_boundary(ix, nx), periodic_boundary(iy, ny), periodic_boundary(iz, nz));
+}
+
+/* clipVolume test of Grid::interpolate (Grid.h:319). */
+static int grid_in_volume(const crp_grid3f_desc *g, v3 pos) {
+    v3 origin = mk(g->origin[0], g->origin[1], g->origin[2]);
+    v3 spacing = mk(g->spacing[0], g->spacing[1], g->spacing[2]);
+    v3 edge = add(origin, mulv(mk((double)g->nx, (double)g->ny, (double)g->nz), spacing));
+    int in = (pos.x >= origin.x) && (pos.x <= edge.x);
+    in &= (pos.y >= origin.y) && (pos.y <= edge.y);
+    in &= (pos.z >= origin.z) && (pos.z <= edge.z);
+    return in;
+}
+
+/* r = (position - gridOrigin) / spacing, gridOrigin = origin + spacing / 2 (Grid.h:227). */
+static v3 grid_unit(const crp_grid3f_desc *g, v3 pos) {
+    v3 origin = mk(g->origin[0], g->origin[1], g->origin[2]);
+    v3 spacing = mk(g->spacing[0], g->spacing[1], g->spacing[2]);
+    return divv(sub(pos, add(origin, divs(spacing, 2))), spacing);
+}
+
+/* CubicInterpolate, SIMD form (Grid.h:435), one lane: float arithmetic,
+ * pos^2 and pos^3 formed in double. */
+static float cubic_f(float p0, float p1, float p2, float p3, double position) {
+    const float c1 = 0.5f, c2 = 1.5f, c3 = 2.f, c4 = 2.5f;
+    float pos = (float)position, pos2 = (float)(position * position),
+          pos3 = (float)(position * position * position);
+    float term = (c1 * p2 - c1 * p0) * pos;
+    float term2 = ((p0 + c3 * p2) - (c4 * p1 + c1 * p3)) * pos2;
+    float term3 = ((c2 * p1 + c1 * p3) - (c1 * p0 + c2 * p2)) * pos3;
+    return ((term3 + term2) + term) + p1;
+}
+
+/* Grid<Vector3f>::tricubicInterpolate, SIMD form (Grid.h:459). */
+static v3 grid_tricubic3(const crp_grid3f_desc *g, v3 pos) {
+    v3 r = grid_unit(g, pos);
+    int ix0 = (int)floor(r.x), iy0 = (int)floor(r.y), iz0 = (int)floor(r.z);
+    double fx = r.x - ix0, fy = r.y - iy0, fz = r.z - iz0;
+    float vx[4][3], vy[4][3], vz[4][3];
+    for (int a = -1; a < 3; a++) {
+        for (int b = -1; b < 3; b++) {
+            for (int c = -1; c < 3; c++) {
+                const float *v = g->values + 3 * grid_cell_bc(g, ix0 + a, iy0 + b, iz0 + c);
+                vz[c + 1][0] = v[0]; vz[c + 1][1] = v[1]; vz[c + 1][2] = v[2];
+            }
+            for (int k = 0; k < 3; k++) vy[b + 1][k] = cubic_f(vz[0][k], vz[1][k], vz[2][k], vz[3][k], fz);
+        }
+        for (int k = 0; k < 3; k++) vx[a + 1][k] = cubic_f(vy[0][k], vy[1][k], vy[2][k], vy[3][k], fy);
+    }
+    float res[3];
+    for (int k = 0; k < 3; k++) res[k] = cubic_f(vx[0][k], vx[1][k], vx[2][k], vx[3][k], fx);
+    return mk(res[0], res[1], res[2]);
+}
+
+/* Grid::closestValue (Grid.h:383): cell of the nearest grid point. */
+static size_t grid_nearest_cell(const crp_grid3f_desc *g, v3 pos) {
+    v3 r = grid_unit(g, pos);
+    int nx = (int)g->nx, ny = (int)g->ny, nz = (int)g->nz;
+    int ix, iy, iz;
+    if (g->reflective) {
+        ix = (int)sym_round(r.x); iy = (int)sym_round(r.y); iz = (int)sym_round(r.z);
+        return grid_cell(g, reflective_boundary(ix, nx), reflective_boundary(iy, ny), reflective_boundary(iz, nz));
+    }
+    ix = (int)sym_round(fmod(r.x, nx));
+    iy = (int)sym_round(fmod(r.y, ny));
+    iz = (int)sym_round(fmod(r.z, nz));
+    ix = (ix + nx * (ix < 0)) % nx;
+    iy = (iy + ny * (iy < 0)) % ny;
+    iz = (iz + nz * (iz < 0)) % nz;
+    return grid_cell(g, ix, iy, iz);
+}
+
+/* CubicInterpolateScalar (Grid.h:498): the Catmull-Rom polynomial in double,
+ * terms grouped as the reference groups them (the sums round differently in
+ * any other order). */
+static double cubic_d(double p0, double p1, double p2, double p3, double pos) {
+    double a = -0.5 * p0 + 1.5 * p1 - 1.5 * p2 + 0.5 * p3;
+    double b = p0 - 2.5 * p1 + p2 * 2 - 0.5 * p3;
+    double c = -0.5 * p0 + 0.5 * p2;
+    return a * pos * pos * pos + b * pos * pos + c * pos + p1;
+}
+
+/* Grid<float>::interpolate (Grid.h:317) of a scalar grid (Grid1f). */
+static float scalar_grid(const crp_grid3f_desc *g, v3 pos) {
+    if (g->clip_volume && !grid_in_volume(g, pos)) return 0.f;
+    if (g->interpolation == CRP_INTERPOLATION_NEAREST_NEIGHBOUR) return g->values[grid_nearest_cell(g, pos)];
+    v3 r = grid_unit(g, pos);
+    if (g->interpolation == CRP_INTERPOLATION_TRICUBIC) {
+        int ix0 = (int)floor(r.x), iy0 = (int)floor(r.y), iz0 = (int)floor(r.z);
+        double fx = r.x - ix0, fy = r.y - iy0, fz = r.z - iz0;
+        double vx[4], vy[4], vz[4];
+        for (int a = -1; a < 3; a++) {
+            for (int b = -1; b < 3; b++) {
+                for (int c = -1; c < 3; c++) vz[c + 1] = g->values[grid_cell_bc(g, ix0 + a, iy0 + b, iz0 + c)];
+                vy[b + 1] = cubic_d(vz[0], vz[1], vz[2], vz[3], fz);
+            }
+            vx[a + 1] = cubic_d(vy[0], vy[1], vy[2], vy[3], fy);
+        }
+        return (float)cubic_d(vx[0], vx[1], vx[2], vx[3], fx);
+    }
+    int n[3] = {(int)g->nx, (int)g->ny, (int)g->nz}, lo[3], hi[3];
+    double rr[3] = {r.x, r.y, r.z}, f0[3], f1[3];
+    for (int a = 0; a < 3; a++) {
+        double x = rr[a];
+        if (g->reflective) { /* reflectiveClamp, Grid.h:49 */
+            while ((x < -0.5) || (x > (n[a] - 0.5))) x = 2 * n[a] * (x > (n[a] - 0.5)) - x - 1;
+            lo[a] = (int)floor(x);
+            hi[a] = lo[a] + (lo[a] < n[a] - 1);
+            if (x < 0) { lo[a] = 0; hi[a] = 0; }
+        } else { /* periodicClamp, Grid.h:29 */
+            lo[a] = (((int)floor(x) % n[a]) + n[a]) % n[a];
+            hi[a] = (lo[a] + 1) % n[a];
+        }
+        f0[a] = x - floor(x);
+        f1[a] = 1 - f0[a];
+    }
+    /* Grid.h:570-577 with T = float: products in double, sum into a float */
+    const int sel[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 0}, {1, 1, 1}};
+    float b = 0.f;
+    for (int k = 0; k < 8; k++) {
+        float v = g->values[grid_cell(g, sel[k][0] ? hi[0] : lo[0], sel[k][1] ? hi[1] : lo[1],
+                                      sel[k][2] ? hi[2] : lo[2])];
+        b += v * (sel[k][0] ? f0[0] : f1[0]) * (sel[k][1] ? f0[1] : f1[1]) * (sel[k][2] ? f0[2] : f1[2]);
+    }
+    return b;
+}
+
 static v3 grid_field(const crp_grid3f_desc *g, v3 pos) {
     v3 origin = mk(g->origin[0], g->origin[1], g->origin[2]);
     v3 spacing = mk(g->spacing[0], g->spacing[1], g->spacing[2]);
     int Nx = (int)g->nx, Ny = (int)g->ny, Nz = (int)g->nz;
-    if (g->clip_volume) { /* Grid.h:320 */
-        v3 edge = add(origin, mulv(mk((double)g->nx, (double)g->ny, (double)g->nz), spacing));
-        int in = (pos.x >= origin.x) && (pos.x <= edge.x);
-        in &= (pos.y >= origin.y) && (pos.y <= edge.y);
-        in &= (pos.z >= origin.z) && (pos.z <= edge.z);
-        if (!in) return mk(0, 0, 0);
+    if (g->clip_volume && !grid_in_volume(g, pos)) return mk(0, 0, 0); /* Grid.h:320 */
+    if (g->interpolation == CRP_INTERPOLATION_TRICUBIC) return grid_tricubic3(g, pos);
+    if (g->interpolation == CRP_INTERPOLATION_NEAREST_NEIGHBOUR) {
+        const float *v = g->values + 3 * grid_nearest_cell(g, pos);
+        return mk(v[0], v[1], v[2]);
     }
     v3 gridOrigin = add(origin, divs(spacing, 2)); /* Grid.h:227 */
     v3 r = divv(sub(pos, gridOrigin), spacing);
@@ -354,6 +496,10 @@ static v3 component_field(const crp_field_component *f, v3 position) {
     }
     switch (f->kind) {
     case CRP_FIELD_GRID: return grid_field(&f->grid, pos);
+    case CRP_FIELD_MODULATED_GRID: { /* ModulatedMagneticFieldGrid::getField, MagneticFieldGrid.cpp:51 */
+        float m = scalar_grid(&f->modulation, pos);
+        return muls(grid_field(&f->grid, pos), (double)m);
+    }
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(&f->plane_wave, pos);
     case CRP_FIELD_UNIFORM: return mk(f->uniform[0], f->uniform[1], f->uniform[2]);
     case CRP_FIELD_TOROIDAL: {

@@ -16,6 +16,7 @@
 #include "crpropa/Source.h"
 #include "crpropa/Units.h"
 #include "crpropa/module/BreakCondition.h"
+#include "crpropa/module/RestrictToRegion.h"
 #include "crpropa/module/SimplePropagation.h"
 #include "crpropa/module/TextOutput.h"
 
@@ -160,8 +161,8 @@ int ref_run_source_textout(const crp_plan_desc *desc, int gpu, int precision, co
 /* The plugin's translation of the chain of `desc` (no device needed):
  * returns 1 and the plan text if the chain is on the device path, 0 and the
  * reason otherwise.  extra: 1 appends a SimplePropagation, 2 a
- * MinimumEnergy, 3 sets MaximumTrajectoryLength observer positions, 4 makes
- * the Grid3f tricubic, 5 sets setMakeRejectedInactive(false) on the
+ * MinimumEnergy, 3 sets MaximumTrajectoryLength observer positions, 4
+ * appends a RestrictToRegion, 5 sets setMakeRejectedInactive(false) on the
  * MaximumTrajectoryLength. */
 int ref_gpu_describe(const crp_plan_desc *desc, int extra, char *buf, size_t size) {
     try {
@@ -178,10 +179,7 @@ int ref_gpu_describe(const crp_plan_desc *desc, int extra, char *buf, size_t siz
             if (m && extra == 5) m->setMakeRejectedInactive(false);
         }
         if (extra == 4)
-            for (size_t i = 0; i < b.keep.size(); i++) {
-                Grid3f *grid = dynamic_cast<Grid3f *>(b.keep[i].get());
-                if (grid) grid->setInterpolationType(TRICUBIC);
-            }
+            g->add(new RestrictToRegion(new MaximumTrajectoryLength(1 * Mpc), new Sphere(Vector3d(0.), 1 * Mpc)));
         std::string why;
         if (!g->isSupported(&why)) {
             copy_text(why, buf, size);

@@ -11,7 +11,8 @@
  * What comes from the reference (unchanged, linked): Candidate, ModuleList
  * (src/ModuleList.cpp.in:97 run(candidate_vector) with OpenMP
  * schedule(static,100)), PropagationCK, PropagationBP, DiffusionSDE,
- * MagneticFieldGrid, PeriodicMagneticField, MagneticFieldList,
+ * MagneticFieldGrid (trilinear, tricubic and nearest-neighbour Grid3f),
+ * ModulatedMagneticFieldGrid, PeriodicMagneticField, MagneticFieldList,
  * UniformMagneticField, PlaneWaveTurbulence, MaximumTrajectoryLength,
  * Observer, ObserverSurface(Sphere), ObserverDetectAll, TextOutput, Source
  * features and Random.
@@ -137,20 +138,33 @@ uint64_t StepCounter::total() const {
     return s;
 }
 
+// A Grid3f (width 3) or Grid1f (width 1) holding a crp_grid3f_desc's values,
+// boundary flags and interpolation type.
+template <typename T>
+static ref_ptr<Grid<T> > make_grid(const crp_grid3f_desc &g, int width, Built &b) {
+    ref_ptr<Grid<T> > grid = new Grid<T>(Vector3d(g.origin[0], g.origin[1], g.origin[2]), g.nx, g.ny,
+                                         g.nz, Vector3d(g.spacing[0], g.spacing[1], g.spacing[2]));
+    grid->setReflective(g.reflective != 0);
+    grid->setClipVolume(g.clip_volume != 0);
+    grid->setInterpolationType((interpolationType)g.interpolation);
+    std::vector<T> &v = grid->getGrid();
+    std::memcpy(&v[0], g.values, sizeof(float) * width * g.nx * g.ny * g.nz);
+    b.keep.push_back(grid.get());
+    return grid;
+}
+
 static ref_ptr<MagneticField> build_component(const crp_field_component &f, Built &b,
                                               const Helpers *h) {
     ref_ptr<MagneticField> m;
     if (f.kind == CRP_FIELD_GRID) {
-        const crp_grid3f_desc &g = f.grid;
-        ref_ptr<Grid3f> grid = new Grid3f(Vector3d(g.origin[0], g.origin[1], g.origin[2]),
-                                          g.nx, g.ny, g.nz,
-                                          Vector3d(g.spacing[0], g.spacing[1], g.spacing[2]));
-        grid->setReflective(g.reflective != 0);
-        grid->setClipVolume(g.clip_volume != 0);
-        std::vector<Vector3f> &v = grid->getGrid();
-        std::memcpy(&v[0], g.values, sizeof(float) * 3 * g.nx * g.ny * g.nz);
-        b.keep.push_back(grid.get());
-        m = new MagneticFieldGrid(grid);
+        m = new MagneticFieldGrid(make_grid<Vector3f>(f.grid, 3, b));
+    } else if (f.kind == CRP_FIELD_MODULATED_GRID) {
+        ref_ptr<Grid3f> grid = make_grid<Vector3f>(f.grid, 3, b);
+        ref_ptr<Grid1f> mod = make_grid<float>(f.modulation, 1, b);
+        ref_ptr<ModulatedMagneticFieldGrid> mm = new ModulatedMagneticFieldGrid(grid, mod);
+        // the constructor resets both flags (MagneticFieldGrid.cpp:22-23)
+        mm->setReflective(f.grid.reflective != 0, f.modulation.reflective != 0);
+        m = mm;
     } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
         const crp_plane_wave_desc &p = f.plane_wave;
         TurbulenceSpectrum *spec = new TurbulenceSpectrum(p.brms, p.lmin, p.lmax, p.lbendover,

@@ -68,7 +68,7 @@ def test_plugin_translates_reference_chains(plugin, oracle):
     (1, "SimplePropagation"),
     (2, "MinimumEnergy"),
     (3, "observer positions"),
-    (4, "TRICUBIC"),
+    (4, "RestrictToRegion"),
     (5, "setMakeRejectedInactive(false)"),
 ])
 def test_plugin_declines_chains_off_the_device_path(plugin, extra, reason):
