@@ -370,6 +370,7 @@ def secondary_configs(dev, peaks):
     out.update(cfg_grid_ck_64(dev, peaks))
     out.update(cfg_grid_ck_nuclei(dev, peaks))
     out.update(cfg_sde_galactic(dev, peaks))
+    out.update(cfg_jf12_backtrack(dev, peaks))
     return out
 
 
@@ -465,6 +466,28 @@ def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
     return out
 
 
+def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000):
+    """PropagationCK backtracking through the JF12 regular field, full runs,
+    FP64 and mixed forms, beside the reference's own CPU run of a sample."""
+    from crpropa3_b200 import _abi, engine, workloads as W
+    res = {"workload": f"{n} antiprotons 5-100 EeV from (-8.5 kpc, 0, 0), JF12Field (regular), "
+                       "PropagationCK 1e-4 0.1-100 pc, Observer sphere 20 kpc, full runs"}
+    for prec, name in ((_abi.PRECISION_FP64, "fp64"), (_abi.PRECISION_MIXED, "mixed")):
+        spec, cands = W.jf12_backtrack(n=n, precision=prec)
+        plan = engine.Plan(spec)
+        t = _timed_runs(plan, cands.to_device(dev), cands.to_device(dev), 2)
+        secs = t["device_ms"] / 1e3
+        res[name] = {"tries_per_s": t["tries"] / secs, "particle_steps_per_s": t["particle_steps"] / secs,
+                     "field_evaluations_per_s": t["field_evaluations"] / secs, "ms_per_run": t["device_ms"] / 2}
+        plan.close()
+    spec, cands = W.jf12_backtrack(n=n_cpu, precision=_abi.PRECISION_FP64)
+    cpu = reference_cpu_rate(spec, cands, n_cpu, cpu_threads())
+    if cpu is not None:
+        res["cpu_reference"] = {"particle_steps_per_s": cpu["value"], "cores": cpu_threads(),
+                                "sample": f"{n_cpu} candidates, full runs"}
+    return {"jf12_backtrack": res}
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -497,7 +520,8 @@ def main():
         dev = f"cuda:{local}"
         runs = {"grid_ck_64": lambda: cfg_grid_ck_64(dev, {}, n=args.n or 10_000),
                 "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or (1 << 20)),
-                "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20))}
+                "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20)),
+                "jf12_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20))}
         if args.workload not in runs:
             log(f"unknown workload {args.workload}")
             return 2

@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 3
+ABI_VERSION = 5
 
 # crp_status
 OK = 0
@@ -33,7 +33,10 @@ STATUS_NAMES = {
     ERR_NO_DEVICE: "CRP_ERR_NO_DEVICE",
 }
 
-FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID = 1, 2, 3, 4, 5
+FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID, FIELD_JF12, FIELD_UF23 = \
+    1, 2, 3, 4, 5, 6, 7
+UF23_BASE, UF23_NECL, UF23_EXPX, UF23_SPUR, UF23_CRE10, UF23_SYNCG, UF23_TWISTX, UF23_NEBCOR = range(8)
+JF12_VARIANT_JF12, JF12_VARIANT_PLANCK = 0, 1
 INTERPOLATION_TRILINEAR, INTERPOLATION_TRICUBIC, INTERPOLATION_NEAREST_NEIGHBOUR = 0, 1, 2
 MODULE_PROPAGATION, MODULE_MAX_TRAJECTORY_LENGTH, MODULE_OBSERVER, MODULE_BOUNDARY = 1, 2, 3, 4
 PROP_CK, PROP_BP, PROP_SDE = 1, 2, 3
@@ -63,11 +66,43 @@ class PlaneWaveDesc(C.Structure):
                 ("lmax", _d), ("lbendover", _d), ("sindex", _d), ("qindex", _d)]
 
 
+TURBULENCE_GRID, TURBULENCE_SIMPLE, TURBULENCE_HELICAL = 0, 1, 2
+
+
+class TurbulenceDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("seed", C.c_int32), ("n", C.c_uint64), ("spacing", _d), ("brms", _d),
+                ("lmin", _d), ("lmax", _d), ("lbendover", _d), ("sindex", _d), ("qindex", _d),
+                ("helicity", _d)]
+
+
+class JF12Desc(C.Structure):
+    _fields_ = [("use_regular", C.c_int32), ("use_disk", C.c_int32), ("use_toroidal_halo", C.c_int32),
+                ("use_x", C.c_int32), ("use_striated", C.c_int32), ("use_turbulent", C.c_int32),
+                ("variant", C.c_int32), ("_pad", C.c_int32), ("kpc", _d), ("sin_pitch", _d), ("cos_pitch", _d), ("tan90_minus_pitch", _d),
+                ("r_arms", _d * 8), ("b_ring", _d), ("h_disk", _d), ("w_disk", _d), ("b_disk", _d * 8),
+                ("b_north", _d), ("b_south", _d), ("r_north", _d), ("r_south", _d), ("w_halo", _d),
+                ("z0", _d), ("b_x", _d), ("sin_theta_x0", _d), ("cos_theta_x0", _d), ("tan_theta_x0", _d),
+                ("r_xc", _d), ("r_x", _d), ("sqrt_beta", _d), ("b_disk_turb", _d * 8),
+                ("b_disk_turb5", _d), ("z_disk_turb", _d), ("b_halo_turb", _d), ("r_halo_turb", _d),
+                ("z_halo_turb", _d)]
+
+
+class UF23Desc(C.Structure):
+    _fields_ = [("model", C.c_int32), ("_pad", C.c_int32)] + [
+        (n, _d) for n in ("disk_b1", "disk_b2", "disk_b3", "disk_h", "disk_phase1", "disk_phase2", "disk_phase3",
+                          "disk_pitch", "disk_w", "poloidal_a", "poloidal_b", "poloidal_p", "poloidal_r",
+                          "poloidal_w", "poloidal_z", "poloidal_xi", "spur_center", "spur_length", "spur_width",
+                          "striation", "toroidal_bn", "toroidal_bs", "toroidal_r", "toroidal_w", "toroidal_z",
+                          "twisting_time", "sin_pitch", "cos_pitch", "tan_pitch", "max_radius_squared", "kpc",
+                          "microgauss")]
+
+
 class FieldComponent(C.Structure):
     _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
                 ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
                 ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
-                ("toroidal_b0", _d), ("modulation", GridDesc)]
+                ("toroidal_b0", _d), ("modulation", GridDesc), ("jf12", JF12Desc),
+                ("uf23", UF23Desc)]
 
 
 class FeatureDesc(C.Structure):

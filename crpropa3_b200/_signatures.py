@@ -34,6 +34,11 @@ SIGNATURES = {
     "crp_bp_adjoint_backward": (_i32, [C.POINTER(_abi.AdjointDesc), C.POINTER(_abi.AdjointIO),
                                        C.c_void_p, C.c_size_t, C.c_void_p]),
     "crp_random_draws": (_i32, [_u32, _i32, _u64, _d, _d, _d, _dp]),
+    "crp_jf12_defaults": (_i32, [_i32, C.POINTER(_abi.JF12Desc)]),
+    "crp_uf23_defaults": (_i32, [_i32, C.POINTER(_abi.UF23Desc)]),
+    "crp_turbulence_draws": (_i32, [_u32, _i32, _u64, _dp]),
+    "crp_turbulence_modes": (_i32, [C.POINTER(_abi.TurbulenceDesc), C.POINTER(C.c_uint64)]),
+    "crp_turbulence_grid": (_i32, [C.POINTER(_abi.TurbulenceDesc), C.c_void_p, C.c_void_p]),
     "crp_plane_wave_modes": (_i32, [_d, _d, _d, _d, _d, _d, _i32, _i32, _dp, _dp, _dp, _dp, _dp]),
     "crp_source_sample": (_i32, [C.c_void_p, _u32, _u64, _i32p, _dp, _dp]),
     "crp_text_output_write": (_i32, [C.c_char_p, _i32, _i32, C.c_void_p, _u64, C.c_void_p]),

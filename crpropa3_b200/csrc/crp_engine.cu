@@ -255,6 +255,54 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         st = upload(p, a32.data(), a32.size(), &d.pw.modes32);
         if (st) return st;
         d.pw.n = n;
+    } else if (f.kind == CRP_FIELD_JF12) {
+        const crp_jf12_desc &J = f.jf12;
+        if (!(J.kpc > 0)) return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: parameters not set (crp_jf12_defaults)");
+        DevJF12 h;
+        std::memset(&h, 0, sizeof(h));
+        h.d = J;
+        h.inv_kpc = 1.0 / J.kpc;
+        // Units.h: muG = 1e-6 gauss, gauss = 1e-4 tesla
+        h.muG = 1e-6 * 1e-4;
+        const double L = 1.0 / J.kpc, B = 1.0 / h.muG;
+        for (int i = 0; i < 8; i++) {
+            h.rarms[i] = (float)(J.r_arms[i] * L);
+            h.bdisk[i] = (float)(J.b_disk[i] * B);
+            h.bdturb[i] = (float)(J.b_disk_turb[i] * B);
+        }
+        h.bring = (float)(J.b_ring * B); h.hdisk = (float)(J.h_disk * L); h.wdisk = (float)(J.w_disk * L);
+        h.bnorth = (float)(J.b_north * B); h.bsouth = (float)(J.b_south * B);
+        h.rnorth = (float)(J.r_north * L); h.rsouth = (float)(J.r_south * L);
+        h.whalo = (float)(J.w_halo * L); h.z0 = (float)(J.z0 * L);
+        h.bx = (float)(J.b_x * B); h.sinthx0 = (float)J.sin_theta_x0; h.costhx0 = (float)J.cos_theta_x0;
+        h.tanthx0 = (float)J.tan_theta_x0; h.rxc = (float)(J.r_xc * L); h.rx = (float)(J.r_x * L);
+        h.sinp = (float)J.sin_pitch; h.cosp = (float)J.cos_pitch; h.tan90mp = (float)J.tan90_minus_pitch;
+        h.sqrtbeta = (float)J.sqrt_beta;
+        h.bdturb5 = (float)(J.b_disk_turb5 * B); h.zdturb = (float)(J.z_disk_turb * L);
+        h.bhturb = (float)(J.b_halo_turb * B); h.rhturb = (float)(J.r_halo_turb * L);
+        h.zhturb = (float)(J.z_halo_turb * L);
+        if (J.use_turbulent) {  // JF12Field::setTurbulentGrid (JF12Field.cpp:118)
+            if (!f.grid.values)
+                return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: No turbulent field set (use_turbulent without a grid)");
+            crp_status st = build_grid(p, f.grid, 3, d.grid);
+            if (st) return st;
+        }
+        if (J.use_striated) {  // JF12Field::setStriatedGrid (JF12Field.cpp:113)
+            if (!f.modulation.values)
+                return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: No striated field set (use_striated without a grid)");
+            crp_status st = build_grid(p, f.modulation, 1, d.mod);
+            if (st) return st;
+        }
+        crp_status st = upload(p, &h, 1, &d.jf);
+        if (st) return st;
+    } else if (f.kind == CRP_FIELD_UF23) {
+        const crp_uf23_desc &U = f.uf23;
+        if (U.model < CRP_UF23_BASE || U.model > CRP_UF23_NEBCOR)
+            return fail(CRP_ERR_INVALID_ARGUMENT, "UF23Field: unknown field model");
+        if (!(U.kpc > 0) || !(U.microgauss > 0))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "UF23Field: parameters not set (crp_uf23_defaults)");
+        crp_status st = upload(p, &U, 1, &d.uf);
+        if (st) return st;
     } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {
     } else {
         return fail(CRP_ERR_UNSUPPORTED, "unsupported field kind %d", f.kind);

@@ -6,6 +6,8 @@
 
 #include <cstdint>
 
+#include "crp_gpu.h"
+
 namespace crp {
 
 constexpr int kMaxFields = 4;
@@ -35,6 +37,18 @@ struct DevPlaneWave {
     int n;
 };
 
+// JF12Field parameters (crp_jf12_desc, SI) for the FP64 form, and the same
+// parameters as floats with lengths in kpc and fields in muG for the mixed
+// form (positions of ~1e20 m would overflow FP32 squares).
+struct DevJF12 {
+    crp_jf12_desc d;
+    double inv_kpc, muG;
+    float rarms[8], bdisk[8], bdturb[8];
+    float bring, hdisk, wdisk, bnorth, bsouth, rnorth, rsouth, whalo, z0;
+    float bx, sinthx0, costhx0, tanthx0, rxc, rx, sinp, cosp, tan90mp, sqrtbeta;
+    float bdturb5, zdturb, bhturb, rhturb, zhturb;
+};
+
 struct DevComponent {
     int kind;       // crp_field_kind
     int periodic;
@@ -45,7 +59,10 @@ struct DevComponent {
     DevPlaneWave pw;
     double uniform[3];
     double b0;
-    DevGrid mod;    // CRP_FIELD_MODULATED_GRID: the Grid1f modulation (values: one float per cell)
+    DevGrid mod;    // CRP_FIELD_MODULATED_GRID: the Grid1f modulation (values: one float per cell);
+                    // CRP_FIELD_JF12: the striated grid (grid: the turbulent grid)
+    const DevJF12 *jf;  // CRP_FIELD_JF12: device copy of the parameters
+    const crp_uf23_desc *uf;  // CRP_FIELD_UF23: device copy of the parameters
 };
 
 struct DevModule {

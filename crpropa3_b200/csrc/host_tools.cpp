@@ -60,6 +60,14 @@ public:
         return y ^ (y >> 18);
     }
     double rand() { return double(u32()) * (1.0 / 4294967295.0); }
+    double exc() { return double(u32()) * (1.0 / 4294967296.0); }               // randExc
+    double dbl_exc() { return (double(u32()) + 0.5) * (1.0 / 4294967296.0); }  // randDblExc
+    // randNorm(0, 1) (Random.cpp:111): Box-Muller, one value per two draws
+    double norm() {
+        const double r = std::sqrt(-2.0 * std::log(1.0 - dbl_exc())) * 1.0;
+        const double phi = 2.0 * 3.14159265358979323846264338328 * exc();
+        return 0.0 + r * std::cos(phi);
+    }
     double uniform(double a, double b) { return a + (b - a) * rand(); }
     void vector(double &x, double &y, double &z) {
         double zz = uniform(-1.0, 1.0);
@@ -125,10 +133,173 @@ crp_status crp_random_draws(uint32_t seed, int32_t kind, uint64_t n, double a, d
         case 1: out[i] = r.uniform(a, b); break;
         case 2: r.vector(out[3 * i], out[3 * i + 1], out[3 * i + 2]); break;
         case 3: out[i] = r.power_law(a, b, c); break;
+        case 4: out[i] = r.norm(); break;
         case 6: out[i] = (double)r.u32(); break;
         default: return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown draw kind");
         }
     }
+    return CRP_OK;
+}
+
+crp_status crp_turbulence_draws(uint32_t seed, int32_t kind, uint64_t n_modes, double *out) {
+    if (!out && n_modes) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (seed == 0) return host_fail(CRP_ERR_INVALID_ARGUMENT, "seed 0 is not reproducible; give a non-zero seed");
+    Mt r(seed);
+    for (uint64_t i = 0; i < n_modes; i++) {
+        switch (kind) {
+        case CRP_TURBULENCE_GRID:  // GridTurbulence.cpp:97, :104
+            out[2 * i] = r.rand();
+            out[2 * i + 1] = r.rand();
+            break;
+        case CRP_TURBULENCE_SIMPLE:  // SimpleGridTurbulence.cpp:88-93
+            out[3 * i] = r.rand();
+            out[3 * i + 1] = r.norm();
+            out[3 * i + 2] = r.rand();
+            break;
+        case CRP_TURBULENCE_HELICAL:  // HelicalGridTurbulence.cpp:88-92
+            out[3 * i] = r.norm();
+            out[3 * i + 1] = r.rand();
+            out[3 * i + 2] = r.rand();
+            break;
+        default: return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown turbulence kind");
+        }
+    }
+    return CRP_OK;
+}
+
+crp_status crp_jf12_defaults(int32_t variant, crp_jf12_desc *out) {
+    if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (variant != 0 && variant != 1) return host_fail(CRP_ERR_INVALID_ARGUMENT, "JF12 variant must be 0 or 1");
+    // Units.h: tesla = 1, gauss = 1e-4 tesla, au = 149597870700 m, parsec = 648000 / pi au
+    const double au = 149597870700.0, parsec = 648000 / M_PI * au, kpc = 1e3 * parsec;
+    const double gauss = 1e-4, muG = 1e-6 * gauss;
+    crp_jf12_desc &j = *out;
+    std::memset(&j, 0, sizeof(j));
+    j.use_regular = j.use_disk = j.use_toroidal_halo = j.use_x = 1;
+    j.variant = variant;
+    j.kpc = kpc;
+    // the constructor evaluates sin, cos and tan at run time (JF12Field.cpp:17-22, 55-58); the
+    // volatile angles keep this compiler from folding them with another rounding
+    volatile double pitch_v = 11.5 * M_PI / 180, theta_v = 49.0 * M_PI / 180;
+    const double pitch = pitch_v, thetaX0 = theta_v;
+    j.sin_pitch = std::sin(pitch);
+    j.cos_pitch = std::cos(pitch);
+    j.tan90_minus_pitch = std::tan(M_PI / 2 - pitch);
+    const double arms[8] = {5.1, 6.3, 7.1, 8.3, 9.8, 11.4, 12.7, 15.5};
+    for (int i = 0; i < 8; i++) j.r_arms[i] = arms[i] * kpc;
+    j.b_ring = 0.1 * muG;
+    j.h_disk = 0.40 * kpc;
+    j.w_disk = 0.27 * kpc;
+    const double disk[8] = {0.1, 3.0, -0.9, -0.8, -2.0, -4.2, 0.0, 2.7};
+    for (int i = 0; i < 8; i++) j.b_disk[i] = disk[i] * muG;
+    j.b_north = 1.4 * muG;
+    j.b_south = -1.1 * muG;
+    j.r_north = 9.22 * kpc;
+    j.r_south = 17 * kpc;
+    j.w_halo = 0.20 * kpc;
+    j.z0 = 5.3 * kpc;
+    j.b_x = 4.6 * muG;
+    j.sin_theta_x0 = std::sin(thetaX0);
+    j.cos_theta_x0 = std::cos(thetaX0);
+    j.tan_theta_x0 = std::tan(thetaX0);
+    j.r_xc = 4.8 * kpc;
+    j.r_x = 2.9 * kpc;
+    volatile double beta_v = 1.36;
+    j.sqrt_beta = std::sqrt((double)beta_v);
+    const double turb[8] = {10.81, 6.96, 9.59, 6.96, 1.96, 16.34, 37.29, 10.35};
+    for (int i = 0; i < 8; i++) j.b_disk_turb[i] = turb[i] * muG;
+    j.b_disk_turb5 = 7.63 * muG;
+    j.z_disk_turb = 0.61 * kpc;
+    j.b_halo_turb = 4.68 * muG;
+    j.r_halo_turb = 10.97 * kpc;
+    j.z_halo_turb = 2.84 * kpc;
+    if (variant == 1) {  // PlanckJF12bField (JF12Field.cpp:352-371)
+        j.b_disk[5] = -3.5 * muG;
+        j.b_x = 1.8 * muG;
+        const double pturb[8] = {3.12, 6.24, 3.12, 6.24, 3.12, 6.24, 3.12, 6.24};
+        for (int i = 0; i < 8; i++) j.b_disk_turb[i] = pturb[i] * muG;
+        j.b_disk_turb5 = 3.90 * muG;
+        j.b_halo_turb = 7.332 * muG;
+    }
+    return CRP_OK;
+}
+
+crp_status crp_uf23_defaults(int32_t model, crp_uf23_desc *out) {
+    if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (model < CRP_UF23_BASE || model > CRP_UF23_NEBCOR) return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown field model");
+    // the model's units (UF23Field.cpp:48-57): kpc = 1, microgauss = 1, megayear = 1
+    const double kPi = 3.1415926535897932384626, degree = kPi / 180.;
+    // Table 3 of the UF23 paper as the constructor sets it (UF23Field.cpp:70-256), one row per
+    // model: B1 B2 B3 H phase1 phase2 phase3 pitch W | poloidal B P R W Z | striation |
+    // toroidal BN BS R W Z  (angles in degrees); spur, twistX and expX add their own below
+    struct Row { double v[20]; };
+    static const Row rows[8] = {
+        /* base */ {{1.0878565e+00, 2.6605034e+00, 3.1166311e+00, 7.9408965e-01, 2.6316589e+02, 9.7782269e+01,
+                     3.5112281e+01, 1.0106900e+01, 1.0720909e-01, 9.7775487e-01, 1.4266186e+00, 7.2925417e+00,
+                     1.1188158e-01, 4.4597373e+00, 3.4557571e-01, 3.2556760e+00, -3.0914569e+00, 1.0193815e+01,
+                     1.6936993e+00, 4.0242749e+00}},
+        /* neCL */ {{1.4259645e+00, 1.3543223e+00, 3.4390669e+00, 6.7405199e-01, 1.9961898e+02, 1.3541461e+02,
+                     6.4909767e+01, 1.1867859e+01, 6.1162799e-02, 9.8387831e-01, 1.6773615e+00, 7.4084361e+00,
+                     1.4168192e-01, 3.6521188e+00, 3.3600213e-01, 2.6256593e+00, -2.5699466e+00, 1.0134257e+01,
+                     1.1547728e+00, 4.5585463e+00}},
+        /* expX */ {{9.9258148e-01, 2.1821124e+00, 3.1197345e+00, 7.1508681e-01, 2.4745741e+02, 9.8578879e+01,
+                     3.4884485e+01, 1.0027070e+01, 9.8524736e-02, 5.8357990e+00, 1.9510779e+00, 2.4994376e+00,
+                     0, 0, 5.1440500e-01, 2.7077434e+00, -2.5677104e+00, 1.0134022e+01, 2.0956159e+00,
+                     5.4564991e+00}},
+        /* spur */ {{-4.2993328e+00, 0, 0, 7.5019749e-01, 1.5589875e+02, 0, 0, 1.2074432e+01, 1.2263120e-01,
+                     9.9302987e-01, 1.3982374e+00, 7.1973387e+00, 1.2262244e-01, 4.4853270e+00, 3.3022369e-01,
+                     2.9286724e+00, -2.5979895e+00, 9.7536425e+00, 1.4210055e+00, 6.0941229e+00}},
+        /* cre10 */ {{1.2035697e+00, 2.7478490e+00, 3.2104342e+00, 8.0844932e-01, 2.6515882e+02, 9.8211313e+01,
+                      3.5944588e+01, 1.0162759e+01, 1.0824003e-01, 9.6938453e-01, 1.4150957e+00, 7.2987296e+00,
+                      1.0923051e-01, 4.5748332e+00, 2.4950386e-01, 3.7308133e+00, -3.5039958e+00, 1.0407507e+01,
+                      1.7398375e+00, 2.9272800e+00}},
+        /* synCG */ {{8.1386878e-01, 2.0586930e+00, 2.9437335e+00, 6.2172353e-01, 2.2988551e+02, 9.7388282e+01,
+                      3.2927367e+01, 9.9034844e+00, 6.6517521e-02, 8.0883734e-01, 1.5820957e+00, 7.4625235e+00,
+                      1.5003765e-01, 3.5338550e+00, 6.3434763e-01, 2.3991193e+00, -2.0919944e+00, 9.4227834e+00,
+                      9.1608418e-01, 5.5844594e+00}},
+        /* twistX */ {{1.3741995e+00, 2.0089881e+00, 1.5212463e+00, 9.3806180e-01, 2.3560316e+02, 1.0189856e+02,
+                       5.6187572e+01, 1.2100979e+01, 1.4933338e-01, 6.2793114e-01, 2.3292519e+00, 7.9212358e+00,
+                       2.9056201e-01, 2.6274437e+00, 7.7616317e-01, 0, 0, 0, 0, 0}},
+        /* nebCor */ {{1.4081935e+00, 3.5292400e+00, 4.1290147e+00, 8.1151971e-01, 2.6447529e+02, 9.7572660e+01,
+                       3.6403798e+01, 1.0151183e+01, 1.1863734e-01, 1.3485916e+00, 1.3414395e+00, 7.2473841e+00,
+                       1.4318227e-01, 4.8242603e+00, 3.8610837e-10, 4.6491142e+00, -4.5006610e+00, 1.0205288e+01,
+                       1.7004868e+00, 3.5557767e+00}},
+    };
+    const double *v = rows[model].v;
+    crp_uf23_desc &u = *out;
+    std::memset(&u, 0, sizeof(u));
+    u.model = model;
+    // the a -> infinity of all but expX: "1 * Gpc" in the constructor names crpropa::Gpc
+    // (Units.h:116, in metres), not uf23::Gpc, so a is 1 Gpc in metres read as kpc
+    const double au_ = 149597870700.0, parsec_ = 648000 / M_PI * au_;
+    u.poloidal_a = 1 * (1e9 * parsec_);
+    u.disk_b1 = v[0]; u.disk_b2 = v[1]; u.disk_b3 = v[2]; u.disk_h = v[3];
+    u.disk_phase1 = v[4] * degree; u.disk_phase2 = v[5] * degree; u.disk_phase3 = v[6] * degree;
+    u.disk_pitch = v[7] * degree; u.disk_w = v[8];
+    u.poloidal_b = v[9]; u.poloidal_p = v[10]; u.poloidal_r = v[11]; u.poloidal_w = v[12];
+    u.poloidal_z = v[13]; u.striation = v[14];
+    u.toroidal_bn = v[15]; u.toroidal_bs = v[16]; u.toroidal_r = v[17]; u.toroidal_w = v[18];
+    u.toroidal_z = v[19];
+    if (model == CRP_UF23_SPUR) {
+        u.spur_center = 1.5718686e+02 * degree;
+        u.spur_length = 3.1839577e+01 * degree;
+        u.spur_width = 1.0318114e+01 * degree;
+    }
+    if (model == CRP_UF23_TWISTX) u.twisting_time = 5.4733549e+01;
+    if (model == CRP_UF23_EXPX) {  // internally xi is fitted and z = tan(xi) a
+        u.poloidal_a = 6.1938701e+00;
+        volatile double xi = 2.0926122e+01 * degree;
+        u.poloidal_xi = xi;
+        u.poloidal_z = u.poloidal_a * std::tan(u.poloidal_xi);
+    }
+    volatile double pitch = u.disk_pitch;  // evaluated at run time, as the constructor does
+    u.sin_pitch = std::sin((double)pitch);
+    u.cos_pitch = std::cos((double)pitch);
+    u.tan_pitch = std::tan((double)pitch);
+    u.max_radius_squared = std::pow(30., 2);
+    const double au = 149597870700.0, parsec = 648000 / M_PI * au;
+    u.kpc = 1e3 * parsec;
+    u.microgauss = 1e-6 * 1e-4;
     return CRP_OK;
 }
 

@@ -19,6 +19,7 @@
 #include "crmath.cuh"
 #include "engine_internal.h"
 #include "grid_interp.cuh"
+#include "uf23.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -162,6 +163,144 @@ __device__ d3 plane_wave_field(const DevPlaneWave &w, d3 pos) {
     return B;
 }
 
+// ---------------------------------------------------------------- JF12Field
+// The reference's arithmetic operation for operation (JF12Field.cpp:195-346);
+// exp, sin, cos and atan2 are CUDA's (within an ulp or two of glibc's);
+// pow(v, 2) is v * v, its correctly rounded value.
+
+// JF12Field::logisticFunction (JF12Field.cpp:195)
+__device__ __forceinline__ double jf_logistic(double x, double x0, double w) {
+    return 1. / (1. + exp(-2. * (fabs(x) - x0) / w));
+}
+
+__device__ __forceinline__ double jf_sq(double v) { return v * v; }
+
+// Vector3::getPhi (Vector3.h:136)
+__device__ __forceinline__ double jf_phi(double x, double y) {
+    const double eps = 2.2250738585072014e-308;  // numeric_limits<double>::min()
+    if ((fabs(x) < eps) && (fabs(y) < eps)) return 0.0;
+    return atan2(y, x);
+}
+
+// Radius of the spiral arm through (r, phi) where it crosses the negative x
+// axis, the arm-region lookup of getDiskField / getTurbulentStrength
+// (JF12Field.cpp:228-233, :315-320).
+__device__ __forceinline__ double jf_r_negx(const crp_jf12_desc &J, double r, double phi) {
+    double r_negx = r * exp(-(phi - M_PI) / J.tan90_minus_pitch);
+    if (r_negx > J.r_arms[7]) r_negx = r * exp(-(phi + M_PI) / J.tan90_minus_pitch);
+    if (r_negx > J.r_arms[7]) r_negx = r * exp(-(phi + 3 * M_PI) / J.tan90_minus_pitch);
+    return r_negx;
+}
+
+// JF12Field::getRegularField (JF12Field.cpp:199) with getDiskField (:216),
+// getToroidalHaloField (:248) and getXField (:267).
+__device__ d3 jf12_regular(const crp_jf12_desc &J, d3 pos) {
+    d3 b = mk(0., 0., 0.);
+    const double kpc = J.kpc;
+    const double d = sqrt(pos.x * pos.x + pos.y * pos.y + pos.z * pos.z);
+    if (!(d < 20 * kpc)) return b;
+    const double r = sqrt(pos.x * pos.x + pos.y * pos.y), z = pos.z;
+    const double phi = jf_phi(pos.x, pos.y);
+    const double sinPhi = sin(phi), cosPhi = cos(phi);
+    d3 bd = mk(0., 0., 0.);
+    if (J.use_disk) {
+        const double lfDisk = jf_logistic(z, J.h_disk, J.w_disk);
+        if (r > 3 * kpc) {
+            if (r < 5 * kpc) {  // molecular ring
+                const double bMag = J.b_ring * (5 * kpc / r) * (1 - lfDisk);
+                bd.x += -bMag * sinPhi;
+                bd.y += bMag * cosPhi;
+            } else {            // spiral region
+                const double r_negx = jf_r_negx(J, r, phi);
+                double bMag = 0;
+                for (int i = 7; i >= 0; i--)
+                    if (r_negx < J.r_arms[i]) bMag = J.b_disk[i];
+                bMag *= (5 * kpc / r) * (1 - lfDisk);
+                bd.x += bMag * (J.sin_pitch * cosPhi - J.cos_pitch * sinPhi);
+                bd.y += bMag * (J.sin_pitch * sinPhi + J.cos_pitch * cosPhi);
+            }
+        }
+    }
+    b = add(b, bd);
+    const bool outside1 = r * r + z * z > 1 * kpc * kpc;
+    d3 bh = mk(0., 0., 0.);
+    if (J.use_toroidal_halo && outside1) {
+        const double lfDisk = jf_logistic(z, J.h_disk, J.w_disk);
+        double bMagH = exp(-fabs(z) / J.z0) * lfDisk;
+        if (z >= 0)
+            bMagH *= J.b_north * (1 - jf_logistic(r, J.r_north, J.w_halo));
+        else
+            bMagH *= J.b_south * (1 - jf_logistic(r, J.r_south, J.w_halo));
+        bh.x += -bMagH * sinPhi;
+        bh.y += bMagH * cosPhi;
+    }
+    b = add(b, bh);
+    d3 bx = mk(0., 0., 0.);
+    if (J.use_x && outside1) {
+        double bMagX, sinThetaX, cosThetaX, rp;
+        const double rc = J.r_xc + fabs(z) / J.tan_theta_x0;
+        if (r < rc) {  // varying elevation region
+            rp = r * J.r_xc / rc;
+            bMagX = J.b_x * exp(-1 * rp / J.r_x) * jf_sq(J.r_xc / rc);
+            double thetaX = atan2(fabs(z), (r - rp));
+            if (z == 0) thetaX = M_PI / 2.;
+            sinThetaX = sin(thetaX);
+            cosThetaX = cos(thetaX);
+        } else {       // constant elevation region
+            rp = r - fabs(z) / J.tan_theta_x0;
+            bMagX = J.b_x * exp(-rp / J.r_x) * (rp / r);
+            sinThetaX = J.sin_theta_x0;
+            cosThetaX = J.cos_theta_x0;
+        }
+        const double zsign = z < 0 ? -1 : 1;
+        bx.x += zsign * bMagX * cosThetaX * cosPhi;
+        bx.y += zsign * bMagX * cosThetaX * sinPhi;
+        bx.z += bMagX * sinThetaX;
+    }
+    return add(b, bx);
+}
+
+// JF12Field::getTurbulentStrength (JF12Field.cpp:301)
+__device__ double jf12_turbulent_strength(const crp_jf12_desc &J, d3 pos) {
+    const double kpc = J.kpc;
+    if (sqrt(pos.x * pos.x + pos.y * pos.y + pos.z * pos.z) > 20 * kpc) return 0;
+    const double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+    const double phi = jf_phi(pos.x, pos.y);
+    double bDisk = 0;
+    if (r < 5 * kpc) {
+        bDisk = J.b_disk_turb5;
+    } else {
+        const double r_negx = jf_r_negx(J, r, phi);
+        for (int i = 7; i >= 0; i--)
+            if (r_negx < J.r_arms[i]) bDisk = J.b_disk_turb[i];
+        bDisk *= (5 * kpc) / r;
+    }
+    bDisk *= exp(-0.5 * jf_sq(pos.z / J.z_disk_turb));
+    const double bHalo = J.b_halo_turb * exp(-r / J.r_halo_turb) * exp(-0.5 * jf_sq(pos.z / J.z_halo_turb));
+    return sqrt(jf_sq(bDisk) + jf_sq(bHalo));
+}
+
+// JF12Field::getField (JF12Field.cpp:346): turbulent + (striated or regular).
+// Not inlined: the generic-field kernels keep their register budget.
+__device__ __noinline__ d3 jf12_field(const DevComponent &f, d3 pos) {
+    const crp_jf12_desc &J = f.jf->d;
+    d3 b = mk(0., 0., 0.);
+    if (J.use_turbulent) {
+        // Vector3f * double: the strength is rounded to float, the product is float
+        const d3 g = grid_field(f.grid, pos);
+        const float s = (float)jf12_turbulent_strength(J, pos);
+        b = add(b, mk((double)__fmul_rn((float)g.x, s), (double)__fmul_rn((float)g.y, s),
+                      (double)__fmul_rn((float)g.z, s)));
+    }
+    if (J.use_striated) {  // JF12Field.cpp:296, closestValue of the striated Grid1f
+        const double v = (double)__ldg(f.mod.values + gi_nearest_cell(f.mod, pos.x, pos.y, pos.z));
+        b = add(b, muls(jf12_regular(J, pos), 1. + J.sqrt_beta * v));
+    } else if (J.use_regular) {
+        b = add(b, jf12_regular(J, pos));
+    }
+    return b;
+}
+
 __device__ d3 component_field(const DevComponent &f, d3 position) {
     d3 pos = position;
     if (f.periodic) {  // PeriodicMagneticField::getField (MagneticField.cpp:41)
@@ -184,6 +323,11 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
     }
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, pos);
     case CRP_FIELD_UNIFORM: return mk(f.uniform[0], f.uniform[1], f.uniform[2]);
+    case CRP_FIELD_JF12: return jf12_field(f, pos);
+    case CRP_FIELD_UF23: {
+        const u3 b = uf23_field(*f.uf, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
     default: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f.b0 / r);

@@ -17,6 +17,7 @@
 #include "chain.cuh"
 #include "engine_internal.h"
 #include "grid_interp.cuh"
+#include "uf23.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -191,6 +192,139 @@ __device__ __forceinline__ f3 plane_wave_field(const DevPlaneWave &w, double x, 
     return pw_sum<false>(reinterpret_cast<const double2 *>(w.kk), w.modes32, w.n, x, y, z);
 }
 
+// ---------------------------------------------------------------- JF12Field
+// FP32 form of JF12Field::getField (JF12Field.cpp:199-346): lengths in kpc,
+// fields in muG (squares of SI positions overflow FP32), the azimuth's sine
+// and cosine as y/r and x/r, the X-field elevation's as ratios of the legs,
+// fast exponentials.  Not inlined: one compiled body, so every kernel that
+// calls it rounds the same way.
+
+__device__ __forceinline__ float jf_logistic_f(float x, float x0, float w) {
+    return __frcp_rn(1.f + __expf(__fdividef(-2.f * (fabsf(x) - x0), w)));
+}
+
+__device__ __forceinline__ float jf_r_negx_f(const DevJF12 &J, float r, float phi) {
+    const float pi = 3.14159265358979f;
+    const float inv = __frcp_rn(J.tan90mp);
+    float r_negx = r * __expf(-(phi - pi) * inv);
+    if (r_negx > J.rarms[7]) r_negx = r * __expf(-(phi + pi) * inv);
+    if (r_negx > J.rarms[7]) r_negx = r * __expf(-(phi + 3.f * pi) * inv);
+    return r_negx;
+}
+
+// regular field [muG] at (x, y, z) [kpc]
+__device__ f3 jf12_regular_f(const DevJF12 &J, float x, float y, float z) {
+    f3 b = f3mk(0.f, 0.f, 0.f);
+    const float r2 = x * x + y * y;
+    if (!(r2 + z * z < 400.f)) return b;  // d < 20 kpc
+    const float r = sqrtf(r2);
+    float cosPhi = 1.f, sinPhi = 0.f;
+    if (r > 0.f) {
+        const float ir = __frcp_rn(r);
+        cosPhi = x * ir;
+        sinPhi = y * ir;
+    }
+    if (J.d.use_disk && r > 3.f) {
+        const float lf = jf_logistic_f(z, J.hdisk, J.wdisk);
+        if (r < 5.f) {
+            const float bMag = J.bring * __fdividef(5.f, r) * (1.f - lf);
+            b.x += -bMag * sinPhi;
+            b.y += bMag * cosPhi;
+        } else {
+            const float r_negx = jf_r_negx_f(J, r, atan2f(y, x));
+            float bMag = 0.f;
+#pragma unroll
+            for (int i = 7; i >= 0; i--)
+                if (r_negx < J.rarms[i]) bMag = J.bdisk[i];
+            bMag *= __fdividef(5.f, r) * (1.f - lf);
+            b.x += bMag * (J.sinp * cosPhi - J.cosp * sinPhi);
+            b.y += bMag * (J.sinp * sinPhi + J.cosp * cosPhi);
+        }
+    }
+    const bool outside1 = r2 + z * z > 1.f;
+    const float az = fabsf(z);
+    if (J.d.use_toroidal_halo && outside1) {
+        float bMagH = __expf(__fdividef(-az, J.z0)) * jf_logistic_f(z, J.hdisk, J.wdisk);
+        if (z >= 0.f)
+            bMagH *= J.bnorth * (1.f - jf_logistic_f(r, J.rnorth, J.whalo));
+        else
+            bMagH *= J.bsouth * (1.f - jf_logistic_f(r, J.rsouth, J.whalo));
+        b.x += -bMagH * sinPhi;
+        b.y += bMagH * cosPhi;
+    }
+    if (J.d.use_x && outside1) {
+        float bMagX, sinT, cosT;
+        const float rc = J.rxc + __fdividef(az, J.tanthx0);
+        if (r < rc) {
+            const float q = __fdividef(J.rxc, rc);
+            const float rp = r * q;
+            bMagX = J.bx * __expf(__fdividef(-rp, J.rx)) * q * q;
+            if (z == 0.f) {
+                sinT = 1.f;
+                cosT = 0.f;
+            } else {
+                const float dr = r - rp, ih = rsqrtf(az * az + dr * dr);
+                sinT = az * ih;
+                cosT = dr * ih;
+            }
+        } else {
+            const float rp = r - __fdividef(az, J.tanthx0);
+            bMagX = J.bx * __expf(__fdividef(-rp, J.rx)) * __fdividef(rp, r);
+            sinT = J.sinthx0;
+            cosT = J.costhx0;
+        }
+        const float zs = z < 0.f ? -bMagX : bMagX;
+        b.x += zs * cosT * cosPhi;
+        b.y += zs * cosT * sinPhi;
+        b.z += bMagX * sinT;
+    }
+    return b;
+}
+
+// turbulent field strength [muG] (JF12Field.cpp:301)
+__device__ float jf12_turbulent_strength_f(const DevJF12 &J, float x, float y, float z) {
+    const float r2 = x * x + y * y;
+    if (r2 + z * z > 400.f) return 0.f;
+    const float r = sqrtf(r2);
+    float bDisk;
+    if (r < 5.f) {
+        bDisk = J.bdturb5;
+    } else {
+        const float r_negx = jf_r_negx_f(J, r, atan2f(y, x));
+        bDisk = 0.f;
+#pragma unroll
+        for (int i = 7; i >= 0; i--)
+            if (r_negx < J.rarms[i]) bDisk = J.bdturb[i];
+        bDisk *= __fdividef(5.f, r);
+    }
+    const float zd = __fdividef(z, J.zdturb), zh = __fdividef(z, J.zhturb);
+    bDisk *= __expf(-0.5f * zd * zd);
+    const float bHalo = J.bhturb * __expf(__fdividef(-r, J.rhturb) - 0.5f * zh * zh);
+    return sqrtf(bDisk * bDisk + bHalo * bHalo);
+}
+
+__device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double y, double z) {
+    const DevJF12 &J = *f.jf;
+    const float xs = (float)(x * J.inv_kpc), ys = (float)(y * J.inv_kpc), zs = (float)(z * J.inv_kpc);
+    const float unit = (float)J.muG;
+    f3 b = f3mk(0.f, 0.f, 0.f);
+    if (J.d.use_turbulent) {
+        const f3 g = grid_field(f.grid, x, y, z);
+        const float s = jf12_turbulent_strength_f(J, xs, ys, zs) * unit;
+        b = f3mk(g.x * s, g.y * s, g.z * s);
+    }
+    if (J.d.use_striated || J.d.use_regular) {
+        float m = unit;
+        if (J.d.use_striated)
+            m *= 1.f + J.sqrtbeta * __ldg(f.mod.values + gi_nearest_cell(f.mod, x, y, z));
+        const f3 r = jf12_regular_f(J, xs, ys, zs);
+        b.x += r.x * m;
+        b.y += r.y * m;
+        b.z += r.z * m;
+    }
+    return b;
+}
+
 // Multiply-adds here are written out (fma) so that the result does not
 // depend on how the compiler contracts the expression in each kernel that
 // inlines it: the chunked and persistent launches must agree bit for bit.
@@ -215,6 +349,11 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     }
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z, sh);
     case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
+    case CRP_FIELD_JF12: return jf12_field_f(f, x, y, z);
+    case CRP_FIELD_UF23: {  // FP64 evaluation (the poloidal halo's powers), FP32 result
+        const u3 b = uf23_field(*f.uf, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
     default: {
         double r = sqrt(fma(x, x, y * y));
         double s = f.b0 / r;

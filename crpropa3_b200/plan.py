@@ -57,6 +57,65 @@ class ModulatedGridField:
 
 
 @dataclass
+class JF12Field:
+    """JF12Field (variant JF12_VARIANT_JF12, JF12Field.cpp:8) or
+    PlanckJF12bField (JF12_VARIANT_PLANCK, :352): the regular disk, toroidal
+    halo and X fields, optionally striated (a Grid1f read by nearest value,
+    setStriatedGrid, :113) and turbulent (a Grid3f scaled by the modelled
+    strength, setTurbulentGrid, :118).  Giving a grid switches its part on, as
+    the setters do; use_striated / use_turbulent override that."""
+    variant: int = _abi.JF12_VARIANT_JF12
+    use_regular: bool = True
+    use_disk: bool = True
+    use_toroidal_halo: bool = True
+    use_x: bool = True
+    striated: Optional[ScalarGrid] = None
+    turbulent: Optional[GridField] = None
+    use_striated: Optional[bool] = None
+    use_turbulent: Optional[bool] = None
+    periodic: Optional[tuple] = None
+
+    @staticmethod
+    def defaults(variant=_abi.JF12_VARIANT_JF12) -> "_abi.JF12Desc":
+        """The constructor's parameters (crp_jf12_defaults)."""
+        d = _abi.JF12Desc()
+        _abi.check(_abi.load().crp_jf12_defaults(int(variant), C.byref(d)))
+        return d
+
+
+@dataclass
+class UF23Field:
+    """UF23Field(model) (UF23Field.cpp:59): one of the eight coherent field
+    models of Unger & Farrar 2023 (model: UF23_BASE ... UF23_NEBCOR, the
+    order of UF23Field::ModelType)."""
+    model: int = _abi.UF23_BASE
+    periodic: Optional[tuple] = None
+
+    @staticmethod
+    def defaults(model=_abi.UF23_BASE) -> "_abi.UF23Desc":
+        """The constructor's parameters (crp_uf23_defaults)."""
+        d = _abi.UF23Desc()
+        _abi.check(_abi.load().crp_uf23_defaults(int(model), C.byref(d)))
+        return d
+
+
+def jf12_random_striated(seed: int) -> ScalarGrid:
+    """JF12Field::randomStriated(seed) (JF12Field.cpp:86): a periodic 100^3
+    Grid1f at the origin with 0.1 kpc spacing, each cell round(rand()) * 2 - 1
+    from crpropa::Random seeded with seed (which must not be 0: the reference
+    then seeds from the system's entropy)."""
+    from . import units as U
+    if seed == 0:
+        raise ValueError("seed 0 is not reproducible")
+    n = 100
+    draws = np.empty(n ** 3, np.float64)
+    _abi.check(_abi.load().crp_random_draws(int(seed), 0, n ** 3, 0.0, 0.0, 0.0,
+                                            draws.ctypes.data_as(C.POINTER(C.c_double))))
+    v = (np.floor(draws + 0.5) * 2 - 1).astype(np.float32).reshape(n, n, n)
+    return ScalarGrid(v, (0.0, 0.0, 0.0), (0.1 * U.kpc,) * 3, reflective=False)
+
+
+@dataclass
 class PlaneWaveField:
     """PlaneWaveTurbulence modes (PlaneWaveTurbulence.cpp:79)."""
     xi: np.ndarray
@@ -187,6 +246,21 @@ class ChainSpec:
             c.kind = _abi.FIELD_MODULATED_GRID
             self._fill_grid(c.grid, f.grid, 3)
             self._fill_grid(c.modulation, f.modulation, 1)
+        elif isinstance(f, JF12Field):
+            c.kind = _abi.FIELD_JF12
+            c.jf12 = JF12Field.defaults(f.variant)
+            j = c.jf12
+            j.use_regular, j.use_disk = int(bool(f.use_regular)), int(bool(f.use_disk))
+            j.use_toroidal_halo, j.use_x = int(bool(f.use_toroidal_halo)), int(bool(f.use_x))
+            j.use_striated = int(bool(f.striated is not None if f.use_striated is None else f.use_striated))
+            j.use_turbulent = int(bool(f.turbulent is not None if f.use_turbulent is None else f.use_turbulent))
+            if f.striated is not None:
+                self._fill_grid(c.modulation, f.striated, 1)
+            if f.turbulent is not None:
+                self._fill_grid(c.grid, f.turbulent, 3)
+        elif isinstance(f, UF23Field):
+            c.kind = _abi.FIELD_UF23
+            c.uf23 = UF23Field.defaults(f.model)
         elif isinstance(f, PlaneWaveField):
             c.kind = _abi.FIELD_PLANE_WAVE
             w = c.plane_wave

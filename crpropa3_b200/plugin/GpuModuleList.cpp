@@ -6,7 +6,10 @@
 
 #include "crpropa/Geometry.h"
 #include "crpropa/Grid.h"
+#include "crpropa/Units.h"
+#include "crpropa/magneticField/JF12Field.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
+#include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
@@ -20,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -78,6 +82,13 @@ CRPGPU_MEMBER(PlaneX0, Plane, Vector3d, x0);                           // Geomet
 CRPGPU_MEMBER(PlaneN, Plane, Vector3d, n);
 CRPGPU_MEMBER(BoxCorner, ParaxialBox, Vector3d, corner);               // Geometry.h:77
 CRPGPU_MEMBER(BoxSize, ParaxialBox, Vector3d, size);
+typedef double UF23Pars[26];
+CRPGPU_MEMBER(UF23Model, UF23Field, const UF23Field::ModelType, fModelType);  // UF23Field.h
+CRPGPU_MEMBER(UF23MaxR2, UF23Field, const double, fMaxRadiusSquared);
+CRPGPU_MEMBER(UF23Parameters, UF23Field, UF23Pars, fParameters);
+CRPGPU_MEMBER(UF23SinPitch, UF23Field, double, fSinPitch);
+CRPGPU_MEMBER(UF23CosPitch, UF23Field, double, fCosPitch);
+CRPGPU_MEMBER(UF23TanPitch, UF23Field, double, fTanPitch);
 CRPGPU_MEMBER(TrackCenter, ObserverTracking, Vector3d, center);        // Observer.h:109
 CRPGPU_MEMBER(TrackRadius, ObserverTracking, double, radius);
 CRPGPU_MEMBER(TrackStep, ObserverTracking, double, stepSize);
@@ -233,6 +244,48 @@ struct Translation {
             fillGrid(*grid, 3, c.grid);
             text << " modulation ";
             fillGrid(*mod, 1, c.modulation);
+        } else if (typeid(*f) == typeid(JF12Field) || typeid(*f) == typeid(PlanckJF12bField)) {
+            // exact types only: the parameters are the constructor's (JF12Field.cpp:8, :352),
+            // which a subclass could change
+            JF12Field *j = const_cast<JF12Field *>(static_cast<const JF12Field *>(f));
+            const int variant = typeid(*f) == typeid(PlanckJF12bField) ? 1 : 0;
+            if (crp_jf12_defaults(variant, &c.jf12) != CRP_OK) throw Unsupported("JF12Field parameters");
+            c.kind = CRP_FIELD_JF12;
+            c.jf12.use_regular = j->isUsingRegularField();
+            c.jf12.use_disk = j->isUsingDiskField();
+            c.jf12.use_toroidal_halo = j->isUsingToroidalHaloField();
+            c.jf12.use_x = j->isUsingXField();
+            c.jf12.use_striated = j->isUsingStriatedField();
+            c.jf12.use_turbulent = j->isUsingTurbulentField();
+            text << "  field: " << (variant ? "PlanckJF12bField" : "JF12Field") << " regular "
+                 << c.jf12.use_regular << " disk " << c.jf12.use_disk << " halo " << c.jf12.use_toroidal_halo
+                 << " X " << c.jf12.use_x;
+            if (c.jf12.use_striated) {
+                ref_ptr<Grid1f> g = j->getStriatedGrid();
+                text << " striated ";
+                fillGrid(*g, 1, c.modulation);
+            }
+            if (c.jf12.use_turbulent) {
+                ref_ptr<Grid3f> g = j->getTurbulentGrid();
+                text << " turbulent ";
+                fillGrid(*g, 3, c.grid);
+            }
+        } else if (const UF23Field *u = dynamic_cast<const UF23Field *>(f)) {
+            if (typeid(*f) != typeid(UF23Field)) throw Unsupported(name_of(f) + " (a UF23Field subclass)");
+            crp_uf23_desc &d = c.uf23;
+            c.kind = CRP_FIELD_UF23;
+            d.model = (int32_t)(u->*member(UF23Model()));
+            // the 26 parameters in UF23Field::EPar order, as crp_uf23_desc lays them out
+            static_assert(offsetof(crp_uf23_desc, twisting_time) - offsetof(crp_uf23_desc, disk_b1) ==
+                              25 * sizeof(double), "crp_uf23_desc parameter block");
+            std::memcpy(&d.disk_b1, u->*member(UF23Parameters()), sizeof(UF23Pars));
+            d.sin_pitch = u->*member(UF23SinPitch());
+            d.cos_pitch = u->*member(UF23CosPitch());
+            d.tan_pitch = u->*member(UF23TanPitch());
+            d.max_radius_squared = u->*member(UF23MaxR2());
+            d.kpc = kpc;
+            d.microgauss = microgauss;
+            text << "  field: UF23Field model " << d.model;
         } else if (const PlaneWaveTurbulence *w = dynamic_cast<const PlaneWaveTurbulence *>(f)) {
             const int nm = w->*member(WavesNm());
             const std::vector<Vector3d> &xi = w->*member(WavesXi());

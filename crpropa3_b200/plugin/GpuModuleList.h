@@ -8,6 +8,8 @@
 //                 DiffusionSDE (no advection field)
 //   fields        MagneticFieldGrid over a Grid3f (trilinear, tricubic or
 //                 nearest-neighbour), ModulatedMagneticFieldGrid,
+//                 JF12Field and PlanckJF12bField (regular, striated and
+//                 turbulent parts), UF23Field (all eight models),
 //                 PeriodicMagneticField, MagneticFieldList,
 //                 UniformMagneticField, PlaneWaveTurbulence,
 //                 ToroidalMagneticField (below)

@@ -122,3 +122,42 @@ def grid_turbulence(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.
 def grid_turbulence_with_draws(n, spacing, brms, lmin, lmax, seed, draws):
     """grid_turbulence with the MT19937 draws supplied by the caller (host FFT)."""
     return grid_turbulence(n, spacing, brms, lmin, lmax, seed=seed, draws=draws)
+
+
+def turbulence_desc(kind, n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0,
+                    seed=42, helicity=0.0) -> "_abi.TurbulenceDesc":
+    d = _abi.TurbulenceDesc()
+    d.kind, d.seed, d.n, d.spacing = int(kind), int(seed), int(n), float(spacing)
+    d.brms, d.lmin, d.lmax = float(brms), float(lmin), float(lmax)
+    d.lbendover, d.sindex, d.qindex, d.helicity = float(lbendover), float(sindex), float(qindex), float(helicity)
+    return d
+
+
+def turbulence_modes(desc) -> int:
+    """Number of modes the k-space loop keeps (crp_turbulence_modes)."""
+    m = C.c_uint64()
+    _abi.check(_abi.load().crp_turbulence_modes(C.byref(desc), C.byref(m)))
+    return m.value
+
+
+def turbulence_draws(seed, kind, n_modes) -> np.ndarray:
+    """The k-space loop's Random draws (crp_turbulence_draws), (n_modes, 2 or 3)."""
+    per = 2 if kind == _abi.TURBULENCE_GRID else 3
+    out = np.zeros(per * n_modes)
+    _abi.check(_abi.load().crp_turbulence_draws(int(seed), int(kind), int(n_modes),
+                                                out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out.reshape(n_modes, per)
+
+
+def grid_turbulence_device(kind, n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0,
+                           seed=42, helicity=0.0, device="cuda"):
+    """GridTurbulence (kind TURBULENCE_GRID), SimpleGridTurbulence
+    (TURBULENCE_SIMPLE) or HelicalGridTurbulence (TURBULENCE_HELICAL)
+    generated on the device (crp_turbulence_grid): a (n, n, n, 3) float32
+    torch tensor of Grid3f values in device memory, ready for a GridField."""
+    import torch
+    out = torch.empty((n, n, n, 3), dtype=torch.float32, device=device)
+    d = turbulence_desc(kind, n, spacing, brms, lmin, lmax, lbendover, sindex, qindex, seed, helicity)
+    stream = torch.cuda.current_stream(out.device).cuda_stream
+    _abi.check(_abi.load().crp_turbulence_grid(C.byref(d), C.c_void_p(out.data_ptr()), C.c_void_p(stream)))
+    return out

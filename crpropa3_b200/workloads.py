@@ -11,6 +11,11 @@ grid_ck_64:   PropagationCK (tolerance 1e-4, 0.1-10 kpc) over a 64^3
 grid_ck_nuclei: PropagationCK (1e-4, 0.1-100 kpc) over the 256^3 grid with
               H, He-4, N-14, Fe-56 in equal parts, E^-2 over 0.1-100 EeV and a
               per-candidate maximum length uniform in 1-50 Mpc.
+jf12_backtrack: PropagationCK (1e-4, 0.1 pc-100 pc) in the JF12 regular
+              field (JF12Field defaults); antiprotons log-uniform 5-100 EeV
+              leaving the Earth's position (-8.5 kpc, 0, 0) isotropically,
+              detected by an Observer sphere of 20 kpc around the galactic
+              centre, MaximumTrajectoryLength 100 kpc (backtracking).
 Inputs are synthetic and seeded; sizes are scaled down through `n`.
 """
 from __future__ import annotations
@@ -133,4 +138,17 @@ def sde_galactic(n=10_000_000, n_modes=1024, precision=_abi.PRECISION_MIXED, see
                                        True, False)],
                        precision=precision, seed=seed)
     cands = source_candidates(n, [IDS["H"]], 1 * U.TeV, 1000 * U.TeV, -1.0, seed, position=source)
+    return spec, cands
+
+
+def jf12_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, variant=_abi.JF12_VARIANT_JF12):
+    """Backtracking through the JF12 regular field (module docstring)."""
+    spec = P.ChainSpec([P.JF12Field(variant=variant)],
+                       [P.Propagation(_abi.PROP_CK, 1e-4, 0.1 * U.pc, 100 * U.pc),
+                        P.MaxTrajectoryLength(100 * U.kpc, record=False),
+                        P.ObserverSpec(_abi.OBSERVER_SURFACE_SPHERE, (0.0, 0.0, 0.0), 20 * U.kpc,
+                                       True, False)],
+                       precision=precision, seed=seed)
+    cands = source_candidates(n, [-IDS["H"]], 5 * U.EeV, 100 * U.EeV, -1.0, seed,
+                              position=(-8.5 * U.kpc, 0.0, 0.0))
     return spec, cands

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 3u
+#define CRP_ABI_VERSION 5u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -56,8 +56,22 @@ enum crp_field_kind {
     CRP_FIELD_PLANE_WAVE = 2, /* PlaneWaveTurbulence (PlaneWaveTurbulence.cpp:231) */
     CRP_FIELD_UNIFORM = 3,    /* UniformMagneticField (MagneticField.h:109) */
     CRP_FIELD_TOROIDAL = 4,   /* B = b0 * (-y, x, 0) / r, r = sqrt(x^2 + y^2) */
-    CRP_FIELD_MODULATED_GRID = 5 /* ModulatedMagneticFieldGrid: Grid3f times a Grid1f
-                                    modulation (MagneticFieldGrid.cpp:51) */
+    CRP_FIELD_MODULATED_GRID = 5, /* ModulatedMagneticFieldGrid: Grid3f times a Grid1f
+                                     modulation (MagneticFieldGrid.cpp:51) */
+    CRP_FIELD_JF12 = 6,           /* JF12Field / PlanckJF12bField (JF12Field.cpp:8-376) */
+    CRP_FIELD_UF23 = 7            /* UF23Field (UF23Field.cpp:59-558) */
+};
+
+/* UF23Field::ModelType (UF23Field.h), same order. */
+enum crp_uf23_model {
+    CRP_UF23_BASE = 0,
+    CRP_UF23_NECL = 1,
+    CRP_UF23_EXPX = 2,
+    CRP_UF23_SPUR = 3,
+    CRP_UF23_CRE10 = 4,
+    CRP_UF23_SYNCG = 5,
+    CRP_UF23_TWISTX = 6,
+    CRP_UF23_NEBCOR = 7
 };
 
 /* Grid::setInterpolationType (Grid.h:255; enum interpolationType, Grid.h:24). */
@@ -99,6 +113,45 @@ typedef struct crp_plane_wave_desc {
 /* One summand of the field (a MagneticFieldList of these is their sum,
  * MagneticField.cpp:64).  A component may be wrapped in a
  * PeriodicMagneticField (MagneticField.cpp:41). */
+/* Parameters of the Jansson-Farrar 2012 galactic field as JF12Field holds
+ * them (JF12Field.h, set by the constructors JF12Field.cpp:8 and :352), SI
+ * units.  crp_jf12_defaults() fills them.  The striated grid (a Grid1f, one
+ * float per cell, read by nearest value, JF12Field.cpp:296) is the
+ * component's `modulation` grid and the turbulent grid (a Grid3f,
+ * JF12Field.cpp:340) its `grid`. */
+typedef struct crp_jf12_desc {
+    int32_t use_regular, use_disk, use_toroidal_halo, use_x, use_striated, use_turbulent;
+    int32_t variant;                    /* constructor the parameters come from: 0 JF12Field,
+                                           1 PlanckJF12bField */
+    int32_t _pad;
+    double kpc;                         /* the kiloparsec the model's constants are written in */
+    double sin_pitch, cos_pitch, tan90_minus_pitch;
+    double r_arms[8];
+    double b_ring, h_disk, w_disk;
+    double b_disk[8];
+    double b_north, b_south, r_north, r_south, w_halo, z0;
+    double b_x, sin_theta_x0, cos_theta_x0, tan_theta_x0, r_xc, r_x;
+    double sqrt_beta;                   /* striation */
+    double b_disk_turb[8];
+    double b_disk_turb5, z_disk_turb, b_halo_turb, r_halo_turb, z_halo_turb;
+} crp_jf12_desc;
+
+/* Parameters of a UF23Field model (UF23Field.h, UF23Field::EPar order; set by
+ * the constructor, UF23Field.cpp:59-266) in the model's own units: kpc,
+ * microgauss, radians, Myr.  crp_uf23_defaults() fills them. */
+typedef struct crp_uf23_desc {
+    int32_t model; /* crp_uf23_model */
+    int32_t _pad;
+    double disk_b1, disk_b2, disk_b3, disk_h, disk_phase1, disk_phase2, disk_phase3, disk_pitch, disk_w;
+    double poloidal_a, poloidal_b, poloidal_p, poloidal_r, poloidal_w, poloidal_z, poloidal_xi;
+    double spur_center, spur_length, spur_width, striation;
+    double toroidal_bn, toroidal_bs, toroidal_r, toroidal_w, toroidal_z, twisting_time;
+    double sin_pitch, cos_pitch, tan_pitch; /* of disk_pitch */
+    double max_radius_squared;              /* kpc^2; B = 0 beyond */
+    double kpc;                             /* position unit [m] */
+    double microgauss;                      /* field unit [T] */
+} crp_uf23_desc;
+
 typedef struct crp_field_component {
     int32_t kind;
     int32_t periodic;            /* wrap in PeriodicMagneticField */
@@ -111,8 +164,11 @@ typedef struct crp_field_component {
     double uniform[3];
     double toroidal_b0;
     /* CRP_FIELD_MODULATED_GRID: the Grid1f modulation, one float per cell
-     * (values: nx*ny*nz floats in the same order as a Grid3f's cells) */
+     * (values: nx*ny*nz floats in the same order as a Grid3f's cells);
+     * CRP_FIELD_JF12: the striated grid */
     crp_grid3f_desc modulation;
+    crp_jf12_desc jf12;
+    crp_uf23_desc uf23;
 } crp_field_component;
 
 /* ------------------------------------------------------------------------
@@ -442,9 +498,58 @@ crp_status crp_particle_charge(int32_t id, double *charge);
 
 /* n draws of crpropa::Random seeded with seed (Random.cpp): kind 0 rand(),
  * 1 randUniform(a, b), 2 randVector() (3 values per draw), 3
- * randPowerLaw(a, b, c), 6 randInt(). */
+ * randPowerLaw(a, b, c), 4 randNorm(), 6 randInt(). */
 crp_status crp_random_draws(uint32_t seed, int32_t kind, uint64_t n, double a, double b,
                             double c, double *out);
+
+/* The parameters JF12Field's constructor sets (variant 0, JF12Field.cpp:8)
+ * or PlanckJF12bField's (variant 1, JF12Field.cpp:352), with the regular
+ * field on and the striated and turbulent fields off, as constructed. */
+crp_status crp_jf12_defaults(int32_t variant, crp_jf12_desc *out);
+
+/* The parameters UF23Field(model) sets (UF23Field.cpp:59-266). */
+crp_status crp_uf23_defaults(int32_t model, crp_uf23_desc *out);
+
+/* Turbulent Grid3f generation: GridTurbulence (GridTurbulence.cpp:29-123,
+ * TurbulenceSpectrum), SimpleGridTurbulence (SimpleGridTurbulence.cpp:19-115,
+ * power law k^alpha, alpha = -sindex - 2) and HelicalGridTurbulence
+ * (HelicalGridTurbulence.cpp:19-127, helicity H). */
+enum crp_turbulence_kind {
+    CRP_TURBULENCE_GRID = 0,
+    CRP_TURBULENCE_SIMPLE = 1,
+    CRP_TURBULENCE_HELICAL = 2
+};
+
+typedef struct crp_turbulence_desc {
+    int32_t kind;       /* crp_turbulence_kind */
+    int32_t seed;       /* Random seed of the k-space draws; 0 is refused (the reference then seeds
+                           from the system's entropy) */
+    uint64_t n;         /* cells per side (GridProperties Nx = Ny = Nz) */
+    double spacing;     /* cell size [m] */
+    double brms, lmin, lmax; /* [T], [m], [m] */
+    double lbendover, sindex, qindex; /* TurbulenceSpectrum (GridTurbulence); Simple and Helical
+                                         use sindex only */
+    double helicity;    /* HelicalGridTurbulence H, in [-1, 1] */
+} crp_turbulence_desc;
+
+/* The Random draws of the k-space loop for n_modes kept modes, in loop
+ * order: GRID 2 per mode (rand theta, rand phase), SIMPLE 3 (rand theta,
+ * randNorm amplitude, rand phase), HELICAL 3 (randNorm amplitude, rand
+ * theta+, rand theta-). */
+crp_status crp_turbulence_draws(uint32_t seed, int32_t kind, uint64_t n_modes, double *out);
+
+/* Number of modes kept by the k-space loop (kMin <= |k| <= kMax). */
+crp_status crp_turbulence_modes(const crp_turbulence_desc *d, uint64_t *n_modes);
+
+/* A turbulent Grid3f generated on the device: the k-space amplitudes from
+ * the reference's draws (host MT19937, crp_turbulence_draws), the inverse
+ * real FFT (cuFFT, unnormalised as FFTW's) and the normalisation to brms
+ * (scaleGrid(grid, Brms / rmsFieldStrength(grid)), GridTools.cpp:16, :59).
+ * out: DEVICE memory for n^3 Vector3f cells (12 B each, Grid.h:338 order).
+ * Allocates and frees its own scratch (k-space and FFT buffers).  FFTW is
+ * not the FFT, so values equal the reference's in distribution, not bit for
+ * bit. */
+crp_status crp_turbulence_grid(const crp_turbulence_desc *d, float *out_device, void *stream);
 
 /* Wave modes of PlaneWaveTurbulence(TurbulenceSpectrum(brms, lmin, lmax,
  * lbendover, sindex, qindex), nm, seed) (PlaneWaveTurbulence.cpp:79-229),

@@ -28,6 +28,7 @@
  */
 #include "crp_gpu.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -480,6 +481,284 @@ static v3 plane_wave_field(const crp_plane_wave_desc *p, v3 pos) {
     return B;
 }
 
+/* ---------------------------------------------------------------- JF12Field
+ * JF12Field::getField and its parts (JF12Field.cpp:195-346), same operation
+ * order, glibc's exp, sin, cos, atan2 and pow as the reference calls them. */
+
+/* JF12Field::logisticFunction (JF12Field.cpp:195) */
+static double jf_logistic(double x, double x0, double w) { return 1. / (1. + exp(-2. * (fabs(x) - x0) / w)); }
+
+/* Vector3::getPhi (Vector3.h:136) */
+static double jf_phi(double x, double y) {
+    if ((fabs(x) < DBL_MIN) && (fabs(y) < DBL_MIN)) return 0.0;
+    return atan2(y, x);
+}
+
+/* arm radius at the negative x axis (JF12Field.cpp:228-233, :315-320) */
+static double jf_r_negx(const crp_jf12_desc *J, double r, double phi) {
+    double r_negx = r * exp(-(phi - M_PI) / J->tan90_minus_pitch);
+    if (r_negx > J->r_arms[7]) r_negx = r * exp(-(phi + M_PI) / J->tan90_minus_pitch);
+    if (r_negx > J->r_arms[7]) r_negx = r * exp(-(phi + 3 * M_PI) / J->tan90_minus_pitch);
+    return r_negx;
+}
+
+/* getRegularField (JF12Field.cpp:199): getDiskField (:216) + getToroidalHaloField
+ * (:248) + getXField (:267) */
+static v3 jf12_regular(const crp_jf12_desc *J, v3 pos) {
+    v3 b = mk(0, 0, 0);
+    double kpc = J->kpc;
+    double d = sqrt(pos.x * pos.x + pos.y * pos.y + pos.z * pos.z);
+    if (!(d < 20 * kpc)) return b;
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y), z = pos.z;
+    double phi = jf_phi(pos.x, pos.y);
+    double sinPhi = sin(phi), cosPhi = cos(phi);
+    v3 bd = mk(0, 0, 0);
+    if (J->use_disk) {
+        double lfDisk = jf_logistic(z, J->h_disk, J->w_disk);
+        if (r > 3 * kpc) {
+            double bMag = 0;
+            if (r < 5 * kpc) {
+                bMag = J->b_ring * (5 * kpc / r) * (1 - lfDisk);
+                bd.x += -bMag * sinPhi;
+                bd.y += bMag * cosPhi;
+            } else {
+                double r_negx = jf_r_negx(J, r, phi);
+                for (int i = 7; i >= 0; i--)
+                    if (r_negx < J->r_arms[i]) bMag = J->b_disk[i];
+                bMag *= (5 * kpc / r) * (1 - lfDisk);
+                bd.x += bMag * (J->sin_pitch * cosPhi - J->cos_pitch * sinPhi);
+                bd.y += bMag * (J->sin_pitch * sinPhi + J->cos_pitch * cosPhi);
+            }
+        }
+    }
+    b = add(b, bd);
+    int outside1 = r * r + z * z > 1 * kpc * kpc;
+    v3 bh = mk(0, 0, 0);
+    if (J->use_toroidal_halo && outside1) {
+        double lfDisk = jf_logistic(z, J->h_disk, J->w_disk);
+        double bMagH = exp(-fabs(z) / J->z0) * lfDisk;
+        if (z >= 0)
+            bMagH *= J->b_north * (1 - jf_logistic(r, J->r_north, J->w_halo));
+        else
+            bMagH *= J->b_south * (1 - jf_logistic(r, J->r_south, J->w_halo));
+        bh.x += -bMagH * sinPhi;
+        bh.y += bMagH * cosPhi;
+    }
+    b = add(b, bh);
+    v3 bx = mk(0, 0, 0);
+    if (J->use_x && outside1) {
+        double bMagX, sinThetaX, cosThetaX, rp;
+        double rc = J->r_xc + fabs(z) / J->tan_theta_x0;
+        if (r < rc) {
+            rp = r * J->r_xc / rc;
+            bMagX = J->b_x * exp(-1 * rp / J->r_x) * pow(J->r_xc / rc, 2.);
+            double thetaX = atan2(fabs(z), (r - rp));
+            if (z == 0) thetaX = M_PI / 2.;
+            sinThetaX = sin(thetaX);
+            cosThetaX = cos(thetaX);
+        } else {
+            rp = r - fabs(z) / J->tan_theta_x0;
+            bMagX = J->b_x * exp(-rp / J->r_x) * (rp / r);
+            sinThetaX = J->sin_theta_x0;
+            cosThetaX = J->cos_theta_x0;
+        }
+        double zsign = z < 0 ? -1 : 1;
+        bx.x += zsign * bMagX * cosThetaX * cosPhi;
+        bx.y += zsign * bMagX * cosThetaX * sinPhi;
+        bx.z += bMagX * sinThetaX;
+    }
+    return add(b, bx);
+}
+
+/* getTurbulentStrength (JF12Field.cpp:301) */
+static double jf12_turbulent_strength(const crp_jf12_desc *J, v3 pos) {
+    double kpc = J->kpc;
+    if (sqrt(pos.x * pos.x + pos.y * pos.y + pos.z * pos.z) > 20 * kpc) return 0;
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+    double phi = jf_phi(pos.x, pos.y);
+    double bDisk = 0;
+    if (r < 5 * kpc) {
+        bDisk = J->b_disk_turb5;
+    } else {
+        double r_negx = jf_r_negx(J, r, phi);
+        for (int i = 7; i >= 0; i--)
+            if (r_negx < J->r_arms[i]) bDisk = J->b_disk_turb[i];
+        bDisk *= (5 * kpc) / r;
+    }
+    bDisk *= exp(-0.5 * pow(pos.z / J->z_disk_turb, 2));
+    double bHalo = J->b_halo_turb * exp(-r / J->r_halo_turb) * exp(-0.5 * pow(pos.z / J->z_halo_turb, 2));
+    return sqrt(pow(bDisk, 2) + pow(bHalo, 2));
+}
+
+/* getField (JF12Field.cpp:346): turbulent + (striated or regular); the
+ * turbulent part is Vector3f * double, a float product (Vector3.h:305). */
+static v3 jf12_field(const crp_field_component *f, v3 pos) {
+    const crp_jf12_desc *J = &f->jf12;
+    v3 b = mk(0, 0, 0);
+    if (J->use_turbulent) {
+        v3 g = grid_field(&f->grid, pos);
+        float s = (float)jf12_turbulent_strength(J, pos);
+        float gx = (float)g.x * s, gy = (float)g.y * s, gz = (float)g.z * s;
+        b = add(b, mk(gx, gy, gz));
+    }
+    if (J->use_striated) { /* JF12Field.cpp:296 */
+        double v = f->modulation.values[grid_nearest_cell(&f->modulation, pos)];
+        b = add(b, muls(jf12_regular(J, pos), 1. + J->sqrt_beta * v));
+    } else if (J->use_regular) {
+        b = add(b, jf12_regular(J, pos));
+    }
+    return b;
+}
+
+/* ---------------------------------------------------------------- UF23Field
+ * UF23Field::getField and its parts (UF23Field.cpp:269-558) in the model's
+ * units (kpc, microgauss), same operation order, glibc's libm. */
+
+static const double UF23_TWO_PI = 2 * 3.1415926535897932384626;
+
+/* uf23::CylToCart (UF23Field.cpp:12) */
+static v3 uf_cyl_to_cart(double v0, double v1, double v2, double cosPhi, double sinPhi) {
+    return mk(v0 * cosPhi - v1 * sinPhi, v0 * sinPhi + v1 * cosPhi, v2);
+}
+
+/* uf23::Sigmoid (UF23Field.cpp:29) */
+static double uf_sigmoid(double x, double x0, double w) { return 1 / (1 + exp(-(x - x0) / w)); }
+
+/* uf23::DeltaPhi (UF23Field.cpp:37) */
+static double uf_delta_phi(double phi0, double phi1) { return acos(cos(phi1) * cos(phi0) + sin(phi1) * sin(phi0)); }
+
+/* getSpiralField (UF23Field.cpp:510) */
+static v3 uf_spiral(const crp_uf23_desc *U, double x, double y, double z) {
+    const double rRef = 5, rInner = 5, wInner = 0.5, rOuter = 20, wOuter = 0.5;
+    double r2 = x * x + y * y;
+    if (r2 == 0) return mk(0, 0, 0);
+    double r = sqrt(r2);
+    double phi = atan2(y, x);
+    double hdz = 1 - uf_sigmoid(fabs(z), U->disk_h, U->disk_w);
+    double rFacI = uf_sigmoid(r, rInner, wInner);
+    double rFacO = 1 - uf_sigmoid(r, rOuter, wOuter);
+    double rFac = r > 1e-5 * (1e-3 * 1) ? (1 - exp(-r * r)) / r : r * (1 - r2 / 2);
+    double gdrTimesRrefByR = rRef * rFac * rFacO * rFacI;
+    double phi0 = phi - log(r / rRef) / U->tan_pitch;
+    double b = U->disk_b1 * cos(1 * (phi0 - U->disk_phase1)) + U->disk_b2 * cos(2 * (phi0 - U->disk_phase2)) +
+               U->disk_b3 * cos(3 * (phi0 - U->disk_phase3));
+    double fac = hdz * gdrTimesRrefByR;
+    return uf_cyl_to_cart(b * fac * U->sin_pitch, b * fac * U->cos_pitch, 0, x / r, y / r);
+}
+
+/* getSpurField (UF23Field.cpp:453) */
+static v3 uf_spur(const crp_uf23_desc *U, double x, double y, double z) {
+    const double rRef = 8.2;
+    double r2 = x * x + y * y;
+    double r = sqrt(r2);
+    if (r < DBL_MIN) return mk(0, 0, 0);
+    double phi = atan2(y, x);
+    if (phi < 0) phi += UF23_TWO_PI;
+    double phiRef = U->disk_phase1;
+    int iBest = -2;
+    double bestDist = -1;
+    for (int i = -1; i <= 1; ++i) {
+        double pphi = phi - phiRef + i * UF23_TWO_PI;
+        double rr = rRef * exp(pphi * U->tan_pitch);
+        if (bestDist < 0 || fabs(r - rr) < bestDist) {
+            bestDist = fabs(r - rr);
+            iBest = i;
+        }
+    }
+    if (iBest != 0) return mk(0, 0, 0);
+    double phi0 = phi - log(r / rRef) / U->tan_pitch;
+    double deltaPhi0 = uf_delta_phi(phiRef, phi0);
+    double delta = deltaPhi0 / U->spur_width;
+    double B = U->disk_b1 * exp(-0.5 * pow(delta, 2));
+    double wS = 5 * (3.1415926535897932384626 / 180.);
+    double deltaPhiC = uf_delta_phi(U->spur_center, phi);
+    double gS = 1 - uf_sigmoid(fabs(deltaPhiC), U->spur_length, wS);
+    double hd = 1 - uf_sigmoid(fabs(z), U->disk_h, U->disk_w);
+    double bS = rRef / r * B * hd * gS;
+    return uf_cyl_to_cart(bS * U->sin_pitch, bS * U->cos_pitch, 0, x / r, y / r);
+}
+
+/* getToroidalHaloField (UF23Field.cpp:361) */
+static v3 uf_toroidal(const crp_uf23_desc *U, double x, double y, double z) {
+    double r2 = x * x + y * y;
+    double r = sqrt(r2);
+    double absZ = fabs(z);
+    double b0 = z >= 0 ? U->toroidal_bn : U->toroidal_bs;
+    double sigmoidR = uf_sigmoid(r, U->toroidal_r, U->toroidal_w);
+    double sigmoidZ = uf_sigmoid(absZ, U->disk_h, U->disk_w);
+    double bPhi = b0 * (1. - sigmoidR) * sigmoidZ * exp(-absZ / U->toroidal_z);
+    double cosPhi = r > DBL_MIN ? x / r : 1;
+    double sinPhi = r > DBL_MIN ? y / r : 0;
+    return uf_cyl_to_cart(0, bPhi, 0, cosPhi, sinPhi);
+}
+
+/* getPoloidalHaloField (UF23Field.cpp:385) */
+static v3 uf_poloidal(const crp_uf23_desc *U, double x, double y, double z) {
+    double r2 = x * x + y * y;
+    double r = sqrt(r2);
+    double P = U->poloidal_p;
+    double c = pow(U->poloidal_a / U->poloidal_z, P);
+    double a0p = pow(U->poloidal_a, P);
+    double rp = pow(r, P);
+    double abszp = pow(fabs(z), P);
+    double cabszp = c * abszp;
+    double t0 = a0p + cabszp - rp;
+    double t1 = sqrt(pow(t0, 2) + 4 * a0p * rp);
+    double ap = 2 * a0p * rp / (t1 + t0);
+    double a = 0;
+    if (ap < 0) {
+        if (r > DBL_MIN) a = NAN; /* the reference throws: "this should never happen" */
+    } else {
+        a = pow(ap, 1 / P);
+    }
+    double radialDependence = U->model == CRP_UF23_EXPX ? exp(-a / U->poloidal_r)
+                                                        : 1 - uf_sigmoid(a, U->poloidal_r, U->poloidal_w);
+    double Bzz = U->poloidal_b * radialDependence;
+    double rOverA = 1 / pow(2 * a0p / (t1 + t0), 1 / P);
+    double signZ = z < 0 ? -1 : 1;
+    double Br = Bzz * c * a / rOverA * signZ * pow(fabs(z), P - 1) / t1;
+    double Bz = Bzz * pow(rOverA, P - 2) * (ap + a0p) / t1;
+    if (r < DBL_MIN) return mk(0, 0, Bz);
+    return uf_cyl_to_cart(Br, 0, Bz, x / r, y / r);
+}
+
+/* getTwistedHaloField (UF23Field.cpp:318) */
+static v3 uf_twisted(const crp_uf23_desc *U, double x, double y, double z) {
+    double r = sqrt(x * x + y * y);
+    double cosPhi = r > DBL_MIN ? x / r : 1;
+    double sinPhi = r > DBL_MIN ? y / r : 0;
+    v3 bX = uf_poloidal(U, x, y, z);
+    /* uf23::CartToCyl (UF23Field.cpp:20) */
+    double bR = bX.x * cosPhi + bX.y * sinPhi;
+    double bZ = bX.z;
+    double bPhi = 0;
+    if (U->twisting_time != 0 && r != 0) {
+        const double kilometer = 1 / 3.0856775807e+16;
+        const double second = 1 / (1e6 * 60 * 60 * 24 * 365.25);
+        const double v0 = -240 * kilometer / second;
+        const double r0 = 1.6, z0 = 10;
+        double fr = 1 - exp(-r / r0);
+        double t0 = exp(2 * fabs(z) / z0);
+        double gz = 2 / (1 + t0);
+        double signZ = z < 0 ? -1 : 1;
+        double deltaZ = -signZ * v0 * fr / z0 * t0 * pow(gz, 2);
+        double deltaR = v0 * ((1 - fr) / r0 - fr / r) * gz;
+        bPhi = (bZ * deltaZ + bR * deltaR) * U->twisting_time;
+    }
+    return uf_cyl_to_cart(bR, bPhi, bZ, cosPhi, sinPhi);
+}
+
+/* UF23Field::getField (UF23Field.cpp:269) and operator() (:277) */
+static v3 uf23_field(const crp_uf23_desc *U, v3 position) {
+    double x = position.x / U->kpc * 1, y = position.y / U->kpc * 1, z = position.z / U->kpc * 1;
+    if (x * x + y * y + z * z > U->max_radius_squared) return mk(0, 0, 0);
+    v3 disk = U->model == CRP_UF23_SPUR ? uf_spur(U, x, y, z) : uf_spiral(U, x, y, z);
+    v3 halo = U->model == CRP_UF23_TWISTX ? uf_twisted(U, x, y, z)
+                                          : add(uf_toroidal(U, x, y, z), uf_poloidal(U, x, y, z));
+    v3 b = divs(add(disk, halo), 1);
+    return muls(divs(b, 1), U->microgauss);
+}
+
 static v3 component_field(const crp_field_component *f, v3 position) {
     v3 pos = position;
     if (f->periodic) { /* MagneticField.cpp:41 */
@@ -502,6 +781,8 @@ static v3 component_field(const crp_field_component *f, v3 position) {
     }
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(&f->plane_wave, pos);
     case CRP_FIELD_UNIFORM: return mk(f->uniform[0], f->uniform[1], f->uniform[2]);
+    case CRP_FIELD_JF12: return jf12_field(f, pos);
+    case CRP_FIELD_UF23: return uf23_field(&f->uf23, pos);
     case CRP_FIELD_TOROIDAL: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f->toroidal_b0 / r);

@@ -218,6 +218,52 @@ class Reference:
         self._check(self.lib.ref_random(seed, kind, n, a, b, c, _dptr(out)))
         return out
 
+    def dump_grid(self, values, path, c=1.0, txt=False, save_prop=False, origin=(0, 0, 0), spacing=(1, 1, 1),
+                  reflective=False, clip=False, interp=0):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        width = 3 if v.ndim == 4 else 1
+        o, sp = np.asarray(origin, np.float64), np.asarray(spacing, np.float64)
+        self.lib.ref_dump_grid.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
+                                           C.c_char_p, C.c_double, C.c_int, C.c_int, _dp, _dp, C.c_int, C.c_int,
+                                           C.c_int]
+        self._check(self.lib.ref_dump_grid(v.ctypes.data_as(C.POINTER(C.c_float)), width, *v.shape[:3],
+                                           str(path).encode(), c, int(txt), int(save_prop), _dptr(o), _dptr(sp),
+                                           int(reflective), int(clip), int(interp)))
+
+    def load_grid(self, shape, path, c=1.0, vector=True, txt=False):
+        out = np.zeros(tuple(shape) + ((3,) if vector else ()), np.float32)
+        self.lib.ref_load_grid.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
+                                           C.c_char_p, C.c_double, C.c_int]
+        self._check(self.lib.ref_load_grid(out.ctypes.data_as(C.POINTER(C.c_float)), 3 if vector else 1,
+                                           *shape, str(path).encode(), c, int(txt)))
+        return out
+
+    def load_grid_props(self, path, c=1.0, vector=True, capacity=1 << 20):
+        shape, o, sp = (C.c_uint64 * 3)(), np.zeros(3), np.zeros(3)
+        flags = (C.c_int * 3)()
+        vals = np.zeros(capacity, np.float32)
+        self.lib.ref_load_grid_props.argtypes = [C.c_char_p, C.c_int, C.c_double, C.POINTER(C.c_uint64), _dp,
+                                                 _dp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_uint64]
+        self._check(self.lib.ref_load_grid_props(str(path).encode(), 3 if vector else 1, c, shape, _dptr(o),
+                                                 _dptr(sp), flags, vals.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 capacity))
+        shp = tuple(int(x) for x in shape)
+        n = int(np.prod(shp)) * (3 if vector else 1)
+        return shp, o, sp, tuple(flags), vals[:n].reshape(shp + ((3,) if vector else ()))
+
+    def turbulence_draws(self, seed, kind, n):
+        per = 2 if kind == 0 else 3
+        out = np.zeros(per * n)
+        self.lib.ref_turbulence_draws.argtypes = [C.c_uint32, C.c_int, C.c_uint64, _dp]
+        self._check(self.lib.ref_turbulence_draws(seed, kind, n, _dptr(out)))
+        return out.reshape(n, per)
+
+    def jf12_random_striated(self, seed):
+        out = np.zeros(100 ** 3, np.float32)
+        self.lib.ref_jf12_random_striated.argtypes = [C.c_int, C.POINTER(C.c_float)]
+        self._check(self.lib.ref_jf12_random_striated(int(seed), out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.reshape(100, 100, 100)
+
     def sample_source(self, seed, n, position, ids, abundances, emin, emax, index):
         ids = np.asarray(ids, dtype=np.int32)
         ab = np.asarray(abundances if abundances is not None else np.ones(len(ids)), dtype=np.float64)

@@ -12,7 +12,8 @@
  * (src/ModuleList.cpp.in:97 run(candidate_vector) with OpenMP
  * schedule(static,100)), PropagationCK, PropagationBP, DiffusionSDE,
  * MagneticFieldGrid (trilinear, tricubic and nearest-neighbour Grid3f),
- * ModulatedMagneticFieldGrid, PeriodicMagneticField, MagneticFieldList,
+ * ModulatedMagneticFieldGrid, JF12Field, PlanckJF12bField, UF23Field,
+ * PeriodicMagneticField, MagneticFieldList,
  * UniformMagneticField, PlaneWaveTurbulence, MaximumTrajectoryLength,
  * Observer, ObserverSurface(Sphere), ObserverDetectAll, TextOutput, Source
  * features and Random.
@@ -31,12 +32,15 @@
 
 #include "crpropa/Candidate.h"
 #include "crpropa/Grid.h"
+#include "crpropa/GridTools.h"
 #include "crpropa/ModuleList.h"
 #include "crpropa/Random.h"
 #include "crpropa/Source.h"
 #include "crpropa/Units.h"
 #include "crpropa/magneticField/MagneticField.h"
+#include "crpropa/magneticField/JF12Field.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
+#include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/magneticField/turbulentField/TurbulentField.h"
 #include "crpropa/module/Boundary.h"
@@ -165,6 +169,23 @@ static ref_ptr<MagneticField> build_component(const crp_field_component &f, Buil
         // the constructor resets both flags (MagneticFieldGrid.cpp:22-23)
         mm->setReflective(f.grid.reflective != 0, f.modulation.reflective != 0);
         m = mm;
+    } else if (f.kind == CRP_FIELD_JF12) {
+        // the constructors set the parameters (JF12Field.cpp:8, :352); the
+        // descriptor's flags and grids go through the public setters
+        const crp_jf12_desc &j = f.jf12;
+        if (j.kpc == 0) throw std::runtime_error("ref_shim: JF12 parameters not set");
+        ref_ptr<JF12Field> jf = j.variant == 1 ? new PlanckJF12bField() : new JF12Field();
+        jf->setUseRegularField(j.use_regular != 0);
+        jf->setUseDiskField(j.use_disk != 0);
+        jf->setUseToroidalHaloField(j.use_toroidal_halo != 0);
+        jf->setUseXField(j.use_x != 0);
+        if (f.modulation.values) jf->setStriatedGrid(make_grid<float>(f.modulation, 1, b));
+        if (f.grid.values) jf->setTurbulentGrid(make_grid<Vector3f>(f.grid, 3, b));
+        jf->setUseStriatedField(j.use_striated != 0);
+        jf->setUseTurbulentField(j.use_turbulent != 0);
+        m = jf;
+    } else if (f.kind == CRP_FIELD_UF23) {
+        m = new UF23Field((UF23Field::ModelType)f.uf23.model);
     } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
         const crp_plane_wave_desc &p = f.plane_wave;
         TurbulenceSpectrum *spec = new TurbulenceSpectrum(p.brms, p.lmin, p.lmax, p.lbendover,
@@ -450,6 +471,131 @@ int ref_random(uint32_t seed, int kind, uint64_t n, double a, double b, double c
         default: g_error = "ref_random: unknown kind"; return 1;
         }
     }
+    return 0;
+}
+
+/* The reference's grid files (GridTools.cpp:134-482): dumpGrid /
+ * dumpGridToTxt of a Grid3f (width 3) or Grid1f (width 1) holding `values`,
+ * and loadGrid / loadGridFromTxt into one of the given shape. */
+static crp_grid3f_desc io_desc(const float *values, uint64_t nx, uint64_t ny, uint64_t nz, const double *origin,
+                               const double *spacing, int reflective, int clip, int interp) {
+    crp_grid3f_desc g;
+    std::memset(&g, 0, sizeof(g));
+    g.values = values;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    for (int a = 0; a < 3; a++) {
+        g.origin[a] = origin ? origin[a] : 0.0;
+        g.spacing[a] = spacing ? spacing[a] : 1.0;
+    }
+    g.reflective = reflective;
+    g.clip_volume = clip;
+    g.interpolation = interp;
+    return g;
+}
+
+int ref_dump_grid(const float *values, int width, uint64_t nx, uint64_t ny, uint64_t nz, const char *path,
+                  double c, int txt, int save_prop, const double *origin, const double *spacing, int reflective,
+                  int clip, int interp) {
+    try {
+        Built b;
+        crp_grid3f_desc g = io_desc(values, nx, ny, nz, origin, spacing, reflective, clip, interp);
+        if (width == 3) {
+            ref_ptr<Grid3f> grid = make_grid<Vector3f>(g, 3, b);
+            if (txt) dumpGridToTxt(grid, path, c, save_prop != 0);
+            else dumpGrid(grid, path, c);
+        } else {
+            ref_ptr<Grid1f> grid = make_grid<float>(g, 1, b);
+            if (txt) dumpGridToTxt(grid, path, c, save_prop != 0);
+            else dumpGrid(grid, path, c);
+        }
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+int ref_load_grid(float *values, int width, uint64_t nx, uint64_t ny, uint64_t nz, const char *path, double c,
+                  int txt) {
+    try {
+        size_t cells = nx * ny * nz;
+        if (width == 3) {
+            ref_ptr<Grid3f> grid = new Grid3f(Vector3d(0.), nx, ny, nz, Vector3d(1.));
+            if (txt) loadGridFromTxt(grid, path, c);
+            else loadGrid(grid, path, c);
+            std::memcpy(values, &grid->getGrid()[0], sizeof(float) * 3 * cells);
+        } else {
+            ref_ptr<Grid1f> grid = new Grid1f(Vector3d(0.), nx, ny, nz, Vector3d(1.));
+            if (txt) loadGridFromTxt(grid, path, c);
+            else loadGrid(grid, path, c);
+            std::memcpy(values, &grid->getGrid()[0], sizeof(float) * cells);
+        }
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/* loadGrid3fFromTxt / loadGrid1fFromTxt (GridTools.cpp:262, :354): the
+ * properties read from the header (shape, origin, spacing, flags), and the
+ * values into `values` if it is large enough (capacity in floats). */
+int ref_load_grid_props(const char *path, int width, double c, uint64_t *shape, double *origin, double *spacing,
+                        int *flags, float *values, uint64_t capacity) {
+    try {
+        if (width == 3) {
+            ref_ptr<Grid3f> g = loadGrid3fFromTxt(path, c);
+            shape[0] = g->getNx(); shape[1] = g->getNy(); shape[2] = g->getNz();
+            for (int a = 0; a < 3; a++) { origin[a] = g->getOrigin().data[a]; spacing[a] = g->getSpacing().data[a]; }
+            flags[0] = g->isReflective(); flags[1] = g->getClipVolume(); flags[2] = g->getInterpolationType();
+            size_t n = 3 * g->getGrid().size();
+            if (n <= capacity) std::memcpy(values, &g->getGrid()[0], sizeof(float) * n);
+        } else {
+            ref_ptr<Grid1f> g = loadGrid1fFromTxt(path, c);
+            shape[0] = g->getNx(); shape[1] = g->getNy(); shape[2] = g->getNz();
+            for (int a = 0; a < 3; a++) { origin[a] = g->getOrigin().data[a]; spacing[a] = g->getSpacing().data[a]; }
+            flags[0] = g->isReflective(); flags[1] = g->getClipVolume(); flags[2] = g->getInterpolationType();
+            size_t n = g->getGrid().size();
+            if (n <= capacity) std::memcpy(values, &g->getGrid()[0], sizeof(float) * n);
+        }
+        return 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/* The draws of the turbulence k-space loops from crpropa::Random seeded
+ * with `seed`, for n modes: kind 0 (GridTurbulence.cpp:97, :104) rand,
+ * rand; kind 1 (SimpleGridTurbulence.cpp:88-93) rand, randNorm, rand; kind 2
+ * (HelicalGridTurbulence.cpp:88-92) randNorm, rand, rand. */
+int ref_turbulence_draws(uint32_t seed, int kind, uint64_t n, double *out) {
+    Random r;
+    r.seed(seed);
+    for (uint64_t i = 0; i < n; i++) {
+        if (kind == 0) {
+            out[2 * i] = r.rand();
+            out[2 * i + 1] = r.rand();
+        } else if (kind == 1) {
+            out[3 * i] = r.rand();
+            out[3 * i + 1] = r.randNorm();
+            out[3 * i + 2] = r.rand();
+        } else {
+            out[3 * i] = r.randNorm();
+            out[3 * i + 1] = r.rand();
+            out[3 * i + 2] = r.rand();
+        }
+    }
+    return 0;
+}
+
+/* The striated grid of JF12Field::randomStriated(seed) (JF12Field.cpp:86):
+ * 100^3 floats in cell order. */
+int ref_jf12_random_striated(int seed, float *out) {
+    ref_ptr<JF12Field> jf = new JF12Field();
+    jf->randomStriated(seed);
+    std::vector<float> &v = jf->getStriatedGrid()->getGrid();
+    std::memcpy(out, &v[0], sizeof(float) * v.size());
     return 0;
 }
 
