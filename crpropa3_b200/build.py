@@ -37,7 +37,7 @@ SOURCES = {
     "host_tools.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }
 PEAKS_SOURCES = {"peaks.cu": []}
-LINK_LIBS = ["-lcufft"]
+LINK_LIBS = ["-lcufft", "-lz"]
 
 
 def _nvcc():

@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include <zlib.h>
+
 #include "crp_gpu.h"
 
 namespace crp {
@@ -496,20 +498,35 @@ crp_status crp_text_output_write(const char *path, int32_t append, int32_t heade
                                  const crp_output_desc *desc, uint64_t n,
                                  const crp_output_rows *rows) {
     if (!path || !desc || (n && !rows)) return host_fail(CRP_ERR_INVALID_ARGUMENT, "NULL argument");
-    FILE *f = fopen(path, append ? "ab" : "wb");
-    if (!f) return host_fail(CRP_ERR_INVALID_ARGUMENT, "Cannot create file");
+    // a name ending in ".gz" writes gzip (TextOutput.cpp:41, :388: zstream over zlib); appending
+    // adds a gzip member, which readers concatenate
+    const size_t len = std::strlen(path);
+    const bool gz = len >= 3 && std::strcmp(path + len - 3, ".gz") == 0;
+    FILE *f = nullptr;
+    gzFile g = nullptr;
+    if (gz) g = gzopen(path, append ? "ab" : "wb");
+    else f = fopen(path, append ? "ab" : "wb");
+    if (!f && !g) return host_fail(CRP_ERR_INVALID_ARGUMENT, "Cannot create file");
+    bool ok = true;
+    auto flush = [&](const std::string &o) {
+        if (o.empty()) return;
+        if (gz) ok = ok && gzwrite(g, o.data(), (unsigned)o.size()) == (int)o.size();
+        else ok = ok && fwrite(o.data(), 1, o.size(), f) == o.size();
+    };
     std::string out;
     out.reserve(256 * (size_t)(n < 4096 ? n + 1 : 4096));
     if (header) format_header(desc, out);
     for (uint64_t i = 0; i < n; i++) {
         format_row(desc, rows, i, out);
         if (out.size() > (1u << 22)) {
-            fwrite(out.data(), 1, out.size(), f);
+            flush(out);
             out.clear();
         }
     }
-    fwrite(out.data(), 1, out.size(), f);
-    fclose(f);
+    flush(out);
+    if (gz) ok = gzclose(g) == Z_OK && ok;
+    else ok = fclose(f) == 0 && ok;
+    if (!ok) return host_fail(CRP_ERR_INVALID_ARGUMENT, "write to the output file failed");
     return CRP_OK;
 }
 

@@ -263,7 +263,10 @@ __device__ f3 jf12_regular_f(const DevJF12 &J, float x, float y, float z) {
                 sinT = 1.f;
                 cosT = 0.f;
             } else {
-                const float dr = r - rp, ih = rsqrtf(az * az + dr * dr);
+                // r - rp = r (rc - rxc) / rc = r (|z| / tan thetaX0) / rc, without the
+                // cancellation of r - rp near the plane
+                const float dr = __fdividef(r * __fdividef(az, J.tanthx0), rc);
+                const float ih = rsqrtf(az * az + dr * dr);
                 sinT = az * ih;
                 cosT = dr * ih;
             }

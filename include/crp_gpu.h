@@ -607,7 +607,8 @@ typedef struct crp_output_rows {
 } crp_output_rows;
 
 /* TextOutput (TextOutput.cpp:55 printHeader, :166 process): write (or
- * append) n lines, optionally preceded by the header. */
+ * append) n lines, optionally preceded by the header; a path ending in
+ * ".gz" is written gzip-compressed (TextOutput.cpp:41, :388). */
 crp_status crp_text_output_write(const char *path, int32_t append, int32_t header,
                                  const crp_output_desc *desc, uint64_t n,
                                  const crp_output_rows *rows);

@@ -20,6 +20,7 @@
 
 #include <stdint.h>
 
+#include <string>
 #include <vector>
 
 namespace crp_ref {
@@ -33,12 +34,23 @@ public:
     uint64_t total() const;
 };
 
+/* Output type that asks build_chain for a ParticleCollector (clone on) as
+ * the observers' detection action instead of a TextOutput; finish_outputs()
+ * dumps the first one to the output path (ParticleCollector::dump,
+ * ParticleCollector.cpp:62: TextOutput Everything). */
+const int kCollectorOutput = 100;
+
 struct Built {
     crpropa::ref_ptr<crpropa::ModuleList> sim;
     crpropa::ref_ptr<crpropa::MagneticField> field;
     std::vector<crpropa::ref_ptr<crpropa::Referenced> > keep;  // spectra, grids
     crpropa::ref_ptr<StepCounter> counter;
+    std::vector<crpropa::ref_ptr<crpropa::Module> > collectors;
+    std::string collector_path;
 };
+
+/* Dumps the chain's ParticleCollector, if any (call after the run). */
+void finish_outputs(Built &b);
 
 /* Factories for the two helpers without a reference class (toroidal field,
  * per-candidate maximum length); null: ref_shim.cpp's own. */

@@ -102,6 +102,7 @@ int ref_gpu_run_textout(const crp_plan_desc *desc, const crp_candidates *c, uint
             g->run(&cands);
             store_candidates(cands, c);
         }
+        finish_outputs(b);
         b.sim = 0;  // closes the TextOutput files
         return 0;
     } catch (std::exception &e) {

@@ -15,7 +15,8 @@
  * ModulatedMagneticFieldGrid, JF12Field, PlanckJF12bField, UF23Field,
  * PeriodicMagneticField, MagneticFieldList,
  * UniformMagneticField, PlaneWaveTurbulence, MaximumTrajectoryLength,
- * Observer, ObserverSurface(Sphere), ObserverDetectAll, TextOutput, Source
+ * Observer, ObserverSurface(Sphere), ObserverDetectAll, TextOutput,
+ * ParticleCollector, Source
  * features and Random.
  *
  * Helpers written here (no reference counterpart):
@@ -47,6 +48,7 @@
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
 #include "crpropa/module/Observer.h"
+#include "crpropa/module/ParticleCollector.h"
 #include "crpropa/module/PropagationBP.h"
 #include "crpropa/module/PropagationCK.h"
 #include "crpropa/module/TextOutput.h"
@@ -281,7 +283,13 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpe
             for (int f = 0; f < m.n_features; f++) o->add(build_feature(m.features[f]));
             o->setDeactivateOnDetection(m.deactivate_on_detection != 0);
             o->setFlag("Detected", "Detected");
-            if (text_output)
+            if (text_output && text_type == kCollectorOutput) {
+                ref_ptr<ParticleCollector> pc = new ParticleCollector();
+                pc->setClone(true);
+                o->onDetection(pc);
+                b.collectors.push_back(pc.get());
+                b.collector_path = text_output;
+            } else if (text_output)
                 o->onDetection(new TextOutput(text_output, (Output::OutputType)text_type));
             else if (m.record)
                 o->onDetection(new RecordAction(rec, i));
@@ -363,6 +371,12 @@ void store_candidates(const ModuleList::candidate_vector_t &cands, const crp_can
     }
 }
 
+void finish_outputs(Built &b) {
+    if (b.collectors.empty()) return;
+    ParticleCollector *pc = dynamic_cast<ParticleCollector *>(b.collectors[0].get());
+    if (pc) pc->dump(b.collector_path);
+}
+
 }  // namespace crp_ref
 
 using namespace crp_ref;
@@ -428,6 +442,7 @@ int ref_run_textout(const crp_plan_desc *desc, const crp_candidates *c, uint64_t
             std::cout.rdbuf(old);
             store_candidates(cands, c);
         }
+        finish_outputs(b);
         b.sim = 0;  // closes the TextOutput files
         return 0;
     } catch (std::exception &e) {

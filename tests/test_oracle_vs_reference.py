@@ -105,8 +105,11 @@ def test_per_candidate_length_and_neutral(oracle, reference):
     _same(a, b)
 
 
-def test_text_output_matches_reference(reference, tmp_path):
-    """crp_text_output_write against the reference's TextOutput (Event3D)."""
+@pytest.mark.parametrize("suffix", [".txt", ".txt.gz"])
+def test_text_output_matches_reference(reference, tmp_path, suffix):
+    """crp_text_output_write against the reference's TextOutput (Event3D);
+    a .gz name is gzip on both sides (TextOutput.cpp:41, zstream), compared
+    after decompression."""
     import ctypes as C
     rng = np.random.default_rng(105)
     n = 50
@@ -119,7 +122,7 @@ def test_text_output_matches_reference(reference, tmp_path):
     src_e = e * 1.0
     src_pos = np.zeros((n, 3))
     src_d = stable_unit_vectors(rng, n)
-    ref_path = str(tmp_path / "ref.txt")
+    ref_path = str(tmp_path / ("ref" + suffix))
     reference.text_output(ref_path, 3, serial, ids, e, pos, d, length, ids, src_e, src_pos, src_d)
     lib = _abi.load()
     desc = _abi.OutputDesc()
@@ -146,6 +149,12 @@ def test_text_output_matches_reference(reference, tmp_path):
     rows.source_energy = ptr(src_e)
     rows.source_position = ptr(src_pos)
     rows.source_direction = ptr(src_d)
-    mine = str(tmp_path / "mine.txt")
+    mine = str(tmp_path / ("mine" + suffix))
     _abi.check(lib.crp_text_output_write(mine.encode(), 0, 1, C.byref(desc), n, C.byref(rows)))
-    assert open(mine).read() == open(ref_path).read()
+    if suffix.endswith(".gz"):
+        import gzip
+        with open(mine, "rb") as f:
+            assert f.read(2) == b"\x1f\x8b"
+        assert gzip.open(mine, "rt").read() == gzip.open(ref_path, "rt").read()
+    else:
+        assert open(mine).read() == open(ref_path).read()

@@ -167,6 +167,25 @@ def test_plugin_text_output_identical_to_reference(plugin, reference, tmp_path, 
 
 
 @pytest.mark.gpu
+def test_plugin_particle_collector_identical_to_reference(plugin, reference, tmp_path):
+    """A ParticleCollector (clone on) as the observer's detection action
+    (ParticleCollector.cpp:23): the plugin replays the detections into the
+    user's collector, whose dump (TextOutput Everything) equals the one of
+    ModuleList::run, line for line, serial numbers included."""
+    spec = _grid_spec(bp_fixed(1 * U.kpc), radius=40 * U.kpc, length=300 * U.kpc)
+    c = _cands(400, seed=12)
+    pr, pg = tmp_path / "ref.txt", tmp_path / "gpu.txt"
+    collector = 100  # the harness's ParticleCollector output type
+    reference.run_textout(spec, c.copy(), pr, collector, threads=1, serial0=1)
+    plugin.run_textout(spec, c.copy(), pg, collector, serial0=1)
+    hr, dr = _data_lines(pr)
+    hg, dg = _data_lines(pg)
+    assert hr == hg
+    assert len(dr) > 100
+    assert dr == dg
+
+
+@pytest.mark.gpu
 def test_plugin_run_source_count_identical_to_reference(plugin, tmp_path):
     """ModuleList::run(source, count) with the reference's Source features:
     the plugin draws the candidates on the calling thread in batches (here
