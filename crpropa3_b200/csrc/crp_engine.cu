@@ -10,6 +10,8 @@
 // ModuleList.cpp.in:110) is a host flag polled between launches.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -82,6 +84,12 @@ struct crp_plan {
     // compaction lists of still-active candidate indices (ping-pong)
     uint64_t list_cap = 0;
     uint32_t *lists = nullptr;
+    // cell ordering of grid runs: keys in / out, the ordered index list and
+    // the radix sort's temporary storage
+    uint64_t sort_cap = 0;
+    uint32_t *sort_buf = nullptr;
+    size_t sort_tmp_bytes = 0;
+    void *sort_tmp = nullptr;
     int tuned_block = 0;
     // autotuned launch configuration (crp_autotune); mode 0: not tuned
     int tuned_mode = 0;
@@ -98,6 +106,8 @@ struct crp_plan {
         if (scratch) cudaFree(scratch);
         if (rec_scratch) cudaFree(rec_scratch);
         if (lists) cudaFree(lists);
+        if (sort_buf) cudaFree(sort_buf);
+        if (sort_tmp) cudaFree(sort_tmp);
         if (trial) cudaFree(trial);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -534,6 +544,78 @@ static crp_status ensure_lists(crp_plan *p, uint64_t n) {
     return CRP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Cell ordering of grid runs.  Candidates that share grid cells share the
+// corner loads of the interpolation (L1 and L2 hits) and change cells at
+// similar steps (less divergence in the gather), so between launches the
+// still-active candidates are ordered by the cell they are in: blocks of 8^3
+// cells in x-major order, cells x-major inside a block (the key), sorted
+// with a radix sort.  The order is a scheduling choice only: every
+// candidate's trajectory is the same whatever order the threads take them in.
+constexpr int kSortedStepsPerLaunch = 512;
+constexpr uint64_t kSortMinCandidates = 1u << 16;
+
+__device__ __forceinline__ int cell_of(double x, double go, double inv_s, int n) {
+    const double c = floor((x - go) * inv_s);
+    long long i = (long long)c % n;
+    return (int)(i < 0 ? i + n : i);
+}
+
+__global__ void cell_key_kernel(DevGrid g, const double *x, const double *y, const double *z,
+                                const uint32_t *list, uint32_t n, int nby, int nbz, uint32_t *keys,
+                                uint32_t *vals) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t i = list ? list[t] : t;
+    const int ix = cell_of(x[i], g.gox, g.inv_sx, g.nx);
+    const int iy = cell_of(y[i], g.goy, g.inv_sy, g.ny);
+    const int iz = cell_of(z[i], g.goz, g.inv_sz, g.nz);
+    const uint32_t block = ((uint32_t)(ix >> 3) * nby + (uint32_t)(iy >> 3)) * nbz + (uint32_t)(iz >> 3);
+    keys[t] = block * 512u + (uint32_t)(((ix & 7) * 8 + (iy & 7)) * 8 + (iz & 7));
+    vals[t] = i;
+}
+
+// Bits of the largest key, or 0 when the grid is too large for 32-bit keys.
+static int cell_key_bits(const DevGrid &g) {
+    const uint64_t nb = (uint64_t)((g.nx + 7) / 8) * ((g.ny + 7) / 8) * ((g.nz + 7) / 8) * 512;
+    if (nb > (1ull << 32)) return 0;
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < nb) bits++;
+    return bits;
+}
+
+static crp_status ensure_sort(crp_plan *p, uint64_t n) {
+    if (p->sort_cap < n) {
+        if (p->sort_buf) { cudaFree(p->sort_buf); p->sort_buf = nullptr; p->sort_cap = 0; }
+        if (p->sort_tmp) { cudaFree(p->sort_tmp); p->sort_tmp = nullptr; p->sort_tmp_bytes = 0; }
+        CUDA_TRY(cudaMalloc(&p->sort_buf, sizeof(uint32_t) * 4 * n));
+        p->sort_cap = n;
+        size_t bytes = 0;
+        CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, p->sort_buf, p->sort_buf + n, p->sort_buf + 2 * n,
+                                                 p->sort_buf + 3 * n, (int)n, 0, 32));
+        CUDA_TRY(cudaMalloc(&p->sort_tmp, bytes));
+        p->sort_tmp_bytes = bytes;
+    }
+    return CRP_OK;
+}
+
+// Orders the n indices of `list` (all candidates when null) by cell; returns
+// the ordered list (inside p->sort_buf).
+static crp_status order_by_cell(crp_plan *p, const DevState &s, const uint32_t *list, uint64_t n, int bits,
+                                cudaStream_t st, const uint32_t **out) {
+    const DevGrid &g = p->dev.fields[0].grid;
+    uint32_t *keys_in = p->sort_buf, *keys_out = p->sort_buf + p->sort_cap;
+    uint32_t *vals_in = p->sort_buf + 2 * p->sort_cap, *vals_out = p->sort_buf + 3 * p->sort_cap;
+    cell_key_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, s.x, s.y, s.z, list, (uint32_t)n,
+                                                                (g.ny + 7) / 8, (g.nz + 7) / 8, keys_in, vals_in);
+    CUDA_TRY(cudaGetLastError());
+    size_t bytes = p->sort_tmp_bytes;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(p->sort_tmp, bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
+                                             bits, st));
+    *out = vals_out;
+    return CRP_OK;
+}
+
 // Persistent mode: bounded launches of SMs x ctas_per_sm CTAs that refill
 // lanes from the device queue; what a launch leaves (lanes still busy at its
 // time budget, queue items not yet taken) is the next launch's queue.
@@ -698,9 +780,16 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
     DevRecords rec = to_dev_records(o.records);
     int block = o.block_size > 0 ? o.block_size : (p->tuned_block > 0 ? p->tuned_block : 128);
     if (block % 32 || block > 1024) return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d", block);
-    int spl = o.steps_per_launch > 0 ? o.steps_per_launch : 4096;
+    // grid runs with the default launch length are cell-ordered between launches
+    const int key_bits = (p->fs == FS_GRID || p->fs == FS_GRID_PERIODIC) ? cell_key_bits(p->dev.fields[0].grid) : 0;
+    const bool cell_order = o.steps_per_launch <= 0 && key_bits > 0 && n >= kSortMinCandidates;
+    int spl = o.steps_per_launch > 0 ? o.steps_per_launch : (cell_order ? kSortedStepsPerLaunch : 4096);
     crp_status ls = ensure_lists(p, n);
     if (ls) return ls;
+    if (cell_order) {
+        ls = ensure_sort(p, n);
+        if (ls) return ls;
+    }
     double ms_total = 0;
     uint64_t launches = 0;
     // launch 1 covers every candidate; later launches only the ones the
@@ -711,6 +800,12 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
     for (;;) {
         CUDA_TRY(cudaMemsetAsync(p->d_cnt, 0, sizeof(DevCounters), st));
         CUDA_TRY(cudaEventRecord(p->ev0, st));
+        // candidates start where their source puts them: order from the second launch on
+        if (cell_order && list_in && n_threads >= kSortMinCandidates) {
+            ls = order_by_cell(p, s, list_in, n_threads, key_bits, st, &list_in);
+            if (ls) return ls;
+            launches++;  // the key kernel (the radix sort is CUB's)
+        }
         cudaError_t e = (p->precision == CRP_PRECISION_FP64)
             ? launch_fp64_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st)
             : launch_mixed_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st);

@@ -4,10 +4,10 @@
  * This is the drop-in boundary for CRPropa's charged-particle stepping path:
  * a chain of one propagation module (PropagationCK, PropagationBP or
  * DiffusionSDE) over a magnetic field (MagneticFieldGrid over a Grid3f,
- * PeriodicMagneticField, PlaneWaveTurbulence, UniformMagneticField, a
- * MagneticFieldList of those, or a toroidal field), followed by
- * MaximumTrajectoryLength and Observer modules, run to completion over a set
- * of candidates.  It replaces, for such chains,
+ * ModulatedMagneticFieldGrid, PeriodicMagneticField, PlaneWaveTurbulence,
+ * UniformMagneticField, JF12Field, UF23Field, a MagneticFieldList of those,
+ * or a toroidal field), followed by MaximumTrajectoryLength, Observer and
+ * boundary modules, run to completion over a set of candidates.  It replaces, for such chains,
  *
  *   ModuleList::run(const candidate_vector_t*, bool, bool)
  *       include/crpropa/ModuleList.h:43, src/ModuleList.cpp.in:97
@@ -110,9 +110,6 @@ typedef struct crp_plane_wave_desc {
     double brms, lmin, lmax, lbendover, sindex, qindex;
 } crp_plane_wave_desc;
 
-/* One summand of the field (a MagneticFieldList of these is their sum,
- * MagneticField.cpp:64).  A component may be wrapped in a
- * PeriodicMagneticField (MagneticField.cpp:41). */
 /* Parameters of the Jansson-Farrar 2012 galactic field as JF12Field holds
  * them (JF12Field.h, set by the constructors JF12Field.cpp:8 and :352), SI
  * units.  crp_jf12_defaults() fills them.  The striated grid (a Grid1f, one
@@ -152,6 +149,9 @@ typedef struct crp_uf23_desc {
     double microgauss;                      /* field unit [T] */
 } crp_uf23_desc;
 
+/* One summand of the field (a MagneticFieldList of these is their sum,
+ * MagneticField.cpp:64).  A component may be wrapped in a
+ * PeriodicMagneticField (MagneticField.cpp:41). */
 typedef struct crp_field_component {
     int32_t kind;
     int32_t periodic;            /* wrap in PeriodicMagneticField */
@@ -343,9 +343,11 @@ typedef struct crp_run_stats {
     uint64_t particle_steps;    /* accepted propagation steps */
     uint64_t tries;             /* propagation tries including rejected ones */
     uint64_t field_evaluations; /* getField calls */
-    uint64_t launches;          /* kernel launches of the stepping path */
+    uint64_t launches;          /* kernel launches of the stepping path (stepping kernels and
+                                   the cell-ordering key kernels between them) */
     uint64_t active_left;       /* candidates still active on return */
-    double device_ms;           /* device time of the stepping kernels */
+    double device_ms;           /* device time of the stepping path: the stepping kernels and the
+                                   cell ordering between them */
 } crp_run_stats;
 
 typedef struct crp_plan crp_plan;
