@@ -34,7 +34,7 @@ import numpy as np  # noqa: E402
 METRIC = "particle-steps/s, 1 B200: mixed-prec vs FP64 at stated error; adjoint cost/fwd"
 UNIT = "particle-steps/s"
 ALGO_BYTES_PER_STEP = 96  # 8 corners x 12 B Grid3f payload per field evaluation
-TRAFFIC_B_PER_STEP = 32.6  # DRAM read+write per particle-step of the mixed kernel (ncu, full size)
+TRAFFIC_B_PER_STEP = 14.4  # DRAM read+write per particle-step of the mixed kernel (ncu, full size)
 
 
 def log(*a):
@@ -674,16 +674,20 @@ def main():
     achieved = ALGO_BYTES_PER_STEP * steps_mx / (kernel_ms / 1e3) / 1e9
     # DRAM bytes per particle-step of this kernel from ncu (dram__bytes_read.sum +
     # dram__bytes_write.sum), scaled to the steps of an average timed launch
-    traffic = TRAFFIC_B_PER_STEP * steps_mx / max(launches, 1)
+    # launches counts the stepping kernels and, between two of them in a run, one cell-ordering
+    # key kernel: args.steps runs of k stepping launches are 2k - 1 launches each
+    step_launches = max((launches + args.steps) // 2, 1)
+    traffic = TRAFFIC_B_PER_STEP * steps_mx / step_launches
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "basis": "96 B (8 corners x 12 B) per particle-step over the stepping kernel time",
                 "note": "the register cell cache reloads corners only on a cell change, so DRAM "
                         "traffic per step (traffic) is below the 96 B basis and frac can exceed 1; "
                         "ncu shows the kernel issue/latency bound, not HBM bound",
-                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step measured by ncu on a "
-                                 "full-size launch (profiles/launches_grid_bp_256.md) x "
-                                 "particle-steps per timed launch"}
+                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step: mean DRAM read+write of "
+                                 "six full-size launches measured by ncu "
+                                 "(profiles/dram_mixed_chunk_kernel_bp_fixed_grid256_full.md) x "
+                                 "particle-steps per timed stepping launch"}
 
     adjoint = None if args.no_adjoint else adjoint_cost(dev, args)
 
