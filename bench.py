@@ -387,7 +387,9 @@ def cfg_grid_ck_64(dev, peaks, n=10_000):
         out.setdefault("grid_ck_64", {
             "workload": f"{n} protons 1-100 EeV, 64^3 Grid3f 1 nG 10 kpc, PropagationCK 1e-4 "
                         "0.1-10 kpc, MaximumTrajectoryLength 10 Mpc, full runs",
-            "note": "10^4 candidates fill 79 of the 148 SMs (one thread per candidate)"})[name] = {
+            "note": "10^4 candidates are 79 blocks of 128 (one thread per candidate); the run time is "
+                    "the serial step chain of the slowest candidates: spreading them over all 148 SMs "
+                    "in single-warp blocks measured no faster (4.24e9 vs 4.20e9 tries/s)"})[name] = {
             "tries_per_s": tries_s, "particle_steps_per_s": t["particle_steps"] / (t["device_ms"] / 1e3),
             "ms_per_run": t["device_ms"] / 3,
             "roofline": {"bound": "l2", "achieved": gbs, "peak": peaks.get("l2_gbs"), "unit": "GB/s",
