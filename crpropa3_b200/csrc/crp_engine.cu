@@ -60,6 +60,7 @@ void set_last_error(const char *msg) { g_error = msg; }
 }  // namespace crp
 
 constexpr double kInv2Pi = 0.15915494309189533577;  // 1 / (2 pi)
+constexpr double kTurnScale = 4294967296.0;          // 2^32: turns as 32-bit fixed point
 
 struct crp_plan {
     int device = 0;
@@ -248,13 +249,13 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             for (int a = 0; a < 3; a++) {
                 m9[9 * i + a] = w.xi[3 * i + a];
                 m9[9 * i + 3 + a] = w.kappa[3 * i + a];
-                // mixed form: phase in turns, k kappa / 2 pi
-                kk[4 * i + a] = w.k[i] * w.kappa[3 * i + a] * kInv2Pi;
+                // mixed form: phase in turns, k kappa / 2 pi, times 2^32 (exact)
+                kk[4 * i + a] = w.k[i] * w.kappa[3 * i + a] * kInv2Pi * kTurnScale;
             }
             m9[9 * i + 6] = w.k[i];
             m9[9 * i + 7] = w.beta[i];
             m9[9 * i + 8] = w.ak[i];
-            kk[4 * i + 3] = w.beta[i] * kInv2Pi;
+            kk[4 * i + 3] = w.beta[i] * kInv2Pi * kTurnScale;
             a32[i] = make_float4((float)(w.ak[i] * w.xi[3 * i]), (float)(w.ak[i] * w.xi[3 * i + 1]),
                                  (float)(w.ak[i] * w.xi[3 * i + 2]), 0.f);
         }
@@ -265,6 +266,15 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         st = upload(p, a32.data(), a32.size(), &d.pw.modes32);
         if (st) return st;
         d.pw.n = n;
+        // the fixed-point phase of the mixed form needs |phase * 2^32| < 2^50 for every mode:
+        // |k kappa . x| + |beta| <= max_i (|kx| + |ky| + |kz|) max(|x|, |y|, |z|) + max |beta|
+        double ksum = 0, bmax = 0;
+        for (int i = 0; i < n; i++) {
+            ksum = std::max(ksum, std::fabs(kk[4 * i]) + std::fabs(kk[4 * i + 1]) + std::fabs(kk[4 * i + 2]));
+            bmax = std::max(bmax, std::fabs(kk[4 * i + 3]));
+        }
+        const double room = 1125899906842624.0 - bmax;  // 2^50
+        d.pw.fast_limit = (ksum > 0 && room > 0) ? room / ksum : (room > 0 ? INFINITY : 0.0);
     } else if (f.kind == CRP_FIELD_JF12) {
         const crp_jf12_desc &J = f.jf12;
         if (!(J.kpc > 0)) return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: parameters not set (crp_jf12_defaults)");

@@ -33,8 +33,9 @@ struct DevGrid {
 struct DevPlaneWave {
     const double *modes;   // FP64 form: per mode {xi x y z, kappa x y z, k, beta, Ak} (9 doubles)
     const float4 *modes32; // mixed form: per mode {k*kappa (FP64 split), Ak*xi} (see step_mixed.cu)
-    const double *kk;      // mixed form: per mode k*kappa and beta in turns (over 2 pi), 4 doubles
+    const double *kk;      // mixed form: per mode k*kappa and beta in turns (over 2 pi) times 2^32, 4 doubles
     int n;
+    double fast_limit;     // mixed form: max(|x|, |y|, |z|) below which every scaled phase stays under 2^50
 };
 
 // JF12Field parameters (crp_jf12_desc, SI) for the FP64 form, and the same

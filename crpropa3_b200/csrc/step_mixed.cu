@@ -148,12 +148,30 @@ struct PwTab {
     const double2 *kk;
     const float4 *a;
     int n;
+    double fast_limit;
 };
 
-template <bool SHARED>
-__device__ __forceinline__ f3 pw_sum(const double2 *kk, const float4 *am, int n, double x, double y,
-                                     double z) {
+// cos(2 pi p) for a phase p in turns given as p * 2^32 (the mode table's scale).
+// FAST (|p * 2^32| < 2^50): adding 1.5 * 2^52 rounds p * 2^32 to an integer whose
+// low 32 bits are the fraction of a turn in fixed point; its top 23 bits, shifted
+// by half a turn, become a float in [-1/2, 1/2) through the exponent bits of 1.0
+// (no conversion instruction, 2^-23-turn steps, rounded).  Otherwise the FP64
+// fraction p - rint(p) rounded to FP32.
+template <bool FAST>
+__device__ __forceinline__ float cos_turns(double ps) {
     const float twopi = 6.28318530717958647692f;
+    if (FAST) {
+        const unsigned lo = (unsigned)__double2loint(ps + 6755399441055744.0);
+        const float f = __int_as_float(0x3f800000u | (((lo + 256u) ^ 0x80000000u) >> 9)) - 1.5f;
+        return __cosf(twopi * f);
+    }
+    const double p = ps * 2.3283064365386962890625e-10;  // 2^-32, exact
+    return __cosf(twopi * (float)(p - rint(p)));
+}
+
+template <bool SHARED, bool FAST>
+__device__ __forceinline__ f3 pw_sum_t(const double2 *kk, const float4 *am, int n, double x, double y,
+                                       double z) {
     float bx0 = 0.f, by0 = 0.f, bz0 = 0.f, bx1 = 0.f, by1 = 0.f, bz1 = 0.f;
     const int n2 = n & ~1;
 #pragma unroll 4
@@ -170,8 +188,8 @@ __device__ __forceinline__ f3 pw_sum(const double2 *kk, const float4 *am, int n,
         }
         const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
         const double p1 = fma(m2.x, x, fma(m2.y, y, fma(m3.x, z, m3.y)));
-        const float c0 = __cosf(twopi * (float)(p0 - rint(p0)));
-        const float c1 = __cosf(twopi * (float)(p1 - rint(p1)));
+        const float c0 = cos_turns<FAST>(p0);
+        const float c1 = cos_turns<FAST>(p1);
         bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
         bx1 = fmaf(b.x, c1, bx1); by1 = fmaf(b.y, c1, by1); bz1 = fmaf(b.z, c1, bz1);
     }
@@ -180,16 +198,23 @@ __device__ __forceinline__ f3 pw_sum(const double2 *kk, const float4 *am, int n,
         const double2 m1 = SHARED ? kk[2 * n2 + 1] : __ldg(kk + 2 * n2 + 1);
         const float4 a = SHARED ? am[n2] : __ldg(am + n2);
         const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
-        const float c0 = __cosf(twopi * (float)(p0 - rint(p0)));
+        const float c0 = cos_turns<FAST>(p0);
         bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
     }
     return f3mk(bx0 + bx1, by0 + by1, bz0 + bz1);
 }
 
+template <bool SHARED>
+__device__ __forceinline__ f3 pw_sum(const double2 *kk, const float4 *am, int n, double lim, double x,
+                                     double y, double z) {
+    if (fmax(fabs(x), fmax(fabs(y), fabs(z))) < lim) return pw_sum_t<SHARED, true>(kk, am, n, x, y, z);
+    return pw_sum_t<SHARED, false>(kk, am, n, x, y, z);
+}
+
 __device__ __forceinline__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double z,
                                                const PwTab *sh = nullptr) {
-    if (sh) return pw_sum<true>(sh->kk, sh->a, sh->n, x, y, z);
-    return pw_sum<false>(reinterpret_cast<const double2 *>(w.kk), w.modes32, w.n, x, y, z);
+    if (sh) return pw_sum<true>(sh->kk, sh->a, sh->n, sh->fast_limit, x, y, z);
+    return pw_sum<false>(reinterpret_cast<const double2 *>(w.kk), w.modes32, w.n, w.fast_limit, x, y, z);
 }
 
 // ---------------------------------------------------------------- JF12Field
@@ -828,7 +853,7 @@ __global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_k
                                                                const uint32_t *perm, uint32_t *perm_out,
                                                                int pw_field) {
     extern __shared__ __align__(16) unsigned char pw_smem[];
-    PwTab tab{nullptr, nullptr, 0};
+    PwTab tab{nullptr, nullptr, 0, 0.0};
     if (pw_field >= 0) {
         const DevPlaneWave &w = P.fields[pw_field].pw;
         double2 *kk = reinterpret_cast<double2 *>(pw_smem);
@@ -837,7 +862,7 @@ __global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_k
         for (int q = threadIdx.x; q < 2 * w.n; q += blockDim.x) kk[q] = __ldg(gk + q);
         for (int q = threadIdx.x; q < w.n; q += blockDim.x) am[q] = __ldg(w.modes32 + q);
         __syncthreads();
-        tab = PwTab{kk, am, w.n};
+        tab = PwTab{kk, am, w.n, w.fast_limit};
     }
     const PwTab *sh = pw_field >= 0 ? &tab : nullptr;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
