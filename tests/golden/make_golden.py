@@ -1,7 +1,10 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
 Needs oracle/_ref/libcrp_ref.so (`make -C oracle ref`, which compiles the
-reference's stepping path from its sources).  Inputs are seeded; the outputs
+reference's stepping path from its sources).  Writes reference_golden.npz
+(the stepping chains, fields, draws, sources, charges) and
+reference_golden_ext.npz (interpolation types, modulated grids, observer
+features and boundaries, the galactic fields, turbulence draws, grid files).  Inputs are seeded; the outputs
 are the reference's own ModuleList::run results, field values, random draws
 and Source samples.  Run:  python tests/golden/make_golden.py
 """
@@ -83,5 +86,60 @@ def main():
     print("wrote", os.path.join(HERE, "reference_golden.npz"), len(out), "arrays")
 
 
+
+
+def main_ext():
+    """reference_golden_ext.npz: the interpolation types, ModulatedMagneticFieldGrid,
+    observer features and boundaries, JF12Field / PlanckJF12bField, UF23Field, the
+    turbulence draw sequences and the grid file formats, from the reference."""
+    import tempfile
+    import test_grid_interpolation as GI
+    import test_jf12 as J
+    import test_observers_boundaries as OB
+    import test_uf23 as UF
+    ref = Reference()
+    out = {}
+    pos = GI._positions(600, seed=201)
+    out["interp/pos"] = pos
+    for interp, refl, clip in GI.VECTOR_CASES:
+        out[f"interp/B_{interp}_{int(refl)}_{int(clip)}"] = ref.field(GI._vector_spec(interp, refl, clip), pos)
+    for gi, mi, mr in GI.MOD_CASES:
+        out[f"modulated/B_{gi}_{mi}_{int(mr)}"] = ref.field(GI._mod_spec(gi, mi, mr), pos)
+    for name in ("box", "cylindrical", "vetoes", "tracking"):
+        c = OB._cands(120, seed=202)
+        res, rec = c.copy(), RecordArrays(20000)
+        ref.run(OB._spec(name), res, rec, threads=1)
+        for m in OB.STATE:
+            out[f"chain_{name}/out_{m}"] = getattr(res, m)
+        for k, v in rec.sorted().items():
+            out[f"chain_{name}/rec_{k}"] = v
+    jpos = J._positions(800, seed=203)
+    out["jf12/pos"] = jpos
+    for name in J.FIELDS:
+        out[f"jf12/B_{name}"] = ref.field(J._spec(name), jpos)
+    out["jf12/striated_12345"] = ref.jf12_random_striated(12345)[:10, :10, :10]
+    upos = UF._positions(800, seed=204)
+    out["uf23/pos"] = upos
+    for name in UF.MODELS:
+        out[f"uf23/B_{name}"] = ref.field(UF._spec(name), upos)
+    for kind in (0, 1, 2):
+        out[f"turbulence/draws_{kind}"] = ref.turbulence_draws(777, kind, 300)
+    rng = np.random.default_rng(205)
+    v3 = (rng.standard_normal((3, 4, 2, 3)) * 1e-10).astype(np.float32)
+    v1 = rng.uniform(-1, 3, (3, 4, 2)).astype(np.float32)
+    out["gridfile/v3"], out["gridfile/v1"] = v3, v1
+    with tempfile.TemporaryDirectory() as d:
+        for key, v, txt, prop in (("v3_raw", v3, False, False), ("v1_raw", v1, False, False),
+                                  ("v3_txt", v3, True, True), ("v1_txt", v1, True, True)):
+            path = os.path.join(d, key)
+            ref.dump_grid(v, path, 2.5, txt=txt, save_prop=prop, origin=(1e19, -2e19, 0.5),
+                          spacing=(3e19, 3e19, 3e19), reflective=True, clip=False, interp=1)
+            with open(path, "rb") as f:
+                out[f"gridfile/{key}"] = np.frombuffer(f.read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "reference_golden_ext.npz"), **out)
+    print("wrote", os.path.join(HERE, "reference_golden_ext.npz"), len(out), "arrays")
+
+
 if __name__ == "__main__":
     main()
+    main_ext()
