@@ -371,6 +371,8 @@ def secondary_configs(dev, peaks):
     out.update(cfg_grid_ck_nuclei(dev, peaks))
     out.update(cfg_sde_galactic(dev, peaks))
     out.update(cfg_jf12_backtrack(dev, peaks))
+    out.update(cfg_jf12_backtrack(dev, peaks, model="uf23"))
+    out.update(cfg_turbulence(dev))
     return out
 
 
@@ -468,26 +470,54 @@ def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
     return out
 
 
-def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000):
-    """PropagationCK backtracking through the JF12 regular field, full runs,
-    FP64 and mixed forms, beside the reference's own CPU run of a sample."""
+def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
+    """PropagationCK backtracking through the JF12 regular field (or the UF23
+    base model), full runs, FP64 and mixed forms, beside the reference's own
+    CPU run of a sample."""
     from crpropa3_b200 import _abi, engine, workloads as W
-    res = {"workload": f"{n} antiprotons 5-100 EeV from (-8.5 kpc, 0, 0), JF12Field (regular), "
+    make = W.jf12_backtrack if model == "jf12" else W.uf23_backtrack
+    field = "JF12Field (regular)" if model == "jf12" else "UF23Field (base)"
+    res = {"workload": f"{n} antiprotons 5-100 EeV from (-8.5 kpc, 0, 0), {field}, "
                        "PropagationCK 1e-4 0.1-100 pc, Observer sphere 20 kpc, full runs"}
     for prec, name in ((_abi.PRECISION_FP64, "fp64"), (_abi.PRECISION_MIXED, "mixed")):
-        spec, cands = W.jf12_backtrack(n=n, precision=prec)
+        spec, cands = make(n=n, precision=prec)
         plan = engine.Plan(spec)
         t = _timed_runs(plan, cands.to_device(dev), cands.to_device(dev), 2)
         secs = t["device_ms"] / 1e3
         res[name] = {"tries_per_s": t["tries"] / secs, "particle_steps_per_s": t["particle_steps"] / secs,
                      "field_evaluations_per_s": t["field_evaluations"] / secs, "ms_per_run": t["device_ms"] / 2}
         plan.close()
-    spec, cands = W.jf12_backtrack(n=n_cpu, precision=_abi.PRECISION_FP64)
+    spec, cands = make(n=n_cpu, precision=_abi.PRECISION_FP64)
     cpu = reference_cpu_rate(spec, cands, n_cpu, cpu_threads())
     if cpu is not None:
         res["cpu_reference"] = {"particle_steps_per_s": cpu["value"], "cores": cpu_threads(),
                                 "sample": f"{n_cpu} candidates, full runs"}
-    return {"jf12_backtrack": res}
+    return {f"{model}_backtrack": res}
+
+
+def cfg_turbulence(dev, sizes=(256, 512)):
+    """Turbulent Grid3f generation on the device (crp_turbulence_grid):
+    GridTurbulence with a Kolmogorov spectrum, lMin = 2 cells, lMax = n cells,
+    timed with CUDA events around the call (k-space flags and scan, host
+    draws and their copy, amplitudes, three cuFFT C2R, normalisation)."""
+    import torch
+    from crpropa3_b200 import _abi, turbulence as T, units as U
+    res = {"workload": "GridTurbulence, Kolmogorov, Brms 1 nG, spacing 1 kpc, lMin 2 kpc, lMax n kpc, seed 42"}
+    for n in sizes:
+        args = (_abi.TURBULENCE_GRID, n, 1 * U.kpc, 1 * U.nG, 2 * U.kpc, n * U.kpc)
+        g = T.grid_turbulence_device(*args, seed=42)  # warm-up (plans, allocations)
+        del g
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        g = T.grid_turbulence_device(*args, seed=42)
+        ev1.record()
+        torch.cuda.synchronize()
+        res[f"n{n}"] = {"ms": ev0.elapsed_time(ev1), "cells": n ** 3,
+                        "modes": T.turbulence_modes(T.turbulence_desc(*args, seed=42))}
+        del g
+        torch.cuda.empty_cache()
+    return {"turbulence_generation": res}
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -523,7 +553,9 @@ def main():
         runs = {"grid_ck_64": lambda: cfg_grid_ck_64(dev, {}, n=args.n or 10_000),
                 "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or (1 << 20)),
                 "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20)),
-                "jf12_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20))}
+                "jf12_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20)),
+                "uf23_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="uf23"),
+                "turbulence": lambda: cfg_turbulence(dev)}
         if args.workload not in runs:
             log(f"unknown workload {args.workload}")
             return 2

@@ -16,6 +16,7 @@ jf12_backtrack: PropagationCK (1e-4, 0.1 pc-100 pc) in the JF12 regular
               leaving the Earth's position (-8.5 kpc, 0, 0) isotropically,
               detected by an Observer sphere of 20 kpc around the galactic
               centre, MaximumTrajectoryLength 100 kpc (backtracking).
+uf23_backtrack: the same in the UF23Field base model.
 Inputs are synthetic and seeded; sizes are scaled down through `n`.
 """
 from __future__ import annotations
@@ -141,9 +142,11 @@ def sde_galactic(n=10_000_000, n_modes=1024, precision=_abi.PRECISION_MIXED, see
     return spec, cands
 
 
-def jf12_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, variant=_abi.JF12_VARIANT_JF12):
-    """Backtracking through the JF12 regular field (module docstring)."""
-    spec = P.ChainSpec([P.JF12Field(variant=variant)],
+def jf12_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, variant=_abi.JF12_VARIANT_JF12,
+                   field=None):
+    """Backtracking through the JF12 regular field (module docstring); `field`
+    replaces the JF12Field (uf23_backtrack passes a UF23Field)."""
+    spec = P.ChainSpec([field if field is not None else P.JF12Field(variant=variant)],
                        [P.Propagation(_abi.PROP_CK, 1e-4, 0.1 * U.pc, 100 * U.pc),
                         P.MaxTrajectoryLength(100 * U.kpc, record=False),
                         P.ObserverSpec(_abi.OBSERVER_SURFACE_SPHERE, (0.0, 0.0, 0.0), 20 * U.kpc,
@@ -152,3 +155,8 @@ def jf12_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, variant=
     cands = source_candidates(n, [-IDS["H"]], 5 * U.EeV, 100 * U.EeV, -1.0, seed,
                               position=(-8.5 * U.kpc, 0.0, 0.0))
     return spec, cands
+
+
+def uf23_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, model=_abi.UF23_BASE):
+    """jf12_backtrack with the UF23Field model `model` instead of JF12."""
+    return jf12_backtrack(n, precision, seed, field=P.UF23Field(model))
