@@ -48,10 +48,12 @@ def _mt_rand(seed: int, count: int) -> np.ndarray:
 
 
 def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0, seed=42,
-           draws=None):
+           draws=None, kind=None):
     """The three complex (n, n, n/2+1) arrays B(k) of initTurbulence.
     `draws(seed, count)` returns count Random::rand() values (default: the
-    engine's MT19937)."""
+    engine's MT19937).  kind TURBULENCE_SIMPLE builds SimpleGridTurbulence's
+    instead (SimpleGridTurbulence.cpp:62-95): amplitude randNorm() k^(alpha/2)
+    with alpha = -sindex - 2, draws rand, randNorm, rand per mode."""
     if seed == 0:
         raise ValueError("seed 0 means a random seed in the reference; give a non-zero seed")
     check_grid_requirements(n, spacing, lmin, lmax)
@@ -63,9 +65,14 @@ def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex
     kmin, kmax = spacing / lmax, spacing / lmin
     keep = ~((k.astype(np.float64) < kmin) | (k.astype(np.float64) > kmax))
     m = int(keep.sum())
-    u = (draws or _mt_rand)(seed, 2 * m)
-    theta = 2 * math.pi * u[0::2]
-    phase = 2 * math.pi * u[1::2]
+    simple = kind == _abi.TURBULENCE_SIMPLE
+    if simple:
+        d = turbulence_draws(seed, _abi.TURBULENCE_SIMPLE, m)
+        theta, norm, phase = 2 * math.pi * d[:, 0], d[:, 1], 2 * math.pi * d[:, 2]
+    else:
+        u = (draws or _mt_rand)(seed, 2 * m)
+        theta = 2 * math.pi * u[0::2]
+        phase = 2 * math.pi * u[1::2]
     kx, ky, kz, kk = ex[keep], ey[keep], ez[keep], k[keep]
     one = np.float32(1.0)
     # e1 = n0 x ek, e2 = ek x e1 with n0 = (1, 1, 1), in float (Vector3f)
@@ -83,9 +90,12 @@ def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex
     e2 /= np.sqrt((e2 * e2).sum(1))[:, None].astype(np.float32)
     b = (e1 * np.cos(theta).astype(np.float32)[:, None] +
          e2 * np.sin(theta).astype(np.float32)[:, None]).astype(np.float32)
-    lam = 1 / spacing * 2 * math.pi
-    amp = np.sqrt(energy_spectrum(kk.astype(np.float64) * lam, brms, lmin, lmax, lbendover, sindex,
-                                  qindex)).astype(np.float32)
+    if simple:
+        amp = (norm * np.power(kk.astype(np.float64), (-sindex - 2) / 2)).astype(np.float32)
+    else:
+        lam = 1 / spacing * 2 * math.pi
+        amp = np.sqrt(energy_spectrum(kk.astype(np.float64) * lam, brms, lmin, lmax, lbendover, sindex,
+                                      qindex)).astype(np.float32)
     b *= amp[:, None]
     cph, sph = np.cos(phase), np.sin(phase)
     out = []
@@ -97,9 +107,10 @@ def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex
 
 
 def grid_turbulence(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0,
-                    seed=42, device=None, draws=None) -> np.ndarray:
-    """(n, n, n, 3) float32 Grid3f values of GridTurbulence(spectrum, grid, seed)."""
-    bk = kspace(n, spacing, brms, lmin, lmax, lbendover, sindex, qindex, seed, draws)
+                    seed=42, device=None, draws=None, kind=None) -> np.ndarray:
+    """(n, n, n, 3) float32 Grid3f values of GridTurbulence(spectrum, grid,
+    seed), or of SimpleGridTurbulence with kind TURBULENCE_SIMPLE."""
+    bk = kspace(n, spacing, brms, lmin, lmax, lbendover, sindex, qindex, seed, draws, kind)
     comps = []
     use_torch = False
     if device is not None:

@@ -67,6 +67,9 @@ def source_candidates(n, ids, emin, emax, index, seed, position=(0.0, 0.0, 0.0),
 
 
 def kolmogorov_grid(n, spacing, brms, lmin, lmax, seed=42, device=None):
+    """GridTurbulence(TurbulenceSpectrum(brms, lmin, lmax), GridProperties(0, n,
+    spacing), seed) with the spectrum's defaults (sIndex 5/3, qIndex 4,
+    lBendover 1 m), as the reference builds it from these arguments."""
     return grid_turbulence(n, spacing, brms, lmin, lmax, seed=seed, device=device)
 
 

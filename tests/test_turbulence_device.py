@@ -7,9 +7,9 @@ CPU: the k-space draw sequences against the reference's crpropa::Random
 (rand and randNorm interleaved as each loop draws them), bit for bit; the
 number of kept modes against the restated k-space mask.  FFTW is absent, so
 the reference's grids cannot be produced here; on the GPU the device grid
-of GridTurbulence is compared with this package's host restatement
-(identical k-space construction and draws, another FFT) within 1e-4 of
-Brms, and every kind is checked for rms = Brms, zero mean, a divergence-free
+of GridTurbulence and SimpleGridTurbulence is compared with this package's
+host restatement (identical k-space construction and draws, another FFT)
+within 1e-4 of Brms, and every kind is checked for rms = Brms, zero mean, a divergence-free
 spectrum and, for the helical kind, the sign of the magnetic helicity.
 """
 import numpy as np
@@ -70,9 +70,10 @@ def _spectral(g):
 
 
 @pytest.mark.gpu
-def test_device_grid_turbulence_matches_host_restatement():
-    g = T.grid_turbulence_device(_abi.TURBULENCE_GRID, N, SPACING, BRMS, LMIN, LMAX, seed=42).cpu().numpy()
-    h = T.grid_turbulence(N, SPACING, BRMS, LMIN, LMAX, seed=42)
+@pytest.mark.parametrize("kind", ["grid", "simple"])
+def test_device_turbulence_matches_host_restatement(kind):
+    g = T.grid_turbulence_device(KINDS[kind], N, SPACING, BRMS, LMIN, LMAX, seed=42).cpu().numpy()
+    h = T.grid_turbulence(N, SPACING, BRMS, LMIN, LMAX, seed=42, kind=KINDS[kind])
     np.testing.assert_allclose(g, h, rtol=0, atol=1e-4 * BRMS)
 
 
