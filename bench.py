@@ -497,26 +497,29 @@ def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
 
 def cfg_turbulence(dev, sizes=(256, 512)):
     """Turbulent Grid3f generation on the device (crp_turbulence_grid):
-    GridTurbulence with a Kolmogorov spectrum, lMin = 2 cells, lMax = n cells,
-    timed with CUDA events around the call (k-space flags and scan, host
-    draws and their copy, amplitudes, three cuFFT C2R, normalisation)."""
+    GridTurbulence (bend-over at lMax) and SimpleGridTurbulence, Kolmogorov,
+    lMin = 2 cells, lMax = n cells, timed with CUDA events around the call
+    (k-space flags and scan, host draws and their copy, amplitudes, three
+    cuFFT C2R, normalisation)."""
     import torch
     from crpropa3_b200 import _abi, turbulence as T, units as U
-    res = {"workload": "GridTurbulence, Kolmogorov, Brms 1 nG, spacing 1 kpc, lMin 2 kpc, lMax n kpc, seed 42"}
-    for n in sizes:
-        args = (_abi.TURBULENCE_GRID, n, 1 * U.kpc, 1 * U.nG, 2 * U.kpc, n * U.kpc)
-        g = T.grid_turbulence_device(*args, seed=42)  # warm-up (plans, allocations)
-        del g
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        ev0.record()
-        g = T.grid_turbulence_device(*args, seed=42)
-        ev1.record()
-        torch.cuda.synchronize()
-        res[f"n{n}"] = {"ms": ev0.elapsed_time(ev1), "cells": n ** 3,
-                        "modes": T.turbulence_modes(T.turbulence_desc(*args, seed=42))}
-        del g
-        torch.cuda.empty_cache()
+    res = {"workload": "Brms 1 nG, spacing 1 kpc, lMin 2 kpc, lMax n kpc, sIndex 5/3, seed 42; "
+                       "GridTurbulence with lBendover = lMax, SimpleGridTurbulence"}
+    for kind, name in ((_abi.TURBULENCE_GRID, "grid"), (_abi.TURBULENCE_SIMPLE, "simple")):
+        for n in sizes:
+            args = (kind, n, 1 * U.kpc, 1 * U.nG, 2 * U.kpc, n * U.kpc, n * U.kpc)
+            g = T.grid_turbulence_device(*args, seed=42)  # warm-up (plans, allocations)
+            del g
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record()
+            g = T.grid_turbulence_device(*args, seed=42)
+            ev1.record()
+            torch.cuda.synchronize()
+            res[f"{name}_n{n}"] = {"ms": ev0.elapsed_time(ev1), "cells": n ** 3,
+                                   "modes": T.turbulence_modes(T.turbulence_desc(*args, seed=42))}
+            del g
+            torch.cuda.empty_cache()
     return {"turbulence_generation": res}
 
 

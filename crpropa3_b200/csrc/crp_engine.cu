@@ -321,7 +321,11 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             return fail(CRP_ERR_INVALID_ARGUMENT, "UF23Field: unknown field model");
         if (!(U.kpc > 0) || !(U.microgauss > 0))
             return fail(CRP_ERR_INVALID_ARGUMENT, "UF23Field: parameters not set (crp_uf23_defaults)");
-        crp_status st = upload(p, &U, 1, &d.uf);
+        DevUF23 h;
+        h.d = U;
+        h.c_pol = std::pow(U.poloidal_a / U.poloidal_z, U.poloidal_p);  // UF23Field.cpp:392-393
+        h.a0p = std::pow(U.poloidal_a, U.poloidal_p);
+        crp_status st = upload(p, &h, 1, &d.uf);
         if (st) return st;
     } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {
     } else {

@@ -50,6 +50,15 @@ struct DevJF12 {
     float bdturb5, zdturb, bhturb, rhturb, zhturb;
 };
 
+// UF23Field parameters with the two powers the poloidal halo recomputes at
+// every call from model constants, evaluated once on the host with the C
+// library's pow (the reference's own values).
+struct DevUF23 {
+    crp_uf23_desc d;
+    double c_pol;  // pow(A / Z, P)
+    double a0p;    // pow(A, P)
+};
+
 struct DevComponent {
     int kind;       // crp_field_kind
     int periodic;
@@ -63,7 +72,7 @@ struct DevComponent {
     DevGrid mod;    // CRP_FIELD_MODULATED_GRID: the Grid1f modulation (values: one float per cell);
                     // CRP_FIELD_JF12: the striated grid (grid: the turbulent grid)
     const DevJF12 *jf;  // CRP_FIELD_JF12: device copy of the parameters
-    const crp_uf23_desc *uf;  // CRP_FIELD_UF23: device copy of the parameters
+    const DevUF23 *uf;        // CRP_FIELD_UF23: device copy of the parameters
 };
 
 struct DevModule {

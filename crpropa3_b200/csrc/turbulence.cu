@@ -17,7 +17,7 @@
 //      arithmetic;
 //   4. cuFFT's C2R (unnormalised like FFTW's) transforms each component;
 //   5. one kernel interleaves the components into Vector3f cells and sums
-//      |b|^2 per block in double; the host finishes the sum and one kernel
+//      |b|^2 per block in double (squares included); the host finishes the sum and one kernel
 //      scales the cells by Brms / rms rounded to float (scaleGrid,
 //      GridTools.cpp:16, rmsFieldStrength :59).
 // Traffic is a few passes over the grid; the FFT dominates.
@@ -201,7 +201,9 @@ __global__ void interleave_kernel(const float *rx, const float *ry, const float 
         out[3 * i] = x;
         out[3 * i + 1] = y;
         out[3 * i + 2] = z;
-        v2 = (double)__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));  // getR2 in float
+        // |b|^2 in double: the float squares of rmsFieldStrength (getR2, GridTools.cpp:59) underflow
+        // to zero for the tiny amplitudes of SI spectra with a small bend-over scale
+        v2 = (double)x * x + (double)y * y + (double)z * z;
     }
     red[threadIdx.x] = v2;
     __syncthreads();

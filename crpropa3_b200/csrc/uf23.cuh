@@ -1,12 +1,12 @@
 // uf23.cuh -- UF23Field (UF23Field.cpp:269-558), the eight coherent
 // galactic field models of Unger & Farrar 2023, in FP64 in the model's own
 // units (kpc, microgauss), the reference's operation order.  exp, log, sin,
-// cos, acos and atan2 are CUDA's (within two ulp of glibc's); pow is the
-// correctly rounded one of crmath.cuh, and pow(v, 2) is v * v.  Included by
-// both stepping units; the FP64 unit compiles it without contraction.
+// cos, acos, atan2 and pow are CUDA's (within two ulp of glibc's), pow(v, 2)
+// is v * v, and the two powers of model constants (A/Z)^P and A^P come
+// precomputed from the host.  Included by both stepping units; the FP64 unit
+// compiles it without contraction.
 #pragma once
 
-#include "crmath.cuh"
 #include "device_plan.cuh"
 
 namespace crp {
@@ -88,13 +88,14 @@ __device__ __forceinline__ u3 uf_toroidal(const crp_uf23_desc &U, double x, doub
 }
 
 // getPoloidalHaloField (UF23Field.cpp:385)
-__device__ __forceinline__ u3 uf_poloidal(const crp_uf23_desc &U, double x, double y, double z) {
+__device__ __forceinline__ u3 uf_poloidal(const DevUF23 &W, double x, double y, double z) {
+    const crp_uf23_desc &U = W.d;
     const double r = sqrt(x * x + y * y);
     const double P = U.poloidal_p;
-    const double c = cr_pow(U.poloidal_a / U.poloidal_z, P);
-    const double a0p = cr_pow(U.poloidal_a, P);
-    const double rp = cr_pow(r, P);
-    const double cabszp = c * cr_pow(fabs(z), P);
+    const double c = W.c_pol;
+    const double a0p = W.a0p;
+    const double rp = pow(r, P);
+    const double cabszp = c * pow(fabs(z), P);
     const double t0 = a0p + cabszp - rp;
     const double t1 = sqrt(uf_sq(t0) + 4 * a0p * rp);
     const double ap = 2 * a0p * rp / (t1 + t0);
@@ -102,25 +103,26 @@ __device__ __forceinline__ u3 uf_poloidal(const crp_uf23_desc &U, double x, doub
     if (ap < 0) {
         if (r > kUfMinNormal) a = __longlong_as_double(0x7ff8000000000000ll);  // the reference throws
     } else {
-        a = cr_pow(ap, 1 / P);
+        a = pow(ap, 1 / P);
     }
     const double radialDependence =
         U.model == CRP_UF23_EXPX ? exp(-a / U.poloidal_r) : 1 - uf_sigmoid(a, U.poloidal_r, U.poloidal_w);
     const double Bzz = U.poloidal_b * radialDependence;
-    const double rOverA = 1 / cr_pow(2 * a0p / (t1 + t0), 1 / P);
+    const double rOverA = 1 / pow(2 * a0p / (t1 + t0), 1 / P);
     const double signZ = z < 0 ? -1 : 1;
-    const double Br = Bzz * c * a / rOverA * signZ * cr_pow(fabs(z), P - 1) / t1;
-    const double Bz = Bzz * cr_pow(rOverA, P - 2) * (ap + a0p) / t1;
+    const double Br = Bzz * c * a / rOverA * signZ * pow(fabs(z), P - 1) / t1;
+    const double Bz = Bzz * pow(rOverA, P - 2) * (ap + a0p) / t1;
     if (r < kUfMinNormal) return {0, 0, Bz};
     return uf_cyl_to_cart(Br, 0, Bz, x / r, y / r);
 }
 
 // getTwistedHaloField (UF23Field.cpp:318)
-__device__ __forceinline__ u3 uf_twisted(const crp_uf23_desc &U, double x, double y, double z) {
+__device__ __forceinline__ u3 uf_twisted(const DevUF23 &W, double x, double y, double z) {
+    const crp_uf23_desc &U = W.d;
     const double r = sqrt(x * x + y * y);
     const double cosPhi = r > kUfMinNormal ? x / r : 1;
     const double sinPhi = r > kUfMinNormal ? y / r : 0;
-    const u3 bX = uf_poloidal(U, x, y, z);
+    const u3 bX = uf_poloidal(W, x, y, z);
     const double bR = bX.x * cosPhi + bX.y * sinPhi;  // uf23::CartToCyl
     const double bZ = bX.z;
     double bPhi = 0;
@@ -143,15 +145,16 @@ __device__ __forceinline__ u3 uf_twisted(const crp_uf23_desc &U, double x, doubl
 // UF23Field::getField (UF23Field.cpp:269) and operator() (:277), [T].
 // Not inlined: one compiled body per unit, and the generic-field kernels keep
 // their register budget.
-static __device__ __noinline__ u3 uf23_field(const crp_uf23_desc &U, double px, double py, double pz) {
+static __device__ __noinline__ u3 uf23_field(const DevUF23 &W, double px, double py, double pz) {
+    const crp_uf23_desc &U = W.d;
     const double x = px / U.kpc * 1, y = py / U.kpc * 1, z = pz / U.kpc * 1;
     if (x * x + y * y + z * z > U.max_radius_squared) return {0, 0, 0};
     const u3 d = U.model == CRP_UF23_SPUR ? uf_spur(U, x, y, z) : uf_spiral(U, x, y, z);
     u3 h;
     if (U.model == CRP_UF23_TWISTX) {
-        h = uf_twisted(U, x, y, z);
+        h = uf_twisted(W, x, y, z);
     } else {
-        const u3 t = uf_toroidal(U, x, y, z), p = uf_poloidal(U, x, y, z);
+        const u3 t = uf_toroidal(U, x, y, z), p = uf_poloidal(W, x, y, z);
         h = {t.x + p.x, t.y + p.y, t.z + p.z};
     }
     return {(d.x + h.x) * U.microgauss, (d.y + h.y) * U.microgauss, (d.z + h.z) * U.microgauss};
