@@ -30,7 +30,6 @@ SOURCES = {
     "step_fp64.cu": ["-fmad=false"],
     "step_mixed.cu": [],
     "adjoint.cu": [],
-    "persistent.cu": [],
     "turbulence.cu": [],
     "crp_engine.cu": [],
     "noalloc.cu": [],
@@ -72,7 +71,10 @@ def build(verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     nvcc = _nvcc()
-    present = {s: f for s, f in SOURCES.items() if os.path.exists(os.path.join(CSRC, s))}
+    missing = [s for s in SOURCES if not os.path.exists(os.path.join(CSRC, s))]
+    if missing:
+        raise RuntimeError(f"engine sources missing: {missing}")
+    present = SOURCES
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda kv: _compile(nvcc, kv[0], kv[1], verbose), present.items()))
         pobjs = list(ex.map(lambda kv: _compile(nvcc, kv[0], kv[1], verbose), PEAKS_SOURCES.items()))
