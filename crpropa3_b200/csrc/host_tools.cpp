@@ -6,12 +6,14 @@
 //   * particle charge (ParticleState::setId, ParticleState.cpp:50);
 //   * the TextOutput line formatter (TextOutput.cpp:55, :166).
 // No device is needed for any of these.
+#include <algorithm>
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <zlib.h>
@@ -146,26 +148,45 @@ crp_status crp_random_draws(uint32_t seed, int32_t kind, uint64_t n, double a, d
 crp_status crp_turbulence_draws(uint32_t seed, int32_t kind, uint64_t n_modes, double *out) {
     if (!out && n_modes) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
     if (seed == 0) return host_fail(CRP_ERR_INVALID_ARGUMENT, "seed 0 is not reproducible; give a non-zero seed");
+    if (kind < CRP_TURBULENCE_GRID || kind > CRP_TURBULENCE_HELICAL)
+        return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown turbulence kind");
+    // The MT19937 stream is sequential, the conversions of its words are not: the words are
+    // drawn first (rand takes one, randNorm two), then converted on all host threads, which
+    // gives the same values as drawing the conversions one after another.
+    const int words = kind == CRP_TURBULENCE_GRID ? 2 : 4;
+    std::vector<uint32_t> u((size_t)words * n_modes);
     Mt r(seed);
-    for (uint64_t i = 0; i < n_modes; i++) {
-        switch (kind) {
-        case CRP_TURBULENCE_GRID:  // GridTurbulence.cpp:97, :104
-            out[2 * i] = r.rand();
-            out[2 * i + 1] = r.rand();
-            break;
-        case CRP_TURBULENCE_SIMPLE:  // SimpleGridTurbulence.cpp:88-93
-            out[3 * i] = r.rand();
-            out[3 * i + 1] = r.norm();
-            out[3 * i + 2] = r.rand();
-            break;
-        case CRP_TURBULENCE_HELICAL:  // HelicalGridTurbulence.cpp:88-92
-            out[3 * i] = r.norm();
-            out[3 * i + 1] = r.rand();
-            out[3 * i + 2] = r.rand();
-            break;
-        default: return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown turbulence kind");
+    for (size_t i = 0; i < u.size(); i++) u[i] = r.u32();
+    auto rand_of = [](uint32_t w) { return double(w) * (1.0 / 4294967295.0); };   // Random::rand
+    auto norm_of = [](uint32_t w1, uint32_t w2) {                                   // randNorm(0, 1)
+        const double r1 = std::sqrt(-2.0 * std::log(1.0 - (double(w1) + 0.5) * (1.0 / 4294967296.0))) * 1.0;
+        const double phi = 2.0 * 3.14159265358979323846264338328 * (double(w2) * (1.0 / 4294967296.0));
+        return 0.0 + r1 * std::cos(phi);
+    };
+    auto convert = [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t i = lo; i < hi; i++) {
+            const uint32_t *w = &u[(size_t)words * i];
+            if (kind == CRP_TURBULENCE_GRID) {          // GridTurbulence.cpp:97, :104
+                out[2 * i] = rand_of(w[0]);
+                out[2 * i + 1] = rand_of(w[1]);
+            } else if (kind == CRP_TURBULENCE_SIMPLE) { // SimpleGridTurbulence.cpp:88-93
+                out[3 * i] = rand_of(w[0]);
+                out[3 * i + 1] = norm_of(w[1], w[2]);
+                out[3 * i + 2] = rand_of(w[3]);
+            } else {                                    // HelicalGridTurbulence.cpp:88-92
+                out[3 * i] = norm_of(w[0], w[1]);
+                out[3 * i + 1] = rand_of(w[2]);
+                out[3 * i + 2] = rand_of(w[3]);
+            }
         }
-    }
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = n_modes < (1u << 16) ? 1u : std::min(hw, 32u);
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt; t++)
+        pool.emplace_back(convert, n_modes * t / nt, n_modes * (t + 1) / nt);
+    convert(0, n_modes / nt);
+    for (auto &th : pool) th.join();
     return CRP_OK;
 }
 
