@@ -48,12 +48,15 @@ def _mt_rand(seed: int, count: int) -> np.ndarray:
 
 
 def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0, seed=42,
-           draws=None, kind=None):
+           draws=None, kind=None, helicity=0.0):
     """The three complex (n, n, n/2+1) arrays B(k) of initTurbulence.
     `draws(seed, count)` returns count Random::rand() values (default: the
     engine's MT19937).  kind TURBULENCE_SIMPLE builds SimpleGridTurbulence's
     instead (SimpleGridTurbulence.cpp:62-95): amplitude randNorm() k^(alpha/2)
-    with alpha = -sindex - 2, draws rand, randNorm, rand per mode."""
+    with alpha = -sindex - 2, draws rand, randNorm, rand per mode;
+    TURBULENCE_HELICAL HelicalGridTurbulence's (HelicalGridTurbulence.cpp:
+    60-116): two helical components of amplitudes mu0 / (4 pi k^3)
+    sqrt((1 +- H) / 2) |randNorm() k^(alpha/2)| and phases 2 pi rand."""
     if seed == 0:
         raise ValueError("seed 0 means a random seed in the reference; give a non-zero seed")
     check_grid_requirements(n, spacing, lmin, lmax)
@@ -66,7 +69,10 @@ def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex
     keep = ~((k.astype(np.float64) < kmin) | (k.astype(np.float64) > kmax))
     m = int(keep.sum())
     simple = kind == _abi.TURBULENCE_SIMPLE
-    if simple:
+    helical = kind == _abi.TURBULENCE_HELICAL
+    if helical:
+        d = turbulence_draws(seed, _abi.TURBULENCE_HELICAL, m)
+    elif simple:
         d = turbulence_draws(seed, _abi.TURBULENCE_SIMPLE, m)
         theta, norm, phase = 2 * math.pi * d[:, 0], d[:, 1], 2 * math.pi * d[:, 2]
     else:
@@ -83,11 +89,31 @@ def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex
     with np.errstate(invalid="ignore", divide="ignore"):
         cosd = ((kx + ky + kz) / np.sqrt(np.float32(3)) / kk).astype(np.float32)
         ang = np.where(cosd >= 1, 0, np.arccos(np.clip(cosd, -1, 1)))
-    par = ang < 1e-3
+    par = ang < (1e-3 if helical else np.float32(1e-3))
     e1[par] = np.array([-1, 1, 0], np.float32)
     e2[par] = np.array([1, 1, -2], np.float32)
     e1 /= np.sqrt((e1 * e1).sum(1))[:, None].astype(np.float32)
     e2 /= np.sqrt((e2 * e2).sum(1))[:, None].astype(np.float32)
+    if helical:
+        k64 = kk.astype(np.float64)
+        mu0 = 4 * math.pi * 1e-7
+        pre = mu0 / (4 * math.pi * k64 ** 3)
+        tot = np.abs(d[:, 0] * np.power(k64, (-sindex - 2) / 2))
+        bp = pre * math.sqrt((1 + helicity) / 2) * tot
+        bm = pre * math.sqrt((1 - helicity) / 2) * tot
+        tp, tm = 2 * math.pi * d[:, 1], 2 * math.pi * d[:, 2]
+        ctp, stp, ctm, stm = np.cos(tp), np.sin(tp), np.cos(tm), np.sin(tm)
+        re1, re2 = bp * ctp + bm * ctm, -bp * stp + bm * stm
+        im1, im2 = bp * stp + bm * stm, bp * ctp - bm * ctm
+        s2 = math.sqrt(2.)
+        out = []
+        for a in range(3):
+            arr = np.zeros((n, n, n2), dtype=np.complex64)
+            e1a, e2a = e1[:, a].astype(np.float64), e2[:, a].astype(np.float64)
+            arr[keep] = (((re1 * e1a + re2 * e2a) / s2).astype(np.float32) +
+                         1j * ((im1 * e1a + im2 * e2a) / s2).astype(np.float32))
+            out.append(arr)
+        return out
     b = (e1 * np.cos(theta).astype(np.float32)[:, None] +
          e2 * np.sin(theta).astype(np.float32)[:, None]).astype(np.float32)
     if simple:
@@ -107,10 +133,11 @@ def kspace(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex
 
 
 def grid_turbulence(n, spacing, brms, lmin, lmax, lbendover=1.0, sindex=5.0 / 3.0, qindex=4.0,
-                    seed=42, device=None, draws=None, kind=None) -> np.ndarray:
+                    seed=42, device=None, draws=None, kind=None, helicity=0.0) -> np.ndarray:
     """(n, n, n, 3) float32 Grid3f values of GridTurbulence(spectrum, grid,
-    seed), or of SimpleGridTurbulence with kind TURBULENCE_SIMPLE."""
-    bk = kspace(n, spacing, brms, lmin, lmax, lbendover, sindex, qindex, seed, draws, kind)
+    seed), or of SimpleGridTurbulence (kind TURBULENCE_SIMPLE) or
+    HelicalGridTurbulence (kind TURBULENCE_HELICAL, helicity H)."""
+    bk = kspace(n, spacing, brms, lmin, lmax, lbendover, sindex, qindex, seed, draws, kind, helicity)
     comps = []
     use_torch = False
     if device is not None:

@@ -70,11 +70,23 @@ def _spectral(g):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["grid", "simple"])
+@pytest.mark.parametrize("kind", ["grid", "simple", "helical"])
 def test_device_turbulence_matches_host_restatement(kind):
-    g = T.grid_turbulence_device(KINDS[kind], N, SPACING, BRMS, LMIN, LMAX, seed=42).cpu().numpy()
-    h = T.grid_turbulence(N, SPACING, BRMS, LMIN, LMAX, seed=42, kind=KINDS[kind])
+    g = T.grid_turbulence_device(KINDS[kind], N, SPACING, BRMS, LMIN, LMAX, seed=42, helicity=0.5).cpu().numpy()
+    h = T.grid_turbulence(N, SPACING, BRMS, LMIN, LMAX, seed=42, kind=KINDS[kind], helicity=0.5)
     np.testing.assert_allclose(g, h, rtol=0, atol=1e-4 * BRMS)
+
+
+def test_host_helical_turbulence_helicity_sign():
+    """The host restatement of HelicalGridTurbulence: opposite signs of the
+    spectral helicity for H = +1 and H = -1, rms = Brms."""
+    out = []
+    for h in (1.0, -1.0):
+        g = T.grid_turbulence(N, SPACING, BRMS, LMIN, LMAX, seed=9, kind=_abi.TURBULENCE_HELICAL, helicity=h)
+        assert abs(np.sqrt((g.astype(np.float64) ** 2).sum(-1).mean()) / BRMS - 1) < 1e-6
+        bk, kv = _spectral(g)
+        out.append(float(np.imag((kv * np.cross(np.conj(bk), bk)).sum(-1)).sum()))
+    assert out[0] * out[1] < 0
 
 
 @pytest.mark.gpu
