@@ -2,9 +2,16 @@
 
 Default workload (grid_bp_256): fixed-step PropagationBP (1 kpc, 5000 steps)
 of 10^6 protons (log-uniform 1-100 EeV, isotropic, from the origin) through a
-256^3 Kolmogorov Grid3f (201 MB float32, 5 kpc spacing, periodic, Brms 10 nG,
-lMin 10 kpc, lMax 500 kpc, seed 42).  One bench step = one full pass of that
-batch (every candidate to MaximumTrajectoryLength).
+256^3 turbulent Grid3f (GridTurbulence with TurbulenceSpectrum(Brms 10 nG,
+lMin 10 kpc, lMax 500 kpc) defaults, 201 MB float32, 5 kpc spacing,
+periodic, seed 42).  One bench step = one full pass of that batch (every
+candidate to MaximumTrajectoryLength).
+
+`configs` adds the other configurations, each timed on the device: the 64^3
+Cash-Karp run (10^4 and 2^20 candidates), the nuclei run (step-capped), the
+DiffusionSDE galactic run (step-capped), JF12 and UF23 backtracking (full
+runs, beside the reference's CPU rate on a sample) and the device turbulence
+generation.
 
 Headline `value`: the mixed-precision form, state resident in HBM.  The same
 line carries the FP64 form's rate, the mixed form's per-candidate error
