@@ -243,38 +243,48 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         if (!w.xi || !w.kappa || !w.k || !w.beta || !w.ak)
             return fail(CRP_ERR_INVALID_ARGUMENT, "PlaneWaveTurbulence: mode arrays missing");
         int n = w.n_modes;
-        std::vector<double> m9((size_t)n * 9), kk((size_t)n * 4);
-        std::vector<float4> a32((size_t)n);
+        std::vector<double> m9((size_t)n * 9);
+        // mixed form, per pair of modes (a, b): {kx_a, ky_a, kz_a, kx_b, ky_b, kz_b} as doubles
+        // (k kappa / 2 pi times 2^32: the phase in turns as 32-bit fixed point, exact scaling),
+        // then {beta_a, beta_b} as unsigned 32-bit fixed-point turns and {A xi_a, A xi_b} as
+        // floats: 48 + 8 + 24 = 80 bytes, five 16-byte loads
+        const int npairs = (n + 1) / 2;
+        std::vector<float4> pairs((size_t)npairs * 5);
+        std::memset(pairs.data(), 0, pairs.size() * sizeof(float4));
+        double ksum = 0;
         for (int i = 0; i < n; i++) {
             for (int a = 0; a < 3; a++) {
                 m9[9 * i + a] = w.xi[3 * i + a];
                 m9[9 * i + 3 + a] = w.kappa[3 * i + a];
-                // mixed form: phase in turns, k kappa / 2 pi, times 2^32 (exact)
-                kk[4 * i + a] = w.k[i] * w.kappa[3 * i + a] * kInv2Pi * kTurnScale;
             }
             m9[9 * i + 6] = w.k[i];
             m9[9 * i + 7] = w.beta[i];
             m9[9 * i + 8] = w.ak[i];
-            kk[4 * i + 3] = w.beta[i] * kInv2Pi * kTurnScale;
-            a32[i] = make_float4((float)(w.ak[i] * w.xi[3 * i]), (float)(w.ak[i] * w.xi[3 * i + 1]),
-                                 (float)(w.ak[i] * w.xi[3 * i + 2]), 0.f);
+            const int q = i / 2, h = i % 2;
+            double *kd = reinterpret_cast<double *>(&pairs[(size_t)q * 5]);
+            uint32_t *bu = reinterpret_cast<uint32_t *>(&pairs[(size_t)q * 5 + 3]);
+            float *af = reinterpret_cast<float *>(&pairs[(size_t)q * 5 + 3]) + 2;
+            double s = 0;
+            for (int a = 0; a < 3; a++) {
+                kd[3 * h + a] = w.k[i] * w.kappa[3 * i + a] * kInv2Pi * kTurnScale;
+                s += std::fabs(kd[3 * h + a]);
+                af[3 * h + a] = (float)(w.ak[i] * w.xi[3 * i + a]);
+            }
+            ksum = std::max(ksum, s);
+            // beta / 2 pi in [0, 1) turns, as 32-bit fixed point
+            double bt = w.beta[i] * kInv2Pi;
+            bt -= std::floor(bt);
+            bu[h] = (uint32_t)(int64_t)std::llround(bt * kTurnScale);
         }
         crp_status st = upload(p, m9.data(), m9.size(), &d.pw.modes);
         if (st) return st;
-        st = upload(p, kk.data(), kk.size(), &d.pw.kk);
-        if (st) return st;
-        st = upload(p, a32.data(), a32.size(), &d.pw.modes32);
+        st = upload(p, pairs.data(), pairs.size(), &d.pw.pairs);
         if (st) return st;
         d.pw.n = n;
-        // the fixed-point phase of the mixed form needs |phase * 2^32| < 2^50 for every mode:
-        // |k kappa . x| + |beta| <= max_i (|kx| + |ky| + |kz|) max(|x|, |y|, |z|) + max |beta|
-        double ksum = 0, bmax = 0;
-        for (int i = 0; i < n; i++) {
-            ksum = std::max(ksum, std::fabs(kk[4 * i]) + std::fabs(kk[4 * i + 1]) + std::fabs(kk[4 * i + 2]));
-            bmax = std::max(bmax, std::fabs(kk[4 * i + 3]));
-        }
-        const double room = 1125899906842624.0 - bmax;  // 2^50
-        d.pw.fast_limit = (ksum > 0 && room > 0) ? room / ksum : (room > 0 ? INFINITY : 0.0);
+        d.pw.npairs = npairs;
+        // the fixed-point phase needs |k kappa . x * 2^32 / 2 pi| < 2^50 for every mode:
+        // max_i (|kx| + |ky| + |kz|) max(|x|, |y|, |z|) < 2^50
+        d.pw.fast_limit = ksum > 0 ? 1125899906842624.0 / ksum : INFINITY;
     } else if (f.kind == CRP_FIELD_JF12) {
         const crp_jf12_desc &J = f.jf12;
         if (!(J.kpc > 0)) return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: parameters not set (crp_jf12_defaults)");

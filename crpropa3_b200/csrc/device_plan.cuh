@@ -32,9 +32,9 @@ struct DevGrid {
 
 struct DevPlaneWave {
     const double *modes;   // FP64 form: per mode {xi x y z, kappa x y z, k, beta, Ak} (9 doubles)
-    const float4 *modes32; // mixed form: per mode {k*kappa (FP64 split), Ak*xi} (see step_mixed.cu)
-    const double *kk;      // mixed form: per mode k*kappa and beta in turns (over 2 pi) times 2^32, 4 doubles
-    int n;
+    const float4 *pairs;   // mixed form: the modes in pairs, 80 B = 5 x 16 B per pair (step_mixed.cu)
+    int n;                 // modes
+    int npairs;            // (n + 1) / 2; an odd count ends with a zero-amplitude mode
     double fast_limit;     // mixed form: max(|x|, |y|, |z|) below which every scaled phase stays under 2^50
 };
 

@@ -140,81 +140,73 @@ __device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
 // turns at kpc distances and pc wavelengths, where FP32 would keep no
 // fraction); its fraction f = p - rint(p) is exact in FP64, and the FP32
 // hardware cosine takes 2 pi f.  Amplitudes A xi and the sums are FP32.
-// Table per mode: kk = {k kappa / 2 pi, beta / 2 pi} (FP64), modes32 =
-// {A xi, 0} (FP32).  Two accumulator sets halve the dependence chain of the
-// sums.  The table is read from global memory (read-only path) or from a
-// copy a kernel staged in shared memory.
+// The table holds the modes in pairs (a, b), 80 bytes = five 16-byte loads:
+// {k kappa / 2 pi times 2^32} of a and b as six FP64, then beta / 2 pi of a
+// and b as unsigned 32-bit fixed-point turns, then A xi of a and b as six
+// FP32.  An odd mode count ends with a zero-amplitude mode.  Two accumulator
+// sets (one per mode of a pair) halve the dependence chain of the sums.  The
+// table is read from global memory (read-only path) or from a copy a kernel
+// staged in shared memory.
 struct PwTab {
-    const double2 *kk;
-    const float4 *a;
-    int n;
+    const float4 *pairs;
+    int npairs;
     double fast_limit;
 };
 
-// cos(2 pi p) for a phase p in turns given as p * 2^32 (the mode table's scale).
-// FAST (|p * 2^32| < 2^50): adding 1.5 * 2^52 rounds p * 2^32 to an integer whose
-// low 32 bits are the fraction of a turn in fixed point; its top 23 bits, shifted
-// by half a turn, become a float in [-1/2, 1/2) through the exponent bits of 1.0
-// (no conversion instruction, 2^-23-turn steps, rounded).  Otherwise the FP64
-// fraction p - rint(p) rounded to FP32.
+// cos(2 pi (p + beta)) for a phase p in turns given as p * 2^32 (the table's
+// scale) and beta in 32-bit fixed-point turns.  FAST (|p * 2^32| < 2^50):
+// adding 1.5 * 2^52 rounds p * 2^32 to an integer whose low 32 bits are the
+// fraction of a turn in fixed point; beta is added there (mod 2^32), and the
+// sum's top 23 bits, shifted by half a turn, become a float in [-1/2, 1/2)
+// through the exponent bits of 1.0 (no conversion instruction, 2^-23-turn
+// steps, rounded).  Otherwise the FP64 fraction of p + beta rounded to FP32.
 template <bool FAST>
-__device__ __forceinline__ float cos_turns(double ps) {
+__device__ __forceinline__ float cos_turns(double ps, unsigned beta) {
     const float twopi = 6.28318530717958647692f;
     if (FAST) {
-        const unsigned lo = (unsigned)__double2loint(ps + 6755399441055744.0);
+        const unsigned lo = (unsigned)__double2loint(ps + 6755399441055744.0) + beta;
         const float f = __int_as_float(0x3f800000u | (((lo + 256u) ^ 0x80000000u) >> 9)) - 1.5f;
         return __cosf(twopi * f);
     }
-    const double p = ps * 2.3283064365386962890625e-10;  // 2^-32, exact
+    const double p = (ps + (double)beta) * 2.3283064365386962890625e-10;  // 2^-32, exact
     return __cosf(twopi * (float)(p - rint(p)));
 }
 
 template <bool SHARED, bool FAST>
-__device__ __forceinline__ f3 pw_sum_t(const double2 *kk, const float4 *am, int n, double x, double y,
-                                       double z) {
+__device__ __forceinline__ f3 pw_sum_t(const float4 *tab, int npairs, double x, double y, double z) {
     float bx0 = 0.f, by0 = 0.f, bz0 = 0.f, bx1 = 0.f, by1 = 0.f, bz1 = 0.f;
-    const int n2 = n & ~1;
 #pragma unroll 4
-    for (int i = 0; i < n2; i += 2) {
-        double2 m0, m1, m2, m3;
-        float4 a, b;
+    for (int q = 0; q < npairs; q++) {
+        const double2 *kd = reinterpret_cast<const double2 *>(tab + 5 * q);
+        double2 k0, k1, k2;
+        float4 u, v;
         if (SHARED) {
-            m0 = kk[2 * i]; m1 = kk[2 * i + 1]; m2 = kk[2 * i + 2]; m3 = kk[2 * i + 3];
-            a = am[i]; b = am[i + 1];
+            k0 = kd[0]; k1 = kd[1]; k2 = kd[2];
+            u = tab[5 * q + 3]; v = tab[5 * q + 4];
         } else {
-            m0 = __ldg(kk + 2 * i); m1 = __ldg(kk + 2 * i + 1);
-            m2 = __ldg(kk + 2 * i + 2); m3 = __ldg(kk + 2 * i + 3);
-            a = __ldg(am + i); b = __ldg(am + i + 1);
+            k0 = __ldg(kd); k1 = __ldg(kd + 1); k2 = __ldg(kd + 2);
+            u = __ldg(tab + 5 * q + 3); v = __ldg(tab + 5 * q + 4);
         }
-        const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
-        const double p1 = fma(m2.x, x, fma(m2.y, y, fma(m3.x, z, m3.y)));
-        const float c0 = cos_turns<FAST>(p0);
-        const float c1 = cos_turns<FAST>(p1);
-        bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
-        bx1 = fmaf(b.x, c1, bx1); by1 = fmaf(b.y, c1, by1); bz1 = fmaf(b.z, c1, bz1);
-    }
-    if (n2 < n) {
-        const double2 m0 = SHARED ? kk[2 * n2] : __ldg(kk + 2 * n2);
-        const double2 m1 = SHARED ? kk[2 * n2 + 1] : __ldg(kk + 2 * n2 + 1);
-        const float4 a = SHARED ? am[n2] : __ldg(am + n2);
-        const double p0 = fma(m0.x, x, fma(m0.y, y, fma(m1.x, z, m1.y)));
-        const float c0 = cos_turns<FAST>(p0);
-        bx0 = fmaf(a.x, c0, bx0); by0 = fmaf(a.y, c0, by0); bz0 = fmaf(a.z, c0, bz0);
+        const double p0 = fma(k0.x, x, fma(k0.y, y, k1.x * z));
+        const double p1 = fma(k1.y, x, fma(k2.x, y, k2.y * z));
+        const float c0 = cos_turns<FAST>(p0, __float_as_uint(u.x));
+        const float c1 = cos_turns<FAST>(p1, __float_as_uint(u.y));
+        bx0 = fmaf(u.z, c0, bx0); by0 = fmaf(u.w, c0, by0); bz0 = fmaf(v.x, c0, bz0);
+        bx1 = fmaf(v.y, c1, bx1); by1 = fmaf(v.z, c1, by1); bz1 = fmaf(v.w, c1, bz1);
     }
     return f3mk(bx0 + bx1, by0 + by1, bz0 + bz1);
 }
 
 template <bool SHARED>
-__device__ __forceinline__ f3 pw_sum(const double2 *kk, const float4 *am, int n, double lim, double x,
-                                     double y, double z) {
-    if (fmax(fabs(x), fmax(fabs(y), fabs(z))) < lim) return pw_sum_t<SHARED, true>(kk, am, n, x, y, z);
-    return pw_sum_t<SHARED, false>(kk, am, n, x, y, z);
+__device__ __forceinline__ f3 pw_sum(const float4 *tab, int npairs, double lim, double x, double y, double z) {
+    if (fmax(fabs(x), fmax(fabs(y), fabs(z))) < lim) return pw_sum_t<SHARED, true>(tab, npairs, x, y, z);
+    return pw_sum_t<SHARED, false>(tab, npairs, x, y, z);
 }
 
 __device__ __forceinline__ f3 plane_wave_field(const DevPlaneWave &w, double x, double y, double z,
                                                const PwTab *sh = nullptr) {
-    if (sh) return pw_sum<true>(sh->kk, sh->a, sh->n, sh->fast_limit, x, y, z);
-    return pw_sum<false>(reinterpret_cast<const double2 *>(w.kk), w.modes32, w.n, w.fast_limit, x, y, z);
+    if (sh) return pw_sum<true>(sh->pairs, sh->npairs, sh->fast_limit, x, y, z);
+    return pw_sum<false>(w.pairs, w.npairs, w.fast_limit, x, y, z);
 }
 
 // ---------------------------------------------------------------- JF12Field
@@ -853,16 +845,13 @@ __global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_k
                                                                const uint32_t *perm, uint32_t *perm_out,
                                                                int pw_field) {
     extern __shared__ __align__(16) unsigned char pw_smem[];
-    PwTab tab{nullptr, nullptr, 0, 0.0};
+    PwTab tab{nullptr, 0, 0.0};
     if (pw_field >= 0) {
         const DevPlaneWave &w = P.fields[pw_field].pw;
-        double2 *kk = reinterpret_cast<double2 *>(pw_smem);
-        float4 *am = reinterpret_cast<float4 *>(pw_smem + (size_t)w.n * 32);
-        const double2 *gk = reinterpret_cast<const double2 *>(w.kk);
-        for (int q = threadIdx.x; q < 2 * w.n; q += blockDim.x) kk[q] = __ldg(gk + q);
-        for (int q = threadIdx.x; q < w.n; q += blockDim.x) am[q] = __ldg(w.modes32 + q);
+        float4 *t4 = reinterpret_cast<float4 *>(pw_smem);
+        for (int q = threadIdx.x; q < 5 * w.npairs; q += blockDim.x) t4[q] = __ldg(w.pairs + q);
         __syncthreads();
-        tab = PwTab{kk, am, w.n, w.fast_limit};
+        tab = PwTab{t4, w.npairs, w.fast_limit};
     }
     const PwTab *sh = pw_field >= 0 ? &tab : nullptr;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1027,8 +1016,8 @@ cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, 
     for (int f = 0; f < P.n_fields; f++)
         if (P.fields[f].kind == CRP_FIELD_PLANE_WAVE) { pw_field = f; n_pw++; }
     size_t smem = 0;
-    if (n_pw == 1 && (size_t)P.fields[pw_field].pw.n * 48 <= 96 * 1024)
-        smem = (size_t)P.fields[pw_field].pw.n * 48;
+    if (n_pw == 1 && (size_t)P.fields[pw_field].pw.npairs * 80 <= 96 * 1024)
+        smem = (size_t)P.fields[pw_field].pw.npairs * 80;
     else
         pw_field = -1;
 #define CRP_SDE_COOP(FSV)                                                                              \

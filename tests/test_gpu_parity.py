@@ -145,8 +145,9 @@ def test_field_eval_mixed_close(oracle):
     pos = rng.uniform(-300, 300, (2000, 3)) * U.kpc
     xi, kappa, k, beta, ak = oracle.plane_wave_modes(1e-13, 10 * U.kpc, 300 * U.kpc, 1.0, 5 / 3, 4, 256, 9)
     Plan = _engine()
+    odd = [xi[:3 * 255], kappa[:3 * 255], k[:255], beta[:255], ak[:255]]  # the mixed table pads to pairs
     for fields in ([P.GridField(grid, (0, 0, 0), (10 * U.kpc,) * 3)],
-                   [P.PlaneWaveField(xi, kappa, k, beta, ak)]):
+                   [P.PlaneWaveField(xi, kappa, k, beta, ak)], [P.PlaneWaveField(*odd)]):
         spec = P.ChainSpec(fields, [bp_fixed(U.kpc)], precision=_abi.PRECISION_MIXED)
         ref = oracle.field(spec, pos)
         got = Plan(spec).field(pos)
