@@ -379,6 +379,7 @@ def secondary_configs(dev, peaks):
     out.update(cfg_sde_galactic(dev, peaks))
     out.update(cfg_jf12_backtrack(dev, peaks))
     out.update(cfg_jf12_backtrack(dev, peaks, model="uf23"))
+    out.update(cfg_jf12_backtrack(dev, peaks, model="pt11"))
     out.update(cfg_turbulence(dev))
     return out
 
@@ -479,11 +480,11 @@ def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
 
 def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
     """PropagationCK backtracking through the JF12 regular field (or the UF23
-    base model), full runs, FP64 and mixed forms, beside the reference's own
-    CPU run of a sample."""
+    base model, or PT11Field), full runs, FP64 and mixed forms, beside the
+    reference's own CPU run of a sample."""
     from crpropa3_b200 import _abi, engine, workloads as W
-    make = W.jf12_backtrack if model == "jf12" else W.uf23_backtrack
-    field = "JF12Field (regular)" if model == "jf12" else "UF23Field (base)"
+    make = {"jf12": W.jf12_backtrack, "uf23": W.uf23_backtrack, "pt11": W.pt11_backtrack}[model]
+    field = {"jf12": "JF12Field (regular)", "uf23": "UF23Field (base)", "pt11": "PT11Field (ASS + halo)"}[model]
     res = {"workload": f"{n} antiprotons 5-100 EeV from (-8.5 kpc, 0, 0), {field}, "
                        "PropagationCK 1e-4 0.1-100 pc, Observer sphere 20 kpc, full runs"}
     for prec, name in ((_abi.PRECISION_FP64, "fp64"), (_abi.PRECISION_MIXED, "mixed")):
@@ -565,6 +566,7 @@ def main():
                 "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20)),
                 "jf12_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20)),
                 "uf23_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="uf23"),
+                "pt11_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="pt11"),
                 "turbulence": lambda: cfg_turbulence(dev)}
         if args.workload not in runs:
             log(f"unknown workload {args.workload}")

@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 # crp_status
 OK = 0
@@ -33,8 +33,9 @@ STATUS_NAMES = {
     ERR_NO_DEVICE: "CRP_ERR_NO_DEVICE",
 }
 
-FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID, FIELD_JF12, FIELD_UF23 = \
-    1, 2, 3, 4, 5, 6, 7
+FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID, FIELD_JF12, FIELD_UF23, \
+    FIELD_PT11 = 1, 2, 3, 4, 5, 6, 7, 8
+PT11_ASS, PT11_BSS, PT11_HALO = 0, 1, 2
 UF23_BASE, UF23_NECL, UF23_EXPX, UF23_SPUR, UF23_CRE10, UF23_SYNCG, UF23_TWISTX, UF23_NEBCOR = range(8)
 JF12_VARIANT_JF12, JF12_VARIANT_PLANCK = 0, 1
 INTERPOLATION_TRILINEAR, INTERPOLATION_TRICUBIC, INTERPOLATION_NEAREST_NEIGHBOUR = 0, 1, 2
@@ -97,12 +98,18 @@ class UF23Desc(C.Structure):
                           "microgauss")]
 
 
+class PT11Desc(C.Structure):
+    _fields_ = [("use_ass", C.c_int32), ("use_bss", C.c_int32), ("use_halo", C.c_int32), ("_pad", C.c_int32)] + [
+        (n, _d) for n in ("d", "r_sun", "r_c", "z0_d", "b0_d", "z0_h", "r0_h", "b0_hn", "b0_hs", "z11_h", "z12_h",
+                          "pitch", "cos_pitch", "sin_pitch", "phi", "cos_phi")]
+
+
 class FieldComponent(C.Structure):
     _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
                 ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
                 ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
                 ("toroidal_b0", _d), ("modulation", GridDesc), ("jf12", JF12Desc),
-                ("uf23", UF23Desc)]
+                ("uf23", UF23Desc), ("pt11", PT11Desc)]
 
 
 class FeatureDesc(C.Structure):

@@ -337,6 +337,16 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         h.a0p = std::pow(U.poloidal_a, U.poloidal_p);
         crp_status st = upload(p, &h, 1, &d.uf);
         if (st) return st;
+    } else if (f.kind == CRP_FIELD_PT11) {
+        const crp_pt11_desc &T = f.pt11;
+        if (T.use_ass && T.use_bss)
+            return fail(CRP_ERR_INVALID_ARGUMENT, "PT11Field: ASS and BSS disk both on (crp_pt11_use)");
+        if ((T.use_ass || T.use_bss) && !(T.r_sun > 0))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "PT11Field: parameters not set (crp_pt11_defaults)");
+        if (T.use_halo && !(T.r0_h > 0))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "PT11Field: parameters not set (crp_pt11_defaults)");
+        crp_status st = upload(p, &T, 1, &d.pt);
+        if (st) return st;
     } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {
     } else {
         return fail(CRP_ERR_UNSUPPORTED, "unsupported field kind %d", f.kind);

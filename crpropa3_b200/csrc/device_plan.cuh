@@ -73,6 +73,7 @@ struct DevComponent {
                     // CRP_FIELD_JF12: the striated grid (grid: the turbulent grid)
     const DevJF12 *jf;  // CRP_FIELD_JF12: device copy of the parameters
     const DevUF23 *uf;        // CRP_FIELD_UF23: device copy of the parameters
+    const crp_pt11_desc *pt;  // CRP_FIELD_PT11: device copy of the parameters
 };
 
 struct DevModule {

@@ -326,6 +326,59 @@ crp_status crp_uf23_defaults(int32_t model, crp_uf23_desc *out) {
     return CRP_OK;
 }
 
+// PT11Field::SetParams (PT11Field.cpp:28): the pitch's cosine and sine and the phase PHI of the
+// first reversal, through the C library at run time (volatile: no compile-time folding)
+static void pt11_set_params(crp_pt11_desc &p) {
+    volatile double pitch = p.pitch, d = p.d, r_sun = p.r_sun;
+    p.cos_pitch = std::cos(pitch);
+    p.sin_pitch = std::sin(pitch);
+    p.phi = p.cos_pitch / p.sin_pitch * std::log1p(d / r_sun) - M_PI / 2;
+    volatile double phi = p.phi;
+    p.cos_phi = std::cos(phi);
+}
+
+crp_status crp_pt11_defaults(crp_pt11_desc *out) {
+    if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    const double au = 149597870700.0, parsec = 648000 / M_PI * au, kpc = 1e3 * parsec;
+    const double gauss = 1e-4, muG = 1e-6 * gauss;
+    crp_pt11_desc &p = *out;
+    std::memset(&p, 0, sizeof(p));
+    // PT11Field() (PT11Field.cpp:8-26): ASS disk and halo
+    p.use_ass = 1;
+    p.use_halo = 1;
+    p.d = -0.6 * kpc;
+    p.r_sun = 8.5 * kpc;
+    p.r_c = 5.0 * kpc;
+    p.z0_d = 1.0 * kpc;
+    p.b0_d = 2.0 * muG;
+    p.z0_h = 1.3 * kpc;
+    p.r0_h = 8.0 * kpc;
+    p.b0_hn = 4.0 * muG;
+    p.b0_hs = 4.0 * muG;
+    p.z11_h = 0.25 * kpc;
+    p.z12_h = 0.4 * kpc;
+    return crp_pt11_use(out, CRP_PT11_ASS, 1);
+}
+
+crp_status crp_pt11_use(crp_pt11_desc *io, int32_t which, int32_t use) {
+    if (!io) return host_fail(CRP_ERR_INVALID_ARGUMENT, "io is NULL");
+    const double muG = 1e-6 * 1e-4;
+    crp_pt11_desc &p = *io;
+    if (which == CRP_PT11_HALO) {  // setUseHalo (PT11Field.cpp:66)
+        p.use_halo = use ? 1 : 0;
+        return CRP_OK;
+    }
+    if (which != CRP_PT11_ASS && which != CRP_PT11_BSS) return host_fail(CRP_ERR_INVALID_ARGUMENT, "unknown PT11 switch");
+    const bool ass = which == CRP_PT11_ASS;
+    (ass ? p.use_ass : p.use_bss) = use ? 1 : 0;
+    if (!use) return CRP_OK;
+    (ass ? p.use_bss : p.use_ass) = 0;  // setUseASS (PT11Field.cpp:35) / setUseBSS (:50)
+    p.pitch = (ass ? -5.0 : -6.0) * M_PI / 180;
+    p.b0_hs = (ass ? 2.0 : 4.0) * muG;
+    pt11_set_params(p);
+    return CRP_OK;
+}
+
 crp_status crp_plane_wave_modes(double brms, double lmin, double lmax, double lbendover,
                                 double sindex, double qindex, int32_t nm, int32_t seed,
                                 double *xi, double *kappa, double *k, double *beta, double *ak) {

@@ -20,6 +20,7 @@
 #include "engine_internal.h"
 #include "grid_interp.cuh"
 #include "uf23.cuh"
+#include "pt11.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -326,6 +327,10 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
     case CRP_FIELD_JF12: return jf12_field(f, pos);
     case CRP_FIELD_UF23: {
         const u3 b = uf23_field(*f.uf, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
+    case CRP_FIELD_PT11: {
+        const u3 b = pt11_field(*f.pt, pos.x, pos.y, pos.z);
         return mk(b.x, b.y, b.z);
     }
     default: {

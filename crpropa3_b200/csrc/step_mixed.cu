@@ -18,6 +18,7 @@
 #include "engine_internal.h"
 #include "grid_interp.cuh"
 #include "uf23.cuh"
+#include "pt11.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -372,6 +373,10 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     case CRP_FIELD_JF12: return jf12_field_f(f, x, y, z);
     case CRP_FIELD_UF23: {  // FP64 evaluation (the poloidal halo's powers), FP32 result
         const u3 b = uf23_field(*f.uf, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
+    case CRP_FIELD_PT11: {  // FP64 evaluation, FP32 result
+        const u3 b = pt11_field(*f.pt, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
     }
     default: {

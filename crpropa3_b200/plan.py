@@ -99,6 +99,34 @@ class UF23Field:
         return d
 
 
+@dataclass
+class PT11Field:
+    """PT11Field() (PT11Field.cpp:8), the field of Pshirkov et al. 2011, with
+    its switches: the ASS disk (the default) or the BSS disk, and the halo.
+    As in the reference, switching one disk on switches the other off and
+    sets its pitch and southern halo strength (setUseASS / setUseBSS,
+    PT11Field.cpp:35-64); both on is an error."""
+    use_ass: bool = True
+    use_bss: bool = False
+    use_halo: bool = True
+    periodic: Optional[tuple] = None
+
+    def desc(self) -> "_abi.PT11Desc":
+        """The reference's state after PT11Field() and the setters that give
+        these switches (crp_pt11_defaults, crp_pt11_use)."""
+        if self.use_ass and self.use_bss:
+            raise ValueError("PT11Field: the ASS and BSS disks exclude each other")
+        lib, d = _abi.load(), _abi.PT11Desc()
+        _abi.check(lib.crp_pt11_defaults(C.byref(d)))
+        if self.use_bss:
+            _abi.check(lib.crp_pt11_use(C.byref(d), _abi.PT11_BSS, 1))
+        elif not self.use_ass:
+            _abi.check(lib.crp_pt11_use(C.byref(d), _abi.PT11_ASS, 0))
+        if not self.use_halo:
+            _abi.check(lib.crp_pt11_use(C.byref(d), _abi.PT11_HALO, 0))
+        return d
+
+
 def jf12_random_striated(seed: int) -> ScalarGrid:
     """JF12Field::randomStriated(seed) (JF12Field.cpp:86): a periodic 100^3
     Grid1f at the origin with 0.1 kpc spacing, each cell round(rand()) * 2 - 1
@@ -261,6 +289,9 @@ class ChainSpec:
         elif isinstance(f, UF23Field):
             c.kind = _abi.FIELD_UF23
             c.uf23 = UF23Field.defaults(f.model)
+        elif isinstance(f, PT11Field):
+            c.kind = _abi.FIELD_PT11
+            c.pt11 = f.desc()
         elif isinstance(f, PlaneWaveField):
             c.kind = _abi.FIELD_PLANE_WAVE
             w = c.plane_wave

@@ -10,6 +10,7 @@
 #include "crpropa/magneticField/JF12Field.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
+#include "crpropa/magneticField/PT11Field.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
@@ -89,6 +90,16 @@ CRPGPU_MEMBER(UF23Parameters, UF23Field, UF23Pars, fParameters);
 CRPGPU_MEMBER(UF23SinPitch, UF23Field, double, fSinPitch);
 CRPGPU_MEMBER(UF23CosPitch, UF23Field, double, fCosPitch);
 CRPGPU_MEMBER(UF23TanPitch, UF23Field, double, fTanPitch);
+CRPGPU_MEMBER(PT11UseASS, PT11Field, bool, useASS);                    // PT11Field.h:28-46
+CRPGPU_MEMBER(PT11UseBSS, PT11Field, bool, useBSS);
+CRPGPU_MEMBER(PT11UseHalo, PT11Field, bool, useHalo);
+#define CRPGPU_PT11(TAG, NAME) CRPGPU_MEMBER(TAG, PT11Field, double, NAME)
+CRPGPU_PT11(PT11Pitch, pitch); CRPGPU_PT11(PT11CosPitch, cos_pitch); CRPGPU_PT11(PT11SinPitch, sin_pitch);
+CRPGPU_PT11(PT11Phi, PHI); CRPGPU_PT11(PT11CosPhi, cos_PHI); CRPGPU_PT11(PT11D, d); CRPGPU_PT11(PT11RSun, R_sun);
+CRPGPU_PT11(PT11Rc, R_c); CRPGPU_PT11(PT11Z0D, z0_D); CRPGPU_PT11(PT11B0D, B0_D); CRPGPU_PT11(PT11Z0H, z0_H);
+CRPGPU_PT11(PT11R0H, R0_H); CRPGPU_PT11(PT11B0Hn, B0_Hn); CRPGPU_PT11(PT11B0Hs, B0_Hs);
+CRPGPU_PT11(PT11Z11H, z11_H); CRPGPU_PT11(PT11Z12H, z12_H);
+#undef CRPGPU_PT11
 CRPGPU_MEMBER(TrackCenter, ObserverTracking, Vector3d, center);        // Observer.h:109
 CRPGPU_MEMBER(TrackRadius, ObserverTracking, double, radius);
 CRPGPU_MEMBER(TrackStep, ObserverTracking, double, stepSize);
@@ -286,6 +297,30 @@ struct Translation {
             d.kpc = kpc;
             d.microgauss = microgauss;
             text << "  field: UF23Field model " << d.model;
+        } else if (const PT11Field *t = dynamic_cast<const PT11Field *>(f)) {
+            if (typeid(*f) != typeid(PT11Field)) throw Unsupported(name_of(f) + " (a PT11Field subclass)");
+            crp_pt11_desc &d = c.pt11;
+            c.kind = CRP_FIELD_PT11;
+            d.use_ass = t->*member(PT11UseASS()) ? 1 : 0;
+            d.use_bss = t->*member(PT11UseBSS()) ? 1 : 0;
+            d.use_halo = t->*member(PT11UseHalo()) ? 1 : 0;
+            d.pitch = t->*member(PT11Pitch());
+            d.cos_pitch = t->*member(PT11CosPitch());
+            d.sin_pitch = t->*member(PT11SinPitch());
+            d.phi = t->*member(PT11Phi());
+            d.cos_phi = t->*member(PT11CosPhi());
+            d.d = t->*member(PT11D());
+            d.r_sun = t->*member(PT11RSun());
+            d.r_c = t->*member(PT11Rc());
+            d.z0_d = t->*member(PT11Z0D());
+            d.b0_d = t->*member(PT11B0D());
+            d.z0_h = t->*member(PT11Z0H());
+            d.r0_h = t->*member(PT11R0H());
+            d.b0_hn = t->*member(PT11B0Hn());
+            d.b0_hs = t->*member(PT11B0Hs());
+            d.z11_h = t->*member(PT11Z11H());
+            d.z12_h = t->*member(PT11Z12H());
+            text << "  field: PT11Field ass " << d.use_ass << " bss " << d.use_bss << " halo " << d.use_halo;
         } else if (const PlaneWaveTurbulence *w = dynamic_cast<const PlaneWaveTurbulence *>(f)) {
             const int nm = w->*member(WavesNm());
             const std::vector<Vector3d> &xi = w->*member(WavesXi());

@@ -9,7 +9,7 @@
 //   fields        MagneticFieldGrid over a Grid3f (trilinear, tricubic or
 //                 nearest-neighbour), ModulatedMagneticFieldGrid,
 //                 JF12Field and PlanckJF12bField (regular, striated and
-//                 turbulent parts), UF23Field (all eight models),
+//                 turbulent parts), UF23Field (all eight models), PT11Field,
 //                 PeriodicMagneticField, MagneticFieldList,
 //                 UniformMagneticField, PlaneWaveTurbulence,
 //                 ToroidalMagneticField (below)

@@ -17,6 +17,7 @@ jf12_backtrack: PropagationCK (1e-4, 0.1 pc-100 pc) in the JF12 regular
               detected by an Observer sphere of 20 kpc around the galactic
               centre, MaximumTrajectoryLength 100 kpc (backtracking).
 uf23_backtrack: the same in the UF23Field base model.
+pt11_backtrack: the same in PT11Field (ASS disk and halo).
 Inputs are synthetic and seeded; sizes are scaled down through `n`.
 """
 from __future__ import annotations
@@ -163,3 +164,8 @@ def jf12_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, variant=
 def uf23_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, model=_abi.UF23_BASE):
     """jf12_backtrack with the UF23Field model `model` instead of JF12."""
     return jf12_backtrack(n, precision, seed, field=P.UF23Field(model))
+
+
+def pt11_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7):
+    """jf12_backtrack with PT11Field() (ASS disk and halo) instead of JF12."""
+    return jf12_backtrack(n, precision, seed, field=P.PT11Field())

@@ -5,7 +5,7 @@
  * a chain of one propagation module (PropagationCK, PropagationBP or
  * DiffusionSDE) over a magnetic field (MagneticFieldGrid over a Grid3f,
  * ModulatedMagneticFieldGrid, PeriodicMagneticField, PlaneWaveTurbulence,
- * UniformMagneticField, JF12Field, UF23Field, a MagneticFieldList of those,
+ * UniformMagneticField, JF12Field, UF23Field, PT11Field, a MagneticFieldList of those,
  * or a toroidal field), followed by MaximumTrajectoryLength, Observer and
  * boundary modules, run to completion over a set of candidates.  It replaces, for such chains,
  *
@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 5u
+#define CRP_ABI_VERSION 6u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -59,7 +59,8 @@ enum crp_field_kind {
     CRP_FIELD_MODULATED_GRID = 5, /* ModulatedMagneticFieldGrid: Grid3f times a Grid1f
                                      modulation (MagneticFieldGrid.cpp:51) */
     CRP_FIELD_JF12 = 6,           /* JF12Field / PlanckJF12bField (JF12Field.cpp:8-376) */
-    CRP_FIELD_UF23 = 7            /* UF23Field (UF23Field.cpp:59-558) */
+    CRP_FIELD_UF23 = 7,           /* UF23Field (UF23Field.cpp:59-558) */
+    CRP_FIELD_PT11 = 8            /* PT11Field (PT11Field.cpp:8-130) */
 };
 
 /* UF23Field::ModelType (UF23Field.h), same order. */
@@ -149,6 +150,20 @@ typedef struct crp_uf23_desc {
     double microgauss;                      /* field unit [T] */
 } crp_uf23_desc;
 
+/* State of a PT11Field (PT11Field.h:26-46), SI units: the ASS/BSS disk and
+ * halo switches and the parameters the constructor and the setters set
+ * (PT11Field.cpp:8-64), with SetParams' derived values (PT11Field.cpp:28).
+ * crp_pt11_defaults() and crp_pt11_use() fill it. */
+typedef struct crp_pt11_desc {
+    int32_t use_ass, use_bss, use_halo, _pad;
+    double d, r_sun, r_c, z0_d, b0_d;                     /* disk [m], [T] */
+    double z0_h, r0_h, b0_hn, b0_hs, z11_h, z12_h;        /* halo [m], [T] */
+    double pitch, cos_pitch, sin_pitch, phi, cos_phi;     /* pitch [rad] and SetParams' values */
+} crp_pt11_desc;
+
+/* crp_pt11_use() switches, PT11Field::setUseASS / setUseBSS / setUseHalo. */
+enum crp_pt11_switch { CRP_PT11_ASS = 0, CRP_PT11_BSS = 1, CRP_PT11_HALO = 2 };
+
 /* One summand of the field (a MagneticFieldList of these is their sum,
  * MagneticField.cpp:64).  A component may be wrapped in a
  * PeriodicMagneticField (MagneticField.cpp:41). */
@@ -169,6 +184,7 @@ typedef struct crp_field_component {
     crp_grid3f_desc modulation;
     crp_jf12_desc jf12;
     crp_uf23_desc uf23;
+    crp_pt11_desc pt11;
 } crp_field_component;
 
 /* ------------------------------------------------------------------------
@@ -511,6 +527,14 @@ crp_status crp_jf12_defaults(int32_t variant, crp_jf12_desc *out);
 
 /* The parameters UF23Field(model) sets (UF23Field.cpp:59-266). */
 crp_status crp_uf23_defaults(int32_t model, crp_uf23_desc *out);
+
+/* The state PT11Field() constructs (PT11Field.cpp:8: ASS disk and halo on). */
+crp_status crp_pt11_defaults(crp_pt11_desc *out);
+
+/* PT11Field::setUseASS / setUseBSS / setUseHalo (PT11Field.cpp:35-68):
+ * switching the ASS or BSS disk on switches the other off and sets its pitch
+ * and southern halo strength; switching a disk off changes nothing else. */
+crp_status crp_pt11_use(crp_pt11_desc *io, int32_t which, int32_t use);
 
 /* Turbulent Grid3f generation: GridTurbulence (GridTurbulence.cpp:29-123,
  * TurbulenceSpectrum), SimpleGridTurbulence (SimpleGridTurbulence.cpp:19-115,

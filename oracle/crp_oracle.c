@@ -759,6 +759,35 @@ static v3 uf23_field(const crp_uf23_desc *U, v3 position) {
     return muls(divs(b, 1), U->microgauss);
 }
 
+/* ---------------------------------------------------------------- PT11Field
+ * PT11Field::getField (PT11Field.cpp:80-128), SI units. */
+static v3 pt11_field(const crp_pt11_desc *P, v3 pos) {
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+    v3 b = mk(0, 0, 0);
+    if (P->use_ass || P->use_bss) {
+        /* Vector3::getPhi (Vector3.h:136) */
+        double phi = (fabs(pos.x) < DBL_MIN && fabs(pos.y) < DBL_MIN) ? 0.0 : atan2(pos.y, pos.x);
+        double theta = M_PI - phi;
+        double cos_theta = -pos.x / r;
+        double sin_theta = pos.y / r;
+        b.x = P->sin_pitch * cos_theta - P->cos_pitch * sin_theta;
+        b.y = -P->sin_pitch * sin_theta - P->cos_pitch * cos_theta;
+        b = muls(b, -1);
+        double bMag = cos(theta - P->cos_pitch / P->sin_pitch * log(r / P->r_sun) + P->phi);
+        if (P->use_ass) bMag = fabs(bMag);
+        bMag *= P->b0_d * P->r_sun / (r < P->r_c ? P->r_c : r) / P->cos_phi * exp(-fabs(pos.z) / P->z0_d);
+        b = muls(b, bMag);
+    }
+    if (P->use_halo) {
+        double bMag = pos.z > 0 ? P->b0_hn : -P->b0_hs;
+        double z1 = fabs(pos.z) < P->z0_h ? P->z11_h : P->z12_h;
+        double v = (fabs(pos.z) - P->z0_h) / z1;
+        bMag *= r / P->r0_h * exp(1 - r / P->r0_h) / (1 + v * v); /* pow(v, 2.) is exact: v * v */
+        b = add(b, muls(mk(-pos.y / r, pos.x / r, 0), bMag));
+    }
+    return b;
+}
+
 static v3 component_field(const crp_field_component *f, v3 position) {
     v3 pos = position;
     if (f->periodic) { /* MagneticField.cpp:41 */
@@ -783,6 +812,7 @@ static v3 component_field(const crp_field_component *f, v3 position) {
     case CRP_FIELD_UNIFORM: return mk(f->uniform[0], f->uniform[1], f->uniform[2]);
     case CRP_FIELD_JF12: return jf12_field(f, pos);
     case CRP_FIELD_UF23: return uf23_field(&f->uf23, pos);
+    case CRP_FIELD_PT11: return pt11_field(&f->pt11, pos);
     case CRP_FIELD_TOROIDAL: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f->toroidal_b0 / r);

@@ -42,6 +42,7 @@
 #include "crpropa/magneticField/JF12Field.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
+#include "crpropa/magneticField/PT11Field.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/magneticField/turbulentField/TurbulentField.h"
 #include "crpropa/module/Boundary.h"
@@ -188,6 +189,12 @@ static ref_ptr<MagneticField> build_component(const crp_field_component &f, Buil
         m = jf;
     } else if (f.kind == CRP_FIELD_UF23) {
         m = new UF23Field((UF23Field::ModelType)f.uf23.model);
+    } else if (f.kind == CRP_FIELD_PT11) {  // PT11Field() and the setters that give the switches
+        PT11Field *t = new PT11Field();
+        if (f.pt11.use_bss) t->setUseBSS(true);
+        else if (!f.pt11.use_ass) t->setUseASS(false);
+        if (!f.pt11.use_halo) t->setUseHalo(false);
+        m = t;
     } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
         const crp_plane_wave_desc &p = f.plane_wave;
         TurbulenceSpectrum *spec = new TurbulenceSpectrum(p.brms, p.lmin, p.lmax, p.lbendover,
