@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 # crp_status
 OK = 0
@@ -34,7 +34,7 @@ STATUS_NAMES = {
 }
 
 FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID, FIELD_JF12, FIELD_UF23, \
-    FIELD_PT11 = 1, 2, 3, 4, 5, 6, 7, 8
+    FIELD_PT11, FIELD_ARCHIMEDEAN_SPIRAL = 1, 2, 3, 4, 5, 6, 7, 8, 9
 PT11_ASS, PT11_BSS, PT11_HALO = 0, 1, 2
 UF23_BASE, UF23_NECL, UF23_EXPX, UF23_SPUR, UF23_CRE10, UF23_SYNCG, UF23_TWISTX, UF23_NEBCOR = range(8)
 JF12_VARIANT_JF12, JF12_VARIANT_PLANCK = 0, 1
@@ -104,12 +104,17 @@ class PT11Desc(C.Structure):
                           "pitch", "cos_pitch", "sin_pitch", "phi", "cos_phi")]
 
 
+class ArchimedeanDesc(C.Structure):
+    _fields_ = [("b0", _d), ("r0", _d), ("omega", _d), ("vw", _d)]
+
+
 class FieldComponent(C.Structure):
     _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
                 ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
                 ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
                 ("toroidal_b0", _d), ("modulation", GridDesc), ("jf12", JF12Desc),
-                ("uf23", UF23Desc), ("pt11", PT11Desc)]
+                ("uf23", UF23Desc), ("pt11", PT11Desc),
+                ("archimedean", ArchimedeanDesc)]
 
 
 class FeatureDesc(C.Structure):

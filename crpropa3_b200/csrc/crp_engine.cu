@@ -347,6 +347,8 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             return fail(CRP_ERR_INVALID_ARGUMENT, "PT11Field: parameters not set (crp_pt11_defaults)");
         crp_status st = upload(p, &T, 1, &d.pt);
         if (st) return st;
+    } else if (f.kind == CRP_FIELD_ARCHIMEDEAN_SPIRAL) {
+        d.arch = f.archimedean;
     } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {
     } else {
         return fail(CRP_ERR_UNSUPPORTED, "unsupported field kind %d", f.kind);

@@ -74,6 +74,7 @@ struct DevComponent {
     const DevJF12 *jf;  // CRP_FIELD_JF12: device copy of the parameters
     const DevUF23 *uf;        // CRP_FIELD_UF23: device copy of the parameters
     const crp_pt11_desc *pt;  // CRP_FIELD_PT11: device copy of the parameters
+    crp_archimedean_desc arch;  // CRP_FIELD_ARCHIMEDEAN_SPIRAL
 };
 
 struct DevModule {

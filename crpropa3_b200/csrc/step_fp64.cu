@@ -333,6 +333,10 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
         const u3 b = pt11_field(*f.pt, pos.x, pos.y, pos.z);
         return mk(b.x, b.y, b.z);
     }
+    case CRP_FIELD_ARCHIMEDEAN_SPIRAL: {
+        const u3 b = archimedean_field(f.arch, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
     default: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f.b0 / r);

@@ -379,6 +379,10 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
         const u3 b = pt11_field(*f.pt, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
     }
+    case CRP_FIELD_ARCHIMEDEAN_SPIRAL: {  // FP64 evaluation, FP32 result
+        const u3 b = archimedean_field(f.arch, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
     default: {
         double r = sqrt(fma(x, x, y * y));
         double s = f.b0 / r;

@@ -127,6 +127,18 @@ class PT11Field:
         return d
 
 
+@dataclass
+class ArchimedeanSpiralField:
+    """ArchimedeanSpiralField(B_0, R_0, Omega, V_w) (ArchimedeanSpiralField.cpp:5):
+    a radial field b0 (r0 / r)^2 wound into an Archimedean spiral by the
+    rotation omega over the wind speed vw, reversed below z = 0 (SI units)."""
+    b0: float
+    r0: float
+    omega: float
+    vw: float
+    periodic: Optional[tuple] = None
+
+
 def jf12_random_striated(seed: int) -> ScalarGrid:
     """JF12Field::randomStriated(seed) (JF12Field.cpp:86): a periodic 100^3
     Grid1f at the origin with 0.1 kpc spacing, each cell round(rand()) * 2 - 1
@@ -292,6 +304,10 @@ class ChainSpec:
         elif isinstance(f, PT11Field):
             c.kind = _abi.FIELD_PT11
             c.pt11 = f.desc()
+        elif isinstance(f, ArchimedeanSpiralField):
+            c.kind = _abi.FIELD_ARCHIMEDEAN_SPIRAL
+            c.archimedean.b0, c.archimedean.r0 = float(f.b0), float(f.r0)
+            c.archimedean.omega, c.archimedean.vw = float(f.omega), float(f.vw)
         elif isinstance(f, PlaneWaveField):
             c.kind = _abi.FIELD_PLANE_WAVE
             w = c.plane_wave

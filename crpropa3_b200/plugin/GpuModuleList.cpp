@@ -11,6 +11,7 @@
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/PT11Field.h"
+#include "crpropa/magneticField/ArchimedeanSpiralField.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
@@ -321,6 +322,15 @@ struct Translation {
             d.z11_h = t->*member(PT11Z11H());
             d.z12_h = t->*member(PT11Z12H());
             text << "  field: PT11Field ass " << d.use_ass << " bss " << d.use_bss << " halo " << d.use_halo;
+        } else if (const ArchimedeanSpiralField *a = dynamic_cast<const ArchimedeanSpiralField *>(f)) {
+            if (typeid(*f) != typeid(ArchimedeanSpiralField))
+                throw Unsupported(name_of(f) + " (an ArchimedeanSpiralField subclass)");
+            c.kind = CRP_FIELD_ARCHIMEDEAN_SPIRAL;
+            c.archimedean.b0 = a->getB0();
+            c.archimedean.r0 = a->getR0();
+            c.archimedean.omega = a->getOmega();
+            c.archimedean.vw = a->getVw();
+            text << "  field: ArchimedeanSpiralField";
         } else if (const PlaneWaveTurbulence *w = dynamic_cast<const PlaneWaveTurbulence *>(f)) {
             const int nm = w->*member(WavesNm());
             const std::vector<Vector3d> &xi = w->*member(WavesXi());

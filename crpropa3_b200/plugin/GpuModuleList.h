@@ -10,6 +10,7 @@
 //                 nearest-neighbour), ModulatedMagneticFieldGrid,
 //                 JF12Field and PlanckJF12bField (regular, striated and
 //                 turbulent parts), UF23Field (all eight models), PT11Field,
+//                 ArchimedeanSpiralField,
 //                 PeriodicMagneticField, MagneticFieldList,
 //                 UniformMagneticField, PlaneWaveTurbulence,
 //                 ToroidalMagneticField (below)

@@ -5,7 +5,8 @@
  * a chain of one propagation module (PropagationCK, PropagationBP or
  * DiffusionSDE) over a magnetic field (MagneticFieldGrid over a Grid3f,
  * ModulatedMagneticFieldGrid, PeriodicMagneticField, PlaneWaveTurbulence,
- * UniformMagneticField, JF12Field, UF23Field, PT11Field, a MagneticFieldList of those,
+ * UniformMagneticField, JF12Field, UF23Field, PT11Field, ArchimedeanSpiralField, a
+ * MagneticFieldList of those,
  * or a toroidal field), followed by MaximumTrajectoryLength, Observer and
  * boundary modules, run to completion over a set of candidates.  It replaces, for such chains,
  *
@@ -33,7 +34,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 6u
+#define CRP_ABI_VERSION 7u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -60,7 +61,8 @@ enum crp_field_kind {
                                      modulation (MagneticFieldGrid.cpp:51) */
     CRP_FIELD_JF12 = 6,           /* JF12Field / PlanckJF12bField (JF12Field.cpp:8-376) */
     CRP_FIELD_UF23 = 7,           /* UF23Field (UF23Field.cpp:59-558) */
-    CRP_FIELD_PT11 = 8            /* PT11Field (PT11Field.cpp:8-130) */
+    CRP_FIELD_PT11 = 8,           /* PT11Field (PT11Field.cpp:8-130) */
+    CRP_FIELD_ARCHIMEDEAN_SPIRAL = 9 /* ArchimedeanSpiralField (ArchimedeanSpiralField.cpp:5-49) */
 };
 
 /* UF23Field::ModelType (UF23Field.h), same order. */
@@ -161,6 +163,14 @@ typedef struct crp_pt11_desc {
     double pitch, cos_pitch, sin_pitch, phi, cos_phi;     /* pitch [rad] and SetParams' values */
 } crp_pt11_desc;
 
+/* ArchimedeanSpiralField(B_0, R_0, Omega, V_w) (ArchimedeanSpiralField.h:46), SI units. */
+typedef struct crp_archimedean_desc {
+    double b0;    /* radial field strength at r0 [T] */
+    double r0;    /* reference radius [m] */
+    double omega; /* angular velocity of the rotation [1/s] */
+    double vw;    /* asymptotic wind speed [m/s] */
+} crp_archimedean_desc;
+
 /* crp_pt11_use() switches, PT11Field::setUseASS / setUseBSS / setUseHalo. */
 enum crp_pt11_switch { CRP_PT11_ASS = 0, CRP_PT11_BSS = 1, CRP_PT11_HALO = 2 };
 
@@ -185,6 +195,7 @@ typedef struct crp_field_component {
     crp_jf12_desc jf12;
     crp_uf23_desc uf23;
     crp_pt11_desc pt11;
+    crp_archimedean_desc archimedean;
 } crp_field_component;
 
 /* ------------------------------------------------------------------------

@@ -788,6 +788,26 @@ static v3 pt11_field(const crp_pt11_desc *P, v3 pos) {
     return b;
 }
 
+/* ArchimedeanSpiralField::getField (ArchimedeanSpiralField.cpp:12-46), with
+ * Vector3::getR / getTheta / getPhi (Vector3.h:126-151). */
+static v3 archimedean_field(const crp_archimedean_desc *A, v3 pos) {
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y + pos.z * pos.z);
+    double theta = (fabs(pos.x) < DBL_MIN && fabs(pos.y) < DBL_MIN && fabs(pos.z) < DBL_MIN)
+                       ? 0.0 : atan2(sqrt(pos.x * pos.x + pos.y * pos.y), pos.z);
+    double phi = (fabs(pos.x) < DBL_MIN && fabs(pos.y) < DBL_MIN) ? 0.0 : atan2(pos.y, pos.x);
+    double cos_phi = cos(phi), sin_phi = sin(phi), cos_theta = cos(theta), sin_theta = sin(theta);
+    v3 B = mk(0, 0, 0);
+    double C1 = A->r0 * A->r0 / r / r;
+    B.x += C1 * cos_phi * sin_theta;
+    B.y += C1 * sin_phi * sin_theta;
+    B.z += C1 * cos_theta;
+    double C2 = -(A->omega * A->r0 * A->r0 * sin_theta) / (r * A->vw);
+    B.x += C2 * (-sin_phi);
+    B.y += C2 * cos_phi;
+    if (pos.z < 0.) B = muls(B, -1);
+    return muls(B, A->b0);
+}
+
 static v3 component_field(const crp_field_component *f, v3 position) {
     v3 pos = position;
     if (f->periodic) { /* MagneticField.cpp:41 */
@@ -813,6 +833,7 @@ static v3 component_field(const crp_field_component *f, v3 position) {
     case CRP_FIELD_JF12: return jf12_field(f, pos);
     case CRP_FIELD_UF23: return uf23_field(&f->uf23, pos);
     case CRP_FIELD_PT11: return pt11_field(&f->pt11, pos);
+    case CRP_FIELD_ARCHIMEDEAN_SPIRAL: return archimedean_field(&f->archimedean, pos);
     case CRP_FIELD_TOROIDAL: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f->toroidal_b0 / r);

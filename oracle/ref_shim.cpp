@@ -43,6 +43,7 @@
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/PT11Field.h"
+#include "crpropa/magneticField/ArchimedeanSpiralField.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/magneticField/turbulentField/TurbulentField.h"
 #include "crpropa/module/Boundary.h"
@@ -195,6 +196,9 @@ static ref_ptr<MagneticField> build_component(const crp_field_component &f, Buil
         else if (!f.pt11.use_ass) t->setUseASS(false);
         if (!f.pt11.use_halo) t->setUseHalo(false);
         m = t;
+    } else if (f.kind == CRP_FIELD_ARCHIMEDEAN_SPIRAL) {
+        const crp_archimedean_desc &a = f.archimedean;
+        m = new ArchimedeanSpiralField(a.b0, a.r0, a.omega, a.vw);
     } else if (f.kind == CRP_FIELD_PLANE_WAVE) {
         const crp_plane_wave_desc &p = f.plane_wave;
         TurbulenceSpectrum *spec = new TurbulenceSpectrum(p.brms, p.lmin, p.lmax, p.lbendover,
