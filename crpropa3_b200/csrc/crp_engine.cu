@@ -57,6 +57,25 @@ bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
 
 namespace crp {
 void set_last_error(const char *msg) { g_error = msg; }
+
+// Every array a device entry point reads or writes must be reachable from
+// the device: device memory, managed memory, or host memory registered /
+// allocated with CUDA (mapped).  Ordinary host memory would make the kernels
+// fault.  A null pointer passes (optional arrays).
+crp_status check_device_ptr(const void *ptr, const char *what) {
+    if (!ptr) return CRP_OK;
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CRP_ERR_INVALID_ARGUMENT, "%s: not a CUDA-accessible pointer", what);
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return CRP_OK;
+    if (a.type == cudaMemoryTypeHost && a.devicePointer == ptr) return CRP_OK;
+    return fail(CRP_ERR_INVALID_ARGUMENT,
+                "%s is host memory the device cannot address: pass device arrays to crp_run_device "
+                "(or host arrays to crp_run)", what);
+}
 }  // namespace crp
 
 constexpr double kInv2Pi = 0.15915494309189533577;  // 1 / (2 pi)
@@ -531,24 +550,6 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
 crp_status crp_plan_destroy(crp_plan *plan) {
     delete plan;
     return CRP_OK;
-}
-
-// Every array handed to crp_run_device must be reachable from the device:
-// device memory, managed memory, or host memory registered / allocated with
-// CUDA (mapped).  Ordinary host memory would make the kernels fault.
-static crp_status check_device_ptr(const void *ptr, const char *what) {
-    if (!ptr) return CRP_OK;
-    cudaPointerAttributes a;
-    cudaError_t e = cudaPointerGetAttributes(&a, ptr);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(CRP_ERR_INVALID_ARGUMENT, "%s: not a CUDA-accessible pointer", what);
-    }
-    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return CRP_OK;
-    if (a.type == cudaMemoryTypeHost && a.devicePointer == ptr) return CRP_OK;
-    return fail(CRP_ERR_INVALID_ARGUMENT,
-                "%s is host memory the device cannot address: pass device arrays to crp_run_device "
-                "(or host arrays to crp_run)", what);
 }
 
 static crp_status check_device_arrays(const crp_candidates *c, const crp_records *r) {

@@ -2,11 +2,10 @@
 // Grid3f with MaximumTrajectoryLength, for callers that cannot allocate
 // device memory.
 //
-// Who needs it: code that runs where cudaMalloc is off limits -- inside a
-// region that is being captured into a CUDA graph (an allocation there is an
-// error or ends the capture), in a host process whose device memory belongs
-// to another allocator (a framework's caching allocator, a real-time loop
-// that must not block on the driver), or in a plugin that may only touch the
+// Who needs it: code that runs where cudaMalloc is off limits -- a host
+// process whose device memory belongs to another allocator (a framework's
+// caching allocator that owns the whole device, a real-time loop that must
+// not block on the driver's allocator), or a plugin that may only touch the
 // buffers its host hands it.  Such a caller owns the grid values and the
 // candidate arrays; it cannot create a crp_plan, because plan creation
 // uploads the grid and allocates the run's scratch.
@@ -18,12 +17,17 @@
 // loads the library holds that array until the process exits.  Host code
 // cannot use the array's name as a device address: the first call on each
 // device looks its address up with cudaGetSymbolAddress, with that device
-// current, and keeps it.  Every call shares the array: the counters are
-// cleared before each launch and the lists are written before they are read,
-// so a call never depends on what an earlier call left there, but two calls
-// whose work overlaps on the GPU race on it.
+// current, and keeps it; make that first call before any stream capture
+// begins.  Every call shares the array: the counters are cleared before each
+// launch and the lists are written before they are read, so a call never
+// depends on what an earlier call left there, but two calls whose work
+// overlaps on the GPU race on it.
+//
+// Between launches the call reads the counters back to the host and waits
+// for the stream, so it returns only when the run is complete.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -32,7 +36,8 @@
 #include "engine_internal.h"
 
 namespace crp {
-void set_last_error(const char *msg);  // crp_engine.cu
+void set_last_error(const char *msg);                        // crp_engine.cu
+crp_status check_device_ptr(const void *ptr, const char *what);  // crp_engine.cu
 }
 
 using namespace crp;
@@ -101,12 +106,33 @@ extern "C" crp_status crp_run_device_noalloc(const crp_noalloc_grid_bp_desc *d,
         return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "Grid3f: empty grid");
     if (d->nx > (1u << 20) || d->ny > (1u << 20) || d->nz > (1u << 20))
         return noalloc_fail(CRP_ERR_CAPACITY, "Grid3f: a dimension beyond 2^20 cells");
-    if (!(d->step > 0)) return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "PropagationBP: step must be > 0");
+    if (!(d->step > 0) || !std::isfinite(d->step))
+        return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "PropagationBP: step must be finite and > 0");
+    for (int a = 0; a < 3; a++) {
+        if (!(d->spacing[a] > 0) || !std::isfinite(d->spacing[a]))
+            return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "Grid3f: spacing must be finite and > 0");
+        if (!std::isfinite(d->origin[a]))
+            return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "Grid3f: origin must be finite");
+    }
+    // a non-finite maximum length would keep candidates active for ever
+    if (!std::isfinite(d->max_length))
+        return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "MaximumTrajectoryLength: maximum length must be finite");
     if (n == 0) return CRP_OK;
-    if (!c->id || !c->charge || !c->energy || !c->x || !c->y || !c->z || !c->dx || !c->dy ||
-        !c->dz || !c->px || !c->py || !c->pz || !c->trajectory_length || !c->time ||
-        !c->current_step || !c->next_step || !c->active || !c->flags)
-        return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "a candidate array is NULL");
+    const void *const arrays[] = {c->id, c->charge, c->energy, c->x, c->y, c->z, c->dx, c->dy, c->dz,
+                                  c->px, c->py, c->pz, c->trajectory_length, c->time,
+                                  c->current_step, c->next_step, c->active, c->flags};
+    for (const void *q : arrays)
+        if (!q) return noalloc_fail(CRP_ERR_INVALID_ARGUMENT, "a candidate array is NULL");
+    // host or freed pointers become an error here instead of a fault in the kernel
+    for (const void *q : arrays) {
+        crp_status st = check_device_ptr(q, "crp_run_device_noalloc: a candidate array");
+        if (st != CRP_OK) return st;
+    }
+    {
+        crp_status st = check_device_ptr(c->step_count, "crp_run_device_noalloc: step_count");
+        if (st == CRP_OK) st = check_device_ptr(d->grid_values, "crp_run_device_noalloc: grid_values");
+        if (st != CRP_OK) return st;
+    }
 
     NoAllocScratch *scratch = nullptr;
     crp_status st = scratch_for_current_device(&scratch);

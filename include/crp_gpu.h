@@ -484,9 +484,10 @@ crp_status crp_bp_adjoint_backward(const crp_adjoint_desc *desc, const crp_adjoi
  * ---------------------------------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot allocate device
- * memory -- code inside a CUDA-graph capture region, a process whose device
- * memory belongs to another allocator, a plugin limited to the buffers its
- * host hands it -- and so cannot create a crp_plan: a fixed-step
+ * memory -- a process whose device memory belongs to another allocator (a
+ * framework's caching allocator that owns the device, a real-time loop that
+ * must not block on the driver's allocator), a plugin limited to the buffers
+ * its host hands it -- and so cannot create a crp_plan: a fixed-step
  * PropagationBP over one Grid3f whose values the caller already holds on the
  * device, followed by MaximumTrajectoryLength.  Nothing is allocated: the
  * run's scratch (counters and compaction lists) is a fixed static device
@@ -495,12 +496,17 @@ crp_status crp_bp_adjoint_backward(const crp_adjoint_desc *desc, const crp_adjoi
  * CRP_ERR_CAPACITY).  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress), so make that first call before any stream
  * capture begins.  All calls share the array: calls whose work overlaps on
- * the GPU race on it.  Results equal crp_run_device with the same chain and
- * precision. */
+ * the GPU race on it.  Every candidate array, step_count (when given) and
+ * grid_values must be device-reachable (CRP_ERR_INVALID_ARGUMENT otherwise);
+ * spacing must be finite and > 0, step finite and > 0, max_length finite.
+ * The call reads the run counters back to the host between launches and
+ * returns when every candidate is inactive.  Results equal crp_run_device
+ * with the same chain and precision. */
 #define CRP_NOALLOC_MAX_CANDIDATES (1u << 20)
 
 typedef struct crp_noalloc_grid_bp_desc {
-    const float *grid_values; /* DEVICE pointer: nx*ny*nz Vector3f cells, Grid.h:338 order */
+    const float *grid_values; /* DEVICE pointer: nx*ny*nz cells of 3 floats, cell (ix, iy, iz) at
+                                 index (ix*ny + iy)*nz + iz */
     uint64_t nx, ny, nz;
     double origin[3];
     double spacing[3];
