@@ -205,6 +205,16 @@ def barrier(world):
         dist.barrier()
 
 
+def headline_config(args, n, world):
+    """The `config` of the headline line, printed identically by both arms."""
+    return {"workload": args.workload, "candidates": n,
+            "grid": f"{args.grid_n}^3 float32 Kolmogorov, 5 kpc, periodic, Brms 10 nG",
+            "propagation": "PropagationBP fixed 1 kpc", "steps_per_candidate": args.track,
+            "precision": "mixed (FP32 field/rotation, FP64 accumulation)",
+            "l2": "grid 201 MB > 126 MB L2 (inputs larger than L2)",
+            "parallelism": f"replicas x{world}"}
+
+
 # ------------------------------------------------------------------ CPU legs
 def reference_cpu_rate(spec_fp64, cands, n_sample, threads):
     """The reference's ModuleList::run (timing build) on n_sample candidates."""
@@ -221,6 +231,33 @@ def reference_cpu_rate(spec_fp64, cands, n_sample, threads):
     sub.n = n_sample
     steps, secs = ref.run(spec_fp64, sub, threads=threads)
     return {"value": steps / secs, "steps": steps, "seconds": secs}
+
+
+def headline_parity(spec_fp64, cands, final_64, final_mx, threads, k=1024):
+    """The reference's parity build (libcrp_ref.so: its sources at -O2 without
+    FMA) on the first k candidates of the headline batch, against the FP64
+    and mixed device results of the same candidates in the timed runs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference, reference_available
+    if not reference_available():
+        return None
+    sub = cands.head(k)
+    t0 = time.time()
+    Reference().run(spec_fp64, sub, threads=threads)
+    secs = time.time() - t0
+    names = ("x", "y", "z", "dx", "dy", "dz", "px", "py", "pz", "trajectory_length", "time",
+             "current_step", "next_step", "active", "flags")
+    same = np.ones(k, dtype=bool)
+    for name in names:
+        same &= getattr(final_64, name)[:k] == getattr(sub, name)
+    p_ref = sub.position()
+    err = np.linalg.norm(final_mx.position()[:k] - p_ref, axis=1) / np.linalg.norm(p_ref, axis=1)
+    return {"reference": "libcrp_ref.so (the reference's sources, -O2, no FMA)", "compared": k,
+            "fp64_mismatches": int((~same).sum()),
+            "mixed_rel_pos_err_vs_reference": {"median": float(np.median(err)),
+                                               "max": float(err.max()),
+                                               "frac_le_1e-6": float(np.mean(err <= 1e-6))},
+            "reference_seconds": secs}
 
 
 def cpu_threads():
@@ -288,8 +325,8 @@ def run_reference_arm(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * tot_secs / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "candidates": n, "grid": f"{args.grid_n}^3",
-                       "steps_per_candidate": args.track},
+            "config": headline_config(args, n, world),
+            "sample_candidates": n_sample,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -440,6 +477,7 @@ def cfg_grid_ck_nuclei(dev, peaks, n3=1 << 20, cap3=2048):
         "workload": f"{n3} candidates (H, He-4, N-14, Fe-56), E^-2 0.1-100 EeV, 256^3 Grid3f, "
                     f"PropagationCK 1e-4 0.1-100 kpc, lengths U[1,50] Mpc; at most {cap3} steps "
                     "per candidate (full runs reach 5e5 steps)",
+        "candidates": n3, "max_steps_per_candidate": cap3,
         "chunked_tries_per_s": rate(chunked),
         "persistent_default_tries_per_s": rate(persistent),
         "autotuned_tries_per_s": rate(auto),
@@ -467,6 +505,7 @@ def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
         "workload": f"{n5} protons 1 TeV-1 PeV, DiffusionSDE (1e-4, 0.1-100 pc, eps 0.1), "
                     f"1 muG toroidal + PlaneWaveTurbulence 1024 modes 0.5 muG 1-100 pc, "
                     f"absorbing sphere 20 kpc; {cap5} steps per candidate (full runs ~1e5)",
+        "candidates": n5, "max_steps_per_candidate": cap5,
         "particle_steps_per_s": t["particle_steps"] / secs,
         "field_evaluations_per_s": t["field_evaluations"] / secs,
         "mode_evaluations_per_s": cos_s,
@@ -486,7 +525,8 @@ def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
     make = {"jf12": W.jf12_backtrack, "uf23": W.uf23_backtrack, "pt11": W.pt11_backtrack}[model]
     field = {"jf12": "JF12Field (regular)", "uf23": "UF23Field (base)", "pt11": "PT11Field (ASS + halo)"}[model]
     res = {"workload": f"{n} antiprotons 5-100 EeV from (-8.5 kpc, 0, 0), {field}, "
-                       "PropagationCK 1e-4 0.1-100 pc, Observer sphere 20 kpc, full runs"}
+                       "PropagationCK 1e-4 0.1-100 pc, Observer sphere 20 kpc, full runs",
+           "candidates": n, "max_steps_per_candidate": None}
     for prec, name in ((_abi.PRECISION_FP64, "fp64"), (_abi.PRECISION_MIXED, "mixed")):
         spec, cands = make(n=n, precision=prec)
         plan = engine.Plan(spec)
@@ -600,13 +640,14 @@ def main():
                 a.copy_(getattr(d_init, name))
 
     # every stepping launch of the process, per form, for comparison with the
-    # ncu launch list of the same command (profiles/launches_grid_bp_256.md)
-    kernel_time = {"mixed_chunk_kernel<BPFixed>": [0, 0.0], "fp64_chunk_kernel<BPFixed>": [0, 0.0]}
+    # ncu launch list of the same command
+    MIXED_KERNEL = "mixed_bp_pair_kernel<CS_PM>"  # two candidates per thread (the default here)
+    kernel_time = {MIXED_KERNEL: [0, 0.0], "fp64_chunk_kernel<BPFixed>": [0, 0.0]}
 
     def one_step(plan):
         reset()
         st = plan.run(d_work)
-        k = kernel_time["mixed_chunk_kernel<BPFixed>" if plan is plan_mx else "fp64_chunk_kernel<BPFixed>"]
+        k = kernel_time[MIXED_KERNEL if plan is plan_mx else "fp64_chunk_kernel<BPFixed>"]
         k[0] += st.launches
         k[1] += st.device_ms
         return st
@@ -705,8 +746,8 @@ def main():
         t1 = time.perf_counter()
         st = plan_mx.run(h_work)
         t2 = time.perf_counter()
-        kernel_time["mixed_chunk_kernel<BPFixed>"][0] += st.launches
-        kernel_time["mixed_chunk_kernel<BPFixed>"][1] += st.device_ms
+        kernel_time[MIXED_KERNEL][0] += st.launches
+        kernel_time[MIXED_KERNEL][1] += st.device_ms
         e2e_steps += st.particle_steps
         e2e_s += t2 - t1
     e2e_value, _, _ = replica_rate(e2e_steps, e2e_s * 1e3, world)
@@ -730,9 +771,9 @@ def main():
                 "note": "the register cell cache reloads corners only on a cell change, so DRAM "
                         "traffic per step (traffic) is below the 96 B basis and frac can exceed 1; "
                         "ncu shows the kernel issue/latency bound, not HBM bound",
-                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step: mean DRAM read+write of "
-                                 "six full-size launches measured by ncu "
-                                 "(profiles/dram_mixed_chunk_kernel_bp_fixed_grid256_full.md) x "
+                "traffic_basis": f"{TRAFFIC_B_PER_STEP} B per particle-step: DRAM read+write "
+                                 "(dram__bytes_read.sum + dram__bytes_write.sum) of this kernel over "
+                                 "the launches of one full-size run, measured by ncu, x "
                                  "particle-steps per timed stepping launch"}
 
     adjoint = None if args.no_adjoint else adjoint_cost(dev, args)
@@ -744,6 +785,10 @@ def main():
     except Exception as e:  # the headline does not depend on these
         log(f"[bench] peaks not measured: {e}")
     configs = None if (args.no_configs or world > 1) else secondary_configs(dev, peaks)
+
+    parity = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        parity = headline_parity(spec_64, cands, final_64, final_mx, cpu_threads())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -760,14 +805,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": args.workload, "candidates": n, "grid": f"{args.grid_n}^3 float32 "
-                       "Kolmogorov, 5 kpc, periodic, Brms 10 nG", "propagation": "PropagationBP fixed 1 kpc",
-                       "steps_per_candidate": args.track, "precision": "mixed (FP32 field/rotation, FP64 accumulation)",
-                       "l2": "grid 201 MB > 126 MB L2 (inputs larger than L2)", "parallelism": f"replicas x{world}"},
-            "fp64": {"value": value_64, "unit": UNIT, "ms_per_step": ms64 / k64,
+            "config": headline_config(args, n, world),
+            "fp64": {"value": value_64, "unit": UNIT, "ms_per_step": ms64 / k64, "dtype": "f64",
                      "mixed_over_fp64": value / value_64},
+            "parity": parity,
             "mixed_error_vs_fp64": dict(stats(err), measure="|x_mixed - x_fp64| / |x_fp64| per candidate",
                                         well_conditioned=dict(
                                             stats(err[stable]) if stable.any() else {},

@@ -74,6 +74,20 @@ class CandidateArrays:
             setattr(out, name, None if a is None else (a.copy() if isinstance(a, np.ndarray) else a.clone()))
         return out
 
+    def head(self, k: int) -> "CandidateArrays":
+        """A copy of the first k candidates (host or device arrays)."""
+        k = min(int(k), self.n)
+        out = CandidateArrays.__new__(CandidateArrays)
+        out.n, out.device = k, self.device
+        for name in self.MEMBERS:
+            a = getattr(self, name)
+            if a is None:
+                setattr(out, name, None)
+            else:
+                setattr(out, name, np.ascontiguousarray(a[:k]) if isinstance(a, np.ndarray)
+                        else a[:k].clone())
+        return out
+
     def to_device(self, device="cuda") -> "CandidateArrays":
         import torch
         out = CandidateArrays.__new__(CandidateArrays)

@@ -8,6 +8,11 @@ grid_bp_256:  fixed-step PropagationBP (1 kpc) over a Kolmogorov Grid3f of
 grid_ck_64:   PropagationCK (tolerance 1e-4, 0.1-10 kpc) over a 64^3
               Kolmogorov grid at 10 kpc (Brms 1 nG, lMin 20 kpc, lMax
               200 kpc, seed 42); 10^4 protons; MaximumTrajectoryLength 10 Mpc.
+grid_bp_backtrack_128: fixed-step PropagationBP (1 kpc, 2000 steps) of
+              antiprotons, log-uniform 5-50 EeV, isotropic, from the origin,
+              through a 128^3 Kolmogorov Grid3f at 10 kpc (Brms 3 nG, lMin
+              20 kpc, lMax 1280 kpc, seed 42): the forward pass of the
+              adjoint workload.
 grid_ck_nuclei: PropagationCK (1e-4, 0.1-100 kpc) over the 256^3 grid with
               H, He-4, N-14, Fe-56 in equal parts, E^-2 over 0.1-100 EeV and a
               per-candidate maximum length uniform in 1-50 Mpc.
@@ -41,9 +46,12 @@ def charge_of(pid: int) -> float:
 
 
 def source_candidates(n, ids, emin, emax, index, seed, position=(0.0, 0.0, 0.0),
-                      abundances=None, per_candidate_length=False) -> CandidateArrays:
+                      abundances=None, per_candidate_length=False,
+                      fixed_point=False) -> CandidateArrays:
     """Candidates from a Source(SourcePosition, particle type(s),
-    SourcePowerLawSpectrum, SourceIsotropicEmission) via crp_source_sample."""
+    SourcePowerLawSpectrum, SourceIsotropicEmission) via crp_source_sample;
+    with fixed_point, directions moved to fixed points of the reference's
+    normalisation (fixed_point_directions), as the workloads use them."""
     lib = _abi.load()
     ids = np.asarray(ids, dtype=np.int32)
     ab = np.ones(len(ids)) if abundances is None else np.asarray(abundances, dtype=np.float64)
@@ -60,11 +68,48 @@ def source_candidates(n, ids, emin, emax, index, seed, position=(0.0, 0.0, 0.0),
                                      c.id.ctypes.data_as(C.POINTER(C.c_int32)),
                                      c.energy.ctypes.data_as(C.POINTER(C.c_double)),
                                      dirs.ctypes.data_as(C.POINTER(C.c_double))))
-    c.set_direction(dirs.reshape(3, n).T)
+    d = dirs.reshape(3, n).T
+    c.set_direction(fixed_point_directions(d) if fixed_point else d)
     c.set_position(np.tile(np.asarray(position, dtype=np.float64), (n, 1)))
     qs = {int(p): charge_of(int(p)) for p in np.unique(c.id)}
     c.charge[:] = np.vectorize(lambda p: qs[int(p)])(c.id) if n else 0
     return c
+
+
+def _normalise(d):
+    r = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    return d / r[:, None]
+
+
+def fixed_point_directions(d):
+    """Directions that ParticleState::setDirection (ParticleState.cpp:30,
+    d / |d|) maps to themselves bit for bit: the reference's Candidate
+    constructor normalises the direction it is given, so a Candidate built
+    from these arrays holds exactly the bits the device starts from.  d is
+    normalised again until it no longer changes; the few that cycle instead
+    get their components moved by single ulps until a fixed point is found.
+    Every change is a few ulp per component."""
+    d = np.array(d, dtype=np.float64)
+    for _ in range(8):
+        d2 = _normalise(d)
+        if np.array_equal(d2, d):
+            break
+        d = d2
+    bad = np.flatnonzero(~np.all(_normalise(d) == d, axis=1))
+    for k in range(1, 5):
+        if not len(bad):
+            break
+        for j in range(3):
+            for sign in (np.inf, -np.inf):
+                if not len(bad):
+                    break
+                t = d[bad].copy()
+                for _ in range(k):
+                    t[:, j] = np.nextafter(t[:, j], sign)
+                ok = np.all(_normalise(t) == t, axis=1)
+                d[bad[ok]] = t[ok]
+                bad = bad[~ok]
+    return d
 
 
 def kolmogorov_grid(n, spacing, brms, lmin, lmax, seed=42, device=None):
@@ -82,7 +127,19 @@ def grid_bp_256(n=1_000_000, grid_n=256, steps=5000, precision=_abi.PRECISION_MI
     spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (spacing,) * 3)],
                        [P.Propagation(_abi.PROP_BP, 0.42, 1 * U.kpc, 1 * U.kpc),
                         P.MaxTrajectoryLength(steps * U.kpc)], precision=precision)
-    cands = source_candidates(n, [IDS["H"]], 1 * U.EeV, 100 * U.EeV, -1.0, seed)
+    cands = source_candidates(n, [IDS["H"]], 1 * U.EeV, 100 * U.EeV, -1.0, seed, fixed_point=True)
+    return spec, cands, grid
+
+
+def grid_bp_backtrack_128(n=100_000, steps=2000, precision=_abi.PRECISION_FP64, grid=None,
+                          device=None, seed=4):
+    spacing = 10 * U.kpc
+    if grid is None:
+        grid = kolmogorov_grid(128, spacing, 3 * U.nG, 20 * U.kpc, 1280 * U.kpc, 42, device)
+    spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (spacing,) * 3)],
+                       [P.Propagation(_abi.PROP_BP, 0.42, 1 * U.kpc, 1 * U.kpc),
+                        P.MaxTrajectoryLength(steps * U.kpc)], precision=precision)
+    cands = source_candidates(n, [-IDS["H"]], 5 * U.EeV, 50 * U.EeV, -1.0, seed, fixed_point=True)
     return spec, cands, grid
 
 
@@ -93,7 +150,7 @@ def grid_ck_64(n=10_000, precision=_abi.PRECISION_FP64, grid=None, device=None, 
     spec = P.ChainSpec([P.GridField(grid, (0, 0, 0), (spacing,) * 3)],
                        [P.Propagation(_abi.PROP_CK, 1e-4, 0.1 * U.kpc, 10 * U.kpc),
                         P.MaxTrajectoryLength(10 * U.Mpc)], precision=precision)
-    cands = source_candidates(n, [IDS["H"]], 1 * U.EeV, 100 * U.EeV, -1.0, seed)
+    cands = source_candidates(n, [IDS["H"]], 1 * U.EeV, 100 * U.EeV, -1.0, seed, fixed_point=True)
     return spec, cands, grid
 
 
@@ -106,7 +163,7 @@ def grid_ck_nuclei(n=10_000_000, grid=None, precision=_abi.PRECISION_MIXED, devi
                        [P.Propagation(_abi.PROP_CK, 1e-4, 0.1 * U.kpc, 100 * U.kpc),
                         P.MaxTrajectoryLength(per_candidate=True)], precision=precision)
     cands = source_candidates(n, [IDS[k] for k in ("H", "He", "N", "Fe")], 0.1 * U.EeV,
-                              100 * U.EeV, -2.0, seed, per_candidate_length=True)
+                              100 * U.EeV, -2.0, seed, per_candidate_length=True, fixed_point=True)
     rng = np.random.default_rng(seed)
     cands.max_length[:] = rng.uniform(1, 50, n) * U.Mpc
     return spec, cands, grid
@@ -142,7 +199,8 @@ def sde_galactic(n=10_000_000, n_modes=1024, precision=_abi.PRECISION_MIXED, see
                         P.ObserverSpec(_abi.OBSERVER_SURFACE_SPHERE, (0.0, 0.0, 0.0), 20 * U.kpc,
                                        True, False)],
                        precision=precision, seed=seed)
-    cands = source_candidates(n, [IDS["H"]], 1 * U.TeV, 1000 * U.TeV, -1.0, seed, position=source)
+    cands = source_candidates(n, [IDS["H"]], 1 * U.TeV, 1000 * U.TeV, -1.0, seed, position=source,
+                              fixed_point=True)
     return spec, cands
 
 
@@ -157,7 +215,7 @@ def jf12_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, variant=
                                        True, False)],
                        precision=precision, seed=seed)
     cands = source_candidates(n, [-IDS["H"]], 5 * U.EeV, 100 * U.EeV, -1.0, seed,
-                              position=(-8.5 * U.kpc, 0.0, 0.0))
+                              position=(-8.5 * U.kpc, 0.0, 0.0), fixed_point=True)
     return spec, cands
 
 

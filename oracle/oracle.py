@@ -4,7 +4,9 @@
   the stepping path (crp_oracle.c).
 * `Reference` wraps oracle/_ref/libcrp_ref.so, the reference itself compiled
   from its sources with the shim ref_shim.cpp (oracle/Makefile), when it has
-  been built (it needs the reference checkout at build time only).
+  been built (it needs the reference checkout at build time only);
+  `Reference(cr_pow=True)` the same sources linked so that every pow call is
+  the correctly rounded pow of the engine's FP64 form (libcrp_ref_crpow.so).
 * `PluginHarness` wraps oracle/_ref/libcrp_ref_gpu.so: the reference's own
   chain objects run through the product's C++ plugin GpuModuleList
   (crpropa3_b200/plugin), the drop-in for ModuleList::run.
@@ -28,6 +30,7 @@ ORACLE_LIB = os.path.join(HERE, "_build", "libcrp_oracle.so")
 ORACLE_CRPOW_LIB = os.path.join(HERE, "_build", "libcrp_oracle_crpow.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcrp_ref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libcrp_ref_fast.so")
+REF_CRPOW_LIB = os.path.join(HERE, "_ref", "libcrp_ref_crpow.so")
 REF_GPU_LIB = os.path.join(HERE, "_ref", "libcrp_ref_gpu.so")
 
 _dp = C.POINTER(C.c_double)
@@ -152,15 +155,15 @@ class Oracle:
         return list(o)
 
 
-def reference_available(fast=False) -> bool:
-    return os.path.exists(REF_FAST_LIB if fast else REF_LIB)
+def reference_available(fast=False, cr_pow=False) -> bool:
+    return os.path.exists(REF_FAST_LIB if fast else REF_CRPOW_LIB if cr_pow else REF_LIB)
 
 
 class Reference:
     """The reference's own modules, driven through ref_shim.cpp."""
 
-    def __init__(self, fast=False):
-        path = REF_FAST_LIB if fast else REF_LIB
+    def __init__(self, fast=False, cr_pow=False):
+        path = REF_FAST_LIB if fast else REF_CRPOW_LIB if cr_pow else REF_LIB
         if not os.path.exists(path):
             raise RuntimeError(f"reference library {path} is not built (make -C oracle ref)")
         lib = C.CDLL(path)
@@ -315,6 +318,8 @@ class PluginHarness:
                                                C.c_double, C.c_double, C.c_uint64, C.c_uint64,
                                                C.c_char_p, C.c_int, C.c_uint32, C.c_uint64,
                                                C.POINTER(_abi.RunStats)]
+        lib.ref_run_interrupted.argtypes = [pd, cd, C.c_uint64, C.c_int, C.c_uint64, C.c_char_p,
+                                            C.POINTER(C.c_int)]
         lib.ref_gpu_describe.argtypes = [pd, C.c_int, C.c_char_p, C.c_size_t]
         lib.ref_gpu_unsupported_throws.argtypes = [pd, C.c_char_p, C.c_size_t]
         self.lib = lib
@@ -349,6 +354,17 @@ class PluginHarness:
             C.byref(spec.desc()), 1 if gpu else 0, precision, _dptr(pos), pid, emin, emax, index,
             count, batch, str(path).encode(), output_type, seed, serial0, C.byref(stats)))
         return stats
+
+    def run_interrupted(self, spec, cands: CandidateArrays, path, gpu, batch=0):
+        """run(candidates) with SIGINT sent at the first detection and a
+        TextOutput(path) interrupt action, on the plugin (gpu, batches of
+        `batch`) or on the reference's ModuleList (one thread).  Returns the
+        signal the run raised again at its end (0: none)."""
+        reraised = C.c_int()
+        self._check(self.lib.ref_run_interrupted(C.byref(spec.desc()), C.byref(cands.struct()),
+                                                 cands.n, 1 if gpu else 0, batch,
+                                                 str(path).encode(), C.byref(reraised)))
+        return reraised.value
 
     def describe(self, spec, extra=0):
         """(on the device path?, plan text or reason) without a device."""

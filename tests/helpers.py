@@ -71,3 +71,19 @@ def ck(tol, min_step, max_step):
 def rel_pos_err(a: CandidateArrays, b: CandidateArrays):
     pa, pb = a.position(), b.position()
     return np.linalg.norm(pa - pb, axis=1) / np.maximum(np.linalg.norm(pb, axis=1), 1e-300)
+
+
+def stabilize_directions(c):
+    """Replace the candidates' directions by a fixed point of setDirection's
+    normalisation (normalised again until it no longer changes), so that the
+    reference's Candidate constructor, which normalises, starts from the same
+    bits as the device.  Returns the mask of candidates that reached a fixed
+    point (the others keep their last iterate)."""
+    d = c.direction()
+    for _ in range(8):
+        d2 = normalize(d)
+        if np.array_equal(d2, d):
+            break
+        d = d2
+    c.set_direction(d)
+    return np.all(normalize(d) == d, axis=1)

@@ -158,3 +158,24 @@ def test_text_output_matches_reference(reference, tmp_path, suffix):
         assert gzip.open(mine, "rt").read() == gzip.open(ref_path, "rt").read()
     else:
         assert open(mine).read() == open(ref_path).read()
+
+
+@pytest.mark.parametrize("prop", [P.Propagation(_abi.PROP_BP, 1e-3, 0.1 * U.kpc, 10 * U.kpc),
+                                  ck(1e-4, 0.1 * U.kpc, 10 * U.kpc)], ids=["bp_adaptive", "ck_adaptive"])
+def test_reference_with_correctly_rounded_pow_matches_crpow_oracle(oracle_crpow, prop):
+    """The reference's sources linked so that pow is the engine's correctly
+    rounded pow (libcrp_ref_crpow.so) against the oracle built with the same
+    pow: bit for bit, adaptive controllers included.  This pins the build the
+    GPU parity tests of the adaptive workloads compare with."""
+    from oracle import Reference, reference_available
+    if not reference_available(cr_pow=True):
+        pytest.skip("reference library not built (make -C oracle ref needs the reference checkout)")
+    ref = Reference(cr_pow=True)
+    rng = np.random.default_rng(111)
+    grid = random_grid(rng, 16, brms=1e-12)
+    spec = grid_chain(grid, 10 * U.kpc, prop, 2 * U.Mpc)
+    c = protons(rng, 256, emin=0.3 * U.EeV, emax=30 * U.EeV)
+    a, b = c.copy(), c.copy()
+    oracle_crpow.run(spec, a)
+    ref.run(spec, b, threads=4)
+    _same(a, b)
