@@ -8,6 +8,7 @@ contraction.  Objects go to _build/ at the repository root.
 from __future__ import annotations
 
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -29,6 +30,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUD
 SOURCES = {
     "step_fp64.cu": ["-fmad=false"],
     "step_mixed.cu": [],
+    "step_mixed_bp.cu": [],
     "adjoint.cu": [],
     "turbulence.cu": [],
     "crp_engine.cu": [],
@@ -46,11 +48,31 @@ def _nvcc():
     raise RuntimeError("nvcc not found")
 
 
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(path, seen=None):
+    """The source and every header it includes with #include "..." (found
+    next to the including file, in csrc/ or in include/), recursively."""
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path, encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    for name in _INCLUDE_RE.findall(text):
+        for d in (os.path.dirname(path), CSRC, INCLUDE):
+            cand = os.path.join(d, name)
+            if os.path.exists(cand):
+                _deps(cand, seen)
+                break
+    return seen
+
+
 def _compile(nvcc, src, flags, verbose):
     out = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
     path = os.path.join(CSRC, src)
-    deps = [path] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    deps.append(os.path.join(INCLUDE, "crp_gpu.h"))
+    deps = sorted(_deps(path)) + [os.path.abspath(__file__)]
     if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
         return out
     cmd = [nvcc] + ARCH + COMMON + flags

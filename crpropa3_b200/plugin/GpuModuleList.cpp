@@ -17,6 +17,7 @@
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
 #include "crpropa/module/Observer.h"
+#include "crpropa/module/Output.h"
 #include "crpropa/module/PropagationBP.h"
 #include "crpropa/module/PropagationCK.h"
 
@@ -29,6 +30,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <iostream>
 #include <sstream>
 #include <stdexcept>
 #include <typeinfo>
@@ -85,6 +87,8 @@ CRPGPU_MEMBER(PlaneN, Plane, Vector3d, n);
 CRPGPU_MEMBER(BoxCorner, ParaxialBox, Vector3d, corner);               // Geometry.h:77
 CRPGPU_MEMBER(BoxSize, ParaxialBox, Vector3d, size);
 typedef double UF23Pars[26];
+CRPGPU_MEMBER(ListInterruptAction, ModuleList, Output *, interruptAction);      // ModuleList.h:63
+CRPGPU_MEMBER(ListHaveInterruptAction, ModuleList, bool, haveInterruptAction);
 CRPGPU_MEMBER(UF23Model, UF23Field, const UF23Field::ModelType, fModelType);  // UF23Field.h
 CRPGPU_MEMBER(UF23MaxR2, UF23Field, const double, fMaxRadiusSquared);
 CRPGPU_MEMBER(UF23Parameters, UF23Field, UF23Pars, fParameters);
@@ -864,6 +868,20 @@ void GpuModuleList::run(ref_ptr<Candidate> candidate, bool recursive, bool secon
     run(candidate.get(), recursive, secondariesFirst);
 }
 
+void GpuModuleList::addStats(crp_run_stats &total, uint64_t &events) const {
+    total.particle_steps += impl->stats.particle_steps;
+    total.tries += impl->stats.tries;
+    total.field_evaluations += impl->stats.field_evaluations;
+    total.launches += impl->stats.launches;
+    total.device_ms += impl->stats.device_ms;
+    events += impl->events;
+}
+
+// ModuleList::run(candidates) (ModuleList.cpp.in:97-151) in batches: a
+// signal stops the batches that have not started; the started one runs to
+// completion.  Then, as the reference does: restore the previous handlers,
+// raise the signal again, report, and hand the sorted indices of the
+// candidates not started to the interrupt action.
 void GpuModuleList::run(const candidate_vector_t *candidates, bool recursive,
                         bool secondariesFirst) {
     std::string why;
@@ -874,9 +892,45 @@ void GpuModuleList::run(const candidate_vector_t *candidates, bool recursive,
         }
         throw std::runtime_error("GpuModuleList: chain is not on the device path: " + why);
     }
-    runDevice(*candidates);
+    const size_t count = candidates->size();
+    crp_run_stats total;
+    std::memset(&total, 0, sizeof(total));
+    uint64_t events = 0;
+    std::vector<int> notFinished;
+    int signal_seen = 0;
+    {
+        SignalScope sig;
+        for (size_t done = 0; done < count;) {
+            const size_t n = std::min(impl->batch, count - done);
+            if (g_cancel != 0) {
+                for (size_t i = done; i < done + n; i++) notFinished.push_back(int(i));
+            } else {
+                candidate_vector_t v(candidates->begin() + done, candidates->begin() + done + n);
+                runDevice(v);
+                addStats(total, events);
+            }
+            done += n;
+        }
+        signal_seen = g_cancel;
+    }
+    impl->stats = total;
+    impl->events = events;
+    if (signal_seen > 0) {
+        raise(signal_seen);
+        std::cerr << "############################################################################\n";
+        std::cerr << "#\tInterrupted CRPropa simulation \n";
+        std::cerr << "# A total of " << notFinished.size() << " candidates have not been started.\n";
+        std::cerr << "# the indices of the vector haven been written to to output file. \n";
+        std::cerr << "############################################################################\n";
+        std::sort(notFinished.begin(), notFinished.end());
+        if (this->*member(ListHaveInterruptAction()))
+            (this->*member(ListInterruptAction()))->dumpIndexList(notFinished);
+    }
 }
 
+// ModuleList::run(source, count) (ModuleList.cpp.in:153-214) in batches of
+// candidates drawn on this thread; a signal stops the draws, as in the
+// reference, which reports the count of candidates not started.
 void GpuModuleList::run(SourceInterface *source, size_t count, bool recursive,
                         bool secondariesFirst) {
     std::string why;
@@ -890,22 +944,34 @@ void GpuModuleList::run(SourceInterface *source, size_t count, bool recursive,
     crp_run_stats total;
     std::memset(&total, 0, sizeof(total));
     uint64_t events = 0;
-    for (size_t done = 0; done < count;) {
-        size_t n = std::min(impl->batch, count - done);
-        candidate_vector_t v;
-        v.reserve(n);
-        for (size_t i = 0; i < n; i++) v.push_back(source->getCandidate());
-        runDevice(v);
-        total.particle_steps += impl->stats.particle_steps;
-        total.tries += impl->stats.tries;
-        total.field_evaluations += impl->stats.field_evaluations;
-        total.launches += impl->stats.launches;
-        total.device_ms += impl->stats.device_ms;
-        events += impl->events;
-        done += n;
+    size_t not_started = 0;
+    int signal_seen = 0;
+    {
+        SignalScope sig;
+        for (size_t done = 0; done < count;) {
+            size_t n = std::min(impl->batch, count - done);
+            if (g_cancel != 0) {
+                not_started += n;
+            } else {
+                candidate_vector_t v;
+                v.reserve(n);
+                for (size_t i = 0; i < n; i++) v.push_back(source->getCandidate());
+                runDevice(v);
+                addStats(total, events);
+            }
+            done += n;
+        }
+        signal_seen = g_cancel;
     }
     impl->stats = total;
     impl->events = events;
+    if (signal_seen > 0) {
+        raise(signal_seen);
+        std::cerr << "############################################################################\n";
+        std::cerr << "# Interrupted CRPropa simulation \n";
+        std::cerr << "# Number of not started candidates from source: " << not_started << "\n";
+        std::cerr << "############################################################################\n";
+    }
 }
 
 void GpuModuleList::runDevice(const candidate_vector_t &cands) {
@@ -973,16 +1039,10 @@ void GpuModuleList::runDevice(const candidate_vector_t &cands) {
         crp_run_opts o;
         std::memset(&o, 0, sizeof(o));
         o.mode = CRP_MODE_AUTO;
-        o.cancel = &g_cancel;
         o.records = nrec ? &rv : 0;
-        crp_status st;
-        {
-            SignalScope sig;
-            st = crp_run(impl->plan, &view, n, &o, &impl->stats);
-        }
-        if (st == CRP_ERR_CANCELLED)
-            throw std::runtime_error("GpuModuleList: run interrupted by a signal; candidates unchanged");
-        check(st);
+        // a started batch runs to completion (no cancel flag): the callers
+        // stop between batches
+        check(crp_run(impl->plan, &view, n, &o, &impl->stats));
         if (rec.count > cap) {
             if (attempt > 0) throw std::runtime_error("GpuModuleList: record count changed between runs");
             cap = rec.count;

@@ -43,7 +43,16 @@
 //   * Actions run after the stepping, one candidate after another, instead
 //     of inside the OpenMP loop: output line order is by candidate, not by
 //     thread timing.
-//   * run(source, count) draws candidates on the calling thread, in batches.
+//   * run(source, count) draws candidates on the calling thread, in batches;
+//     run(candidates) also runs in batches of setBatchSize().
+//   * SIGINT / SIGTERM during a run (ModuleList.cpp.in:110-150): a batch
+//     that has started runs to completion, as a started candidate does in
+//     the reference; the candidates of the batches not yet started are left
+//     unchanged and their indices go, sorted, to the interrupt action's
+//     dumpIndexList (run(candidates) with setInterruptAction, as in the
+//     reference); then the previous handlers are restored and the signal is
+//     raised again.  A started candidate of the reference is one candidate
+//     per thread; here it is a whole batch.
 //   * Secondaries: the supported modules create none.
 #ifndef CRPGPU_GPU_MODULE_LIST_H
 #define CRPGPU_GPU_MODULE_LIST_H
@@ -110,7 +119,8 @@ public:
     Precision getPrecision() const;
     /// Key of DiffusionSDE's counter-based random stream.  Default 0.
     void setSeed(uint64_t seed);
-    /// Candidates per device batch in run(source, count).  Default 2^20.
+    /// Candidates per device batch in run(source, count) and
+    /// run(candidates).  Default 2^20.
     void setBatchSize(size_t n);
     /// Run unsupported chains with ModuleList::run instead of throwing.
     void setCpuFallback(bool allow);
@@ -134,6 +144,7 @@ private:
     GpuModuleList(const GpuModuleList &);
     GpuModuleList &operator=(const GpuModuleList &);
     void runDevice(const candidate_vector_t &candidates);
+    void addStats(crp_run_stats &total, uint64_t &events) const;
 };
 
 }  // namespace crpgpu

@@ -16,11 +16,14 @@
 #include "crpropa/Source.h"
 #include "crpropa/Units.h"
 #include "crpropa/module/BreakCondition.h"
+#include "crpropa/module/Observer.h"
 #include "crpropa/module/RestrictToRegion.h"
 #include "crpropa/module/SimplePropagation.h"
 #include "crpropa/module/TextOutput.h"
 
 #include <omp.h>
+#include <signal.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cstring>
@@ -48,6 +51,21 @@ void copy_text(const std::string &s, char *buf, size_t size) {
     std::memcpy(buf, s.data(), n);
     buf[n] = 0;
 }
+
+// A detection action that sends SIGINT to the process at its first event:
+// an interruption at a known point of a run.
+struct SignalAtFirstDetection : public Module {
+    mutable bool fired = false;
+    void process(Candidate *) const {
+        if (!fired) {
+            fired = true;
+            kill(getpid(), SIGINT);
+        }
+    }
+};
+
+volatile sig_atomic_t g_reraised = 0;
+extern "C" void shim_on_signal(int sig) { g_reraised = sig; }
 
 crpgpu::GpuModuleList *make_list(int precision, uint64_t seed) {
     crpgpu::GpuModuleList *g = new crpgpu::GpuModuleList();
@@ -157,6 +175,63 @@ int ref_run_source_textout(const crp_plan_desc *desc, int gpu, int precision, co
         g_error = e.what();
         return 1;
     }
+}
+
+/* ModuleList::run(candidate_vector_t*) interrupted by SIGINT: every
+ * Observer of the chain gets SignalAtFirstDetection as its detection action
+ * and the run a TextOutput(path) as its interrupt action
+ * (ModuleList::setInterruptAction).  On the plugin when gpu != 0 (batches of
+ * `batch`), else on the reference's ModuleList with one thread.  The
+ * harness catches the signal the run raises again at its end and reports it
+ * in *reraised; the caller's SIGINT handler is restored afterwards. */
+int ref_run_interrupted(const crp_plan_desc *desc, const crp_candidates *c, uint64_t n, int gpu,
+                        uint64_t batch, const char *path, int *reraised) {
+    struct sigaction sa, old;
+    std::memset(&sa, 0, sizeof(sa));
+    sa.sa_handler = shim_on_signal;
+    sigaction(SIGINT, &sa, &old);
+    g_reraised = 0;
+    int rc = 0;
+    try {
+        ensure_data_path();
+        PluginHelpers h;
+        Built b;
+        {
+            crpgpu::GpuModuleList *g = 0;
+            if (gpu) {
+                g = make_list(desc->precision, desc->seed);
+                if (batch) g->setBatchSize(batch);
+            }
+            build_chain(desc, 0, b, gpu ? &h : 0, g, false, 0, 0);
+            ref_ptr<Module> signal_action = new SignalAtFirstDetection();
+            for (ModuleList::iterator it = b.sim->begin(); it != b.sim->end(); ++it) {
+                Observer *obs = dynamic_cast<Observer *>(it->get());
+                if (obs) obs->onDetection(signal_action.get());
+            }
+            ref_ptr<TextOutput> interrupt = new TextOutput(path);
+            b.sim->setInterruptAction(interrupt.get());
+            ModuleList::candidate_vector_t cands;
+            load_candidates(c, n, cands);
+            omp_set_num_threads(1);
+            std::streambuf *old_out = std::cout.rdbuf();
+            std::ostringstream sink;
+            std::cout.rdbuf(sink.rdbuf());
+            if (g)
+                g->run(&cands);  // run() is not virtual: call the plugin's own
+            else
+                b.sim->run(&cands);
+            std::cout.rdbuf(old_out);
+            store_candidates(cands, c);
+            interrupt->close();
+        }
+        b.sim = 0;
+    } catch (std::exception &e) {
+        g_error = e.what();
+        rc = 1;
+    }
+    *reraised = g_reraised;
+    sigaction(SIGINT, &old, 0);
+    return rc;
 }
 
 /* The plugin's translation of the chain of `desc` (no device needed):

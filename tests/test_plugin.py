@@ -12,7 +12,7 @@ chains that have no device form.
 import numpy as np
 import pytest
 
-from helpers import P, U, _abi, bp_fixed, ck, protons, random_grid, stable_unit_vectors
+from helpers import P, U, _abi, bp_fixed, ck, grid_chain, protons, random_grid, stable_unit_vectors
 from crpropa3_b200.state import CandidateArrays, RecordArrays
 
 
@@ -254,3 +254,54 @@ def test_plugin_observer_features_and_boundaries_bitwise(plugin, reference, name
     reference.run(spec, a, ra, threads=2)
     plugin.run(spec, b, rb)
     T._compare(a, b, ra, rb)
+
+
+def _interrupt_chain():
+    rng = np.random.default_rng(61)
+    grid = random_grid(rng, 16)
+    spec = grid_chain(grid, 10 * U.kpc, bp_fixed(1 * U.kpc), 1 * U.Mpc, observer_radius=0.2 * U.Mpc,
+                      record=False)
+    return spec, protons(rng, 4000, spread=0.0)
+
+
+def _index_list_text(indices):
+    """TextOutput::dumpIndexList (TextOutput.cpp:396): '#', then each index,
+    each followed by a tab."""
+    return "#\t" + "".join(f"{i}\t" for i in indices)
+
+
+def test_reference_interrupt_semantics_and_index_list_format(plugin, tmp_path):
+    """The reference's own ModuleList::run(candidates), one thread, with SIGINT
+    sent by an observer's detection action: the candidates after the one
+    being run are not started, their indices go to the interrupt action in
+    TextOutput::dumpIndexList's format, and the signal is raised again at
+    the end (ModuleList.cpp.in:110-150).  This pins what the plugin test
+    below holds the plugin to.  No GPU."""
+    spec, c = _interrupt_chain()
+    ref = c.copy()
+    path = tmp_path / "ref_interrupt.txt"
+    assert plugin.run_interrupted(spec, ref, path, gpu=False) == 2  # SIGINT raised again
+    first = int(np.flatnonzero(ref.flags & _abi.FLAG_DETECTED)[0])
+    assert path.read_text() == _index_list_text(range(first + 1, c.n))
+    np.testing.assert_array_equal(ref.trajectory_length[first + 1:], c.trajectory_length[first + 1:])
+
+
+@pytest.mark.gpu
+def test_plugin_interrupted_run_matches_the_reference_semantics(plugin, tmp_path):
+    """SIGINT during GpuModuleList::run(candidates), sent at a known point (the
+    first detection, replayed during the first batch's write-back): the
+    started batch completes exactly as in an uninterrupted run, the later
+    batches are left as they were, their indices go to the interrupt action
+    in the reference's format, and the signal is raised again at the end."""
+    spec, c = _interrupt_chain()
+    batch = 1000
+    full, got = c.copy(), c.copy()
+    plugin.run(spec, full)
+    path = tmp_path / "gpu_interrupt.txt"
+    assert plugin.run_interrupted(spec, got, path, gpu=True, batch=batch) == 2
+    assert path.read_text() == _index_list_text(range(batch, c.n))
+    for name in ("x", "y", "z", "dx", "dy", "dz", "trajectory_length", "active", "flags"):
+        np.testing.assert_array_equal(getattr(got, name)[:batch], getattr(full, name)[:batch],
+                                      err_msg=name)
+        np.testing.assert_array_equal(getattr(got, name)[batch:], getattr(c, name)[batch:],
+                                      err_msg=name)
