@@ -235,15 +235,15 @@ def reference_cpu_rate(spec_fp64, cands, n_sample, threads):
 
 def headline_parity(spec_fp64, cands, final_64, final_mx, threads, k=1024):
     """The reference's parity build (libcrp_ref.so: its sources at -O2 without
-    FMA) on the first k candidates of the headline batch, against the FP64
-    and mixed device results of the same candidates in the timed runs."""
+    FMA) on the first k candidates of the headline batch, in a spawned
+    process without CUDA, against the FP64 and mixed device results of the
+    same candidates in the timed runs."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import Reference, reference_available
+    from oracle import reference_available, run_reference_isolated
     if not reference_available():
         return None
-    sub = cands.head(k)
     t0 = time.time()
-    Reference().run(spec_fp64, sub, threads=threads)
+    sub = run_reference_isolated(spec_fp64, cands.head(k), threads=threads)
     secs = time.time() - t0
     names = ("x", "y", "z", "dx", "dy", "dz", "px", "py", "pz", "trajectory_length", "time",
              "current_step", "next_step", "active", "flags")
@@ -517,6 +517,35 @@ def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
     return out
 
 
+def cfg_sde_galactic_full(dev, n=1 << 16):
+    """The DiffusionSDE workload run to absorption at the 20 kpc sphere (no
+    step cap): n candidates, mixed form, one run after a capped warm-up."""
+    import torch
+    from crpropa3_b200 import engine, workloads as W
+    spec, cands = W.sde_galactic(n=n)
+    plan = engine.Plan(spec)
+    warm = cands.to_device(dev)
+    plan.run(warm, max_steps=8)
+    d = cands.to_device(dev)
+    t0 = time.time()
+    st = plan.run(d)
+    torch.cuda.synchronize()
+    wall = time.time() - t0
+    steps = d.step_count.cpu().numpy().astype(np.float64)
+    secs = st.device_ms / 1e3
+    return {"sde_galactic_full": {
+        "workload": f"{n} protons 1 TeV-1 PeV from (8.5 kpc, 0, 0), DiffusionSDE (1e-4, 0.1-100 pc, "
+                    "eps 0.1), 1 muG toroidal + PlaneWaveTurbulence 1024 modes 0.5 muG 1-100 pc, "
+                    "absorbing sphere 20 kpc, every candidate run to absorption",
+        "candidates": n, "max_steps_per_candidate": None,
+        "particle_steps_per_s": st.particle_steps / secs, "device_s": secs, "wall_s": wall,
+        "field_evaluations_per_s": st.field_evaluations / secs,
+        "mode_evaluations_per_s": st.field_evaluations * 1024 / secs,
+        "launches": st.launches, "active_left": st.active_left,
+        "steps_per_candidate": {"mean": float(steps.mean()), "median": float(np.median(steps)),
+                                "max": float(steps.max())}}}
+
+
 def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
     """PropagationCK backtracking through the JF12 regular field (or the UF23
     base model, or PT11Field), full runs, FP64 and mixed forms, beside the
@@ -604,6 +633,7 @@ def main():
         runs = {"grid_ck_64": lambda: cfg_grid_ck_64(dev, {}, n=args.n or 10_000),
                 "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or (1 << 20)),
                 "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20)),
+                "sde_galactic_full": lambda: cfg_sde_galactic_full(dev, n=args.n or (1 << 16)),
                 "jf12_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20)),
                 "uf23_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="uf23"),
                 "pt11_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="pt11"),
@@ -641,7 +671,7 @@ def main():
 
     # every stepping launch of the process, per form, for comparison with the
     # ncu launch list of the same command
-    MIXED_KERNEL = "mixed_bp_pair_kernel<CS_PM>"  # two candidates per thread (the default here)
+    MIXED_KERNEL = "mixed_chunk_kernel<BPFixed>"
     kernel_time = {MIXED_KERNEL: [0, 0.0], "fp64_chunk_kernel<BPFixed>": [0, 0.0]}
 
     def one_step(plan):

@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 8
+ABI_VERSION = 7
 
 # crp_status
 OK = 0
@@ -199,8 +199,7 @@ class RunOpts(C.Structure):
                 ("steps_per_launch", C.c_int32), ("refill_threshold", C.c_int32),
                 ("budget_us", C.c_int32), ("max_steps", C.c_uint64),
                 ("cancel", C.POINTER(C.c_int32)), ("stream", C.c_void_p),
-                ("records", C.POINTER(Records)), ("candidates_per_thread", C.c_int32),
-                ("_pad0", C.c_int32)]
+                ("records", C.POINTER(Records))]
 
 
 class AdjointDesc(C.Structure):
@@ -217,7 +216,7 @@ class AdjointIO(C.Structure):
 
 class AutotuneResult(C.Structure):
     _fields_ = [("mode", C.c_int32), ("ctas_per_sm", C.c_int32), ("refill_threshold", C.c_int32),
-                ("burst", C.c_int32), ("trials", C.c_int32), ("candidates_per_thread", C.c_int32),
+                ("burst", C.c_int32), ("trials", C.c_int32), ("_pad0", C.c_int32),
                 ("steps_per_second", _d), ("chunked_steps_per_second", _d)]
 
 

@@ -114,7 +114,6 @@ struct crp_plan {
     // autotuned launch configuration (crp_autotune); mode 0: not tuned
     int tuned_mode = 0;
     int tuned_ctas = 0, tuned_refill = 0, tuned_burst = 0;
-    int tuned_per_thread = 0;  // chunked mode, 0: untuned
     int num_sms = 0;
     // device copy of a sample for the autotuner's trials
     uint64_t trial_n = 0;
@@ -818,10 +817,6 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
     DevRecords rec = to_dev_records(o.records);
     int block = o.block_size > 0 ? o.block_size : (p->tuned_block > 0 ? p->tuned_block : 128);
     if (block % 32 || block > 1024) return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d", block);
-    if (o.candidates_per_thread < 0 || o.candidates_per_thread > 2)
-        return fail(CRP_ERR_INVALID_ARGUMENT, "candidates_per_thread %d (0, 1 or 2)", o.candidates_per_thread);
-    const int per_thread = o.candidates_per_thread > 0 ? o.candidates_per_thread
-                         : (p->tuned_per_thread > 0 ? p->tuned_per_thread : 2);
     // grid runs with the default launch length are cell-ordered between launches
     const int key_bits = (p->fs == FS_GRID || p->fs == FS_GRID_PERIODIC) ? cell_key_bits(p->dev.fields[0].grid) : 0;
     const bool cell_order = o.steps_per_launch <= 0 && key_bits > 0 && n >= kSortMinCandidates;
@@ -850,8 +845,7 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
         }
         cudaError_t e = (p->precision == CRP_PRECISION_FP64)
             ? launch_fp64_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st)
-            : launch_mixed_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block,
-                                 per_thread, st);
+            : launch_mixed_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st);
         if (e != cudaSuccess) return cuda_fail(e, "stepping kernel launch");
         CUDA_TRY(cudaEventRecord(p->ev1, st));
         CUDA_TRY(cudaMemcpyAsync(p->h_cnt, p->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
@@ -1009,13 +1003,11 @@ crp_status crp_autotune(crp_plan *p, const crp_candidates *c, uint64_t n, uint64
         CUDA_TRY(cudaMemcpyAsync(t.active, c->active, m, cudaMemcpyDeviceToDevice, st));
         return CRP_OK;
     };
-    struct Cfg { int mode, ctas, refill, burst, per_thread; };
-    std::vector<Cfg> cfgs = {{CRP_MODE_CHUNKED, 0, 0, 0, 1}};
-    if (p->precision == CRP_PRECISION_MIXED && mixed_chunk_max_per_thread(p->dev, p->fs) == 2)
-        cfgs.push_back({CRP_MODE_CHUNKED, 0, 0, 0, 2});
+    struct Cfg { int mode, ctas, refill, burst; };
+    std::vector<Cfg> cfgs = {{CRP_MODE_CHUNKED, 0, 0, 0}};
     for (int ctas : {1, 2, 3, 4, 6})
         for (int refill : {1, 8, 16, 32})
-            for (int burst : {4, 16, 64}) cfgs.push_back({CRP_MODE_PERSISTENT, ctas, refill, burst, 1});
+            for (int burst : {4, 16, 64}) cfgs.push_back({CRP_MODE_PERSISTENT, ctas, refill, burst});
     double best = -1, chunked = 0;
     Cfg bestc = cfgs[0];
     int trials = 0;
@@ -1029,25 +1021,22 @@ crp_status crp_autotune(crp_plan *p, const crp_candidates *c, uint64_t n, uint64
         o.steps_per_launch = g.mode == CRP_MODE_PERSISTENT ? g.burst : 0;
         o.max_steps = cap;
         o.stream = stream;
-        o.candidates_per_thread = g.per_thread;
         crp_run_stats rstats{};
         rs = crp_run_device(p, &t, m, &o, &rstats);
         if (rs) return rs;
         trials++;
         const double rate = rstats.device_ms > 0 ? rstats.particle_steps / (rstats.device_ms * 1e-3) : 0;
-        if (g.mode == CRP_MODE_CHUNKED) chunked = std::max(chunked, rate);
+        if (g.mode == CRP_MODE_CHUNKED) chunked = rate;
         if (rate > best) { best = rate; bestc = g; }
     }
     p->tuned_mode = bestc.mode;
     p->tuned_ctas = bestc.ctas;
     p->tuned_refill = bestc.refill;
     p->tuned_burst = bestc.burst;
-    p->tuned_per_thread = bestc.per_thread;
     res->mode = bestc.mode;
     res->ctas_per_sm = bestc.ctas;
     res->refill_threshold = bestc.refill;
     res->burst = bestc.burst;
-    res->candidates_per_thread = bestc.per_thread;
     res->trials = trials;
     res->steps_per_second = best;
     res->chunked_steps_per_second = chunked;

@@ -51,21 +51,15 @@ cudaError_t launch_fp64_persistent(const DevPlan &P, const DevState &s, const Pe
                                    cudaStream_t st);
 
 // step_mixed.cu
-// per_thread: candidates each thread advances (1, or 2 where
-// mixed_chunk_max_per_thread allows it; other values act as 1).
 cudaError_t launch_mixed_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
                                uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
                                const uint32_t *perm, uint32_t *perm_out, int fs, int block,
-                               int per_thread, cudaStream_t st);
+                               cudaStream_t st);
 // step_mixed_bp.cu: the Boris-push part of launch_mixed_chunk
 cudaError_t launch_mixed_bp_chunk(const DevPlan &P, const DevState &s, uint64_t n, int max_steps,
                                   uint64_t step_cap, DevCounters *cnt, const DevRecords &rec,
                                   const uint32_t *perm, uint32_t *perm_out, int fs, int block,
-                                  int per_thread, cudaStream_t st);
-// Candidates per thread the mixed chunked kernel of this chain can take: 2
-// for the fixed-step Boris push over a periodic power-of-two Grid3f followed
-// by MaximumTrajectoryLength (and an Observer), else 1.
-int mixed_chunk_max_per_thread(const DevPlan &P, int fs);
+                                  cudaStream_t st);
 cudaError_t launch_mixed_persistent(const DevPlan &P, const DevState &s, const PersistentArgs &a,
                                     DevCounters *cnt, const DevRecords &rec, int fs, int grid,
                                     cudaStream_t st);

@@ -78,14 +78,15 @@ __device__ __forceinline__ CellFrac grid_cell_load(const DevGrid &g, double x, d
     const unsigned b00 = (unsigned)ix0 * sx + (unsigned)iy0 * sy, b10 = (unsigned)ix1 * sx + (unsigned)iy0 * sy;
     const unsigned b01 = (unsigned)ix0 * sx + (unsigned)iy1 * sy, b11 = (unsigned)ix1 * sx + (unsigned)iy1 * sy;
     const unsigned idx[8] = {b00 + iz0, b10 + iz0, b01 + iz0, b00 + iz1, b10 + iz1, b01 + iz1, b11 + iz0, b11 + iz1};
-    const long long k0 = (long long)idx[0], k7 = (long long)idx[7];
-    if (k0 != cc.cell0 || k7 != cc.cell7) {
+    // in a periodic grid the first corner's index identifies the cell
+    const long long k0 = (long long)idx[0];
+    if (k0 != cc.cell0) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             const float4 v = __ldg(g.values4 + idx[k]);
             cc.corner[k][0] = v.x; cc.corner[k][1] = v.y; cc.corner[k][2] = v.z;
         }
-        cc.cell0 = k0; cc.cell7 = k7;
+        cc.cell0 = k0;
     }
     return f;
 }
@@ -196,10 +197,9 @@ __device__ f3 grid_field(const DevGrid &g, double x, double y, double z) {
 // The table holds the modes in pairs (a, b), 80 bytes = five 16-byte loads:
 // {k kappa / 2 pi times 2^32} of a and b as six FP64, then beta / 2 pi of a
 // and b as unsigned 32-bit fixed-point turns, then A xi of a and b as six
-// FP32.  An odd mode count ends with a zero-amplitude mode.  Two accumulator
-// sets (one per mode of a pair) halve the dependence chain of the sums.  The
-// table is read from global memory (read-only path) or from a copy a kernel
-// staged in shared memory.
+// FP32.  An odd mode count ends with a zero-amplitude mode.  The table is
+// read from global memory (read-only path) or from a copy a kernel staged in
+// shared memory.
 struct PwTab {
     const float4 *pairs;
     int npairs;
@@ -225,11 +225,33 @@ __device__ __forceinline__ float cos_turns(double ps, unsigned beta) {
     return __cosf(twopi * (float)(p - rint(p)));
 }
 
+// One mode pair's contribution to a position's two accumulator sets.
+template <bool FAST>
+__device__ __forceinline__ void pw_pair_add(double2 k0, double2 k1, double2 k2, float4 u, float4 v, double x,
+                                            double y, double z, float (&acc)[6]) {
+    const double p0 = fma(k0.x, x, fma(k0.y, y, k1.x * z));
+    const double p1 = fma(k1.y, x, fma(k2.x, y, k2.y * z));
+    const float c0 = cos_turns<FAST>(p0, __float_as_uint(u.x));
+    const float c1 = cos_turns<FAST>(p1, __float_as_uint(u.y));
+    acc[0] = fmaf(u.z, c0, acc[0]); acc[1] = fmaf(u.w, c0, acc[1]); acc[2] = fmaf(v.x, c0, acc[2]);
+    acc[3] = fmaf(v.y, c1, acc[3]); acc[4] = fmaf(v.z, c1, acc[4]); acc[5] = fmaf(v.w, c1, acc[5]);
+}
+
+// The modes are summed in kPwGroups groups of consecutive pairs (group g:
+// pairs [g np / 4, (g + 1) np / 4)), each with two accumulator sets (one per
+// mode of a pair, which halves the dependence chain), and the groups are
+// added as (G0 + G1) + (G2 + G3).  This is the order in which the
+// DiffusionSDE kernel's block evaluates the sum cooperatively (four warps,
+// one group each), so the lane-by-lane sum here gives the same bits.
+constexpr int kPwGroups = 4;
+
+__device__ __forceinline__ int pw_group_begin(int npairs, int g) { return (g * npairs) / kPwGroups; }
+
 template <bool SHARED, bool FAST>
-__device__ __forceinline__ f3 pw_sum_t(const float4 *tab, int npairs, double x, double y, double z) {
-    float bx0 = 0.f, by0 = 0.f, bz0 = 0.f, bx1 = 0.f, by1 = 0.f, bz1 = 0.f;
+__device__ __forceinline__ f3 pw_group_sum(const float4 *tab, int q0, int q1, double x, double y, double z) {
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 4
-    for (int q = 0; q < npairs; q++) {
+    for (int q = q0; q < q1; q++) {
         const double2 *kd = reinterpret_cast<const double2 *>(tab + 5 * q);
         double2 k0, k1, k2;
         float4 u, v;
@@ -240,14 +262,22 @@ __device__ __forceinline__ f3 pw_sum_t(const float4 *tab, int npairs, double x, 
             k0 = __ldg(kd); k1 = __ldg(kd + 1); k2 = __ldg(kd + 2);
             u = __ldg(tab + 5 * q + 3); v = __ldg(tab + 5 * q + 4);
         }
-        const double p0 = fma(k0.x, x, fma(k0.y, y, k1.x * z));
-        const double p1 = fma(k1.y, x, fma(k2.x, y, k2.y * z));
-        const float c0 = cos_turns<FAST>(p0, __float_as_uint(u.x));
-        const float c1 = cos_turns<FAST>(p1, __float_as_uint(u.y));
-        bx0 = fmaf(u.z, c0, bx0); by0 = fmaf(u.w, c0, by0); bz0 = fmaf(v.x, c0, bz0);
-        bx1 = fmaf(v.y, c1, bx1); by1 = fmaf(v.z, c1, by1); bz1 = fmaf(v.w, c1, bz1);
+        pw_pair_add<FAST>(k0, k1, k2, u, v, x, y, z, acc);
     }
-    return f3mk(bx0 + bx1, by0 + by1, bz0 + bz1);
+    return f3mk(acc[0] + acc[3], acc[1] + acc[4], acc[2] + acc[5]);
+}
+
+__device__ __forceinline__ f3 pw_combine(f3 g0, f3 g1, f3 g2, f3 g3) {
+    return f3mk((g0.x + g1.x) + (g2.x + g3.x), (g0.y + g1.y) + (g2.y + g3.y), (g0.z + g1.z) + (g2.z + g3.z));
+}
+
+template <bool SHARED, bool FAST>
+__device__ __forceinline__ f3 pw_sum_t(const float4 *tab, int npairs, double x, double y, double z) {
+    const f3 g0 = pw_group_sum<SHARED, FAST>(tab, pw_group_begin(npairs, 0), pw_group_begin(npairs, 1), x, y, z);
+    const f3 g1 = pw_group_sum<SHARED, FAST>(tab, pw_group_begin(npairs, 1), pw_group_begin(npairs, 2), x, y, z);
+    const f3 g2 = pw_group_sum<SHARED, FAST>(tab, pw_group_begin(npairs, 2), pw_group_begin(npairs, 3), x, y, z);
+    const f3 g3 = pw_group_sum<SHARED, FAST>(tab, pw_group_begin(npairs, 3), npairs, x, y, z);
+    return pw_combine(g0, g1, g2, g3);
 }
 
 template <bool SHARED>
@@ -401,8 +431,9 @@ __device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double 
 // Multiply-adds here are written out (fma) so that the result does not
 // depend on how the compiler contracts the expression in each kernel that
 // inlines it: the chunked and persistent launches must agree bit for bit.
-__device__ __forceinline__ f3 component_field(const DevComponent &f, double x, double y, double z,
-                                             const PwTab *sh = nullptr) {
+// PeriodicMagneticField's map of a position into the component's cell
+// (MagneticField.cpp:41-58).
+__device__ __forceinline__ void component_position(const DevComponent &f, double &x, double &y, double &z) {
     if (f.periodic) {
         double qx = x - f.po[0], qy = y - f.po[1], qz = z - f.po[2];
         double nx = floor(qx / f.pe[0]), ny = floor(qy / f.pe[1]), nz = floor(qz / f.pe[2]);
@@ -413,6 +444,11 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
             if ((long long)fabs(nz) % 2 == 1) z = f.pe[2] - z;
         }
     }
+}
+
+__device__ __forceinline__ f3 component_field(const DevComponent &f, double x, double y, double z,
+                                             const PwTab *sh = nullptr) {
+    component_position(f, x, y, z);
     switch (f.kind) {
     case CRP_FIELD_GRID: return grid_field(f.grid, x, y, z);
     case CRP_FIELD_MODULATED_GRID: {  // MagneticFieldGrid.cpp:51
@@ -521,8 +557,9 @@ struct BP {
         }
         double newStep = step;
         // t = B * q / 2 / m * step / c with m = E/c^2  ->  B * (q c step / (2 E)),
-        // formed in FP32 like the rotation it scales
-        const float kq = __fdividef((float)(q * (0.5 * kCLight)), (float)c.E);
+        // formed in FP32 like the rotation it scales (c.kq, set when the
+        // candidate is loaded)
+        const float kq = c.kq;
         double xo = c.x, yo = c.y, zo = c.z, uxo = c.dx, uyo = c.dy, uzo = c.dz;
         if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
             bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, kq * (float)step, &c);

@@ -193,7 +193,7 @@ extern "C" crp_status crp_run_device_noalloc(const crp_noalloc_grid_bp_desc *d,
         if (e != cudaSuccess) return cuda_noalloc_fail(e, "clearing the scratch counters");
         e = (d->precision == CRP_PRECISION_FP64)
             ? launch_fp64_chunk(P, s, n_threads, spl, 0, cnt, rec, list_in, list_out, FS_GRID, 128, stm)
-            : launch_mixed_chunk(P, s, n_threads, spl, 0, cnt, rec, list_in, list_out, FS_GRID, 128, 1, stm);
+            : launch_mixed_chunk(P, s, n_threads, spl, 0, cnt, rec, list_in, list_out, FS_GRID, 128, stm);
         if (e != cudaSuccess) return cuda_noalloc_fail(e, "stepping kernel launch");
         DevCounters h;
         e = cudaMemcpyAsync(&h, cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, stm);

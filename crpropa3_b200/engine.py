@@ -47,10 +47,9 @@ class Plan:
     @staticmethod
     def _opts(mode=_abi.MODE_AUTO, block_size=0, steps_per_launch=0, max_steps=0, stream=None,
               records: Optional[RecordArrays] = None, cancel=None, ctas_per_sm=0,
-              refill_threshold=0, budget_us=0, candidates_per_thread=0):
+              refill_threshold=0, budget_us=0):
         o = _abi.RunOpts()
         o.mode, o.block_size, o.steps_per_launch = mode, block_size, steps_per_launch
-        o.candidates_per_thread = candidates_per_thread
         o.max_steps, o.ctas_per_sm, o.refill_threshold = max_steps, ctas_per_sm, refill_threshold
         o.budget_us = budget_us
         o.stream = stream

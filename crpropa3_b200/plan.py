@@ -246,6 +246,13 @@ class ChainSpec:
     seed: int = 0
     _keep: list = field(default_factory=list, repr=False)
 
+    def __getstate__(self):
+        # the ctypes views of the last desc() are not picklable; desc()
+        # rebuilds them
+        state = dict(self.__dict__)
+        state["_keep"] = []
+        return state
+
     def desc(self) -> _abi.PlanDesc:
         self._keep = []
         comps = (_abi.FieldComponent * max(1, len(self.fields)))()

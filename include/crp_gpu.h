@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 8u
+#define CRP_ABI_VERSION 7u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -364,11 +364,6 @@ typedef struct crp_run_opts {
     volatile int32_t *cancel;  /* host flag polled between launches, may be NULL */
     void *stream;              /* cudaStream_t, NULL: the legacy default stream */
     crp_records *records;      /* may be NULL */
-    int32_t candidates_per_thread; /* chunked mode: candidates one thread advances; 0: the tuned
-                                      value, else 2 where the chain allows it (mixed fixed-step
-                                      PropagationBP over a periodic power-of-two Grid3f followed
-                                      by MaximumTrajectoryLength [and an Observer]), else 1 */
-    int32_t _pad0;
 } crp_run_opts;
 
 typedef struct crp_run_stats {
@@ -418,7 +413,7 @@ typedef struct crp_autotune_result {
     int32_t refill_threshold;
     int32_t burst;             /* chain iterations between refills */
     int32_t trials;
-    int32_t candidates_per_thread; /* chunked mode */
+    int32_t _pad0;
     double steps_per_second;   /* of the chosen configuration on the sample */
     double chunked_steps_per_second;
 } crp_autotune_result;

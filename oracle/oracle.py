@@ -296,6 +296,33 @@ class Reference:
             _dptr(src_pos), _dptr(src_dir)))
 
 
+def _reference_worker(spec, arrays, n, cr_pow, threads):
+    c = CandidateArrays.__new__(CandidateArrays)
+    c.n, c.device = n, None
+    for name in CandidateArrays.MEMBERS:
+        setattr(c, name, arrays.get(name))
+    Reference(cr_pow=cr_pow).run(spec, c, threads=threads)
+    return {name: getattr(c, name) for name in CandidateArrays.MEMBERS if getattr(c, name) is not None}
+
+
+def run_reference_isolated(spec, cands: CandidateArrays, cr_pow=False, threads=0) -> CandidateArrays:
+    """Reference.run on a copy of the candidates in a freshly spawned process,
+    for callers whose own process has run CUDA work: on the GPU box such
+    in-process runs of the reference returned differing current_step and
+    flags for every candidate of an adaptive Cash-Karp chain (the cause was
+    not found), while a clean process reproduced the device bit for bit."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    arrays = {name: getattr(cands, name) for name in cands.MEMBERS if getattr(cands, name) is not None}
+    # a failed child raises here (BrokenProcessPool) instead of being respawned
+    with ProcessPoolExecutor(max_workers=1, mp_context=mp.get_context("spawn")) as ex:
+        out = ex.submit(_reference_worker, spec, arrays, cands.n, cr_pow, threads).result()
+    c = cands.copy()
+    for name, a in out.items():
+        setattr(c, name, a)
+    return c
+
+
 def plugin_harness_available() -> bool:
     return os.path.exists(REF_GPU_LIB)
 

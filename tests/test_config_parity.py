@@ -24,8 +24,9 @@ compaction.  Only the first candidates (at least 1536) go through the
 reference: the device result must not depend on which other candidates share
 the run.
 
-Tolerances: fixed-step Boris push bit-identical to the reference's parity
-build.  Adaptive Cash-Karp: bit-identical to the reference's sources linked
+The reference runs in a spawned process without CUDA (oracle.
+run_reference_isolated).  Tolerances: fixed-step Boris push bit-identical to
+the reference's parity build.  Adaptive Cash-Karp: bit-identical to the reference's sources linked
 with the engine's correctly rounded pow (the only call whose rounding the
 C library does not fix; libcrp_ref_crpow.so); against the C library's pow a
 last-bit difference in one controller decision changes the rest of that
@@ -67,10 +68,11 @@ def _device_run(spec, cands, **kw):
 
 
 def _reference_run(spec, cands, k, cr_pow=False):
-    ref = _reference(cr_pow)
-    sub = cands.head(k)
-    ref.run(spec, sub)
-    return sub
+    """The reference on the first k candidates, in a spawned process without
+    CUDA (see oracle.run_reference_isolated)."""
+    from oracle import run_reference_isolated
+    _reference(cr_pow)  # skips when not built
+    return run_reference_isolated(spec, cands.head(k), cr_pow=cr_pow)
 
 
 def _bitwise(a, b, mask=None):
@@ -126,14 +128,11 @@ def test_cash_karp_workload_fp64_matches_reference():
     head = got.head(k)
     ref_cr = _reference_run(spec, cands, k, cr_pow=True)
     _assert_bitwise(head, ref_cr, stable[:k], "grid_ck_64 vs reference with correctly rounded pow")
+    # the C library's pow: one misrounded controller decision changes the rest
+    # of that trajectory; on this workload (steps mostly at maxStep) it is rare
     ref = _reference_run(spec, cands, k)
     same = _bitwise(head, ref, stable[:k])
     assert same.mean() >= 0.8, same.mean()
-    # where the C library's pow differs, the trajectories still end within the
-    # integrator's accuracy of each other (tolerance 1e-4 per step)
-    pa, pb = head.position()[stable[:k]], ref.position()[stable[:k]]
-    err = np.linalg.norm(pa - pb, axis=1) / np.linalg.norm(pb, axis=1)
-    assert np.median(err) == 0.0
 
 
 @pytest.mark.parametrize("mode", [_abi.MODE_CHUNKED, _abi.MODE_PERSISTENT], ids=["chunked", "persistent"])

@@ -124,18 +124,27 @@ def test_sde_exit_distributions_match_reference(oracle, reference):
     assert stats.ks_2samp(gz, rz).pvalue > 1e-4
 
 
-@pytest.mark.parametrize("field", ["plane_wave", "toroidal_plus_waves", "grid"])
+@pytest.mark.parametrize("field", ["plane_wave", "toroidal_plus_waves", "toroidal_plus_1024_waves",
+                                   "six_waves_periodic", "grid"])
 def test_sde_mixed_coroutine_kernel_equals_per_lane_kernel(oracle, field):
     """The mixed form's chunked launches run DiffusionSDE as a coroutine
-    (converged field passes for all waiting lanes); its persistent launches
-    run the per-lane step.  Same arithmetic, so bit-identical results."""
+    whose plane-wave sums the block evaluates together (four warps, one
+    mode group each; a grid field: converged passes of the waiting lanes);
+    its persistent launches run the per-lane step.  Same arithmetic in the
+    same order, so bit-identical results.  Six modes make three pairs, so
+    one of the four mode groups is empty."""
     from helpers import random_grid
     from crpropa3_b200.engine import Plan
-    xi, kappa, k, beta, ak = oracle.plane_wave_modes(0.5 * U.muG, 1 * U.pc, 100 * U.pc, 1.0, 5 / 3, 4.0, 64, 11)
-    pw = P.PlaneWaveField(xi, kappa, k, beta, ak, spectrum=(0.5 * U.muG, 1 * U.pc, 100 * U.pc, 1.0, 5 / 3, 4.0),
-                          seed=11)
+    spectrum = (0.5 * U.muG, 1 * U.pc, 100 * U.pc, 1.0, 5 / 3, 4.0)
+    nm = {"toroidal_plus_1024_waves": 1024, "six_waves_periodic": 6}.get(field, 64)
+    xi, kappa, k, beta, ak = oracle.plane_wave_modes(*spectrum, nm, 11)
+    pw = P.PlaneWaveField(xi, kappa, k, beta, ak, spectrum=spectrum, seed=11)
+    if field == "six_waves_periodic":
+        pw.periodic = ((-100 * U.pc,) * 3, (250 * U.pc,) * 3, True)
     fields = {"plane_wave": [pw],
               "toroidal_plus_waves": [P.ToroidalField(1 * U.muG), pw],
+              "toroidal_plus_1024_waves": [P.ToroidalField(1 * U.muG), pw],
+              "six_waves_periodic": [P.ToroidalField(1 * U.muG), pw],
               "grid": [P.GridField(random_grid(np.random.default_rng(5), 16, brms=1e-10),
                                    (-8 * U.pc,) * 3, (1 * U.pc,) * 3)]}[field]
     obs = P.ObserverSpec(_abi.OBSERVER_SURFACE_SPHERE, (0, 0, 0), 300 * U.pc, True, True)
@@ -154,3 +163,77 @@ def test_sde_mixed_coroutine_kernel_equals_per_lane_kernel(oracle, field):
         np.testing.assert_array_equal(getattr(ha, m), getattr(hb, m), err_msg=m)
     assert sa.particle_steps == sb.particle_steps and sa.tries == sb.tries
     assert sa.launches > 1
+
+
+def _galactic(n, precision, sphere):
+    """The DiffusionSDE workload: 1 muG toroidal field plus 1024-mode
+    PlaneWaveTurbulence (0.5 muG, 1-100 pc), epsilon 0.1, 0.1-100 pc steps,
+    tolerance 1e-4, protons log-uniform 1 TeV - 1 PeV from (8.5 kpc, 0, 0),
+    absorbed by an Observer sphere of radius `sphere` around the origin."""
+    from crpropa3_b200 import workloads as W
+    spec, cands = W.sde_galactic(n=n, precision=precision)
+    spec.modules[1].radius = sphere
+    spec.modules[1].record = True
+    return spec, cands
+
+
+def _exit_records(plan_or_ref, spec, cands, n_rec, **kw):
+    from crpropa3_b200.state import RecordArrays
+    r = RecordArrays(n_rec)
+    if hasattr(plan_or_ref, "field"):  # an engine Plan
+        plan_or_ref.run(cands, records=r)
+    else:
+        plan_or_ref.run(spec, cands, r, **kw)
+    return r.sorted()
+
+
+def _exit_stats(r):
+    pos = np.stack([r["x"], r["y"], r["z"]], axis=1)
+    return r["time"], pos[:, 2] / np.linalg.norm(pos, axis=1)
+
+
+def test_sde_galactic_exits_match_reference_at_2kpc(reference):
+    """The DiffusionSDE workload's field, diffusion and energies with the
+    absorbing sphere at 2 kpc and sources at 1 kpc (the 20 kpc sphere takes
+    ~1e5 steps per candidate: ~20 core-minutes of the reference per 1000
+    candidates): exit time and exit direction, device (mixed form, run to
+    absorption) against the reference's ModuleList::run, two-sample KS."""
+    from scipy import stats
+    from crpropa3_b200.engine import Plan
+    from oracle import Reference, reference_available
+    spec, cands = _galactic(8192, _abi.PRECISION_MIXED, 2 * U.kpc)
+    cands.set_position(np.tile([1 * U.kpc, 0.0, 0.0], (cands.n, 1)))
+    gpu = cands.copy()
+    g = _exit_records(Plan(spec), spec, gpu, cands.n)
+    assert len(g["time"]) == cands.n and not gpu.active.any()
+    spec64, _ = _galactic(1, _abi.PRECISION_FP64, 2 * U.kpc)
+    n_ref = 1000
+    ref = cands.head(n_ref)
+    fast = Reference(fast=True) if reference_available(fast=True) else reference
+    r = _exit_records(fast, spec64, ref, n_ref, threads=0, seed=3)
+    assert len(r["time"]) == n_ref
+    gt, gz = _exit_stats(g)
+    rt, rz = _exit_stats(r)
+    assert stats.ks_2samp(gt, rt).pvalue > 1e-4
+    assert stats.ks_2samp(gz, rz).pvalue > 1e-4
+
+
+def test_sde_galactic_full_sphere_mixed_matches_fp64():
+    """The DiffusionSDE workload as stated (20 kpc sphere), run to absorption
+    on the device in both forms: the mixed form's exit time and exit
+    direction distributions against the FP64 form's (two-sample KS)."""
+    from scipy import stats
+    from crpropa3_b200.engine import Plan
+    spec_mx, cands = _galactic(4096, _abi.PRECISION_MIXED, 20 * U.kpc)
+    spec_64, _ = _galactic(1, _abi.PRECISION_FP64, 20 * U.kpc)
+    a, b = cands.to_device("cuda"), cands.head(1024).to_device("cuda")
+    from crpropa3_b200.state import RecordArrays
+    ra, rb = RecordArrays(cands.n, device="cuda"), RecordArrays(1024, device="cuda")
+    Plan(spec_mx).run(a, records=ra)
+    Plan(spec_64).run(b, records=rb)
+    ga, gb = ra.to_host().sorted(), rb.to_host().sorted()
+    assert len(ga["time"]) == cands.n and len(gb["time"]) == 1024
+    at, az = _exit_stats(ga)
+    bt, bz = _exit_stats(gb)
+    assert stats.ks_2samp(at, bt).pvalue > 1e-4
+    assert stats.ks_2samp(az, bz).pvalue > 1e-4
