@@ -373,14 +373,22 @@ def adjoint_cost(dev, args):
         return best
     args6 = (grid, (0, 0, 0), 10 * U.kpc, U.kpc, steps, pos, u0, e, q, tg)
     f_ms = timed(lambda: bp_forward_loss(*args6))
-    fc_ms = timed(lambda: bp_adjoint_forward(*args6, k))
-    tape = bp_adjoint_forward(*args6, k)
-    b_ms = timed(lambda: bp_adjoint_backward(tape))
-    return {"workload": "10^5 antiprotons 5-50 EeV, 128^3 Grid3f 3 nG 10 kpc, 2000 x 1 kpc Boris, K=100",
-            "forward_ms": f_ms, "forward_checkpointed_ms": fc_ms, "backward_ms": b_ms,
-            "cost_ratio": b_ms / f_ms, "cost_ratio_with_checkpointed_forward": (fc_ms + b_ms) / f_ms,
-            "definition": "cost_ratio = reverse pass (recompute from checkpoints + adjoint) / plain forward",
-            "forward_particle_steps_per_s": n * steps / (f_ms / 1e3)}
+    out = {"workload": "10^5 antiprotons 5-50 EeV, 128^3 Grid3f 3 nG 10 kpc, 2000 x 1 kpc Boris",
+           "forward_ms": f_ms, "forward_particle_steps_per_s": n * steps / (f_ms / 1e3),
+           "definition": "cost = what a gradient costs through BorisArrivalLoss (the autograd "
+                         "Function): its forward (loss + checkpoints) plus its backward (recompute "
+                         "between checkpoints + adjoint), over the plain forward pass (loss only)"}
+    for kk in (k, 1):
+        fc_ms = timed(lambda: bp_adjoint_forward(*args6, kk))
+        tape = bp_adjoint_forward(*args6, kk)
+        b_ms = timed(lambda: bp_adjoint_backward(tape))
+        del tape
+        torch.cuda.empty_cache()
+        out[f"checkpoint_every_{kk}"] = {
+            "forward_checkpointed_ms": fc_ms, "backward_ms": b_ms, "cost_ratio": (fc_ms + b_ms) / f_ms,
+            "backward_over_forward": b_ms / f_ms,
+            "checkpoint_bytes": int(((steps + kk - 1) // kk) * 6 * n * 8)}
+    return out
 
 
 def _timed_runs(plan, d_init, d_work, repeats, **kw):
@@ -517,6 +525,34 @@ def cfg_sde_galactic(dev, peaks, n5=1 << 20, cap5=32):
     return out
 
 
+def cfg_grid_ck_nuclei_full(dev, n=1 << 20, repeats=1):
+    """The nuclei workload run to completion (no step cap): chunked launches
+    with compaction and cell ordering, the persistent refill kernel at several
+    launch shapes, and the autotuner's choice, each timed on the device."""
+    import torch
+    from crpropa3_b200 import _abi, engine, workloads as W
+    spec, cands, grid = W.grid_ck_nuclei(n=n, device=dev)
+    plan = engine.Plan(spec)
+    d_init, d_work = cands.to_device(dev), cands.to_device(dev)
+    res = {"workload": f"{n} candidates (H, He-4, N-14, Fe-56), E^-2 0.1-100 EeV, 256^3 Grid3f, "
+                       "PropagationCK 1e-4 0.1-100 kpc, lengths U[1,50] Mpc, every candidate run to its length",
+           "candidates": n, "max_steps_per_candidate": None}
+    rate = lambda t: t["tries"] / (t["device_ms"] / 1e3)
+    t = _timed_runs(plan, d_init, d_work, repeats, mode=_abi.MODE_CHUNKED)
+    res["chunked"] = {"tries_per_s": rate(t), "device_s": t["device_ms"] / 1e3 / repeats,
+                      "launches": t["launches"] // repeats}
+    steps = d_work.step_count.cpu().numpy().astype(np.float64)
+    res["steps_per_candidate"] = {"mean": float(steps.mean()), "median": float(np.median(steps)),
+                                  "p99": float(np.quantile(steps, 0.99)), "max": float(steps.max())}
+    for ctas, refill, burst in ((2, 8, 16), (4, 8, 16), (2, 16, 64), (6, 32, 64)):
+        t = _timed_runs(plan, d_init, d_work, repeats, mode=_abi.MODE_PERSISTENT, ctas_per_sm=ctas,
+                        refill_threshold=refill, steps_per_launch=burst)
+        res[f"persistent_c{ctas}_r{refill}_b{burst}"] = {"tries_per_s": rate(t),
+                                                         "device_s": t["device_ms"] / 1e3 / repeats}
+    plan.close()
+    return {"grid_ck_nuclei_full": res}
+
+
 def cfg_sde_galactic_full(dev, n=1 << 16):
     """The DiffusionSDE workload run to absorption at the 20 kpc sphere (no
     step cap): n candidates, mixed form, one run after a capped warm-up."""
@@ -634,6 +670,7 @@ def main():
                 "grid_ck_nuclei": lambda: cfg_grid_ck_nuclei(dev, {}, n3=args.n or (1 << 20)),
                 "sde_galactic": lambda: cfg_sde_galactic(dev, {}, n5=args.n or (1 << 20)),
                 "sde_galactic_full": lambda: cfg_sde_galactic_full(dev, n=args.n or (1 << 16)),
+                "grid_ck_nuclei_full": lambda: cfg_grid_ck_nuclei_full(dev, n=args.n or (1 << 20)),
                 "jf12_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20)),
                 "uf23_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="uf23"),
                 "pt11_backtrack": lambda: cfg_jf12_backtrack(dev, {}, n=args.n or (1 << 20), model="pt11"),

@@ -52,9 +52,15 @@ __device__ __forceinline__ double norm(v3 a) { return sqrt(a.x * a.x + a.y * a.y
 struct AdjGrid {
     const float *g;
     int nx, ny, nz;
+    bool pow2;  // every dimension a power of two: indices wrap with a mask
     double gox, goy, goz, sx, sy, sz;
     double isx, isy, isz;  // 1 / spacing
 };
+
+// periodic index: i mod n in [0, n) (a mask for power-of-two n, the same value)
+__device__ __forceinline__ int wrap_index(int i, int n, bool pow2) {
+    return pow2 ? (i & (n - 1)) : ((i % n) + n) % n;
+}
 
 // corner indices, weights and weight gradients of the cell around x
 __device__ __forceinline__ void cell(const AdjGrid &G, v3 x, size_t idx[8], double w[8], double dw[8][3]) {
@@ -66,8 +72,8 @@ __device__ __forceinline__ void cell(const AdjGrid &G, v3 x, size_t idx[8], doub
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         double fl = floor(r[a]);
-        lo[a] = (((int)fl % n[a]) + n[a]) % n[a];
-        hi[a] = (lo[a] + 1) % n[a];
+        lo[a] = wrap_index((int)fl, n[a], G.pow2);
+        hi[a] = G.pow2 ? (lo[a] + 1) & (n[a] - 1) : (lo[a] + 1) % n[a];
         f0[a] = r[a] - fl;
         f1[a] = 1 - f0[a];
     }
@@ -168,8 +174,8 @@ __device__ __forceinline__ CellW cellw(const AdjGrid &G, v3 x) {
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         const double fl = floor(r[a]);
-        c.lo[a] = (((int)fl % n[a]) + n[a]) % n[a];
-        c.hi[a] = (c.lo[a] + 1) % n[a];
+        c.lo[a] = wrap_index((int)fl, n[a], G.pow2);
+        c.hi[a] = G.pow2 ? (c.lo[a] + 1) & (n[a] - 1) : (c.lo[a] + 1) % n[a];
         c.f0[a] = r[a] - fl;
         c.f1[a] = 1 - c.f0[a];
     }
@@ -229,9 +235,11 @@ __global__ void __launch_bounds__(128, 3) reverse_kernel(AdjGrid G, IO io, doubl
         const double *c = ckpt + (size_t)j * 6 * n;
         const int k0 = j * K, k1 = (k0 + K < n_steps) ? k0 + K : n_steps;
         v3 x = mk(c[i], c[n + i], c[2 * n + i]), u = mk(c[3 * n + i], c[4 * n + i], c[5 * n + i]);
+        // the states before each step of the segment (the segment's own end
+        // state is not needed: checkpoint_every = 1 recomputes nothing)
         for (int k = k0; k < k1; k++) {
             xs[k - k0] = x; us[k - k0] = u;
-            step(G, x, u, hh, kappa);
+            if (k + 1 < k1) step(G, x, u, hh, kappa);
         }
         for (int k = k1 - 1; k >= k0; k--) {
             const v3 u0 = us[k - k0];
@@ -341,6 +349,8 @@ AdjGrid make_grid(const crp_adjoint_desc *d) {
     AdjGrid G;
     G.g = d->grid_values;
     G.nx = (int)d->nx; G.ny = (int)d->ny; G.nz = (int)d->nz;
+    auto p2 = [](uint64_t v) { return v && !(v & (v - 1)); };
+    G.pow2 = p2(d->nx) && p2(d->ny) && p2(d->nz);
     G.gox = d->origin[0] + d->spacing[0] / 2;
     G.goy = d->origin[1] + d->spacing[1] / 2;
     G.goz = d->origin[2] + d->spacing[2] / 2;

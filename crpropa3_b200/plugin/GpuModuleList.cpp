@@ -792,9 +792,10 @@ struct GpuModuleList::Impl {
     uint64_t planFingerprint;
     crp_run_stats stats;
     uint64_t events;
+    double eventsPerCandidate;  // most records per candidate seen by this plan's runs
 
     Impl() : precision(CRP_PRECISION_FP64), seed(0), batch(size_t(1) << 20), cpuFallback(false),
-             plan(0), planFingerprint(0), events(0) {
+             plan(0), planFingerprint(0), events(0), eventsPerCandidate(0) {
         std::memset(&stats, 0, sizeof(stats));
     }
     ~Impl() {
@@ -999,6 +1000,7 @@ void GpuModuleList::runDevice(const candidate_vector_t &cands) {
         d.seed = impl->seed;
         check(crp_plan_create(&d, &impl->plan));
         impl->planFingerprint = t.fp.h;
+        impl->eventsPerCandidate = 0;
     }
 
     const bool per = !t.perCandidateKey.empty();
@@ -1026,12 +1028,15 @@ void GpuModuleList::runDevice(const candidate_vector_t &cands) {
     }
 
     // every recording module fires at most once per candidate when it
-    // deactivates; observers that keep candidates active may fire more often
-    // (the run is repeated with the exact count then: the inputs are intact)
+    // deactivates; observers that keep candidates active may fire more often.
+    // The capacity also covers the most records per candidate an earlier run
+    // of this plan produced; when a run still overflows it, the batch is run
+    // again with the exact count (the inputs are intact) and a note says so.
     size_t nrec = 0;
     for (size_t m = 0; m < t.modules.size(); m++) nrec += t.modules[m].record ? 1 : 0;
     Records rec;
-    uint64_t cap = uint64_t(n) * std::max<size_t>(nrec, 1) + 1024;
+    const double per_cand = std::max<double>(double(std::max<size_t>(nrec, 1)), 1.25 * impl->eventsPerCandidate);
+    uint64_t cap = uint64_t(double(n) * per_cand) + 1024;
     for (int attempt = 0;; attempt++) {
         Batch work = b;
         crp_candidates view = work.view();
@@ -1045,9 +1050,12 @@ void GpuModuleList::runDevice(const candidate_vector_t &cands) {
         check(crp_run(impl->plan, &view, n, &o, &impl->stats));
         if (rec.count > cap) {
             if (attempt > 0) throw std::runtime_error("GpuModuleList: record count changed between runs");
+            std::cerr << "GpuModuleList: " << rec.count << " detection/reject records overflowed the "
+                      << cap << " reserved; running the batch of " << n << " candidates again\n";
             cap = rec.count;
             continue;
         }
+        if (n) impl->eventsPerCandidate = std::max(impl->eventsPerCandidate, double(rec.count) / double(n));
         std::swap(b, work);  // keep the results
         break;
     }

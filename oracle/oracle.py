@@ -296,27 +296,38 @@ class Reference:
             _dptr(src_pos), _dptr(src_dir)))
 
 
-def _reference_worker(spec, arrays, n, cr_pow, threads):
+def _reference_worker(spec, arrays, n, cr_pow, threads, fast=False, seed=0, rec_capacity=0):
     c = CandidateArrays.__new__(CandidateArrays)
     c.n, c.device = n, None
     for name in CandidateArrays.MEMBERS:
         setattr(c, name, arrays.get(name))
-    Reference(cr_pow=cr_pow).run(spec, c, threads=threads)
-    return {name: getattr(c, name) for name in CandidateArrays.MEMBERS if getattr(c, name) is not None}
+    rec = RecordArrays(rec_capacity) if rec_capacity else None
+    Reference(fast=fast, cr_pow=cr_pow).run(spec, c, rec, threads=threads, seed=seed)
+    out = {name: getattr(c, name) for name in CandidateArrays.MEMBERS if getattr(c, name) is not None}
+    if rec is not None:
+        out["__records__"] = {name: getattr(rec, name) for name in RecordArrays.MEMBERS}
+        out["__records__"]["count"] = rec.count
+    return out
 
 
-def run_reference_isolated(spec, cands: CandidateArrays, cr_pow=False, threads=0) -> CandidateArrays:
+def run_reference_isolated(spec, cands: CandidateArrays, cr_pow=False, threads=0, fast=False, seed=0,
+                           records: RecordArrays = None) -> CandidateArrays:
     """Reference.run on a copy of the candidates in a freshly spawned process,
     for callers whose own process has run CUDA work: on the GPU box such
     in-process runs of the reference returned differing current_step and
     flags for every candidate of an adaptive Cash-Karp chain (the cause was
-    not found), while a clean process reproduced the device bit for bit."""
+    not found), while a clean process reproduced the device bit for bit.
+    `records` (host RecordArrays) is filled with the run's records."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
     arrays = {name: getattr(cands, name) for name in cands.MEMBERS if getattr(cands, name) is not None}
+    cap = records.capacity if records is not None else 0
     # a failed child raises here (BrokenProcessPool) instead of being respawned
     with ProcessPoolExecutor(max_workers=1, mp_context=mp.get_context("spawn")) as ex:
-        out = ex.submit(_reference_worker, spec, arrays, cands.n, cr_pow, threads).result()
+        out = ex.submit(_reference_worker, spec, arrays, cands.n, cr_pow, threads, fast, seed, cap).result()
+    if records is not None:
+        for name, a in out.pop("__records__").items():
+            getattr(records, name)[...] = a
     c = cands.copy()
     for name, a in out.items():
         setattr(c, name, a)
