@@ -224,9 +224,11 @@ __global__ void __launch_bounds__(128, 3) reverse_kernel(AdjGrid G, IO io, doubl
     v3 xs[kMaxK], us[kMaxK];
     v3 xb = mk(0, 0, 0), ub = mk(-io.tx[i], -io.ty[i], -io.tz[i]);
     double kb = 0;
-    // grid-gradient contributions of the cell the candidate is in, summed in
-    // registers and flushed with atomics when it leaves the cell
+    // the cell the candidate is in: its corner values, and its grid-gradient
+    // contributions summed in registers and flushed with atomics when the
+    // candidate leaves the cell
     int clo[3] = {-1, -1, -1}, chi[3] = {-1, -1, -1};
+    float gc[8][3];
     double gacc[8][3];
 #pragma unroll
     for (int q = 0; q < 8; q++) gacc[q][0] = gacc[q][1] = gacc[q][2] = 0;
@@ -245,11 +247,18 @@ __global__ void __launch_bounds__(128, 3) reverse_kernel(AdjGrid G, IO io, doubl
             const v3 u0 = us[k - k0];
             const v3 x1 = add(xs[k - k0], muls(u0, hh));
             const CellW cw = cellw(G, x1);
-            float gc[8][3];
+            // a new cell: flush the previous cell's gradient, load this one's corners
+            // (a candidate stays in one cell for several steps)
+            if (cw.lo[0] != clo[0] || cw.lo[1] != clo[1] || cw.lo[2] != clo[2] || cw.hi[0] != chi[0] ||
+                cw.hi[1] != chi[1] || cw.hi[2] != chi[2]) {
+                if (acc) flush(G, acc, clo, chi, gacc, scale);
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const float *cg = G.g + 3 * corner_index(G, cw.lo, cw.hi, q);
-                gc[q][0] = __ldg(cg); gc[q][1] = __ldg(cg + 1); gc[q][2] = __ldg(cg + 2);
+                for (int a = 0; a < 3; a++) { clo[a] = cw.lo[a]; chi[a] = cw.hi[a]; }
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const float *cg = G.g + 3 * corner_index(G, cw.lo, cw.hi, q);
+                    gc[q][0] = __ldg(cg); gc[q][1] = __ldg(cg + 1); gc[q][2] = __ldg(cg + 2);
+                }
             }
             v3 B = mk(0, 0, 0);
 #pragma unroll
@@ -279,12 +288,6 @@ __global__ void __launch_bounds__(128, 3) reverse_kernel(AdjGrid G, IO io, doubl
             const v3 Bb = muls(tb, kappa);
             kb += dot(tb, B);
             // reverse of the interpolation: position Jacobian and grid values
-            if (acc && (cw.lo[0] != clo[0] || cw.lo[1] != clo[1] || cw.lo[2] != clo[2] ||
-                        cw.hi[0] != chi[0] || cw.hi[1] != chi[1] || cw.hi[2] != chi[2])) {
-                flush(G, acc, clo, chi, gacc, scale);
-#pragma unroll
-                for (int a = 0; a < 3; a++) { clo[a] = cw.lo[a]; chi[a] = cw.hi[a]; }
-            }
             v3 x1b = xb;
 #pragma unroll
             for (int q = 0; q < 8; q++) {

@@ -31,9 +31,6 @@ struct Cand {
     // the values are the grid's own, so results do not change.
     long long cell0, cell7;
     float corner[8][3];
-    // q c / (2 E) in FP32: the mixed form's Boris factor per unit step
-    // (the energy and charge do not change along these chains)
-    float kq;
 };
 
 __device__ __forceinline__ void load_cand(const DevState &s, uint64_t i, Cand &c) {
@@ -50,7 +47,6 @@ __device__ __forceinline__ void load_cand(const DevState &s, uint64_t i, Cand &c
     c.active = s.active[i] != 0;
     c.cell0 = -1;
     c.cell7 = -1;
-    c.kq = __fdividef((float)(c.q * (0.5 * kCLight)), (float)c.E);
 }
 
 __device__ __forceinline__ void store_cand(const DevState &s, const Cand &c) {

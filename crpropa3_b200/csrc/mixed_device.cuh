@@ -59,11 +59,10 @@ __device__ __forceinline__ int wrap(int i, int n, bool pow2) {
 // cell changes.
 // PER: the grid is periodic with power-of-two dimensions, has no clipVolume
 // and has the padded copy (FS_GRID_PERIODIC): those branches are compiled out.
-// The periodic power-of-two case in two parts, so that a kernel stepping two
-// candidates per thread can issue both candidates' corner loads before it
-// waits for either: grid_cell_load finds the cell of (x, y, z) and, when it
-// is not the cached one, loads its 8 corners into the candidate's cache;
-// grid_cell_interp forms the trilinear sum from the cache.
+// The periodic power-of-two case in two parts: grid_cell_load finds the
+// cell of (x, y, z) and, when it is not the cached one, loads its 8 corners
+// into the candidate's cache; grid_cell_interp forms the trilinear sum from
+// the cache.
 struct CellFrac { float fx0, fy0, fz0; };
 
 __device__ __forceinline__ CellFrac grid_cell_load(const DevGrid &g, double x, double y, double z, Cand &cc) {
@@ -78,15 +77,14 @@ __device__ __forceinline__ CellFrac grid_cell_load(const DevGrid &g, double x, d
     const unsigned b00 = (unsigned)ix0 * sx + (unsigned)iy0 * sy, b10 = (unsigned)ix1 * sx + (unsigned)iy0 * sy;
     const unsigned b01 = (unsigned)ix0 * sx + (unsigned)iy1 * sy, b11 = (unsigned)ix1 * sx + (unsigned)iy1 * sy;
     const unsigned idx[8] = {b00 + iz0, b10 + iz0, b01 + iz0, b00 + iz1, b10 + iz1, b01 + iz1, b11 + iz0, b11 + iz1};
-    // in a periodic grid the first corner's index identifies the cell
-    const long long k0 = (long long)idx[0];
-    if (k0 != cc.cell0) {
+    const long long k0 = (long long)idx[0], k7 = (long long)idx[7];
+    if (k0 != cc.cell0 || k7 != cc.cell7) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             const float4 v = __ldg(g.values4 + idx[k]);
             cc.corner[k][0] = v.x; cc.corner[k][1] = v.y; cc.corner[k][2] = v.z;
         }
-        cc.cell0 = k0;
+        cc.cell0 = k0; cc.cell7 = k7;
     }
     return f;
 }
@@ -557,9 +555,8 @@ struct BP {
         }
         double newStep = step;
         // t = B * q / 2 / m * step / c with m = E/c^2  ->  B * (q c step / (2 E)),
-        // formed in FP32 like the rotation it scales (c.kq, set when the
-        // candidate is loaded)
-        const float kq = c.kq;
+        // formed in FP32 like the rotation it scales
+        const float kq = __fdividef((float)(q * (0.5 * kCLight)), (float)c.E);
         double xo = c.x, yo = c.y, zo = c.z, uxo = c.dx, uyo = c.dy, uzo = c.dz;
         if (MODE == 1 || (MODE == 0 && m.min_step == m.max_step)) {
             bp_dy<FS>(P, xo, yo, zo, uxo, uyo, uzo, step, kq * (float)step, &c);
