@@ -41,7 +41,7 @@ import numpy as np  # noqa: E402
 METRIC = "particle-steps/s, 1 B200: mixed-prec vs FP64 at stated error; adjoint cost/fwd"
 UNIT = "particle-steps/s"
 ALGO_BYTES_PER_STEP = 96  # 8 corners x 12 B Grid3f payload per field evaluation
-TRAFFIC_B_PER_STEP = 14.4  # DRAM read+write per particle-step of the mixed kernel (ncu, full size)
+TRAFFIC_B_PER_STEP = 13.65  # DRAM read+write per particle-step of the mixed kernel (ncu, all launches of a full run)
 
 
 def log(*a):

@@ -209,7 +209,7 @@ __device__ __forceinline__ void flush(const AdjGrid &G, unsigned long long *acc,
     for (int q = 0; q < 8; q++) g[q][0] = g[q][1] = g[q][2] = 0;
 }
 
-__global__ void __launch_bounds__(128, 3) reverse_kernel(AdjGrid G, IO io, double h, int n_steps, int K,
+__global__ void __launch_bounds__(128, 2) reverse_kernel(AdjGrid G, IO io, double h, int n_steps, int K,
                                                       const double *ckpt,
                                                       unsigned long long *acc,
                                                       const unsigned long long *kmax_bits) {

@@ -816,7 +816,9 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
     DevState s = to_dev_state(*c);
     DevRecords rec = to_dev_records(o.records);
     int block = o.block_size > 0 ? o.block_size : (p->tuned_block > 0 ? p->tuned_block : 128);
-    if (block % 32 || block > 1024) return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d", block);
+    if (block % 32 || block <= 0 || block > 128)
+        return fail(CRP_ERR_INVALID_ARGUMENT, "block size %d: a multiple of 32 up to 128 (the stepping kernels' "
+                    "launch bound)", block);
     // grid runs with the default launch length are cell-ordered between launches
     const int key_bits = (p->fs == FS_GRID || p->fs == FS_GRID_PERIODIC) ? cell_key_bits(p->dev.fields[0].grid) : 0;
     const bool cell_order = o.steps_per_launch <= 0 && key_bits > 0 && n >= kSortMinCandidates;

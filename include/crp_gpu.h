@@ -355,7 +355,7 @@ enum crp_run_mode {
 
 typedef struct crp_run_opts {
     int32_t mode;
-    int32_t block_size;        /* 0: autotuned */
+    int32_t block_size;        /* 0: autotuned; else a multiple of 32 up to 128 */
     int32_t ctas_per_sm;       /* 0: autotuned (persistent mode) */
     int32_t steps_per_launch;  /* 0: default (chunked mode) */
     int32_t refill_threshold;  /* persistent: lanes idle before a warp refills, 0: autotuned */
