@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 # crp_status
 OK = 0
@@ -34,8 +34,13 @@ STATUS_NAMES = {
 }
 
 FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID, FIELD_JF12, FIELD_UF23, \
-    FIELD_PT11, FIELD_ARCHIMEDEAN_SPIRAL = 1, 2, 3, 4, 5, 6, 7, 8, 9
+    FIELD_PT11, FIELD_ARCHIMEDEAN_SPIRAL, FIELD_TF17, FIELD_SINGLE_MODE = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
 PT11_ASS, PT11_BSS, PT11_HALO = 0, 1, 2
+TF17_AD1, TF17_BD1, TF17_DD1 = 0, 1, 2
+TF17_C0, TF17_C1 = 0, 1
+SINGLE_MODE_AMPLITUDE, SINGLE_MODE_RMS = 0, 1
+SINGLE_MODE_POLARIZATION, SINGLE_MODE_HELICITY = 0, 1
+SINGLE_MODE_ELLIPTICAL, SINGLE_MODE_CIRCULAR, SINGLE_MODE_LINEAR = 0, 1, 2
 UF23_BASE, UF23_NECL, UF23_EXPX, UF23_SPUR, UF23_CRE10, UF23_SYNCG, UF23_TWISTX, UF23_NEBCOR = range(8)
 JF12_VARIANT_JF12, JF12_VARIANT_PLANCK = 0, 1
 INTERPOLATION_TRILINEAR, INTERPOLATION_TRICUBIC, INTERPOLATION_NEAREST_NEIGHBOUR = 0, 1, 2
@@ -108,13 +113,28 @@ class ArchimedeanDesc(C.Structure):
     _fields_ = [("b0", _d), ("r0", _d), ("omega", _d), ("vw", _d)]
 
 
+class TF17Desc(C.Structure):
+    _fields_ = [("disk_model", C.c_int32), ("halo_model", C.c_int32), ("use_disk", C.c_int32),
+                ("use_halo", C.c_int32)] + [
+        (n, _d) for n in ("a_disk", "z1_disk", "r1_disk", "b1_disk", "l_disk", "phi_star_disk", "h_disk",
+                          "a_halo", "z1_halo", "b1_halo", "l_halo", "phi_star_halo",
+                          "p0", "cot_p0", "h_p", "l_p", "epsilon")]
+
+
+class SingleModeDesc(C.Structure):
+    _fields_ = [("b_max", _d), ("sigma", _d), ("r0", _d * 3), ("u1", _d * 3), ("u2", _d * 3), ("k", _d * 3),
+                ("b0", _d), ("wavelength", _d), ("e1", _d * 3), ("e2", _d * 3),
+                ("amplitude_rms", C.c_int32), ("polarization_helicity", C.c_int32), ("mode", C.c_int32),
+                ("_pad", C.c_int32)]
+
+
 class FieldComponent(C.Structure):
     _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
                 ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
                 ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
                 ("toroidal_b0", _d), ("modulation", GridDesc), ("jf12", JF12Desc),
                 ("uf23", UF23Desc), ("pt11", PT11Desc),
-                ("archimedean", ArchimedeanDesc)]
+                ("archimedean", ArchimedeanDesc), ("tf17", TF17Desc), ("single_mode", SingleModeDesc)]
 
 
 class FeatureDesc(C.Structure):

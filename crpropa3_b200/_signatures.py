@@ -38,6 +38,9 @@ SIGNATURES = {
     "crp_uf23_defaults": (_i32, [_i32, C.POINTER(_abi.UF23Desc)]),
     "crp_pt11_defaults": (_i32, [C.POINTER(_abi.PT11Desc)]),
     "crp_pt11_use": (_i32, [C.POINTER(_abi.PT11Desc), _i32, _i32]),
+    "crp_tf17_defaults": (_i32, [_i32, _i32, C.POINTER(_abi.TF17Desc)]),
+    "crp_single_mode_field": (_i32, [_d, _d, _d, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), _i32, _i32, _i32,
+                                     C.POINTER(_abi.SingleModeDesc)]),
     "crp_turbulence_draws": (_i32, [_u32, _i32, _u64, _dp]),
     "crp_turbulence_modes": (_i32, [C.POINTER(_abi.TurbulenceDesc), C.POINTER(C.c_uint64)]),
     "crp_turbulence_grid": (_i32, [C.POINTER(_abi.TurbulenceDesc), C.c_void_p, C.c_void_p]),

@@ -366,6 +366,17 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             return fail(CRP_ERR_INVALID_ARGUMENT, "PT11Field: parameters not set (crp_pt11_defaults)");
         crp_status st = upload(p, &T, 1, &d.pt);
         if (st) return st;
+    } else if (f.kind == CRP_FIELD_TF17) {
+        const crp_tf17_desc &T = f.tf17;
+        if (T.disk_model < CRP_TF17_AD1 || T.disk_model > CRP_TF17_DD1 || T.halo_model < CRP_TF17_C0 ||
+            T.halo_model > CRP_TF17_C1)
+            return fail(CRP_ERR_INVALID_ARGUMENT, "TF17Field: unknown disk or halo model");
+        if (!(T.h_p > 0) || !(T.l_p > 0))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "TF17Field: parameters not set (crp_tf17_defaults)");
+        crp_status st = upload(p, &T, 1, &d.tf);
+        if (st) return st;
+    } else if (f.kind == CRP_FIELD_SINGLE_MODE) {
+        d.mode = f.single_mode;
     } else if (f.kind == CRP_FIELD_ARCHIMEDEAN_SPIRAL) {
         d.arch = f.archimedean;
     } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {

@@ -74,6 +74,8 @@ struct DevComponent {
     const DevJF12 *jf;  // CRP_FIELD_JF12: device copy of the parameters
     const DevUF23 *uf;        // CRP_FIELD_UF23: device copy of the parameters
     const crp_pt11_desc *pt;  // CRP_FIELD_PT11: device copy of the parameters
+    const crp_tf17_desc *tf;  // CRP_FIELD_TF17: device copy of the parameters
+    crp_single_mode_desc mode;  // CRP_FIELD_SINGLE_MODE
     crp_archimedean_desc arch;  // CRP_FIELD_ARCHIMEDEAN_SPIRAL
 };
 

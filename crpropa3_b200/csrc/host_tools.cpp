@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cinttypes>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -358,6 +359,125 @@ crp_status crp_pt11_defaults(crp_pt11_desc *out) {
     p.z11_h = 0.25 * kpc;
     p.z12_h = 0.4 * kpc;
     return crp_pt11_use(out, CRP_PT11_ASS, 1);
+}
+
+// TF17Field(disk, halo) (TF17Field.cpp:10-118): the parameters of the six model combinations,
+// formed with the constructor's own expressions, and set_p0's cotangent (TF17Field.cpp:146)
+// through the C library at run time.
+crp_status crp_tf17_defaults(int32_t disk, int32_t halo, crp_tf17_desc *out) {
+    if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (disk < CRP_TF17_AD1 || disk > CRP_TF17_DD1 || halo < CRP_TF17_C0 || halo > CRP_TF17_C1)
+        return host_fail(CRP_ERR_INVALID_ARGUMENT, "TF17Field: unknown disk or halo model");
+    const double au = 149597870700.0, parsec = 648000 / M_PI * au, kpc = 1e3 * parsec;
+    const double muG = 1e-6 * 1e-4;
+    crp_tf17_desc &t = *out;
+    std::memset(&t, 0, sizeof(t));
+    t.disk_model = disk;
+    t.halo_model = halo;
+    t.use_disk = 1;
+    t.use_halo = 1;
+    double p0 = 0;
+    if (halo == CRP_TF17_C0 && disk == CRP_TF17_AD1) {
+        t.r1_disk = 3 * kpc; t.b1_disk = 19.0 * muG; t.h_disk = 0.055 * kpc;
+        t.phi_star_disk = -54 * M_PI / 180; t.a_disk = 0.9 / kpc / kpc;
+        t.z1_halo = 0; t.b1_halo = 0.36 * muG; t.l_halo = 3.0 * kpc; t.a_halo = 1.17 / kpc / kpc;
+        p0 = -7.9 * M_PI / 180; t.h_p = 5 * kpc; t.l_p = 50 * kpc;
+    } else if (halo == CRP_TF17_C0 && disk == CRP_TF17_BD1) {
+        t.r1_disk = 3 * kpc; t.b1_disk = 2.0 * muG; t.h_disk = 0.32 * kpc;
+        t.phi_star_disk = 153 * M_PI / 180;
+        t.z1_halo = 0; t.b1_halo = 0.29 * muG; t.l_halo = 3.4 * kpc; t.a_halo = 0.88 / kpc / kpc;
+        p0 = -7.2 * M_PI / 180; t.h_p = 9 * kpc; t.l_p = 50 * kpc;
+    } else if (halo == CRP_TF17_C0 && disk == CRP_TF17_DD1) {
+        t.z1_disk = 1.5 * kpc; t.b1_disk = 0.065 * muG; t.l_disk = 9.8 * kpc;
+        t.phi_star_disk = 14 * M_PI / 180;
+        t.z1_halo = 0; t.b1_halo = 0.18 * muG; t.l_halo = 4.8 * kpc; t.a_halo = 0.61 / kpc / kpc;
+        p0 = -7.4 * M_PI / 180; t.h_p = 4.2 * kpc; t.l_p = 50 * kpc;
+    } else if (halo == CRP_TF17_C1 && disk == CRP_TF17_AD1) {
+        t.r1_disk = 3 * kpc; t.b1_disk = 32.0 * muG; t.h_disk = 0.054 * kpc;
+        t.phi_star_disk = -31 * M_PI / 180; t.a_disk = 0.031 / kpc / kpc;
+        t.z1_halo = 0; t.b1_halo = 9.0 * muG; t.l_halo = 2.1 * kpc;
+        t.phi_star_halo = 198 * M_PI / 180; t.a_halo = 0.33 / kpc / kpc;
+        p0 = -9.1 * M_PI / 180; t.h_p = 1.2 * kpc; t.l_p = 50 * kpc;
+    } else if (halo == CRP_TF17_C1 && disk == CRP_TF17_BD1) {
+        t.r1_disk = 3 * kpc; t.b1_disk = 24 * muG; t.h_disk = 0.090 * kpc;
+        t.phi_star_disk = -34 * M_PI / 180;
+        t.z1_halo = 0; t.b1_halo = 8.2 * muG; t.l_halo = 2.2 * kpc;
+        t.phi_star_halo = 197 * M_PI / 180; t.a_halo = 0.38 / kpc / kpc;
+        p0 = -9.0 * M_PI / 180; t.h_p = 1.2 * kpc; t.l_p = 50 * kpc;
+    } else {  // C1, Dd1
+        t.z1_disk = 1.5 * kpc; t.b1_disk = 0.40 * muG; t.l_disk = 2.9 * kpc;
+        t.phi_star_disk = 120 * M_PI / 180;
+        t.z1_halo = 0; t.b1_halo = 9.5 * muG; t.l_halo = 2.1 * kpc;
+        t.phi_star_halo = 179 * M_PI / 180; t.a_halo = 0.45 / kpc / kpc;
+        p0 = -8.4 * M_PI / 180; t.h_p = 1.2 * kpc; t.l_p = 50 * kpc;
+    }
+    t.p0 = p0;
+    volatile double vp0 = p0;
+    t.cot_p0 = std::cos(vp0) / std::sin(vp0);
+    t.epsilon = std::numeric_limits<double>::epsilon();
+    return CRP_OK;
+}
+
+// PolarizedSingleModeMagneticField's constructor (PolarizedSingleModeMagneticField.cpp:5-52):
+// its checks in its order, with its messages, and its derived values with Vector3's arithmetic
+// (getR = sqrt(x*x + y*y + z*z), cross, componentwise scaling).
+crp_status crp_single_mode_field(double b0, double wavelength, double sigma, const double r0[3],
+                                 const double e1[3], const double e2[3], int32_t amplitude_rms,
+                                 int32_t polarization_helicity, int32_t mode, crp_single_mode_desc *out) {
+    if (!out || !r0 || !e1 || !e2) return host_fail(CRP_ERR_INVALID_ARGUMENT, "NULL argument");
+    const char *who = "PolarizedSingleModeMagneticField: ";
+    auto bad = [&](const char *msg) { return host_fail(CRP_ERR_INVALID_ARGUMENT, (std::string(who) + msg).c_str()); };
+    if (mode == CRP_SINGLE_MODE_ELLIPTICAL) {
+        if (std::fabs(sigma) > 1)
+            return bad("The value of the  polarization parameter has to lie in the range [-1;+1].");
+    } else if (mode == CRP_SINGLE_MODE_CIRCULAR) {
+        if (std::fabs(sigma) != 1)
+            return bad("For circular polarization the value of the polarization parameter has to be equal to -1 or +1.");
+    } else if (mode == CRP_SINGLE_MODE_LINEAR) {
+        if (std::fabs(sigma) != 0)
+            return bad("For linear polarization the value of the polarization parameter has to be equal to 0.");
+    } else {
+        return bad("Wrong value for flagMode. Please choose \"elliptical\" or \"circular\" or \"linear\".");
+    }
+    if (e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2] != 0)
+        return bad("e_1 and e_2 have to be orthogonal to each other.");
+    const double r1 = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    if (r1 == 0) return bad("Vector e_1 cannot be zero.");
+    const double r2 = std::sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    if (r2 == 0) return bad("Vector e_2 cannot be zero.");
+    crp_single_mode_desc &d = *out;
+    std::memset(&d, 0, sizeof(d));
+    for (int a = 0; a < 3; a++) {
+        d.u1[a] = e1[a] / r1;
+        d.u2[a] = e2[a] / r2;
+        d.r0[a] = r0[a];
+    }
+    // e_2 x e_1, normalised, times 2 pi / wavelength
+    double k[3] = {e2[1] * e1[2] - e1[1] * e2[2], e2[2] * e1[0] - e1[2] * e2[0], e2[0] * e1[1] - e1[0] * e2[1]};
+    const double rk = std::sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+    for (int a = 0; a < 3; a++) k[a] = k[a] / rk;
+    if (wavelength == 0) return bad("The correlation length cannot be zero.");
+    for (int a = 0; a < 3; a++) d.k[a] = k[a] * 2 * M_PI / wavelength;
+    if (polarization_helicity != CRP_SINGLE_MODE_POLARIZATION && polarization_helicity != CRP_SINGLE_MODE_HELICITY)
+        return bad("Wrong value for flagPolarizationHelicity. Please choose \"polarization\" or \"helicity\".");
+    if (polarization_helicity == CRP_SINGLE_MODE_HELICITY && std::fabs(sigma) != 1)
+        return bad("In helicity mode only the maximum helicity case (sigma = +1 or sigma = -1) may be chosen.");
+    if (amplitude_rms == CRP_SINGLE_MODE_AMPLITUDE) {
+        d.b_max = b0;
+    } else if (amplitude_rms == CRP_SINGLE_MODE_RMS) {
+        volatile double q = 2 / (1 + sigma * sigma);
+        d.b_max = std::sqrt(q) * b0;
+    } else {
+        return bad("Wrong value for flagAmplitudeRms. Please choose \"amplitude\" or \"rms\".");
+    }
+    d.sigma = sigma;
+    d.b0 = b0;
+    d.wavelength = wavelength;
+    for (int a = 0; a < 3; a++) { d.e1[a] = e1[a]; d.e2[a] = e2[a]; }
+    d.amplitude_rms = amplitude_rms;
+    d.polarization_helicity = polarization_helicity;
+    d.mode = mode;
+    return CRP_OK;
 }
 
 crp_status crp_pt11_use(crp_pt11_desc *io, int32_t which, int32_t use) {

@@ -23,6 +23,7 @@
 #include "grid_interp.cuh"
 #include "uf23.cuh"
 #include "pt11.cuh"
+#include "tf17.cuh"
 
 
 // Resident blocks of 128 threads per SM the register budget of the
@@ -467,6 +468,14 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     }
     case CRP_FIELD_ARCHIMEDEAN_SPIRAL: {  // FP64 evaluation, FP32 result
         const u3 b = archimedean_field(f.arch, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
+    case CRP_FIELD_TF17: {  // FP64 evaluation, FP32 result
+        const u3 b = tf17_field(*f.tf, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
+    case CRP_FIELD_SINGLE_MODE: {  // FP64 evaluation (the phase reaches many turns), FP32 result
+        const u3 b = single_mode_field(f.mode, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
     }
     default: {

@@ -21,6 +21,7 @@
 #include "grid_interp.cuh"
 #include "uf23.cuh"
 #include "pt11.cuh"
+#include "tf17.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -335,6 +336,14 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
     }
     case CRP_FIELD_ARCHIMEDEAN_SPIRAL: {
         const u3 b = archimedean_field(f.arch, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
+    case CRP_FIELD_TF17: {
+        const u3 b = tf17_field(*f.tf, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
+    case CRP_FIELD_SINGLE_MODE: {
+        const u3 b = single_mode_field(f.mode, pos.x, pos.y, pos.z);
         return mk(b.x, b.y, b.z);
     }
     default: {

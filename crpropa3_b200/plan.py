@@ -128,6 +128,55 @@ class PT11Field:
 
 
 @dataclass
+class TF17Field:
+    """TF17Field(disk, halo) (TF17Field.cpp:10), the field of Terral &
+    Ferriere 2017: disk model Ad1 (the default), Bd1 or Dd1 and halo model C0
+    or C1 (the default), with setUseDiskField / setUseHaloField."""
+    disk: int = _abi.TF17_AD1
+    halo: int = _abi.TF17_C1
+    use_disk: bool = True
+    use_halo: bool = True
+    periodic: Optional[tuple] = None
+
+    def desc(self) -> "_abi.TF17Desc":
+        """The reference's state after TF17Field(disk, halo) and the switches
+        (crp_tf17_defaults)."""
+        d = _abi.TF17Desc()
+        _abi.check(_abi.load().crp_tf17_defaults(int(self.disk), int(self.halo), C.byref(d)))
+        d.use_disk, d.use_halo = int(bool(self.use_disk)), int(bool(self.use_halo))
+        return d
+
+
+@dataclass
+class SingleModeField:
+    """PolarizedSingleModeMagneticField(B_0, wavelength, sigma, r_0, e_1, e_2,
+    flagAmplitudeRms, flagPolarizationHelicity, flagMode)
+    (PolarizedSingleModeMagneticField.cpp:5): one polarised mode, SI units;
+    the flags as strings, as the reference takes them."""
+    b0: float
+    wavelength: float
+    sigma: float
+    r0: Sequence[float] = (0.0, 0.0, 0.0)
+    e1: Sequence[float] = (1.0, 0.0, 0.0)
+    e2: Sequence[float] = (0.0, 1.0, 0.0)
+    amplitude_rms: str = "amplitude"
+    polarization_helicity: str = "polarization"
+    mode: str = "elliptical"
+    periodic: Optional[tuple] = None
+
+    def desc(self) -> "_abi.SingleModeDesc":
+        """The constructor's checks and derived values (crp_single_mode_field)."""
+        flags = ({"amplitude": 0, "rms": 1}.get(self.amplitude_rms, -1),
+                 {"polarization": 0, "helicity": 1}.get(self.polarization_helicity, -1),
+                 {"elliptical": 0, "circular": 1, "linear": 2}.get(self.mode, -1))
+        d = _abi.SingleModeDesc()
+        v = [(C.c_double * 3)(*map(float, a)) for a in (self.r0, self.e1, self.e2)]
+        _abi.check(_abi.load().crp_single_mode_field(float(self.b0), float(self.wavelength), float(self.sigma),
+                                                     v[0], v[1], v[2], *flags, C.byref(d)))
+        return d
+
+
+@dataclass
 class ArchimedeanSpiralField:
     """ArchimedeanSpiralField(B_0, R_0, Omega, V_w) (ArchimedeanSpiralField.cpp:5):
     a radial field b0 (r0 / r)^2 wound into an Archimedean spiral by the
@@ -311,6 +360,12 @@ class ChainSpec:
         elif isinstance(f, PT11Field):
             c.kind = _abi.FIELD_PT11
             c.pt11 = f.desc()
+        elif isinstance(f, TF17Field):
+            c.kind = _abi.FIELD_TF17
+            c.tf17 = f.desc()
+        elif isinstance(f, SingleModeField):
+            c.kind = _abi.FIELD_SINGLE_MODE
+            c.single_mode = f.desc()
         elif isinstance(f, ArchimedeanSpiralField):
             c.kind = _abi.FIELD_ARCHIMEDEAN_SPIRAL
             c.archimedean.b0, c.archimedean.r0 = float(f.b0), float(f.r0)

@@ -12,6 +12,8 @@
 #include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/PT11Field.h"
 #include "crpropa/magneticField/ArchimedeanSpiralField.h"
+#include "crpropa/magneticField/TF17Field.h"
+#include "crpropa/magneticField/PolarizedSingleModeMagneticField.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
@@ -105,6 +107,25 @@ CRPGPU_PT11(PT11Rc, R_c); CRPGPU_PT11(PT11Z0D, z0_D); CRPGPU_PT11(PT11B0D, B0_D)
 CRPGPU_PT11(PT11R0H, R0_H); CRPGPU_PT11(PT11B0Hn, B0_Hn); CRPGPU_PT11(PT11B0Hs, B0_Hs);
 CRPGPU_PT11(PT11Z11H, z11_H); CRPGPU_PT11(PT11Z12H, z12_H);
 #undef CRPGPU_PT11
+CRPGPU_MEMBER(TF17Disk, TF17Field, TF17DiskModel, disk_model);           // TF17Field.h:27-57
+CRPGPU_MEMBER(TF17Halo, TF17Field, TF17HaloModel, halo_model);
+CRPGPU_MEMBER(TF17UseDisk, TF17Field, bool, useDiskField);
+CRPGPU_MEMBER(TF17UseHalo, TF17Field, bool, useHaloField);
+#define CRPGPU_TF17(TAG, NAME) CRPGPU_MEMBER(TAG, TF17Field, double, NAME)
+CRPGPU_TF17(TF17ADisk, a_disk); CRPGPU_TF17(TF17Z1Disk, z1_disk); CRPGPU_TF17(TF17R1Disk, r1_disk);
+CRPGPU_TF17(TF17B1Disk, B1_disk); CRPGPU_TF17(TF17LDisk, L_disk); CRPGPU_TF17(TF17PhiDisk, phi_star_disk);
+CRPGPU_TF17(TF17HDisk, H_disk); CRPGPU_TF17(TF17AHalo, a_halo); CRPGPU_TF17(TF17Z1Halo, z1_halo);
+CRPGPU_TF17(TF17B1Halo, B1_halo); CRPGPU_TF17(TF17LHalo, L_halo); CRPGPU_TF17(TF17PhiHalo, phi_star_halo);
+CRPGPU_TF17(TF17P0, p_0); CRPGPU_TF17(TF17CotP0, cot_p0); CRPGPU_TF17(TF17Hp, H_p); CRPGPU_TF17(TF17Lp, L_p);
+CRPGPU_TF17(TF17Eps, epsilon);
+#undef CRPGPU_TF17
+// the derived state; the constructor stores no other argument (PolarizedSingleModeMagneticField.cpp:62-63)
+CRPGPU_MEMBER(ModeU1, PolarizedSingleModeMagneticField, Vector3d, unitVector_1);  // PolarizedSingleModeMagneticField.h:34
+CRPGPU_MEMBER(ModeU2, PolarizedSingleModeMagneticField, Vector3d, unitVector_2);
+CRPGPU_MEMBER(ModeK, PolarizedSingleModeMagneticField, Vector3d, wavevector);
+CRPGPU_MEMBER(ModeBMax, PolarizedSingleModeMagneticField, double, B_max);
+CRPGPU_MEMBER(ModeSigma, PolarizedSingleModeMagneticField, double, sigma);
+CRPGPU_MEMBER(ModeR0, PolarizedSingleModeMagneticField, Vector3d, r_0);
 CRPGPU_MEMBER(TrackCenter, ObserverTracking, Vector3d, center);        // Observer.h:109
 CRPGPU_MEMBER(TrackRadius, ObserverTracking, double, radius);
 CRPGPU_MEMBER(TrackStep, ObserverTracking, double, stepSize);
@@ -326,6 +347,40 @@ struct Translation {
             d.z11_h = t->*member(PT11Z11H());
             d.z12_h = t->*member(PT11Z12H());
             text << "  field: PT11Field ass " << d.use_ass << " bss " << d.use_bss << " halo " << d.use_halo;
+        } else if (const TF17Field *t = dynamic_cast<const TF17Field *>(f)) {
+            if (typeid(*f) != typeid(TF17Field)) throw Unsupported(name_of(f) + " (a TF17Field subclass)");
+            crp_tf17_desc &d = c.tf17;
+            c.kind = CRP_FIELD_TF17;
+            d.disk_model = (int32_t)(t->*member(TF17Disk()));
+            d.halo_model = (int32_t)(t->*member(TF17Halo()));
+            d.use_disk = t->*member(TF17UseDisk()) ? 1 : 0;
+            d.use_halo = t->*member(TF17UseHalo()) ? 1 : 0;
+            // every parameter as the object holds it (the ones its models do not
+            // read may be uninitialised in the reference: the device does not read them either)
+            d.a_disk = t->*member(TF17ADisk()); d.z1_disk = t->*member(TF17Z1Disk());
+            d.r1_disk = t->*member(TF17R1Disk()); d.b1_disk = t->*member(TF17B1Disk());
+            d.l_disk = t->*member(TF17LDisk()); d.phi_star_disk = t->*member(TF17PhiDisk());
+            d.h_disk = t->*member(TF17HDisk()); d.a_halo = t->*member(TF17AHalo());
+            d.z1_halo = t->*member(TF17Z1Halo()); d.b1_halo = t->*member(TF17B1Halo());
+            d.l_halo = t->*member(TF17LHalo()); d.phi_star_halo = t->*member(TF17PhiHalo());
+            d.p0 = t->*member(TF17P0()); d.cot_p0 = t->*member(TF17CotP0());
+            d.h_p = t->*member(TF17Hp()); d.l_p = t->*member(TF17Lp());
+            d.epsilon = t->*member(TF17Eps());
+            text << "  field: TF17Field disk " << t->getDiskModel() << " halo " << t->getHaloModel()
+                 << " use disk " << d.use_disk << " halo " << d.use_halo;
+        } else if (const PolarizedSingleModeMagneticField *s =
+                       dynamic_cast<const PolarizedSingleModeMagneticField *>(f)) {
+            if (typeid(*f) != typeid(PolarizedSingleModeMagneticField))
+                throw Unsupported(name_of(f) + " (a PolarizedSingleModeMagneticField subclass)");
+            crp_single_mode_desc &d = c.single_mode;
+            c.kind = CRP_FIELD_SINGLE_MODE;
+            const Vector3d &u1 = s->*member(ModeU1()), &u2 = s->*member(ModeU2()), &k = s->*member(ModeK()),
+                           &r0 = s->*member(ModeR0());
+            const double v[4][3] = {{u1.x, u1.y, u1.z}, {u2.x, u2.y, u2.z}, {k.x, k.y, k.z}, {r0.x, r0.y, r0.z}};
+            for (int a = 0; a < 3; a++) { d.u1[a] = v[0][a]; d.u2[a] = v[1][a]; d.k[a] = v[2][a]; d.r0[a] = v[3][a]; }
+            d.b_max = s->*member(ModeBMax());
+            d.sigma = s->*member(ModeSigma());
+            text << "  field: PolarizedSingleModeMagneticField sigma " << d.sigma;
         } else if (const ArchimedeanSpiralField *a = dynamic_cast<const ArchimedeanSpiralField *>(f)) {
             if (typeid(*f) != typeid(ArchimedeanSpiralField))
                 throw Unsupported(name_of(f) + " (an ArchimedeanSpiralField subclass)");

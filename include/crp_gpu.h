@@ -5,7 +5,8 @@
  * a chain of one propagation module (PropagationCK, PropagationBP or
  * DiffusionSDE) over a magnetic field (MagneticFieldGrid over a Grid3f,
  * ModulatedMagneticFieldGrid, PeriodicMagneticField, PlaneWaveTurbulence,
- * UniformMagneticField, JF12Field, UF23Field, PT11Field, ArchimedeanSpiralField, a
+ * UniformMagneticField, JF12Field, UF23Field, PT11Field, ArchimedeanSpiralField, TF17Field,
+ * PolarizedSingleModeMagneticField, a
  * MagneticFieldList of those,
  * or a toroidal field), followed by MaximumTrajectoryLength, Observer and
  * boundary modules, run to completion over a set of candidates.  It replaces, for such chains,
@@ -34,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 7u
+#define CRP_ABI_VERSION 8u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -62,7 +63,10 @@ enum crp_field_kind {
     CRP_FIELD_JF12 = 6,           /* JF12Field / PlanckJF12bField (JF12Field.cpp:8-376) */
     CRP_FIELD_UF23 = 7,           /* UF23Field (UF23Field.cpp:59-558) */
     CRP_FIELD_PT11 = 8,           /* PT11Field (PT11Field.cpp:8-130) */
-    CRP_FIELD_ARCHIMEDEAN_SPIRAL = 9 /* ArchimedeanSpiralField (ArchimedeanSpiralField.cpp:5-49) */
+    CRP_FIELD_ARCHIMEDEAN_SPIRAL = 9, /* ArchimedeanSpiralField (ArchimedeanSpiralField.cpp:5-49) */
+    CRP_FIELD_TF17 = 10,          /* TF17Field (TF17Field.cpp:10-307) */
+    CRP_FIELD_SINGLE_MODE = 11    /* PolarizedSingleModeMagneticField
+                                     (PolarizedSingleModeMagneticField.cpp:5-64) */
 };
 
 /* UF23Field::ModelType (UF23Field.h), same order. */
@@ -171,6 +175,46 @@ typedef struct crp_archimedean_desc {
     double vw;    /* asymptotic wind speed [m/s] */
 } crp_archimedean_desc;
 
+/* TF17DiskModel and TF17HaloModel (TF17Field.h:20-21), same order. */
+enum crp_tf17_disk { CRP_TF17_AD1 = 0, CRP_TF17_BD1 = 1, CRP_TF17_DD1 = 2 };
+enum crp_tf17_halo { CRP_TF17_C0 = 0, CRP_TF17_C1 = 1 };
+
+/* State of a TF17Field (TF17Field.h:27-57), SI units: the disk and halo
+ * models and switches and the parameters TF17Field(disk, halo) sets
+ * (TF17Field.cpp:10-118), cot_p0 as set_p0 forms it (TF17Field.cpp:146).
+ * Parameters a model combination does not set are 0 here (the reference
+ * leaves them uninitialised; that model never reads them).
+ * crp_tf17_defaults() fills it. */
+typedef struct crp_tf17_desc {
+    int32_t disk_model, halo_model;                  /* crp_tf17_disk, crp_tf17_halo */
+    int32_t use_disk, use_halo;                      /* setUseDiskField, setUseHaloField */
+    double a_disk, z1_disk, r1_disk, b1_disk, l_disk, phi_star_disk, h_disk;
+    double a_halo, z1_halo, b1_halo, l_halo, phi_star_halo;
+    double p0, cot_p0, h_p, l_p;
+    double epsilon;                                  /* numeric_limits<double>::epsilon() */
+} crp_tf17_desc;
+
+/* PolarizedSingleModeMagneticField's derived state (PolarizedSingleModeMagneticField.h:34-38),
+ * SI units: B = b_max (u1 cos(k . (x - r0)) + u2 sigma sin(k . (x - r0))).
+ * crp_single_mode_field() forms it from the constructor's arguments. */
+typedef struct crp_single_mode_desc {
+    double b_max, sigma;
+    double r0[3];
+    double u1[3], u2[3]; /* unit vectors of e_1 and e_2 */
+    double k[3];         /* wave vector, along e_2 x e_1, |k| = 2 pi / wavelength */
+    /* the constructor's own arguments (the device reads the values above) */
+    double b0, wavelength;
+    double e1[3], e2[3];
+    int32_t amplitude_rms, polarization_helicity, mode, _pad;
+} crp_single_mode_desc;
+
+/* The constructor's string flags as numbers. */
+enum crp_single_mode_flag {
+    CRP_SINGLE_MODE_AMPLITUDE = 0, CRP_SINGLE_MODE_RMS = 1,             /* flagAmplitudeRms */
+    CRP_SINGLE_MODE_POLARIZATION = 0, CRP_SINGLE_MODE_HELICITY = 1,     /* flagPolarizationHelicity */
+    CRP_SINGLE_MODE_ELLIPTICAL = 0, CRP_SINGLE_MODE_CIRCULAR = 1, CRP_SINGLE_MODE_LINEAR = 2 /* flagMode */
+};
+
 /* crp_pt11_use() switches, PT11Field::setUseASS / setUseBSS / setUseHalo. */
 enum crp_pt11_switch { CRP_PT11_ASS = 0, CRP_PT11_BSS = 1, CRP_PT11_HALO = 2 };
 
@@ -196,6 +240,8 @@ typedef struct crp_field_component {
     crp_uf23_desc uf23;
     crp_pt11_desc pt11;
     crp_archimedean_desc archimedean;
+    crp_tf17_desc tf17;
+    crp_single_mode_desc single_mode;
 } crp_field_component;
 
 /* ------------------------------------------------------------------------
@@ -552,6 +598,18 @@ crp_status crp_pt11_defaults(crp_pt11_desc *out);
  * switching the ASS or BSS disk on switches the other off and sets its pitch
  * and southern halo strength; switching a disk off changes nothing else. */
 crp_status crp_pt11_use(crp_pt11_desc *io, int32_t which, int32_t use);
+
+/* The state TF17Field(disk, halo) constructs (TF17Field.cpp:10-118: disk
+ * and halo on). */
+crp_status crp_tf17_defaults(int32_t disk, int32_t halo, crp_tf17_desc *out);
+
+/* PolarizedSingleModeMagneticField(B_0, wavelength, sigma, r_0, e_1, e_2,
+ * flagAmplitudeRms, flagPolarizationHelicity, flagMode)
+ * (PolarizedSingleModeMagneticField.cpp:5-52): the constructor's checks
+ * (CRP_ERR_INVALID_ARGUMENT with its message) and derived values. */
+crp_status crp_single_mode_field(double b0, double wavelength, double sigma, const double r0[3],
+                                 const double e1[3], const double e2[3], int32_t amplitude_rms,
+                                 int32_t polarization_helicity, int32_t mode, crp_single_mode_desc *out);
 
 /* Turbulent Grid3f generation: GridTurbulence (GridTurbulence.cpp:29-123,
  * TurbulenceSpectrum), SimpleGridTurbulence (SimpleGridTurbulence.cpp:19-115,

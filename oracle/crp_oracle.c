@@ -808,6 +808,122 @@ static v3 archimedean_field(const crp_archimedean_desc *A, v3 pos) {
     return muls(B, A->b0);
 }
 
+/* ---------------------------------------------------------------- TF17Field
+ * TF17Field::getField and its helpers (TF17Field.cpp:197-307), SI units, the
+ * reference's operation order. */
+static double tf17_zscale(const crp_tf17_desc *T, double z) { return 1 + z * z / T->h_p / T->h_p; }
+
+static double tf17_winding(const crp_tf17_desc *T, double r, double z) {
+    return T->cot_p0 * log(1 - exp(-r / T->l_p) + T->epsilon) / tf17_zscale(T, z);
+}
+
+static double tf17_radial_scale(const crp_tf17_desc *T, double B1, double phi_star, double z1, double phi,
+                                double r, double z) {
+    double phi_prime = phi - tf17_winding(T, r, z) - phi_star;
+    return B1 * exp(-fabs(z1) / T->h_disk) * cos(phi_prime);
+}
+
+static double tf17_azimuthal(const crp_tf17_desc *T, double r, double z, double B_r, double B_z) {
+    double r_ = r / T->l_p;
+    double rscale = r > T->epsilon ? r_ * exp(-r_) / (1 - exp(-r_)) : 1 - r_ / 2. - r_ * r_ / 12.;
+    double B_phi = T->cot_p0 / tf17_zscale(T, z) * rscale * B_r;
+    B_phi = B_phi - 2 * z * r / (T->h_p * T->h_p) / tf17_zscale(T, z) * tf17_winding(T, r, z) * B_z;
+    return B_phi;
+}
+
+static v3 tf17_xyz(double B_r, double B_phi, double B_z, double sinPhi, double cosPhi) {
+    return mk(-(B_r * cosPhi - B_phi * sinPhi), B_r * sinPhi + B_phi * cosPhi, B_z);
+}
+
+static v3 tf17_disk(const crp_tf17_desc *T, double r, double z, double phi, double sinPhi, double cosPhi) {
+    double B_r = 0, B_phi = 0, B_z = 0;
+    if (T->disk_model == CRP_TF17_AD1) {
+        if (r > T->r1_disk) {
+            double z1_disk_z = (1. + T->a_disk * T->r1_disk * T->r1_disk) / (1. + T->a_disk * r * r);
+            double B_r0 = tf17_radial_scale(T, T->b1_disk, T->phi_star_disk, z1_disk_z * z, phi, r, z);
+            B_r = (T->r1_disk / r) * z1_disk_z * B_r0;
+            B_z = 2 * T->a_disk * T->r1_disk * z1_disk_z * z / (1 + T->a_disk * r * r) * B_r0;
+            B_phi = tf17_azimuthal(T, r, z, B_r, B_z);
+        } else {
+            double phi1_disk = tf17_winding(T, T->r1_disk, z) + T->phi_star_disk;
+            double B_amp = T->b1_disk * exp(-fabs(z) / T->h_disk);
+            B_r = cos(phi1_disk - phi) * B_amp;
+            B_phi = sin(phi1_disk - phi) * B_amp;
+        }
+    } else if (T->disk_model == CRP_TF17_BD1) {
+        if (r > T->epsilon) {
+            double r1_disk_r = T->r1_disk / r;
+            double z1_disk_z = 5. / (r1_disk_r * r1_disk_r + 4. / sqrt(r1_disk_r));
+            double B_r0 = tf17_radial_scale(T, T->b1_disk, T->phi_star_disk, z1_disk_z * z, phi, r, z);
+            B_r = r1_disk_r * z1_disk_z * B_r0;
+            B_z = -0.4 * r1_disk_r / r * z1_disk_z * z1_disk_z * z * (r1_disk_r * r1_disk_r - 1. / sqrt(r1_disk_r)) *
+                  B_r0;
+        } else {
+            double z1_disk_z = 5. * r * r / (T->r1_disk * T->r1_disk);
+            double B_r0 = tf17_radial_scale(T, T->b1_disk, T->phi_star_disk, z1_disk_z * z, phi, r, z);
+            B_r = 5. * r / T->r1_disk * B_r0;
+            B_z = -10. * z / T->r1_disk * B_r0;
+        }
+        B_phi = tf17_azimuthal(T, r, z, B_r, B_z);
+    } else { /* Dd1 */
+        double z_sign = z >= 0 ? 1. : -1.;
+        double z_abs = fabs(z);
+        if (z_abs > T->epsilon) {
+            double z1_disk_z = T->z1_disk / z_abs;
+            double r1_disk_r = 1.5 / (sqrt(z1_disk_z) + 0.5 / z1_disk_z);
+            double F_r = r1_disk_r * r <= T->l_disk ? 1. : exp(1. - r1_disk_r * r / T->l_disk);
+            double B_z0 = z_sign * T->b1_disk * F_r * cos(phi - tf17_winding(T, r, z) - T->phi_star_disk);
+            B_r = -0.5 / 1.5 * r1_disk_r * r1_disk_r * r1_disk_r * r / z_abs * (sqrt(z1_disk_z) - 1 / z1_disk_z) * B_z0;
+            B_z = z_sign * r1_disk_r * r1_disk_r * B_z0;
+        } else {
+            double z_z1_disk = z_abs / T->z1_disk;
+            double r1_disk_r = 1.5 * sqrt(z_abs / T->z1_disk);
+            double F_r = r1_disk_r * r <= T->l_disk ? 1. : exp(1. - r1_disk_r * r / T->l_disk);
+            double B_z0 = z_sign * T->b1_disk * F_r * cos(phi - tf17_winding(T, r, z) - T->phi_star_disk);
+            B_r = -1.125 * r / T->z1_disk * (1 - 2.5 * z_z1_disk * sqrt(z_z1_disk)) * B_z0;
+            B_z = z_sign * r1_disk_r * r1_disk_r * B_z0;
+        }
+        B_phi = tf17_azimuthal(T, r, z, B_r, B_z);
+    }
+    return tf17_xyz(B_r, B_phi, B_z, sinPhi, cosPhi);
+}
+
+static v3 tf17_halo(const crp_tf17_desc *T, double r, double z, double phi, double sinPhi, double cosPhi) {
+    double r1_halo_r = (1. + T->a_halo * T->z1_halo * T->z1_halo) / (1. + T->a_halo * z * z);
+    double B_z0;
+    if (T->halo_model == CRP_TF17_C0) {
+        B_z0 = T->b1_halo * exp(-r1_halo_r * r / T->l_halo);
+    } else {
+        double phi_prime = phi - tf17_winding(T, r, z) - T->phi_star_halo;
+        B_z0 = T->b1_halo * exp(-r1_halo_r * r / T->l_halo) * cos(phi_prime);
+    }
+    double B_r = 2 * T->a_halo * r1_halo_r * r1_halo_r * r * z / (1. + T->a_halo * z * z) * B_z0;
+    double B_z = r1_halo_r * r1_halo_r * B_z0;
+    double B_phi = tf17_azimuthal(T, r, z, B_r, B_z);
+    return tf17_xyz(B_r, B_phi, B_z, sinPhi, cosPhi);
+}
+
+static v3 tf17_field(const crp_tf17_desc *T, v3 pos) {
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+    /* pi - Vector3::getPhi (Vector3.h:136) */
+    double phi = M_PI - ((fabs(pos.x) < DBL_MIN && fabs(pos.y) < DBL_MIN) ? 0.0 : atan2(pos.y, pos.x));
+    double cosPhi = cos(phi), sinPhi = sin(phi);
+    v3 b = mk(0., 0., 0.);
+    if (T->use_disk) b = add(b, tf17_disk(T, r, pos.z, phi, sinPhi, cosPhi));
+    if (T->use_halo) b = add(b, tf17_halo(T, r, pos.z, phi, sinPhi, cosPhi));
+    return b;
+}
+
+/* PolarizedSingleModeMagneticField::getField (PolarizedSingleModeMagneticField.cpp:59) */
+static v3 single_mode_field(const crp_single_mode_desc *S, v3 pos) {
+    v3 d = mk(pos.x - S->r0[0], pos.y - S->r0[1], pos.z - S->r0[2]);
+    double ph = S->k[0] * d.x + S->k[1] * d.y + S->k[2] * d.z;
+    double c = cos(ph), s = sin(ph);
+    v3 a = mk(S->u1[0] * c, S->u1[1] * c, S->u1[2] * c);
+    v3 b = mk(S->u2[0] * S->sigma * s, S->u2[1] * S->sigma * s, S->u2[2] * S->sigma * s);
+    return muls(add(a, b), S->b_max);
+}
+
 static v3 component_field(const crp_field_component *f, v3 position) {
     v3 pos = position;
     if (f->periodic) { /* MagneticField.cpp:41 */
@@ -834,6 +950,8 @@ static v3 component_field(const crp_field_component *f, v3 position) {
     case CRP_FIELD_UF23: return uf23_field(&f->uf23, pos);
     case CRP_FIELD_PT11: return pt11_field(&f->pt11, pos);
     case CRP_FIELD_ARCHIMEDEAN_SPIRAL: return archimedean_field(&f->archimedean, pos);
+    case CRP_FIELD_TF17: return tf17_field(&f->tf17, pos);
+    case CRP_FIELD_SINGLE_MODE: return single_mode_field(&f->single_mode, pos);
     case CRP_FIELD_TOROIDAL: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f->toroidal_b0 / r);

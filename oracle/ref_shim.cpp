@@ -43,6 +43,8 @@
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/PT11Field.h"
+#include "crpropa/magneticField/TF17Field.h"
+#include "crpropa/magneticField/PolarizedSingleModeMagneticField.h"
 #include "crpropa/magneticField/ArchimedeanSpiralField.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/magneticField/turbulentField/TurbulentField.h"
@@ -196,6 +198,18 @@ static ref_ptr<MagneticField> build_component(const crp_field_component &f, Buil
         else if (!f.pt11.use_ass) t->setUseASS(false);
         if (!f.pt11.use_halo) t->setUseHalo(false);
         m = t;
+    } else if (f.kind == CRP_FIELD_TF17) {  // TF17Field(disk, halo) and its switches
+        TF17Field *t = new TF17Field((TF17DiskModel)f.tf17.disk_model, (TF17HaloModel)f.tf17.halo_model);
+        t->setUseDiskField(f.tf17.use_disk != 0);
+        t->setUseHaloField(f.tf17.use_halo != 0);
+        m = t;
+    } else if (f.kind == CRP_FIELD_SINGLE_MODE) {  // the constructor with the original arguments
+        const crp_single_mode_desc &s = f.single_mode;
+        static const char *ar[] = {"amplitude", "rms"}, *ph[] = {"polarization", "helicity"},
+                          *md[] = {"elliptical", "circular", "linear"};
+        m = new PolarizedSingleModeMagneticField(
+            s.b0, s.wavelength, s.sigma, Vector3d(s.r0[0], s.r0[1], s.r0[2]), Vector3d(s.e1[0], s.e1[1], s.e1[2]),
+            Vector3d(s.e2[0], s.e2[1], s.e2[2]), ar[s.amplitude_rms], ph[s.polarization_helicity], md[s.mode]);
     } else if (f.kind == CRP_FIELD_ARCHIMEDEAN_SPIRAL) {
         const crp_archimedean_desc &a = f.archimedean;
         m = new ArchimedeanSpiralField(a.b0, a.r0, a.omega, a.vw);
