@@ -425,7 +425,10 @@ def secondary_configs(dev, peaks):
     out.update(cfg_jf12_backtrack(dev, peaks))
     out.update(cfg_jf12_backtrack(dev, peaks, model="uf23"))
     out.update(cfg_jf12_backtrack(dev, peaks, model="pt11"))
+    for model in ("tf17", "kst24", "jf12_solenoidal"):
+        out.update(cfg_jf12_backtrack(dev, peaks, n=1 << 18, n_cpu=2000, model=model))
     out.update(cfg_turbulence(dev))
+    out.update(cfg_source_sampling(dev, peaks))
     return out
 
 
@@ -593,8 +596,12 @@ def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
     base model, or PT11Field), full runs, FP64 and mixed forms, beside the
     reference's own CPU run of a sample."""
     from crpropa3_b200 import _abi, engine, workloads as W
-    make = {"jf12": W.jf12_backtrack, "uf23": W.uf23_backtrack, "pt11": W.pt11_backtrack}[model]
-    field = {"jf12": "JF12Field (regular)", "uf23": "UF23Field (base)", "pt11": "PT11Field (ASS + halo)"}[model]
+    make = {"jf12": W.jf12_backtrack, "uf23": W.uf23_backtrack, "pt11": W.pt11_backtrack,
+            "tf17": W.tf17_backtrack, "kst24": W.kst24_backtrack,
+            "jf12_solenoidal": W.jf12_solenoidal_backtrack}[model]
+    field = {"jf12": "JF12Field (regular)", "uf23": "UF23Field (base)", "pt11": "PT11Field (ASS + halo)",
+             "tf17": "TF17Field (Ad1 + C1)", "kst24": "KST24Field",
+             "jf12_solenoidal": "JF12FieldSolenoidal (regular)"}[model]
     res = {"workload": f"{n} antiprotons 5-100 EeV from (-8.5 kpc, 0, 0), {field}, "
                        "PropagationCK 1e-4 0.1-100 pc, Observer sphere 20 kpc, full runs",
            "candidates": n, "max_steps_per_candidate": None}
@@ -612,6 +619,45 @@ def cfg_jf12_backtrack(dev, peaks, n=1 << 20, n_cpu=4000, model="jf12"):
         res["cpu_reference"] = {"particle_steps_per_s": cpu["value"], "cores": cpu_threads(),
                                 "sample": f"{n_cpu} candidates, full runs"}
     return {f"{model}_backtrack": res}
+
+
+def cfg_source_sampling(dev, peaks, n=1 << 25):
+    """Source sampling on the device (crp_source_sample_device): four
+    particle types by abundance, power-law spectrum, isotropic emission;
+    36 B written per candidate (id, energy, direction), timed with CUDA events
+    around the call after a warm-up call."""
+    import ctypes as C
+    import torch
+    from crpropa3_b200 import _abi
+    lib = _abi.load()
+    ids = np.array([1000010010, 1000020040, 1000070140, 1000260560], dtype=np.int32)
+    ab = np.array([0.5, 0.3, 0.15, 0.05])
+    d = _abi.SourceDesc()
+    d.n_types, d.spectrum, d.isotropic = 4, 1, 1
+    d.ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
+    d.abundances = ab.ctypes.data_as(C.POINTER(C.c_double))
+    d.emin, d.emax, d.index = 1e17 * 1.602176634e-19, 1e20 * 1.602176634e-19, -2.7
+    out_id = torch.empty(n, dtype=torch.int32, device=dev)
+    out_e = torch.empty(n, dtype=torch.float64, device=dev)
+    out_d = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    call = lambda seed: _abi.check(lib.crp_source_sample_device(C.byref(d), seed, 0, n, out_id.data_ptr(),
+                                                                out_e.data_ptr(), out_d.data_ptr(), stream))
+    call(1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for s in range(3):
+        call(2 + s)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / 3
+    gbs = 36.0 * n / (ms * 1e-3) / 1e9
+    peak, kind = measured_peaks()
+    return {"source_sampling": {"workload": f"{n} candidates: 4 types by abundance, power law -2.7 "
+                                            "0.1-100 EeV, isotropic",
+                                "candidates_per_s": n / (ms * 1e-3), "ms": ms, "write_gbs": gbs,
+                                "write_frac_of_hbm": gbs / peak, "hbm_peak": kind}}
 
 
 def cfg_turbulence(dev, sizes=(256, 512)):

@@ -34,7 +34,8 @@ STATUS_NAMES = {
 }
 
 FIELD_GRID, FIELD_PLANE_WAVE, FIELD_UNIFORM, FIELD_TOROIDAL, FIELD_MODULATED_GRID, FIELD_JF12, FIELD_UF23, \
-    FIELD_PT11, FIELD_ARCHIMEDEAN_SPIRAL, FIELD_TF17, FIELD_SINGLE_MODE = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+    FIELD_PT11, FIELD_ARCHIMEDEAN_SPIRAL, FIELD_TF17, FIELD_SINGLE_MODE, FIELD_KST24, FIELD_CMZ = \
+    1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13
 PT11_ASS, PT11_BSS, PT11_HALO = 0, 1, 2
 TF17_AD1, TF17_BD1, TF17_DD1 = 0, 1, 2
 TF17_C0, TF17_C1 = 0, 1
@@ -42,7 +43,7 @@ SINGLE_MODE_AMPLITUDE, SINGLE_MODE_RMS = 0, 1
 SINGLE_MODE_POLARIZATION, SINGLE_MODE_HELICITY = 0, 1
 SINGLE_MODE_ELLIPTICAL, SINGLE_MODE_CIRCULAR, SINGLE_MODE_LINEAR = 0, 1, 2
 UF23_BASE, UF23_NECL, UF23_EXPX, UF23_SPUR, UF23_CRE10, UF23_SYNCG, UF23_TWISTX, UF23_NEBCOR = range(8)
-JF12_VARIANT_JF12, JF12_VARIANT_PLANCK = 0, 1
+JF12_VARIANT_JF12, JF12_VARIANT_PLANCK, JF12_VARIANT_SOLENOIDAL = 0, 1, 2
 INTERPOLATION_TRILINEAR, INTERPOLATION_TRICUBIC, INTERPOLATION_NEAREST_NEIGHBOUR = 0, 1, 2
 MODULE_PROPAGATION, MODULE_MAX_TRAJECTORY_LENGTH, MODULE_OBSERVER, MODULE_BOUNDARY = 1, 2, 3, 4
 PROP_CK, PROP_BP, PROP_SDE = 1, 2, 3
@@ -90,7 +91,9 @@ class JF12Desc(C.Structure):
                 ("z0", _d), ("b_x", _d), ("sin_theta_x0", _d), ("cos_theta_x0", _d), ("tan_theta_x0", _d),
                 ("r_xc", _d), ("r_x", _d), ("sqrt_beta", _d), ("b_disk_turb", _d * 8),
                 ("b_disk_turb5", _d), ("z_disk_turb", _d), ("b_halo_turb", _d), ("r_halo_turb", _d),
-                ("z_halo_turb", _d)]
+                ("z_halo_turb", _d), ("cot_pitch", _d), ("cot_theta_x0", _d), ("z_s", _d), ("delta", _d),
+                ("r1", _d), ("r2", _d), ("r1s", _d), ("r2s", _d), ("phi0_arms", _d * 11), ("b_arms", _d * 11),
+                ("phi_coeff", _d * 10)]
 
 
 class UF23Desc(C.Structure):
@@ -128,13 +131,41 @@ class SingleModeDesc(C.Structure):
                 ("_pad", C.c_int32)]
 
 
+class KST24Arm(C.Structure):
+    _fields_ = [(n, _d) for n in ("b", "pitch_deg", "phi0_deg", "x_shift", "y_shift", "arc_radius1", "arc_radius2",
+                                  "arc_eps", "arc_div_deg", "rmin", "rmax", "zmin", "zmax")]
+
+
+class KST24Desc(C.Structure):
+    _fields_ = [(n, _d) for n in ("north_b", "north_zmin", "north_zmax", "north_rmin", "north_rmax",
+                                  "south_b", "south_zmin", "south_zmax", "south_rmin", "south_rmax",
+                                  "x_b", "x_rmin", "x_rmax", "x_theta_rad",
+                                  "lb_b", "lb_rmin", "lb_dr", "lb_x0", "lb_y0", "lb_z0")] + [
+        ("lb_dir", _d * 3), ("arms", KST24Arm * 5), ("kpc", _d), ("gauss", _d)]
+
+
+class CMZCloud(C.Structure):
+    _fields_ = [("mid", _d * 3), ("b1", _d), ("eta", _d), ("r", _d)]
+
+
+class CMZPoloidal(C.Structure):
+    _fields_ = [("mid", _d * 3), ("b", _d), ("a", _d), ("l", _d)]
+
+
+class CMZDesc(C.Structure):
+    _fields_ = [("use_mc", C.c_int32), ("use_ic", C.c_int32), ("use_ntf", C.c_int32), ("use_radio_arc", C.c_int32),
+                ("clouds", CMZCloud * 12), ("sgra_shift", _d * 3), ("sgra_r", _d), ("sgra_b1", _d),
+                ("ic", CMZPoloidal), ("ntf", CMZPoloidal * 7), ("radio_arc", CMZPoloidal), ("gauss", _d)]
+
+
 class FieldComponent(C.Structure):
     _fields_ = [("kind", C.c_int32), ("periodic", C.c_int32), ("periodic_reflective", C.c_int32),
                 ("_pad0", C.c_int32), ("periodic_origin", _d * 3), ("periodic_extends", _d * 3),
                 ("grid", GridDesc), ("plane_wave", PlaneWaveDesc), ("uniform", _d * 3),
                 ("toroidal_b0", _d), ("modulation", GridDesc), ("jf12", JF12Desc),
                 ("uf23", UF23Desc), ("pt11", PT11Desc),
-                ("archimedean", ArchimedeanDesc), ("tf17", TF17Desc), ("single_mode", SingleModeDesc)]
+                ("archimedean", ArchimedeanDesc), ("tf17", TF17Desc), ("single_mode", SingleModeDesc),
+                ("kst24", KST24Desc), ("cmz", CMZDesc)]
 
 
 class FeatureDesc(C.Structure):

@@ -35,10 +35,13 @@ SIGNATURES = {
                                        C.c_void_p, C.c_size_t, C.c_void_p]),
     "crp_random_draws": (_i32, [_u32, _i32, _u64, _d, _d, _d, _dp]),
     "crp_jf12_defaults": (_i32, [_i32, C.POINTER(_abi.JF12Desc)]),
+    "crp_jf12_solenoidal": (_i32, [_d, _d, C.POINTER(_abi.JF12Desc)]),
     "crp_uf23_defaults": (_i32, [_i32, C.POINTER(_abi.UF23Desc)]),
     "crp_pt11_defaults": (_i32, [C.POINTER(_abi.PT11Desc)]),
     "crp_pt11_use": (_i32, [C.POINTER(_abi.PT11Desc), _i32, _i32]),
     "crp_tf17_defaults": (_i32, [_i32, _i32, C.POINTER(_abi.TF17Desc)]),
+    "crp_kst24_defaults": (_i32, [C.POINTER(_abi.KST24Desc)]),
+    "crp_cmz_defaults": (_i32, [C.POINTER(_abi.CMZDesc)]),
     "crp_single_mode_field": (_i32, [_d, _d, _d, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), _i32, _i32, _i32,
                                      C.POINTER(_abi.SingleModeDesc)]),
     "crp_turbulence_draws": (_i32, [_u32, _i32, _u64, _dp]),
@@ -46,6 +49,8 @@ SIGNATURES = {
     "crp_turbulence_grid": (_i32, [C.POINTER(_abi.TurbulenceDesc), C.c_void_p, C.c_void_p]),
     "crp_plane_wave_modes": (_i32, [_d, _d, _d, _d, _d, _d, _i32, _i32, _dp, _dp, _dp, _dp, _dp]),
     "crp_source_sample": (_i32, [C.c_void_p, _u32, _u64, _i32p, _dp, _dp]),
+    "crp_source_sample_device": (_i32, [C.c_void_p, _u64, _u64, _u64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]),
     "crp_text_output_write": (_i32, [C.c_char_p, _i32, _i32, C.c_void_p, _u64, C.c_void_p]),
     "crp_run_device_noalloc": (_i32, [C.POINTER(_abi.NoAllocGridBpDesc), C.POINTER(_abi.Candidates),
                                       _u64, C.c_void_p, C.POINTER(_abi.RunStats)]),

@@ -34,6 +34,7 @@ SOURCES = {
     "adjoint.cu": [],
     "turbulence.cu": [],
     "crp_engine.cu": [],
+    "source.cu": [],
     "noalloc.cu": [],
     "host_tools.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }

@@ -307,6 +307,10 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
     } else if (f.kind == CRP_FIELD_JF12) {
         const crp_jf12_desc &J = f.jf12;
         if (!(J.kpc > 0)) return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: parameters not set (crp_jf12_defaults)");
+        if (J.variant < CRP_JF12_JF12 || J.variant > CRP_JF12_SOLENOIDAL)
+            return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: unknown variant");
+        if (J.variant == CRP_JF12_SOLENOIDAL && !(J.r1 > 0 && J.r2 > J.r1))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "JF12FieldSolenoidal: parameters not set (crp_jf12_solenoidal)");
         DevJF12 h;
         std::memset(&h, 0, sizeof(h));
         h.d = J;
@@ -377,6 +381,16 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         if (st) return st;
     } else if (f.kind == CRP_FIELD_SINGLE_MODE) {
         d.mode = f.single_mode;
+    } else if (f.kind == CRP_FIELD_KST24) {
+        if (!(f.kst24.kpc > 0) || !(f.kst24.gauss > 0))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "KST24Field: parameters not set (crp_kst24_defaults)");
+        crp_status st = upload(p, &f.kst24, 1, &d.kst);
+        if (st) return st;
+    } else if (f.kind == CRP_FIELD_CMZ) {
+        if (!(f.cmz.gauss > 0))
+            return fail(CRP_ERR_INVALID_ARGUMENT, "CMZField: parameters not set (crp_cmz_defaults)");
+        crp_status st = upload(p, &f.cmz, 1, &d.cmz);
+        if (st) return st;
     } else if (f.kind == CRP_FIELD_ARCHIMEDEAN_SPIRAL) {
         d.arch = f.archimedean;
     } else if (f.kind == CRP_FIELD_UNIFORM || f.kind == CRP_FIELD_TOROIDAL) {

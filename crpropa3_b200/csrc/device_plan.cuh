@@ -76,6 +76,8 @@ struct DevComponent {
     const crp_pt11_desc *pt;  // CRP_FIELD_PT11: device copy of the parameters
     const crp_tf17_desc *tf;  // CRP_FIELD_TF17: device copy of the parameters
     crp_single_mode_desc mode;  // CRP_FIELD_SINGLE_MODE
+    const crp_kst24_desc *kst;  // CRP_FIELD_KST24: device copy of the parameters
+    const crp_cmz_desc *cmz;    // CRP_FIELD_CMZ: device copy of the switches and objects
     crp_archimedean_desc arch;  // CRP_FIELD_ARCHIMEDEAN_SPIRAL
 };
 

@@ -193,7 +193,11 @@ crp_status crp_turbulence_draws(uint32_t seed, int32_t kind, uint64_t n_modes, d
 
 crp_status crp_jf12_defaults(int32_t variant, crp_jf12_desc *out) {
     if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
-    if (variant != 0 && variant != 1) return host_fail(CRP_ERR_INVALID_ARGUMENT, "JF12 variant must be 0 or 1");
+    if (variant == CRP_JF12_SOLENOIDAL) {  // the constructor's default arguments (JF12FieldSolenoidal.h:62)
+        const double parsec = 648000 / M_PI * 149597870700.0;
+        return crp_jf12_solenoidal(3 * (1e3 * parsec), 0.5 * (1e3 * parsec), out);
+    }
+    if (variant != 0 && variant != 1) return host_fail(CRP_ERR_INVALID_ARGUMENT, "JF12 variant must be 0, 1 or 2");
     // Units.h: tesla = 1, gauss = 1e-4 tesla, au = 149597870700 m, parsec = 648000 / pi au
     const double au = 149597870700.0, parsec = 648000 / M_PI * au, kpc = 1e3 * parsec;
     const double gauss = 1e-4, muG = 1e-6 * gauss;
@@ -245,6 +249,50 @@ crp_status crp_jf12_defaults(int32_t variant, crp_jf12_desc *out) {
         j.b_disk_turb5 = 3.90 * muG;
         j.b_halo_turb = 7.332 * muG;
     }
+    return CRP_OK;
+}
+
+crp_status crp_jf12_solenoidal(double delta, double zs, crp_jf12_desc *out) {
+    // JF12FieldSolenoidal::JF12FieldSolenoidal (JF12FieldSolenoidal.cpp:8-77) on JF12Field's state
+    crp_status st = crp_jf12_defaults(CRP_JF12_JF12, out);
+    if (st != CRP_OK) return st;
+    crp_jf12_desc &j = *out;
+    j.variant = CRP_JF12_SOLENOIDAL;
+    const double kpc = j.kpc, muG = 1e-6 * 1e-4;
+    // the constructor's tan and log run at run time; volatile operands keep them from folding
+    volatile double pitch_v = 11.5 * M_PI / 180;
+    const double pitch = pitch_v;
+    j.cot_pitch = 1. / std::tan(pitch);
+    j.cot_theta_x0 = 1. / j.tan_theta_x0;
+    j.z_s = zs;
+    j.delta = delta;
+    j.r1 = 5 * kpc;
+    j.r2 = 20 * kpc;
+    j.r1s = j.r1 + delta;
+    j.r2s = j.r2 - delta;
+    const double phi0 = 0.;
+    double *a = j.phi0_arms, *b = j.b_arms, *c = j.phi_coeff;
+    for (int i = 1; i < 9; i++) {
+        volatile double ratio = j.r_arms[i - 1] / j.r1;
+        a[i] = M_PI - j.cot_pitch * std::log((double)ratio);
+    }
+    a[0] = a[8] + 2 * M_PI;
+    a[9] = a[1] - 2 * M_PI;
+    a[10] = a[2] - 2 * M_PI;
+    int idx0 = 1;
+    while (idx0 < 10 && phi0 < a[idx0]) idx0 += 1;
+    const double arms[8] = {0, 0.1, 3.0, -0.9, -0.8, -2.0, -4.2, 0.0};
+    for (int i = 1; i < 8; i++) b[i] = arms[i] * muG;
+    double flux1to7 = 0.;  // the eighth arm closes the net flux through r1
+    for (int i = 1; i < 8; i++) flux1to7 += (a[i - 1] - a[i]) * b[i];
+    b[8] = -flux1to7 / (a[7] - a[8]);
+    b[0] = b[8];
+    b[9] = b[1];
+    b[10] = b[2];
+    c[0] = 0;
+    for (int i = 1; i < 10; i++) c[i] = c[i - 1] + (b[i - 1] - b[i]) * a[i - 1];
+    const double corr = c[idx0] + b[idx0] * phi0;  // H(phi0) = 0
+    for (int i = 1; i < 10; i++) c[i] = c[i] - corr;
     return CRP_OK;
 }
 
@@ -421,6 +469,91 @@ crp_status crp_tf17_defaults(int32_t disk, int32_t halo, crp_tf17_desc *out) {
 // PolarizedSingleModeMagneticField's constructor (PolarizedSingleModeMagneticField.cpp:5-52):
 // its checks in its order, with its messages, and its derived values with Vector3's arithmetic
 // (getR = sqrt(x*x + y*y + z*z), cross, componentwise scaling).
+crp_status crp_kst24_defaults(crp_kst24_desc *out) {
+    if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    // KST24Field::KST24Field (KST24Field.cpp:15-124): the model's published parameters
+    crp_kst24_desc &k = *out;
+    std::memset(&k, 0, sizeof(k));
+    k.north_b = -3.2e-6; k.north_zmin = 1.185; k.north_zmax = 2.1; k.north_rmin = 1.0; k.north_rmax = 9.1;
+    k.south_b = 3.2e-6; k.south_zmin = -2.5; k.south_zmax = -1.22; k.south_rmin = 1.0; k.south_rmax = 14.0;
+    k.x_b = 1.8e-6; k.x_rmin = 1.0; k.x_rmax = 6.2;
+    k.x_theta_rad = 28.0 * M_PI / 180.;
+    k.lb_b = -3.5e-6; k.lb_rmin = 0.2; k.lb_dr = 0.03; k.lb_x0 = -8.2; k.lb_y0 = 0.095; k.lb_z0 = -0.05;
+    // the constructor's cos and sin run at run time; volatile angles keep them from folding
+    volatile double lB = 50.0, bB = 2.0;
+    const double l = lB * M_PI / 180, b = bB * M_PI / 180;
+    k.lb_dir[0] = std::cos(b) * std::cos(l);
+    k.lb_dir[1] = std::cos(b) * std::sin(l);
+    k.lb_dir[2] = std::sin(b);
+    // b, pitch, phi0, x_shift, y_shift, arc_radius1, arc_radius2, arc_eps, arc_div, rmin, rmax, zmin, zmax
+    static const crp_kst24_arm arms[5] = {
+        {4.9e-6, 20, -134.0, 1.0, 0.0, 0.8, 1.0, 2.0, 0.0, 3.0, 16.0, -1.0, 1.0},     // Scutum
+        {1.3e-6, 20, -80.0, 1.37, 0.0, 1.0, 0.79, 2.3, 3.0, 3.0, 15.0, -1.2, 1.2},    // Carina-Sagittarius
+        {-3.5e-6, 20, -2.2, -0.15, 0.0, 0.73, 1.0, 1.45, 0.0, 3.3, 14.0, -1.0, 1.0},  // Local
+        {-2.0e-6, 20, 46.0, -1.0, 0.0, 0.4, 1.1, 2.0, 0.0, 3.0, 17.0, -1.0, 1.0},     // Perseus 1
+        {-3.5e-6, 20, 46.0, -1.0, 0.0, 1.2, 1.1, 2.0, 0.0, 3.0, 17.0, -2.0, 2.0}};    // Perseus 2
+    for (int i = 0; i < 5; i++) k.arms[i] = arms[i];
+    // Units.h: kpc = 1e3 parsec, parsec = 648000 / pi au; gauss = 1e-4 tesla
+    k.kpc = 1e3 * (648000 / M_PI * 149597870700.0);
+    k.gauss = 1e-4;
+    return CRP_OK;
+}
+
+crp_status crp_cmz_defaults(crp_cmz_desc *out) {
+    if (!out) return host_fail(CRP_ERR_INVALID_ARGUMENT, "out is NULL");
+    crp_cmz_desc &c = *out;
+    std::memset(&c, 0, sizeof(c));
+    c.use_ic = 1;  // CMZField::CMZField (CMZField.cpp:6)
+    const double pc = 648000 / M_PI * 149597870700.0, gauss = 1e-4;
+    volatile double two_v = 2;
+    const double ln2 = std::log((double)two_v);
+    // getMCField (CMZField.cpp:116-200): centre (y, z) [pc], R [pc], B1, eta
+    const double N = 59;
+    struct Cloud { double y, z, r, b1, eta; };
+    const Cloud clouds[12] = {
+        {-81.59, -16.32, 1.7, 2.1e-3 / N, 0.01},  // Sgr C
+        {37.53, -2.37, 2.4, 2.5e-3 / N, 0.01},    // Dust Ridge A
+        {50.44, 8.16, 1.9, 0.9e-3 / N, 0.01},     // B
+        {56.37, 7.71, 1.9, 1.2e-3 / N, 0.01},     // C
+        {60.82, 7.42, 3.3, 1.7e-3 / N, 0.01},     // D
+        {70.91, 0.74, 3.5, 4.1e-3 / N, 0.01},     // E
+        {73.58, 2.97, 2.4, 3.9e-3 / N, 0.01},     // F
+        {166.14, -10.38, 1.8, 0.8e-3 / N, 0.01},  // Sgr D
+        {97.01, -5.93, 14, 1.0e-3 / N, 0.01},     // Sgr B2
+        {-8.3, -6.9, 5, 3.0e-3 / 0.91, 0.77},     // inner 5 pc
+        {-19.29, -11.87, 9.4, 2.7e-3 / N, 0.01},  // 20 km/s cloud
+        {-2.97, -10.38, 9.4, 3.7e-3 / N, 0.01}};  // 50 km/s cloud
+    for (int i = 0; i < 12; i++)
+        c.clouds[i] = {{0, clouds[i].y * pc, clouds[i].z * pc}, clouds[i].b1, clouds[i].eta, clouds[i].r * pc};
+    c.sgra_shift[0] = 0;
+    c.sgra_shift[1] = 8.3 * pc;
+    c.sgra_shift[2] = 6.9 * pc;
+    c.sgra_r = 1.2e12;
+    c.sgra_b1 = 65. / 3.07;
+    // getICField (CMZField.cpp:202)
+    const double icB1 = 1e-5 * gauss;
+    volatile double ic_len = 70 * pc;
+    c.ic = {{0., -8.3 * pc, -6.9 * pc}, icB1 / 0.85, 4 * ln2 / std::pow((double)ic_len, 2), 158 * pc / ln2};
+    // getNTFField (CMZField.cpp:214-271): centre (y, z) [pc], a1 [m], a2 [m], B1; getA and getL
+    struct Filament { double y, z, a1, a2, b1; };
+    const double eta = 0.48;
+    const Filament f[7] = {
+        {-81.59, -1.48, 27.44 * pc, 1.73 * pc, 1.e-4},         // Sgr C
+        {-126.1, -25.22, 12.86 * pc, 2.22 * pc, 88.e-6},       // the Snake
+        {-68.24, 25.22, 15.08 * pc, 2.72, 1.e-3},              // G359.54+0.18 (a2 as the reference gives it)
+        {-31.15, 23.74, 16.07 * pc, 3.46 * pc, 1.e-3},         // G359.79+0.17
+        {5.93, 16.32, 28.68 * pc, 1.73 * pc, 1.e-4},           // southern thread
+        {13.35, 25.22, 29.42 * pc, 2.23 * pc, 140.e-6},        // northern thread
+        {-22.25, 69.73, 11.37 * pc, 2.23 * pc, 70.e-6 / eta}}; // the Pelican
+    for (int i = 0; i < 7; i++)
+        c.ntf[i] = {{0, f[i].y * pc, f[i].z * pc}, f[i].b1 / eta, 4 * ln2 / f[i].a1 / f[i].a1, f[i].a2 / 2 * ln2};
+    // getRadioArcField (CMZField.cpp:273)
+    const double a1 = 70.47 * pc, a2 = 9.89 * pc;
+    c.radio_arc = {{0, 26.7 * pc, 10.38 * pc}, 1.e-3 / eta, 4 * ln2 / a1 / a1, a2 / 2 * ln2};
+    c.gauss = gauss;
+    return CRP_OK;
+}
+
 crp_status crp_single_mode_field(double b0, double wavelength, double sigma, const double r0[3],
                                  const double e1[3], const double e2[3], int32_t amplitude_rms,
                                  int32_t polarization_helicity, int32_t mode, crp_single_mode_desc *out) {

@@ -24,6 +24,8 @@
 #include "uf23.cuh"
 #include "pt11.cuh"
 #include "tf17.cuh"
+#include "jf12.cuh"
+#include "kst24_cmz.cuh"
 
 
 // Resident blocks of 128 threads per SM the register budget of the
@@ -415,7 +417,15 @@ __device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double 
         const float s = jf12_turbulent_strength_f(J, xs, ys, zs) * unit;
         b = f3mk(g.x * s, g.y * s, g.z * s);
     }
-    if (J.d.use_striated || J.d.use_regular) {
+    if ((J.d.use_striated || J.d.use_regular) && J.d.variant == CRP_JF12_SOLENOIDAL) {
+        // JF12FieldSolenoidal: FP64 evaluation, FP32 result
+        double m = 1.;
+        if (J.d.use_striated) m = 1. + J.d.sqrt_beta * (double)__ldg(f.mod.values + gi_nearest_cell(f.mod, x, y, z));
+        const u3 r = jf12_regular_fp64(J.d, x, y, z);
+        b.x += (float)(r.x * m);
+        b.y += (float)(r.y * m);
+        b.z += (float)(r.z * m);
+    } else if (J.d.use_striated || J.d.use_regular) {
         float m = unit;
         if (J.d.use_striated)
             m *= 1.f + J.sqrtbeta * __ldg(f.mod.values + gi_nearest_cell(f.mod, x, y, z));
@@ -476,6 +486,14 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     }
     case CRP_FIELD_SINGLE_MODE: {  // FP64 evaluation (the phase reaches many turns), FP32 result
         const u3 b = single_mode_field(f.mode, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
+    case CRP_FIELD_KST24: {  // FP64 evaluation, FP32 result
+        const u3 b = kst24_field(*f.kst, x, y, z);
+        return f3mk((float)b.x, (float)b.y, (float)b.z);
+    }
+    case CRP_FIELD_CMZ: {  // FP64 evaluation, FP32 result
+        const u3 b = cmz_field(*f.cmz, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
     }
     default: {

@@ -22,6 +22,8 @@
 #include "uf23.cuh"
 #include "pt11.cuh"
 #include "tf17.cuh"
+#include "jf12.cuh"
+#include "kst24_cmz.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -167,99 +169,12 @@ __device__ d3 plane_wave_field(const DevPlaneWave &w, d3 pos) {
 
 // ---------------------------------------------------------------- JF12Field
 // The reference's arithmetic operation for operation (JF12Field.cpp:195-346);
-// exp, sin, cos and atan2 are CUDA's (within an ulp or two of glibc's);
-// pow(v, 2) is v * v, its correctly rounded value.
+// the regular field (JF12Field, PlanckJF12bField and JF12FieldSolenoidal) is
+// in jf12.cuh.
 
-// JF12Field::logisticFunction (JF12Field.cpp:195)
-__device__ __forceinline__ double jf_logistic(double x, double x0, double w) {
-    return 1. / (1. + exp(-2. * (fabs(x) - x0) / w));
-}
-
-__device__ __forceinline__ double jf_sq(double v) { return v * v; }
-
-// Vector3::getPhi (Vector3.h:136)
-__device__ __forceinline__ double jf_phi(double x, double y) {
-    const double eps = 2.2250738585072014e-308;  // numeric_limits<double>::min()
-    if ((fabs(x) < eps) && (fabs(y) < eps)) return 0.0;
-    return atan2(y, x);
-}
-
-// Radius of the spiral arm through (r, phi) where it crosses the negative x
-// axis, the arm-region lookup of getDiskField / getTurbulentStrength
-// (JF12Field.cpp:228-233, :315-320).
-__device__ __forceinline__ double jf_r_negx(const crp_jf12_desc &J, double r, double phi) {
-    double r_negx = r * exp(-(phi - M_PI) / J.tan90_minus_pitch);
-    if (r_negx > J.r_arms[7]) r_negx = r * exp(-(phi + M_PI) / J.tan90_minus_pitch);
-    if (r_negx > J.r_arms[7]) r_negx = r * exp(-(phi + 3 * M_PI) / J.tan90_minus_pitch);
-    return r_negx;
-}
-
-// JF12Field::getRegularField (JF12Field.cpp:199) with getDiskField (:216),
-// getToroidalHaloField (:248) and getXField (:267).
-__device__ d3 jf12_regular(const crp_jf12_desc &J, d3 pos) {
-    d3 b = mk(0., 0., 0.);
-    const double kpc = J.kpc;
-    const double d = sqrt(pos.x * pos.x + pos.y * pos.y + pos.z * pos.z);
-    if (!(d < 20 * kpc)) return b;
-    const double r = sqrt(pos.x * pos.x + pos.y * pos.y), z = pos.z;
-    const double phi = jf_phi(pos.x, pos.y);
-    const double sinPhi = sin(phi), cosPhi = cos(phi);
-    d3 bd = mk(0., 0., 0.);
-    if (J.use_disk) {
-        const double lfDisk = jf_logistic(z, J.h_disk, J.w_disk);
-        if (r > 3 * kpc) {
-            if (r < 5 * kpc) {  // molecular ring
-                const double bMag = J.b_ring * (5 * kpc / r) * (1 - lfDisk);
-                bd.x += -bMag * sinPhi;
-                bd.y += bMag * cosPhi;
-            } else {            // spiral region
-                const double r_negx = jf_r_negx(J, r, phi);
-                double bMag = 0;
-                for (int i = 7; i >= 0; i--)
-                    if (r_negx < J.r_arms[i]) bMag = J.b_disk[i];
-                bMag *= (5 * kpc / r) * (1 - lfDisk);
-                bd.x += bMag * (J.sin_pitch * cosPhi - J.cos_pitch * sinPhi);
-                bd.y += bMag * (J.sin_pitch * sinPhi + J.cos_pitch * cosPhi);
-            }
-        }
-    }
-    b = add(b, bd);
-    const bool outside1 = r * r + z * z > 1 * kpc * kpc;
-    d3 bh = mk(0., 0., 0.);
-    if (J.use_toroidal_halo && outside1) {
-        const double lfDisk = jf_logistic(z, J.h_disk, J.w_disk);
-        double bMagH = exp(-fabs(z) / J.z0) * lfDisk;
-        if (z >= 0)
-            bMagH *= J.b_north * (1 - jf_logistic(r, J.r_north, J.w_halo));
-        else
-            bMagH *= J.b_south * (1 - jf_logistic(r, J.r_south, J.w_halo));
-        bh.x += -bMagH * sinPhi;
-        bh.y += bMagH * cosPhi;
-    }
-    b = add(b, bh);
-    d3 bx = mk(0., 0., 0.);
-    if (J.use_x && outside1) {
-        double bMagX, sinThetaX, cosThetaX, rp;
-        const double rc = J.r_xc + fabs(z) / J.tan_theta_x0;
-        if (r < rc) {  // varying elevation region
-            rp = r * J.r_xc / rc;
-            bMagX = J.b_x * exp(-1 * rp / J.r_x) * jf_sq(J.r_xc / rc);
-            double thetaX = atan2(fabs(z), (r - rp));
-            if (z == 0) thetaX = M_PI / 2.;
-            sinThetaX = sin(thetaX);
-            cosThetaX = cos(thetaX);
-        } else {       // constant elevation region
-            rp = r - fabs(z) / J.tan_theta_x0;
-            bMagX = J.b_x * exp(-rp / J.r_x) * (rp / r);
-            sinThetaX = J.sin_theta_x0;
-            cosThetaX = J.cos_theta_x0;
-        }
-        const double zsign = z < 0 ? -1 : 1;
-        bx.x += zsign * bMagX * cosThetaX * cosPhi;
-        bx.y += zsign * bMagX * cosThetaX * sinPhi;
-        bx.z += bMagX * sinThetaX;
-    }
-    return add(b, bx);
+__device__ __forceinline__ d3 jf12_regular(const crp_jf12_desc &J, d3 pos) {
+    const u3 b = jf12_regular_fp64(J, pos.x, pos.y, pos.z);
+    return mk(b.x, b.y, b.z);
 }
 
 // JF12Field::getTurbulentStrength (JF12Field.cpp:301)
@@ -344,6 +259,14 @@ __device__ d3 component_field(const DevComponent &f, d3 position) {
     }
     case CRP_FIELD_SINGLE_MODE: {
         const u3 b = single_mode_field(f.mode, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
+    case CRP_FIELD_KST24: {
+        const u3 b = kst24_field(*f.kst, pos.x, pos.y, pos.z);
+        return mk(b.x, b.y, b.z);
+    }
+    case CRP_FIELD_CMZ: {
+        const u3 b = cmz_field(*f.cmz, pos.x, pos.y, pos.z);
         return mk(b.x, b.y, b.z);
     }
     default: {

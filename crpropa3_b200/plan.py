@@ -58,12 +58,17 @@ class ModulatedGridField:
 
 @dataclass
 class JF12Field:
-    """JF12Field (variant JF12_VARIANT_JF12, JF12Field.cpp:8) or
-    PlanckJF12bField (JF12_VARIANT_PLANCK, :352): the regular disk, toroidal
-    halo and X fields, optionally striated (a Grid1f read by nearest value,
-    setStriatedGrid, :113) and turbulent (a Grid3f scaled by the modelled
-    strength, setTurbulentGrid, :118).  Giving a grid switches its part on, as
-    the setters do; use_striated / use_turbulent override that."""
+    """JF12Field (variant JF12_VARIANT_JF12, JF12Field.cpp:8),
+    PlanckJF12bField (JF12_VARIANT_PLANCK, :352) or JF12FieldSolenoidal
+    (JF12_VARIANT_SOLENOIDAL, JF12FieldSolenoidal.cpp:8): the regular disk,
+    toroidal halo and X fields, optionally striated (a Grid1f read by nearest
+    value, setStriatedGrid, :113) and turbulent (a Grid3f scaled by the
+    modelled strength, setTurbulentGrid, :118).  Giving a grid switches its
+    part on, as the setters do; use_striated / use_turbulent override that.
+    For JF12FieldSolenoidal, delta and zs are the constructor's arguments
+    (the disk's transition width and the X field's scale height, metres;
+    None: 3 kpc and 0.5 kpc) and outer_transition=False stands for
+    deactivateOuterTransition()."""
     variant: int = _abi.JF12_VARIANT_JF12
     use_regular: bool = True
     use_disk: bool = True
@@ -74,12 +79,30 @@ class JF12Field:
     use_striated: Optional[bool] = None
     use_turbulent: Optional[bool] = None
     periodic: Optional[tuple] = None
+    delta: Optional[float] = None
+    zs: Optional[float] = None
+    outer_transition: bool = True
 
     @staticmethod
     def defaults(variant=_abi.JF12_VARIANT_JF12) -> "_abi.JF12Desc":
         """The constructor's parameters (crp_jf12_defaults)."""
         d = _abi.JF12Desc()
         _abi.check(_abi.load().crp_jf12_defaults(int(variant), C.byref(d)))
+        return d
+
+    def parameters(self) -> "_abi.JF12Desc":
+        """The constructor's parameters with this object's solenoidal
+        arguments and setters applied (crp_jf12_solenoidal)."""
+        d = self.defaults(self.variant)
+        if self.variant == _abi.JF12_VARIANT_SOLENOIDAL:
+            if self.delta is not None or self.zs is not None:
+                delta = 3 * d.kpc if self.delta is None else float(self.delta)
+                zs = 0.5 * d.kpc if self.zs is None else float(self.zs)
+                _abi.check(_abi.load().crp_jf12_solenoidal(delta, zs, C.byref(d)))
+            if not self.outer_transition:
+                d.r2s = d.r2  # JF12FieldSolenoidal::deactivateOuterTransition (JF12FieldSolenoidal.cpp:89)
+        elif self.delta is not None or self.zs is not None or not self.outer_transition:
+            raise ValueError("JF12Field: delta, zs and outer_transition belong to JF12FieldSolenoidal")
         return d
 
 
@@ -173,6 +196,42 @@ class SingleModeField:
         v = [(C.c_double * 3)(*map(float, a)) for a in (self.r0, self.e1, self.e2)]
         _abi.check(_abi.load().crp_single_mode_field(float(self.b0), float(self.wavelength), float(self.sigma),
                                                      v[0], v[1], v[2], *flags, C.byref(d)))
+        return d
+
+
+@dataclass
+class KST24Field:
+    """KST24Field() (KST24Field.cpp:15): the galactic field of Korochkin,
+    Semikoz & Tinyakov 2024 -- toroidal halo, X field, Local Bubble shell and
+    five logarithmic spiral arms; no parameters."""
+    periodic: Optional[tuple] = None
+
+    @staticmethod
+    def desc() -> "_abi.KST24Desc":
+        """The constructor's parameters (crp_kst24_defaults)."""
+        d = _abi.KST24Desc()
+        _abi.check(_abi.load().crp_kst24_defaults(C.byref(d)))
+        return d
+
+
+@dataclass
+class CMZField:
+    """CMZField() (CMZField.cpp:6), the Galactic-centre field of Guenduez et
+    al., with its switches (setUseMCField, setUseICField, setUseNTFField,
+    setUseRadioArc): molecular clouds, the intercloud medium (on by default),
+    non-thermal filaments and the radio arc."""
+    use_mc: bool = False
+    use_ic: bool = True
+    use_ntf: bool = False
+    use_radio_arc: bool = False
+    periodic: Optional[tuple] = None
+
+    def desc(self) -> "_abi.CMZDesc":
+        """The objects of the four parts (crp_cmz_defaults) with these switches."""
+        d = _abi.CMZDesc()
+        _abi.check(_abi.load().crp_cmz_defaults(C.byref(d)))
+        d.use_mc, d.use_ic = int(bool(self.use_mc)), int(bool(self.use_ic))
+        d.use_ntf, d.use_radio_arc = int(bool(self.use_ntf)), int(bool(self.use_radio_arc))
         return d
 
 
@@ -344,7 +403,7 @@ class ChainSpec:
             self._fill_grid(c.modulation, f.modulation, 1)
         elif isinstance(f, JF12Field):
             c.kind = _abi.FIELD_JF12
-            c.jf12 = JF12Field.defaults(f.variant)
+            c.jf12 = f.parameters()
             j = c.jf12
             j.use_regular, j.use_disk = int(bool(f.use_regular)), int(bool(f.use_disk))
             j.use_toroidal_halo, j.use_x = int(bool(f.use_toroidal_halo)), int(bool(f.use_x))
@@ -366,6 +425,12 @@ class ChainSpec:
         elif isinstance(f, SingleModeField):
             c.kind = _abi.FIELD_SINGLE_MODE
             c.single_mode = f.desc()
+        elif isinstance(f, KST24Field):
+            c.kind = _abi.FIELD_KST24
+            c.kst24 = f.desc()
+        elif isinstance(f, CMZField):
+            c.kind = _abi.FIELD_CMZ
+            c.cmz = f.desc()
         elif isinstance(f, ArchimedeanSpiralField):
             c.kind = _abi.FIELD_ARCHIMEDEAN_SPIRAL
             c.archimedean.b0, c.archimedean.r0 = float(f.b0), float(f.r0)

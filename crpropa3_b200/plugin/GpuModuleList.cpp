@@ -8,12 +8,15 @@
 #include "crpropa/Grid.h"
 #include "crpropa/Units.h"
 #include "crpropa/magneticField/JF12Field.h"
+#include "crpropa/magneticField/JF12FieldSolenoidal.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/PT11Field.h"
 #include "crpropa/magneticField/ArchimedeanSpiralField.h"
 #include "crpropa/magneticField/TF17Field.h"
 #include "crpropa/magneticField/PolarizedSingleModeMagneticField.h"
+#include "crpropa/magneticField/KST24Field.h"
+#include "crpropa/magneticField/CMZField.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
@@ -107,6 +110,18 @@ CRPGPU_PT11(PT11Rc, R_c); CRPGPU_PT11(PT11Z0D, z0_D); CRPGPU_PT11(PT11B0D, B0_D)
 CRPGPU_PT11(PT11R0H, R0_H); CRPGPU_PT11(PT11B0Hn, B0_Hn); CRPGPU_PT11(PT11B0Hs, B0_Hs);
 CRPGPU_PT11(PT11Z11H, z11_H); CRPGPU_PT11(PT11Z12H, z12_H);
 #undef CRPGPU_PT11
+typedef double JF12Arms[11];
+typedef double JF12Coeff[10];
+CRPGPU_MEMBER(JF12CotPitch, JF12Field, double, cotPitch);                 // JF12Field.h:47-61
+CRPGPU_MEMBER(JF12CotThetaX0, JF12Field, double, cotThetaX0);
+CRPGPU_MEMBER(JF12BDisk, JF12Field, JF12Arms, bDisk);
+CRPGPU_MEMBER(JF12SZs, JF12FieldSolenoidal, double, zS);                 // JF12FieldSolenoidal.h:35-55
+CRPGPU_MEMBER(JF12SPhi0Arms, JF12FieldSolenoidal, JF12Arms, phi0Arms);
+CRPGPU_MEMBER(JF12SPhiCoeff, JF12FieldSolenoidal, JF12Coeff, phiCoeff);
+CRPGPU_MEMBER(JF12SR1, JF12FieldSolenoidal, double, r1);
+CRPGPU_MEMBER(JF12SR2, JF12FieldSolenoidal, double, r2);
+CRPGPU_MEMBER(JF12SR1s, JF12FieldSolenoidal, double, r1s);
+CRPGPU_MEMBER(JF12SR2s, JF12FieldSolenoidal, double, r2s);
 CRPGPU_MEMBER(TF17Disk, TF17Field, TF17DiskModel, disk_model);           // TF17Field.h:27-57
 CRPGPU_MEMBER(TF17Halo, TF17Field, TF17HaloModel, halo_model);
 CRPGPU_MEMBER(TF17UseDisk, TF17Field, bool, useDiskField);
@@ -281,12 +296,30 @@ struct Translation {
             fillGrid(*grid, 3, c.grid);
             text << " modulation ";
             fillGrid(*mod, 1, c.modulation);
-        } else if (typeid(*f) == typeid(JF12Field) || typeid(*f) == typeid(PlanckJF12bField)) {
+        } else if (typeid(*f) == typeid(JF12Field) || typeid(*f) == typeid(PlanckJF12bField) ||
+                   typeid(*f) == typeid(JF12FieldSolenoidal)) {
             // exact types only: the parameters are the constructor's (JF12Field.cpp:8, :352),
             // which a subclass could change
             JF12Field *j = const_cast<JF12Field *>(static_cast<const JF12Field *>(f));
-            const int variant = typeid(*f) == typeid(PlanckJF12bField) ? 1 : 0;
+            const bool sol = typeid(*f) == typeid(JF12FieldSolenoidal);
+            const int variant = typeid(*f) == typeid(PlanckJF12bField) ? CRP_JF12_PLANCK : CRP_JF12_JF12;
             if (crp_jf12_defaults(variant, &c.jf12) != CRP_OK) throw Unsupported("JF12Field parameters");
+            if (sol) {  // JF12Field's constants and the solenoidal state as the object holds it
+                const JF12FieldSolenoidal *s = static_cast<const JF12FieldSolenoidal *>(f);
+                crp_jf12_desc &d = c.jf12;
+                d.variant = CRP_JF12_SOLENOIDAL;
+                d.cot_pitch = j->*member(JF12CotPitch());
+                d.cot_theta_x0 = j->*member(JF12CotThetaX0());
+                d.z_s = s->*member(JF12SZs());
+                d.r1 = s->*member(JF12SR1());
+                d.r2 = s->*member(JF12SR2());
+                d.r1s = s->*member(JF12SR1s());
+                d.r2s = s->*member(JF12SR2s());
+                d.delta = d.r1s - d.r1;
+                std::memcpy(d.phi0_arms, s->*member(JF12SPhi0Arms()), sizeof(d.phi0_arms));
+                std::memcpy(d.b_arms, j->*member(JF12BDisk()), sizeof(d.b_arms));
+                std::memcpy(d.phi_coeff, s->*member(JF12SPhiCoeff()), sizeof(d.phi_coeff));
+            }
             c.kind = CRP_FIELD_JF12;
             c.jf12.use_regular = j->isUsingRegularField();
             c.jf12.use_disk = j->isUsingDiskField();
@@ -294,7 +327,8 @@ struct Translation {
             c.jf12.use_x = j->isUsingXField();
             c.jf12.use_striated = j->isUsingStriatedField();
             c.jf12.use_turbulent = j->isUsingTurbulentField();
-            text << "  field: " << (variant ? "PlanckJF12bField" : "JF12Field") << " regular "
+            text << "  field: " << (sol ? "JF12FieldSolenoidal" : variant ? "PlanckJF12bField" : "JF12Field")
+                 << " regular "
                  << c.jf12.use_regular << " disk " << c.jf12.use_disk << " halo " << c.jf12.use_toroidal_halo
                  << " X " << c.jf12.use_x;
             if (c.jf12.use_striated) {
@@ -381,6 +415,22 @@ struct Translation {
             d.b_max = s->*member(ModeBMax());
             d.sigma = s->*member(ModeSigma());
             text << "  field: PolarizedSingleModeMagneticField sigma " << d.sigma;
+        } else if (typeid(*f) == typeid(KST24Field)) {
+            // exact type: no setters, every parameter is the constructor's (KST24Field.cpp:15-124)
+            if (crp_kst24_defaults(&c.kst24) != CRP_OK) throw Unsupported("KST24Field parameters");
+            c.kind = CRP_FIELD_KST24;
+            text << "  field: KST24Field";
+        } else if (typeid(*f) == typeid(CMZField)) {
+            // exact type: the objects are the methods' constants (CMZField.cpp:116-287), the switches the object's
+            const CMZField *z = static_cast<const CMZField *>(f);
+            if (crp_cmz_defaults(&c.cmz) != CRP_OK) throw Unsupported("CMZField parameters");
+            c.kind = CRP_FIELD_CMZ;
+            c.cmz.use_mc = z->getUseMCField();
+            c.cmz.use_ic = z->getUseICField();
+            c.cmz.use_ntf = z->getUseNTFField();
+            c.cmz.use_radio_arc = z->getUseRadioArc();
+            text << "  field: CMZField MC " << c.cmz.use_mc << " IC " << c.cmz.use_ic << " NTF " << c.cmz.use_ntf
+                 << " radio arc " << c.cmz.use_radio_arc;
         } else if (const ArchimedeanSpiralField *a = dynamic_cast<const ArchimedeanSpiralField *>(f)) {
             if (typeid(*f) != typeid(ArchimedeanSpiralField))
                 throw Unsupported(name_of(f) + " (an ArchimedeanSpiralField subclass)");

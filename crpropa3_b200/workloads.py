@@ -76,6 +76,43 @@ def source_candidates(n, ids, emin, emax, index, seed, position=(0.0, 0.0, 0.0),
     return c
 
 
+def source_candidates_device(n, ids, emin, emax, index, seed, position=(0.0, 0.0, 0.0),
+                             abundances=None, first=0, device="cuda") -> CandidateArrays:
+    """The candidates of source_candidates drawn on the device
+    (crp_source_sample_device): the same features and distributions from a
+    counter-based Philox stream, so candidate first + i is the same whichever
+    call or rank draws it.  Nothing crosses from the host but the source's
+    parameters."""
+    import torch
+    lib = _abi.load()
+    ids = np.asarray(ids, dtype=np.int32)
+    ab = np.ones(len(ids)) if abundances is None else np.asarray(abundances, dtype=np.float64)
+    d = _abi.SourceDesc()
+    d.n_types = len(ids)
+    d.spectrum = 1
+    d.ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
+    d.abundances = ab.ctypes.data_as(C.POINTER(C.c_double))
+    d.emin, d.emax, d.index = emin, emax, index
+    d.isotropic = 1
+    c = CandidateArrays(n, device=device)
+    if n == 0:
+        return c
+    dirs = torch.empty(3 * n, dtype=torch.float64, device=device)
+    stream = torch.cuda.current_stream(c.id.device).cuda_stream
+    _abi.check(lib.crp_source_sample_device(C.byref(d), int(seed), int(first), int(n), c.id.data_ptr(),
+                                            c.energy.data_ptr(), dirs.data_ptr(), stream))
+    c.dx.copy_(dirs[:n])
+    c.dy.copy_(dirs[n:2 * n])
+    c.dz.copy_(dirs[2 * n:])
+    for k, v in enumerate(np.asarray(position, dtype=np.float64)):
+        for name in (("x", "px"), ("y", "py"), ("z", "pz"))[k]:
+            getattr(c, name).fill_(float(v))
+    for p in np.unique(ids):
+        c.charge.masked_fill_(c.id == int(p), charge_of(int(p)))
+    c.active.fill_(1)
+    return c
+
+
 def _normalise(d):
     r = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
     return d / r[:, None]
@@ -227,3 +264,18 @@ def uf23_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7, model=_a
 def pt11_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7):
     """jf12_backtrack with PT11Field() (ASS disk and halo) instead of JF12."""
     return jf12_backtrack(n, precision, seed, field=P.PT11Field())
+
+
+def tf17_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7):
+    """jf12_backtrack with TF17Field() (disk Ad1, halo C1) instead of JF12."""
+    return jf12_backtrack(n, precision, seed, field=P.TF17Field())
+
+
+def kst24_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7):
+    """jf12_backtrack with KST24Field() instead of JF12."""
+    return jf12_backtrack(n, precision, seed, field=P.KST24Field())
+
+
+def jf12_solenoidal_backtrack(n=1_000_000, precision=_abi.PRECISION_MIXED, seed=7):
+    """jf12_backtrack with JF12FieldSolenoidal() (regular field) instead of JF12Field."""
+    return jf12_backtrack(n, precision, seed, variant=_abi.JF12_VARIANT_SOLENOIDAL)

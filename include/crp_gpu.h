@@ -65,8 +65,10 @@ enum crp_field_kind {
     CRP_FIELD_PT11 = 8,           /* PT11Field (PT11Field.cpp:8-130) */
     CRP_FIELD_ARCHIMEDEAN_SPIRAL = 9, /* ArchimedeanSpiralField (ArchimedeanSpiralField.cpp:5-49) */
     CRP_FIELD_TF17 = 10,          /* TF17Field (TF17Field.cpp:10-307) */
-    CRP_FIELD_SINGLE_MODE = 11    /* PolarizedSingleModeMagneticField
+    CRP_FIELD_SINGLE_MODE = 11,   /* PolarizedSingleModeMagneticField
                                      (PolarizedSingleModeMagneticField.cpp:5-64) */
+    CRP_FIELD_KST24 = 12,         /* KST24Field (KST24Field.cpp:15-374) */
+    CRP_FIELD_CMZ = 13            /* CMZField (CMZField.cpp:6-304) */
 };
 
 /* UF23Field::ModelType (UF23Field.h), same order. */
@@ -117,11 +119,19 @@ typedef struct crp_plane_wave_desc {
     double brms, lmin, lmax, lbendover, sindex, qindex;
 } crp_plane_wave_desc;
 
+/* Constructor a crp_jf12_desc's parameters come from. */
+enum crp_jf12_variant {
+    CRP_JF12_JF12 = 0,       /* JF12Field (JF12Field.cpp:8) */
+    CRP_JF12_PLANCK = 1,     /* PlanckJF12bField (JF12Field.cpp:352) */
+    CRP_JF12_SOLENOIDAL = 2  /* JF12FieldSolenoidal (JF12FieldSolenoidal.cpp:8) */
+};
+
 /* Parameters of the Jansson-Farrar 2012 galactic field as JF12Field holds
  * them (JF12Field.h, set by the constructors JF12Field.cpp:8 and :352), SI
- * units.  crp_jf12_defaults() fills them.  The striated grid (a Grid1f, one
- * float per cell, read by nearest value, JF12Field.cpp:296) is the
- * component's `modulation` grid and the turbulent grid (a Grid3f,
+ * units, and the state JF12FieldSolenoidal adds (JF12FieldSolenoidal.h:35-55).
+ * crp_jf12_defaults() and crp_jf12_solenoidal() fill them.  The striated grid
+ * (a Grid1f, one float per cell, read by nearest value, JF12Field.cpp:296) is
+ * the component's `modulation` grid and the turbulent grid (a Grid3f,
  * JF12Field.cpp:340) its `grid`. */
 typedef struct crp_jf12_desc {
     int32_t use_regular, use_disk, use_toroidal_halo, use_x, use_striated, use_turbulent;
@@ -138,6 +148,14 @@ typedef struct crp_jf12_desc {
     double sqrt_beta;                   /* striation */
     double b_disk_turb[8];
     double b_disk_turb5, z_disk_turb, b_halo_turb, r_halo_turb, z_halo_turb;
+    /* JF12FieldSolenoidal only (variant CRP_JF12_SOLENOIDAL): */
+    double cot_pitch, cot_theta_x0;     /* 1 / tan of the pitch and of thetaX0 */
+    double z_s;                         /* X field: parabolic field lines below |z| = z_s */
+    double delta;                       /* the transition width the constructor was given */
+    double r1, r2, r1s, r2s;            /* disk between r1 and r2, transitions [r1, r1s] and [r2s, r2] */
+    double phi0_arms[11];               /* azimuths where the arms cross r1, periodically closed */
+    double b_arms[11];                  /* arm strengths at r1, periodically closed (bDisk) */
+    double phi_coeff[10];               /* the azimuth integral H(phi) = phi_coeff[j] + b_arms[j] phi */
 } crp_jf12_desc;
 
 /* Parameters of a UF23Field model (UF23Field.h, UF23Field::EPar order; set by
@@ -215,6 +233,51 @@ enum crp_single_mode_flag {
     CRP_SINGLE_MODE_ELLIPTICAL = 0, CRP_SINGLE_MODE_CIRCULAR = 1, CRP_SINGLE_MODE_LINEAR = 2 /* flagMode */
 };
 
+/* One logarithmic spiral arm of KST24Field (KST24Field.h:53-120), the
+ * model's units: strength [gauss], pitch, phase and the cross-section's
+ * growth [degrees], centre shift, cross-section radii (height, plane) and the
+ * ranges in r and z [kpc], the cross-section's super-ellipse exponent. */
+typedef struct crp_kst24_arm {
+    double b, pitch_deg, phi0_deg, x_shift, y_shift, arc_radius1, arc_radius2, arc_eps, arc_div_deg;
+    double rmin, rmax, zmin, zmax;
+} crp_kst24_arm;
+
+/* KST24Field's parameters (KST24Field.h:22-120, set by the constructor,
+ * KST24Field.cpp:15-124) in the model's units (kpc, gauss).
+ * crp_kst24_defaults() fills them. */
+typedef struct crp_kst24_desc {
+    double north_b, north_zmin, north_zmax, north_rmin, north_rmax; /* toroidal halo, north */
+    double south_b, south_zmin, south_zmax, south_rmin, south_rmax; /* and south */
+    double x_b, x_rmin, x_rmax, x_theta_rad;                        /* X field */
+    double lb_b, lb_rmin, lb_dr, lb_x0, lb_y0, lb_z0;               /* Local Bubble shell */
+    double lb_dir[3];                                               /* its field direction */
+    crp_kst24_arm arms[5]; /* Scutum, Carina-Sagittarius, Local, Perseus 1, Perseus 2 */
+    double kpc, gauss;     /* the units [m], [T] */
+} crp_kst24_desc;
+
+/* A molecular cloud of CMZField's azimuthal model (CMZField::BAz,
+ * CMZField.cpp:36): centre [m], strength B1 [gauss], eta, radius R [m]. */
+typedef struct crp_cmz_cloud { double mid[3], b1, eta, r; } crp_cmz_cloud;
+
+/* An object of CMZField's poloidal model (CMZField::BPol, CMZField.cpp:18):
+ * centre [m], strength (B1 / eta) and the model parameters a [1/m^2] and L [m]. */
+typedef struct crp_cmz_poloidal { double mid[3], b, a, l; } crp_cmz_poloidal;
+
+/* CMZField (CMZField.h:21-79), the Galactic-centre field of Guenduez et al.:
+ * the switches (setUseMCField, setUseICField, setUseNTFField, setUseRadioArc)
+ * and the objects getMCField, getICField, getNTFField and getRadioArcField
+ * sum, in their order (CMZField.cpp:116-287).  crp_cmz_defaults() fills it. */
+typedef struct crp_cmz_desc {
+    int32_t use_mc, use_ic, use_ntf, use_radio_arc;
+    crp_cmz_cloud clouds[12];     /* molecular clouds */
+    double sgra_shift[3];         /* Sgr A*: added to the position */
+    double sgra_r, sgra_b1;       /* its radius [m] and strength */
+    crp_cmz_poloidal ic;          /* the intercloud medium [T] */
+    crp_cmz_poloidal ntf[7];      /* non-thermal filaments; the last (the Pelican) with y and z swapped */
+    crp_cmz_poloidal radio_arc;
+    double gauss;                 /* [T] */
+} crp_cmz_desc;
+
 /* crp_pt11_use() switches, PT11Field::setUseASS / setUseBSS / setUseHalo. */
 enum crp_pt11_switch { CRP_PT11_ASS = 0, CRP_PT11_BSS = 1, CRP_PT11_HALO = 2 };
 
@@ -242,6 +305,8 @@ typedef struct crp_field_component {
     crp_archimedean_desc archimedean;
     crp_tf17_desc tf17;
     crp_single_mode_desc single_mode;
+    crp_kst24_desc kst24;
+    crp_cmz_desc cmz;
 } crp_field_component;
 
 /* ------------------------------------------------------------------------
@@ -583,10 +648,19 @@ crp_status crp_particle_charge(int32_t id, double *charge);
 crp_status crp_random_draws(uint32_t seed, int32_t kind, uint64_t n, double a, double b,
                             double c, double *out);
 
-/* The parameters JF12Field's constructor sets (variant 0, JF12Field.cpp:8)
- * or PlanckJF12bField's (variant 1, JF12Field.cpp:352), with the regular
+/* The parameters JF12Field's constructor sets (variant 0, JF12Field.cpp:8),
+ * PlanckJF12bField's (variant 1, JF12Field.cpp:352) or JF12FieldSolenoidal's
+ * with its default arguments (variant 2), with the regular
  * field on and the striated and turbulent fields off, as constructed. */
 crp_status crp_jf12_defaults(int32_t variant, crp_jf12_desc *out);
+
+/* The parameters JF12FieldSolenoidal(delta, zs) sets (JF12FieldSolenoidal.cpp:8):
+ * JF12Field's, with the disk's transition width delta and the X field's
+ * scale height zs [m]; the arm crossings, the flux-closing eighth arm
+ * strength and the azimuth integral's coefficients derived as the
+ * constructor derives them.  Its setters change r1s / r2s (delta),
+ * z_s (zs) and r2s = r2 (deactivateOuterTransition). */
+crp_status crp_jf12_solenoidal(double delta, double zs, crp_jf12_desc *out);
 
 /* The parameters UF23Field(model) sets (UF23Field.cpp:59-266). */
 crp_status crp_uf23_defaults(int32_t model, crp_uf23_desc *out);
@@ -610,6 +684,14 @@ crp_status crp_tf17_defaults(int32_t disk, int32_t halo, crp_tf17_desc *out);
 crp_status crp_single_mode_field(double b0, double wavelength, double sigma, const double r0[3],
                                  const double e1[3], const double e2[3], int32_t amplitude_rms,
                                  int32_t polarization_helicity, int32_t mode, crp_single_mode_desc *out);
+
+/* The parameters KST24Field's constructor sets (KST24Field.cpp:15-124). */
+crp_status crp_kst24_defaults(crp_kst24_desc *out);
+
+/* CMZField() (CMZField.cpp:6, the intercloud field on, the others off) and the
+ * objects of its four parts with the derived a, L and strengths as its
+ * methods form them (CMZField.cpp:14-287). */
+crp_status crp_cmz_defaults(crp_cmz_desc *out);
 
 /* Turbulent Grid3f generation: GridTurbulence (GridTurbulence.cpp:29-123,
  * TurbulenceSpectrum), SimpleGridTurbulence (SimpleGridTurbulence.cpp:19-115,
@@ -678,6 +760,19 @@ typedef struct crp_source_desc {
 
 crp_status crp_source_sample(const crp_source_desc *src, uint32_t seed, uint64_t n, int32_t *id,
                              double *energy, double *dir_xyz /* planar x[n] y[n] z[n] */);
+
+/* The same source features drawn on the device, for throughput runs that
+ * should not copy candidates from the host (Source::getCandidate,
+ * Source.cpp:22, with the features above).  Candidate first + i takes its
+ * draws from a counter-based Philox4x32-10 stream keyed by seed, so a run
+ * split over calls or ranks (first = the index of its first candidate) draws
+ * the same candidates as one call; the distributions are the reference's,
+ * the sequence is not MT19937's (crp_source_sample reproduces that).  id,
+ * energy and dir_xyz (planar x[n] y[n] z[n]) are device arrays; stream is a
+ * cudaStream_t (NULL: the legacy default stream); the call returns after the
+ * launch.  1 to 256 particle types. */
+crp_status crp_source_sample_device(const crp_source_desc *src, uint64_t seed, uint64_t first, uint64_t n,
+                                    int32_t *id, double *energy, double *dir_xyz, void *stream);
 
 /* Output columns (Output.h:76 OutputColumn, bit = enum value). */
 enum crp_output_column {

@@ -211,6 +211,62 @@ void oracle_philox_block(const uint32_t *ctr, const uint32_t *key, uint32_t *out
     memcpy(out, o.v, sizeof(o.v));
 }
 
+/* The source features of oracle_sample_source (Source.cpp:74-150, :742, :808)
+ * drawn from the counter-based stream of the device sampler: candidate c's
+ * words are those of Philox({lo(c), hi(c), 0x536f7572 + block, 0}, seed),
+ * each uniform 53 bits of two words; Random::randBin, randPowerLaw and
+ * randVector map them as the reference maps its MT19937 draws. */
+static double philox_uniform53(uint32_t hi, uint32_t lo) {
+    return (double)(((uint64_t)hi << 21) | (uint64_t)(lo >> 11)) * 0x1.0p-53;
+}
+
+int oracle_sample_source_philox(uint64_t seed, uint64_t first, uint64_t n, int ntypes, const int32_t *ids,
+                                const double *abundances, int spectrum, double emin, double emax, double index,
+                                double energy, int isotropic, const double *direction, int32_t *id_out,
+                                double *e_out, double *dir_out) {
+    double cdf[256];
+    if (ntypes < 1 || ntypes > 256) return 1;
+    double acc = 0;
+    for (int i = 0; i < ntypes; i++) { acc = acc + (abundances ? abundances[i] : 1.0); cdf[i] = acc; }
+    int log_uniform = fabs(index + 1.0) < 2.220446049250313e-16;
+    double p1 = log_uniform ? log(emax) : pow(emax, index + 1), p2 = log_uniform ? log(emin) : pow(emin, index + 1);
+    double ex = 1 / (index + 1);
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t c = first + i;
+        u32x4 ca = {{(uint32_t)c, (uint32_t)(c >> 32), 0x536f7572u, 0u}};
+        u32x4 cb = {{(uint32_t)c, (uint32_t)(c >> 32), 0x536f7573u, 0u}};
+        u32x4 a = oracle_philox(ca, (uint32_t)seed, (uint32_t)(seed >> 32));
+        u32x4 b = oracle_philox(cb, (uint32_t)seed, (uint32_t)(seed >> 32));
+        int32_t pid = ids[0];
+        if (ntypes > 1) {
+            double u = philox_uniform53(a.v[0], a.v[1]) * cdf[ntypes - 1];
+            int k = 0;
+            while (k < ntypes - 1 && cdf[k] < u) k++;
+            pid = ids[k];
+        }
+        id_out[i] = pid;
+        double e = energy;
+        if (spectrum) {
+            double u = philox_uniform53(a.v[2], a.v[3]);
+            e = log_uniform ? exp((p1 - p2) * u + p2) : pow((p1 - p2) * u + p2, ex);
+        }
+        e_out[i] = e;
+        double x = direction[0], y = direction[1], z = direction[2];
+        if (isotropic) {
+            z = -1.0 + 2.0 * philox_uniform53(b.v[0], b.v[1]);
+            double t = -M_PI + (M_PI - -M_PI) * philox_uniform53(b.v[2], b.v[3]);
+            double r = sqrt(1 - z * z);
+            x = r * cos(t);
+            y = r * sin(t);
+        }
+        double nrm = sqrt(x * x + y * y + z * z);
+        dir_out[i] = x / nrm;
+        dir_out[n + i] = y / nrm;
+        dir_out[2 * n + i] = z / nrm;
+    }
+    return 0;
+}
+
 /* Per-step stream of a candidate: word w of step s of candidate i is word
  * (w % 4) of Philox(ctr = {lo(4s + w/4), hi(4s + w/4), lo(i), hi(i)},
  * key = {lo(seed), hi(seed)}). */
@@ -482,8 +538,10 @@ static v3 plane_wave_field(const crp_plane_wave_desc *p, v3 pos) {
 }
 
 /* ---------------------------------------------------------------- JF12Field
- * JF12Field::getField and its parts (JF12Field.cpp:195-346), same operation
- * order, glibc's exp, sin, cos, atan2 and pow as the reference calls them. */
+ * JF12Field::getField and its parts (JF12Field.cpp:195-346) and
+ * JF12FieldSolenoidal's disk and X fields (JF12FieldSolenoidal.cpp:115-302),
+ * same operation order, glibc's exp, log, sin, cos, atan, atan2 and pow as the
+ * reference calls them. */
 
 /* JF12Field::logisticFunction (JF12Field.cpp:195) */
 static double jf_logistic(double x, double x0, double w) { return 1. / (1. + exp(-2. * (fabs(x) - x0) / w)); }
@@ -502,6 +560,106 @@ static double jf_r_negx(const crp_jf12_desc *J, double r, double phi) {
     return r_negx;
 }
 
+/* JF12FieldSolenoidal: the spiral arm of (r, phi) at r1 along the logarithmic
+ * spiral (getHPhiIntegral :241, getSpiralFieldStrengthConstant :260) */
+static int jf12s_arm(const crp_jf12_desc *J, double r, double phi, double *phi1_out) {
+    double phi1 = phi - log(r / J->r1) * J->cot_pitch;
+    phi1 = atan2(sin(phi1), cos(phi1));
+    int idx = 1;
+    while (idx < 10 && phi1 < J->phi0_arms[idx]) idx += 1;
+    *phi1_out = phi1;
+    return idx;
+}
+
+/* getDiskTransitionPolynomial (:197) and its derivative (:219) */
+static void jf12s_transition(const crp_jf12_desc *J, double r, double *p, double *q) {
+    if ((r < J->r1) || (r > J->r2)) { *p = 0.; *q = 0.; return; }
+    if ((r > J->r1s) && (r < J->r2s)) { *p = J->r1 / r; *q = 0.; return; }
+    double r_a = J->r1, r_b = J->r1s;
+    if (r >= J->r2s) { r_a = J->r2; r_b = J->r2s; }
+    double fakt = (r_a / r_b - 2.) / ((r_a - r_b) * (r_a - r_b));
+    *p = (J->r1 / r_b) * (2. - r / r_b + fakt * (r - r_b) * (r - r_b));
+    *q = (J->r1 / r_b) * (2. - 2. * r / r_b + fakt * (3. * r * r - 4. * r * r_b + r_b * r_b));
+}
+
+/* JF12FieldSolenoidal::getDiskField (:115) */
+static v3 jf12s_disk(const crp_jf12_desc *J, double r, double z, double phi, double sinPhi, double cosPhi) {
+    v3 b = mk(0, 0, 0);
+    if (!J->use_disk) return b;
+    double lfDisk = jf_logistic(z, J->h_disk, J->w_disk);
+    if (!((J->r1 < r) && (r < J->r2))) return b;
+    double phi1;
+    int idx = jf12s_arm(J, r, phi, &phi1);
+    double hint = phi1 * J->b_arms[idx] + J->phi_coeff[idx];
+    double mag1 = J->b_arms[idx];
+    double pdelta, qdelta;
+    jf12s_transition(J, r, &pdelta, &qdelta);
+    double br = pdelta * mag1 * J->sin_pitch;
+    double bphi = pdelta * mag1 * J->cos_pitch - qdelta * hint * J->sin_pitch;
+    b.x += br * cosPhi - bphi * sinPhi;
+    b.y += br * sinPhi + bphi * cosPhi;
+    return muls(b, 1 - lfDisk);
+}
+
+/* JF12FieldSolenoidal::getXField (:131) */
+static v3 jf12s_x(const crp_jf12_desc *J, double r, double z, double sinPhi, double cosPhi) {
+    v3 b = mk(0, 0, 0);
+    if (!J->use_x) return b;
+    double zS = J->z_s, rXc = J->r_xc, rX = J->r_x, bX = J->b_x, tanT = J->tan_theta_x0;
+    double rc = rXc + fabs(z) / tanT;
+    double r0c = rXc + zS / tanT;
+    if (fabs(z) > zS) {
+        if (r == 0.) {
+            b.z = bX / ((1. + fabs(z) * J->cot_theta_x0 / rXc) * (1. + fabs(z) * J->cot_theta_x0 / rXc));
+            return b;
+        }
+        double bMagX, sinThetaX, cosThetaX, rp;
+        if (r < rc) {
+            rp = r * rXc / rc;
+            bMagX = bX * exp(-1 * rp / rX) * (rXc / rc) * (rXc / rc);
+            double thetaX = atan(fabs(z) / (r - rp));
+            if (z == 0) thetaX = M_PI / 2.;
+            sinThetaX = sin(thetaX);
+            cosThetaX = cos(thetaX);
+        } else {
+            rp = r - fabs(z) / tanT;
+            bMagX = bX * exp(-rp / rX) * (rp / r);
+            sinThetaX = J->sin_theta_x0;
+            cosThetaX = J->cos_theta_x0;
+        }
+        double zsign = z < 0 ? -1 : 1;
+        b.x += zsign * bMagX * cosThetaX * cosPhi;
+        b.y += zsign * bMagX * cosThetaX * sinPhi;
+        b.z += bMagX * sinThetaX;
+        return b;
+    }
+    double r0 = r * 1. / (1. - 1. / (2. * (zS + rXc * tanT)) * (zS - z * z / zS));
+    double f, br0, bz0;
+    if (r0 >= r0c) {
+        r0 = r + 1. / (2. * tanT) * (zS - z * z / zS);
+        f = 1. + 1 / (2 * r * tanT / zS) * (1. - (z / zS) * (z / zS));
+    } else {
+        double g = 1. - 1. / (2. + 2. * (rXc * tanT / zS)) * (1. - (z / zS) * (z / zS));
+        f = 1. / (g * g);
+    }
+    if (r0 < r0c) {
+        double rp = r0 * rXc / r0c;
+        double thetaX = atan(zS / (r0 - rp));
+        br0 = bX * exp(-rp / rX) * (rXc / r0c) * (rXc / r0c) * cos(thetaX);
+        bz0 = bX * exp(-rp / rX) * (rXc / r0c) * (rXc / r0c) * sin(thetaX);
+    } else {
+        double rp = r0 - zS / tanT;
+        br0 = bX * exp(-rp / rX) * (rp / r0) * J->cos_theta_x0;
+        bz0 = bX * exp(-rp / rX) * (rp / r0) * J->sin_theta_x0;
+    }
+    double br = z / zS * f * br0;
+    double bz = bz0 * f;
+    b.x += br * cosPhi;
+    b.y += br * sinPhi;
+    b.z += bz;
+    return b;
+}
+
 /* getRegularField (JF12Field.cpp:199): getDiskField (:216) + getToroidalHaloField
  * (:248) + getXField (:267) */
 static v3 jf12_regular(const crp_jf12_desc *J, v3 pos) {
@@ -512,8 +670,11 @@ static v3 jf12_regular(const crp_jf12_desc *J, v3 pos) {
     double r = sqrt(pos.x * pos.x + pos.y * pos.y), z = pos.z;
     double phi = jf_phi(pos.x, pos.y);
     double sinPhi = sin(phi), cosPhi = cos(phi);
+    int sol = J->variant == CRP_JF12_SOLENOIDAL;
     v3 bd = mk(0, 0, 0);
-    if (J->use_disk) {
+    if (sol) {
+        bd = jf12s_disk(J, r, z, phi, sinPhi, cosPhi);
+    } else if (J->use_disk) {
         double lfDisk = jf_logistic(z, J->h_disk, J->w_disk);
         if (r > 3 * kpc) {
             double bMag = 0;
@@ -546,7 +707,9 @@ static v3 jf12_regular(const crp_jf12_desc *J, v3 pos) {
     }
     b = add(b, bh);
     v3 bx = mk(0, 0, 0);
-    if (J->use_x && outside1) {
+    if (sol) {
+        bx = jf12s_x(J, r, z, sinPhi, cosPhi);
+    } else if (J->use_x && outside1) {
         double bMagX, sinThetaX, cosThetaX, rp;
         double rc = J->r_xc + fabs(z) / J->tan_theta_x0;
         if (r < rc) {
@@ -924,6 +1087,225 @@ static v3 single_mode_field(const crp_single_mode_desc *S, v3 pos) {
     return muls(add(a, b), S->b_max);
 }
 
+/* ---------------------------------------------------------------- KST24Field
+ * KST24Field::getField and its parts (KST24Field.cpp:128-374) in the model's
+ * units (kpc, gauss), same operation order, glibc's libm as the reference
+ * calls it (pow(x, 2) included). */
+
+/* get_toroidal (KST24Field.cpp:209) */
+static v3 kst24_toroidal(v3 p, double B, double zmin, double zmax, double rmin, double rmax) {
+    v3 v = mk(0, 0, 0);
+    if ((p.z <= zmin) || (zmax <= p.z)) return v;
+    double cR = sqrt(pow(p.x, 2) + pow(p.y, 2));
+    if ((rmin <= cR) && (cR <= rmax)) {
+        double theta = atan2(p.y, p.x);
+        v.x = B * sin(theta);
+        v.y = -B * cos(theta);
+        v.z = 0;
+    }
+    return v;
+}
+
+/* get_Xfield (KST24Field.cpp:228) */
+static v3 kst24_x(const crp_kst24_desc *K, v3 p) {
+    v3 v = mk(0, 0, 0);
+    int sign = 1;
+    if (p.z < 0) sign = -1;
+    if (fabs(p.z) > 10) return v;
+    double cR = sqrt(p.x * p.x + p.y * p.y);
+    double cR_0 = cR - p.z * sign * tan(K->x_theta_rad);
+    if ((cR_0 < K->x_rmin) || (K->x_rmax < cR_0)) return v;
+    double mgn_frc = cR_0 / cR;
+    double xy_theta = atan2(p.y, p.x);
+    v.x = K->x_b * mgn_frc * cos(xy_theta) * sign * sin(K->x_theta_rad);
+    v.y = K->x_b * mgn_frc * sin(xy_theta) * sign * sin(K->x_theta_rad);
+    v.z = K->x_b * mgn_frc * cos(K->x_theta_rad);
+    return v;
+}
+
+/* is_LB (KST24Field.cpp:194) */
+static int kst24_in_lb(const crp_kst24_desc *K, v3 p) {
+    double ex = p.x - K->lb_x0, ey = p.y - K->lb_y0, ez = p.z - K->lb_z0;
+    double cR = sqrt(ex * ex + ey * ey + ez * ez);
+    return cR < K->lb_rmin + K->lb_dr;
+}
+
+/* get_LB (KST24Field.cpp:252) */
+static v3 kst24_lb(const crp_kst24_desc *K, v3 p) {
+    v3 v = mk(0, 0, 0);
+    double ex = p.x - K->lb_x0, ey = p.y - K->lb_y0, ez = p.z - K->lb_z0;
+    double cR = sqrt(ex * ex + ey * ey + ez * ez);
+    if ((cR < K->lb_rmin) || (K->lb_rmin + K->lb_dr < cR)) return v;
+    ex /= cR;
+    ey /= cR;
+    ez /= cR;
+    double cosTheta = ex * K->lb_dir[0] + ey * K->lb_dir[1] + ez * K->lb_dir[2];
+    double fx = K->lb_dir[0] - ex * cosTheta, fy = K->lb_dir[1] - ey * cosTheta, fz = K->lb_dir[2] - ez * cosTheta;
+    double ampl = (1 + pow(K->lb_rmin, 2) / (2 * K->lb_rmin * K->lb_dr + K->lb_dr * K->lb_dr));
+    v.x = K->lb_b * ampl * fx;
+    v.y = K->lb_b * ampl * fy;
+    v.z = K->lb_b * ampl * fz;
+    return v;
+}
+
+/* get_logspiral (KST24Field.cpp:282) */
+static v3 kst24_arm(const crp_kst24_arm *A, v3 p) {
+    v3 v = mk(0, 0, 0);
+    if ((p.z < A->zmin) || (A->zmax < p.z)) return v;
+    double p0 = p.x + A->x_shift, p1 = p.y + A->y_shift, p2 = p.z;
+    double r = sqrt(p0 * p0 + p1 * p1);
+    if ((r < A->rmin) || (A->rmax < r)) return v;
+    double a_kpc = 3;
+    double k = tan(A->pitch_deg * M_PI / 180.);
+    double cos_pitch = cos(A->pitch_deg * M_PI / 180.);
+    double sin_pitch = sin(A->pitch_deg * M_PI / 180.);
+    double phi0 = A->phi0_deg * M_PI / 180.;
+    double arc_div_rad = A->arc_div_deg * M_PI / 180.;
+    double phi = atan2(p1, p0);
+    int nn = floor((log(r / a_kpc) - k * (phi + phi0)) / (2 * M_PI * k));
+    double r1 = a_kpc * exp(k * (phi + phi0 + 2 * M_PI * nn));
+    double r2 = r1 * exp(k * 2 * M_PI);
+    if (fabs(r - r1) > fabs(r - r2)) {
+        r1 = r2;
+        nn++;
+    }
+    double xi = r1 * cos(phi), yi = r1 * sin(phi);
+    double dir1 = k * xi - yi, dir2 = k * yi + xi;
+    double dirtmp = sqrt(dir1 * dir1 + dir2 * dir2);
+    dir1 /= dirtmp;
+    dir2 /= dirtmp;
+    double delta_phi = -((xi - p0) * dir1 + (yi - p1) * dir2) / (r1 / cos_pitch);
+    r1 = a_kpc * exp(k * (phi + phi0 + delta_phi + 2 * M_PI * nn));
+    xi = r1 * cos(phi + delta_phi);
+    yi = r1 * sin(phi + delta_phi);
+    dir1 = k * xi - yi;
+    dir2 = k * yi + xi;
+    dirtmp = sqrt(dir1 * dir1 + dir2 * dir2);
+    dir1 /= dirtmp;
+    dir2 /= dirtmp;
+    double d1 = sqrt(pow((xi - p0), 2) + pow((yi - p1), 2));
+    double L1 = r1 / sin_pitch;
+    double r_scale = 5;
+    double L1_at_r_scale = r_scale / sin_pitch;
+    double g_plane = A->arc_radius2 * (1 + (L1 - L1_at_r_scale) * arc_div_rad);
+    double g_z = A->arc_radius1 * (1 + (L1 - L1_at_r_scale) * arc_div_rad);
+    double arc_r_plane = (A->arc_radius2 < g_plane) ? g_plane : A->arc_radius2; /* std::max */
+    double arc_r_z = (A->arc_radius1 < g_z) ? g_z : A->arc_radius1;
+    if (arc_r_plane > 1.2) arc_r_plane = 1.2;
+    if (arc_r_z > 1.2) arc_r_z = 1.2;
+    double d_at_L1 = sqrt(pow(fabs(d1 / arc_r_plane), A->arc_eps) + pow(fabs(p2 / arc_r_z), A->arc_eps));
+    if ((d_at_L1 > 1) || (d_at_L1 < 0.)) return v;
+    double scaling_factor = (A->arc_radius1 * A->arc_radius2) / (arc_r_plane * arc_r_z);
+    v.x = A->b * dir1 * scaling_factor;
+    v.y = A->b * dir2 * scaling_factor;
+    v.z = 0;
+    return v;
+}
+
+/* getField (KST24Field.cpp:128) */
+static v3 kst24_field(const crp_kst24_desc *K, v3 pos) {
+    v3 vals = mk(0, 0, 0);
+    v3 p = divs(pos, K->kpc);
+    if (p.z > K->north_zmin) {
+        vals = add(vals, kst24_toroidal(p, K->north_b, K->north_zmin, K->north_zmax, K->north_rmin, K->north_rmax));
+        vals = add(vals, kst24_x(K, p));
+        return muls(vals, K->gauss);
+    }
+    if (p.z < K->south_zmax) {
+        vals = add(vals, kst24_toroidal(p, K->south_b, K->south_zmin, K->south_zmax, K->south_rmin, K->south_rmax));
+        vals = add(vals, kst24_x(K, p));
+        return muls(vals, K->gauss);
+    }
+    if (kst24_in_lb(K, p)) {
+        vals = add(vals, kst24_lb(K, p));
+        return muls(vals, K->gauss);
+    }
+    for (int i = 0; i < 5; i++) vals = add(vals, kst24_arm(&K->arms[i], p));
+    vals = add(vals, kst24_x(K, p));
+    return muls(vals, K->gauss);
+}
+
+/* ---------------------------------------------------------------- CMZField
+ * CMZField::getField and its parts (CMZField.cpp:14-304), SI units, same
+ * operation order, glibc's libm. */
+
+/* BPol (CMZField.cpp:18); pow_integer<3>(r1) is (r1 r1) r1 (Common.h:58) */
+static v3 cmz_bpol(const crp_cmz_poloidal *P, v3 position) {
+    v3 pos = sub(position, mk(P->mid[0], P->mid[1], P->mid[2]));
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+    double phi = atan2(pos.y, pos.x);
+    double r1 = 1 / (1 + P->a * pos.z * pos.z);
+    double Bs = P->b * exp(-r1 * r / P->l);
+    double Br = 2 * P->a * ((r1 * r1) * r1) * r * pos.z * Bs;
+    v3 b = mk(0, 0, 0);
+    b.z = r1 * r1 * Bs;
+    b.x = Br * cos(phi);
+    b.y = Br * sin(phi);
+    return b;
+}
+
+/* BAz (CMZField.cpp:36) */
+static v3 cmz_baz(const crp_cmz_cloud *C, v3 position) {
+    v3 pos = sub(position, mk(C->mid[0], C->mid[1], C->mid[2]));
+    double r = sqrt(pos.x * pos.x + pos.y * pos.y);
+    double phi = atan2(pos.y, pos.x);
+    double R = C->r, eta = C->eta, B1 = C->b1;
+    double Hc = R / sqrt(log(2));
+    double b = 1.;
+    double m = 1;
+    double r1 = R / 10;
+    double v = m / eta * log((r + b) / (R + b));
+    double cosV = cos(v + m * phi);
+    double Br = 0, Bphi = 0;
+    if (r > r1) {
+        double Pre = B1 * cosV * exp(-pos.z * pos.z / Hc / Hc);
+        Br = Pre * R / r;
+        Bphi = -Pre / eta * R / (r + b);
+    } else {
+        double Pre = B1 * exp(-pos.z * pos.z / Hc / Hc) * R / r1 * (3 * r / r1 - 2 * r * r / r1 / r1) * cosV;
+        Br = Pre;
+        Bphi = 1 + 6 * (r - r1) / (2 * r - 3 * r1) * (sin(v + m * phi) - sin(v)) / cosV;
+        Bphi *= -Pre * r / eta / (r + b);
+    }
+    return mk(Br * cos(phi) - Bphi * sin(phi), Br * sin(phi) + Bphi * cos(phi), 0);
+}
+
+/* getField (CMZField.cpp:289): getMCField (:116), getICField (:202),
+ * getNTFField (:214), getRadioArcField (:273) */
+static v3 cmz_field(const crp_cmz_desc *M, v3 pos) {
+    v3 out = mk(0, 0, 0);
+    if (M->use_mc) {
+        v3 b = mk(0, 0, 0);
+        for (int i = 0; i < 12; i++) b = add(b, cmz_baz(&M->clouds[i], pos));
+        double x = pos.x + M->sgra_shift[0], y = pos.y + M->sgra_shift[1], z = pos.z + M->sgra_shift[2];
+        double R = M->sgra_r, B1 = M->sgra_b1;
+        double Hc = R / sqrt(log(2));
+        double r = sqrt(x * x + y * y);
+        double r1 = R / 10;
+        double phi = atan2(y, x);
+        double Bphi;
+        if (r > r1)
+            Bphi = -B1 * exp(-z * z / Hc / Hc) * R / r;
+        else
+            Bphi = -B1 * exp(-z * z / Hc / Hc) * R / r1 * (3 * r / r1 - 2 * r * r / r1 * r1);
+        b.x -= Bphi * sin(phi);
+        b.y += Bphi * cos(phi);
+        out = add(out, muls(b, M->gauss));
+    }
+    if (M->use_ic) out = add(out, cmz_bpol(&M->ic, pos));
+    if (M->use_ntf) {
+        v3 b = mk(0, 0, 0);
+        for (int i = 0; i < 6; i++) b = add(b, cmz_bpol(&M->ntf[i], pos));
+        v3 pel = cmz_bpol(&M->ntf[6], pos);
+        b.x += pel.x;
+        b.y += pel.z;
+        b.z += pel.y;
+        out = add(out, muls(b, M->gauss));
+    }
+    if (M->use_radio_arc) out = add(out, muls(cmz_bpol(&M->radio_arc, pos), M->gauss));
+    return out;
+}
+
 static v3 component_field(const crp_field_component *f, v3 position) {
     v3 pos = position;
     if (f->periodic) { /* MagneticField.cpp:41 */
@@ -952,6 +1334,8 @@ static v3 component_field(const crp_field_component *f, v3 position) {
     case CRP_FIELD_ARCHIMEDEAN_SPIRAL: return archimedean_field(&f->archimedean, pos);
     case CRP_FIELD_TF17: return tf17_field(&f->tf17, pos);
     case CRP_FIELD_SINGLE_MODE: return single_mode_field(&f->single_mode, pos);
+    case CRP_FIELD_KST24: return kst24_field(&f->kst24, pos);
+    case CRP_FIELD_CMZ: return cmz_field(&f->cmz, pos);
     case CRP_FIELD_TOROIDAL: {
         double r = sqrt(pos.x * pos.x + pos.y * pos.y);
         return muls(mk(-pos.y, pos.x, 0.), f->toroidal_b0 / r);

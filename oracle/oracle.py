@@ -69,6 +69,10 @@ class Oracle:
                                              C.POINTER(C.c_int32), _dp, C.c_double, C.c_double,
                                              C.c_double, C.POINTER(C.c_int32), _dp, _dp]
         lib.oracle_philox_block.argtypes = [C.POINTER(C.c_uint32)] * 3
+        lib.oracle_sample_source_philox.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_int,
+                                                    C.POINTER(C.c_int32), _dp, C.c_int, C.c_double, C.c_double,
+                                                    C.c_double, C.c_double, C.c_int, _dp, C.POINTER(C.c_int32),
+                                                    _dp, _dp]
         adj = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_int,
                C.c_uint64, _dp, _dp, _dp, _dp, _dp]
         lib.oracle_bp_adjoint.argtypes = adj + [_dp, _dp, _dp, _dp]
@@ -125,6 +129,20 @@ class Oracle:
                                              out_id.ctypes.data_as(C.POINTER(C.c_int32)),
                                              _dptr(e), _dptr(d)) == 0
         return out_id, e, d.reshape(n, 3)
+
+    def sample_source_philox(self, seed, first, n, ids, abundances=None, spectrum=True, emin=1.0, emax=10.0,
+                             index=-1.0, energy=1.0, isotropic=True, direction=(1.0, 0.0, 0.0)):
+        """The counter-based source draws of crp_source_sample_device, restated:
+        (ids, energies, directions as an (n, 3) array)."""
+        ids = np.asarray(ids, dtype=np.int32)
+        ab = None if abundances is None else np.asarray(abundances, dtype=np.float64)
+        dirv = np.asarray(direction, dtype=np.float64)
+        out_id, e, d = np.zeros(n, np.int32), np.zeros(n), np.zeros(3 * n)
+        assert self.lib.oracle_sample_source_philox(
+            seed, first, n, len(ids), ids.ctypes.data_as(C.POINTER(C.c_int32)),
+            _dptr(ab) if ab is not None else None, int(spectrum), emin, emax, index, energy, int(isotropic),
+            _dptr(dirv), out_id.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(e), _dptr(d)) == 0
+        return out_id, e, d.reshape(3, n).T.copy()
 
     def _adj_args(self, grid, origin, spacing, step, n_steps, pos, u0, energy, charge, target):
         g = np.ascontiguousarray(grid, dtype=np.float32)

@@ -40,11 +40,14 @@
 #include "crpropa/Units.h"
 #include "crpropa/magneticField/MagneticField.h"
 #include "crpropa/magneticField/JF12Field.h"
+#include "crpropa/magneticField/JF12FieldSolenoidal.h"
 #include "crpropa/magneticField/MagneticFieldGrid.h"
 #include "crpropa/magneticField/UF23Field.h"
 #include "crpropa/magneticField/PT11Field.h"
 #include "crpropa/magneticField/TF17Field.h"
 #include "crpropa/magneticField/PolarizedSingleModeMagneticField.h"
+#include "crpropa/magneticField/KST24Field.h"
+#include "crpropa/magneticField/CMZField.h"
 #include "crpropa/magneticField/ArchimedeanSpiralField.h"
 #include "crpropa/magneticField/turbulentField/PlaneWaveTurbulence.h"
 #include "crpropa/magneticField/turbulentField/TurbulentField.h"
@@ -180,7 +183,16 @@ static ref_ptr<MagneticField> build_component(const crp_field_component &f, Buil
         // descriptor's flags and grids go through the public setters
         const crp_jf12_desc &j = f.jf12;
         if (j.kpc == 0) throw std::runtime_error("ref_shim: JF12 parameters not set");
-        ref_ptr<JF12Field> jf = j.variant == 1 ? new PlanckJF12bField() : new JF12Field();
+        ref_ptr<JF12Field> jf;
+        if (j.variant == CRP_JF12_SOLENOIDAL) {  // JF12FieldSolenoidal(delta, zs) and its setters
+            JF12FieldSolenoidal *s = new JF12FieldSolenoidal(j.delta, j.z_s);
+            if (j.r2s == j.r2) s->deactivateOuterTransition();
+            jf = s;
+        } else if (j.variant == CRP_JF12_PLANCK) {
+            jf = new PlanckJF12bField();
+        } else {
+            jf = new JF12Field();
+        }
         jf->setUseRegularField(j.use_regular != 0);
         jf->setUseDiskField(j.use_disk != 0);
         jf->setUseToroidalHaloField(j.use_toroidal_halo != 0);
@@ -210,6 +222,15 @@ static ref_ptr<MagneticField> build_component(const crp_field_component &f, Buil
         m = new PolarizedSingleModeMagneticField(
             s.b0, s.wavelength, s.sigma, Vector3d(s.r0[0], s.r0[1], s.r0[2]), Vector3d(s.e1[0], s.e1[1], s.e1[2]),
             Vector3d(s.e2[0], s.e2[1], s.e2[2]), ar[s.amplitude_rms], ph[s.polarization_helicity], md[s.mode]);
+    } else if (f.kind == CRP_FIELD_KST24) {  // no parameters
+        m = new KST24Field();
+    } else if (f.kind == CRP_FIELD_CMZ) {  // CMZField() and its four switches
+        CMZField *c = new CMZField();
+        c->setUseMCField(f.cmz.use_mc != 0);
+        c->setUseICField(f.cmz.use_ic != 0);
+        c->setUseNTFField(f.cmz.use_ntf != 0);
+        c->setUseRadioArc(f.cmz.use_radio_arc != 0);
+        m = c;
     } else if (f.kind == CRP_FIELD_ARCHIMEDEAN_SPIRAL) {
         const crp_archimedean_desc &a = f.archimedean;
         m = new ArchimedeanSpiralField(a.b0, a.r0, a.omega, a.vw);
