@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) source_kernel(const SourceParams P, int32
         // SourceMultipleParticleTypes: Random::randBin, the first bin whose cumulative weight reaches u
         int32_t pid = P.ids[0];
         if (P.n_types > 1) {
-            const double u = uniform53(a.x, a.y) * P.cdf[P.n_types - 1];
+            const double u = __dmul_rn(uniform53(a.x, a.y), P.cdf[P.n_types - 1]);
             int k = 0;
             while (k < P.n_types - 1 && P.cdf[k] < u) k++;
             pid = P.ids[k];
@@ -77,21 +77,21 @@ __global__ void __launch_bounds__(256) source_kernel(const SourceParams P, int32
         double e = P.energy;
         if (P.spectrum) {
             const double u = uniform53(a.z, a.w);
-            e = P.log_uniform ? exp((P.p1 - P.p2) * u + P.p2) : pow((P.p1 - P.p2) * u + P.p2, P.ex);
+            // products and sums rounded separately (no contraction), as the reference's host code
+            const double v = __dadd_rn(__dmul_rn(__dsub_rn(P.p1, P.p2), u), P.p2);
+            e = P.log_uniform ? exp(v) : pow(v, P.ex);
         }
         energy[i] = e;
         // SourceIsotropicEmission: Random::randVector; then ParticleState::setDirection's normalisation
         double x = P.dir[0], y = P.dir[1], z = P.dir[2];
         if (P.isotropic) {
-            z = -1.0 + 2.0 * uniform53(b.x, b.y);
-            const double t = -M_PI + (M_PI - -M_PI) * uniform53(b.z, b.w);
-            const double r = sqrt(1 - z * z);
-            double s, co;
-            sincos(t, &s, &co);
-            x = r * co;
-            y = r * s;
+            z = __dadd_rn(-1.0, __dmul_rn(2.0, uniform53(b.x, b.y)));
+            const double t = __dadd_rn(-M_PI, __dmul_rn(M_PI - -M_PI, uniform53(b.z, b.w)));
+            const double r = sqrt(__dsub_rn(1.0, __dmul_rn(z, z)));
+            x = __dmul_rn(r, cos(t));
+            y = __dmul_rn(r, sin(t));
         }
-        const double nrm = sqrt(x * x + y * y + z * z);
+        const double nrm = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
         dir[i] = x / nrm;
         dir[P.n + i] = y / nrm;
         dir[2 * P.n + i] = z / nrm;

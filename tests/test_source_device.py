@@ -10,8 +10,8 @@ reference's own Source sampler, in distribution (two-sample Kolmogorov-
 Smirnov on energies, direction cosines and azimuths; chi-square on the
 particle types), and split runs (first > 0) equal to one run.
 GPU: the device against that restatement draw for draw: ids exactly,
-energies within 4e-16 relative (CUDA's pow and exp against glibc's, within
-two ulp), direction components within 4e-16.
+energies within 5e-16 relative (CUDA's pow and exp against glibc's, within
+two ulp, on the same rounded argument), direction components within 5e-16.
 """
 import ctypes as C
 
@@ -125,8 +125,8 @@ def test_device_draws_follow_the_restatement(oracle, case):
     a = oracle.sample_source_philox(seed, first, n, ids, ab, spectrum, emin, emax, index, energy=5.0)
     d = _device(seed, first, n, ids, ab, spectrum, emin, emax, index, energy=5.0)
     np.testing.assert_array_equal(d[0], a[0])
-    np.testing.assert_allclose(d[1], a[1], rtol=4e-16, atol=0)
-    np.testing.assert_allclose(d[2], a[2], rtol=0, atol=4e-16)
+    np.testing.assert_allclose(d[1], a[1], rtol=5e-16, atol=0)
+    np.testing.assert_allclose(d[2], a[2], rtol=0, atol=5e-16)
 
 
 @pytest.mark.gpu
