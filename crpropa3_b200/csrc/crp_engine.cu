@@ -80,6 +80,10 @@ crp_status check_device_ptr(const void *ptr, const char *what) {
 
 constexpr double kInv2Pi = 0.15915494309189533577;  // 1 / (2 pi)
 constexpr double kTurnScale = 4294967296.0;          // 2^32: turns as 32-bit fixed point
+// crp_run() on host arrays: input chunks overlapped with the first launch,
+// for runs of at least kPipelineMinCandidates
+constexpr int kInputChunks = 8;
+constexpr uint64_t kPipelineMinCandidates = 1u << 18;
 
 struct crp_plan {
     int device = 0;
@@ -99,6 +103,17 @@ struct crp_plan {
     // device copies for crp_run() on host arrays
     uint64_t scratch_n = 0;
     void *scratch = nullptr;
+    // crp_run() on host arrays, chunked mode: the inputs are copied in
+    // kInputChunks chunks on copy_stream, and the first launch starts on each
+    // chunk (on its own stream, so that the chunks run side by side) as soon
+    // as the chunk has arrived; ident is the identity index list those
+    // first-launch parts read their candidates through
+    cudaStream_t copy_stream = nullptr;
+    cudaStream_t part_stream[kInputChunks] = {};
+    cudaEvent_t ev_chunk[kInputChunks] = {}, ev_part[kInputChunks] = {};
+    cudaEvent_t ev_ready = nullptr;
+    uint64_t ident_cap = 0;
+    uint32_t *ident = nullptr;
     uint64_t rec_cap = 0;
     void *rec_scratch = nullptr;
     // compaction lists of still-active candidate indices (ping-pong)
@@ -136,6 +151,14 @@ struct crp_plan {
         if (gstream) cudaStreamDestroy(gstream);
         if (ev_in) cudaEventDestroy(ev_in);
         if (ev_out) cudaEventDestroy(ev_out);
+        if (ident) cudaFree(ident);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (ev_ready) cudaEventDestroy(ev_ready);
+        for (int k = 0; k < kInputChunks; k++) {
+            if (part_stream[k]) cudaStreamDestroy(part_stream[k]);
+            if (ev_chunk[k]) cudaEventDestroy(ev_chunk[k]);
+            if (ev_part[k]) cudaEventDestroy(ev_part[k]);
+        }
     }
 };
 
@@ -610,9 +633,9 @@ static crp_status ensure_lists(crp_plan *p, uint64_t n) {
 // Cell ordering of grid runs.  Candidates that share grid cells share the
 // corner loads of the interpolation (L1 and L2 hits) and change cells at
 // similar steps (less divergence in the gather), so between launches the
-// still-active candidates are ordered by the cell they are in: blocks of 8^3
-// cells in x-major order, cells x-major inside a block (the key), sorted
-// with a radix sort.  The order is a scheduling choice only: every
+// still-active candidates are ordered by the cell they are in (the Morton
+// code of its indices, or blocks of 8^3 cells for grids above 1024 cells in
+// a dimension; cell_key_kernel), sorted with a radix sort.  The order is a scheduling choice only: every
 // candidate's trajectory is the same whatever order the threads take them in.
 constexpr int kSortedStepsPerLaunch = 512;
 constexpr uint64_t kSortMinCandidates = 1u << 16;
@@ -623,8 +646,12 @@ __device__ __forceinline__ int cell_of(double x, double go, double inv_s, int n)
     return (int)(i < 0 ? i + n : i);
 }
 
+// The sort key of a candidate's cell: with mb > 0 (every dimension at most
+// 2^mb <= 1024 cells) the Morton code of (ix, iy, iz), 3 mb bits, so that
+// cells close in all three directions get close keys; larger grids: blocks
+// of 8^3 cells in x-major order, cells x-major inside a block.
 __global__ void cell_key_kernel(DevGrid g, const double *x, const double *y, const double *z,
-                                const uint32_t *list, uint32_t n, int nby, int nbz, uint32_t *keys,
+                                const uint32_t *list, uint32_t n, int nby, int nbz, int mb, uint32_t *keys,
                                 uint32_t *vals) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -632,13 +659,32 @@ __global__ void cell_key_kernel(DevGrid g, const double *x, const double *y, con
     const int ix = cell_of(x[i], g.gox, g.inv_sx, g.nx);
     const int iy = cell_of(y[i], g.goy, g.inv_sy, g.ny);
     const int iz = cell_of(z[i], g.goz, g.inv_sz, g.nz);
-    const uint32_t block = ((uint32_t)(ix >> 3) * nby + (uint32_t)(iy >> 3)) * nbz + (uint32_t)(iz >> 3);
-    keys[t] = block * 512u + (uint32_t)(((ix & 7) * 8 + (iy & 7)) * 8 + (iz & 7));
+    if (mb > 0) {
+        uint32_t key = 0;
+        for (int b = mb - 1; b >= 0; b--)
+            key = (key << 3) | ((((uint32_t)ix >> b) & 1u) << 2) | ((((uint32_t)iy >> b) & 1u) << 1) |
+                  (((uint32_t)iz >> b) & 1u);
+        keys[t] = key;
+    } else {
+        const uint32_t block = ((uint32_t)(ix >> 3) * nby + (uint32_t)(iy >> 3)) * nbz + (uint32_t)(iz >> 3);
+        keys[t] = block * 512u + (uint32_t)(((ix & 7) * 8 + (iy & 7)) * 8 + (iz & 7));
+    }
     vals[t] = i;
+}
+
+// Bits per dimension of the Morton key (0: the grid is larger than 1024
+// cells in some dimension).
+static int cell_morton_bits(const DevGrid &g) {
+    const int m = std::max(g.nx, std::max(g.ny, g.nz));
+    if (m > 1024) return 0;
+    int b = 1;
+    while ((1 << b) < m) b++;
+    return b;
 }
 
 // Bits of the largest key, or 0 when the grid is too large for 32-bit keys.
 static int cell_key_bits(const DevGrid &g) {
+    if (const int mb = cell_morton_bits(g)) return 3 * mb;
     const uint64_t nb = (uint64_t)((g.nx + 7) / 8) * ((g.ny + 7) / 8) * ((g.nz + 7) / 8) * 512;
     if (nb > (1ull << 32)) return 0;
     int bits = 1;
@@ -669,7 +715,8 @@ static crp_status order_by_cell(crp_plan *p, const DevState &s, const uint32_t *
     uint32_t *keys_in = p->sort_buf, *keys_out = p->sort_buf + p->sort_cap;
     uint32_t *vals_in = p->sort_buf + 2 * p->sort_cap, *vals_out = p->sort_buf + 3 * p->sort_cap;
     cell_key_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, s.x, s.y, s.z, list, (uint32_t)n,
-                                                                (g.ny + 7) / 8, (g.nz + 7) / 8, keys_in, vals_in);
+                                                                (g.ny + 7) / 8, (g.nz + 7) / 8, cell_morton_bits(g),
+                                                                keys_in, vals_in);
     CUDA_TRY(cudaGetLastError());
     size_t bytes = p->sort_tmp_bytes;
     CUDA_TRY(cub::DeviceRadixSort::SortPairs(p->sort_tmp, bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
@@ -816,8 +863,48 @@ static crp_status run_persistent(crp_plan *p, const crp_candidates *c, uint64_t 
     return result;
 }
 
+// The first launch's input chunks of crp_run(): part k covers candidates
+// [bounds[k], bounds[k + 1]) and may start once p->ev_chunk[k] has completed.
+struct InputChunks {
+    uint64_t bounds[kInputChunks + 1];
+};
+
+__global__ void iota_kernel(uint32_t *out, uint64_t n) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = (uint32_t)t;
+}
+
+// Streams, events and the identity list of crp_run()'s input pipeline.
+static crp_status ensure_pipeline(crp_plan *p, uint64_t n, cudaStream_t st) {
+    if (!p->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_ready, cudaEventDisableTiming));
+        for (int k = 0; k < kInputChunks; k++) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&p->part_stream[k], cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&p->ev_chunk[k], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&p->ev_part[k], cudaEventDisableTiming));
+        }
+    }
+    if (p->ident_cap < n) {
+        if (p->ident) { cudaFree(p->ident); p->ident = nullptr; p->ident_cap = 0; }
+        CUDA_TRY(cudaMalloc(&p->ident, sizeof(uint32_t) * n));
+        iota_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p->ident, n);
+        CUDA_TRY(cudaGetLastError());
+        p->ident_cap = n;
+    }
+    return CRP_OK;
+}
+
+static crp_status run_device(crp_plan *p, const crp_candidates *c, uint64_t n, const crp_run_opts *opts,
+                             crp_run_stats *stats, const InputChunks *in);
+
 crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
                           const crp_run_opts *opts, crp_run_stats *stats) {
+    return run_device(p, c, n, opts, stats, nullptr);
+}
+
+static crp_status run_device(crp_plan *p, const crp_candidates *c, uint64_t n, const crp_run_opts *opts,
+                             crp_run_stats *stats, const InputChunks *in) {
     if (!p || !c) return fail(CRP_ERR_INVALID_ARGUMENT, "plan or candidates is NULL");
     crp_run_opts o{};
     if (opts) o = *opts;
@@ -870,9 +957,26 @@ crp_status crp_run_device(crp_plan *p, const crp_candidates *c, uint64_t n,
             if (ls) return ls;
             launches++;  // the key kernel (the radix sort is CUB's)
         }
-        cudaError_t e = (p->precision == CRP_PRECISION_FP64)
-            ? launch_fp64_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st)
-            : launch_mixed_chunk(p->dev, s, n_threads, spl, o.max_steps, p->d_cnt, rec, list_in, list_out, p->fs, block, st);
+        auto step = [&](uint64_t nt, const uint32_t *li, cudaStream_t ss) {
+            return (p->precision == CRP_PRECISION_FP64)
+                ? launch_fp64_chunk(p->dev, s, nt, spl, o.max_steps, p->d_cnt, rec, li, list_out, p->fs, block, ss)
+                : launch_mixed_chunk(p->dev, s, nt, spl, o.max_steps, p->d_cnt, rec, li, list_out, p->fs, block, ss);
+        };
+        cudaError_t e = cudaSuccess;
+        if (in && !list_in) {
+            // first launch of crp_run(): each input chunk on its own stream once it has arrived
+            for (int k = 0; k < kInputChunks && e == cudaSuccess; k++) {
+                const uint64_t a = in->bounds[k], b = in->bounds[k + 1];
+                cudaStream_t ps = p->part_stream[k];
+                CUDA_TRY(cudaStreamWaitEvent(ps, p->ev0, 0));
+                CUDA_TRY(cudaStreamWaitEvent(ps, p->ev_chunk[k], 0));
+                if (b > a) e = step(b - a, p->ident + a, ps);
+                if (e == cudaSuccess) e = cudaEventRecord(p->ev_part[k], ps);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(st, p->ev_part[k], 0);
+            }
+        } else {
+            e = step(n_threads, list_in, st);
+        }
         if (e != cudaSuccess) return cuda_fail(e, "stepping kernel launch");
         CUDA_TRY(cudaEventRecord(p->ev1, st));
         CUDA_TRY(cudaMemcpyAsync(p->h_cnt, p->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
@@ -933,14 +1037,7 @@ crp_status crp_run(crp_plan *p, const crp_candidates *h, uint64_t n, const crp_r
     d.id = (int32_t *)take(4 * n); d.flags = (uint32_t *)take(4 * n);
     d.active = (uint8_t *)take(n);
     if (off > per_cand * n + slack) return fail(CRP_ERR_CUDA, "scratch layout overflow");
-#define H2D(m, bytes) CUDA_TRY(cudaMemcpyAsync(d.m, h->m, (bytes), cudaMemcpyHostToDevice, st))
 #define D2H(m, bytes) CUDA_TRY(cudaMemcpyAsync(h->m, d.m, (bytes), cudaMemcpyDeviceToHost, st))
-    H2D(charge, 8 * n); H2D(energy, 8 * n); H2D(x, 8 * n); H2D(y, 8 * n); H2D(z, 8 * n);
-    H2D(dx, 8 * n); H2D(dy, 8 * n); H2D(dz, 8 * n); H2D(px, 8 * n); H2D(py, 8 * n); H2D(pz, 8 * n);
-    H2D(trajectory_length, 8 * n); H2D(time, 8 * n); H2D(current_step, 8 * n); H2D(next_step, 8 * n);
-    if (per) H2D(max_length, 8 * n);
-    if (steps) H2D(step_count, 8 * n);
-    H2D(id, 4 * n); H2D(flags, 4 * n); H2D(active, n);
     // records: device buffer of the same capacity, copied back afterwards
     crp_records drec{};
     crp_records *hrec = o.records;
@@ -966,7 +1063,38 @@ crp_status crp_run(crp_plan *p, const crp_candidates *h, uint64_t n, const crp_r
         CUDA_TRY(cudaMemcpyAsync(drec.count, hrec->count, 8, cudaMemcpyHostToDevice, st));
         o.records = &drec;
     }
-    crp_status rs = crp_run_device(p, &d, n, &o, stats);
+    // inputs: one chunk (the whole range on st) or kInputChunks chunks on the copy stream, the
+    // first launch starting on each as it arrives (chunked mode, large runs)
+    const int mode = o.mode == CRP_MODE_AUTO ? (p->tuned_mode ? p->tuned_mode : CRP_MODE_CHUNKED) : o.mode;
+    const bool pipe = mode == CRP_MODE_CHUNKED && n >= kPipelineMinCandidates;
+    InputChunks chunks{};
+    cudaStream_t cs = st;
+    if (pipe) {
+        crp_status ps = ensure_pipeline(p, n, st);
+        if (ps) return ps;
+        // the copies overwrite the scratch: after everything st has queued on it
+        CUDA_TRY(cudaEventRecord(p->ev_ready, st));
+        CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->ev_ready, 0));
+        cs = p->copy_stream;
+    }
+    const int nchunks = pipe ? kInputChunks : 1;
+    for (int k = 0; k < nchunks; k++) {
+        const uint64_t a = n * k / nchunks, b = n * (k + 1) / nchunks, m = b - a;
+        chunks.bounds[k] = a;
+        chunks.bounds[k + 1] = b;
+#define H2D(f, sz) CUDA_TRY(cudaMemcpyAsync(d.f + a, h->f + a, (sz) * m, cudaMemcpyHostToDevice, cs))
+        H2D(charge, 8); H2D(energy, 8); H2D(x, 8); H2D(y, 8); H2D(z, 8);
+        H2D(dx, 8); H2D(dy, 8); H2D(dz, 8); H2D(px, 8); H2D(py, 8); H2D(pz, 8);
+        H2D(trajectory_length, 8); H2D(time, 8); H2D(current_step, 8); H2D(next_step, 8);
+        if (per) H2D(max_length, 8);
+        if (steps) H2D(step_count, 8);
+        H2D(id, 4); H2D(flags, 4); H2D(active, 1);
+#undef H2D
+        if (pipe) CUDA_TRY(cudaEventRecord(p->ev_chunk[k], cs));
+    }
+    crp_status rs = run_device(p, &d, n, &o, stats, pipe ? &chunks : nullptr);
+    // no copy from the caller's arrays may still be in flight when this returns
+    if (pipe) CUDA_TRY(cudaStreamSynchronize(p->copy_stream));
     if (rs != CRP_OK && rs != CRP_ERR_CANCELLED) return rs;
     D2H(x, 8 * n); D2H(y, 8 * n); D2H(z, 8 * n); D2H(dx, 8 * n); D2H(dy, 8 * n); D2H(dz, 8 * n);
     D2H(px, 8 * n); D2H(py, 8 * n); D2H(pz, 8 * n);
@@ -985,7 +1113,6 @@ crp_status crp_run(crp_plan *p, const crp_candidates *h, uint64_t n, const crp_r
 #undef RD2H
         }
     }
-#undef H2D
 #undef D2H
     CUDA_TRY(cudaStreamSynchronize(st));
     return rs;

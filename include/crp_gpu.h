@@ -503,7 +503,11 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **plan);
 crp_status crp_plan_destroy(crp_plan *plan);
 
 /* Run every active candidate until it is inactive (or max_steps).  Host
- * arrays: copied to the device and back inside the call. */
+ * arrays: copied to the device and back inside the call; in the chunked mode,
+ * from 2^18 candidates on, the inputs go in 8 chunks on a copy stream and the
+ * first launch starts on each chunk as it arrives (the first launch's
+ * device_ms then includes that wait).  Pinned host arrays give the fastest
+ * copies. */
 crp_status crp_run(crp_plan *plan, const crp_candidates *host, uint64_t n,
                    const crp_run_opts *opts, crp_run_stats *stats);
 /* Same, on device-resident arrays, asynchronous with respect to the host

@@ -72,3 +72,36 @@ def test_cell_ordered_run_equals_unordered(case, precision):
     assert len(ga["index"]) > 1000
     for k in ga:
         np.testing.assert_array_equal(ga[k], gb[k], err_msg=k)
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_MIXED, _abi.PRECISION_FP64])
+def test_host_run_with_chunked_inputs_equals_device_run(precision):
+    """crp_run on host arrays of at least 2^18 candidates copies the inputs
+    in chunks and starts the first launch on each chunk as it arrives (one
+    stream per chunk): the same candidates, states and records as the device
+    run, bit for bit; a count that does not split evenly included."""
+    from crpropa3_b200.engine import Plan
+    plan = Plan(_spec("periodic_pow2_bp", precision))
+    n = (1 << 18) + 5
+    rng = np.random.default_rng(83)
+    c = CandidateArrays(n)
+    from crpropa3_b200.workloads import charge_of
+    c.id[:] = 1000010010
+    c.charge[:] = charge_of(1000010010)
+    c.energy[:] = np.exp(rng.uniform(np.log(1), np.log(100), n)) * U.EeV
+    c.set_position(rng.uniform(-100, 100, (n, 3)) * U.kpc)
+    c.set_direction(stable_unit_vectors(rng, n))
+    c.next_step[:] = 1e30
+    h, d = c.copy(), c.to_device("cuda")
+    rh, rd = RecordArrays(2 * n), RecordArrays(2 * n, device="cuda")
+    sh = plan.run(h, records=rh, mode=_abi.MODE_CHUNKED)
+    sd = plan.run(d, records=rd, mode=_abi.MODE_CHUNKED)
+    assert sh.particle_steps == sd.particle_steps > 0
+    hd = d.to_host()
+    for m in STATE:
+        if getattr(h, m) is not None:
+            np.testing.assert_array_equal(getattr(h, m), getattr(hd, m), err_msg=m)
+    gh, gd = _records(rh), _records(rd.to_host())
+    assert len(gh["index"]) > 1000
+    for k in gh:
+        np.testing.assert_array_equal(gh[k], gd[k], err_msg=k)
