@@ -12,7 +12,7 @@ import os
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcrp_b200.so")
 
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 # crp_status
 OK = 0
@@ -173,10 +173,22 @@ class FeatureDesc(C.Structure):
                 ("r", _d), ("step", _d)]
 
 
+ADVECTION_UNIFORM, ADVECTION_CONSTANT_SPHERICAL, ADVECTION_SPHERICAL, ADVECTION_CARTESIAN_SHOCK, \
+    ADVECTION_SPHERICAL_SHOCK_1D, ADVECTION_OBLIQUE_SHOCK, ADVECTION_SPHERICAL_SHOCK = 1, 2, 3, 4, 5, 6, 7
+MAX_ADVECTION = 4
+
+
+class AdvectionDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("cool_upstream", C.c_int32), ("value", _d * 3), ("origin", _d * 3)] + [
+        (n, _d) for n in ("v", "radius", "tau", "alpha", "compression", "length", "vy", "r_rot", "v_phi")]
+
+
 class ModuleDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("propagator", C.c_int32), ("tolerance", _d),
                 ("min_step", _d), ("max_step", _d), ("sde_epsilon", _d), ("sde_alpha", _d),
-                ("sde_scale", _d), ("max_length", _d), ("per_candidate_length", C.c_int32),
+                ("sde_scale", _d), ("n_advection", C.c_int32), ("_pad_adv", C.c_int32),
+                ("advection", AdvectionDesc * MAX_ADVECTION),
+                ("max_length", _d), ("per_candidate_length", C.c_int32),
                 ("observer_feature", C.c_int32), ("sphere_center", _d * 3),
                 ("sphere_radius", _d), ("deactivate_on_detection", C.c_int32),
                 ("record", C.c_int32), ("n_features", C.c_int32), ("boundary", C.c_int32),

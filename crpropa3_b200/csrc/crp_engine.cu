@@ -195,6 +195,14 @@ crp_status validate_module(const crp_module_desc &m) {
                 return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: alpha not in range 0-2");
             if (m.sde_scale < 0)
                 return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: Scale error: Scale < 0");
+            if (m.n_advection < 0 || m.n_advection > CRP_MAX_ADVECTION)
+                return fail(CRP_ERR_UNSUPPORTED, "DiffusionSDE: at most %d advection fields", CRP_MAX_ADVECTION);
+            for (int a = 0; a < m.n_advection; a++)
+                if (m.advection[a].kind < CRP_ADVECTION_UNIFORM || m.advection[a].kind > CRP_ADVECTION_SPHERICAL_SHOCK)
+                    return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: unknown advection field kind %d",
+                                m.advection[a].kind);
+        } else if (m.n_advection != 0) {
+            return fail(CRP_ERR_INVALID_ARGUMENT, "%s: advection fields belong to DiffusionSDE", name);
         }
     } else if (m.kind == CRP_MODULE_MAX_TRAJECTORY_LENGTH) {
     } else if (m.kind == CRP_MODULE_OBSERVER) {
@@ -539,6 +547,13 @@ crp_status crp_plan_create(const crp_plan_desc *desc, crp_plan **out) {
         dm.kind = m.kind; dm.propagator = m.propagator;
         dm.tolerance = m.tolerance; dm.min_step = m.min_step; dm.max_step = m.max_step;
         dm.eps = m.sde_epsilon; dm.alpha = m.sde_alpha; dm.scale = m.sde_scale;
+        dm.n_adv = 0;
+        dm.adv = nullptr;
+        if (m.kind == CRP_MODULE_PROPAGATION && m.propagator == CRP_PROP_SDE && m.n_advection > 0) {
+            crp_status st = upload(p, m.advection, (size_t)m.n_advection, &dm.adv);
+            if (st) { delete p; return st; }
+            dm.n_adv = m.n_advection;
+        }
         dm.max_length = m.max_length; dm.per_candidate = m.per_candidate_length;
         dm.observer = m.observer_feature;
         dm.cx = m.sphere_center[0]; dm.cy = m.sphere_center[1]; dm.cz = m.sphere_center[2];

@@ -86,6 +86,8 @@ struct DevModule {
     int propagator;  // crp_propagator
     double tolerance, min_step, max_step;
     double eps, alpha, scale;
+    int n_adv;                        // DiffusionSDE: advection fields, summed (0: none)
+    const crp_advection_desc *adv;    // device copy of the n_adv descriptors
     double max_length;
     int per_candidate;
     int observer;    // crp_observer_feature

@@ -26,6 +26,7 @@
 #include "tf17.cuh"
 #include "jf12.cuh"
 #include "kst24_cmz.cuh"
+#include "advection.cuh"
 
 
 // Resident blocks of 128 threads per SM the register budget of the
@@ -791,6 +792,17 @@ __device__ __forceinline__ void sde_co_start_try(SdeCo &co, double x, double y, 
     co.qx = x; co.qy = y; co.qz = z;
 }
 
+// DiffusionSDE::driftStep (DiffusionSDE.cpp:255): the advection drift over
+// the step time h at the step's start position (zero without a field).
+__device__ __forceinline__ void sde_lin_prop(const DevModule &m, double x, double y, double z, double h, double &lx,
+                                             double &ly, double &lz) {
+    lx = ly = lz = 0.;
+    if (m.n_adv) {
+        const u3 v = advection_at(m.adv, m.n_adv, x, y, z);
+        lx = v.x * h; ly = v.y * h; lz = v.z * h;
+    }
+}
+
 // First part of SDE::process up to the first field evaluation.  Returns
 // false when the step needs no field (neutral candidate): it is then done.
 template <int FS>
@@ -798,7 +810,10 @@ __device__ __forceinline__ bool sde_co_begin(const DevPlan &P, const DevModule &
     c.px = c.x; c.py = c.y; c.pz = c.z;
     const double h = clipd(c.next, m.min_step, m.max_step) * kInvCLight;
     if (c.q == 0) {
-        c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+        double lx, ly, lz;
+        sde_lin_prop(m, c.x, c.y, c.z, h, lx, ly, lz);
+        c.x = fma(c.dx, h * kCLight, c.x + lx); c.y = fma(c.dy, h * kCLight, c.y + ly);
+        c.z = fma(c.dz, h * kCLight, c.z + lz);
         set_current_step(c, h * kCLight);
         c.next = m.max_step;
         return false;
@@ -824,8 +839,14 @@ __device__ __forceinline__ void sde_co_finish(const DevPlan &P, const DevModule 
     double tx = co.ox - c.x, ty = co.oy - c.y, tz = co.oz - c.z;
     double tn = sqrt(ddot(tx, ty, tz, tx, ty, tz));
     tx /= tn; ty /= tn; tz /= tn;
+    double lx, ly, lz;
+    sde_lin_prop(m, c.x, c.y, c.z, h, lx, ly, lz);
     if (!(tn == tn) || tn == 0.0) {
-        c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+        if (m.n_adv) {  // only the advection drift
+            c.x += lx; c.y += ly; c.z += lz;
+        } else {
+            c.x = fma(c.dx, h * kCLight, c.x); c.y = fma(c.dy, h * kCLight, c.y); c.z = fma(c.dz, h * kCLight, c.z);
+        }
         set_current_step(c, h * kCLight);
         c.next = clipd(5 * h * kCLight, m.min_step, m.max_step);
         return;
@@ -846,9 +867,9 @@ __device__ __forceinline__ void sde_co_finish(const DevPlan &P, const DevModule 
     double bx = dcross_c(ty, nz, ny, tz), by = dcross_c(tz, nx, nz, tx), bz = dcross_c(tx, ny, nx, ty);
     double bn = sqrt(ddot(bx, by, bz, bx, by, bz));
     bx /= bn; by /= bn; bz /= bn;
-    double POx = fma(fma(nx, co.NStep, bx * co.BStep), sh, co.ox);
-    double POy = fma(fma(ny, co.NStep, by * co.BStep), sh, co.oy);
-    double POz = fma(fma(nz, co.NStep, bz * co.BStep), sh, co.oz);
+    double POx = fma(fma(nx, co.NStep, bx * co.BStep), sh, co.ox + lx);
+    double POy = fma(fma(ny, co.NStep, by * co.BStep), sh, co.oy + ly);
+    double POz = fma(fma(nz, co.NStep, bz * co.BStep), sh, co.oz + lz);
     if (isnan(POx + POy + POz)) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
     s.cursor = 12;
     double theta = acos(s_uniform(s, 1, cos(kPi / 2.)));

@@ -24,6 +24,7 @@
 #include "tf17.cuh"
 #include "jf12.cuh"
 #include "kst24_cmz.cuh"
+#include "advection.cuh"
 
 // Resident blocks of 128 threads per SM the register budget of the
 // fixed-step Boris and the Cash-Karp kernels is sized for (measured on the
@@ -498,13 +499,19 @@ __device__ __forceinline__ void sde_try(const DevPlan &P, d3 PosIn, d3 &POut, d3
 template <int FS>
 struct SDE {
     static constexpr bool kReadsStepCount = true;  // the Philox counter
-    // DiffusionSDE::process (DiffusionSDE.cpp:47), without advection field.
+    // DiffusionSDE::process (DiffusionSDE.cpp:47); the advection drift of
+    // driftStep (:255) is LinProp = 0 + v_adv(PosIn) h.
+    __device__ static d3 lin_prop(const DevModule &m, d3 pos, double h) {
+        if (m.n_adv == 0) return mk(0, 0, 0);
+        const u3 v = advection_at(m.adv, m.n_adv, pos.x, pos.y, pos.z);
+        return add(mk(0, 0, 0), muls(mk(v.x, v.y, v.z), h));
+    }
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
         c.px = c.x; c.py = c.y; c.pz = c.z;
         double h = clipd(c.next, m.min_step, m.max_step) / kCLight;
         d3 PosIn = mk(c.x, c.y, c.z);
         if (c.q == 0) {
-            d3 p = add(add(PosIn, mk(0, 0, 0)), muls(muls(mk(c.dx, c.dy, c.dz), h), kCLight));
+            d3 p = add(add(PosIn, lin_prop(m, PosIn, h)), muls(muls(mk(c.dx, c.dy, c.dz), h), kCLight));
             c.x = p.x; c.y = p.y; c.z = p.z;
             set_current_step(c, h * kCLight);
             c.next = m.max_step;
@@ -539,7 +546,12 @@ struct SDE {
         d3 TVec = unit(sub(PosOut, PosIn));
         double tTest = norm(TVec);
         if (tTest != tTest) {
-            c.x = c.x + c.dx * h * kCLight; c.y = c.y + c.dy * h * kCLight; c.z = c.z + c.dz * h * kCLight;
+            if (m.n_adv) {  // only the advection drift
+                const d3 p = add(PosIn, lin_prop(m, PosIn, h));
+                c.x = p.x; c.y = p.y; c.z = p.z;
+            } else {
+                c.x = c.x + c.dx * h * kCLight; c.y = c.y + c.dy * h * kCLight; c.z = c.z + c.dz * h * kCLight;
+            }
             set_current_step(c, h * kCLight);
             double newStep = 5 * h * kCLight;
             c.next = clipd(newStep, m.min_step, m.max_step);
@@ -550,7 +562,7 @@ struct SDE {
         if (norm(NVec) == 0.) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
         NVec = unit(NVec);
         d3 BVec = unit(cross(TVec, NVec));
-        d3 PO = add(add(PosOut, mk(0, 0, 0)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
+        d3 PO = add(add(PosOut, lin_prop(m, PosIn, h)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
         if (isnan(norm(PO))) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
         s.cursor = 12;  // the cone draw takes the fourth block of the step
         double theta = acos(s_uniform(s, 1, cos(kPi / 2.)));

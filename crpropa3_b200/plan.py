@@ -298,6 +298,110 @@ class Propagation:
     epsilon: float = 0.1
     alpha: float = 1.0 / 3.0
     scale: float = 1.0
+    # DiffusionSDE's advection field (DiffusionSDE(magneticField, advectionField, ...),
+    # DiffusionSDE.cpp:34): up to four of the classes below, summed in order
+    advection: Sequence = ()
+
+
+def _adv(kind, **kw) -> "_abi.AdvectionDesc":
+    d = _abi.AdvectionDesc()
+    d.kind = kind
+    for k, v in kw.items():
+        if k in ("value", "origin"):
+            for a in range(3):
+                getattr(d, k)[a] = float(v[a])
+        else:
+            setattr(d, k, int(v) if k == "cool_upstream" else float(v))
+    return d
+
+
+@dataclass
+class UniformAdvectionField:
+    """UniformAdvectionField(value) (AdvectionField.cpp:29) [m/s]."""
+    value: Sequence[float]
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_UNIFORM, value=self.value)
+
+
+@dataclass
+class ConstantSphericalAdvectionField:
+    """ConstantSphericalAdvectionField(origin, vWind) (AdvectionField.cpp:49)."""
+    origin: Sequence[float]
+    v_wind: float
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_CONSTANT_SPHERICAL, origin=self.origin, v=self.v_wind)
+
+
+@dataclass
+class SphericalAdvectionField:
+    """SphericalAdvectionField(origin, radius, vMax, tau, alpha) (AdvectionField.cpp:93)."""
+    origin: Sequence[float]
+    radius: float
+    v_max: float
+    tau: float
+    alpha: float
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_SPHERICAL, origin=self.origin, radius=self.radius, v=self.v_max,
+                    tau=self.tau, alpha=self.alpha)
+
+
+@dataclass
+class OneDimensionalCartesianShock:
+    """OneDimensionalCartesianShock(compressionRatio, vUp, lShock) (AdvectionField.cpp:182)."""
+    compression: float
+    v_up: float
+    l_shock: float
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_CARTESIAN_SHOCK, compression=self.compression, v=self.v_up,
+                    length=self.l_shock)
+
+
+@dataclass
+class OneDimensionalSphericalShock:
+    """OneDimensionalSphericalShock(rShock, vUp, compressionRatio, lShock,
+    coolUpstream) (AdvectionField.cpp:246)."""
+    r_shock: float
+    v_up: float
+    compression: float
+    l_shock: float
+    cool_upstream: bool
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_SPHERICAL_SHOCK_1D, radius=self.r_shock, v=self.v_up,
+                    compression=self.compression, length=self.l_shock, cool_upstream=self.cool_upstream)
+
+
+@dataclass
+class ObliqueAdvectionShock:
+    """ObliqueAdvectionShock(compressionRatio, vXUp, vY, lShock) (AdvectionField.cpp:353)."""
+    compression: float
+    v_x_up: float
+    v_y: float
+    l_shock: float
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_OBLIQUE_SHOCK, compression=self.compression, v=self.v_x_up, vy=self.v_y,
+                    length=self.l_shock)
+
+
+@dataclass
+class SphericalAdvectionShock:
+    """SphericalAdvectionShock(origin, r_0, v_0, lambda) (AdvectionField.cpp:432)
+    with setRRot (default r_0) and setAzimuthalSpeed (default 0)."""
+    origin: Sequence[float]
+    r_0: float
+    v_0: float
+    lambda_: float
+    r_rot: Optional[float] = None
+    v_phi: float = 0.0
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_SPHERICAL_SHOCK, origin=self.origin, radius=self.r_0, v=self.v_0,
+                    length=self.lambda_, r_rot=self.r_0 if self.r_rot is None else self.r_rot, v_phi=self.v_phi)
 
 
 @dataclass
@@ -476,6 +580,12 @@ class ChainSpec:
             d.propagator = int(m.propagator)
             d.tolerance, d.min_step, d.max_step = float(m.tolerance), float(m.min_step), float(m.max_step)
             d.sde_epsilon, d.sde_alpha, d.sde_scale = float(m.epsilon), float(m.alpha), float(m.scale)
+            adv = list(m.advection or ())
+            if len(adv) > _abi.MAX_ADVECTION:
+                raise ValueError(f"DiffusionSDE: at most {_abi.MAX_ADVECTION} advection fields")
+            d.n_advection = len(adv)
+            for i, a in enumerate(adv):
+                d.advection[i] = a.desc()
         elif isinstance(m, MaxTrajectoryLength):
             d.kind = _abi.MODULE_MAX_TRAJECTORY_LENGTH
             d.max_length = float(m.max_length)

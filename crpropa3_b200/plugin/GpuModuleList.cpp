@@ -21,6 +21,7 @@
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
+#include "crpropa/advectionField/AdvectionField.h"
 #include "crpropa/module/Observer.h"
 #include "crpropa/module/Output.h"
 #include "crpropa/module/PropagationBP.h"
@@ -110,6 +111,8 @@ CRPGPU_PT11(PT11Rc, R_c); CRPGPU_PT11(PT11Z0D, z0_D); CRPGPU_PT11(PT11B0D, B0_D)
 CRPGPU_PT11(PT11R0H, R0_H); CRPGPU_PT11(PT11B0Hn, B0_Hn); CRPGPU_PT11(PT11B0Hs, B0_Hs);
 CRPGPU_PT11(PT11Z11H, z11_H); CRPGPU_PT11(PT11Z12H, z12_H);
 #undef CRPGPU_PT11
+typedef std::vector<ref_ptr<AdvectionField> > AdvectionVector;
+CRPGPU_MEMBER(AdvectionListFields, AdvectionFieldList, AdvectionVector, fields);  // AdvectionField.h:37
 typedef double JF12Arms[11];
 typedef double JF12Coeff[10];
 CRPGPU_MEMBER(JF12CotPitch, JF12Field, double, cotPitch);                 // JF12Field.h:47-61
@@ -189,6 +192,67 @@ std::string type_name(const void *obj, const std::type_info &ti) {
 template <class T>
 std::string name_of(const T *obj) {
     return type_name(obj, typeid(*obj));
+}
+
+// The advection field of a DiffusionSDE (exact types, AdvectionField.h:36-265)
+// as crp_advection_desc entries of the module: a list becomes its fields in
+// order (AdvectionFieldList::getField sums them, AdvectionField.cpp:12).
+void addAdvection(const AdvectionField *f, crp_module_desc &d) {
+    if (d.n_advection >= CRP_MAX_ADVECTION)
+        throw Unsupported("DiffusionSDE with more than " + std::to_string(CRP_MAX_ADVECTION) + " advection fields");
+    crp_advection_desc &A = d.advection[d.n_advection];
+    std::memset(&A, 0, sizeof(A));
+    auto origin = [&](const Vector3d &o) { A.origin[0] = o.x; A.origin[1] = o.y; A.origin[2] = o.z; };
+    const std::type_info &t = typeid(*f);
+    if (t == typeid(UniformAdvectionField)) {
+        A.kind = CRP_ADVECTION_UNIFORM;  // a constant field: its value anywhere
+        const Vector3d v = f->getField(Vector3d(0.), 0.);
+        A.value[0] = v.x; A.value[1] = v.y; A.value[2] = v.z;
+    } else if (t == typeid(ConstantSphericalAdvectionField)) {
+        const ConstantSphericalAdvectionField *c = static_cast<const ConstantSphericalAdvectionField *>(f);
+        A.kind = CRP_ADVECTION_CONSTANT_SPHERICAL;
+        origin(c->getOrigin());
+        A.v = c->getVWind();
+    } else if (t == typeid(SphericalAdvectionField)) {
+        const SphericalAdvectionField *c = static_cast<const SphericalAdvectionField *>(f);
+        A.kind = CRP_ADVECTION_SPHERICAL;
+        origin(c->getOrigin());
+        A.radius = c->getRadius(); A.v = c->getVMax(); A.tau = c->getTau(); A.alpha = c->getAlpha();
+    } else if (t == typeid(OneDimensionalCartesianShock)) {
+        const OneDimensionalCartesianShock *c = static_cast<const OneDimensionalCartesianShock *>(f);
+        A.kind = CRP_ADVECTION_CARTESIAN_SHOCK;
+        A.compression = c->getComp(); A.v = c->getVup(); A.length = c->getShockwidth();
+    } else if (t == typeid(OneDimensionalSphericalShock)) {
+        const OneDimensionalSphericalShock *c = static_cast<const OneDimensionalSphericalShock *>(f);
+        A.kind = CRP_ADVECTION_SPHERICAL_SHOCK_1D;
+        A.radius = c->getShockRadius(); A.v = c->getVup(); A.compression = c->getComp();
+        A.length = c->getShockwidth(); A.cool_upstream = c->getCooling() ? 1 : 0;
+    } else if (t == typeid(ObliqueAdvectionShock)) {
+        const ObliqueAdvectionShock *c = static_cast<const ObliqueAdvectionShock *>(f);
+        A.kind = CRP_ADVECTION_OBLIQUE_SHOCK;
+        A.compression = c->getComp(); A.v = c->getVup(); A.vy = c->getVy(); A.length = c->getShockwidth();
+    } else if (t == typeid(SphericalAdvectionShock)) {
+        const SphericalAdvectionShock *c = static_cast<const SphericalAdvectionShock *>(f);
+        A.kind = CRP_ADVECTION_SPHERICAL_SHOCK;
+        origin(c->getOrigin());
+        A.radius = c->getR0(); A.v = c->getV0(); A.length = c->getLambda();
+        A.r_rot = c->getRRot(); A.v_phi = c->getAzimuthalSpeed();
+    } else {
+        throw Unsupported(name_of(f) + " (an advection field without a device form)");
+    }
+    d.n_advection++;
+}
+
+void translateAdvection(const AdvectionField *f, crp_module_desc &d) {
+    if (typeid(*f) == typeid(AdvectionFieldList)) {
+        const AdvectionFieldList *l = static_cast<const AdvectionFieldList *>(f);
+        for (const ref_ptr<AdvectionField> &g : l->*member(AdvectionListFields())) {
+            if (typeid(*g) == typeid(AdvectionFieldList)) throw Unsupported("a nested AdvectionFieldList");
+            addAdvection(g.get(), d);
+        }
+    } else {
+        addAdvection(f, d);
+    }
 }
 
 std::string crp_error(crp_status st) {
@@ -556,9 +620,8 @@ struct Translation {
             setField(p->getField().get());
             push(d, Action());
         } else if (const DiffusionSDE *p = dynamic_cast<const DiffusionSDE *>(m)) {
-            if (p->getAdvectionField().valid())
-                throw Unsupported("DiffusionSDE with an advection field");
             crp_module_desc d = blank(CRP_MODULE_PROPAGATION);
+            if (p->getAdvectionField().valid()) translateAdvection(p->getAdvectionField().get(), d);
             d.propagator = CRP_PROP_SDE;
             d.tolerance = p->getTolerance();
             d.min_step = p->getMinimumStep();

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CRP_ABI_VERSION 8u
+#define CRP_ABI_VERSION 9u
 
 typedef enum crp_status {
     CRP_OK = 0,
@@ -363,6 +363,34 @@ enum crp_boundary_kind {
     CRP_BOUNDARY_CYLINDRICAL = 4 /* CylindricalBoundary (Boundary.cpp:303): a = origin, size = height, radius */
 };
 
+/* Advection fields of DiffusionSDE (AdvectionField.h:23-265, getField of
+ * AdvectionField.cpp:12-420), SI units.  The fields each kind reads:
+ *   UNIFORM             value
+ *   CONSTANT_SPHERICAL  origin, v (vWind)
+ *   SPHERICAL           origin, radius, v (vMax), tau, alpha
+ *   CARTESIAN_SHOCK     compression, v (vUp), length (lShock)
+ *   SPHERICAL_SHOCK_1D  radius (rShock), v (vUp), compression, length (lShock), cool_upstream
+ *   OBLIQUE_SHOCK       compression, v (vXUp), vy, length (lShock)
+ *   SPHERICAL_SHOCK     origin, radius (r_0), v (v_0), length (lambda), r_rot, v_phi */
+enum crp_advection_kind {
+    CRP_ADVECTION_UNIFORM = 1,            /* UniformAdvectionField */
+    CRP_ADVECTION_CONSTANT_SPHERICAL = 2, /* ConstantSphericalAdvectionField */
+    CRP_ADVECTION_SPHERICAL = 3,          /* SphericalAdvectionField */
+    CRP_ADVECTION_CARTESIAN_SHOCK = 4,    /* OneDimensionalCartesianShock */
+    CRP_ADVECTION_SPHERICAL_SHOCK_1D = 5, /* OneDimensionalSphericalShock */
+    CRP_ADVECTION_OBLIQUE_SHOCK = 6,      /* ObliqueAdvectionShock */
+    CRP_ADVECTION_SPHERICAL_SHOCK = 7     /* SphericalAdvectionShock */
+};
+#define CRP_MAX_ADVECTION 4
+
+typedef struct crp_advection_desc {
+    int32_t kind;          /* crp_advection_kind */
+    int32_t cool_upstream; /* OneDimensionalSphericalShock::setCooling */
+    double value[3];
+    double origin[3];
+    double v, radius, tau, alpha, compression, length, vy, r_rot, v_phi;
+} crp_advection_desc;
+
 typedef struct crp_module_desc {
     int32_t kind;
     /* CRP_MODULE_PROPAGATION */
@@ -373,6 +401,11 @@ typedef struct crp_module_desc {
     double sde_epsilon; /* DiffusionSDE::setEpsilon */
     double sde_alpha;   /* DiffusionSDE::setAlpha */
     double sde_scale;   /* DiffusionSDE::setScale */
+    /* DiffusionSDE::setAdvectionField: n_advection fields, summed in order
+     * (an AdvectionFieldList, AdvectionField.cpp:12); 0: none */
+    int32_t n_advection;
+    int32_t _pad_adv;
+    crp_advection_desc advection[CRP_MAX_ADVECTION];
     /* CRP_MODULE_MAX_TRAJECTORY_LENGTH */
     double max_length;            /* [m] */
     int32_t per_candidate_length; /* use crp_candidates.max_length[i] instead */

@@ -1578,14 +1578,86 @@ static void sde_try(const crp_plan_desc *d, v3 PosIn, v3 *POut, v3 *PosErr, doub
     }
 }
 
-/* DiffusionSDE::process (DiffusionSDE.cpp:47), without an advection field. */
+/* ------------------------------------------------------------ AdvectionField
+ * getField of the advection fields (AdvectionField.cpp:12-460), glibc's libm
+ * as the reference calls it. */
+static v3 advection_one(const crp_advection_desc *A, v3 pos) {
+    switch (A->kind) {
+    case CRP_ADVECTION_UNIFORM: /* :33 */
+        return mk(A->value[0], A->value[1], A->value[2]);
+    case CRP_ADVECTION_CONSTANT_SPHERICAL: { /* :54 */
+        v3 P = sub(pos, mk(A->origin[0], A->origin[1], A->origin[2]));
+        v3 u = unit(P);
+        return mk(A->v * u.x, A->v * u.y, A->v * u.z);
+    }
+    case CRP_ADVECTION_SPHERICAL: { /* :101, getV :120 */
+        v3 P = sub(pos, mk(A->origin[0], A->origin[1], A->origin[2]));
+        double R = norm(P);
+        if (R > A->radius) return mk(0, 0, 0);
+        double vR = A->v * (1 - exp(-(pow(R, A->alpha) / A->tau)));
+        v3 u = unit(P);
+        return mk(vR * u.x, vR * u.y, vR * u.z);
+    }
+    case CRP_ADVECTION_CARTESIAN_SHOCK: /* :188 */
+    case CRP_ADVECTION_OBLIQUE_SHOCK: { /* :359 */
+        double vDown = A->v / A->compression;
+        double a = (A->v + vDown) * 0.5, b = (A->v - vDown) * 0.5;
+        v3 v = mk(0, 0, 0);
+        v.x = a - b * tanh(pos.x / A->length);
+        if (A->kind == CRP_ADVECTION_OBLIQUE_SHOCK) v.y = A->vy;
+        return v;
+    }
+    case CRP_ADVECTION_SPHERICAL_SHOCK_1D: { /* :254 */
+        double r = norm(pos);
+        v3 e_r = unit(pos);
+        double vDown = A->v / A->compression;
+        double a = (A->v + vDown) * 0.5, b = (A->v - vDown) * 0.5;
+        double v;
+        if (A->cool_upstream) {
+            if (r <= A->radius) v = a - b * tanh((r - A->radius) / A->length);
+            else v = (a - b * tanh((r - A->radius) / A->length)) * (A->radius / r) * (A->radius / r);
+        } else {
+            v = (a - b * tanh((r - A->radius) / A->length)) * (A->radius / r) * (A->radius / r);
+        }
+        return mk(v * e_r.x, v * e_r.y, v * e_r.z);
+    }
+    default: { /* CRP_ADVECTION_SPHERICAL_SHOCK, :441; g :463 */
+        v3 R = sub(pos, mk(A->origin[0], A->origin[1], A->origin[2]));
+        v3 e_r = unit(R);
+        double phi = ((fabs(R.x) < DBL_MIN) && (fabs(R.y) < DBL_MIN)) ? 0.0 : atan2(R.y, R.x);
+        v3 e_phi = mk(-sin(phi), cos(phi), 0);
+        double r = norm(R);
+        double g = 1. / (1 + exp(-((r - A->radius) / A->length)));
+        double v_r = A->v * (1 + (pow(A->radius / (2 * r), 2.) - 1) * g);
+        double v_p = A->v_phi * (A->r_rot / r);
+        return add(muls(e_r, v_r), muls(e_phi, v_p));
+    }
+    }
+}
+
+/* DiffusionSDE::driftStep (DiffusionSDE.cpp:255): LinProp = 0 + v(pos) h;
+ * several fields are an AdvectionFieldList (:12), summed in order. */
+static v3 sde_lin_prop(const crp_module_desc *m, v3 pos, double h) {
+    if (m->n_advection == 0) return mk(0, 0, 0);
+    v3 v;
+    if (m->n_advection == 1) {
+        v = advection_one(&m->advection[0], pos);
+    } else {
+        v = mk(0, 0, 0);
+        for (int i = 0; i < m->n_advection; i++) v = add(v, advection_one(&m->advection[i], pos));
+    }
+    return add(mk(0, 0, 0), muls(v, h));
+}
+
+/* DiffusionSDE::process (DiffusionSDE.cpp:47) with the advection drift of
+ * driftStep. */
 static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t *c, uint64_t *tries) {
     c->prev = c->pos;
     double h = clipd(c->next, m->min_step, m->max_step) / c_light;
     v3 PosIn = c->pos, DirIn = c->dir;
     (void)DirIn;
     if (c->q == 0) {
-        c->pos = add(add(c->pos, mk(0, 0, 0)), muls(muls(c->dir, h), c_light));
+        c->pos = add(add(c->pos, sde_lin_prop(m, PosIn, h)), muls(muls(c->dir, h), c_light));
         set_current_step(c, h * c_light);
         c->next = m->max_step;
         return;
@@ -1620,7 +1692,8 @@ static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t
     v3 TVec = unit(sub(PosOut, PosIn));
     double tTest = norm(TVec);
     if (tTest != tTest) {
-        c->pos = add(c->pos, muls(muls(c->dir, h), c_light));
+        if (m->n_advection) c->pos = add(c->pos, sde_lin_prop(m, PosIn, h));  /* advection only */
+        else c->pos = add(c->pos, muls(muls(c->dir, h), c_light));
         set_current_step(c, h * c_light);
         double newStep = 5 * h * c_light;
         c->next = clipd(newStep, m->min_step, m->max_step);
@@ -1632,7 +1705,7 @@ static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t
     if (norm(NVec) == 0.) { c->active = 0; c->flags |= CRP_FLAG_NAN; return; }
     NVec = unit(NVec);
     v3 BVec = unit(cross(TVec, NVec));
-    v3 PO = add(add(PosOut, mk(0, 0, 0)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
+    v3 PO = add(add(PosOut, sde_lin_prop(m, PosIn, h)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
     if (isnan(norm(PO))) { c->active = 0; c->flags |= CRP_FLAG_NAN; return; }
     s.cursor = 12; /* the cone draw uses the fourth block of the step */
     v3 DirOut = stream_cone(&s, TVec, M_PI / 2.);

@@ -54,6 +54,7 @@
 #include "crpropa/module/Boundary.h"
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
+#include "crpropa/advectionField/AdvectionField.h"
 #include "crpropa/module/Observer.h"
 #include "crpropa/module/ParticleCollector.h"
 #include "crpropa/module/PropagationBP.h"
@@ -304,6 +305,45 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpe
                                                      m.sde_epsilon);
                 sde->setAlpha(m.sde_alpha);
                 sde->setScale(m.sde_scale);
+                if (m.n_advection > 0) {  // the advection fields' constructors and setters
+                    std::vector<ref_ptr<AdvectionField> > fs;
+                    for (int a = 0; a < m.n_advection; a++) {
+                        const crp_advection_desc &A = m.advection[a];
+                        const Vector3d o(A.origin[0], A.origin[1], A.origin[2]);
+                        AdvectionField *f = nullptr;
+                        switch (A.kind) {
+                        case CRP_ADVECTION_UNIFORM:
+                            f = new UniformAdvectionField(Vector3d(A.value[0], A.value[1], A.value[2])); break;
+                        case CRP_ADVECTION_CONSTANT_SPHERICAL: f = new ConstantSphericalAdvectionField(o, A.v); break;
+                        case CRP_ADVECTION_SPHERICAL:
+                            f = new SphericalAdvectionField(o, A.radius, A.v, A.tau, A.alpha); break;
+                        case CRP_ADVECTION_CARTESIAN_SHOCK:
+                            f = new OneDimensionalCartesianShock(A.compression, A.v, A.length); break;
+                        case CRP_ADVECTION_SPHERICAL_SHOCK_1D:
+                            f = new OneDimensionalSphericalShock(A.radius, A.v, A.compression, A.length,
+                                                                 A.cool_upstream != 0);
+                            break;
+                        case CRP_ADVECTION_OBLIQUE_SHOCK:
+                            f = new ObliqueAdvectionShock(A.compression, A.v, A.vy, A.length); break;
+                        case CRP_ADVECTION_SPHERICAL_SHOCK: {
+                            SphericalAdvectionShock *s = new SphericalAdvectionShock(o, A.radius, A.v, A.length);
+                            s->setRRot(A.r_rot);
+                            s->setAzimuthalSpeed(A.v_phi);
+                            f = s;
+                            break;
+                        }
+                        default: throw std::runtime_error("ref_shim: unknown advection field");
+                        }
+                        fs.push_back(f);
+                    }
+                    if (fs.size() == 1) {
+                        sde->setAdvectionField(fs[0]);
+                    } else {
+                        AdvectionFieldList *l = new AdvectionFieldList();
+                        for (auto &f : fs) l->addField(f);
+                        sde->setAdvectionField(l);
+                    }
+                }
                 b.sim->add(sde);
             } else {
                 throw std::runtime_error("ref_shim: unknown propagator");
