@@ -174,13 +174,15 @@ class FeatureDesc(C.Structure):
 
 
 ADVECTION_UNIFORM, ADVECTION_CONSTANT_SPHERICAL, ADVECTION_SPHERICAL, ADVECTION_CARTESIAN_SHOCK, \
-    ADVECTION_SPHERICAL_SHOCK_1D, ADVECTION_OBLIQUE_SHOCK, ADVECTION_SPHERICAL_SHOCK = 1, 2, 3, 4, 5, 6, 7
+    ADVECTION_SPHERICAL_SHOCK_1D, ADVECTION_OBLIQUE_SHOCK, ADVECTION_SPHERICAL_SHOCK, ADVECTION_TIME_SHOCK, \
+    ADVECTION_SEDOV_TAYLOR = 1, 2, 3, 4, 5, 6, 7, 8, 9
 MAX_ADVECTION = 4
 
 
 class AdvectionDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("cool_upstream", C.c_int32), ("value", _d * 3), ("origin", _d * 3)] + [
-        (n, _d) for n in ("v", "radius", "tau", "alpha", "compression", "length", "vy", "r_rot", "v_phi")]
+        (n, _d) for n in ("v", "radius", "tau", "alpha", "compression", "length", "vy", "r_rot", "v_phi",
+                          "v1", "v0", "x0", "t0", "energy", "density")]
 
 
 class ModuleDesc(C.Structure):

@@ -16,9 +16,31 @@ __device__ __forceinline__ u3 adv_radial(double x, double y, double z, double f)
     return {f * (x / R), f * (y / R), f * (z / R)};
 }
 
-// One advection field (crp_advection_desc) at (x, y, z).
-__device__ __forceinline__ u3 advection_one(const crp_advection_desc &A, double x, double y, double z) {
+// pow_integer<8> (Common.h:58): ((x^2)^2)^2
+__device__ __forceinline__ double adv_pow8(double x) {
+    const double c = x * x, d = c * c;
+    return d * d;
+}
+
+// One advection field (crp_advection_desc) at (x, y, z) and time t.
+__device__ __forceinline__ u3 advection_one(const crp_advection_desc &A, double x, double y, double z, double t) {
     switch (A.kind) {
+    case CRP_ADVECTION_TIME_SHOCK: {  // OneDimensionalTimeDependentShock::getField (TimeDependentAdvectionField.cpp:16)
+        const double a = 0.5 * (A.v1 + A.v0), b = 0.5 * (A.v1 - A.v0);
+        const double xsh = A.v * (t - A.t0) + A.x0;
+        return {a - b * tanh((x - xsh) / A.length), 0., 0.};
+    }
+    case CRP_ADVECTION_SEDOV_TAYLOR: {  // SedovTaylorBlastWave::getField (TimeDependentAdvectionField.cpp:103)
+        const double r = sqrt(x * x + y * y + z * z);
+        if (t == 0) return adv_radial(x, y, z, 0.);
+        const double ea = pow(A.energy / A.density, 1. / 5.);
+        const double R = ea * pow(t, 2. / 5.);
+        const double vs = 2. / 5. * ea * pow(t, -3. / 5.);
+        const double xi = r / R;
+        const double V = 3 * (adv_pow8(xi) + 1) / (3 * adv_pow8(xi) + 5);
+        const double u = 0.5 * xi * vs * V * (1 - tanh((xi - 1) * R / A.length));
+        return adv_radial(x, y, z, u);
+    }
     case CRP_ADVECTION_UNIFORM:  // UniformAdvectionField::getField (:33)
         return {A.value[0], A.value[1], A.value[2]};
     case CRP_ADVECTION_CONSTANT_SPHERICAL:  // ConstantSphericalAdvectionField::getField (:54)
@@ -64,13 +86,15 @@ __device__ __forceinline__ u3 advection_one(const crp_advection_desc &A, double 
     }
 }
 
-// DiffusionSDE::driftStep's field (DiffusionSDE.cpp:255, :371): the sum of
-// the n fields in order (AdvectionFieldList::getField, :12).
-__device__ __forceinline__ u3 advection_at(const crp_advection_desc *adv, int n, double x, double y, double z) {
-    if (n == 1) return advection_one(adv[0], x, y, z);
+// DiffusionSDE::driftStep's field (DiffusionSDE.cpp:255, :371) at the
+// candidate's time t: one field, or the sum of the n fields in order
+// (AdvectionFieldList::getField, :12, which passes them time 0).
+__device__ __forceinline__ u3 advection_at(const crp_advection_desc *adv, int n, double x, double y, double z,
+                                           double t) {
+    if (n == 1) return advection_one(adv[0], x, y, z, t);
     u3 b = {0., 0., 0.};
     for (int i = 0; i < n; i++) {
-        const u3 a = advection_one(adv[i], x, y, z);
+        const u3 a = advection_one(adv[i], x, y, z, 0.);
         b = {b.x + a.x, b.y + a.y, b.z + a.z};
     }
     return b;

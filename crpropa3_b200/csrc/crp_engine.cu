@@ -198,7 +198,7 @@ crp_status validate_module(const crp_module_desc &m) {
             if (m.n_advection < 0 || m.n_advection > CRP_MAX_ADVECTION)
                 return fail(CRP_ERR_UNSUPPORTED, "DiffusionSDE: at most %d advection fields", CRP_MAX_ADVECTION);
             for (int a = 0; a < m.n_advection; a++)
-                if (m.advection[a].kind < CRP_ADVECTION_UNIFORM || m.advection[a].kind > CRP_ADVECTION_SPHERICAL_SHOCK)
+                if (m.advection[a].kind < CRP_ADVECTION_UNIFORM || m.advection[a].kind > CRP_ADVECTION_SEDOV_TAYLOR)
                     return fail(CRP_ERR_INVALID_ARGUMENT, "DiffusionSDE: unknown advection field kind %d",
                                 m.advection[a].kind);
         } else if (m.n_advection != 0) {

@@ -794,11 +794,11 @@ __device__ __forceinline__ void sde_co_start_try(SdeCo &co, double x, double y, 
 
 // DiffusionSDE::driftStep (DiffusionSDE.cpp:255): the advection drift over
 // the step time h at the step's start position (zero without a field).
-__device__ __forceinline__ void sde_lin_prop(const DevModule &m, double x, double y, double z, double h, double &lx,
-                                             double &ly, double &lz) {
+__device__ __forceinline__ void sde_lin_prop(const DevModule &m, double x, double y, double z, double t, double h,
+                                             double &lx, double &ly, double &lz) {
     lx = ly = lz = 0.;
     if (m.n_adv) {
-        const u3 v = advection_at(m.adv, m.n_adv, x, y, z);
+        const u3 v = advection_at(m.adv, m.n_adv, x, y, z, t);
         lx = v.x * h; ly = v.y * h; lz = v.z * h;
     }
 }
@@ -811,7 +811,7 @@ __device__ __forceinline__ bool sde_co_begin(const DevPlan &P, const DevModule &
     const double h = clipd(c.next, m.min_step, m.max_step) * kInvCLight;
     if (c.q == 0) {
         double lx, ly, lz;
-        sde_lin_prop(m, c.x, c.y, c.z, h, lx, ly, lz);
+        sde_lin_prop(m, c.x, c.y, c.z, c.time, h, lx, ly, lz);
         c.x = fma(c.dx, h * kCLight, c.x + lx); c.y = fma(c.dy, h * kCLight, c.y + ly);
         c.z = fma(c.dz, h * kCLight, c.z + lz);
         set_current_step(c, h * kCLight);
@@ -840,7 +840,7 @@ __device__ __forceinline__ void sde_co_finish(const DevPlan &P, const DevModule 
     double tn = sqrt(ddot(tx, ty, tz, tx, ty, tz));
     tx /= tn; ty /= tn; tz /= tn;
     double lx, ly, lz;
-    sde_lin_prop(m, c.x, c.y, c.z, h, lx, ly, lz);
+    sde_lin_prop(m, c.x, c.y, c.z, c.time, h, lx, ly, lz);
     if (!(tn == tn) || tn == 0.0) {
         if (m.n_adv) {  // only the advection drift
             c.x += lx; c.y += ly; c.z += lz;

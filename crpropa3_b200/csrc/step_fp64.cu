@@ -501,9 +501,9 @@ struct SDE {
     static constexpr bool kReadsStepCount = true;  // the Philox counter
     // DiffusionSDE::process (DiffusionSDE.cpp:47); the advection drift of
     // driftStep (:255) is LinProp = 0 + v_adv(PosIn) h.
-    __device__ static d3 lin_prop(const DevModule &m, d3 pos, double h) {
+    __device__ static d3 lin_prop(const DevModule &m, d3 pos, double h, double t) {
         if (m.n_adv == 0) return mk(0, 0, 0);
-        const u3 v = advection_at(m.adv, m.n_adv, pos.x, pos.y, pos.z);
+        const u3 v = advection_at(m.adv, m.n_adv, pos.x, pos.y, pos.z, t);
         return add(mk(0, 0, 0), muls(mk(v.x, v.y, v.z), h));
     }
     __device__ static void process(const DevPlan &P, const DevModule &m, Cand &c, StepCount &sc) {
@@ -511,7 +511,7 @@ struct SDE {
         double h = clipd(c.next, m.min_step, m.max_step) / kCLight;
         d3 PosIn = mk(c.x, c.y, c.z);
         if (c.q == 0) {
-            d3 p = add(add(PosIn, lin_prop(m, PosIn, h)), muls(muls(mk(c.dx, c.dy, c.dz), h), kCLight));
+            d3 p = add(add(PosIn, lin_prop(m, PosIn, h, c.time)), muls(muls(mk(c.dx, c.dy, c.dz), h), kCLight));
             c.x = p.x; c.y = p.y; c.z = p.z;
             set_current_step(c, h * kCLight);
             c.next = m.max_step;
@@ -547,7 +547,7 @@ struct SDE {
         double tTest = norm(TVec);
         if (tTest != tTest) {
             if (m.n_adv) {  // only the advection drift
-                const d3 p = add(PosIn, lin_prop(m, PosIn, h));
+                const d3 p = add(PosIn, lin_prop(m, PosIn, h, c.time));
                 c.x = p.x; c.y = p.y; c.z = p.z;
             } else {
                 c.x = c.x + c.dx * h * kCLight; c.y = c.y + c.dy * h * kCLight; c.z = c.z + c.dz * h * kCLight;
@@ -562,7 +562,7 @@ struct SDE {
         if (norm(NVec) == 0.) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
         NVec = unit(NVec);
         d3 BVec = unit(cross(TVec, NVec));
-        d3 PO = add(add(PosOut, lin_prop(m, PosIn, h)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
+        d3 PO = add(add(PosOut, lin_prop(m, PosIn, h, c.time)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
         if (isnan(norm(PO))) { c.active = false; c.flags |= CRP_FLAG_NAN; return; }
         s.cursor = 12;  // the cone draw takes the fourth block of the step
         double theta = acos(s_uniform(s, 1, cos(kPi / 2.)));

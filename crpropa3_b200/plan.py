@@ -389,6 +389,35 @@ class ObliqueAdvectionShock:
 
 
 @dataclass
+class OneDimensionalTimeDependentShock:
+    """OneDimensionalTimeDependentShock(v_sh, v1, v0, l_sh)
+    (TimeDependentAdvectionField.cpp:7) with setShockPosition (x_sh0, default
+    0) and setShockTime (t_sh0, default 0): depends on the candidate's time."""
+    v_sh: float
+    v1: float
+    v0: float
+    l_sh: float
+    x_sh0: float = 0.0
+    t_sh0: float = 0.0
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_TIME_SHOCK, v=self.v_sh, v1=self.v1, v0=self.v0, length=self.l_sh,
+                    x0=self.x_sh0, t0=self.t_sh0)
+
+
+@dataclass
+class SedovTaylorBlastWave:
+    """SedovTaylorBlastWave(E0, rho0, l_sh) (TimeDependentAdvectionField.cpp:97):
+    depends on the candidate's time."""
+    energy: float
+    density: float
+    l_sh: float
+
+    def desc(self):
+        return _adv(_abi.ADVECTION_SEDOV_TAYLOR, energy=self.energy, density=self.density, length=self.l_sh)
+
+
+@dataclass
 class SphericalAdvectionShock:
     """SphericalAdvectionShock(origin, r_0, v_0, lambda) (AdvectionField.cpp:432)
     with setRRot (default r_0) and setAzimuthalSpeed (default 0)."""

@@ -22,6 +22,7 @@
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
 #include "crpropa/advectionField/AdvectionField.h"
+#include "crpropa/advectionField/TimeDependentAdvectionField.h"
 #include "crpropa/module/Observer.h"
 #include "crpropa/module/Output.h"
 #include "crpropa/module/PropagationBP.h"
@@ -237,6 +238,16 @@ void addAdvection(const AdvectionField *f, crp_module_desc &d) {
         origin(c->getOrigin());
         A.radius = c->getR0(); A.v = c->getV0(); A.length = c->getLambda();
         A.r_rot = c->getRRot(); A.v_phi = c->getAzimuthalSpeed();
+    } else if (t == typeid(OneDimensionalTimeDependentShock)) {
+        const OneDimensionalTimeDependentShock *c = static_cast<const OneDimensionalTimeDependentShock *>(f);
+        A.kind = CRP_ADVECTION_TIME_SHOCK;
+        A.v = c->getVshock(); A.v1 = c->getV1(); A.v0 = c->getV0(); A.length = c->getShockWidth();
+        A.t0 = c->getShockTime();
+        A.x0 = c->getShockPosition(A.t0);  // x_sh0 + v_sh (t_sh0 - t_sh0)
+    } else if (t == typeid(SedovTaylorBlastWave)) {
+        const SedovTaylorBlastWave *c = static_cast<const SedovTaylorBlastWave *>(f);
+        A.kind = CRP_ADVECTION_SEDOV_TAYLOR;
+        A.energy = c->getEnergy(); A.density = c->getDensity(); A.length = c->getShockWidth();
     } else {
         throw Unsupported(name_of(f) + " (an advection field without a device form)");
     }

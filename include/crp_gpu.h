@@ -371,7 +371,12 @@ enum crp_boundary_kind {
  *   CARTESIAN_SHOCK     compression, v (vUp), length (lShock)
  *   SPHERICAL_SHOCK_1D  radius (rShock), v (vUp), compression, length (lShock), cool_upstream
  *   OBLIQUE_SHOCK       compression, v (vXUp), vy, length (lShock)
- *   SPHERICAL_SHOCK     origin, radius (r_0), v (v_0), length (lambda), r_rot, v_phi */
+ *   SPHERICAL_SHOCK     origin, radius (r_0), v (v_0), length (lambda), r_rot, v_phi
+ *   TIME_SHOCK          v (v_sh), v1, v0, length (l_sh), x0 (x_sh0), t0 (t_sh0)
+ *   SEDOV_TAYLOR        energy (E0), density (rho0), length (l_sh)
+ * The last two depend on the candidate's time at the step's start
+ * (TimeDependentAdvectionField.cpp:16, :103); inside a list they get time 0,
+ * as AdvectionFieldList::getField passes none (AdvectionField.cpp:15). */
 enum crp_advection_kind {
     CRP_ADVECTION_UNIFORM = 1,            /* UniformAdvectionField */
     CRP_ADVECTION_CONSTANT_SPHERICAL = 2, /* ConstantSphericalAdvectionField */
@@ -379,7 +384,9 @@ enum crp_advection_kind {
     CRP_ADVECTION_CARTESIAN_SHOCK = 4,    /* OneDimensionalCartesianShock */
     CRP_ADVECTION_SPHERICAL_SHOCK_1D = 5, /* OneDimensionalSphericalShock */
     CRP_ADVECTION_OBLIQUE_SHOCK = 6,      /* ObliqueAdvectionShock */
-    CRP_ADVECTION_SPHERICAL_SHOCK = 7     /* SphericalAdvectionShock */
+    CRP_ADVECTION_SPHERICAL_SHOCK = 7,    /* SphericalAdvectionShock */
+    CRP_ADVECTION_TIME_SHOCK = 8,         /* OneDimensionalTimeDependentShock */
+    CRP_ADVECTION_SEDOV_TAYLOR = 9        /* SedovTaylorBlastWave */
 };
 #define CRP_MAX_ADVECTION 4
 
@@ -389,6 +396,7 @@ typedef struct crp_advection_desc {
     double value[3];
     double origin[3];
     double v, radius, tau, alpha, compression, length, vy, r_rot, v_phi;
+    double v1, v0, x0, t0, energy, density;
 } crp_advection_desc;
 
 typedef struct crp_module_desc {

@@ -1581,8 +1581,35 @@ static void sde_try(const crp_plan_desc *d, v3 PosIn, v3 *POut, v3 *PosErr, doub
 /* ------------------------------------------------------------ AdvectionField
  * getField of the advection fields (AdvectionField.cpp:12-460), glibc's libm
  * as the reference calls it. */
-static v3 advection_one(const crp_advection_desc *A, v3 pos) {
+/* pow_integer<8> (Common.h:58) */
+static double adv_pow8(double x) {
+    double c = x * x, d = c * c;
+    return (1 * (d * d));
+}
+
+static v3 advection_one(const crp_advection_desc *A, v3 pos, double time) {
     switch (A->kind) {
+    case CRP_ADVECTION_TIME_SHOCK: { /* TimeDependentAdvectionField.cpp:16 */
+        double Aa = 0.5 * (A->v1 + A->v0);
+        double B = 0.5 * (A->v1 - A->v0);
+        double x = pos.x;
+        double xsh = A->v * (time - A->t0) + A->x0;
+        v3 v = mk(0, 0, 0);
+        v.x = Aa - B * tanh((x - xsh) / A->length);
+        return v;
+    }
+    case CRP_ADVECTION_SEDOV_TAYLOR: { /* TimeDependentAdvectionField.cpp:103 */
+        double r = norm(pos);
+        v3 e_r = unit(pos);
+        if (time == 0) return muls(e_r, 0.);
+        double Aa = A->density;
+        double R = pow(A->energy / Aa, 1. / 5.) * pow(time, 2. / 5.);
+        double vs = 2. / 5. * pow(A->energy / Aa, 1. / 5.) * pow(time, -3. / 5.);
+        double xi = r / R;
+        double V = 3 * (adv_pow8(xi) + 1) / (3 * adv_pow8(xi) + 5);
+        double u = 0.5 * xi * vs * V * (1 - tanh((xi - 1) * R / A->length));
+        return muls(e_r, u);
+    }
     case CRP_ADVECTION_UNIFORM: /* :33 */
         return mk(A->value[0], A->value[1], A->value[2]);
     case CRP_ADVECTION_CONSTANT_SPHERICAL: { /* :54 */
@@ -1637,14 +1664,14 @@ static v3 advection_one(const crp_advection_desc *A, v3 pos) {
 
 /* DiffusionSDE::driftStep (DiffusionSDE.cpp:255): LinProp = 0 + v(pos) h;
  * several fields are an AdvectionFieldList (:12), summed in order. */
-static v3 sde_lin_prop(const crp_module_desc *m, v3 pos, double h) {
+static v3 sde_lin_prop(const crp_module_desc *m, v3 pos, double h, double time) {
     if (m->n_advection == 0) return mk(0, 0, 0);
     v3 v;
     if (m->n_advection == 1) {
-        v = advection_one(&m->advection[0], pos);
-    } else {
+        v = advection_one(&m->advection[0], pos, time);
+    } else { /* AdvectionFieldList::getField passes no time: 0 */
         v = mk(0, 0, 0);
-        for (int i = 0; i < m->n_advection; i++) v = add(v, advection_one(&m->advection[i], pos));
+        for (int i = 0; i < m->n_advection; i++) v = add(v, advection_one(&m->advection[i], pos, 0.));
     }
     return add(mk(0, 0, 0), muls(v, h));
 }
@@ -1656,8 +1683,9 @@ static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t
     double h = clipd(c->next, m->min_step, m->max_step) / c_light;
     v3 PosIn = c->pos, DirIn = c->dir;
     (void)DirIn;
+    double time = c->time; /* candidate->getTime() at the step's start */
     if (c->q == 0) {
-        c->pos = add(add(c->pos, sde_lin_prop(m, PosIn, h)), muls(muls(c->dir, h), c_light));
+        c->pos = add(add(c->pos, sde_lin_prop(m, PosIn, h, time)), muls(muls(c->dir, h), c_light));
         set_current_step(c, h * c_light);
         c->next = m->max_step;
         return;
@@ -1692,7 +1720,7 @@ static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t
     v3 TVec = unit(sub(PosOut, PosIn));
     double tTest = norm(TVec);
     if (tTest != tTest) {
-        if (m->n_advection) c->pos = add(c->pos, sde_lin_prop(m, PosIn, h));  /* advection only */
+        if (m->n_advection) c->pos = add(c->pos, sde_lin_prop(m, PosIn, h, time));  /* advection only */
         else c->pos = add(c->pos, muls(muls(c->dir, h), c_light));
         set_current_step(c, h * c_light);
         double newStep = 5 * h * c_light;
@@ -1705,7 +1733,7 @@ static void sde_process(const crp_plan_desc *d, const crp_module_desc *m, cand_t
     if (norm(NVec) == 0.) { c->active = 0; c->flags |= CRP_FLAG_NAN; return; }
     NVec = unit(NVec);
     v3 BVec = unit(cross(TVec, NVec));
-    v3 PO = add(add(PosOut, sde_lin_prop(m, PosIn, h)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
+    v3 PO = add(add(PosOut, sde_lin_prop(m, PosIn, h, time)), muls(add(muls(NVec, NStep), muls(BVec, BStep)), sqrt(h)));
     if (isnan(norm(PO))) { c->active = 0; c->flags |= CRP_FLAG_NAN; return; }
     s.cursor = 12; /* the cone draw uses the fourth block of the step */
     v3 DirOut = stream_cone(&s, TVec, M_PI / 2.);

@@ -55,6 +55,7 @@
 #include "crpropa/module/BreakCondition.h"
 #include "crpropa/module/DiffusionSDE.h"
 #include "crpropa/advectionField/AdvectionField.h"
+#include "crpropa/advectionField/TimeDependentAdvectionField.h"
 #include "crpropa/module/Observer.h"
 #include "crpropa/module/ParticleCollector.h"
 #include "crpropa/module/PropagationBP.h"
@@ -332,6 +333,16 @@ void build_chain(const crp_plan_desc *d, crp_records *rec, Built &b, const Helpe
                             f = s;
                             break;
                         }
+                        case CRP_ADVECTION_TIME_SHOCK: {
+                            OneDimensionalTimeDependentShock *s =
+                                new OneDimensionalTimeDependentShock(A.v, A.v1, A.v0, A.length);
+                            s->setShockPosition(A.x0);
+                            s->setShockTime(A.t0);
+                            f = s;
+                            break;
+                        }
+                        case CRP_ADVECTION_SEDOV_TAYLOR:
+                            f = new SedovTaylorBlastWave(A.energy, A.density, A.length); break;
                         default: throw std::runtime_error("ref_shim: unknown advection field");
                         }
                         fs.push_back(f);

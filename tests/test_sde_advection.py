@@ -2,7 +2,10 @@
 :255; the fields of AdvectionField.cpp:12-460): UniformAdvectionField,
 ConstantSphericalAdvectionField, SphericalAdvectionField, the
 one-dimensional Cartesian and spherical shocks, ObliqueAdvectionShock,
-SphericalAdvectionShock and their list.
+SphericalAdvectionShock, the time-dependent OneDimensionalTimeDependentShock
+and SedovTaylorBlastWave (TimeDependentAdvectionField.cpp:7-130; the
+candidate's time, or 0 inside a list, as AdvectionFieldList passes none) and
+their list.
 
 CPU: the oracle's drift against the reference's own DiffusionSDE, bit for
 bit, where the step draws no random number into the position: neutral
@@ -35,6 +38,11 @@ ADVECTION = {
     "spherical_shock_1d_warm": lambda: [P.OneDimensionalSphericalShock(2 * KPC, 1e7, 4.0, 50 * PC, False)],
     "oblique_shock": lambda: [P.ObliqueAdvectionShock(3.5, 8e6, 2e6, 200 * PC)],
     "spherical_shock": lambda: [P.SphericalAdvectionShock((0.5 * KPC, 0, 0), 3 * KPC, 2e6, 0.4 * KPC, 2 * KPC, 1e5)],
+    "time_shock": lambda: [P.OneDimensionalTimeDependentShock(1e7, 1e7, 2.5e6, 100 * PC, x_sh0=-1 * KPC,
+                                                              t_sh0=1e10)],
+    "sedov_taylor": lambda: [P.SedovTaylorBlastWave(1e44, 4e-32, 100 * PC)],
+    "list_with_time_shock": lambda: [P.UniformAdvectionField((2e5, 0, 0)),
+                                     P.OneDimensionalTimeDependentShock(1e7, 1e7, 2.5e6, 100 * PC, x_sh0=1 * KPC)],
     "list": lambda: [P.UniformAdvectionField((2e5, 0, 0)),
                      P.SphericalAdvectionShock((0, 0, 0), 3 * KPC, 2e6, 0.4 * KPC),
                      P.OneDimensionalCartesianShock(4.0, 1e6, 1 * KPC)],
