@@ -410,6 +410,26 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             return fail(CRP_ERR_INVALID_ARGUMENT, "TF17Field: parameters not set (crp_tf17_defaults)");
         crp_status st = upload(p, &T, 1, &d.tf);
         if (st) return st;
+        // Units.h: kpc = 1e3 parsec, parsec = 648000 / pi au; muG = 1e-6 gauss, gauss = 1e-4 tesla
+        const double kpc = 1e3 * (648000 / M_PI * 149597870700.0), muG = 1e-6 * 1e-4;
+        DevTF17 f32;
+        std::memset(&f32, 0, sizeof(f32));
+        f32.disk_model = T.disk_model; f32.halo_model = T.halo_model;
+        f32.use_disk = T.use_disk; f32.use_halo = T.use_halo;
+        const double L = 1.0 / kpc, B = 1.0 / muG;
+        f32.a_disk = (float)(T.a_disk * kpc * kpc); f32.z1_disk = (float)(T.z1_disk * L);
+        f32.r1_disk = (float)(T.r1_disk * L); f32.b1_disk = (float)(T.b1_disk * B);
+        f32.l_disk = (float)(T.l_disk * L); f32.phi_star_disk = (float)T.phi_star_disk;
+        f32.h_disk = (float)(T.h_disk * L);
+        f32.a_halo = (float)(T.a_halo * kpc * kpc); f32.z1_halo = (float)(T.z1_halo * L);
+        f32.b1_halo = (float)(T.b1_halo * B); f32.l_halo = (float)(T.l_halo * L);
+        f32.phi_star_halo = (float)T.phi_star_halo;
+        f32.cot_p0 = (float)T.cot_p0; f32.h_p = (float)(T.h_p * L); f32.l_p = (float)(T.l_p * L);
+        f32.eps = (float)T.epsilon;
+        f32.inv_kpc = L;
+        f32.muG = (float)muG;
+        st = upload(p, &f32, 1, &d.tf32);
+        if (st) return st;
     } else if (f.kind == CRP_FIELD_SINGLE_MODE) {
         d.mode = f.single_mode;
     } else if (f.kind == CRP_FIELD_KST24) {

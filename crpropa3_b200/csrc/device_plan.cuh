@@ -50,6 +50,17 @@ struct DevJF12 {
     float bdturb5, zdturb, bhturb, rhturb, zhturb;
 };
 
+// TF17Field parameters as floats in kpc and muG for the mixed form (the FP64
+// form reads crp_tf17_desc).
+struct DevTF17 {
+    int disk_model, halo_model, use_disk, use_halo;
+    float a_disk, z1_disk, r1_disk, b1_disk, l_disk, phi_star_disk, h_disk;
+    float a_halo, z1_halo, b1_halo, l_halo, phi_star_halo;
+    float cot_p0, h_p, l_p, eps;
+    double inv_kpc;  // 1/kpc [1/m]
+    float muG;       // [T]
+};
+
 // UF23Field parameters with the two powers the poloidal halo recomputes at
 // every call from model constants, evaluated once on the host with the C
 // library's pow (the reference's own values).
@@ -75,6 +86,7 @@ struct DevComponent {
     const DevUF23 *uf;        // CRP_FIELD_UF23: device copy of the parameters
     const crp_pt11_desc *pt;  // CRP_FIELD_PT11: device copy of the parameters
     const crp_tf17_desc *tf;  // CRP_FIELD_TF17: device copy of the parameters
+    const DevTF17 *tf32;      // and their float form (mixed)
     crp_single_mode_desc mode;  // CRP_FIELD_SINGLE_MODE
     const crp_kst24_desc *kst;  // CRP_FIELD_KST24: device copy of the parameters
     const crp_cmz_desc *cmz;    // CRP_FIELD_CMZ: device copy of the switches and objects

@@ -438,6 +438,106 @@ __device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double 
     return b;
 }
 
+// ---------------------------------------------------------------- TF17Field
+// The mixed form of TF17Field::getField (TF17Field.cpp:197-303): FP32 in kpc
+// and muG, the reference's formulas, with 1 - exp(-x) formed as -expm1(-x)
+// (no cancellation near the axis in single precision).
+__device__ __forceinline__ float tf17f_zscale(const DevTF17 &T, float z) { return 1.f + z * z / T.h_p / T.h_p; }
+
+__device__ __forceinline__ float tf17f_winding(const DevTF17 &T, float r, float z) {
+    return T.cot_p0 * logf(-expm1f(-r / T.l_p) + T.eps) / tf17f_zscale(T, z);
+}
+
+__device__ __forceinline__ float tf17f_radial_scale(const DevTF17 &T, float B1, float phi_star, float z1, float phi,
+                                                   float r, float z) {
+    return B1 * expf(-fabsf(z1) / T.h_disk) * cosf(phi - tf17f_winding(T, r, z) - phi_star);
+}
+
+__device__ __forceinline__ float tf17f_azimuthal(const DevTF17 &T, float r, float z, float B_r, float B_z) {
+    const float r_ = r / T.l_p;
+    const float rscale = r > T.eps ? r_ * expf(-r_) / (-expm1f(-r_)) : 1.f - r_ / 2.f - r_ * r_ / 12.f;
+    const float zs = tf17f_zscale(T, z);
+    return T.cot_p0 / zs * rscale * B_r - 2.f * z * r / (T.h_p * T.h_p) / zs * tf17f_winding(T, r, z) * B_z;
+}
+
+__device__ __noinline__ f3 tf17_field_f(const DevComponent &f, double px, double py, double pz) {
+    const DevTF17 &T = *f.tf32;
+    const float x = (float)(px * T.inv_kpc), y = (float)(py * T.inv_kpc), z = (float)(pz * T.inv_kpc);
+    const float r = sqrtf(x * x + y * y);
+    const float phi = 3.14159265358979f - ((x == 0.f && y == 0.f) ? 0.f : atan2f(y, x));
+    float sinPhi, cosPhi;
+    sincosf(phi, &sinPhi, &cosPhi);
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    if (T.use_disk) {
+        float B_r = 0.f, B_phi = 0.f, B_z = 0.f;
+        if (T.disk_model == CRP_TF17_AD1) {
+            if (r > T.r1_disk) {
+                const float z1z = (1.f + T.a_disk * T.r1_disk * T.r1_disk) / (1.f + T.a_disk * r * r);
+                const float B_r0 = tf17f_radial_scale(T, T.b1_disk, T.phi_star_disk, z1z * z, phi, r, z);
+                B_r = (T.r1_disk / r) * z1z * B_r0;
+                B_z = 2.f * T.a_disk * T.r1_disk * z1z * z / (1.f + T.a_disk * r * r) * B_r0;
+                B_phi = tf17f_azimuthal(T, r, z, B_r, B_z);
+            } else {
+                const float phi1 = tf17f_winding(T, T.r1_disk, z) + T.phi_star_disk;
+                const float B_amp = T.b1_disk * expf(-fabsf(z) / T.h_disk);
+                float s1, c1;
+                sincosf(phi1 - phi, &s1, &c1);
+                B_r = c1 * B_amp;
+                B_phi = s1 * B_amp;
+            }
+        } else if (T.disk_model == CRP_TF17_BD1) {
+            if (r > T.eps) {
+                const float rr = T.r1_disk / r;
+                const float z1z = 5.f / (rr * rr + 4.f / sqrtf(rr));
+                const float B_r0 = tf17f_radial_scale(T, T.b1_disk, T.phi_star_disk, z1z * z, phi, r, z);
+                B_r = rr * z1z * B_r0;
+                B_z = -0.4f * rr / r * z1z * z1z * z * (rr * rr - 1.f / sqrtf(rr)) * B_r0;
+            } else {
+                const float z1z = 5.f * r * r / (T.r1_disk * T.r1_disk);
+                const float B_r0 = tf17f_radial_scale(T, T.b1_disk, T.phi_star_disk, z1z * z, phi, r, z);
+                B_r = 5.f * r / T.r1_disk * B_r0;
+                B_z = -10.f * z / T.r1_disk * B_r0;
+            }
+            B_phi = tf17f_azimuthal(T, r, z, B_r, B_z);
+        } else {  // CRP_TF17_DD1
+            const float zsg = z >= 0.f ? 1.f : -1.f;
+            const float za = fabsf(z);
+            const float wind = tf17f_winding(T, r, z);
+            if (za > T.eps) {
+                const float z1z = T.z1_disk / za;
+                const float rr = 1.5f / (sqrtf(z1z) + 0.5f / z1z);
+                const float F_r = rr * r <= T.l_disk ? 1.f : expf(1.f - rr * r / T.l_disk);
+                const float B_z0 = zsg * T.b1_disk * F_r * cosf(phi - wind - T.phi_star_disk);
+                B_r = -0.5f / 1.5f * rr * rr * rr * r / za * (sqrtf(z1z) - 1.f / z1z) * B_z0;
+                B_z = zsg * rr * rr * B_z0;
+            } else {
+                const float zz = za / T.z1_disk;
+                const float rr = 1.5f * sqrtf(za / T.z1_disk);
+                const float F_r = rr * r <= T.l_disk ? 1.f : expf(1.f - rr * r / T.l_disk);
+                const float B_z0 = zsg * T.b1_disk * F_r * cosf(phi - wind - T.phi_star_disk);
+                B_r = -1.125f * r / T.z1_disk * (1.f - 2.5f * zz * sqrtf(zz)) * B_z0;
+                B_z = zsg * rr * rr * B_z0;
+            }
+            B_phi = tf17f_azimuthal(T, r, z, B_r, B_z);
+        }
+        bx += -(B_r * cosPhi - B_phi * sinPhi);
+        by += B_r * sinPhi + B_phi * cosPhi;
+        bz += B_z;
+    }
+    if (T.use_halo) {
+        const float r1h = (1.f + T.a_halo * T.z1_halo * T.z1_halo) / (1.f + T.a_halo * z * z);
+        float B_z0 = T.b1_halo * expf(-r1h * r / T.l_halo);
+        if (T.halo_model == CRP_TF17_C1) B_z0 *= cosf(phi - tf17f_winding(T, r, z) - T.phi_star_halo);
+        const float B_r = 2.f * T.a_halo * r1h * r1h * r * z / (1.f + T.a_halo * z * z) * B_z0;
+        const float B_z = r1h * r1h * B_z0;
+        const float B_phi = tf17f_azimuthal(T, r, z, B_r, B_z);
+        bx += -(B_r * cosPhi - B_phi * sinPhi);
+        by += B_r * sinPhi + B_phi * cosPhi;
+        bz += B_z;
+    }
+    return f3mk(bx * T.muG, by * T.muG, bz * T.muG);
+}
+
 // Multiply-adds here are written out (fma) so that the result does not
 // depend on how the compiler contracts the expression in each kernel that
 // inlines it: the chunked and persistent launches must agree bit for bit.
@@ -481,10 +581,7 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
         const u3 b = archimedean_field(f.arch, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
     }
-    case CRP_FIELD_TF17: {  // FP64 evaluation, FP32 result
-        const u3 b = tf17_field(*f.tf, x, y, z);
-        return f3mk((float)b.x, (float)b.y, (float)b.z);
-    }
+    case CRP_FIELD_TF17: return tf17_field_f(f, x, y, z);  // FP32 in kpc and muG
     case CRP_FIELD_SINGLE_MODE: {  // FP64 evaluation (the phase reaches many turns), FP32 result
         const u3 b = single_mode_field(f.mode, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
