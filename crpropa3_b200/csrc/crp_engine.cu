@@ -365,6 +365,11 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         h.bdturb5 = (float)(J.b_disk_turb5 * B); h.zdturb = (float)(J.z_disk_turb * L);
         h.bhturb = (float)(J.b_halo_turb * B); h.rhturb = (float)(J.r_halo_turb * L);
         h.zhturb = (float)(J.z_halo_turb * L);
+        h.s_cotp = (float)J.cot_pitch; h.s_cotx = (float)J.cot_theta_x0; h.s_zs = (float)(J.z_s * L);
+        h.s_r1 = (float)(J.r1 * L); h.s_r2 = (float)(J.r2 * L); h.s_r1s = (float)(J.r1s * L);
+        h.s_r2s = (float)(J.r2s * L);
+        for (int i = 0; i < 11; i++) { h.s_phi0[i] = (float)J.phi0_arms[i]; h.s_b[i] = (float)(J.b_arms[i] * B); }
+        for (int i = 0; i < 10; i++) h.s_coeff[i] = (float)(J.phi_coeff[i] * B);
         if (J.use_turbulent) {  // JF12Field::setTurbulentGrid (JF12Field.cpp:118)
             if (!f.grid.values)
                 return fail(CRP_ERR_INVALID_ARGUMENT, "JF12Field: No turbulent field set (use_turbulent without a grid)");
@@ -436,6 +441,35 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         if (!(f.kst24.kpc > 0) || !(f.kst24.gauss > 0))
             return fail(CRP_ERR_INVALID_ARGUMENT, "KST24Field: parameters not set (crp_kst24_defaults)");
         crp_status st = upload(p, &f.kst24, 1, &d.kst);
+        if (st) return st;
+        const crp_kst24_desc &K = f.kst24;
+        DevKST24 k32;
+        std::memset(&k32, 0, sizeof(k32));
+        k32.north_b = (float)K.north_b; k32.north_zmin = (float)K.north_zmin; k32.north_zmax = (float)K.north_zmax;
+        k32.north_rmin = (float)K.north_rmin; k32.north_rmax = (float)K.north_rmax;
+        k32.south_b = (float)K.south_b; k32.south_zmin = (float)K.south_zmin; k32.south_zmax = (float)K.south_zmax;
+        k32.south_rmin = (float)K.south_rmin; k32.south_rmax = (float)K.south_rmax;
+        k32.x_b = (float)K.x_b; k32.x_rmin = (float)K.x_rmin; k32.x_rmax = (float)K.x_rmax;
+        k32.tan_x = (float)std::tan(K.x_theta_rad); k32.sin_x = (float)std::sin(K.x_theta_rad);
+        k32.cos_x = (float)std::cos(K.x_theta_rad);
+        k32.lb_b = (float)K.lb_b; k32.lb_rmin = (float)K.lb_rmin; k32.lb_dr = (float)K.lb_dr;
+        k32.lb_x0 = (float)K.lb_x0; k32.lb_y0 = (float)K.lb_y0; k32.lb_z0 = (float)K.lb_z0;
+        for (int a = 0; a < 3; a++) k32.lb_dir[a] = (float)K.lb_dir[a];
+        k32.lb_ampl = (float)(1 + (K.lb_rmin * K.lb_rmin) / (2 * K.lb_rmin * K.lb_dr + K.lb_dr * K.lb_dr));
+        for (int a = 0; a < 5; a++) {
+            const crp_kst24_arm &A = K.arms[a];
+            DevKST24Arm &B = k32.arms[a];
+            const double pr = A.pitch_deg * M_PI / 180.;
+            B.b = (float)A.b; B.k = (float)std::tan(pr); B.cos_pitch = (float)std::cos(pr);
+            B.sin_pitch = (float)std::sin(pr); B.phi0 = (float)(A.phi0_deg * M_PI / 180.);
+            B.arc_div = (float)(A.arc_div_deg * M_PI / 180.);
+            B.x_shift = (float)A.x_shift; B.y_shift = (float)A.y_shift;
+            B.arc_radius1 = (float)A.arc_radius1; B.arc_radius2 = (float)A.arc_radius2; B.arc_eps = (float)A.arc_eps;
+            B.rmin = (float)A.rmin; B.rmax = (float)A.rmax; B.zmin = (float)A.zmin; B.zmax = (float)A.zmax;
+        }
+        k32.inv_kpc = 1.0 / K.kpc;
+        k32.gauss = (float)K.gauss;
+        st = upload(p, &k32, 1, &d.kst32);
         if (st) return st;
     } else if (f.kind == CRP_FIELD_CMZ) {
         if (!(f.cmz.gauss > 0))

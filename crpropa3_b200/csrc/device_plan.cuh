@@ -48,6 +48,9 @@ struct DevJF12 {
     float bring, hdisk, wdisk, bnorth, bsouth, rnorth, rsouth, whalo, z0;
     float bx, sinthx0, costhx0, tanthx0, rxc, rx, sinp, cosp, tan90mp, sqrtbeta;
     float bdturb5, zdturb, bhturb, rhturb, zhturb;
+    // JF12FieldSolenoidal (variant CRP_JF12_SOLENOIDAL), kpc and muG
+    float s_cotp, s_cotx, s_zs, s_r1, s_r2, s_r1s, s_r2s;
+    float s_phi0[11], s_b[11], s_coeff[10];
 };
 
 // TF17Field parameters as floats in kpc and muG for the mixed form (the FP64
@@ -59,6 +62,22 @@ struct DevTF17 {
     float cot_p0, h_p, l_p, eps;
     double inv_kpc;  // 1/kpc [1/m]
     float muG;       // [T]
+};
+
+// KST24Field parameters as floats in the model's units (kpc, gauss) for the
+// mixed form, with each arm's trigonometric constants formed once.
+struct DevKST24Arm {
+    float b, k, cos_pitch, sin_pitch, phi0, arc_div, x_shift, y_shift;
+    float arc_radius1, arc_radius2, arc_eps, rmin, rmax, zmin, zmax;
+};
+struct DevKST24 {
+    float north_b, north_zmin, north_zmax, north_rmin, north_rmax;
+    float south_b, south_zmin, south_zmax, south_rmin, south_rmax;
+    float x_b, x_rmin, x_rmax, tan_x, sin_x, cos_x;
+    float lb_b, lb_rmin, lb_dr, lb_x0, lb_y0, lb_z0, lb_dir[3], lb_ampl;
+    DevKST24Arm arms[5];
+    double inv_kpc;  // 1/kpc [1/m]
+    float gauss;     // [T]
 };
 
 // UF23Field parameters with the two powers the poloidal halo recomputes at
@@ -89,6 +108,7 @@ struct DevComponent {
     const DevTF17 *tf32;      // and their float form (mixed)
     crp_single_mode_desc mode;  // CRP_FIELD_SINGLE_MODE
     const crp_kst24_desc *kst;  // CRP_FIELD_KST24: device copy of the parameters
+    const DevKST24 *kst32;      // and their float form (mixed)
     const crp_cmz_desc *cmz;    // CRP_FIELD_CMZ: device copy of the switches and objects
     crp_archimedean_desc arch;  // CRP_FIELD_ARCHIMEDEAN_SPIRAL
 };

@@ -314,6 +314,89 @@ __device__ __forceinline__ float jf_r_negx_f(const DevJF12 &J, float r, float ph
     return r_negx;
 }
 
+// JF12FieldSolenoidal's disk (JF12FieldSolenoidal.cpp:115) in FP32, kpc and
+// muG: the arm of (r, phi) found at r1 along the spiral, the transition
+// polynomial and its derivative (:197, :219), the azimuth integral H.
+__device__ __forceinline__ f3 jf12s_disk_f(const DevJF12 &J, float r, float z, float phi, float sinPhi,
+                                           float cosPhi) {
+    if (!((J.s_r1 < r) && (r < J.s_r2))) return f3mk(0.f, 0.f, 0.f);
+    const float lf = jf_logistic_f(z, J.hdisk, J.wdisk);
+    float phi1 = phi - logf(r / J.s_r1) * J.s_cotp;
+    float s1, c1;
+    sincosf(phi1, &s1, &c1);
+    phi1 = atan2f(s1, c1);
+    int idx = 1;
+    while (idx < 10 && phi1 < J.s_phi0[idx]) idx += 1;
+    const float hint = phi1 * J.s_b[idx] + J.s_coeff[idx];
+    const float mag1 = J.s_b[idx];
+    float p, q;
+    if ((r > J.s_r1s) && (r < J.s_r2s)) {
+        p = J.s_r1 / r;
+        q = 0.f;
+    } else {
+        float ra = J.s_r1, rb = J.s_r1s;
+        if (r >= J.s_r2s) { ra = J.s_r2; rb = J.s_r2s; }
+        const float fakt = (ra / rb - 2.f) / ((ra - rb) * (ra - rb));
+        p = (J.s_r1 / rb) * (2.f - r / rb + fakt * (r - rb) * (r - rb));
+        q = (J.s_r1 / rb) * (2.f - 2.f * r / rb + fakt * (3.f * r * r - 4.f * r * rb + rb * rb));
+    }
+    const float br = p * mag1 * J.sinp;
+    const float bphi = p * mag1 * J.cosp - q * hint * J.sinp;
+    const float s = 1.f - lf;
+    return f3mk((br * cosPhi - bphi * sinPhi) * s, (br * sinPhi + bphi * cosPhi) * s, 0.f);
+}
+
+// JF12FieldSolenoidal's X field (JF12FieldSolenoidal.cpp:131) in FP32, kpc and muG.
+__device__ __forceinline__ f3 jf12s_x_f(const DevJF12 &J, float r, float z, float sinPhi, float cosPhi) {
+    const float zS = J.s_zs, rXc = J.rxc, rX = J.rx, bX = J.bx, tanT = J.tanthx0, az = fabsf(z);
+    const float rc = rXc + az / tanT, r0c = rXc + zS / tanT;
+    if (az > zS) {
+        if (r == 0.f) {
+            const float a = 1.f + az * J.s_cotx / rXc;
+            return f3mk(0.f, 0.f, bX / (a * a));
+        }
+        float bMagX, sT, cT;
+        if (r < rc) {
+            const float rp = r * rXc / rc;
+            bMagX = bX * expf(-rp / rX) * (rXc / rc) * (rXc / rc);
+            const float th = atanf(az / (r - rp));
+            sincosf(th, &sT, &cT);
+        } else {
+            const float rp = r - az / tanT;
+            bMagX = bX * expf(-rp / rX) * (rp / r);
+            sT = J.sinthx0;
+            cT = J.costhx0;
+        }
+        const float zs = z < 0.f ? -bMagX : bMagX;
+        return f3mk(zs * cT * cosPhi, zs * cT * sinPhi, bMagX * sT);
+    }
+    float r0 = r / (1.f - 1.f / (2.f * (zS + rXc * tanT)) * (zS - z * z / zS));
+    float f;
+    if (r0 >= r0c) {
+        r0 = r + 1.f / (2.f * tanT) * (zS - z * z / zS);
+        f = 1.f + 1.f / (2.f * r * tanT / zS) * (1.f - (z / zS) * (z / zS));
+    } else {
+        const float g = 1.f - 1.f / (2.f + 2.f * (rXc * tanT / zS)) * (1.f - (z / zS) * (z / zS));
+        f = 1.f / (g * g);
+    }
+    float br0, bz0;
+    if (r0 < r0c) {
+        const float rp = r0 * rXc / r0c;
+        float st, ct;
+        sincosf(atanf(zS / (r0 - rp)), &st, &ct);
+        const float m = bX * expf(-rp / rX) * (rXc / r0c) * (rXc / r0c);
+        br0 = m * ct;
+        bz0 = m * st;
+    } else {
+        const float rp = r0 - zS / tanT;
+        const float m = bX * expf(-rp / rX) * (rp / r0);
+        br0 = m * J.costhx0;
+        bz0 = m * J.sinthx0;
+    }
+    const float br = z / zS * f * br0;
+    return f3mk(br * cosPhi, br * sinPhi, bz0 * f);
+}
+
 // regular field [muG] at (x, y, z) [kpc]
 __device__ f3 jf12_regular_f(const DevJF12 &J, float x, float y, float z) {
     f3 b = f3mk(0.f, 0.f, 0.f);
@@ -326,7 +409,13 @@ __device__ f3 jf12_regular_f(const DevJF12 &J, float x, float y, float z) {
         cosPhi = x * ir;
         sinPhi = y * ir;
     }
-    if (J.d.use_disk && r > 3.f) {
+    const bool sol = J.d.variant == CRP_JF12_SOLENOIDAL;
+    if (sol) {
+        if (J.d.use_disk) {
+            const f3 d = jf12s_disk_f(J, r, z, (x == 0.f && y == 0.f) ? 0.f : atan2f(y, x), sinPhi, cosPhi);
+            b.x += d.x; b.y += d.y;
+        }
+    } else if (J.d.use_disk && r > 3.f) {
         const float lf = jf_logistic_f(z, J.hdisk, J.wdisk);
         if (r < 5.f) {
             const float bMag = J.bring * __fdividef(5.f, r) * (1.f - lf);
@@ -354,7 +443,12 @@ __device__ f3 jf12_regular_f(const DevJF12 &J, float x, float y, float z) {
         b.x += -bMagH * sinPhi;
         b.y += bMagH * cosPhi;
     }
-    if (J.d.use_x && outside1) {
+    if (sol) {
+        if (J.d.use_x) {
+            const f3 xf = jf12s_x_f(J, r, z, sinPhi, cosPhi);
+            b.x += xf.x; b.y += xf.y; b.z += xf.z;
+        }
+    } else if (J.d.use_x && outside1) {
         float bMagX, sinT, cosT;
         const float rc = J.rxc + __fdividef(az, J.tanthx0);
         if (r < rc) {
@@ -418,15 +512,7 @@ __device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double 
         const float s = jf12_turbulent_strength_f(J, xs, ys, zs) * unit;
         b = f3mk(g.x * s, g.y * s, g.z * s);
     }
-    if ((J.d.use_striated || J.d.use_regular) && J.d.variant == CRP_JF12_SOLENOIDAL) {
-        // JF12FieldSolenoidal: FP64 evaluation, FP32 result
-        double m = 1.;
-        if (J.d.use_striated) m = 1. + J.d.sqrt_beta * (double)__ldg(f.mod.values + gi_nearest_cell(f.mod, x, y, z));
-        const u3 r = jf12_regular_fp64(J.d, x, y, z);
-        b.x += (float)(r.x * m);
-        b.y += (float)(r.y * m);
-        b.z += (float)(r.z * m);
-    } else if (J.d.use_striated || J.d.use_regular) {
+    if (J.d.use_striated || J.d.use_regular) {
         float m = unit;
         if (J.d.use_striated)
             m *= 1.f + J.sqrtbeta * __ldg(f.mod.values + gi_nearest_cell(f.mod, x, y, z));
@@ -538,6 +624,109 @@ __device__ __noinline__ f3 tf17_field_f(const DevComponent &f, double px, double
     return f3mk(bx * T.muG, by * T.muG, bz * T.muG);
 }
 
+// ---------------------------------------------------------------- KST24Field
+// The mixed form of KST24Field::getField (KST24Field.cpp:128-374): FP32 in
+// the model's units (kpc, gauss), each arm's trigonometric constants formed
+// once on the host.
+__device__ __forceinline__ void kst24f_toroidal(float x, float y, float z, float B, float zmin, float zmax,
+                                                float rmin, float rmax, f3 &v) {
+    if ((z <= zmin) || (zmax <= z)) return;
+    const float cR = sqrtf(x * x + y * y);
+    if ((rmin <= cR) && (cR <= rmax)) {
+        const float th = atan2f(y, x);
+        float s, c;
+        sincosf(th, &s, &c);
+        v.x += B * s;
+        v.y += -B * c;
+    }
+}
+
+__device__ __forceinline__ void kst24f_x(const DevKST24 &K, float x, float y, float z, f3 &v) {
+    const float sign = z < 0.f ? -1.f : 1.f;
+    if (fabsf(z) > 10.f) return;
+    const float cR = sqrtf(x * x + y * y);
+    const float cR_0 = cR - z * sign * K.tan_x;
+    if ((cR_0 < K.x_rmin) || (K.x_rmax < cR_0)) return;
+    const float m = K.x_b * (cR_0 / cR);
+    const float th = atan2f(y, x);
+    float s, c;
+    sincosf(th, &s, &c);
+    v.x += m * c * sign * K.sin_x;
+    v.y += m * s * sign * K.sin_x;
+    v.z += m * K.cos_x;
+}
+
+__device__ __forceinline__ void kst24f_arm(const DevKST24Arm &A, float x, float y, float z, f3 &v) {
+    if ((z < A.zmin) || (A.zmax < z)) return;
+    const float p0 = x + A.x_shift, p1 = y + A.y_shift;
+    const float r = sqrtf(p0 * p0 + p1 * p1);
+    if ((r < A.rmin) || (A.rmax < r)) return;
+    const float a_kpc = 3.f, k = A.k, twopi = 6.28318530717959f;
+    const float phi = atan2f(p1, p0);
+    int nn = (int)floorf((logf(r / a_kpc) - k * (phi + A.phi0)) / (twopi * k));
+    float r1 = a_kpc * expf(k * (phi + A.phi0 + twopi * nn));
+    const float r2 = r1 * expf(k * twopi);
+    if (fabsf(r - r1) > fabsf(r - r2)) {
+        r1 = r2;
+        nn++;
+    }
+    float s, c;
+    sincosf(phi, &s, &c);
+    float xi = r1 * c, yi = r1 * s;
+    float d1x = k * xi - yi, d1y = k * yi + xi;
+    float dn = rsqrtf(d1x * d1x + d1y * d1y);
+    d1x *= dn; d1y *= dn;
+    const float dphi = -((xi - p0) * d1x + (yi - p1) * d1y) / (r1 / A.cos_pitch);
+    r1 = a_kpc * expf(k * (phi + A.phi0 + dphi + twopi * nn));
+    sincosf(phi + dphi, &s, &c);
+    xi = r1 * c; yi = r1 * s;
+    d1x = k * xi - yi; d1y = k * yi + xi;
+    dn = rsqrtf(d1x * d1x + d1y * d1y);
+    d1x *= dn; d1y *= dn;
+    const float d1 = sqrtf((xi - p0) * (xi - p0) + (yi - p1) * (yi - p1));
+    const float L1 = r1 / A.sin_pitch, L1s = 5.f / A.sin_pitch;
+    const float gp = A.arc_radius2 * (1.f + (L1 - L1s) * A.arc_div);
+    const float gz = A.arc_radius1 * (1.f + (L1 - L1s) * A.arc_div);
+    float arp = (A.arc_radius2 < gp) ? gp : A.arc_radius2;
+    float arz = (A.arc_radius1 < gz) ? gz : A.arc_radius1;
+    if (arp > 1.2f) arp = 1.2f;
+    if (arz > 1.2f) arz = 1.2f;
+    const float d_at = sqrtf(powf(fabsf(d1 / arp), A.arc_eps) + powf(fabsf(z / arz), A.arc_eps));
+    if ((d_at > 1.f) || (d_at < 0.f)) return;
+    const float sf = (A.arc_radius1 * A.arc_radius2) / (arp * arz);
+    v.x += A.b * d1x * sf;
+    v.y += A.b * d1y * sf;
+}
+
+__device__ __noinline__ f3 kst24_field_f(const DevComponent &f, double px, double py, double pz) {
+    const DevKST24 &K = *f.kst32;
+    const float x = (float)(px * K.inv_kpc), y = (float)(py * K.inv_kpc), z = (float)(pz * K.inv_kpc);
+    f3 v = f3mk(0.f, 0.f, 0.f);
+    if (z > K.north_zmin) {
+        kst24f_toroidal(x, y, z, K.north_b, K.north_zmin, K.north_zmax, K.north_rmin, K.north_rmax, v);
+        kst24f_x(K, x, y, z, v);
+    } else if (z < K.south_zmax) {
+        kst24f_toroidal(x, y, z, K.south_b, K.south_zmin, K.south_zmax, K.south_rmin, K.south_rmax, v);
+        kst24f_x(K, x, y, z, v);
+    } else {
+        const float ex = x - K.lb_x0, ey = y - K.lb_y0, ez = z - K.lb_z0;
+        const float cR = sqrtf(ex * ex + ey * ey + ez * ez);
+        if (cR < K.lb_rmin + K.lb_dr) {  // the Local Bubble: its shell field only
+            if (!((cR < K.lb_rmin) || (K.lb_rmin + K.lb_dr < cR))) {
+                const float ux = ex / cR, uy = ey / cR, uz = ez / cR;
+                const float ct = ux * K.lb_dir[0] + uy * K.lb_dir[1] + uz * K.lb_dir[2];
+                const float m = K.lb_b * K.lb_ampl;
+                v = f3mk(m * (K.lb_dir[0] - ux * ct), m * (K.lb_dir[1] - uy * ct), m * (K.lb_dir[2] - uz * ct));
+            }
+        } else {
+#pragma unroll 1
+            for (int i = 0; i < 5; i++) kst24f_arm(K.arms[i], x, y, z, v);
+            kst24f_x(K, x, y, z, v);
+        }
+    }
+    return f3mk(v.x * K.gauss, v.y * K.gauss, v.z * K.gauss);
+}
+
 // Multiply-adds here are written out (fma) so that the result does not
 // depend on how the compiler contracts the expression in each kernel that
 // inlines it: the chunked and persistent launches must agree bit for bit.
@@ -586,10 +775,7 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
         const u3 b = single_mode_field(f.mode, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
     }
-    case CRP_FIELD_KST24: {  // FP64 evaluation, FP32 result
-        const u3 b = kst24_field(*f.kst, x, y, z);
-        return f3mk((float)b.x, (float)b.y, (float)b.z);
-    }
+    case CRP_FIELD_KST24: return kst24_field_f(f, x, y, z);  // FP32 in kpc and gauss
     case CRP_FIELD_CMZ: {  // FP64 evaluation, FP32 result
         const u3 b = cmz_field(*f.cmz, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
