@@ -394,6 +394,21 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
         h.d = U;
         h.c_pol = std::pow(U.poloidal_a / U.poloidal_z, U.poloidal_p);  // UF23Field.cpp:392-393
         h.a0p = std::pow(U.poloidal_a, U.poloidal_p);
+        h.b1 = (float)U.disk_b1; h.b2 = (float)U.disk_b2; h.b3 = (float)U.disk_b3;
+        h.disk_h = (float)U.disk_h; h.disk_w = (float)U.disk_w;
+        h.ph1 = (float)U.disk_phase1; h.ph2 = (float)U.disk_phase2; h.ph3 = (float)U.disk_phase3;
+        h.sinp = (float)U.sin_pitch; h.cosp = (float)U.cos_pitch;
+        h.inv_tanp = (float)(1.0 / U.tan_pitch); h.tanp = (float)U.tan_pitch;
+        h.spur_center = (float)U.spur_center; h.spur_length = (float)U.spur_length;
+        h.spur_inv_width = U.spur_width != 0 ? (float)(1.0 / U.spur_width) : 0.f;
+        h.tbn = (float)U.toroidal_bn; h.tbs = (float)U.toroidal_bs; h.tr = (float)U.toroidal_r;
+        h.tw = (float)U.toroidal_w; h.tz = (float)U.toroidal_z;
+        h.pb = (float)U.poloidal_b; h.pp = (float)U.poloidal_p; h.pr = (float)U.poloidal_r;
+        h.pw = (float)U.poloidal_w; h.pa = (float)U.poloidal_a; h.pzz = (float)U.poloidal_z;
+        h.inv_pp = (float)(1.0 / U.poloidal_p);
+        h.twist = (float)U.twisting_time; h.r2max = (float)U.max_radius_squared;
+        h.muG = (float)U.microgauss;
+        h.inv_kpc = 1.0 / U.kpc;
         crp_status st = upload(p, &h, 1, &d.uf);
         if (st) return st;
     } else if (f.kind == CRP_FIELD_PT11) {

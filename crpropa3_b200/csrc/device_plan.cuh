@@ -87,6 +87,14 @@ struct DevUF23 {
     crp_uf23_desc d;
     double c_pol;  // pow(A / Z, P)
     double a0p;    // pow(A, P)
+    // the mixed form's floats, same units (kpc, microgauss, radians)
+    float b1, b2, b3, disk_h, disk_w, ph1, ph2, ph3, sinp, cosp, inv_tanp, tanp;
+    float spur_center, spur_length, spur_inv_width;
+    float tbn, tbs, tr, tw, tz;
+    float pa, pb, pp, pr, pw, pzz, inv_pp;  // poloidal A, B, P, R, W, Z and 1/P
+    float twist, r2max;
+    float muG;       // [T]
+    double inv_kpc;  // 1/kpc [1/m]
 };
 
 struct DevComponent {

@@ -524,6 +524,144 @@ __device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double 
     return b;
 }
 
+// ---------------------------------------------------------------- UF23Field
+// The mixed form of UF23Field::getField (UF23Field.cpp:269-558): FP32 in the
+// model's units (kpc, microgauss), the reference's formulas, with three
+// rewritings that keep FP32 digits: 1 - exp(-x) as -expm1(-x); the azimuth
+// difference acos(cos a cos b + sin a sin b) as |a - b| reduced to [0, pi]
+// (the same angle, without acos's loss near 0); and the poloidal halo's
+// t1 + t0 as 4 A^P r^P / (t1 - t0) where t0 < 0 (the same value, from
+// (t1 + t0)(t1 - t0) = 4 A^P r^P, without the cancellation).
+constexpr float kUffMinNormal = 1.17549435e-38f;  // numeric_limits<float>::min()
+constexpr float kUffTwoPi = 6.28318530717958648f;
+
+__device__ __forceinline__ float uff_sigmoid(float x, float x0, float w) { return 1.f / (1.f + expf(-(x - x0) / w)); }
+
+__device__ __forceinline__ float uff_delta_phi(float a, float b) { return fabsf(remainderf(a - b, kUffTwoPi)); }
+
+// getSpiralField (UF23Field.cpp:510)
+__device__ __forceinline__ f3 uff_spiral(const DevUF23 &W, float x, float y, float z) {
+    const float r2 = x * x + y * y;
+    if (r2 == 0.f) return f3mk(0.f, 0.f, 0.f);
+    const float r = sqrtf(r2);
+    const float phi = atan2f(y, x);
+    const float hdz = 1.f - uff_sigmoid(fabsf(z), W.disk_h, W.disk_w);
+    const float rFacI = uff_sigmoid(r, 5.f, 0.5f);
+    const float rFacO = 1.f - uff_sigmoid(r, 20.f, 0.5f);
+    const float rFac = r > 1e-8f ? -expm1f(-r2) / r : r;
+    const float fac = hdz * 5.f * rFac * rFacO * rFacI;
+    const float phi0 = phi - logf(r / 5.f) * W.inv_tanp;
+    const float b = W.b1 * cosf(phi0 - W.ph1) + W.b2 * cosf(2.f * (phi0 - W.ph2)) +
+                    W.b3 * cosf(3.f * (phi0 - W.ph3));
+    const float br = b * fac * W.sinp, bphi = b * fac * W.cosp, cp = x / r, sp = y / r;
+    return f3mk(br * cp - bphi * sp, br * sp + bphi * cp, 0.f);
+}
+
+// getSpurField (UF23Field.cpp:453)
+__device__ __forceinline__ f3 uff_spur(const DevUF23 &W, float x, float y, float z, float r) {
+    const float rRef = 8.2f;
+    if (r < kUffMinNormal) return f3mk(0.f, 0.f, 0.f);
+    float phi = atan2f(y, x);
+    if (phi < 0.f) phi += kUffTwoPi;
+    const float phiRef = W.ph1;
+    int iBest = -2;
+    float bestDist = -1.f;
+    for (int i = -1; i <= 1; ++i) {
+        const float rr = rRef * expf((phi - phiRef + i * kUffTwoPi) * W.tanp);
+        if (bestDist < 0.f || fabsf(r - rr) < bestDist) {
+            bestDist = fabsf(r - rr);
+            iBest = i;
+        }
+    }
+    if (iBest != 0) return f3mk(0.f, 0.f, 0.f);
+    const float phi0 = phi - logf(r / rRef) * W.inv_tanp;
+    const float delta = uff_delta_phi(phiRef, phi0) * W.spur_inv_width;
+    const float B = W.b1 * expf(-0.5f * delta * delta);
+    const float wS = 5.f * (3.14159265358979f / 180.f);
+    const float gS = 1.f - uff_sigmoid(uff_delta_phi(W.spur_center, phi), W.spur_length, wS);
+    const float hd = 1.f - uff_sigmoid(fabsf(z), W.disk_h, W.disk_w);
+    const float bS = rRef / r * B * hd * gS;
+    const float br = bS * W.sinp, bphi = bS * W.cosp, cp = x / r, sp = y / r;
+    return f3mk(br * cp - bphi * sp, br * sp + bphi * cp, 0.f);
+}
+
+// getToroidalHaloField (UF23Field.cpp:361)
+__device__ __forceinline__ f3 uff_toroidal(const DevUF23 &W, float x, float y, float z, float r) {
+    const float absZ = fabsf(z);
+    const float b0 = z >= 0.f ? W.tbn : W.tbs;
+    const float bPhi = b0 * (1.f - uff_sigmoid(r, W.tr, W.tw)) * uff_sigmoid(absZ, W.disk_h, W.disk_w) *
+                       expf(-absZ / W.tz);
+    const float cp = r > kUffMinNormal ? x / r : 1.f, sp = r > kUffMinNormal ? y / r : 0.f;
+    return f3mk(-bPhi * sp, bPhi * cp, 0.f);
+}
+
+// getPoloidalHaloField (UF23Field.cpp:385), scaled so that no power of r,
+// |z| or A is formed (A^P and t0^2 overflow FP32 for the models' constants):
+// with R = (r/A)^P, Zc = (|z|/Z)^P (c |z|^P = A^P Zc) and m = max(0, ln R,
+// ln Zc), t0 = A^P e^m t0s and t1 = A^P e^m t1s, where t0s = e^-m + Zc e^-m -
+// R e^-m and t1s = sqrt(t0s^2 + 4 R e^-2m) have every term in [0, 1].  Then,
+// with s = t1s + t0s and g = ln(2 e^-m / s) / P: a = r e^g, a / rOverA =
+// r e^2g and rOverA^(P-2) (a^P + A^P) / t1 = e^2g (s / 2 + R e^-m) / t1s.
+__device__ __forceinline__ f3 uff_poloidal(const DevUF23 &W, int model, float x, float y, float z, float r) {
+    const float ln2 = 0.693147180559945309f, az = fabsf(z);
+    const float lr = W.pp * logf(r / W.pa), lz = W.pp * logf(az / W.pzz);  // ln R, ln Zc (-inf at 0)
+    const float m = fmaxf(0.f, fmaxf(lr, lz));
+    const float eR = expf(lr - m), eZ = expf(lz - m), q = expf(lr - 2.f * m);
+    const float t0 = expf(-m) + eZ - eR;
+    const float t1 = sqrtf(t0 * t0 + 4.f * q);
+    const float s = t0 >= 0.f ? t1 + t0 : 4.f * q / (t1 - t0);  // (t1 + t0)(t1 - t0) = 4 R e^-2m
+    const float g = (ln2 - m - logf(s)) * W.inv_pp;
+    const float a = r * expf(g);
+    const float radial = model == CRP_UF23_EXPX ? expf(-a / W.pr) : 1.f - uff_sigmoid(a, W.pr, W.pw);
+    const float Bzz = W.pb * radial, e2g = expf(2.f * g);
+    const float signZ = z < 0.f ? -1.f : 1.f;
+    // c |z|^(P-1) / t1 = Zc e^-m / (|z| t1s)
+    const float zt = az > 0.f ? eZ / (az * t1) : 0.f;
+    const float Br = Bzz * r * e2g * signZ * zt;
+    const float Bz = Bzz * e2g * (0.5f * s + eR) / t1;
+    if (r < kUffMinNormal) return f3mk(0.f, 0.f, Bz);
+    return f3mk(Br * (x / r), Br * (y / r), Bz);
+}
+
+// getTwistedHaloField (UF23Field.cpp:318)
+__device__ __forceinline__ f3 uff_twisted(const DevUF23 &W, float x, float y, float z, float r) {
+    const float cp = r > kUffMinNormal ? x / r : 1.f, sp = r > kUffMinNormal ? y / r : 0.f;
+    const f3 bX = uff_poloidal(W, CRP_UF23_TWISTX, x, y, z, r);
+    const float bR = bX.x * cp + bX.y * sp, bZ = bX.z;
+    float bPhi = 0.f;
+    if (W.twist != 0.f && r != 0.f) {
+        // -240 km/s in kpc/Myr
+        constexpr float v0 = (float)(-240 * (1 / 3.0856775807e+16) / (1 / (1e6 * 60 * 60 * 24 * 365.25)));
+        const float r0 = 1.6f, z0 = 10.f;
+        const float e = expf(-r / r0), fr = -expm1f(-r / r0);
+        const float t0 = expf(2.f * fabsf(z) / z0);
+        const float gz = 2.f / (1.f + t0);
+        const float signZ = z < 0.f ? -1.f : 1.f;
+        const float deltaZ = -signZ * v0 * fr / z0 * t0 * gz * gz;
+        const float deltaR = v0 * (e / r0 - fr / r) * gz;
+        bPhi = (bZ * deltaZ + bR * deltaR) * W.twist;
+    }
+    return f3mk(bR * cp - bPhi * sp, bR * sp + bPhi * cp, bZ);
+}
+
+// UF23Field::getField (UF23Field.cpp:269) and operator() (:277), [T]
+__device__ __noinline__ f3 uf23_field_f(const DevComponent &f, double px, double py, double pz) {
+    const DevUF23 &W = *f.uf;
+    const int model = W.d.model;
+    const float x = (float)(px * W.inv_kpc), y = (float)(py * W.inv_kpc), z = (float)(pz * W.inv_kpc);
+    if (x * x + y * y + z * z > W.r2max) return f3mk(0.f, 0.f, 0.f);
+    const float r = sqrtf(x * x + y * y);
+    const f3 d = model == CRP_UF23_SPUR ? uff_spur(W, x, y, z, r) : uff_spiral(W, x, y, z);
+    f3 h;
+    if (model == CRP_UF23_TWISTX) {
+        h = uff_twisted(W, x, y, z, r);
+    } else {
+        const f3 t = uff_toroidal(W, x, y, z, r), p = uff_poloidal(W, model, x, y, z, r);
+        h = f3mk(t.x + p.x, t.y + p.y, t.z + p.z);
+    }
+    return f3mk((d.x + h.x) * W.muG, (d.y + h.y) * W.muG, (d.z + h.z) * W.muG);
+}
+
 // ---------------------------------------------------------------- TF17Field
 // The mixed form of TF17Field::getField (TF17Field.cpp:197-303): FP32 in kpc
 // and muG, the reference's formulas, with 1 - exp(-x) formed as -expm1(-x)
@@ -758,10 +896,7 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     case CRP_FIELD_PLANE_WAVE: return plane_wave_field(f.pw, x, y, z, sh);
     case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
     case CRP_FIELD_JF12: return jf12_field_f(f, x, y, z);
-    case CRP_FIELD_UF23: {  // FP64 evaluation (the poloidal halo's powers), FP32 result
-        const u3 b = uf23_field(*f.uf, x, y, z);
-        return f3mk((float)b.x, (float)b.y, (float)b.z);
-    }
+    case CRP_FIELD_UF23: return uf23_field_f(f, x, y, z);  // FP32 in kpc and microgauss
     case CRP_FIELD_PT11: {  // FP64 evaluation, FP32 result
         const u3 b = pt11_field(*f.pt, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
