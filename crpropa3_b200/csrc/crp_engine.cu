@@ -421,6 +421,23 @@ crp_status build_component(crp_plan *p, const crp_field_component &f, DevCompone
             return fail(CRP_ERR_INVALID_ARGUMENT, "PT11Field: parameters not set (crp_pt11_defaults)");
         crp_status st = upload(p, &T, 1, &d.pt);
         if (st) return st;
+        // Units.h: kpc = 1e3 parsec, parsec = 648000 / pi au; muG = 1e-6 gauss, gauss = 1e-4 tesla
+        const double kpc = 1e3 * (648000 / M_PI * 149597870700.0), muG = 1e-6 * 1e-4;
+        const double L = 1.0 / kpc, B = 1.0 / muG;
+        DevPT11 f32;
+        std::memset(&f32, 0, sizeof(f32));
+        f32.use_ass = T.use_ass; f32.use_bss = T.use_bss; f32.use_halo = T.use_halo;
+        f32.r_sun = (float)(T.r_sun * L); f32.r_c = (float)(T.r_c * L); f32.z0_d = (float)(T.z0_d * L);
+        f32.b0_d = (float)(T.b0_d * B);
+        f32.z0_h = (float)(T.z0_h * L); f32.r0_h = (float)(T.r0_h * L); f32.b0_hn = (float)(T.b0_hn * B);
+        f32.b0_hs = (float)(T.b0_hs * B); f32.z11_h = (float)(T.z11_h * L); f32.z12_h = (float)(T.z12_h * L);
+        f32.sinp = (float)T.sin_pitch; f32.cosp = (float)T.cos_pitch;
+        f32.cotp = T.sin_pitch != 0 ? (float)(T.cos_pitch / T.sin_pitch) : 0.f;
+        f32.phi = (float)T.phi; f32.cos_phi = (float)T.cos_phi;
+        f32.inv_kpc = L;
+        f32.muG = (float)muG;
+        st = upload(p, &f32, 1, &d.pt32);
+        if (st) return st;
     } else if (f.kind == CRP_FIELD_TF17) {
         const crp_tf17_desc &T = f.tf17;
         if (T.disk_model < CRP_TF17_AD1 || T.disk_model > CRP_TF17_DD1 || T.halo_model < CRP_TF17_C0 ||

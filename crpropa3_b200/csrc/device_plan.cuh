@@ -64,6 +64,16 @@ struct DevTF17 {
     float muG;       // [T]
 };
 
+// PT11Field parameters as floats in kpc and muG for the mixed form (the FP64
+// form reads crp_pt11_desc), cot of the pitch formed once.
+struct DevPT11 {
+    int use_ass, use_bss, use_halo, pad;
+    float r_sun, r_c, z0_d, b0_d, z0_h, r0_h, b0_hn, b0_hs, z11_h, z12_h;
+    float sinp, cosp, cotp, phi, cos_phi;
+    double inv_kpc;  // 1/kpc [1/m]
+    float muG;       // [T]
+};
+
 // KST24Field parameters as floats in the model's units (kpc, gauss) for the
 // mixed form, with each arm's trigonometric constants formed once.
 struct DevKST24Arm {
@@ -112,6 +122,7 @@ struct DevComponent {
     const DevJF12 *jf;  // CRP_FIELD_JF12: device copy of the parameters
     const DevUF23 *uf;        // CRP_FIELD_UF23: device copy of the parameters
     const crp_pt11_desc *pt;  // CRP_FIELD_PT11: device copy of the parameters
+    const DevPT11 *pt32;      // and their float form (mixed)
     const crp_tf17_desc *tf;  // CRP_FIELD_TF17: device copy of the parameters
     const DevTF17 *tf32;      // and their float form (mixed)
     crp_single_mode_desc mode;  // CRP_FIELD_SINGLE_MODE

@@ -524,6 +524,42 @@ __device__ __noinline__ f3 jf12_field_f(const DevComponent &f, double x, double 
     return b;
 }
 
+// ---------------------------------------------------------------- PT11Field
+// The mixed form of PT11Field::getField (PT11Field.cpp:80-128): FP32 in kpc
+// and muG, the reference's formulas; r = 0 divides by zero as the reference
+// does.
+__device__ __noinline__ f3 pt11_field_f(const DevComponent &f, double px, double py, double pz) {
+    const DevPT11 &P = *f.pt32;
+    const float x = (float)(px * P.inv_kpc), y = (float)(py * P.inv_kpc), z = (float)(pz * P.inv_kpc);
+    const float r = sqrtf(x * x + y * y);
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    if (P.use_ass || P.use_bss) {
+        // theta = pi - phi, phi of Vector3::getPhi (0 on the axis)
+        const float theta = 3.14159265358979f - ((x == 0.f && y == 0.f) ? 0.f : atan2f(y, x));
+        const float cos_theta = -x / r, sin_theta = y / r;
+        bx = -(P.sinp * cos_theta - P.cosp * sin_theta);
+        by = -(-P.sinp * sin_theta - P.cosp * cos_theta);
+        float m = cosf(theta - P.cotp * logf(r / P.r_sun) + P.phi);
+        if (P.use_ass) m = fabsf(m);
+        const float rr = r < P.r_c ? P.r_c : r;  // std::max(r, R_c)
+        m *= P.b0_d * P.r_sun / rr / P.cos_phi * expf(-fabsf(z) / P.z0_d);
+        bx *= m;
+        by *= m;
+        bz = -0.f * m;  // NaN with m on the axis, as in the reference
+    }
+    if (P.use_halo) {
+        const float az = fabsf(z);
+        float m = z > 0.f ? P.b0_hn : -P.b0_hs;
+        const float z1 = az < P.z0_h ? P.z11_h : P.z12_h;
+        const float v = (az - P.z0_h) / z1;
+        m *= r / P.r0_h * expf(1.f - r / P.r0_h) / (1.f + v * v);
+        bx += m * (-y / r);
+        by += m * (x / r);
+        bz += m * 0.f;
+    }
+    return f3mk(bx * P.muG, by * P.muG, bz * P.muG);
+}
+
 // ---------------------------------------------------------------- UF23Field
 // The mixed form of UF23Field::getField (UF23Field.cpp:269-558): FP32 in the
 // model's units (kpc, microgauss), the reference's formulas, with three
@@ -897,10 +933,7 @@ __device__ __forceinline__ f3 component_field(const DevComponent &f, double x, d
     case CRP_FIELD_UNIFORM: return f3mk((float)f.uniform[0], (float)f.uniform[1], (float)f.uniform[2]);
     case CRP_FIELD_JF12: return jf12_field_f(f, x, y, z);
     case CRP_FIELD_UF23: return uf23_field_f(f, x, y, z);  // FP32 in kpc and microgauss
-    case CRP_FIELD_PT11: {  // FP64 evaluation, FP32 result
-        const u3 b = pt11_field(*f.pt, x, y, z);
-        return f3mk((float)b.x, (float)b.y, (float)b.z);
-    }
+    case CRP_FIELD_PT11: return pt11_field_f(f, x, y, z);  // FP32 in kpc and muG
     case CRP_FIELD_ARCHIMEDEAN_SPIRAL: {  // FP64 evaluation, FP32 result
         const u3 b = archimedean_field(f.arch, x, y, z);
         return f3mk((float)b.x, (float)b.y, (float)b.z);
