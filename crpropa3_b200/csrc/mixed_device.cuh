@@ -1445,7 +1445,7 @@ template <int FS> using CKFixed = CK<FS, 1>;
 template <int FS> using CKAdaptive = CK<FS, 2>;
 
 template <template <int> class Prop, int FS, int CS>
-__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_chunk_kernel(DevPlan P, DevState s, uint64_t n,
+__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_chunk_kernel(const __grid_constant__ DevPlan P, DevState s, uint64_t n,
                                                           int max_steps, uint64_t step_cap,
                                                           DevCounters *cnt, DevRecords rec,
                                                           const uint32_t *perm, uint32_t *perm_out) {

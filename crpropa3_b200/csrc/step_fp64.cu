@@ -592,7 +592,7 @@ template <int FS> using CKFixed = CK<FS, 1>;
 template <int FS> using CKAdaptive = CK<FS, 2>;
 
 template <template <int> class Prop, int FS, int CS>
-__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_chunk_kernel(DevPlan P, DevState s, uint64_t n,
+__global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_chunk_kernel(const __grid_constant__ DevPlan P, DevState s, uint64_t n,
                                                          int max_steps, uint64_t step_cap,
                                                          DevCounters *cnt, DevRecords rec,
                                                          const uint32_t *perm, uint32_t *perm_out) {
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_chunk_ke
 
 template <template <int> class Prop, int FS, int CS>
 __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) fp64_persistent_kernel(
-    DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
+    const __grid_constant__ DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
     // the queue is written only between launches (advance_kernel)
     const DevQueue q = *a.q;
     const uint32_t *pending_in = q.cur ? a.list_b : a.list_a;
@@ -632,7 +632,7 @@ cudaError_t launch_persistent_prop(const DevPlan &P, const DevState &s, const Pe
     return cudaGetLastError();
 }
 
-__global__ void fp64_field_kernel(DevPlan P, uint64_t n, const double *pos, double *out) {
+__global__ void fp64_field_kernel(const __grid_constant__ DevPlan P, uint64_t n, const double *pos, double *out) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     d3 b = field_at<FS_GENERIC>(P, mk(pos[i], pos[n + i], pos[2 * n + i]));

@@ -30,7 +30,7 @@ namespace {
 // pw_field >= 0: index of the plan's plane-wave component, whose mode
 // table the block stages in shared memory (dynamic, 48 B per mode) first.
 template <int FS>
-__global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_kernel(DevPlan P, DevState s, uint64_t n,
+__global__ void __launch_bounds__(128, CRP_SDE_COOP_MIN_BLOCKS) mixed_sde_coop_kernel(const __grid_constant__ DevPlan P, DevState s, uint64_t n,
                                                                int max_steps, uint64_t step_cap,
                                                                DevCounters *cnt, DevRecords rec,
                                                                const uint32_t *perm, uint32_t *perm_out,
@@ -171,7 +171,7 @@ __device__ __forceinline__ void pw_batch(const float4 *tab, int npairs, const do
 
 template <int FS>
 __global__ void __launch_bounds__(kBatchThreads, CRP_SDE_BATCH_MIN_BLOCKS)
-mixed_sde_batch_kernel(DevPlan P, DevState s, uint64_t n, int max_steps, uint64_t step_cap, DevCounters *cnt,
+mixed_sde_batch_kernel(const __grid_constant__ DevPlan P, DevState s, uint64_t n, int max_steps, uint64_t step_cap, DevCounters *cnt,
                        DevRecords rec, const uint32_t *perm, uint32_t *perm_out, int pw_field) {
     extern __shared__ __align__(16) unsigned char smem[];
     const DevComponent &pwc = P.fields[pw_field];
@@ -280,7 +280,7 @@ mixed_sde_batch_kernel(DevPlan P, DevState s, uint64_t n, int max_steps, uint64_
 
 template <template <int> class Prop, int FS, int CS>
 __global__ void __launch_bounds__(128, MinBlocks<Prop<FS>>::value) mixed_persistent_kernel(
-    DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
+    const __grid_constant__ DevPlan P, DevState s, PersistentArgs a, DevCounters *cnt, DevRecords rec) {
     // the queue is written only between launches (advance_kernel)
     const DevQueue q = *a.q;
     const uint32_t *pending_in = q.cur ? a.list_b : a.list_a;
@@ -311,7 +311,7 @@ cudaError_t launch_persistent_prop(const DevPlan &P, const DevState &s, const Pe
     return cudaGetLastError();
 }
 
-__global__ void mixed_field_kernel(DevPlan P, uint64_t n, const double *pos, double *out) {
+__global__ void mixed_field_kernel(const __grid_constant__ DevPlan P, uint64_t n, const double *pos, double *out) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     f3 b = field_at<FS_GENERIC>(P, pos[i], pos[n + i], pos[2 * n + i]);
